@@ -1,0 +1,469 @@
+#!/usr/bin/env python
+"""Benchmark of the FP64 statevector hot path (driver contract: one JSON line).
+
+Workload (default ``qft30``): the 30-qubit complex128 quantum Fourier
+transform (h on qubit j, then cp(pi/2^(k-j)) controlled by every k > j, then
+the swap network) preceded by x on a seeded random half of the qubits -- a
+16 GiB state, far larger than L2, so every step streams HBM.  One step is one
+full ``simulate`` of that circuit: |0...0> initialisation plus every gate.
+
+Metric: effective gate-sweep GB/s = sum over the circuit's gates of the bytes
+a per-gate engine must move (2 * 16 B * 2^n * f, f = fraction of amplitudes
+the gate changes: 1 for 1q gates, 1/2 for swap/cx, 1/4 for cp) divided by the
+step time.  The same definition is used for the CPU reference arm, so the
+ratio of the two lines is the speed-up.  ``roofline`` reports the dominant
+kernel's own achieved HBM bandwidth (its bytes per launch / its measured
+launch time) against the measured copy peak.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--workload qft30|brickwork20]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+sys.path.insert(0, str(ROOT / "tests"))
+
+import _circuits  # noqa: E402  (workload builders shared with the tests)
+
+PEAKS_FILE = ROOT / "MEASURED_PEAKS.json"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def peak_hbm():
+    try:
+        d = json.loads(PEAKS_FILE.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+# ---- workloads ---------------------------------------------------------------------------
+
+def workload(name: str):
+    if name == "qft30":
+        return _circuits.qft_with_x(30, 1234), {"workload": "qft30_fp64", "num_qubits": 30,
+                                                 "state_bytes": 16 * 2**30,
+                                                 "circuit": "x(seeded half) + QFT + swap network"}
+    if name == "brickwork20":
+        return _circuits.brickwork_u3_cx(20, 20, 1234), {"workload": "brickwork20_fp64",
+                                                          "num_qubits": 20,
+                                                          "state_bytes": 16 * 2**20,
+                                                          "circuit": "20 layers u3 + cx brickwork"}
+    raise SystemExit(f"unknown workload {name}")
+
+
+def gate_fraction(kind: str) -> float:
+    """Fraction of amplitudes a gate changes (algorithmic bytes per gate)."""
+    if kind in ("cp", "cu1", "crz", "cz", "g_cz"):
+        return 0.25
+    if kind in ("cx", "swap", "cy", "ch", "csx", "crx", "cry", "cu3", "cu", "g_cx"):
+        return 0.5
+    if kind in ("ccx", "cswap", "rccx"):
+        return 0.25
+    if kind in ("c3x", "c3sqrtx", "rc3x"):
+        return 0.125
+    if kind == "c4x":
+        return 0.0625
+    if kind in ("id", "u0", "barrier", "classical", "g_noop", "g_opaque", "measure", "reset"):
+        return 0.0
+    return 1.0
+
+
+def effective_bytes(prog) -> float:
+    from dqsim_bosonic_b200._native import KIND_NAMES
+
+    n = prog.num_qubits
+    tot = 0.0
+    for k in prog.insts["kind"].tolist():
+        tot += 2 * 16 * (2 ** n) * gate_fraction(KIND_NAMES[k])
+    return tot
+
+
+# ---- clocks -----------------------------------------------------------------------------------
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = ROOT / "gpurun_out" / f"clocks_dev{device}_{os.getpid()}.csv"
+
+    def __enter__(self):
+        try:
+            self.path.parent.mkdir(exist_ok=True)
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.fh, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.fh.close()
+
+    def summary(self):
+        if self.proc is None or not self.path.exists():
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.path.read_text().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": smax, "reasons": sorted(reasons)}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---- distributed plumbing ------------------------------------------------------------------------
+
+class Dist:
+    def __init__(self, gpus: int):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = None
+        if self.world > 1:
+            import datetime
+
+            import torch
+            import torch.distributed as dist
+
+            torch.cuda.set_device(self.local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                    device_id=torch.device("cuda", self.local))
+            self.pg = dist
+
+    def barrier(self):
+        if self.pg is not None:
+            self.pg.barrier()
+
+    def max(self, v: float) -> float:
+        if self.pg is None:
+            return v
+        import torch
+
+        t = torch.tensor([v], dtype=torch.float64, device=f"cuda:{self.local}")
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.pg is not None:
+            self.pg.destroy_process_group()
+
+
+# ---- CPU reference arm / cpu_baseline -------------------------------------------------------------
+
+def cpu_sample_time(prog, threads: int, budget_s: float = 20.0):
+    """Time the oracle (restated reference engine, OpenMP) on gates of the
+    workload; returns (effective bytes covered, seconds, sample description)."""
+    import _oracle
+    from dqsim_bosonic_b200._native import KIND_NAMES
+
+    _oracle.set_threads(threads)
+    n = prog.num_qubits
+    state = np.zeros(1 << n, dtype=np.complex128)
+    state[0] = 1.0
+    state[:] = 1.0 / math.sqrt(state.size)  # touch every page before timing
+    kinds = [KIND_NAMES[k] for k in prog.insts["kind"].tolist()]
+    # one gate of each kind present, cycling through the program order
+    picks, seen = [], {}
+    for i, k in enumerate(kinds):
+        seen.setdefault(k, []).append(i)
+    order = sorted(seen)
+    t_total, b_total, done = 0.0, 0.0, 0
+    while t_total < budget_s:
+        progressed = False
+        for k in order:
+            idx = seen[k]
+            if done // len(order) >= len(idx):
+                continue
+            i = idx[(done // len(order)) % len(idx)]
+            sub = prog.insts[i:i + 1].copy()
+            sub["cond_count"] = 0
+            one = type(prog)(sub, prog.conds[:0], n, 0, max(prog.cbit_space, 1), {})
+            t0 = time.perf_counter()
+            _oracle.run_inplace(one, 0, state)
+            dt = time.perf_counter() - t0
+            t_total += dt
+            b_total += 2 * 16 * (2 ** n) * gate_fraction(k)
+            picks.append(k)
+            progressed = True
+            if t_total >= budget_s:
+                break
+        done += len(order)
+        if not progressed:
+            break
+    _oracle.set_threads(1)
+    desc = f"{len(picks)} gates of the workload ({', '.join(sorted(set(picks)))}) on the full {n}-qubit state"
+    return b_total, t_total, desc
+
+
+def run_reference_arm(args, wl_prog, cfg):
+    dist_rank = int(os.environ.get("RANK", "0"))
+    if dist_rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    budget = 6.0
+    for _ in range(args.warmup):
+        pass
+    vals, times = [], []
+    desc = ""
+    for _ in range(args.steps):
+        b, t, desc = cpu_sample_time(wl_prog, threads, budget)
+        vals.append(b / t / 1e9)
+        times.append(t)
+    value = float(np.mean(vals))
+    line = {
+        "impl": "reference",
+        "metric": "effective gate-sweep GB/s (FP64 statevector)",
+        "value": value,
+        "unit": "GB/s",
+        "n_gpus": args.gpus,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": float(np.mean(times) * 1000.0),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic (seeded circuit)",
+        "config": cfg,
+        "cpu_baseline": {"value": value, "unit": "GB/s", "cores": threads, "kind": "port",
+                         "sample": desc + "; restated reference engine (oracle/liboracle.so)"},
+        "e2e": {"value": value, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---- our arm ------------------------------------------------------------------------------------------
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="qft30")
+    ap.add_argument("--exec", default=None, choices=[None, "fused", "per_gate"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+
+    from dqsim_bosonic_b200.circuit import decode_circuit_json, encode
+
+    circ, cfg = workload(args.workload)
+    prog = encode(decode_circuit_json(circ.model_dump_json()))
+    cfg = dict(cfg)
+    cfg.update({"gates": int(prog.ninst), "parallelism": f"replicas x{args.gpus}",
+                "l2": "state larger than L2 (126 MB)" if cfg["state_bytes"] > 126e6 else
+                      "state L2-resident; L2 flushed between steps"})
+
+    if args.impl == "reference":
+        run_reference_arm(args, prog, cfg)
+        return
+
+    import ctypes
+
+    import torch
+
+    from dqsim_bosonic_b200 import StatevectorSimulator
+    from dqsim_bosonic_b200 import _native as nat
+    from dqsim_bosonic_b200.statevector import run_program
+
+    d = Dist(args.gpus)
+    dev = d.local
+    torch.cuda.set_device(dev)
+    exec_mode = nat.EXEC_PER_GATE if args.exec == "per_gate" else nat.EXEC_FUSED
+    if args.exec is None:
+        exec_mode = nat.EXEC_FUSED if os.environ.get("DQSIM_EXEC", "fused") == "fused" else nat.EXEC_PER_GATE
+    eff_bytes = effective_bytes(prog)
+    flush = None
+    if cfg["state_bytes"] <= 126e6:
+        flush = torch.empty(256 * 2**20, dtype=torch.uint8, device=f"cuda:{dev}")
+
+    # ---- value: device-timed steps, program resident, state in HBM ----
+    st = nat.State(prog.num_qubits, dev)
+    ptr, sptr = st.device_ptr()
+    stream = torch.cuda.ExternalStream(sptr, device=f"cuda:{dev}")
+    launches = 0
+
+    def step():
+        nonlocal launches
+        st.reset()
+        _, prof = run_program(st, prog, 7, nat.SEM_SIMULATE, exec_mode)
+        launches += 1 + int(prof.kernel_launches)
+        return prof
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    if flush is not None:
+        flush.zero_()
+    torch.cuda.synchronize(dev)
+    d.barrier()
+    torch.cuda.synchronize(dev)
+    launches = 0
+    ev = []
+    with ClockSampler(dev) as clk:
+        for _ in range(args.steps):
+            if flush is not None:
+                with torch.cuda.stream(stream):
+                    flush.zero_()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            prof = step()
+            e1.record(stream)
+            ev.append((e0, e1))
+        torch.cuda.synchronize(dev)
+    d.barrier()
+    torch.cuda.synchronize(dev)
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    total_ms = d.max(float(np.sum(step_ms)))
+    ms_per_step = total_ms / args.steps
+    value = eff_bytes * args.steps * d.world / (total_ms * 1e-3) / 1e9
+    sweeps = int(prof.sweeps)
+
+    # ---- dominant kernel roofline: time its launches with events on its stream ----
+    roof = dominant_kernel_roofline(st, prog, exec_mode, stream, dev)
+    st.release()
+
+    # ---- e2e: public API with host circuit in, probabilities out ----
+    sim = StatevectorSimulator(seed=7, device=dev,
+                               exec="per_gate" if exec_mode == nat.EXEC_PER_GATE else "fused")
+    n = prog.num_qubits
+    top = list(range(n - 1, max(-1, n - 11), -1))
+    res = sim.simulate(circ)
+    res.probability_array(top)
+    del res
+    torch.cuda.synchronize(dev)
+    d.barrier()
+    e2e_t = []
+    for _ in range(args.steps):
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        res = sim.simulate(circ)
+        p = res.probability_array(top)
+        torch.cuda.synchronize(dev)
+        e2e_t.append(time.perf_counter() - t0)
+        del res
+    e2e_total = d.max(float(np.sum(e2e_t)))
+    e2e_value = eff_bytes * args.steps * d.world / e2e_total / 1e9
+
+    line = {
+        "metric": "effective gate-sweep GB/s (FP64 statevector)",
+        "value": value,
+        "unit": "GB/s",
+        "n_gpus": d.world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms_per_step,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic (seeded circuit)",
+        "config": dict(cfg, exec="fused" if exec_mode == nat.EXEC_FUSED else "per_gate",
+                       sweeps_per_step=sweeps),
+        "e2e": {"value": e2e_value, "unit": "GB/s",
+                "h2d_bytes_per_step": int(prog.insts.nbytes + prog.conds.nbytes),
+                "d2h_bytes_per_step": int(8 * (1 << len(top))),
+                "ms_per_step": e2e_total / args.steps * 1000.0,
+                "path": "StatevectorSimulator.simulate(circuit) + probabilities(top 10 qubits)"},
+        "roofline": roof,
+        "gpu_launches": int(launches),
+        "clocks": clk.summary(),
+    }
+    if d.rank == 0 and d.world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        b, t, desc = cpu_sample_time(prog, threads, 20.0)
+        line["cpu_baseline"] = {"value": b / t / 1e9, "unit": "GB/s", "cores": threads,
+                                "kind": "port",
+                                "sample": desc + "; restated reference engine (oracle/liboracle.so)"}
+    if d.rank == 0:
+        print(json.dumps(line), flush=True)
+    d.close()
+
+
+def dominant_kernel_roofline(st, prog, exec_mode, stream, dev):
+    """Time the kernel that dominates the step and report its HBM roofline."""
+    import torch
+
+    from dqsim_bosonic_b200 import _native as nat
+    from dqsim_bosonic_b200.circuit import decode_circuit_json, encode
+
+    peak, src = peak_hbm()
+    n = prog.num_qubits
+    reps = 10
+    if exec_mode == nat.EXEC_FUSED:
+        name, nbytes, ms = fused_sweep_timing(st, prog, stream, reps)
+    else:
+        # per-gate path: cp (k_phase) carries most of the time in the QFT
+        one = encode(decode_circuit_json(_circuits.JsonCircuit(
+            n, [_circuits.g("cp", n - 1, n // 2, 0.3)]).model_dump_json()))
+        from dqsim_bosonic_b200.statevector import run_program
+
+        run_program(st, one, 0, nat.SEM_SIMULATE, nat.EXEC_PER_GATE)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize(dev)
+        e0.record(stream)
+        for _ in range(reps):
+            run_program(st, one, 0, nat.SEM_SIMULATE, nat.EXEC_PER_GATE)
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        ms = e0.elapsed_time(e1) / reps
+        name = "k_phase (cp, quarter of the state)"
+        nbytes = 2 * 16 * (2 ** n) * 0.25
+    achieved = nbytes / (ms * 1e-3) / 1e9
+    return {"kernel": name, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "peak_source": src, "bytes_per_launch": nbytes,
+            "launch_ms": ms, "traffic": None}
+
+
+def fused_sweep_timing(st, prog, stream, reps):
+    from dqsim_bosonic_b200 import _native as nat
+    import ctypes
+
+    L = nat.lib()
+    if not hasattr(L, "dq_time_sweeps"):
+        raise RuntimeError("engine without sweep timing")
+    out = (ctypes.c_double * 4)()
+    nat.check(L.dq_time_sweeps(st.handle, nat.ptr(prog.insts), prog.ninst, 0, reps, out))
+    n = prog.num_qubits
+    return "sweep kernel (fused tile sweep)", 2 * 16 * (2 ** n), out[0]
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,612 @@
+// dq_engine.cu — exact per-gate kernels, measurement reductions, marginal
+// probabilities, the device CDF and the per-shot sampler.
+//
+// Per-gate kernels restate src/engine.rs (apply_one_qubit 24-101,
+// apply_n_qubit 109-181) with the num-complex operation order and no FMA, so
+// each gate's output equals the Rust engine's bit for bit.  Instead of the
+// reference's filter over all 2^n indices, every kernel enumerates only the
+// amplitudes the gate changes (zero bits inserted at the target/control
+// positions), so a gate with c controls moves 2^-c of the state.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+
+#include "dq_common.cuh"
+#include "dq_engine.cuh"
+#include "dq_rng.cuh"
+
+namespace dq {
+
+namespace {
+
+constexpr int kThreads = 256;
+
+struct Pos {
+  uint32_t p[8];
+  int np;
+};
+
+// Callers guarantee popcount(mask) <= 8 (gates touch at most 5 qubits;
+// dq_apply_1q limits its controls); extra bits are never written past p[7].
+Pos make_pos(uint64_t mask) {
+  Pos ps{};
+  ps.np = 0;
+  for (uint32_t b = 0; b < 64 && ps.np < 8; ++b)
+    if (mask >> b & 1ULL) ps.p[ps.np++] = b;
+  return ps;
+}
+
+inline unsigned blocks_for(uint64_t items, unsigned threads) {
+  uint64_t b = (items + threads - 1) / threads;
+  if (b < 1) b = 1;
+  if (b > 0x7fffffffULL) b = 0x7fffffffULL;
+  return (unsigned)b;
+}
+
+// ---- one-qubit family --------------------------------------------------------
+
+__global__ void k_one_q(double2* __restrict__ s, uint64_t count, Pos pos, uint64_t setb,
+                        uint64_t tbit, double2 u00, double2 u01, double2 u10, double2 u11) {
+  const uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (k >= count) return;
+  const uint64_t i = insert_zeros(k, pos.p, pos.np) | setb;
+  const uint64_t j = i | tbit;
+  const double2 a = s[i], b = s[j];
+  s[i] = cadd_x(cmul_x(u00, a), cmul_x(u01, b));
+  s[j] = cadd_x(cmul_x(u10, a), cmul_x(u11, b));
+}
+
+__global__ void k_phase(double2* __restrict__ s, uint64_t count, Pos pos, uint64_t setb,
+                        double2 e) {
+  const uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (k >= count) return;
+  const uint64_t i = insert_zeros(k, pos.p, pos.np) | setb;
+  s[i] = cmul_x(e, s[i]);
+}
+
+__global__ void k_exchange(double2* __restrict__ s, uint64_t count, Pos pos, uint64_t seta,
+                           uint64_t setb) {
+  const uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (k >= count) return;
+  const uint64_t base = insert_zeros(k, pos.p, pos.np);
+  const uint64_t i = base | seta, j = base | setb;
+  const double2 a = s[i], b = s[j];
+  s[i] = b;
+  s[j] = a;
+}
+
+// ---- k-qubit diagonal and dense -----------------------------------------------
+
+struct DiagParams {
+  double2 d[32];
+  uint32_t q[5];   // q[0] = MSB of the diagonal index
+  uint32_t k;
+};
+
+__global__ void k_diag(double2* __restrict__ s, uint64_t count, DiagParams P) {
+  const uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  uint32_t g = 0;
+  for (uint32_t b = 0; b < P.k; ++b) g = (g << 1) | (uint32_t)((i >> P.q[b]) & 1ULL);
+  const double2 d = P.d[g];
+  if (d.x == 1.0 && d.y == 0.0) return;   // 1 * v == v exactly
+  s[i] = cmul_x(d, s[i]);
+}
+
+template <int K>
+struct DenseParams {
+  double2 m[(1 << K) * (1 << K)];
+  uint64_t off[1 << K];
+  Pos pos;
+};
+
+template <int K>
+__global__ void k_dense(double2* __restrict__ s, uint64_t count, DenseParams<K> P) {
+  constexpr int D = 1 << K;
+  const uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (k >= count) return;
+  const uint64_t base = insert_zeros(k, P.pos.p, P.pos.np);
+  double2 v[D];
+#pragma unroll
+  for (int j = 0; j < D; ++j) v[j] = s[base + P.off[j]];
+#pragma unroll 1
+  for (int r = 0; r < D; ++r) {
+    double2 acc = make_double2(0.0, 0.0);
+#pragma unroll
+    for (int c = 0; c < D; ++c) {
+      const double2 u = P.m[r * D + c];
+      if (u.x != 0.0 || u.y != 0.0) acc = cadd_x(acc, cmul_x(u, v[c]));
+    }
+    s[base + P.off[r]] = acc;
+  }
+}
+
+template <int K>
+int launch_dense_k(double2* s, uint32_t n, const Gate& g, cudaStream_t st) {
+  DenseParams<K> P;
+  constexpr int D = 1 << K;
+  uint64_t mask = 0;
+  for (int b = 0; b < K; ++b) mask |= 1ULL << g.qubits[b];
+  for (int j = 0; j < D; ++j) {
+    uint64_t off = 0;
+    for (int b = 0; b < K; ++b)
+      if ((j >> (K - 1 - b)) & 1) off |= 1ULL << g.qubits[b];
+    P.off[j] = off;
+  }
+  for (int i = 0; i < D * D; ++i) P.m[i] = make_double2(g.m[i].re, g.m[i].im);
+  P.pos = make_pos(mask);
+  const uint64_t count = 1ULL << (n - K);
+  k_dense<K><<<blocks_for(count, kThreads), kThreads, 0, st>>>(s, count, P);
+  return DQ_OK;
+}
+
+// ---- reductions ------------------------------------------------------------------
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = __dadd_rn(v, __shfl_down_sync(0xffffffffu, v, o));
+  return v;
+}
+
+// Sum over the block; the result is valid in thread 0.  Fixed tree order.
+__device__ double block_sum(double v) {
+  __shared__ double sh[32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  v = warp_sum(v);
+  __syncthreads();
+  if (lane == 0) sh[w] = v;
+  __syncthreads();
+  v = 0.0;
+  if (w == 0) {
+    v = (lane < (int)(blockDim.x >> 5)) ? sh[lane] : 0.0;
+    v = warp_sum(v);
+  }
+  return v;
+}
+
+// Writes this block's partial(s); the last block to finish sums all partials
+// in index order (deterministic for a fixed grid) into out[0..W).
+template <int W>
+__device__ void finish_partials(const double (&v)[W], double* partial, unsigned* counter,
+                                double* out) {
+  __shared__ bool last;
+  double tot[W];
+#pragma unroll
+  for (int c = 0; c < W; ++c) tot[c] = block_sum(v[c]);
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int c = 0; c < W; ++c) partial[c * gridDim.x + blockIdx.x] = tot[c];
+    __threadfence();
+    const unsigned t = atomicAdd(counter, 1u);
+    last = (t == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+#pragma unroll
+  for (int c = 0; c < W; ++c) {
+    double a = 0.0;
+    for (unsigned i = threadIdx.x; i < gridDim.x; i += blockDim.x)
+      a = __dadd_rn(a, __ldcg(partial + c * gridDim.x + i));
+    a = block_sum(a);
+    if (threadIdx.x == 0) out[c] = a;
+  }
+  if (threadIdx.x == 0) *counter = 0u;
+}
+
+__global__ void k_p1(const double2* __restrict__ s, uint64_t count, uint32_t q,
+                     double* partial, unsigned* counter, double* out) {
+  double acc = 0.0;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  const uint64_t bit = 1ULL << q;
+  for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < count; k += stride)
+    acc = __dadd_rn(acc, norm_sqr_x(s[insert_zero(k, q) | bit]));
+  double v[1] = {acc};
+  finish_partials<1>(v, partial, counter, out);
+}
+
+__global__ void k_norm(const double2* __restrict__ s, uint64_t count, double* partial,
+                       unsigned* counter, double* out) {
+  double acc = 0.0;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < count; i += stride)
+    acc = __dadd_rn(acc, norm_sqr_x(s[i]));
+  double v[1] = {acc};
+  finish_partials<1>(v, partial, counter, out);
+}
+
+// sum conj(a_i) * b_i  (SimulationResult::fidelity, simulator.rs:184-191)
+__global__ void k_inner(const double2* __restrict__ a, const double2* __restrict__ b,
+                        uint64_t count, double* partial, unsigned* counter, double* out) {
+  double re = 0.0, im = 0.0;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < count; i += stride) {
+    const double2 x = a[i], y = b[i];
+    const double2 p = cmul_x(make_double2(x.x, -x.y), y);
+    re = __dadd_rn(re, p.x);
+    im = __dadd_rn(im, p.y);
+  }
+  double v[2] = {re, im};
+  finish_partials<2>(v, partial, counter, out);
+}
+
+unsigned red_blocks(uint64_t items, int device) {
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  uint64_t want = (items + kRedThreads - 1) / kRedThreads;
+  // W * grid partials stay below kPartials - 8, clear of the result slots
+  uint64_t cap = (uint64_t)sms * 4;
+  if (cap > (uint64_t)kPartials / 4) cap = kPartials / 4;
+  if (want > cap) want = cap;
+  if (want < 1) want = 1;
+  return (unsigned)want;
+}
+
+// ---- collapse / init ------------------------------------------------------------------
+
+__global__ void k_collapse(double2* __restrict__ s, uint64_t count, uint64_t bit, int outcome,
+                           double norm) {
+  const uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  const bool set = (i & bit) != 0;
+  if (set != (outcome == 1)) {
+    s[i] = make_double2(0.0, 0.0);
+  } else {
+    const double2 a = s[i];
+    s[i] = make_double2(__ddiv_rn(a.x, norm), __ddiv_rn(a.y, norm));
+  }
+}
+
+__global__ void k_set_basis(double2* __restrict__ s, uint64_t count, uint64_t index) {
+  const uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  s[i] = make_double2(i == index ? 1.0 : 0.0, 0.0);
+}
+
+// ---- marginal probabilities -----------------------------------------------------------
+//
+// marginal_probs (engine.rs:368-390): out[j] = sum of |psi_i|^2 over i whose
+// marginal bits spell j (qubits[0] = MSB of j), in ascending i.  When each
+// output has few terms a thread owns one j and adds its terms in ascending
+// i, which is exactly the reference's sum.  Otherwise (S, j) segments are
+// reduced by blocks and the segment partials summed in order.
+
+struct MargParams {
+  uint32_t q[32];     // marginal qubits, q[0] = MSB of j
+  Pos rest;           // the marginal qubits, ascending (zero bits inserted there)
+  uint32_t k;
+};
+
+__device__ __forceinline__ uint64_t deposit_j(uint64_t j, const MargParams& P) {
+  uint64_t bits = 0;
+  for (uint32_t b = 0; b < P.k; ++b) bits |= ((j >> (P.k - 1 - b)) & 1ULL) << P.q[b];
+  return bits;
+}
+
+__global__ void k_marg_thread(const double2* __restrict__ s, uint64_t nj, uint64_t nterms,
+                              MargParams P, double* __restrict__ out) {
+  const uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (j >= nj) return;
+  const uint64_t jb = deposit_j(j, P);
+  double acc = 0.0;
+  for (uint64_t r = 0; r < nterms; ++r)
+    acc = __dadd_rn(acc, norm_sqr_x(s[insert_zeros(r, P.rest.p, P.rest.np) | jb]));
+  out[j] = acc;
+}
+
+__global__ void k_marg_seg(const double2* __restrict__ s, uint64_t nterms, uint32_t nseg,
+                           MargParams P, double* __restrict__ partial) {
+  const uint64_t j = blockIdx.x / nseg;
+  const uint32_t seg = blockIdx.x % nseg;
+  const uint64_t per = (nterms + nseg - 1) / nseg;
+  const uint64_t r0 = (uint64_t)seg * per;
+  const uint64_t r1 = min(nterms, r0 + per);
+  const uint64_t jb = deposit_j(j, P);
+  double acc = 0.0;
+  for (uint64_t r = r0 + threadIdx.x; r < r1; r += blockDim.x)
+    acc = __dadd_rn(acc, norm_sqr_x(s[insert_zeros(r, P.rest.p, P.rest.np) | jb]));
+  acc = block_sum(acc);
+  if (threadIdx.x == 0) partial[blockIdx.x] = acc;
+}
+
+__global__ void k_marg_sum(const double* __restrict__ partial, uint64_t nj, uint32_t nseg,
+                           double* __restrict__ out) {
+  const uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (j >= nj) return;
+  double acc = 0.0;
+  for (uint32_t g = 0; g < nseg; ++g) acc = __dadd_rn(acc, partial[j * nseg + g]);
+  out[j] = acc;
+}
+
+// ---- CDF (inclusive prefix sum) and sampling ----------------------------------------------
+
+constexpr int kScanThreads = 256;
+constexpr int kScanPer = 8;                       // elements per thread
+constexpr int kScanChunk = kScanThreads * kScanPer;
+
+// Exclusive scan of per-thread values across the block (fixed order).
+__device__ double block_exclusive_scan(double v, double* total) {
+  __shared__ double sh[kScanThreads / 32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  double inc = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const double t = __shfl_up_sync(0xffffffffu, inc, o);
+    if (lane >= o) inc = __dadd_rn(inc, t);
+  }
+  __syncthreads();
+  if (lane == 31) sh[w] = inc;
+  __syncthreads();
+  double woff = 0.0, tot = 0.0;
+  for (int i = 0; i < kScanThreads / 32; ++i) {
+    if (i < w) woff = __dadd_rn(woff, sh[i]);
+    tot = __dadd_rn(tot, sh[i]);
+  }
+  *total = tot;
+  double exw = __shfl_up_sync(0xffffffffu, inc, 1);
+  if (lane == 0) exw = 0.0;
+  (void)v;
+  return __dadd_rn(woff, exw);
+}
+
+__device__ __forceinline__ double thread_segment_sum(const double* d, uint64_t len, uint64_t b0) {
+  double a = 0.0;
+#pragma unroll
+  for (int e = 0; e < kScanPer; ++e) {
+    const uint64_t i = b0 + e;
+    if (i < len) a = __dadd_rn(a, d[i]);
+  }
+  return a;
+}
+
+__global__ void k_scan_sums(const double* __restrict__ d, uint64_t len, double* __restrict__ sums) {
+  const uint64_t b0 = (uint64_t)blockIdx.x * kScanChunk + (uint64_t)threadIdx.x * kScanPer;
+  double tot;
+  (void)block_exclusive_scan(thread_segment_sum(d, len, b0), &tot);
+  if (threadIdx.x == 0) sums[blockIdx.x] = tot;
+}
+
+// Single block: in-place exclusive scan of sums[nb], looping with a carry.
+__global__ void k_scan_offsets(double* __restrict__ sums, uint64_t nb) {
+  __shared__ double carry;
+  if (threadIdx.x == 0) carry = 0.0;
+  __syncthreads();
+  for (uint64_t base = 0; base < nb; base += kScanThreads) {
+    const uint64_t i = base + threadIdx.x;
+    const double v = i < nb ? sums[i] : 0.0;
+    double tot;
+    const double ex = block_exclusive_scan(v, &tot);
+    const double c = carry;
+    if (i < nb) sums[i] = __dadd_rn(c, ex);
+    __syncthreads();
+    if (threadIdx.x == 0) carry = __dadd_rn(c, tot);
+    __syncthreads();
+  }
+}
+
+__global__ void k_scan_apply(double* __restrict__ d, uint64_t len, const double* __restrict__ offs) {
+  const uint64_t b0 = (uint64_t)blockIdx.x * kScanChunk + (uint64_t)threadIdx.x * kScanPer;
+  double tot;
+  const double ex = block_exclusive_scan(thread_segment_sum(d, len, b0), &tot);
+  double run = __dadd_rn(offs[blockIdx.x], ex);
+#pragma unroll
+  for (int e = 0; e < kScanPer; ++e) {
+    const uint64_t i = b0 + e;
+    if (i < len) {
+      run = __dadd_rn(run, d[i]);
+      d[i] = run;
+    }
+  }
+}
+
+__global__ void k_set_last_one(double* d, uint64_t len) { d[len - 1] = 1.0; }
+
+struct Key8 {
+  uint32_t k[8];
+};
+
+// sample_counts inner loop (engine.rs:426-431) with draw s computed from the
+// stream position: idx = partition_point(cdf < r).min(len - 1).
+__global__ void k_sample(const double* __restrict__ cdf, uint64_t len, Key8 key, uint64_t shots,
+                         uint32_t* __restrict__ out, unsigned long long* __restrict__ nboundary) {
+  const uint64_t s = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (s >= shots) return;
+  const double r = chacha8_draw(key.k, s);
+  uint64_t lo = 0, hi = len;
+  while (lo < hi) {
+    const uint64_t mid = lo + ((hi - lo) >> 1);
+    if (cdf[mid] < r) lo = mid + 1; else hi = mid;
+  }
+  if (lo > len - 1) lo = len - 1;
+  out[s] = (uint32_t)lo;
+  const double up = cdf[lo];
+  bool near = fabs(up - r) <= 1e-12;
+  if (lo > 0) near = near || fabs(r - cdf[lo - 1]) <= 1e-12;
+  if (near) atomicAdd(nboundary, 1ULL);
+}
+
+}  // namespace
+
+unsigned grid_for(uint64_t work, unsigned threads, int device) {
+  (void)device;
+  return blocks_for(work, threads);
+}
+
+int launch_gate(double2* s, uint32_t n, const GateOp& op, cudaStream_t st, int device,
+                uint64_t* launches) {
+  (void)device;
+  auto d2 = [](hc z) { return make_double2(z.re, z.im); };
+  switch (op.cls) {
+    case GC_ONE_Q: {
+      const uint64_t tb = 1ULL << op.target;
+      const Pos pos = make_pos(op.ctrl_mask | tb);
+      const uint64_t count = 1ULL << (n - pos.np);
+      k_one_q<<<blocks_for(count, kThreads), kThreads, 0, st>>>(
+          s, count, pos, op.ctrl_mask, tb, d2(op.u[0]), d2(op.u[1]), d2(op.u[2]), d2(op.u[3]));
+      break;
+    }
+    case GC_PHASE: {
+      const uint64_t tb = 1ULL << op.target;
+      const Pos pos = make_pos(op.ctrl_mask | tb);
+      const uint64_t count = 1ULL << (n - pos.np);
+      k_phase<<<blocks_for(count, kThreads), kThreads, 0, st>>>(s, count, pos, op.ctrl_mask | tb,
+                                                                 d2(op.u[0]));
+      break;
+    }
+    case GC_XPERM: {
+      const uint64_t tb = 1ULL << op.target;
+      const Pos pos = make_pos(op.ctrl_mask | tb);
+      const uint64_t count = 1ULL << (n - pos.np);
+      k_exchange<<<blocks_for(count, kThreads), kThreads, 0, st>>>(s, count, pos, op.ctrl_mask,
+                                                                    op.ctrl_mask | tb);
+      break;
+    }
+    case GC_SWAP: {
+      const uint64_t ta = 1ULL << op.target, tb = 1ULL << op.target2;
+      const Pos pos = make_pos(op.ctrl_mask | ta | tb);
+      const uint64_t count = 1ULL << (n - pos.np);
+      k_exchange<<<blocks_for(count, kThreads), kThreads, 0, st>>>(s, count, pos,
+                                                                    op.ctrl_mask | tb,
+                                                                    op.ctrl_mask | ta);
+      break;
+    }
+    case GC_DIAG: {
+      DiagParams P{};
+      const Gate& g = op.dense;
+      const uint32_t dim = 1u << g.k;
+      for (uint32_t i = 0; i < dim; ++i) P.d[i] = d2(g.m[i * dim + i]);
+      for (uint32_t b = 0; b < g.k; ++b) P.q[b] = g.qubits[b];
+      P.k = g.k;
+      const uint64_t count = 1ULL << n;
+      k_diag<<<blocks_for(count, kThreads), kThreads, 0, st>>>(s, count, P);
+      break;
+    }
+    case GC_DENSE: {
+      const Gate& g = op.dense;
+      switch (g.k) {
+        case 1: DQ_TRY(launch_dense_k<1>(s, n, g, st)); break;
+        case 2: DQ_TRY(launch_dense_k<2>(s, n, g, st)); break;
+        case 3: DQ_TRY(launch_dense_k<3>(s, n, g, st)); break;
+        case 4: DQ_TRY(launch_dense_k<4>(s, n, g, st)); break;
+        case 5: DQ_TRY(launch_dense_k<5>(s, n, g, st)); break;
+        default: return fail(DQ_ERR_INTERNAL, "dense gate with k outside 1..5");
+      }
+      break;
+    }
+    default:
+      return fail(DQ_ERR_INTERNAL, "unclassified gate");
+  }
+  if (launches) ++*launches;
+  DQ_CUDA_TRY(cudaGetLastError());
+  return DQ_OK;
+}
+
+int launch_p1(const double2* s, uint32_t n, uint32_t q, Scratch& sc, double* d_out,
+              cudaStream_t st, int device) {
+  const uint64_t count = 1ULL << (n - 1);
+  k_p1<<<red_blocks(count, device), kRedThreads, 0, st>>>(s, count, q, sc.d_partial,
+                                                          sc.d_counter, d_out);
+  DQ_CUDA_TRY(cudaGetLastError());
+  return DQ_OK;
+}
+
+int launch_norm(const double2* a, uint32_t n, Scratch& sc, double* d_out, cudaStream_t st,
+                int device) {
+  const uint64_t count = 1ULL << n;
+  k_norm<<<red_blocks(count, device), kRedThreads, 0, st>>>(a, count, sc.d_partial, sc.d_counter,
+                                                            d_out);
+  DQ_CUDA_TRY(cudaGetLastError());
+  return DQ_OK;
+}
+
+int launch_inner(const double2* a, const double2* b, uint32_t n, Scratch& sc, double* d_out,
+                 cudaStream_t st, int device) {
+  const uint64_t count = 1ULL << n;
+  k_inner<<<red_blocks(count, device), kRedThreads, 0, st>>>(a, b, count, sc.d_partial,
+                                                             sc.d_counter, d_out);
+  DQ_CUDA_TRY(cudaGetLastError());
+  return DQ_OK;
+}
+
+int launch_collapse(double2* s, uint32_t n, uint32_t q, int outcome, double norm,
+                    cudaStream_t st, int device) {
+  (void)device;
+  const uint64_t count = 1ULL << n;
+  k_collapse<<<blocks_for(count, kThreads), kThreads, 0, st>>>(s, count, 1ULL << q, outcome, norm);
+  DQ_CUDA_TRY(cudaGetLastError());
+  return DQ_OK;
+}
+
+int launch_set_basis(double2* s, uint32_t n, uint64_t index, cudaStream_t st, int device) {
+  (void)device;
+  const uint64_t count = 1ULL << n;
+  k_set_basis<<<blocks_for(count, kThreads), kThreads, 0, st>>>(s, count, index);
+  DQ_CUDA_TRY(cudaGetLastError());
+  return DQ_OK;
+}
+
+int launch_marginal(const double2* s, uint32_t n, const uint32_t* qubits, uint32_t k,
+                    double* d_out, Scratch& sc, cudaStream_t st, int device) {
+  MargParams P{};
+  uint64_t mask = 0;
+  for (uint32_t b = 0; b < k; ++b) {
+    P.q[b] = qubits[b];
+    mask |= 1ULL << qubits[b];
+  }
+  P.k = k;
+  P.rest = make_pos(mask);
+  const uint64_t nj = 1ULL << k;
+  const uint64_t nterms = 1ULL << (n - k);
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  // thread-per-output (exact reference order) when there are enough outputs
+  // to fill the GPU or few terms per output
+  if (nterms <= 64 || nj >= (uint64_t)sms * 1024) {
+    k_marg_thread<<<blocks_for(nj, kThreads), kThreads, 0, st>>>(s, nj, nterms, P, d_out);
+  } else {
+    uint64_t target_blocks = (uint64_t)sms * 8;
+    uint64_t nseg = (target_blocks + nj - 1) / nj;
+    const uint64_t max_seg = (nterms + kRedThreads - 1) / kRedThreads;
+    if (nseg > max_seg) nseg = max_seg;
+    if (nseg < 1) nseg = 1;
+    while (nj * nseg > (uint64_t)kPartials && nseg > 1) nseg >>= 1;
+    double* partial = sc.d_partial;
+    double* tmp = nullptr;
+    if (nj * nseg > (uint64_t)kPartials) {
+      DQ_CUDA_TRY(cudaMallocAsync((void**)&tmp, sizeof(double) * nj * nseg, st));
+      partial = tmp;
+    }
+    k_marg_seg<<<(unsigned)(nj * nseg), kRedThreads, 0, st>>>(s, nterms, (uint32_t)nseg, P, partial);
+    k_marg_sum<<<blocks_for(nj, kThreads), kThreads, 0, st>>>(partial, nj, (uint32_t)nseg, d_out);
+    if (tmp) DQ_CUDA_TRY(cudaFreeAsync(tmp, st));
+  }
+  DQ_CUDA_TRY(cudaGetLastError());
+  return DQ_OK;
+}
+
+int launch_cdf(double* d, uint64_t len, cudaStream_t st, int device) {
+  (void)device;
+  const uint64_t nb = (len + kScanChunk - 1) / kScanChunk;
+  double* sums = nullptr;
+  DQ_CUDA_TRY(cudaMallocAsync((void**)&sums, sizeof(double) * nb, st));
+  k_scan_sums<<<(unsigned)nb, kScanThreads, 0, st>>>(d, len, sums);
+  k_scan_offsets<<<1, kScanThreads, 0, st>>>(sums, nb);
+  k_scan_apply<<<(unsigned)nb, kScanThreads, 0, st>>>(d, len, sums);
+  k_set_last_one<<<1, 1, 0, st>>>(d, len);
+  DQ_CUDA_TRY(cudaFreeAsync(sums, st));
+  DQ_CUDA_TRY(cudaGetLastError());
+  return DQ_OK;
+}
+
+int launch_sample(const double* cdf, uint64_t len, const uint32_t key[8], uint64_t shots,
+                  uint32_t* d_idx, unsigned long long* d_boundary, cudaStream_t st, int device) {
+  (void)device;
+  if (shots == 0) return DQ_OK;
+  Key8 K;
+  for (int i = 0; i < 8; ++i) K.k[i] = key[i];
+  k_sample<<<blocks_for(shots, kThreads), kThreads, 0, st>>>(cdf, len, K, shots, d_idx, d_boundary);
+  DQ_CUDA_TRY(cudaGetLastError());
+  return DQ_OK;
+}
+
+}  // namespace dq

@@ -1,0 +1,50 @@
+// dq_engine.cuh — host launchers of the exact per-gate kernels and the
+// reduction / sampling kernels (dq_engine.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "dq_common.cuh"
+#include "dq_gates.hpp"
+
+namespace dq {
+
+struct Scratch {            // per-handle device/pinned scratch
+  double* d_partial = nullptr;   // kPartials doubles
+  unsigned* d_counter = nullptr; // last-block counters
+  double* h_pinned = nullptr;    // 64 doubles pinned
+  unsigned long long* d_ull = nullptr;
+};
+
+constexpr int kPartials = 4096;
+constexpr int kRedThreads = 512;
+
+// One classified gate on a state of n qubits.  Returns DQ_OK or an error.
+int launch_gate(double2* s, uint32_t n, const GateOp& op, cudaStream_t st, int device,
+                uint64_t* launches);
+
+// p1 = sum over amplitudes with bit q set (device value in *d_out).
+int launch_p1(const double2* s, uint32_t n, uint32_t q, Scratch& sc, double* d_out,
+              cudaStream_t st, int device);
+// Zero the other half, divide the kept half by norm.
+int launch_collapse(double2* s, uint32_t n, uint32_t q, int outcome, double norm,
+                    cudaStream_t st, int device);
+int launch_set_basis(double2* s, uint32_t n, uint64_t index, cudaStream_t st, int device);
+
+// marginal probabilities into a device buffer d_out[2^k].
+int launch_marginal(const double2* s, uint32_t n, const uint32_t* qubits, uint32_t k,
+                    double* d_out, Scratch& sc, cudaStream_t st, int device);
+// in-place inclusive prefix sum of d[len] (deterministic order), last = 1.0.
+int launch_cdf(double* d, uint64_t len, cudaStream_t st, int device);
+// per-shot lower_bound in the CDF with device ChaCha8 draws.
+int launch_sample(const double* cdf, uint64_t len, const uint32_t key[8], uint64_t shots,
+                  uint32_t* d_idx, unsigned long long* d_boundary, cudaStream_t st, int device);
+
+// sum conj(a)*b -> d_out[0..1]; sum |a|^2 -> d_out[0]
+int launch_inner(const double2* a, const double2* b, uint32_t n, Scratch& sc, double* d_out,
+                 cudaStream_t st, int device);
+int launch_norm(const double2* a, uint32_t n, Scratch& sc, double* d_out, cudaStream_t st,
+                int device);
+
+}  // namespace dq

@@ -1,0 +1,233 @@
+/*
+ * dqsim_cuda.h — C ABI of the B200 (sm_100a) FP64 statevector engine.
+ *
+ * This header is the drop-in boundary for the statevector hot path of dqsim
+ * (Rust crate `dqsim`, module `_core`).  It replaces the free functions of
+ * `src/engine.rs` and the per-instruction dispatch of
+ * `src/monolithic/statevector/simulator.rs` with calls into a shared library
+ * (`libdqsim_cuda.so`) whose state vector stays resident in HBM.
+ *
+ * Conventions
+ *   - Every entry point returns an int status: DQ_OK (0) or a negative
+ *     DQ_ERR_* code.  dq_last_error() returns a thread-local message for the
+ *     last failing call on the calling thread.  Nothing aborts and no C++
+ *     exception crosses this boundary.
+ *   - Amplitudes are complex128, stored interleaved (re, im) as double pairs,
+ *     index bit q = qubit q (qubit 0 is the least significant bit), exactly the
+ *     layout of the reference's `Vec<Complex64>`.
+ *   - Gate matrices are row-major complex128 (interleaved), qubits[0] is the
+ *     most significant bit of the gate's row/column index (`src/gates.rs`).
+ *   - Host buffers are caller-owned; device memory is handle-owned.  Each
+ *     handle owns one CUDA stream.  A handle is not thread-safe; distinct
+ *     handles may be used concurrently from different threads.
+ *   - Calls block until their results are visible to the host.
+ *   - No torch types appear in any signature.
+ */
+#ifndef DQSIM_CUDA_H
+#define DQSIM_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DQ_ABI_VERSION 1
+
+#if defined(__GNUC__)
+#define DQ_API __attribute__((visibility("default")))
+#else
+#define DQ_API
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define DQ_OK 0
+#define DQ_ERR_INVALID_ARG (-1)    /* bad pointer, size, qubit index ...      */
+#define DQ_ERR_CUDA (-2)           /* a CUDA runtime call failed              */
+#define DQ_ERR_OOM (-3)            /* device or pinned host allocation failed */
+#define DQ_ERR_UNSUPPORTED (-4)    /* unsupported generic gate (NotImplemented) */
+#define DQ_ERR_NO_DEVICE (-5)      /* no CUDA device visible                  */
+#define DQ_ERR_INTERNAL (-6)       /* invariant violated inside the engine    */
+
+/* ---- instruction IR ------------------------------------------------------
+ * One dq_inst per `Instruction` variant of the reference IR
+ * (`src/types.rs:60-135`).  The JSON decoding (serde) stays on the host; the
+ * host encodes each decoded instruction into this POD record.
+ *
+ * Field use per kind (reference field names in brackets):
+ *   1q gates            q[0] = qubit
+ *   u3/u                p = {theta, phi, lam}
+ *   u2                  p = {phi, lam}
+ *   u1/p/crz/cu1/cp     p[0] = lam
+ *   rx/ry/crx/cry/rxx/rzz p[0] = theta
+ *   rz                  p[0] = phi
+ *   cu3                 p = {theta, phi, lam};  cu: p = {theta, phi, lam, gamma}
+ *   2q controlled       q = {control, target}
+ *   swap/rxx/rzz        q = {a, b}
+ *   ccx/rccx            q = {control1, control2, target}
+ *   cswap               q = {control, target1, target2}
+ *   rc3x/c3x/c3sqrtx    q = {control1, control2, control3, target}
+ *   c4x                 q = {control1 .. control4, target}
+ *   generic gate        q = qubits (nq of them, at most DQ_MAX_INST_QUBITS);
+ *                       the host resolves the lower-cased name to a DQ_G_* kind
+ *   measure             q[0] = qubit, cbit = cbit
+ *   reset               q[0] = qubit
+ *   conditional         the wrapped instruction carries cond_count > 0
+ *                       conditions starting at conds[cond_first]; nested
+ *                       conditionals are flattened (all must hold).
+ * ------------------------------------------------------------------------ */
+enum dq_kind {
+  DQ_ID = 0, DQ_X, DQ_Y, DQ_Z, DQ_H, DQ_S, DQ_SDG, DQ_T, DQ_TDG, DQ_SX, DQ_SXDG,
+  DQ_U3, DQ_U2, DQ_U1, DQ_U, DQ_P, DQ_RX, DQ_RY, DQ_RZ, DQ_U0,
+  DQ_CX, DQ_CZ, DQ_CY, DQ_CH, DQ_SWAP, DQ_CSX,
+  DQ_CRX, DQ_CRY, DQ_CRZ, DQ_CU1, DQ_CP, DQ_CU3, DQ_CU, DQ_RXX, DQ_RZZ,
+  DQ_CCX, DQ_CSWAP, DQ_RCCX, DQ_RC3X, DQ_C3X, DQ_C3SQRTX, DQ_C4X,
+  /* generic `gate` instructions, resolved by lower-cased name */
+  DQ_G_PHI_PLUS,     /* remote_link_phi_plus, remote_epr */
+  DQ_G_PSI_MINUS,    /* remote_link_psi_minus */
+  DQ_G_PSI_PLUS,     /* remote_link_psi_plus */
+  DQ_G_CZ,           /* nonlocal_cz, remote_cz */
+  DQ_G_CX,           /* remote_cx */
+  DQ_G_NOOP,         /* remote_barrier, remote_cu1 */
+  DQ_G_OPAQUE,       /* circuit-*: no-op in the shots path, unsupported in simulate */
+  DQ_G_UNSUPPORTED,  /* any other name: DQ_ERR_UNSUPPORTED when executed */
+  DQ_MEASURE, DQ_RESET, DQ_BARRIER, DQ_CLASSICAL,
+  DQ_KIND_COUNT
+};
+
+#define DQ_MAX_INST_QUBITS 8
+#define DQ_MAX_GATE_QUBITS 5   /* c4x: the widest gate the engine applies */
+
+typedef struct dq_inst {
+  int32_t kind;                      /* enum dq_kind                        */
+  int32_t nq;                        /* number of valid entries in q[]      */
+  int32_t q[DQ_MAX_INST_QUBITS];     /* qubits in reference field order     */
+  int64_t cbit;                      /* measure: target classical bit       */
+  double p[4];                       /* parameters in reference field order */
+  uint32_t cond_first;               /* index of first condition            */
+  uint32_t cond_count;               /* 0 = unconditional                   */
+} dq_inst;
+
+typedef struct dq_cond {             /* `Condition` (src/types.rs:54-58)    */
+  uint64_t creg_base;
+  uint64_t creg_size;                /* <= 64                               */
+  uint64_t creg_value;
+} dq_cond;
+
+/* ---- options and profile ------------------------------------------------ */
+enum dq_semantics {
+  DQ_SEM_SIMULATE = 0,  /* run_instruction (simulate):  circuit-* unsupported */
+  DQ_SEM_SHOTS = 1      /* run_instruction_par + fuse_circuit (simulate_shots) */
+};
+
+enum dq_exec {
+  DQ_EXEC_PER_GATE = 0, /* one exact-arithmetic kernel per instruction        */
+  DQ_EXEC_FUSED = 1     /* gate runs fused into shared-memory tile sweeps     */
+};
+
+typedef struct dq_run_opts {
+  int32_t semantics;        /* enum dq_semantics                             */
+  int32_t exec;             /* enum dq_exec                                  */
+  int32_t fusion_width;     /* local qubits per fused tile; 0 = engine default */
+  int32_t profile;          /* nonzero: time each kernel class (per-gate exec) */
+} dq_run_opts;
+
+typedef struct dq_profile {         /* SimulationProfile (simulator.rs:53-68) */
+  uint64_t apply_one_qubit_calls;
+  double apply_one_qubit_time;      /* seconds */
+  uint64_t apply_n_qubit_calls;
+  double apply_n_qubit_time;
+  uint64_t measure_qubit_calls;
+  double measure_qubit_time;
+  double total_time;
+  uint64_t kernel_launches;         /* engine kernels launched by the call    */
+  uint64_t sweeps;                  /* fused tile sweeps (DQ_EXEC_FUSED)      */
+  uint64_t boundary_draws;          /* measure draws with |r - p1| < 1e-12   */
+  int64_t failed_inst;              /* index of the failing instruction or -1 */
+} dq_profile;
+
+typedef struct dq_state_s* dq_state_t;
+
+/* ---- library ------------------------------------------------------------ */
+DQ_API int dq_abi_version(void);
+DQ_API const char* dq_last_error(void);
+DQ_API int dq_device_count(int* count);
+
+/* ---- state lifecycle ----------------------------------------------------
+ * Replaces `vec![C::new(0.0, 0.0); 1 << n]; state[0] = 1`
+ * (statevector/simulator.rs:337-339) with an HBM allocation. */
+DQ_API int dq_state_create(uint32_t n, int device, dq_state_t* out);
+DQ_API int dq_state_destroy(dq_state_t h);
+DQ_API int dq_state_num_qubits(dq_state_t h, uint32_t* n);
+DQ_API int dq_state_reset(dq_state_t h);                         /* |0...0>          */
+DQ_API int dq_state_set_basis(dq_state_t h, uint64_t index);     /* |index>          */
+DQ_API int dq_state_upload(dq_state_t h, const double* amps, uint64_t len);   /* len = 2^n */
+DQ_API int dq_state_download(dq_state_t h, double* amps, uint64_t len);
+DQ_API int dq_state_copy(dq_state_t dst, dq_state_t src);
+DQ_API int dq_state_device_ptr(dq_state_t h, void** dev_ptr, void** stream);
+DQ_API int dq_state_synchronize(dq_state_t h);
+
+/* ---- gate primitives ----------------------------------------------------
+ * dq_apply_1q replaces engine::apply_one_qubit (src/engine.rs:24-101):
+ * (psi[i], psi[i|2^t]) <- U (psi[i], psi[i|2^t]) for every i with bit t clear
+ * and (i & ctrl_mask) == ctrl_val.  u = {u00, u01, u10, u11} interleaved.   */
+DQ_API int dq_apply_1q(dq_state_t h, const double* u, uint32_t target, uint64_t ctrl_mask,
+                uint64_t ctrl_val);
+/* dq_apply_dense replaces engine::apply_n_qubit (src/engine.rs:109-181):
+ * dense 2^k x 2^k (k <= 5) on arbitrary distinct qubits, qubits[0] = MSB.   */
+DQ_API int dq_apply_dense(dq_state_t h, const double* u, const uint32_t* qubits, uint32_t k);
+/* dq_apply_inst applies one IR instruction exactly as run_instruction
+ * (statevector/simulator.rs:386-632) would; measure/reset/conditional are
+ * rejected here (use dq_run). */
+DQ_API int dq_apply_inst(dq_state_t h, const dq_inst* inst);
+
+/* ---- measurement ---------------------------------------------------------
+ * engine::measure_qubit (src/engine.rs:193-257) split at the draw:
+ * p1 = sum |psi_i|^2 over bit q set; the caller draws r; outcome = r < p1;
+ * the collapse zeroes the other half and divides the kept half by
+ * sqrt(p1).max(1e-15) (outcome 1) or sqrt((1-p1).max(0)).max(1e-15).   */
+DQ_API int dq_measure_p1(dq_state_t h, uint32_t qubit, double* p1);
+DQ_API int dq_collapse(dq_state_t h, uint32_t qubit, int outcome, double p1);
+DQ_API int dq_measure(dq_state_t h, uint32_t qubit, double r, int* outcome, double* p1);
+
+/* ---- whole program --------------------------------------------------------
+ * Replaces the instruction loop of StatevectorSimulator::simulate
+ * (statevector/simulator.rs:351-356) and, with DQ_SEM_SHOTS, one shot of the
+ * simulate_shots loop (statevector/simulator.rs:277-285).  The state must
+ * hold num_qubits = n.  Outcomes are drawn from ChaCha8Rng::seed_from_u64(seed)
+ * in program order, one f64 per executed measure/reset.  cbits[ncbits] is
+ * caller-initialised (use -1 for "never written"); measure writes 0/1. */
+DQ_API int dq_run(dq_state_t h, const dq_inst* prog, uint64_t ninst, const dq_cond* conds,
+           uint64_t nconds, uint64_t seed, int32_t* cbits, uint64_t ncbits,
+           const dq_run_opts* opts, dq_profile* prof);
+
+/* ---- queries --------------------------------------------------------------
+ * engine::marginal_probs (src/engine.rs:368-390): out[j] for j < 2^k,
+ * qubits[0] = MSB of j.  k <= n, k <= 30 for this call.                    */
+DQ_API int dq_marginal_probs(dq_state_t h, const uint32_t* qubits, uint32_t k, double* out);
+/* engine::sample_counts (src/engine.rs:398-433) with the CDF built on the
+ * device: out_idx[s] = partition_point(cdf < r_s).min(2^k - 1), r_s the s-th
+ * f64 of ChaCha8Rng::seed_from_u64(seed).  *n_boundary counts draws with
+ * |r_s - cdf boundary| <= 1e-12 (outcome may differ from a sequential CDF). */
+DQ_API int dq_sample(dq_state_t h, const uint32_t* qubits, uint32_t k, uint64_t seed,
+              uint64_t shots, uint32_t* out_idx, uint64_t* n_boundary);
+/* Same as dq_sample with the 32-byte ChaCha8 key given directly (the
+ * reference's from_entropy() path seeds the full key). */
+DQ_API int dq_sample_key(dq_state_t h, const uint32_t* qubits, uint32_t k, const uint32_t* key8,
+                  uint64_t shots, uint32_t* out_idx, uint64_t* n_boundary);
+/* SimulationResult::fidelity inner product <self|other> (simulator.rs:184-191). */
+DQ_API int dq_inner(dq_state_t h, const double* other, uint64_t len, double* re, double* im);
+DQ_API int dq_norm_sqr(dq_state_t h, double* out);
+
+/* ---- RNG (host side; same stream the device uses) ------------------------
+ * ChaCha8Rng::seed_from_u64(seed) (rand_chacha 0.3.1 / rand_core 0.6.4),
+ * gen::<f64>() (rand 0.8.5): the draws at positions [skip, skip + count). */
+DQ_API int dq_rng_f64(uint64_t seed, uint64_t skip, uint64_t count, double* out);
+DQ_API int dq_rng_seed_key(uint64_t seed, uint32_t* key8);
+DQ_API int dq_chacha_block(const uint32_t* in16, uint32_t rounds, uint32_t* out16);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DQSIM_CUDA_H */
