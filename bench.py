@@ -425,7 +425,7 @@ def dominant_kernel_roofline(st, prog, exec_mode, stream, dev):
 
     peak, src = peak_hbm()
     n = prog.num_qubits
-    reps = 10
+    reps = 3
     if exec_mode == nat.EXEC_FUSED:
         name, nbytes, ms = fused_sweep_timing(st, prog, stream, reps)
     else:
@@ -453,16 +453,19 @@ def dominant_kernel_roofline(st, prog, exec_mode, stream, dev):
 
 
 def fused_sweep_timing(st, prog, stream, reps):
+    """Average duration of one fused sweep, from CUDA events around every
+    sweep launch on the state's stream (dq_run_opts.time_sweeps)."""
     from dqsim_bosonic_b200 import _native as nat
-    import ctypes
+    from dqsim_bosonic_b200.statevector import run_program
 
-    L = nat.lib()
-    if not hasattr(L, "dq_time_sweeps"):
-        raise RuntimeError("engine without sweep timing")
-    out = (ctypes.c_double * 4)()
-    nat.check(L.dq_time_sweeps(st.handle, nat.ptr(prog.insts), prog.ninst, 0, reps, out))
+    tot, cnt = 0.0, 0
+    for _ in range(reps):
+        st.reset()
+        _, prof = run_program(st, prog, 7, nat.SEM_SIMULATE, nat.EXEC_FUSED, time_sweeps=True)
+        tot += prof.sweep_time
+        cnt += int(prof.sweeps)
     n = prog.num_qubits
-    return "sweep kernel (fused tile sweep)", 2 * 16 * (2 ** n), out[0]
+    return "k_sweep (fused tile sweep)", 2 * 16 * (2 ** n), tot / max(cnt, 1) * 1e3
 
 
 if __name__ == "__main__":

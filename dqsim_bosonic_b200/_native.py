@@ -66,6 +66,8 @@ class RunOpts(ctypes.Structure):
         ("exec", ctypes.c_int32),
         ("fusion_width", ctypes.c_int32),
         ("profile", ctypes.c_int32),
+        ("time_sweeps", ctypes.c_int32),
+        ("max_cost", ctypes.c_int32),
     ]
 
 
@@ -80,6 +82,7 @@ class Profile(ctypes.Structure):
         ("total_time", ctypes.c_double),
         ("kernel_launches", ctypes.c_uint64),
         ("sweeps", ctypes.c_uint64),
+        ("sweep_time", ctypes.c_double),
         ("boundary_draws", ctypes.c_uint64),
         ("failed_inst", ctypes.c_int64),
     ]

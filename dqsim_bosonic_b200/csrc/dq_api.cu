@@ -20,6 +20,7 @@
 
 #include "dq_common.cuh"
 #include "dq_engine.cuh"
+#include "dq_fused.cuh"
 #include "dq_gates.hpp"
 #include "dq_rng.cuh"
 
@@ -101,6 +102,11 @@ struct dq_state_s {
   double2* amp = nullptr;
   cudaStream_t stream = nullptr;
   dq::Scratch sc;
+  dq::FusedWork fw;
+  // perm[l] = physical bit position holding logical qubit l (fused runs
+  // relabel swap gates instead of moving data)
+  uint32_t perm[64];
+  bool permuted = false;
 };
 
 using namespace dq;
@@ -117,6 +123,32 @@ int check_handle(dq_state_t h) {
 int sync_stream(dq_state_t h) {
   DQ_CUDA_TRY(cudaStreamSynchronize(h->stream));
   return DQ_OK;
+}
+
+void reset_perm(dq_state_t h) {
+  for (uint32_t l = 0; l < 64; ++l) h->perm[l] = l;
+  h->permuted = false;
+}
+
+// Make the physical layout canonical (perm = identity).
+int canonicalize(dq_state_t h) {
+  if (!h->permuted) return DQ_OK;
+  DQ_TRY(materialize_perm(h->amp, h->n, h->perm, h->stream, nullptr));
+  h->permuted = false;
+  return DQ_OK;
+}
+
+void update_permuted(dq_state_t h) {
+  h->permuted = false;
+  for (uint32_t l = 0; l < h->n; ++l)
+    if (h->perm[l] != l) h->permuted = true;
+}
+
+uint64_t map_mask(dq_state_t h, uint64_t mask) {
+  uint64_t out = 0;
+  for (uint32_t l = 0; l < h->n; ++l)
+    if (mask >> l & 1ULL) out |= 1ULL << h->perm[l];
+  return out;
 }
 
 int read_scalars(dq_state_t h, const double* d_src, int count, double* out) {
@@ -193,72 +225,6 @@ bool inst_to_op(const dq_inst& in, GateOp& op) {
   if (!matrix_nq(in, g)) return false;
   classify(g, op);
   return true;
-}
-
-// ---- fuse_circuit (types.rs:239-293) ------------------------------------------
-// One simulate_shots trajectory runs the fused program: consecutive
-// unconditional single-qubit gates on a qubit are multiplied into one 2x2
-// (new = gate * pending), a pending matrix is flushed right before the first
-// non-fusable instruction touching its qubit, matrices within 1e-10 of the
-// identity are dropped, and the rest are flushed at the end (ascending qubit
-// order; the reference iterates a HashMap there, which only affects the
-// discarded final state).
-struct FusedEntry {
-  int64_t inst;  // >= 0: original instruction index; -1: fused 2x2 below
-  uint32_t qubit;
-  hc m[4];
-};
-
-void matmul2(const hc a[4], const hc b[4], hc out[4]) {
-  const hc r0 = a[0] * b[0] + a[1] * b[2];
-  const hc r1 = a[0] * b[1] + a[1] * b[3];
-  const hc r2 = a[2] * b[0] + a[3] * b[2];
-  const hc r3 = a[2] * b[1] + a[3] * b[3];
-  out[0] = r0; out[1] = r1; out[2] = r2; out[3] = r3;
-}
-
-bool near_identity(const hc m[4]) {
-  return hypot(m[0].re - 1.0, m[0].im) < 1e-10 && hypot(m[1].re, m[1].im) < 1e-10 &&
-         hypot(m[2].re, m[2].im) < 1e-10 && hypot(m[3].re - 1.0, m[3].im) < 1e-10;
-}
-
-std::vector<FusedEntry> fuse_program(const dq_inst* prog, uint64_t ninst, uint32_t n) {
-  std::vector<FusedEntry> out;
-  out.reserve(ninst + n);
-  std::vector<hc> pend(4 * (size_t)(n ? n : 1));
-  std::vector<char> has(n ? n : 1, 0);
-  auto flush = [&](uint32_t q) {
-    if (q >= n || !has[q]) return;
-    has[q] = 0;
-    if (near_identity(&pend[4 * q])) return;
-    FusedEntry e;
-    e.inst = -1;
-    e.qubit = q;
-    for (int i = 0; i < 4; ++i) e.m[i] = pend[4 * q + i];
-    out.push_back(e);
-  };
-  for (uint64_t i = 0; i < ninst; ++i) {
-    const dq_inst& in = prog[i];
-    hc m[4];
-    if (in.cond_count == 0 && matrix_1q(in.kind, in.p, m)) {
-      const uint32_t q = (uint32_t)in.q[0];
-      if (!has[q]) {
-        has[q] = 1;
-        pend[4 * q] = R(1); pend[4 * q + 1] = R(0); pend[4 * q + 2] = R(0); pend[4 * q + 3] = R(1);
-      }
-      matmul2(m, &pend[4 * q], &pend[4 * q]);
-      continue;
-    }
-    if (in.kind != DQ_BARRIER && in.kind != DQ_CLASSICAL)
-      for (int t = 0; t < in.nq && t < DQ_MAX_INST_QUBITS; ++t)
-        if (in.q[t] >= 0) flush((uint32_t)in.q[t]);
-    FusedEntry e;
-    e.inst = (int64_t)i;
-    e.qubit = 0;
-    out.push_back(e);
-  }
-  for (uint32_t q = 0; q < n; ++q) flush(q);
-  return out;
 }
 
 // Timing of one kernel class (profile=True): events bracketing the calls.
@@ -439,6 +405,7 @@ int dq_state_create(uint32_t n, int device, dq_state_t* out) {
     return rc;
   }
   h->amp = (double2*)p;
+  reset_perm(h);
   auto cleanup = [&](int code, const char* what, cudaError_t e) {
     set_error(std::string(what) + ": " + cudaGetErrorString(e));
     cudaGetLastError();
@@ -476,6 +443,7 @@ int dq_state_destroy(dq_state_t h) {
   if (!h) return DQ_OK;
   DeviceGuard g(h->device);
   if (h->stream) cudaStreamSynchronize(h->stream);
+  fused_release(h->fw);
   if (h->amp) cache_free(h->device, h->bytes, h->amp);
   if (h->sc.d_partial) cudaFree(h->sc.d_partial);
   if (h->sc.d_counter) cudaFree(h->sc.d_counter);
@@ -498,6 +466,7 @@ int dq_state_set_basis(dq_state_t h, uint64_t index) {
   if (index >= h->len) return fail(DQ_ERR_INVALID_ARG, "basis index out of range");
   DeviceGuard g(h->device);
   DQ_TRY(launch_set_basis(h->amp, h->n, index, h->stream, h->device));
+  reset_perm(h);
   return sync_stream(h);
 }
 
@@ -508,6 +477,7 @@ int dq_state_upload(dq_state_t h, const double* amps, uint64_t len) {
   if (!amps || len != h->len) return fail(DQ_ERR_INVALID_ARG, "upload length must be 2^n amplitudes");
   DeviceGuard g(h->device);
   DQ_CUDA_TRY(cudaMemcpyAsync(h->amp, amps, h->bytes, cudaMemcpyHostToDevice, h->stream));
+  reset_perm(h);
   return sync_stream(h);
 }
 
@@ -515,6 +485,7 @@ int dq_state_download(dq_state_t h, double* amps, uint64_t len) {
   DQ_TRY(check_handle(h));
   if (!amps || len != h->len) return fail(DQ_ERR_INVALID_ARG, "download length must be 2^n amplitudes");
   DeviceGuard g(h->device);
+  DQ_TRY(canonicalize(h));
   DQ_CUDA_TRY(cudaMemcpyAsync(amps, h->amp, h->bytes, cudaMemcpyDeviceToHost, h->stream));
   return sync_stream(h);
 }
@@ -524,13 +495,23 @@ int dq_state_copy(dq_state_t dst, dq_state_t src) {
   DQ_TRY(check_handle(src));
   if (dst->n != src->n) return fail(DQ_ERR_INVALID_ARG, "state sizes differ");
   DeviceGuard g(dst->device);
+  {
+    DeviceGuard gs(src->device);
+    DQ_TRY(canonicalize(src));
+  }
   DQ_TRY(sync_stream(src));
+  reset_perm(dst);
   DQ_CUDA_TRY(cudaMemcpyAsync(dst->amp, src->amp, dst->bytes, cudaMemcpyDefault, dst->stream));
   return sync_stream(dst);
 }
 
 int dq_state_device_ptr(dq_state_t h, void** dev_ptr, void** stream) {
   DQ_TRY(check_handle(h));
+  {
+    DeviceGuard g(h->device);
+    DQ_TRY(canonicalize(h));
+    DQ_TRY(sync_stream(h));
+  }
   if (dev_ptr) *dev_ptr = h->amp;
   if (stream) *stream = (void*)h->stream;
   return DQ_OK;
@@ -552,6 +533,9 @@ int dq_apply_1q(dq_state_t h, const double* u, uint32_t target, uint64_t ctrl_ma
   if ((ctrl_val & ~ctrl_mask) != 0) return fail(DQ_ERR_INVALID_ARG, "control value outside the mask");
   if (__builtin_popcountll(ctrl_mask) > 7) return fail(DQ_ERR_INVALID_ARG, "at most 7 controls");
   DeviceGuard g(h->device);
+  ctrl_val = map_mask(h, ctrl_val);
+  ctrl_mask = map_mask(h, ctrl_mask);
+  target = h->perm[target];
   GateOp op;
   op.cls = GC_ONE_Q;
   op.target = target;
@@ -597,10 +581,10 @@ int dq_apply_dense(dq_state_t h, const double* u, const uint32_t* qubits, uint32
   gt.k = k;
   const uint32_t dim = 1u << k;
   for (uint32_t i = 0; i < dim * dim; ++i) gt.m[i] = hc{u[2 * i], u[2 * i + 1]};
-  for (uint32_t b = 0; b < k; ++b) gt.qubits[b] = qubits[b];
+  for (uint32_t b = 0; b < k; ++b) gt.qubits[b] = h->perm[qubits[b]];
   GateOp op;
   if (k == 1) {
-    classify_1q(gt.m, qubits[0], 0, op);
+    classify_1q(gt.m, gt.qubits[0], 0, op);
   } else {
     classify(gt, op);
   }
@@ -621,8 +605,11 @@ int dq_apply_inst(dq_state_t h, const dq_inst* inst) {
     default: break;
   }
   DeviceGuard g(h->device);
+  dq_inst mapped = *inst;
+  for (int i = 0; i < mapped.nq && i < DQ_MAX_INST_QUBITS; ++i)
+    if (mapped.q[i] >= 0 && (uint32_t)mapped.q[i] < h->n) mapped.q[i] = (int32_t)h->perm[mapped.q[i]];
   GateOp op;
-  if (!inst_to_op(*inst, op)) return fail(DQ_ERR_INTERNAL, "instruction kind without a matrix");
+  if (!inst_to_op(mapped, op)) return fail(DQ_ERR_INTERNAL, "instruction kind without a matrix");
   DQ_TRY(launch_gate(h->amp, h->n, op, h->stream, h->device, nullptr));
   return sync_stream(h);
 }
@@ -632,7 +619,7 @@ int dq_measure_p1(dq_state_t h, uint32_t qubit, double* p1) {
   if (!p1 || qubit >= h->n) return fail(DQ_ERR_INVALID_ARG, "bad qubit or null output");
   DeviceGuard g(h->device);
   double* d = h->sc.d_partial + kPartials - 1;
-  DQ_TRY(launch_p1(h->amp, h->n, qubit, h->sc, d, h->stream, h->device));
+  DQ_TRY(launch_p1(h->amp, h->n, h->perm[qubit], h->sc, d, h->stream, h->device));
   return read_scalars(h, d, 1, p1);
 }
 
@@ -651,7 +638,7 @@ int dq_collapse(dq_state_t h, uint32_t qubit, int outcome, double p1) {
     norm = sqrt(t);
     if (norm < 1e-15) norm = 1e-15;
   }
-  DQ_TRY(launch_collapse(h->amp, h->n, qubit, outcome, norm, h->stream, h->device));
+  DQ_TRY(launch_collapse(h->amp, h->n, h->perm[qubit], outcome, norm, h->stream, h->device));
   return sync_stream(h);
 }
 
@@ -692,7 +679,20 @@ int dq_run(dq_state_t h, const dq_inst* prog, uint64_t ninst, const dq_cond* con
   c.timer.on = o.profile != 0;
   c.timer.st = h->stream;
   int rc = DQ_OK;
-  if (o.semantics == DQ_SEM_SHOTS) {
+  const bool fused = o.exec == DQ_EXEC_FUSED && !o.profile && h->n >= kFusedMinQubits;
+  if (fused) {
+    FusedHooks hooks;
+    hooks.measure = [&c](uint32_t q, int* out) { return do_measure(c, q, out); };
+    hooks.exact_gate = [&c](const GateOp& op) { return do_gate_op(c, op, 0); };
+    hooks.cbits = cbits;
+    hooks.ncbits = ncbits;
+    hooks.conds = conds;
+    rc = fused_run(h->amp, h->n, prog, ninst, o, h->fw, h->stream, h->device, hooks, &c.prof,
+                   h->perm);
+    update_permuted(h);
+  } else if ((rc = canonicalize(h)) != DQ_OK) {
+    // error already recorded
+  } else if (o.semantics == DQ_SEM_SHOTS) {
     const std::vector<FusedEntry> fused = fuse_program(prog, ninst, h->n);
     for (const FusedEntry& e : fused) {
       if (e.inst < 0) {
@@ -738,6 +738,9 @@ int dq_marginal_probs(dq_state_t h, const uint32_t* qubits, uint32_t k, double* 
       if (qubits[a] == qubits[b]) return fail(DQ_ERR_INVALID_ARG, "repeated qubit");
   }
   DeviceGuard g(h->device);
+  std::vector<uint32_t> mq(qubits, qubits + k);
+  for (auto& q : mq) q = h->perm[q];
+  qubits = mq.data();
   const uint64_t nj = 1ULL << k;
   double* d = nullptr;
   DQ_CUDA_TRY(cudaMallocAsync((void**)&d, sizeof(double) * nj, h->stream));
@@ -763,6 +766,9 @@ int dq_sample_key(dq_state_t h, const uint32_t* qubits, uint32_t k, const uint32
       if (qubits[a] == qubits[b]) return fail(DQ_ERR_INVALID_ARG, "repeated qubit");
   }
   DeviceGuard g(h->device);
+  std::vector<uint32_t> mq(qubits, qubits + k);
+  for (auto& q : mq) q = h->perm[q];
+  qubits = mq.data();
   const uint64_t nj = 1ULL << k;
   double* cdf = nullptr;
   uint32_t* idx = nullptr;
@@ -808,6 +814,7 @@ int dq_inner(dq_state_t h, const double* other, uint64_t len, double* re, double
   if (!other || !re || !im) return fail(DQ_ERR_INVALID_ARG, "null argument");
   if (len != h->len) return fail(DQ_ERR_INVALID_ARG, "length mismatch");
   DeviceGuard g(h->device);
+  DQ_TRY(canonicalize(h));
   double2* d = nullptr;
   DQ_CUDA_TRY(cudaMallocAsync((void**)&d, h->bytes, h->stream));
   int rc = DQ_OK;

@@ -271,9 +271,14 @@ __global__ void k_set_basis(double2* __restrict__ s, uint64_t count, uint64_t in
 // i, which is exactly the reference's sum.  Otherwise (S, j) segments are
 // reduced by blocks and the segment partials summed in order.
 
+struct Pos32 {
+  uint32_t p[32];
+  int np;
+};
+
 struct MargParams {
   uint32_t q[32];     // marginal qubits, q[0] = MSB of j
-  Pos rest;           // the marginal qubits, ascending (zero bits inserted there)
+  Pos32 rest;         // the marginal qubits, ascending (zero bits inserted there)
   uint32_t k;
 };
 
@@ -554,7 +559,9 @@ int launch_marginal(const double2* s, uint32_t n, const uint32_t* qubits, uint32
     mask |= 1ULL << qubits[b];
   }
   P.k = k;
-  P.rest = make_pos(mask);
+  P.rest.np = 0;
+  for (uint32_t b = 0; b < 64 && P.rest.np < 32; ++b)
+    if (mask >> b & 1ULL) P.rest.p[P.rest.np++] = b;
   const uint64_t nj = 1ULL << k;
   const uint64_t nterms = 1ULL << (n - k);
   int sms = 148;

@@ -1,0 +1,1330 @@
+// dq_fused.cu — the tile-sweep engine: planner (host) and sweep kernel (sm_100a).
+//
+// Kernel geometry.  A tile holds 2^m amplitudes (m = 7 + RB local qubits,
+// RB = register bits per thread, m <= 12, 64 KiB of FP64 complex at m = 12).
+// 128 threads per CTA, 3 CTAs per SM.  Local bit k of a tile is physical
+// qubit local_pos[k] (ascending); local bits 0..4 are qubits 0..4, so a tile
+// is made of 2^(m-5) runs of 32 consecutive amplitudes (512 B) that a warp
+// moves with one coalesced cp.async each.  In shared memory the element
+// index is XOR-swizzled (low 3 bits ^= a linear function of the high bits)
+// so that any 7 of the 12 local bits can serve as thread bits without bank
+// conflicts.
+//
+// A sweep is a list of phases.  In a phase each thread holds 2^RB amplitudes
+// in registers: the ones whose RB "register" local bits vary, at the thread
+// bits given by its thread index.  Gate ops of the phase act on register
+// bits only (dense 2x2 / 4x4, controlled X), so no data is exchanged between
+// threads inside a phase; a new phase re-reads the tile with a new register
+// assignment.  Per-gate arithmetic uses FMA (the tile path is held to the
+// 1e-12 amplitude tolerance, the per-gate kernels to bit-exactness).
+//
+// Diagonal gates never need locality: they are accumulated on the host as a
+// phase polynomial  c * prod_q w_q^{x_q} * prod_{q<r} w_qr^{x_q x_r}  and a
+// FLUSH op applies all terms containing a qubit q right before the first
+// non-diagonal gate on q.  A FLUSH multiplies the amplitudes with x_q = 1 by
+// slot[s] * prod_{thread partners set} w * F[register index], where the
+// per-tile factor slot[s] (q's linear term times its non-local partners
+// whose bits are set in this tile's base index) is computed once per tile.
+#include <cuda_runtime.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <algorithm>
+#include <string>
+#include <vector>
+
+#include "dq_common.cuh"
+#include "dq_fused.cuh"
+#include "dq_gates.hpp"
+
+namespace dq {
+
+namespace {
+
+constexpr int kSwThreads = 128;
+constexpr int kSwTB = 7;      // thread bits (5 lane + 2 warp)
+constexpr int kMaxM = 12;
+constexpr int kMaxSlots = 128;
+
+enum : uint32_t { OP_U1 = 0, OP_U1R, OP_U1X, OP_U2, OP_FLUSH_R, OP_FLUSH_T, OP_GPHASE };
+
+// swizzle vectors of local bits 3..11 (bits 0..2 map to themselves)
+__host__ __device__ constexpr uint32_t swz_g(int k) {
+  return k == 3 ? 3u : k == 4 ? 5u : k == 5 ? 6u : k == 6 ? 7u : k == 7 ? 3u : k == 8 ? 5u
+       : k == 9 ? 6u : k == 10 ? 7u : k == 11 ? 1u : 0u;
+}
+__host__ __device__ constexpr uint32_t swz_vec(int k) { return k < 3 ? (1u << k) : swz_g(k); }
+__host__ __device__ constexpr uint32_t swz(uint32_t e) {
+  uint32_t g = 0;
+  for (int k = 3; k < kMaxM; ++k)
+    if ((e >> k) & 1u) g ^= swz_g(k);
+  return e ^ g;
+}
+
+// ---- device program layout ------------------------------------------------------
+struct SwHeader {
+  uint32_t m, rb, nphase, nslots;
+  uint32_t local_pos[kMaxM];
+  uint32_t off_phase, off_op, off_slot, off_slotent;
+  uint32_t off_data, pad0, pad1, pad2;
+};
+struct SwPhase {
+  uint32_t tpos[kSwTB];
+  uint32_t rpos[5];
+  uint32_t op_begin, op_end, pad0, pad1;
+};
+struct SwOp {
+  uint32_t type, b0, b1, creg;
+  uint32_t ctl_thr, slot, data, flags;
+  uint64_t cnl, pad;
+};
+struct SwSlot {
+  uint32_t count, start, pad0, pad1;
+  double2 w0;
+};
+struct SwSlotEnt {
+  uint64_t mask, pad;
+  double2 w;
+};
+static_assert(sizeof(SwHeader) % 16 == 0 && sizeof(SwPhase) % 16 == 0, "layout");
+static_assert(sizeof(SwOp) % 16 == 0 && sizeof(SwSlot) % 16 == 0 && sizeof(SwSlotEnt) % 16 == 0,
+              "layout");
+
+constexpr uint32_t FL_THR_MASK = 0x7f;     // flags bits 0..6: thread partners present
+                                           // flags bits 8..12: register partners present
+
+// ---- device helpers -------------------------------------------------------------------
+
+// Hide a value's provenance from the optimiser so that addresses are
+// recomputed instead of being kept live (in registers) across a phase.
+__device__ __forceinline__ uint32_t opaque(uint32_t x) {
+  asm volatile("" : "+r"(x));
+  return x;
+}
+__device__ __forceinline__ uint64_t opaque64(uint64_t x) {
+  asm volatile("" : "+l"(x));
+  return x;
+}
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const uint32_t sa = (uint32_t)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
+}
+
+template <int RB, int B>
+__device__ __forceinline__ void u1_gen(double2 (&a)[1 << RB], const double2* __restrict__ D,
+                                       uint32_t creg) {
+  const double2 u00 = D[0], u01 = D[1], u10 = D[2], u11 = D[3];
+#pragma unroll
+  for (int j = 0; j < (1 << RB); ++j) {
+    if (j & (1 << B)) continue;
+    if ((j & creg) != creg) continue;
+    const int k = j | (1 << B);
+    const double2 x = a[j], y = a[k];
+    a[j] = cmac2_f(u00, x, u01, y);
+    a[k] = cmac2_f(u10, x, u11, y);
+  }
+}
+
+template <int RB, int B>
+__device__ __forceinline__ void u1_real(double2 (&a)[1 << RB], const double2* __restrict__ D,
+                                        uint32_t creg) {
+  const double u00 = D[0].x, u01 = D[1].x, u10 = D[2].x, u11 = D[3].x;
+#pragma unroll
+  for (int j = 0; j < (1 << RB); ++j) {
+    if (j & (1 << B)) continue;
+    if ((j & creg) != creg) continue;
+    const int k = j | (1 << B);
+    const double2 x = a[j], y = a[k];
+    a[j] = make_double2(fma(u00, x.x, u01 * y.x), fma(u00, x.y, u01 * y.y));
+    a[k] = make_double2(fma(u10, x.x, u11 * y.x), fma(u10, x.y, u11 * y.y));
+  }
+}
+
+template <int RB, int B>
+__device__ __forceinline__ void u1_x(double2 (&a)[1 << RB], uint32_t creg) {
+#pragma unroll
+  for (int j = 0; j < (1 << RB); ++j) {
+    if (j & (1 << B)) continue;
+    if ((j & creg) != creg) continue;
+    const int k = j | (1 << B);
+    const double2 t = a[j];
+    a[j] = a[k];
+    a[k] = t;
+  }
+}
+
+// dense 4x4 on register bits B0 (MSB of the gate index) and B1, B0 < B1 or not
+template <int RB, int B0, int B1>
+__device__ __forceinline__ void u2_gen(double2 (&a)[1 << RB], const double2* __restrict__ D,
+                                       uint32_t creg) {
+#pragma unroll
+  for (int j = 0; j < (1 << RB); ++j) {
+    if (j & ((1 << B0) | (1 << B1))) continue;
+    if ((j & creg) != creg) continue;
+    const int i0 = j, i1 = j | (1 << B1), i2 = j | (1 << B0), i3 = j | (1 << B0) | (1 << B1);
+    const double2 v0 = a[i0], v1 = a[i1], v2 = a[i2], v3 = a[i3];
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      const double2 s01 = cmac2_f(D[4 * r], v0, D[4 * r + 1], v1);
+      const double2 s23 = cmac2_f(D[4 * r + 2], v2, D[4 * r + 3], v3);
+      const double2 w = make_double2(s01.x + s23.x, s01.y + s23.y);
+      if (r == 0) a[i0] = w;
+      else if (r == 1) a[i1] = w;
+      else if (r == 2) a[i2] = w;
+      else a[i3] = w;
+    }
+  }
+}
+
+// amplitudes with register bit B set: a[j] *= W
+template <int RB, int B>
+__device__ __forceinline__ void scale_reg(double2 (&a)[1 << RB], double2 W) {
+#pragma unroll
+  for (int j = 0; j < (1 << RB); ++j) {
+    if (!(j & (1 << B))) continue;
+    a[j] = cmul_f(a[j], W);
+  }
+}
+
+// amplitudes whose register bits in `sel` are all set: a[j] *= W  (sel static per call site)
+template <int RB>
+__device__ __forceinline__ void scale_sel(double2 (&a)[1 << RB], uint32_t sel, double2 W) {
+#pragma unroll
+  for (int j = 0; j < (1 << RB); ++j) {
+    if ((j & sel) != sel) continue;
+    a[j] = cmul_f(a[j], W);
+  }
+}
+
+#define DQ_SW_CASES1(FN, ...)                    \
+  switch (op.b0) {                               \
+    case 0: FN<RB, 0>(__VA_ARGS__); break;       \
+    case 1: if (RB > 1) FN<RB, (RB > 1 ? 1 : 0)>(__VA_ARGS__); break; \
+    case 2: if (RB > 2) FN<RB, (RB > 2 ? 2 : 0)>(__VA_ARGS__); break; \
+    case 3: if (RB > 3) FN<RB, (RB > 3 ? 3 : 0)>(__VA_ARGS__); break; \
+    case 4: if (RB > 4) FN<RB, (RB > 4 ? 4 : 0)>(__VA_ARGS__); break; \
+    default: break;                              \
+  }
+
+template <int RB>
+__device__ __forceinline__ void u2_dispatch(double2 (&a)[1 << RB], const SwOp& op,
+                                            const double2* __restrict__ D) {
+#define DQ_U2C(X, Y)                                                                   \
+  if (op.b0 == X && op.b1 == Y) {                                                      \
+    if (RB > X && RB > Y) u2_gen<RB, (RB > X ? X : 0), (RB > Y ? Y : 1)>(a, D, op.creg); \
+    return;                                                                            \
+  }
+  DQ_U2C(0, 1) DQ_U2C(0, 2) DQ_U2C(0, 3) DQ_U2C(0, 4) DQ_U2C(1, 2) DQ_U2C(1, 3) DQ_U2C(1, 4)
+  DQ_U2C(2, 3) DQ_U2C(2, 4) DQ_U2C(3, 4)
+#undef DQ_U2C
+}
+
+template <int RB>
+__device__ __forceinline__ void exec_op(const SwOp& op, double2 (&a)[1 << RB],
+                                        const double2* __restrict__ DATA,
+                                        const double2* __restrict__ slots, uint32_t tid,
+                                        uint64_t base) {
+  if ((base & op.cnl) != op.cnl) return;
+  if ((tid & op.ctl_thr) != op.ctl_thr) return;
+  const double2* D = DATA + op.data;
+  switch (op.type) {
+    case OP_U1: DQ_SW_CASES1(u1_gen, a, D, op.creg); break;
+    case OP_U1R: DQ_SW_CASES1(u1_real, a, D, op.creg); break;
+    case OP_U1X: DQ_SW_CASES1(u1_x, a, op.creg); break;
+    case OP_U2: u2_dispatch<RB>(a, op, D); break;
+    case OP_FLUSH_R:
+    case OP_FLUSH_T: {
+      if (op.type == OP_FLUSH_T && !((tid >> op.b0) & 1u)) break;
+      double2 W = slots[op.slot];
+      const uint32_t tm = op.flags & FL_THR_MASK;
+#pragma unroll
+      for (int i = 0; i < kSwTB; ++i)
+        if (((tm & tid) >> i) & 1u) W = cmul_f(W, D[i]);
+      // register partners r: amplitudes with both the target and r set
+      const uint32_t tsel = (op.type == OP_FLUSH_R) ? (1u << op.b0) : 0u;
+      const uint32_t rmask = (op.flags >> 8) & 0x1fu;
+      if (op.type == OP_FLUSH_R) {
+        DQ_SW_CASES1(scale_reg, a, W);
+      } else {
+#pragma unroll
+        for (int j = 0; j < (1 << RB); ++j) a[j] = cmul_f(a[j], W);
+      }
+#pragma unroll 1
+      for (int b = 0; b < RB; ++b)
+        if ((rmask >> b) & 1u) scale_sel<RB>(a, tsel | (1u << b), D[kSwTB + b]);
+      break;
+    }
+    case OP_GPHASE: {
+      const double2 W = slots[op.slot];
+#pragma unroll
+      for (int j = 0; j < (1 << RB); ++j) a[j] = cmul_f(a[j], W);
+      break;
+    }
+    default: break;
+  }
+}
+
+template <int RB>
+__global__ void __launch_bounds__(kSwThreads, 2)
+    k_sweep(double2* __restrict__ state, const uint8_t* __restrict__ blob) {
+  constexpr int M = kSwTB + RB;
+  constexpr int R = 1 << RB;
+  constexpr int NI = 1 << (M - 7);  // runs per warp
+  extern __shared__ __align__(16) unsigned char smraw[];
+  double2* tile = reinterpret_cast<double2*>(smraw);
+  double2* slots = tile + (1 << M);
+  const SwHeader* H = reinterpret_cast<const SwHeader*>(blob);
+  const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
+
+  uint32_t lp[M];
+#pragma unroll
+  for (int k = 0; k < M; ++k) lp[k] = H->local_pos[k];
+  uint64_t base = blockIdx.x;
+#pragma unroll
+  for (int k = 0; k < M; ++k) base = insert_zero(base, lp[k]);
+
+  // per-tile factors of the FLUSH / GPHASE slots
+  {
+    const SwSlot* SL = reinterpret_cast<const SwSlot*>(blob + H->off_slot);
+    const SwSlotEnt* SE = reinterpret_cast<const SwSlotEnt*>(blob + H->off_slotent);
+    for (uint32_t s = tid; s < H->nslots; s += kSwThreads) {
+      double2 w = SL[s].w0;
+      const uint32_t c = SL[s].count, st = SL[s].start;
+      for (uint32_t e = 0; e < c; ++e) {
+        const SwSlotEnt& E = SE[st + e];
+        if ((base & E.mask) == E.mask) w = cmul_f(w, E.w);
+      }
+      slots[s] = w;
+    }
+  }
+
+  // stage the tile: run r = warp | i << 2 covers local bits 5..M-1
+  uint64_t wofs = base | lane;
+  if (warp & 1u) wofs |= 1ULL << lp[5];
+  if (warp & 2u) wofs |= 1ULL << lp[6];
+  const uint32_t swt = swz(lane | (warp << 5));
+#pragma unroll
+  for (int i = 0; i < NI; ++i) {
+    uint64_t g = wofs;
+#pragma unroll
+    for (int b = 0; b < M - 7; ++b)
+      if ((i >> b) & 1) g |= 1ULL << lp[7 + b];
+    cp_async16(&tile[swt ^ swz((uint32_t)i << 7)], state + g);
+  }
+  cp_async_wait_all();
+  __syncthreads();
+
+  const SwPhase* PH = reinterpret_cast<const SwPhase*>(blob + H->off_phase);
+  const SwOp* OPS = reinterpret_cast<const SwOp*>(blob + H->off_op);
+  const double2* DATA = reinterpret_cast<const double2*>(blob + H->off_data);
+  const uint32_t nph = H->nphase;
+  for (uint32_t p = 0; p < nph; ++p) {
+    const SwPhase& P = PH[p];
+    uint32_t tl = 0;
+#pragma unroll
+    for (int i = 0; i < kSwTB; ++i) tl |= ((tid >> i) & 1u) << P.tpos[i];
+    const uint32_t pt = swz(tl);
+    uint32_t V[RB > 0 ? RB : 1];
+#pragma unroll
+    for (int b = 0; b < RB; ++b) V[b] = swz(1u << P.rpos[b]);
+    double2 a[R];
+#pragma unroll
+    for (int j = 0; j < R; ++j) {
+      uint32_t x = pt;
+#pragma unroll
+      for (int b = 0; b < RB; ++b)
+        if ((j >> b) & 1) x ^= V[b];
+      a[j] = tile[x];
+    }
+    for (uint32_t o = P.op_begin; o < P.op_end; ++o) exec_op<RB>(OPS[o], a, DATA, slots, tid, base);
+    const uint32_t pt2 = opaque(pt);
+#pragma unroll
+    for (int b = 0; b < RB; ++b) V[b] = opaque(V[b]);
+#pragma unroll
+    for (int j = 0; j < R; ++j) {
+      uint32_t x = pt2;
+#pragma unroll
+      for (int b = 0; b < RB; ++b)
+        if ((j >> b) & 1) x ^= V[b];
+      tile[x] = a[j];
+    }
+    __syncthreads();
+  }
+
+  // store: recompute the run offsets (nothing of the load loop stays live)
+  const uint64_t wofs2 = opaque64(wofs);
+  const uint32_t swt2 = opaque(swt);
+  const SwHeader* H2 = reinterpret_cast<const SwHeader*>(opaque64(reinterpret_cast<uint64_t>(H)));
+  uint64_t hib[M - 7 > 0 ? M - 7 : 1];
+#pragma unroll
+  for (int b = 0; b < M - 7; ++b) hib[b] = 1ULL << H2->local_pos[7 + b];
+#pragma unroll
+  for (int i = 0; i < NI; ++i) {
+    uint64_t g = wofs2;
+#pragma unroll
+    for (int b = 0; b < M - 7; ++b)
+      if ((i >> b) & 1) g |= hib[b];
+    state[g] = tile[swt2 ^ swz((uint32_t)i << 7)];
+  }
+}
+
+// ---- relabel materialisation: paired-tile involution of bit positions ------------
+//
+// A bit-position involution tau (tau(tau(p)) = p) moves amplitude i to tau(i).
+// With a local set L closed under tau, tile T maps onto tile tau(T), element
+// e onto tau_L(e); one CTA exchanges the pair (T, tau(T)) so the permutation
+// is race-free in place.
+
+struct PermParams {
+  uint32_t m;             // |L|
+  uint32_t L[kMaxM];      // local positions, ascending
+  uint32_t tauL[kMaxM];   // local index of tau(L[k])
+  uint32_t tau[64];       // tau on all positions
+  uint32_t n;
+};
+
+__device__ __forceinline__ uint32_t perm_slot(uint32_t e) { return e + (e >> 4); }  // pad 1 per 16
+
+__global__ void __launch_bounds__(256) k_permute_pairs(double2* __restrict__ state, PermParams P) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  const uint32_t cnt = 1u << P.m;
+  double2* A = reinterpret_cast<double2*>(smraw);
+  double2* B = A + perm_slot(cnt);
+  uint64_t bT = blockIdx.x;
+  for (uint32_t k = 0; k < P.m; ++k) bT = insert_zero(bT, P.L[k]);
+  uint64_t bU = 0;
+  for (uint32_t p = 0; p < P.n; ++p)
+    if ((bT >> p) & 1ULL) bU |= 1ULL << P.tau[p];
+  if (bU < bT) return;  // the partner CTA handles this pair
+  const bool self = (bU == bT);
+  // element e of a tile: global offset dep(e)
+  for (uint32_t e = threadIdx.x; e < cnt; e += blockDim.x) {
+    uint64_t d = 0;
+    for (uint32_t k = 0; k < P.m; ++k)
+      if ((e >> k) & 1u) d |= 1ULL << P.L[k];
+    A[perm_slot(e)] = state[bT | d];
+    if (!self) B[perm_slot(e)] = state[bU | d];
+  }
+  __syncthreads();
+  for (uint32_t e = threadIdx.x; e < cnt; e += blockDim.x) {
+    uint64_t d = 0;
+    uint32_t te = 0;
+    for (uint32_t k = 0; k < P.m; ++k)
+      if ((e >> k) & 1u) {
+        d |= 1ULL << P.L[k];
+        te |= 1u << P.tauL[k];
+      }
+    // destination element e of tile U receives source element tau_L(e) of tile T
+    state[bU | d] = A[perm_slot(te)];
+    if (!self) state[bT | d] = B[perm_slot(te)];
+  }
+}
+
+// =========================================================================
+// host side: planner
+// =========================================================================
+
+inline hc conj(hc a) { return hc{a.re, -a.im}; }
+inline bool is_unit_phase(hc a) { return fabs(a.re * a.re + a.im * a.im - 1.0) < 1e-12; }
+
+enum PKind { PG_DIAG, PG_U1, PG_U1X, PG_U2 };
+
+struct PGate {
+  PKind kind = PG_DIAG;
+  uint32_t t0 = 0, t1 = 0;  // physical targets (U2: t0 = MSB of the gate index)
+  uint64_t ctrl = 0;        // physical controls (all must be 1)
+  hc u[16];
+  bool real = false;
+  // diagonal terms
+  hc cst{1, 0};
+  int nlin = 0;
+  uint32_t lq[2] = {0, 0};
+  hc lw[2];
+  bool quad = false;
+  uint32_t qa = 0, qb = 0;
+  hc qw{1, 0};
+  uint64_t touched = 0;
+};
+
+struct Poly {
+  uint32_t n = 0;
+  std::vector<hc> lin;
+  std::vector<char> hl;
+  std::vector<hc> quad;
+  std::vector<char> hq;
+  std::vector<int> cnt;
+  hc cst{1, 0};
+  bool has_cst = false;
+
+  void init(uint32_t nq) {
+    n = nq;
+    lin.assign(n, hc{1, 0});
+    hl.assign(n, 0);
+    quad.assign((size_t)n * n, hc{1, 0});
+    hq.assign((size_t)n * n, 0);
+    cnt.assign(n, 0);
+    cst = hc{1, 0};
+    has_cst = false;
+  }
+  void mul_lin(uint32_t q, hc w) {
+    if (!hl[q]) { hl[q] = 1; ++cnt[q]; lin[q] = w; } else lin[q] = lin[q] * w;
+  }
+  void mul_quad(uint32_t a, uint32_t b, hc w) {
+    const uint32_t lo = std::min(a, b), hi = std::max(a, b);
+    const size_t k = (size_t)lo * n + hi;
+    if (!hq[k]) { hq[k] = 1; ++cnt[lo]; ++cnt[hi]; quad[k] = w; } else quad[k] = quad[k] * w;
+  }
+  void add(const PGate& g) {
+    if (!(g.cst.re == 1.0 && g.cst.im == 0.0)) { cst = cst * g.cst; has_cst = true; }
+    for (int i = 0; i < g.nlin; ++i) mul_lin(g.lq[i], g.lw[i]);
+    if (g.quad) mul_quad(g.qa, g.qb, g.qw);
+  }
+  bool pending(uint32_t q) const { return cnt[q] > 0; }
+  bool empty() const {
+    for (uint32_t q = 0; q < n; ++q)
+      if (cnt[q]) return false;
+    return true;
+  }
+  // remove and return all terms containing q
+  void take(uint32_t q, hc* wlin, std::vector<std::pair<uint32_t, hc>>& partners) {
+    *wlin = hl[q] ? lin[q] : hc{1, 0};
+    if (hl[q]) { hl[q] = 0; --cnt[q]; lin[q] = hc{1, 0}; }
+    partners.clear();
+    for (uint32_t r = 0; r < n; ++r) {
+      if (r == q) continue;
+      const uint32_t lo = std::min(q, r), hi = std::max(q, r);
+      const size_t k = (size_t)lo * n + hi;
+      if (!hq[k]) continue;
+      partners.push_back({r, quad[k]});
+      hq[k] = 0;
+      quad[k] = hc{1, 0};
+      --cnt[q];
+      --cnt[r];
+    }
+  }
+};
+
+struct POp {
+  uint32_t type;
+  int gate = -1;            // index into the segment's gate list
+  uint32_t q = 0;           // FLUSH target (physical)
+  hc wlin{1, 0};
+  std::vector<std::pair<uint32_t, hc>> partners;   // FLUSH partners (physical)
+  hc gcst{1, 0};                                  // GPHASE constant
+  std::vector<std::pair<uint64_t, hc>> gterms;     // GPHASE per-tile terms (masks)
+};
+
+struct PSweep {
+  std::vector<uint32_t> local;  // physical, ascending, size m
+  std::vector<POp> ops;
+};
+
+// Blob writer (16-byte aligned sections)
+struct Blob {
+  std::vector<uint8_t> buf;
+  size_t align16() {
+    while (buf.size() % 16) buf.push_back(0);
+    return buf.size();
+  }
+  template <class T>
+  size_t put(const T* p, size_t count) {
+    const size_t off = align16();
+    const uint8_t* s = reinterpret_cast<const uint8_t*>(p);
+    buf.insert(buf.end(), s, s + sizeof(T) * count);
+    return off;
+  }
+};
+
+struct Planner {
+  uint32_t n = 0, M = 12, RB = 5;
+  double budget = 64.0;
+  bool single_tile = false;
+
+  // cost in FP64 instructions per amplitude
+  double gate_cost(const PGate& g) const {
+    const double frac = 1.0 / (double)(1ULL << __builtin_popcountll(g.ctrl));
+    switch (g.kind) {
+      case PG_U1: return (g.real ? 4.0 : 8.0) * frac;
+      case PG_U1X: return 0.5;
+      case PG_U2: return 16.0 * frac;
+      default: return 0.0;
+    }
+  }
+
+  static uint64_t targets(const PGate& g) {
+    if (g.kind == PG_DIAG) return 0;
+    if (g.kind == PG_U2) return (1ULL << g.t0) | (1ULL << g.t1);
+    return 1ULL << g.t0;
+  }
+
+  // Split the gate list into sweeps; poly carries pending diagonal terms.
+  void plan(std::vector<PGate>& G, Poly& poly, std::vector<PSweep>& out) {
+    std::vector<int> rem(G.size());
+    for (size_t i = 0; i < G.size(); ++i) rem[i] = (int)i;
+    const uint64_t low_mask = single_tile ? ((n >= 64) ? ~0ULL : ((1ULL << n) - 1)) : 0x1FULL;
+    while (!rem.empty()) {
+      uint64_t S = low_mask;
+      uint64_t blocked = 0;
+      double cost = 0.0;
+      std::vector<int> incl, next;
+      bool any_nd = false;
+      for (int gi : rem) {
+        const PGate& g = G[gi];
+        if (g.touched & blocked) {
+          next.push_back(gi);
+          blocked |= g.touched;
+          continue;
+        }
+        if (g.kind == PG_DIAG) {
+          incl.push_back(gi);
+          continue;
+        }
+        const uint64_t need = targets(g);
+        const uint64_t ns = S | need;
+        double c = gate_cost(g);
+        uint64_t tm = need;
+        while (tm) {
+          const int t = __builtin_ctzll(tm);
+          tm &= tm - 1;
+          c += 2.5;  // a flush of the target, if pending
+          (void)t;
+        }
+        const bool fits = (uint32_t)__builtin_popcountll(ns) <= M;
+        const bool afford = single_tile || !any_nd || cost + c <= budget;
+        if (!fits || !afford) {
+          next.push_back(gi);
+          blocked |= g.touched;
+          continue;
+        }
+        S = ns;
+        cost += c;
+        any_nd = true;
+        incl.push_back(gi);
+      }
+      // pad the local set to M qubits now: every later decision (which flush
+      // partners are local, which per-tile terms test base bits) depends on it
+      for (uint32_t q = 0; q < n && (uint32_t)__builtin_popcountll(S) < M; ++q) S |= 1ULL << q;
+      PSweep sw;
+      for (int gi : incl) {
+        const PGate& g = G[gi];
+        if (g.kind == PG_DIAG) {
+          poly.add(g);
+          continue;
+        }
+        uint64_t tm = targets(g);
+        while (tm) {
+          const uint32_t t = (uint32_t)__builtin_ctzll(tm);
+          tm &= tm - 1;
+          if (poly.pending(t)) {
+            POp f;
+            f.type = OP_FLUSH_R;
+            f.q = t;
+            poly.take(t, &f.wlin, f.partners);
+            sw.ops.push_back(std::move(f));
+          }
+        }
+        POp op;
+        op.type = g.kind == PG_U1 ? (g.real ? OP_U1R : OP_U1) : g.kind == PG_U1X ? OP_U1X : OP_U2;
+        op.gate = gi;
+        sw.ops.push_back(std::move(op));
+      }
+      for (uint32_t q = 0; q < n; ++q)
+        if (S >> q & 1ULL) sw.local.push_back(q);
+      out.push_back(std::move(sw));
+      rem.swap(next);
+    }
+  }
+
+  // Apply every pending term in the last sweep (appending one if needed).
+  void final_flush(Poly& poly, std::vector<PSweep>& sweeps) {
+    if (poly.empty() && !poly.has_cst) return;
+    if (sweeps.empty()) {
+      PSweep sw;
+      uint64_t S = single_tile ? ((n >= 64) ? ~0ULL : ((1ULL << n) - 1)) : 0x1FULL;
+      for (uint32_t q = 0; q < n && (uint32_t)__builtin_popcountll(S) < M; ++q)
+        if (poly.pending(q)) S |= 1ULL << q;
+      for (uint32_t q = 0; q < n && (uint32_t)__builtin_popcountll(S) < M; ++q) S |= 1ULL << q;
+      for (uint32_t q = 0; q < n; ++q)
+        if (S >> q & 1ULL) sw.local.push_back(q);
+      sweeps.push_back(std::move(sw));
+    }
+    PSweep& last = sweeps.back();
+    uint64_t S = 0;
+    for (uint32_t q : last.local) S |= 1ULL << q;
+    for (uint32_t q = 0; q < n; ++q) {
+      if (!(S >> q & 1ULL) || !poly.pending(q)) continue;
+      POp f;
+      f.type = OP_FLUSH_T;  // resolved to R/T by the phase layout
+      f.q = q;
+      poly.take(q, &f.wlin, f.partners);
+      last.ops.push_back(std::move(f));
+    }
+    // what is left involves non-local qubits only: a per-tile constant
+    POp gp;
+    gp.type = OP_GPHASE;
+    gp.gcst = poly.has_cst ? poly.cst : hc{1, 0};
+    for (uint32_t q = 0; q < n; ++q) {
+      if (poly.hl[q]) gp.gterms.push_back({1ULL << q, poly.lin[q]});
+      for (uint32_t r = q + 1; r < n; ++r) {
+        const size_t k = (size_t)q * n + r;
+        if (poly.hq[k]) gp.gterms.push_back({(1ULL << q) | (1ULL << r), poly.quad[k]});
+      }
+    }
+    const bool trivial = gp.gterms.empty() && gp.gcst.re == 1.0 && gp.gcst.im == 0.0;
+    if (!trivial) last.ops.push_back(std::move(gp));
+    poly.init(n);
+  }
+};
+
+// choose thread-bit order: lanes 0..2 need linearly independent swizzle vectors
+bool order_thread_bits(std::vector<uint32_t>& tb) {
+  const size_t c = tb.size();
+  for (size_t i = 0; i < c; ++i)
+    for (size_t j = i + 1; j < c; ++j)
+      for (size_t k = j + 1; k < c; ++k) {
+        const uint32_t a = swz_vec(tb[i]), b = swz_vec(tb[j]), d = swz_vec(tb[k]);
+        if (a == b || (a ^ b) == 0 || d == a || d == b || d == (a ^ b)) continue;
+        std::vector<uint32_t> o = {tb[i], tb[j], tb[k]};
+        for (size_t x = 0; x < c; ++x)
+          if (x != i && x != j && x != k) o.push_back(tb[x]);
+        tb = o;
+        return true;
+      }
+  return false;
+}
+
+// Encode a planned sweep into the device blob format.
+int encode_sweep(const PSweep& sw, const std::vector<PGate>& G, uint32_t RB, Blob& blob,
+                 size_t* offset) {
+  const uint32_t m = (uint32_t)sw.local.size();
+  if (m != kSwTB + RB) return fail(DQ_ERR_INTERNAL, "sweep local set size mismatch");
+  int lidx[64];
+  for (int i = 0; i < 64; ++i) lidx[i] = -1;
+  for (uint32_t k = 0; k < m; ++k) lidx[sw.local[k]] = (int)k;
+
+  // phases: consecutive ops whose register needs fit RB register bits
+  struct PhaseTmp {
+    std::vector<uint32_t> regs;  // local bits
+    size_t ob, oe;
+  };
+  std::vector<PhaseTmp> phases;
+  auto need_of = [&](const POp& op, std::vector<uint32_t>& nd) {
+    nd.clear();
+    if (op.type == OP_U1 || op.type == OP_U1R || op.type == OP_U1X) {
+      nd.push_back((uint32_t)lidx[G[op.gate].t0]);
+    } else if (op.type == OP_U2) {
+      nd.push_back((uint32_t)lidx[G[op.gate].t0]);
+      nd.push_back((uint32_t)lidx[G[op.gate].t1]);
+    } else if (op.type == OP_FLUSH_R) {
+      nd.push_back((uint32_t)lidx[op.q]);   // precedes the gate on q: same phase
+    }
+  };
+  {
+    size_t i = 0;
+    std::vector<uint32_t> nd;
+    while (i < sw.ops.size()) {
+      PhaseTmp ph;
+      ph.ob = i;
+      size_t j = i;
+      while (j < sw.ops.size()) {
+        need_of(sw.ops[j], nd);
+        std::vector<uint32_t> u = ph.regs;
+        for (uint32_t b : nd)
+          if (std::find(u.begin(), u.end(), b) == u.end()) u.push_back(b);
+        if (u.size() > RB) break;
+        ph.regs = u;
+        ++j;
+      }
+      if (j == i) return fail(DQ_ERR_INTERNAL, "op needs more register bits than a phase has");
+      ph.oe = j;
+      phases.push_back(ph);
+      i = j;
+    }
+    if (phases.empty()) phases.push_back(PhaseTmp{{}, 0, 0});
+  }
+
+  std::vector<SwPhase> P;
+  std::vector<SwOp> O;
+  std::vector<SwSlot> SL;
+  std::vector<SwSlotEnt> SE;
+  std::vector<double2> D;
+  auto d2 = [](hc z) { return make_double2(z.re, z.im); };
+  auto add_slot = [&](hc w0, const std::vector<std::pair<uint64_t, hc>>& ents) -> uint32_t {
+    SwSlot s{};
+    s.count = (uint32_t)ents.size();
+    s.start = (uint32_t)SE.size();
+    s.w0 = d2(w0);
+    for (auto& e : ents) {
+      SwSlotEnt x{};
+      x.mask = e.first;
+      x.w = d2(e.second);
+      SE.push_back(x);
+    }
+    SL.push_back(s);
+    return (uint32_t)SL.size() - 1;
+  };
+
+  for (const PhaseTmp& ph : phases) {
+    SwPhase sp{};
+    std::vector<uint32_t> regs = ph.regs;
+    for (uint32_t b = 0; b < m && regs.size() < RB; ++b)
+      if (std::find(regs.begin(), regs.end(), b) == regs.end()) regs.push_back(b);
+    std::vector<uint32_t> tb;
+    for (uint32_t b = 0; b < m; ++b)
+      if (std::find(regs.begin(), regs.end(), b) == regs.end()) tb.push_back(b);
+    if (tb.size() != (size_t)kSwTB || !order_thread_bits(tb))
+      return fail(DQ_ERR_INTERNAL, "no bank-conflict-free thread layout");
+    int rix[kMaxM], tix[kMaxM];
+    for (int i = 0; i < kMaxM; ++i) rix[i] = tix[i] = -1;
+    for (uint32_t b = 0; b < RB; ++b) { sp.rpos[b] = regs[b]; rix[regs[b]] = (int)b; }
+    for (int i = 0; i < kSwTB; ++i) { sp.tpos[i] = tb[i]; tix[tb[i]] = i; }
+    sp.op_begin = (uint32_t)O.size();
+    for (size_t oi = ph.ob; oi < ph.oe; ++oi) {
+      const POp& op = sw.ops[oi];
+      SwOp so{};
+      so.type = op.type;
+      if (op.type == OP_U1 || op.type == OP_U1R || op.type == OP_U1X || op.type == OP_U2) {
+        const PGate& g = G[op.gate];
+        // controls: register bits, thread bits, non-local
+        uint64_t cm = g.ctrl;
+        while (cm) {
+          const uint32_t c = (uint32_t)__builtin_ctzll(cm);
+          cm &= cm - 1;
+          const int l = lidx[c];
+          if (l < 0) so.cnl |= 1ULL << c;
+          else if (rix[l] >= 0) so.creg |= 1u << rix[l];
+          else so.ctl_thr |= 1u << tix[l];
+        }
+        so.data = (uint32_t)D.size();
+        if (op.type == OP_U2) {
+          int r0 = rix[lidx[g.t0]], r1 = rix[lidx[g.t1]];
+          hc mm[16];
+          for (int i = 0; i < 16; ++i) mm[i] = g.u[i];
+          if (r0 > r1) {  // put the lower register bit first: swap the gate's index bits
+            const int perm[4] = {0, 2, 1, 3};
+            for (int r = 0; r < 4; ++r)
+              for (int c = 0; c < 4; ++c) mm[r * 4 + c] = g.u[perm[r] * 4 + perm[c]];
+            std::swap(r0, r1);
+          }
+          so.b0 = (uint32_t)r0;
+          so.b1 = (uint32_t)r1;
+          for (int i = 0; i < 16; ++i) D.push_back(d2(mm[i]));
+        } else {
+          so.b0 = (uint32_t)rix[lidx[g.t0]];
+          for (int i = 0; i < 4; ++i) D.push_back(d2(g.u[i]));
+        }
+      } else if (op.type == OP_FLUSH_R || op.type == OP_FLUSH_T) {
+        const int l = lidx[op.q];
+        std::vector<std::pair<uint64_t, hc>> nl;
+        hc wthr[kSwTB];
+        for (int i = 0; i < kSwTB; ++i) wthr[i] = hc{1, 0};
+        hc wreg[5];
+        for (int i = 0; i < 5; ++i) wreg[i] = hc{1, 0};
+        bool hasF = false;
+        for (auto& pr : op.partners) {
+          const int pl = lidx[pr.first];
+          if (pl < 0) {
+            nl.push_back({1ULL << pr.first, pr.second});
+          } else if (rix[pl] >= 0) {
+            wreg[rix[pl]] = wreg[rix[pl]] * pr.second;
+            hasF = true;
+          } else {
+            wthr[tix[pl]] = wthr[tix[pl]] * pr.second;
+            so.flags |= 1u << tix[pl];
+          }
+        }
+        so.slot = add_slot(op.wlin, nl);
+        if (rix[l] >= 0) {
+          so.type = OP_FLUSH_R;
+          so.b0 = (uint32_t)rix[l];
+        } else {
+          so.type = OP_FLUSH_T;
+          so.b0 = (uint32_t)tix[l];
+        }
+        so.data = (uint32_t)D.size();
+        for (int i = 0; i < kSwTB; ++i) D.push_back(d2(wthr[i]));
+        for (uint32_t b = 0; b < 5; ++b) {
+          D.push_back(d2(wreg[b]));
+          if (b < RB && !(wreg[b].re == 1.0 && wreg[b].im == 0.0)) so.flags |= 1u << (8 + b);
+        }
+        (void)hasF;
+      } else if (op.type == OP_GPHASE) {
+        so.slot = add_slot(op.gcst, op.gterms);
+      }
+      O.push_back(so);
+    }
+    sp.op_end = (uint32_t)O.size();
+    P.push_back(sp);
+  }
+  if (SL.size() > (size_t)kMaxSlots) return fail(DQ_ERR_INTERNAL, "too many per-tile slots");
+
+  for (const SwPhase& sp : P) {
+    for (int i = 0; i < kSwTB; ++i)
+      if (sp.tpos[i] >= m) return fail(DQ_ERR_INTERNAL, "thread bit outside the tile");
+    for (uint32_t b = 0; b < RB; ++b)
+      if (sp.rpos[b] >= m) return fail(DQ_ERR_INTERNAL, "register bit outside the tile");
+  }
+  for (const SwOp& so : O)
+    if ((so.type <= OP_U2 && so.b0 >= RB) || (so.type == OP_U2 && so.b1 >= RB) ||
+        so.slot >= SL.size() + (SL.empty() ? 1 : 0) || so.data > D.size())
+      return fail(DQ_ERR_INTERNAL, "op encoding out of range");
+  SwHeader h{};
+  h.m = m;
+  h.rb = RB;
+  h.nphase = (uint32_t)P.size();
+  h.nslots = (uint32_t)SL.size();
+  for (uint32_t k = 0; k < m; ++k) h.local_pos[k] = sw.local[k];
+  const size_t hoff = blob.put(&h, 1);
+  const size_t po = blob.put(P.data(), P.size());
+  const size_t oo = O.empty() ? blob.align16() : blob.put(O.data(), O.size());
+  const size_t so = SL.empty() ? blob.align16() : blob.put(SL.data(), SL.size());
+  const size_t eo = SE.empty() ? blob.align16() : blob.put(SE.data(), SE.size());
+  const size_t dd = D.empty() ? blob.align16() : blob.put(D.data(), D.size());
+  SwHeader* hp = reinterpret_cast<SwHeader*>(blob.buf.data() + hoff);
+  hp->off_phase = (uint32_t)(po - hoff);
+  hp->off_op = (uint32_t)(oo - hoff);
+  hp->off_slot = (uint32_t)(so - hoff);
+  hp->off_slotent = (uint32_t)(eo - hoff);
+  hp->off_data = (uint32_t)(dd - hoff);
+  *offset = hoff;
+  return DQ_OK;
+}
+
+// ---- gate conversion ----------------------------------------------------------------
+
+// Convert one instruction (logical qubits mapped through perm) into planner
+// gates.  Returns false if the fused path cannot represent it.
+bool convert_inst(const dq_inst& in, const uint32_t* perm, std::vector<PGate>& out,
+                  uint32_t* swap_a, uint32_t* swap_b, bool* is_swap) {
+  *is_swap = false;
+  hc u[4];
+  auto diag1 = [&](uint32_t t, hc u00, hc u11, uint64_t ctrl) -> bool {
+    // diag(u00, u11) on t with <= 1 control; returns false for more controls
+    PGate g;
+    g.kind = PG_DIAG;
+    const int nc = __builtin_popcountll(ctrl);
+    if (nc > 1 || !is_unit_phase(u00) || !is_unit_phase(u11)) return false;
+    const hc rel = (u00.re == 1.0 && u00.im == 0.0) ? u11 : u11 * conj(u00);
+    if (nc == 0) {
+      if (!(u00.re == 1.0 && u00.im == 0.0)) g.cst = u00;
+      g.nlin = 1;
+      g.lq[0] = t;
+      g.lw[0] = rel;
+      g.touched = 1ULL << t;
+    } else {
+      const uint32_t c = (uint32_t)__builtin_ctzll(ctrl);
+      if (!(u00.re == 1.0 && u00.im == 0.0)) {
+        g.nlin = 1;
+        g.lq[0] = c;
+        g.lw[0] = u00;
+      }
+      g.quad = true;
+      g.qa = c;
+      g.qb = t;
+      g.qw = rel;
+      g.touched = (1ULL << t) | ctrl;
+    }
+    out.push_back(g);
+    return true;
+  };
+  auto u1 = [&](uint32_t t, const hc* m, uint64_t ctrl, bool xperm) {
+    PGate g;
+    g.kind = xperm ? PG_U1X : PG_U1;
+    g.t0 = t;
+    g.ctrl = ctrl;
+    for (int i = 0; i < 4; ++i) g.u[i] = m[i];
+    g.real = !xperm && m[0].im == 0.0 && m[1].im == 0.0 && m[2].im == 0.0 && m[3].im == 0.0;
+    g.touched = (1ULL << t) | ctrl;
+    out.push_back(g);
+  };
+  if (matrix_1q(in.kind, in.p, u)) {
+    const uint32_t t = perm[in.q[0]];
+    if (is_zero(u[1]) && is_zero(u[2]) && diag1(t, u[0], u[3], 0)) return true;
+    const bool xp = is_zero(u[0]) && is_zero(u[3]) && is_one(u[1]) && is_one(u[2]);
+    u1(t, u, 0, xp);
+    return true;
+  }
+  Gate g;
+  if (!matrix_nq(in, g)) return false;
+  for (uint32_t b = 0; b < g.k; ++b) g.qubits[b] = perm[g.qubits[b]];
+  GateOp op;
+  classify(g, op);
+  switch (op.cls) {
+    case GC_PHASE: {
+      const hc one{1, 0};
+      if (__builtin_popcountll(op.ctrl_mask) <= 1 && diag1(op.target, one, op.u[0], op.ctrl_mask))
+        return true;
+      hc m[4] = {one, hc{0, 0}, hc{0, 0}, op.u[0]};
+      u1(op.target, m, op.ctrl_mask, false);
+      return true;
+    }
+    case GC_ONE_Q:
+      if (is_zero(op.u[1]) && is_zero(op.u[2]) && __builtin_popcountll(op.ctrl_mask) <= 1 &&
+          diag1(op.target, op.u[0], op.u[3], op.ctrl_mask))
+        return true;
+      u1(op.target, op.u, op.ctrl_mask, false);
+      return true;
+    case GC_XPERM: {
+      hc m[4] = {hc{0, 0}, hc{1, 0}, hc{1, 0}, hc{0, 0}};
+      u1(op.target, m, op.ctrl_mask, true);
+      return true;
+    }
+    case GC_SWAP: {
+      if (op.ctrl_mask == 0) {
+        *is_swap = true;
+        // logical qubits of the swap (relabel the logical -> physical map)
+        *swap_a = (uint32_t)in.q[in.nq - 2];
+        *swap_b = (uint32_t)in.q[in.nq - 1];
+        return true;
+      }
+      // controlled swap = cx(b->a) . ccx(c, a -> b) . cx(b->a), exact permutations
+      const uint32_t a = op.target, b = op.target2;
+      hc xm[4] = {hc{0, 0}, hc{1, 0}, hc{1, 0}, hc{0, 0}};
+      u1(a, xm, (1ULL << b), true);
+      u1(b, xm, op.ctrl_mask | (1ULL << a), true);
+      u1(a, xm, (1ULL << b), true);
+      return true;
+    }
+    case GC_DIAG: {
+      if (g.k != 2) return false;
+      const hc d00 = g.m[0], d01 = g.m[5], d10 = g.m[10], d11 = g.m[15];
+      if (!is_unit_phase(d00) || !is_unit_phase(d01) || !is_unit_phase(d10) || !is_unit_phase(d11))
+        return false;
+      PGate p;
+      p.kind = PG_DIAG;
+      const uint32_t qa = g.qubits[0], qb = g.qubits[1];
+      p.cst = d00;
+      p.nlin = 2;
+      p.lq[0] = qa;
+      p.lw[0] = d10 * conj(d00);
+      p.lq[1] = qb;
+      p.lw[1] = d01 * conj(d00);
+      p.quad = true;
+      p.qa = qa;
+      p.qb = qb;
+      p.qw = d11 * d00 * conj(d01) * conj(d10);
+      p.touched = (1ULL << qa) | (1ULL << qb);
+      out.push_back(p);
+      return true;
+    }
+    case GC_DENSE: {
+      if (g.k != 2) return false;
+      PGate p;
+      p.kind = PG_U2;
+      p.t0 = g.qubits[0];
+      p.t1 = g.qubits[1];
+      for (int i = 0; i < 16; ++i) p.u[i] = g.m[i];
+      p.touched = (1ULL << p.t0) | (1ULL << p.t1);
+      out.push_back(p);
+      return true;
+    }
+    default:
+      return false;
+  }
+}
+
+template <int RB>
+int launch_sweep_rb(double2* amp, uint32_t n, const uint8_t* dblob, cudaStream_t st) {
+  constexpr int M = kSwTB + RB;
+  const size_t smem = sizeof(double2) * ((1u << M) + kMaxSlots);
+  static uint64_t attr_done = 0;  // one bit per device
+  int dev = 0;
+  DQ_CUDA_TRY(cudaGetDevice(&dev));
+  if (!((attr_done >> (dev & 63)) & 1ULL)) {
+    DQ_CUDA_TRY(cudaFuncSetAttribute(k_sweep<RB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)smem));
+    attr_done |= 1ULL << (dev & 63);
+  }
+  const uint64_t tiles = 1ULL << (n - M);
+  k_sweep<RB><<<(unsigned)tiles, kSwThreads, smem, st>>>(amp, dblob);
+  DQ_CUDA_TRY(cudaGetLastError());
+  return DQ_OK;
+}
+
+int launch_sweep(double2* amp, uint32_t n, uint32_t RB, const uint8_t* dblob, cudaStream_t st) {
+  switch (RB) {
+    case 2: return launch_sweep_rb<2>(amp, n, dblob, st);
+    case 3: return launch_sweep_rb<3>(amp, n, dblob, st);
+    case 4: return launch_sweep_rb<4>(amp, n, dblob, st);
+    case 5: return launch_sweep_rb<5>(amp, n, dblob, st);
+    default: return fail(DQ_ERR_INTERNAL, "unsupported register width");
+  }
+}
+
+int ensure_capacity(FusedWork& fw, size_t bytes, cudaStream_t st) {
+  if (bytes <= fw.d_cap && bytes <= fw.h_cap) return DQ_OK;
+  DQ_CUDA_TRY(cudaStreamSynchronize(st));
+  size_t cap = std::max<size_t>(bytes, 1 << 16);
+  cap = std::max(cap, fw.d_cap * 2);
+  if (fw.d_blob) cudaFree(fw.d_blob);
+  if (fw.h_blob) cudaFreeHost(fw.h_blob);
+  fw.d_blob = nullptr;
+  fw.h_blob = nullptr;
+  fw.d_cap = fw.h_cap = 0;
+  DQ_CUDA_TRY(cudaMalloc((void**)&fw.d_blob, cap));
+  DQ_CUDA_TRY(cudaMallocHost((void**)&fw.h_blob, cap));
+  fw.d_cap = fw.h_cap = cap;
+  return DQ_OK;
+}
+
+}  // namespace
+
+void fused_release(FusedWork& fw) {
+  if (fw.d_blob) cudaFree(fw.d_blob);
+  if (fw.h_blob) cudaFreeHost(fw.h_blob);
+  for (auto e : fw.events) cudaEventDestroy(e);
+  fw = FusedWork();
+}
+
+// ---- relabel materialisation ------------------------------------------------------------
+
+int materialize_perm(double2* amp, uint32_t n, uint32_t* perm, cudaStream_t st, uint64_t* launches) {
+  // sigma(p) = logical qubit stored at physical p: data bit p moves to sigma(p)
+  uint32_t sigma[64];
+  bool ident = true;
+  for (uint32_t l = 0; l < n; ++l) {
+    sigma[perm[l]] = l;
+    if (perm[l] != l) ident = false;
+  }
+  if (ident) return DQ_OK;
+  // sigma = tau2 o tau1, both involutions (cycle reflections)
+  uint32_t tau1[64], tau2[64];
+  for (uint32_t p = 0; p < n; ++p) tau1[p] = tau2[p] = p;
+  std::vector<char> seen(n, 0);
+  for (uint32_t p = 0; p < n; ++p) {
+    if (seen[p]) continue;
+    std::vector<uint32_t> cyc;
+    uint32_t x = p;
+    while (!seen[x]) {
+      seen[x] = 1;
+      cyc.push_back(x);
+      x = sigma[x];
+    }
+    const size_t k = cyc.size();
+    for (size_t i = 0; i < k; ++i) {
+      tau1[cyc[i]] = cyc[(k - i) % k];
+      tau2[cyc[i]] = cyc[(k + 1 - i) % k];
+    }
+  }
+  const uint32_t* taus[2] = {tau1, tau2};
+  for (int r = 0; r < 2; ++r) {
+    const uint32_t* tau = taus[r];
+    bool id = true;
+    for (uint32_t p = 0; p < n; ++p)
+      if (tau[p] != p) id = false;
+    if (id) continue;
+    // local set: closed under tau, contains 0..4 (or everything for small n)
+    uint64_t L = 0;
+    const uint32_t want = std::min<uint32_t>(n, 11);
+    for (uint32_t p = 0; p < std::min<uint32_t>(n, 5); ++p) L |= (1ULL << p) | (1ULL << tau[p]);
+    for (uint32_t p = 0; p < n && (uint32_t)__builtin_popcountll(L) < want; ++p) {
+      if (L >> p & 1ULL) continue;
+      const uint64_t add = (1ULL << p) | (1ULL << tau[p]);
+      if ((uint32_t)__builtin_popcountll(L | add) <= (uint32_t)kMaxM) L |= add;
+    }
+    PermParams P{};
+    P.n = n;
+    P.m = 0;
+    int li[64];
+    for (uint32_t p = 0; p < n; ++p) {
+      P.tau[p] = tau[p];
+      li[p] = -1;
+      if (L >> p & 1ULL) {
+        li[p] = (int)P.m;
+        P.L[P.m++] = p;
+      }
+    }
+    for (uint32_t k = 0; k < P.m; ++k) P.tauL[k] = (uint32_t)li[tau[P.L[k]]];
+    const size_t smem = sizeof(double2) * 2 * ((1u << P.m) + ((1u << P.m) >> 4));
+    static uint64_t attr_done = 0;  // one bit per device
+    int dev = 0;
+    DQ_CUDA_TRY(cudaGetDevice(&dev));
+    if (!((attr_done >> (dev & 63)) & 1ULL)) {
+      DQ_CUDA_TRY(cudaFuncSetAttribute(k_permute_pairs, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)(sizeof(double2) * 2 * (4096 + 256))));
+      attr_done |= 1ULL << (dev & 63);
+    }
+    const uint64_t tiles = 1ULL << (n - P.m);
+    k_permute_pairs<<<(unsigned)tiles, 256, smem, st>>>(amp, P);
+    DQ_CUDA_TRY(cudaGetLastError());
+    if (launches) ++*launches;
+  }
+  for (uint32_t l = 0; l < n; ++l) perm[l] = l;
+  return DQ_OK;
+}
+
+// ---- program runner ------------------------------------------------------------------------
+
+int fused_run_segment(double2* amp, uint32_t n, std::vector<PGate>& G, Planner& pl, Poly& poly,
+                      FusedWork& fw, cudaStream_t st, bool timing, dq_profile* prof) {
+  std::vector<PSweep> sweeps;
+  pl.plan(G, poly, sweeps);
+  pl.final_flush(poly, sweeps);
+  if (sweeps.empty()) return DQ_OK;
+  Blob blob;
+  std::vector<size_t> offs(sweeps.size());
+  for (size_t i = 0; i < sweeps.size(); ++i) DQ_TRY(encode_sweep(sweeps[i], G, pl.RB, blob, &offs[i]));
+  blob.align16();
+  // the pinned staging buffer may still feed an earlier copy
+  DQ_CUDA_TRY(cudaStreamSynchronize(st));
+  DQ_TRY(ensure_capacity(fw, blob.buf.size(), st));
+  memcpy(fw.h_blob, blob.buf.data(), blob.buf.size());
+  DQ_CUDA_TRY(cudaMemcpyAsync(fw.d_blob, fw.h_blob, blob.buf.size(), cudaMemcpyHostToDevice, st));
+  for (size_t i = 0; i < sweeps.size(); ++i) {
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (timing) {
+      cudaEventCreate(&e0);
+      cudaEventCreate(&e1);
+      cudaEventRecord(e0, st);
+    }
+    DQ_TRY(launch_sweep(amp, n, pl.RB, fw.d_blob + offs[i], st));
+    if (timing) {
+      cudaEventRecord(e1, st);
+      fw.events.push_back(e0);
+      fw.events.push_back(e1);
+    }
+    ++prof->sweeps;
+    ++prof->kernel_launches;
+  }
+  return DQ_OK;
+}
+
+int fused_run(double2* amp, uint32_t n, const dq_inst* prog, uint64_t ninst, const dq_run_opts& o,
+              FusedWork& fw, cudaStream_t st, int device, FusedHooks& hooks, dq_profile* prof,
+              uint32_t* perm) {
+  (void)device;
+  Planner pl;
+  pl.n = n;
+  uint32_t M = 12;
+  if (o.fusion_width >= (int)kFusedMinQubits && o.fusion_width <= kMaxM) M = (uint32_t)o.fusion_width;
+  if (M > n) M = n;
+  pl.M = M;
+  pl.RB = M - kSwTB;
+  pl.single_tile = (M == n);
+  if (o.max_cost > 0) pl.budget = (double)o.max_cost;
+  Poly poly;
+  poly.init(n);
+  for (auto e : fw.events) cudaEventDestroy(e);
+  fw.events.clear();
+  const bool timing = o.time_sweeps != 0;
+
+  // shots semantics: run the reference's fuse_circuit output
+  std::vector<FusedEntry> fe;
+  if (o.semantics == DQ_SEM_SHOTS) {
+    fe = fuse_program(prog, ninst, n);
+  } else {
+    fe.resize(ninst);
+    for (uint64_t i = 0; i < ninst; ++i) fe[i].inst = (int64_t)i;
+  }
+
+  std::vector<PGate> G;
+  auto flush_segment = [&]() -> int {
+    if (G.empty() && poly.empty()) return DQ_OK;
+    int rc = fused_run_segment(amp, n, G, pl, poly, fw, st, timing, prof);
+    G.clear();
+    return rc;
+  };
+  for (const FusedEntry& e : fe) {
+    if (e.inst < 0) {  // a fused 2x2 of the shots path
+      PGate g;
+      const uint32_t t = perm[e.qubit];
+      if (is_zero(e.m[1]) && is_zero(e.m[2]) && is_unit_phase(e.m[0]) && is_unit_phase(e.m[3])) {
+        g.kind = PG_DIAG;
+        if (!(e.m[0].re == 1.0 && e.m[0].im == 0.0)) g.cst = e.m[0];
+        g.nlin = 1;
+        g.lq[0] = t;
+        g.lw[0] = (e.m[0].re == 1.0 && e.m[0].im == 0.0) ? e.m[3] : e.m[3] * conj(e.m[0]);
+      } else {
+        g.kind = PG_U1;
+        g.t0 = t;
+        for (int k = 0; k < 4; ++k) g.u[k] = e.m[k];
+        g.real = e.m[0].im == 0.0 && e.m[1].im == 0.0 && e.m[2].im == 0.0 && e.m[3].im == 0.0;
+      }
+      g.touched = 1ULL << t;
+      G.push_back(g);
+      continue;
+    }
+    const dq_inst& in = prog[e.inst];
+    const int64_t src = e.inst;
+    // conditions are final: no measurement inside a segment
+    bool ok = true;
+    for (uint32_t c = 0; c < in.cond_count && ok; ++c) {
+      const dq_cond& cd = hooks.conds[in.cond_first + c];
+      uint64_t actual = 0;
+      for (uint64_t b = 0; b < cd.creg_size; ++b) {
+        const uint64_t idx = cd.creg_base + b;
+        const uint64_t v = (idx < hooks.ncbits && hooks.cbits[idx] > 0) ? (uint64_t)hooks.cbits[idx] : 0;
+        actual |= v << b;
+      }
+      ok = (actual == cd.creg_value);
+    }
+    if (!ok) continue;
+    switch (in.kind) {
+      case DQ_ID: case DQ_U0: case DQ_BARRIER: case DQ_CLASSICAL: case DQ_G_NOOP:
+        continue;
+      case DQ_G_OPAQUE:
+        if (o.semantics == DQ_SEM_SHOTS) continue;
+        prof->failed_inst = src;
+        return fail(DQ_ERR_UNSUPPORTED, "unsupported generic gate");
+      case DQ_G_UNSUPPORTED:
+        prof->failed_inst = src;
+        return fail(DQ_ERR_UNSUPPORTED, "unsupported generic gate");
+      case DQ_MEASURE:
+      case DQ_RESET: {
+        DQ_TRY(flush_segment());
+        int out = 0;
+        DQ_TRY(hooks.measure(perm[in.q[0]], &out));
+        if (in.kind == DQ_MEASURE) {
+          hooks.cbits[in.cbit] = out;
+        } else if (out == 1) {
+          GateOp op;
+          hc xm[4] = {hc{0, 0}, hc{1, 0}, hc{1, 0}, hc{0, 0}};
+          classify_1q(xm, perm[in.q[0]], 0, op);
+          DQ_TRY(hooks.exact_gate(op));
+        }
+        continue;
+      }
+      default:
+        break;
+    }
+    uint32_t sa = 0, sb = 0;
+    bool is_swap = false;
+    const size_t before = G.size();
+    if (convert_inst(in, perm, G, &sa, &sb, &is_swap)) {
+      if (is_swap) std::swap(perm[sa], perm[sb]);
+      continue;
+    }
+    G.resize(before);
+    // not representable in a sweep: flush, then the exact per-gate kernel
+    DQ_TRY(flush_segment());
+    GateOp op;
+    hc u[4];
+    if (matrix_1q(in.kind, in.p, u)) {
+      classify_1q(u, perm[in.q[0]], 0, op);
+    } else {
+      Gate g;
+      if (!matrix_nq(in, g)) return fail(DQ_ERR_INTERNAL, "instruction kind without a matrix");
+      for (uint32_t b = 0; b < g.k; ++b) g.qubits[b] = perm[g.qubits[b]];
+      classify(g, op);
+    }
+    DQ_TRY(hooks.exact_gate(op));
+  }
+  DQ_TRY(flush_segment());
+  if (timing) {
+    DQ_CUDA_TRY(cudaStreamSynchronize(st));
+    double t = 0;
+    for (size_t i = 0; i + 1 < fw.events.size(); i += 2) {
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, fw.events[i], fw.events[i + 1]);
+      t += ms * 1e-3;
+    }
+    prof->sweep_time += t;
+  }
+  return DQ_OK;
+}
+
+}  // namespace dq

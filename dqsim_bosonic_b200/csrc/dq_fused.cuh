@@ -1,0 +1,60 @@
+// dq_fused.cuh — fused tile-sweep execution of gate programs.
+//
+// A unitary stretch of the program (between measurements) is planned into
+// "sweeps".  Each sweep streams the state through HBM once: a CTA stages a
+// tile of 2^m amplitudes (the m "local" qubits: qubits 0..4 plus up to m-5
+// chosen ones) in shared memory, applies every gate of the sweep whose
+// non-diagonal action stays on local qubits, and writes the tile back.
+// Diagonal gates of degree <= 2 (z, s, t, p, rz, cz, cp, crz, rzz, ...) are
+// kept as a pending phase polynomial and applied lazily right before the
+// first non-diagonal gate on one of their qubits, whether that qubit is
+// local or not.  swap gates relabel qubits (no data movement); the final
+// relabeling is undone by the store of the last sweep.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <functional>
+#include <vector>
+
+#include "dq_common.cuh"
+#include "dq_gates.hpp"
+
+namespace dq {
+
+struct FusedWork {
+  uint8_t* d_blob = nullptr;
+  size_t d_cap = 0;
+  uint8_t* h_blob = nullptr;  // pinned staging
+  size_t h_cap = 0;
+  std::vector<cudaEvent_t> events;
+};
+
+void fused_release(FusedWork& fw);
+
+struct FusedHooks {
+  // p1 + draw + collapse on a physical qubit (the host RNG cursor lives in the caller)
+  std::function<int(uint32_t phys_q, int* outcome)> measure;
+  // exact per-gate kernel on physical qubits (reset's X, gates the planner cannot fuse)
+  std::function<int(const GateOp& op)> exact_gate;
+  int32_t* cbits = nullptr;
+  uint64_t ncbits = 0;
+  const dq_cond* conds = nullptr;
+};
+
+// perm[l] = physical position of logical qubit l; updated in place (swap
+// gates relabel instead of moving data).
+int fused_run(double2* amp, uint32_t n, const dq_inst* prog, uint64_t ninst, const dq_run_opts& o,
+              FusedWork& fw, cudaStream_t st, int device, FusedHooks& hooks, dq_profile* prof,
+              uint32_t* perm);
+
+// Move the data so that perm becomes the identity (two paired-tile sweeps at
+// most); sets perm[l] = l.
+int materialize_perm(double2* amp, uint32_t n, uint32_t* perm, cudaStream_t st,
+                     uint64_t* launches);
+
+// Smallest register width the fused path runs (smaller states use per-gate kernels).
+constexpr uint32_t kFusedMinQubits = 9;
+
+}  // namespace dq

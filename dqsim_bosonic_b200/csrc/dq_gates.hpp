@@ -278,4 +278,70 @@ inline void classify(const Gate& g, GateOp& op) {
   op.dense = g;
 }
 
+// ---- fuse_circuit (types.rs:239-293) ------------------------------------------
+// One simulate_shots trajectory runs the fused program: consecutive
+// unconditional single-qubit gates on a qubit are multiplied into one 2x2
+// (new = gate * pending), a pending matrix is flushed right before the first
+// non-fusable instruction touching its qubit, matrices within 1e-10 of the
+// identity are dropped, and the rest are flushed at the end (ascending qubit
+// order; the reference iterates a HashMap there, which only affects the
+// discarded final state).
+struct FusedEntry {
+  int64_t inst;  // >= 0: original instruction index; -1: fused 2x2 below
+  uint32_t qubit;
+  hc m[4];
+};
+
+inline void matmul2(const hc a[4], const hc b[4], hc out[4]) {
+  const hc r0 = a[0] * b[0] + a[1] * b[2];
+  const hc r1 = a[0] * b[1] + a[1] * b[3];
+  const hc r2 = a[2] * b[0] + a[3] * b[2];
+  const hc r3 = a[2] * b[1] + a[3] * b[3];
+  out[0] = r0; out[1] = r1; out[2] = r2; out[3] = r3;
+}
+
+inline bool near_identity(const hc m[4]) {
+  return hypot(m[0].re - 1.0, m[0].im) < 1e-10 && hypot(m[1].re, m[1].im) < 1e-10 &&
+         hypot(m[2].re, m[2].im) < 1e-10 && hypot(m[3].re - 1.0, m[3].im) < 1e-10;
+}
+
+inline std::vector<FusedEntry> fuse_program(const dq_inst* prog, uint64_t ninst, uint32_t n) {
+  std::vector<FusedEntry> out;
+  out.reserve(ninst + n);
+  std::vector<hc> pend(4 * (size_t)(n ? n : 1));
+  std::vector<char> has(n ? n : 1, 0);
+  auto flush = [&](uint32_t q) {
+    if (q >= n || !has[q]) return;
+    has[q] = 0;
+    if (near_identity(&pend[4 * q])) return;
+    FusedEntry e;
+    e.inst = -1;
+    e.qubit = q;
+    for (int i = 0; i < 4; ++i) e.m[i] = pend[4 * q + i];
+    out.push_back(e);
+  };
+  for (uint64_t i = 0; i < ninst; ++i) {
+    const dq_inst& in = prog[i];
+    hc m[4];
+    if (in.cond_count == 0 && matrix_1q(in.kind, in.p, m)) {
+      const uint32_t q = (uint32_t)in.q[0];
+      if (!has[q]) {
+        has[q] = 1;
+        pend[4 * q] = R(1); pend[4 * q + 1] = R(0); pend[4 * q + 2] = R(0); pend[4 * q + 3] = R(1);
+      }
+      matmul2(m, &pend[4 * q], &pend[4 * q]);
+      continue;
+    }
+    if (in.kind != DQ_BARRIER && in.kind != DQ_CLASSICAL)
+      for (int t = 0; t < in.nq && t < DQ_MAX_INST_QUBITS; ++t)
+        if (in.q[t] >= 0) flush((uint32_t)in.q[t]);
+    FusedEntry e;
+    e.inst = (int64_t)i;
+    e.qubit = 0;
+    out.push_back(e);
+  }
+  for (uint32_t q = 0; q < n; ++q) flush(q);
+  return out;
+}
+
 }  // namespace dq

@@ -203,10 +203,12 @@ def _unsupported_message(prog: Program, failed: int) -> str:
 
 
 def run_program(state: nat.State, prog: Program, seed: int, semantics: int, exec_mode: int,
-                fusion_width: int = 0, profile: bool = False) -> tuple[np.ndarray, nat.Profile]:
+                fusion_width: int = 0, profile: bool = False, time_sweeps: bool = False,
+                max_cost: int = 0) -> tuple[np.ndarray, nat.Profile]:
     """One ``dq_run`` over ``prog``; returns (cbits array, engine profile)."""
     cbits = np.full(prog.cbit_space, -1, dtype=np.int32)
-    opts = nat.RunOpts(semantics, exec_mode, fusion_width, 1 if profile else 0)
+    opts = nat.RunOpts(semantics, exec_mode, fusion_width, 1 if profile else 0,
+                       1 if time_sweeps else 0, int(max_cost))
     prof = nat.Profile()
     rc = nat.lib().dq_run(state.handle, nat.ptr(prog.insts), prog.ninst,
                           nat.ptr(prog.conds) if prog.conds.size else None, prog.conds.shape[0],

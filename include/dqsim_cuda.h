@@ -131,6 +131,8 @@ typedef struct dq_run_opts {
   int32_t exec;             /* enum dq_exec                                  */
   int32_t fusion_width;     /* local qubits per fused tile; 0 = engine default */
   int32_t profile;          /* nonzero: time each kernel class (per-gate exec) */
+  int32_t time_sweeps;      /* nonzero: CUDA-event timing of every fused sweep */
+  int32_t max_cost;         /* FP64 ops per amplitude per sweep; 0 = default   */
 } dq_run_opts;
 
 typedef struct dq_profile {         /* SimulationProfile (simulator.rs:53-68) */
@@ -143,6 +145,7 @@ typedef struct dq_profile {         /* SimulationProfile (simulator.rs:53-68) */
   double total_time;
   uint64_t kernel_launches;         /* engine kernels launched by the call    */
   uint64_t sweeps;                  /* fused tile sweeps (DQ_EXEC_FUSED)      */
+  double sweep_time;                /* seconds in sweeps (time_sweeps != 0)   */
   uint64_t boundary_draws;          /* measure draws with |r - p1| < 1e-12   */
   int64_t failed_inst;              /* index of the failing instruction or -1 */
 } dq_profile;
