@@ -41,12 +41,14 @@ namespace dq {
 
 namespace {
 
-constexpr int kSwThreads = 128;
-constexpr int kSwTB = 7;      // thread bits (5 lane + 2 warp)
+constexpr int kSwThreads = 256;
+constexpr int kSwTB = 8;      // thread bits (5 lane + 3 warp)
 constexpr int kMaxM = 12;
 constexpr int kMaxSlots = 128;
+constexpr int kMaxProg = 64 * 1024;   // bytes of one sweep program (staged in shared memory)
 
-enum : uint32_t { OP_U1 = 0, OP_U1R, OP_U1X, OP_U2, OP_FLUSH_R, OP_FLUSH_T, OP_GPHASE };
+enum : uint32_t { OP_U1 = 0, OP_U1R, OP_U1X, OP_U2, OP_FLUSH_R, OP_FLUSH_T, OP_GPHASE, OP_U1H,
+                  OP_SCALE };
 
 // swizzle vectors of local bits 3..11 (bits 0..2 map to themselves)
 __host__ __device__ constexpr uint32_t swz_g(int k) {
@@ -61,16 +63,16 @@ __host__ __device__ constexpr uint32_t swz(uint32_t e) {
   return e ^ g;
 }
 
-// ---- device program layout ------------------------------------------------------
+// ---- sweep program layout (copied verbatim into shared memory) ----------------
 struct SwHeader {
   uint32_t m, rb, nphase, nslots;
   uint32_t local_pos[kMaxM];
   uint32_t off_phase, off_op, off_slot, off_slotent;
-  uint32_t off_data, pad0, pad1, pad2;
+  uint32_t off_data, prog_bytes, pad1, pad2;
 };
 struct SwPhase {
   uint32_t tpos[kSwTB];
-  uint32_t rpos[5];
+  uint32_t rpos[4];
   uint32_t op_begin, op_end, pad0, pad1;
 };
 struct SwOp {
@@ -90,8 +92,11 @@ static_assert(sizeof(SwHeader) % 16 == 0 && sizeof(SwPhase) % 16 == 0, "layout")
 static_assert(sizeof(SwOp) % 16 == 0 && sizeof(SwSlot) % 16 == 0 && sizeof(SwSlotEnt) % 16 == 0,
               "layout");
 
-constexpr uint32_t FL_THR_MASK = 0x7f;     // flags bits 0..6: thread partners present
-                                           // flags bits 8..12: register partners present
+// FLUSH flags: thread-partner tables present (32 lane + 8 warp factors), then
+// a register-partner table (2^(RB-1) entries for a register target, 2^RB for
+// a thread target).
+constexpr uint32_t FL_THR = 1u;
+constexpr uint32_t FL_REG = 2u;
 
 // ---- device helpers -------------------------------------------------------------------
 
@@ -110,8 +115,10 @@ __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
   const uint32_t sa = (uint32_t)__cvta_generic_to_shared(smem);
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
 }
-__device__ __forceinline__ void cp_async_wait_all() {
-  asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
 
 template <int RB, int B>
@@ -144,6 +151,19 @@ __device__ __forceinline__ void u1_real(double2 (&a)[1 << RB], const double2* __
   }
 }
 
+// [[1, 1], [1, -1]] (a Hadamard whose 1/sqrt(2) is applied by a later SCALE)
+template <int RB, int B>
+__device__ __forceinline__ void u1_had(double2 (&a)[1 << RB]) {
+#pragma unroll
+  for (int j = 0; j < (1 << RB); ++j) {
+    if (j & (1 << B)) continue;
+    const int k = j | (1 << B);
+    const double2 x = a[j], y = a[k];
+    a[j] = make_double2(x.x + y.x, x.y + y.y);
+    a[k] = make_double2(x.x - y.x, x.y - y.y);
+  }
+}
+
 template <int RB, int B>
 __device__ __forceinline__ void u1_x(double2 (&a)[1 << RB], uint32_t creg) {
 #pragma unroll
@@ -157,7 +177,7 @@ __device__ __forceinline__ void u1_x(double2 (&a)[1 << RB], uint32_t creg) {
   }
 }
 
-// dense 4x4 on register bits B0 (MSB of the gate index) and B1, B0 < B1 or not
+// dense 4x4 on register bits B0 (MSB of the gate index) and B1
 template <int RB, int B0, int B1>
 __device__ __forceinline__ void u2_gen(double2 (&a)[1 << RB], const double2* __restrict__ D,
                                        uint32_t creg) {
@@ -180,46 +200,40 @@ __device__ __forceinline__ void u2_gen(double2 (&a)[1 << RB], const double2* __r
   }
 }
 
-// amplitudes with register bit B set: a[j] *= W
+// flush on register bit B: a[j] *= W * F[compress(j)] for j with bit B set
 template <int RB, int B>
-__device__ __forceinline__ void scale_reg(double2 (&a)[1 << RB], double2 W) {
+__device__ __forceinline__ void flush_reg(double2 (&a)[1 << RB], double2 W,
+                                          const double2* __restrict__ F) {
 #pragma unroll
   for (int j = 0; j < (1 << RB); ++j) {
     if (!(j & (1 << B))) continue;
-    a[j] = cmul_f(a[j], W);
+    if (F) {
+      const int idx = ((j >> (B + 1)) << B) | (j & ((1 << B) - 1));
+      a[j] = cmul_f(a[j], cmul_f(W, F[idx]));
+    } else {
+      a[j] = cmul_f(a[j], W);
+    }
   }
 }
 
-// amplitudes whose register bits in `sel` are all set: a[j] *= W  (sel static per call site)
-template <int RB>
-__device__ __forceinline__ void scale_sel(double2 (&a)[1 << RB], uint32_t sel, double2 W) {
-#pragma unroll
-  for (int j = 0; j < (1 << RB); ++j) {
-    if ((j & sel) != sel) continue;
-    a[j] = cmul_f(a[j], W);
-  }
-}
-
-#define DQ_SW_CASES1(FN, ...)                    \
-  switch (op.b0) {                               \
-    case 0: FN<RB, 0>(__VA_ARGS__); break;       \
-    case 1: if (RB > 1) FN<RB, (RB > 1 ? 1 : 0)>(__VA_ARGS__); break; \
-    case 2: if (RB > 2) FN<RB, (RB > 2 ? 2 : 0)>(__VA_ARGS__); break; \
-    case 3: if (RB > 3) FN<RB, (RB > 3 ? 3 : 0)>(__VA_ARGS__); break; \
-    case 4: if (RB > 4) FN<RB, (RB > 4 ? 4 : 0)>(__VA_ARGS__); break; \
-    default: break;                              \
+#define DQ_SW_CASES1(FN, ...)                                          \
+  switch (op.b0) {                                                     \
+    case 0: FN<RB, 0>(__VA_ARGS__); break;                             \
+    case 1: if (RB > 1) FN<RB, (RB > 1 ? 1 : 0)>(__VA_ARGS__); break;  \
+    case 2: if (RB > 2) FN<RB, (RB > 2 ? 2 : 0)>(__VA_ARGS__); break;  \
+    case 3: if (RB > 3) FN<RB, (RB > 3 ? 3 : 0)>(__VA_ARGS__); break;  \
+    default: break;                                                    \
   }
 
 template <int RB>
 __device__ __forceinline__ void u2_dispatch(double2 (&a)[1 << RB], const SwOp& op,
                                             const double2* __restrict__ D) {
-#define DQ_U2C(X, Y)                                                                   \
-  if (op.b0 == X && op.b1 == Y) {                                                      \
+#define DQ_U2C(X, Y)                                                                     \
+  if (op.b0 == X && op.b1 == Y) {                                                        \
     if (RB > X && RB > Y) u2_gen<RB, (RB > X ? X : 0), (RB > Y ? Y : 1)>(a, D, op.creg); \
-    return;                                                                            \
+    return;                                                                              \
   }
-  DQ_U2C(0, 1) DQ_U2C(0, 2) DQ_U2C(0, 3) DQ_U2C(0, 4) DQ_U2C(1, 2) DQ_U2C(1, 3) DQ_U2C(1, 4)
-  DQ_U2C(2, 3) DQ_U2C(2, 4) DQ_U2C(3, 4)
+  DQ_U2C(0, 1) DQ_U2C(0, 2) DQ_U2C(0, 3) DQ_U2C(1, 2) DQ_U2C(1, 3) DQ_U2C(2, 3)
 #undef DQ_U2C
 }
 
@@ -234,28 +248,29 @@ __device__ __forceinline__ void exec_op(const SwOp& op, double2 (&a)[1 << RB],
   switch (op.type) {
     case OP_U1: DQ_SW_CASES1(u1_gen, a, D, op.creg); break;
     case OP_U1R: DQ_SW_CASES1(u1_real, a, D, op.creg); break;
+    case OP_U1H: DQ_SW_CASES1(u1_had, a); break;
     case OP_U1X: DQ_SW_CASES1(u1_x, a, op.creg); break;
     case OP_U2: u2_dispatch<RB>(a, op, D); break;
     case OP_FLUSH_R:
     case OP_FLUSH_T: {
       if (op.type == OP_FLUSH_T && !((tid >> op.b0) & 1u)) break;
       double2 W = slots[op.slot];
-      const uint32_t tm = op.flags & FL_THR_MASK;
-#pragma unroll
-      for (int i = 0; i < kSwTB; ++i)
-        if (((tm & tid) >> i) & 1u) W = cmul_f(W, D[i]);
-      // register partners r: amplitudes with both the target and r set
-      const uint32_t tsel = (op.type == OP_FLUSH_R) ? (1u << op.b0) : 0u;
-      const uint32_t rmask = (op.flags >> 8) & 0x1fu;
+      const double2* F = D;
+      if (op.flags & FL_THR) {
+        W = cmul_f(W, cmul_f(D[tid & 31u], D[32 + (tid >> 5)]));
+        F = D + 40;
+      }
+      if (!(op.flags & FL_REG)) F = nullptr;
       if (op.type == OP_FLUSH_R) {
-        DQ_SW_CASES1(scale_reg, a, W);
+        if (F) { DQ_SW_CASES1(flush_reg, a, W, F); }
+        else { DQ_SW_CASES1(flush_reg, a, W, nullptr); }
+      } else if (F) {
+#pragma unroll
+        for (int j = 0; j < (1 << RB); ++j) a[j] = cmul_f(a[j], cmul_f(W, F[j]));
       } else {
 #pragma unroll
         for (int j = 0; j < (1 << RB); ++j) a[j] = cmul_f(a[j], W);
       }
-#pragma unroll 1
-      for (int b = 0; b < RB; ++b)
-        if ((rmask >> b) & 1u) scale_sel<RB>(a, tsel | (1u << b), D[kSwTB + b]);
       break;
     }
     case OP_GPHASE: {
@@ -264,34 +279,82 @@ __device__ __forceinline__ void exec_op(const SwOp& op, double2 (&a)[1 << RB],
       for (int j = 0; j < (1 << RB); ++j) a[j] = cmul_f(a[j], W);
       break;
     }
+    case OP_SCALE: {
+      const double f = D[0].x;
+#pragma unroll
+      for (int j = 0; j < (1 << RB); ++j) a[j] = make_double2(a[j].x * f, a[j].y * f);
+      break;
+    }
     default: break;
   }
 }
 
+// One persistent CTA per SM walks tiles blockIdx.x, + gridDim.x, ...: the
+// next tile is prefetched (cp.async into the second buffer) while the
+// current one is computed.
 template <int RB>
-__global__ void __launch_bounds__(kSwThreads, 2)
-    k_sweep(double2* __restrict__ state, const uint8_t* __restrict__ blob) {
+__global__ void __launch_bounds__(kSwThreads, 1)
+    k_sweep(double2* __restrict__ state, const uint8_t* __restrict__ gprog, uint32_t prog_bytes,
+            uint32_t ntiles) {
   constexpr int M = kSwTB + RB;
+  constexpr int T = 1 << M;
   constexpr int R = 1 << RB;
-  constexpr int NI = 1 << (M - 7);  // runs per warp
+  constexpr int NI = 1 << (M - kSwTB);  // runs of 32 per warp
   extern __shared__ __align__(16) unsigned char smraw[];
-  double2* tile = reinterpret_cast<double2*>(smraw);
-  double2* slots = tile + (1 << M);
-  const SwHeader* H = reinterpret_cast<const SwHeader*>(blob);
+  double2* buf0 = reinterpret_cast<double2*>(smraw);
+  double2* buf1 = buf0 + T;
+  double2* slots = buf1 + T;
+  uint8_t* prog = reinterpret_cast<uint8_t*>(slots + kMaxSlots);
   const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
 
-  uint32_t lp[M];
-#pragma unroll
-  for (int k = 0; k < M; ++k) lp[k] = H->local_pos[k];
-  uint64_t base = blockIdx.x;
-#pragma unroll
-  for (int k = 0; k < M; ++k) base = insert_zero(base, lp[k]);
+  for (uint32_t i = tid * 16u; i < prog_bytes; i += kSwThreads * 16u)
+    *reinterpret_cast<uint4*>(prog + i) = __ldg(reinterpret_cast<const uint4*>(gprog + i));
+  __syncthreads();
+  const SwHeader* H = reinterpret_cast<const SwHeader*>(prog);
+  const SwPhase* PH = reinterpret_cast<const SwPhase*>(prog + H->off_phase);
+  const SwOp* OPS = reinterpret_cast<const SwOp*>(prog + H->off_op);
+  const SwSlot* SL = reinterpret_cast<const SwSlot*>(prog + H->off_slot);
+  const SwSlotEnt* SE = reinterpret_cast<const SwSlotEnt*>(prog + H->off_slotent);
+  const double2* DATA = reinterpret_cast<const double2*>(prog + H->off_data);
+  const uint32_t nph = H->nphase, nslots = H->nslots;
+  const uint32_t swt = swz(lane | (warp << 5));
 
-  // per-tile factors of the FLUSH / GPHASE slots
-  {
-    const SwSlot* SL = reinterpret_cast<const SwSlot*>(blob + H->off_slot);
-    const SwSlotEnt* SE = reinterpret_cast<const SwSlotEnt*>(blob + H->off_slotent);
-    for (uint32_t s = tid; s < H->nslots; s += kSwThreads) {
+  auto tile_base = [&](uint32_t t) {
+    uint64_t b = t;
+#pragma unroll
+    for (int k = 0; k < M; ++k) b = insert_zero(b, H->local_pos[k]);
+    return b;
+  };
+  auto run_base = [&](uint64_t base) {
+    uint64_t w = base | lane;
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+      if ((warp >> k) & 1u) w |= 1ULL << H->local_pos[5 + k];
+    return w;
+  };
+  auto load_tile = [&](uint32_t t, double2* dst) {
+    const uint64_t w = run_base(tile_base(t));
+#pragma unroll
+    for (int i = 0; i < NI; ++i) {
+      uint64_t g = w;
+#pragma unroll
+      for (int b = 0; b < M - kSwTB; ++b)
+        if ((i >> b) & 1) g |= 1ULL << H->local_pos[kSwTB + b];
+      cp_async16(&dst[swt ^ swz((uint32_t)i << kSwTB)], state + g);
+    }
+    cp_async_commit();
+  };
+
+  uint32_t tile = blockIdx.x;
+  if (tile < ntiles) load_tile(tile, buf0);
+  for (uint32_t it = 0; tile < ntiles; ++it, tile += gridDim.x) {
+    double2* cur = (it & 1u) ? buf1 : buf0;
+    double2* nxt = (it & 1u) ? buf0 : buf1;
+    const uint32_t ntile = tile + gridDim.x;
+    const bool has_next = ntile < ntiles;
+    if (has_next) load_tile(ntile, nxt);
+    const uint64_t base = tile_base(tile);
+    for (uint32_t s = tid; s < nslots; s += kSwThreads) {
       double2 w = SL[s].w0;
       const uint32_t c = SL[s].count, st = SL[s].start;
       for (uint32_t e = 0; e < c; ++e) {
@@ -300,75 +363,53 @@ __global__ void __launch_bounds__(kSwThreads, 2)
       }
       slots[s] = w;
     }
-  }
+    if (has_next) cp_async_wait<1>(); else cp_async_wait<0>();
+    __syncthreads();
 
-  // stage the tile: run r = warp | i << 2 covers local bits 5..M-1
-  uint64_t wofs = base | lane;
-  if (warp & 1u) wofs |= 1ULL << lp[5];
-  if (warp & 2u) wofs |= 1ULL << lp[6];
-  const uint32_t swt = swz(lane | (warp << 5));
+    for (uint32_t p = 0; p < nph; ++p) {
+      const SwPhase& P = PH[p];
+      uint32_t tl = 0;
 #pragma unroll
-  for (int i = 0; i < NI; ++i) {
-    uint64_t g = wofs;
+      for (int i = 0; i < kSwTB; ++i) tl |= ((tid >> i) & 1u) << P.tpos[i];
+      const uint32_t pt = swz(tl);
+      uint32_t V[RB];
 #pragma unroll
-    for (int b = 0; b < M - 7; ++b)
-      if ((i >> b) & 1) g |= 1ULL << lp[7 + b];
-    cp_async16(&tile[swt ^ swz((uint32_t)i << 7)], state + g);
-  }
-  cp_async_wait_all();
-  __syncthreads();
-
-  const SwPhase* PH = reinterpret_cast<const SwPhase*>(blob + H->off_phase);
-  const SwOp* OPS = reinterpret_cast<const SwOp*>(blob + H->off_op);
-  const double2* DATA = reinterpret_cast<const double2*>(blob + H->off_data);
-  const uint32_t nph = H->nphase;
-  for (uint32_t p = 0; p < nph; ++p) {
-    const SwPhase& P = PH[p];
-    uint32_t tl = 0;
+      for (int b = 0; b < RB; ++b) V[b] = swz(1u << P.rpos[b]);
+      double2 a[R];
 #pragma unroll
-    for (int i = 0; i < kSwTB; ++i) tl |= ((tid >> i) & 1u) << P.tpos[i];
-    const uint32_t pt = swz(tl);
-    uint32_t V[RB > 0 ? RB : 1];
+      for (int j = 0; j < R; ++j) {
+        uint32_t x = pt;
 #pragma unroll
-    for (int b = 0; b < RB; ++b) V[b] = swz(1u << P.rpos[b]);
-    double2 a[R];
+        for (int b = 0; b < RB; ++b)
+          if ((j >> b) & 1) x ^= V[b];
+        a[j] = cur[x];
+      }
+      const uint32_t oe = P.op_end;
+      for (uint32_t o = P.op_begin; o < oe; ++o) exec_op<RB>(OPS[o], a, DATA, slots, tid, base);
+      const uint32_t pt2 = opaque(pt);
 #pragma unroll
-    for (int j = 0; j < R; ++j) {
-      uint32_t x = pt;
+      for (int b = 0; b < RB; ++b) V[b] = opaque(V[b]);
 #pragma unroll
-      for (int b = 0; b < RB; ++b)
-        if ((j >> b) & 1) x ^= V[b];
-      a[j] = tile[x];
+      for (int j = 0; j < R; ++j) {
+        uint32_t x = pt2;
+#pragma unroll
+        for (int b = 0; b < RB; ++b)
+          if ((j >> b) & 1) x ^= V[b];
+        cur[x] = a[j];
+      }
+      __syncthreads();
     }
-    for (uint32_t o = P.op_begin; o < P.op_end; ++o) exec_op<RB>(OPS[o], a, DATA, slots, tid, base);
-    const uint32_t pt2 = opaque(pt);
+
+    const uint64_t w = opaque64(run_base(base));
 #pragma unroll
-    for (int b = 0; b < RB; ++b) V[b] = opaque(V[b]);
+    for (int i = 0; i < NI; ++i) {
+      uint64_t g = w;
 #pragma unroll
-    for (int j = 0; j < R; ++j) {
-      uint32_t x = pt2;
-#pragma unroll
-      for (int b = 0; b < RB; ++b)
-        if ((j >> b) & 1) x ^= V[b];
-      tile[x] = a[j];
+      for (int b = 0; b < M - kSwTB; ++b)
+        if ((i >> b) & 1) g |= 1ULL << H->local_pos[kSwTB + b];
+      state[g] = cur[swt ^ swz((uint32_t)i << kSwTB)];
     }
     __syncthreads();
-  }
-
-  // store: recompute the run offsets (nothing of the load loop stays live)
-  const uint64_t wofs2 = opaque64(wofs);
-  const uint32_t swt2 = opaque(swt);
-  const SwHeader* H2 = reinterpret_cast<const SwHeader*>(opaque64(reinterpret_cast<uint64_t>(H)));
-  uint64_t hib[M - 7 > 0 ? M - 7 : 1];
-#pragma unroll
-  for (int b = 0; b < M - 7; ++b) hib[b] = 1ULL << H2->local_pos[7 + b];
-#pragma unroll
-  for (int i = 0; i < NI; ++i) {
-    uint64_t g = wofs2;
-#pragma unroll
-    for (int b = 0; b < M - 7; ++b)
-      if ((i >> b) & 1) g |= hib[b];
-    state[g] = tile[swt2 ^ swz((uint32_t)i << 7)];
   }
 }
 
@@ -439,6 +480,7 @@ struct PGate {
   uint64_t ctrl = 0;        // physical controls (all must be 1)
   hc u[16];
   bool real = false;
+  bool had = false;         // uncontrolled s*[[1,1],[1,-1]]: add/sub, scale deferred
   // diagonal terms
   hc cst{1, 0};
   int nlin = 0;
@@ -541,14 +583,15 @@ struct Blob {
 
 struct Planner {
   uint32_t n = 0, M = 12, RB = 5;
-  double budget = 64.0;
+  double budget = 48.0;
+  uint32_t max_ops = 40;    // non-diagonal gates per sweep (bounds the staged program)
   bool single_tile = false;
 
   // cost in FP64 instructions per amplitude
   double gate_cost(const PGate& g) const {
     const double frac = 1.0 / (double)(1ULL << __builtin_popcountll(g.ctrl));
     switch (g.kind) {
-      case PG_U1: return (g.real ? 4.0 : 8.0) * frac;
+      case PG_U1: return g.had ? 2.0 : (g.real ? 4.0 : 8.0) * frac;
       case PG_U1X: return 0.5;
       case PG_U2: return 16.0 * frac;
       default: return 0.0;
@@ -572,6 +615,11 @@ struct Planner {
       double cost = 0.0;
       std::vector<int> incl, next;
       bool any_nd = false;
+      uint32_t nd_count = 0;
+      // conservative size of the encoded program: op + matrix, and a flush
+      // per target (op, lane/warp/register tables, slot and its non-local terms)
+      size_t bytes = 4096;
+      const size_t flush_bytes = 48 + 16 * (32 + 8 + 16) + 32 + 32 * (size_t)n;
       for (int gi : rem) {
         const PGate& g = G[gi];
         if (g.touched & blocked) {
@@ -590,10 +638,12 @@ struct Planner {
         while (tm) {
           const int t = __builtin_ctzll(tm);
           tm &= tm - 1;
-          c += 2.5;  // a flush of the target, if pending
+          c += 4.0;  // a flush of the target, if pending
           (void)t;
         }
-        const bool fits = (uint32_t)__builtin_popcountll(ns) <= M;
+        const size_t gb = 48 + 16 * 16 + flush_bytes * (size_t)__builtin_popcountll(need);
+        const bool fits = (uint32_t)__builtin_popcountll(ns) <= M && nd_count < max_ops &&
+                          bytes + gb <= (size_t)kMaxProg - 8192;
         const bool afford = single_tile || !any_nd || cost + c <= budget;
         if (!fits || !afford) {
           next.push_back(gi);
@@ -602,7 +652,9 @@ struct Planner {
         }
         S = ns;
         cost += c;
+        bytes += gb;
         any_nd = true;
+        ++nd_count;
         incl.push_back(gi);
       }
       // pad the local set to M qubits now: every later decision (which flush
@@ -628,7 +680,8 @@ struct Planner {
           }
         }
         POp op;
-        op.type = g.kind == PG_U1 ? (g.real ? OP_U1R : OP_U1) : g.kind == PG_U1X ? OP_U1X : OP_U2;
+        op.type = g.kind == PG_U1 ? (g.had ? OP_U1H : g.real ? OP_U1R : OP_U1)
+                  : g.kind == PG_U1X ? OP_U1X : OP_U2;
         op.gate = gi;
         sw.ops.push_back(std::move(op));
       }
@@ -714,7 +767,7 @@ int encode_sweep(const PSweep& sw, const std::vector<PGate>& G, uint32_t RB, Blo
   std::vector<PhaseTmp> phases;
   auto need_of = [&](const POp& op, std::vector<uint32_t>& nd) {
     nd.clear();
-    if (op.type == OP_U1 || op.type == OP_U1R || op.type == OP_U1X) {
+    if (op.type == OP_U1 || op.type == OP_U1R || op.type == OP_U1X || op.type == OP_U1H) {
       nd.push_back((uint32_t)lidx[G[op.gate].t0]);
     } else if (op.type == OP_U2) {
       nd.push_back((uint32_t)lidx[G[op.gate].t0]);
@@ -747,6 +800,7 @@ int encode_sweep(const PSweep& sw, const std::vector<PGate>& G, uint32_t RB, Blo
     if (phases.empty()) phases.push_back(PhaseTmp{{}, 0, 0});
   }
 
+  double scale = 1.0;  // product of the deferred Hadamard factors
   std::vector<SwPhase> P;
   std::vector<SwOp> O;
   std::vector<SwSlot> SL;
@@ -781,14 +835,17 @@ int encode_sweep(const PSweep& sw, const std::vector<PGate>& G, uint32_t RB, Blo
     int rix[kMaxM], tix[kMaxM];
     for (int i = 0; i < kMaxM; ++i) rix[i] = tix[i] = -1;
     for (uint32_t b = 0; b < RB; ++b) { sp.rpos[b] = regs[b]; rix[regs[b]] = (int)b; }
+    for (uint32_t b = RB; b < 4; ++b) sp.rpos[b] = 0;
     for (int i = 0; i < kSwTB; ++i) { sp.tpos[i] = tb[i]; tix[tb[i]] = i; }
     sp.op_begin = (uint32_t)O.size();
     for (size_t oi = ph.ob; oi < ph.oe; ++oi) {
       const POp& op = sw.ops[oi];
       SwOp so{};
       so.type = op.type;
-      if (op.type == OP_U1 || op.type == OP_U1R || op.type == OP_U1X || op.type == OP_U2) {
+      if (op.type == OP_U1 || op.type == OP_U1R || op.type == OP_U1X || op.type == OP_U2 ||
+          op.type == OP_U1H) {
         const PGate& g = G[op.gate];
+        if (op.type == OP_U1H) scale = scale * g.u[0].re;
         // controls: register bits, thread bits, non-local
         uint64_t cm = g.ctrl;
         while (cm) {
@@ -846,16 +903,66 @@ int encode_sweep(const PSweep& sw, const std::vector<PGate>& G, uint32_t RB, Blo
           so.b0 = (uint32_t)tix[l];
         }
         so.data = (uint32_t)D.size();
-        for (int i = 0; i < kSwTB; ++i) D.push_back(d2(wthr[i]));
-        for (uint32_t b = 0; b < 5; ++b) {
-          D.push_back(d2(wreg[b]));
-          if (b < RB && !(wreg[b].re == 1.0 && wreg[b].im == 0.0)) so.flags |= 1u << (8 + b);
+        bool thr = false;
+        for (int i = 0; i < kSwTB; ++i)
+          if (!(wthr[i].re == 1.0 && wthr[i].im == 0.0)) thr = true;
+        if (thr) {
+          so.flags |= FL_THR;
+          for (uint32_t ln = 0; ln < 32; ++ln) {  // lane factor: thread bits 0..4
+            hc f{1, 0};
+            for (int i = 0; i < 5; ++i)
+              if ((ln >> i) & 1u) f = f * wthr[i];
+            D.push_back(d2(f));
+          }
+          for (uint32_t wp = 0; wp < 8; ++wp) {   // warp factor: thread bits 5..7
+            hc f{1, 0};
+            for (int i = 0; i < 3; ++i)
+              if ((wp >> i) & 1u) f = f * wthr[5 + i];
+            D.push_back(d2(f));
+          }
         }
-        (void)hasF;
+        if (hasF) {
+          so.flags |= FL_REG;
+          if (so.type == OP_FLUSH_R) {
+            const uint32_t B = so.b0;
+            for (uint32_t idx = 0; idx < (1u << (RB - 1)); ++idx) {
+              const uint32_t j = ((idx >> B) << (B + 1)) | (idx & ((1u << B) - 1));
+              hc f{1, 0};
+              for (uint32_t b = 0; b < RB; ++b)
+                if (b != B && ((j >> b) & 1u)) f = f * wreg[b];
+              D.push_back(d2(f));
+            }
+          } else {
+            for (uint32_t j = 0; j < (1u << RB); ++j) {
+              hc f{1, 0};
+              for (uint32_t b = 0; b < RB; ++b)
+                if ((j >> b) & 1u) f = f * wreg[b];
+              D.push_back(d2(f));
+            }
+          }
+        }
       } else if (op.type == OP_GPHASE) {
         so.slot = add_slot(op.gcst, op.gterms);
       }
       O.push_back(so);
+    }
+    if (&ph == &phases.back() && scale != 1.0) {
+      // the deferred 1/sqrt(2) factors: fold into a per-tile phase if there is one
+      bool folded = false;
+      for (size_t oi = sp.op_begin; oi < O.size(); ++oi)
+        if (O[oi].type == OP_GPHASE) {
+          SL[O[oi].slot].w0.x *= scale;
+          SL[O[oi].slot].w0.y *= scale;
+          folded = true;
+          break;
+        }
+      if (!folded) {
+        SwOp so{};
+        so.type = OP_SCALE;
+        so.data = (uint32_t)D.size();
+        D.push_back(make_double2(scale, 0.0));
+        O.push_back(so);
+      }
     }
     sp.op_end = (uint32_t)O.size();
     P.push_back(sp);
@@ -869,7 +976,8 @@ int encode_sweep(const PSweep& sw, const std::vector<PGate>& G, uint32_t RB, Blo
       if (sp.rpos[b] >= m) return fail(DQ_ERR_INTERNAL, "register bit outside the tile");
   }
   for (const SwOp& so : O)
-    if ((so.type <= OP_U2 && so.b0 >= RB) || (so.type == OP_U2 && so.b1 >= RB) ||
+    if (((so.type <= OP_U2 || so.type == OP_U1H || so.type == OP_FLUSH_R) && so.b0 >= RB) ||
+        (so.type == OP_FLUSH_T && so.b0 >= (uint32_t)kSwTB) || (so.type == OP_U2 && so.b1 >= RB) ||
         so.slot >= SL.size() + (SL.empty() ? 1 : 0) || so.data > D.size())
       return fail(DQ_ERR_INTERNAL, "op encoding out of range");
   SwHeader h{};
@@ -890,6 +998,10 @@ int encode_sweep(const PSweep& sw, const std::vector<PGate>& G, uint32_t RB, Blo
   hp->off_slot = (uint32_t)(so - hoff);
   hp->off_slotent = (uint32_t)(eo - hoff);
   hp->off_data = (uint32_t)(dd - hoff);
+  blob.align16();
+  hp = reinterpret_cast<SwHeader*>(blob.buf.data() + hoff);
+  hp->prog_bytes = (uint32_t)(blob.buf.size() - hoff);
+  if (hp->prog_bytes > (uint32_t)kMaxProg) return fail(DQ_ERR_INTERNAL, "sweep program too large");
   *offset = hoff;
   return DQ_OK;
 }
@@ -938,6 +1050,8 @@ bool convert_inst(const dq_inst& in, const uint32_t* perm, std::vector<PGate>& o
     g.ctrl = ctrl;
     for (int i = 0; i < 4; ++i) g.u[i] = m[i];
     g.real = !xperm && m[0].im == 0.0 && m[1].im == 0.0 && m[2].im == 0.0 && m[3].im == 0.0;
+    g.had = g.real && ctrl == 0 && m[0].re == m[1].re && m[0].re == m[2].re &&
+            m[0].re == -m[3].re;
     g.touched = (1ULL << t) | ctrl;
     out.push_back(g);
   };
@@ -1028,29 +1142,34 @@ bool convert_inst(const dq_inst& in, const uint32_t* perm, std::vector<PGate>& o
 }
 
 template <int RB>
-int launch_sweep_rb(double2* amp, uint32_t n, const uint8_t* dblob, cudaStream_t st) {
+int launch_sweep_rb(double2* amp, uint32_t n, const uint8_t* dblob, uint32_t prog_bytes,
+                    cudaStream_t st) {
   constexpr int M = kSwTB + RB;
-  const size_t smem = sizeof(double2) * ((1u << M) + kMaxSlots);
+  const size_t smem_max = sizeof(double2) * (2 * (1u << M) + kMaxSlots) + kMaxProg;
+  const size_t smem = sizeof(double2) * (2 * (1u << M) + kMaxSlots) + prog_bytes;
   static uint64_t attr_done = 0;  // one bit per device
   int dev = 0;
   DQ_CUDA_TRY(cudaGetDevice(&dev));
   if (!((attr_done >> (dev & 63)) & 1ULL)) {
     DQ_CUDA_TRY(cudaFuncSetAttribute(k_sweep<RB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)smem));
+                                     (int)smem_max));
     attr_done |= 1ULL << (dev & 63);
   }
+  int sms = 148;
+  DQ_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
   const uint64_t tiles = 1ULL << (n - M);
-  k_sweep<RB><<<(unsigned)tiles, kSwThreads, smem, st>>>(amp, dblob);
+  const unsigned grid = (unsigned)std::min<uint64_t>(tiles, (uint64_t)sms);
+  k_sweep<RB><<<grid, kSwThreads, smem, st>>>(amp, dblob, prog_bytes, (uint32_t)tiles);
   DQ_CUDA_TRY(cudaGetLastError());
   return DQ_OK;
 }
 
-int launch_sweep(double2* amp, uint32_t n, uint32_t RB, const uint8_t* dblob, cudaStream_t st) {
+int launch_sweep(double2* amp, uint32_t n, uint32_t RB, const uint8_t* dblob, uint32_t prog_bytes,
+                 cudaStream_t st) {
   switch (RB) {
-    case 2: return launch_sweep_rb<2>(amp, n, dblob, st);
-    case 3: return launch_sweep_rb<3>(amp, n, dblob, st);
-    case 4: return launch_sweep_rb<4>(amp, n, dblob, st);
-    case 5: return launch_sweep_rb<5>(amp, n, dblob, st);
+    case 2: return launch_sweep_rb<2>(amp, n, dblob, prog_bytes, st);
+    case 3: return launch_sweep_rb<3>(amp, n, dblob, prog_bytes, st);
+    case 4: return launch_sweep_rb<4>(amp, n, dblob, prog_bytes, st);
     default: return fail(DQ_ERR_INTERNAL, "unsupported register width");
   }
 }
@@ -1181,7 +1300,8 @@ int fused_run_segment(double2* amp, uint32_t n, std::vector<PGate>& G, Planner& 
       cudaEventCreate(&e1);
       cudaEventRecord(e0, st);
     }
-    DQ_TRY(launch_sweep(amp, n, pl.RB, fw.d_blob + offs[i], st));
+    const SwHeader* hh = reinterpret_cast<const SwHeader*>(blob.buf.data() + offs[i]);
+    DQ_TRY(launch_sweep(amp, n, pl.RB, fw.d_blob + offs[i], hh->prog_bytes, st));
     if (timing) {
       cudaEventRecord(e1, st);
       fw.events.push_back(e0);

@@ -55,6 +55,6 @@ int materialize_perm(double2* amp, uint32_t n, uint32_t* perm, cudaStream_t st,
                      uint64_t* launches);
 
 // Smallest register width the fused path runs (smaller states use per-gate kernels).
-constexpr uint32_t kFusedMinQubits = 9;
+constexpr uint32_t kFusedMinQubits = 10;
 
 }  // namespace dq
