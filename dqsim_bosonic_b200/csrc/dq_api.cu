@@ -841,6 +841,40 @@ int dq_norm_sqr(dq_state_t h, double* out) {
   return read_scalars(h, d, 1, out);
 }
 
+int dq_debug_plan(uint32_t n, const dq_inst* prog, uint64_t ninst, const dq_run_opts* opts,
+                  uint8_t* out, uint64_t cap, uint64_t* len) {
+  if (!len || (ninst && !prog)) return fail(DQ_ERR_INVALID_ARG, "null argument");
+  if (n < kFusedMinQubits || n > kMaxQubits)
+    return fail(DQ_ERR_INVALID_ARG, "fused planning needs 10..34 qubits");
+  dq_run_opts o{};
+  if (opts) o = *opts;
+  o.exec = DQ_EXEC_FUSED;
+  for (uint64_t i = 0; i < ninst; ++i) {
+    DQ_TRY(validate_inst(prog[i], n, 0, 0, nullptr, i));
+    if (prog[i].cond_count) return fail(DQ_ERR_INVALID_ARG, "plan-only mode takes unitary programs");
+  }
+  FusedWork fw;
+  std::vector<uint8_t> blob;
+  std::vector<uint64_t> offs;
+  fw.plan_out = &blob;
+  fw.plan_offs = &offs;
+  FusedHooks hooks;
+  dq_profile prof{};
+  uint32_t perm[64];
+  for (uint32_t l = 0; l < 64; ++l) perm[l] = l;
+  DQ_TRY(fused_run(nullptr, n, prog, ninst, o, fw, nullptr, 0, hooks, &prof, perm));
+  const uint64_t hdr = 16 + 4 * 64 + 8 * offs.size();
+  const uint64_t need = hdr + blob.size();
+  *len = need;
+  if (!out || cap < need) return out ? fail(DQ_ERR_INVALID_ARG, "output buffer too small") : DQ_OK;
+  uint32_t h4[4] = {0x4C505144u, (uint32_t)offs.size(), fw.plan_rb, 0};
+  memcpy(out, h4, 16);
+  memcpy(out + 16, perm, 4 * 64);
+  memcpy(out + 16 + 256, offs.data(), 8 * offs.size());
+  memcpy(out + hdr, blob.data(), blob.size());
+  return DQ_OK;
+}
+
 int dq_rng_f64(uint64_t seed, uint64_t skip, uint64_t count, double* out) {
   if (count && !out) return fail(DQ_ERR_INVALID_ARG, "null output");
   uint32_t key[8];

@@ -64,15 +64,20 @@ __host__ __device__ constexpr uint32_t swz(uint32_t e) {
 }
 
 // ---- sweep program layout (copied verbatim into shared memory) ----------------
+constexpr int kMaxRuns = 1 << (kMaxM - 5);
+
 struct SwHeader {
   uint32_t m, rb, nphase, nslots;
   uint32_t local_pos[kMaxM];
   uint32_t off_phase, off_op, off_slot, off_slotent;
   uint32_t off_data, prog_bytes, pad1, pad2;
+  uint64_t runoff[kMaxRuns];   // physical offset of run r (local bits 5..m-1 = r)
+  uint32_t runswz[kMaxRuns];   // swizzled shared-memory index of run r's first element
 };
 struct SwPhase {
-  uint32_t tpos[kSwTB];
-  uint32_t rpos[4];
+  uint32_t lanesw[32];         // swizzled local index of the lane bits (thread bits 0..4)
+  uint32_t warpsw[8];          // swizzled local index of the warp bits (thread bits 5..7)
+  uint32_t V[4];               // swizzled local index of each register bit
   uint32_t op_begin, op_end, pad0, pad1;
 };
 struct SwOp {
@@ -317,7 +322,7 @@ __global__ void __launch_bounds__(kSwThreads, 1)
   const SwSlotEnt* SE = reinterpret_cast<const SwSlotEnt*>(prog + H->off_slotent);
   const double2* DATA = reinterpret_cast<const double2*>(prog + H->off_data);
   const uint32_t nph = H->nphase, nslots = H->nslots;
-  const uint32_t swt = swz(lane | (warp << 5));
+  const uint32_t swl = swz(lane);  // lane part of a run element's index (bits 0..4)
 
   auto tile_base = [&](uint32_t t) {
     uint64_t b = t;
@@ -325,35 +330,26 @@ __global__ void __launch_bounds__(kSwThreads, 1)
     for (int k = 0; k < M; ++k) b = insert_zero(b, H->local_pos[k]);
     return b;
   };
-  auto run_base = [&](uint64_t base) {
-    uint64_t w = base | lane;
-#pragma unroll
-    for (int k = 0; k < 3; ++k)
-      if ((warp >> k) & 1u) w |= 1ULL << H->local_pos[5 + k];
-    return w;
-  };
-  auto load_tile = [&](uint32_t t, double2* dst) {
-    const uint64_t w = run_base(tile_base(t));
+  // run r = warp + 8 i: all of a tile's 2^(m-5) runs of 32 amplitudes
+  auto load_tile = [&](uint64_t base, double2* dst) {
 #pragma unroll
     for (int i = 0; i < NI; ++i) {
-      uint64_t g = w;
-#pragma unroll
-      for (int b = 0; b < M - kSwTB; ++b)
-        if ((i >> b) & 1) g |= 1ULL << H->local_pos[kSwTB + b];
-      cp_async16(&dst[swt ^ swz((uint32_t)i << kSwTB)], state + g);
+      const uint32_t r = warp + (uint32_t)i * 8u;
+      cp_async16(&dst[H->runswz[r] ^ swl], state + (base + H->runoff[r] + lane));
     }
     cp_async_commit();
   };
 
   uint32_t tile = blockIdx.x;
-  if (tile < ntiles) load_tile(tile, buf0);
+  uint64_t base = (tile < ntiles) ? tile_base(tile) : 0;
+  if (tile < ntiles) load_tile(base, buf0);
   for (uint32_t it = 0; tile < ntiles; ++it, tile += gridDim.x) {
     double2* cur = (it & 1u) ? buf1 : buf0;
     double2* nxt = (it & 1u) ? buf0 : buf1;
     const uint32_t ntile = tile + gridDim.x;
     const bool has_next = ntile < ntiles;
-    if (has_next) load_tile(ntile, nxt);
-    const uint64_t base = tile_base(tile);
+    const uint64_t nbase = has_next ? tile_base(ntile) : 0;
+    if (has_next) load_tile(nbase, nxt);
     for (uint32_t s = tid; s < nslots; s += kSwThreads) {
       double2 w = SL[s].w0;
       const uint32_t c = SL[s].count, st = SL[s].start;
@@ -368,13 +364,10 @@ __global__ void __launch_bounds__(kSwThreads, 1)
 
     for (uint32_t p = 0; p < nph; ++p) {
       const SwPhase& P = PH[p];
-      uint32_t tl = 0;
-#pragma unroll
-      for (int i = 0; i < kSwTB; ++i) tl |= ((tid >> i) & 1u) << P.tpos[i];
-      const uint32_t pt = swz(tl);
+      const uint32_t pt = P.lanesw[lane] ^ P.warpsw[warp];
       uint32_t V[RB];
 #pragma unroll
-      for (int b = 0; b < RB; ++b) V[b] = swz(1u << P.rpos[b]);
+      for (int b = 0; b < RB; ++b) V[b] = P.V[b];
       double2 a[R];
 #pragma unroll
       for (int j = 0; j < R; ++j) {
@@ -400,16 +393,13 @@ __global__ void __launch_bounds__(kSwThreads, 1)
       __syncthreads();
     }
 
-    const uint64_t w = opaque64(run_base(base));
 #pragma unroll
     for (int i = 0; i < NI; ++i) {
-      uint64_t g = w;
-#pragma unroll
-      for (int b = 0; b < M - kSwTB; ++b)
-        if ((i >> b) & 1) g |= 1ULL << H->local_pos[kSwTB + b];
-      state[g] = cur[swt ^ swz((uint32_t)i << kSwTB)];
+      const uint32_t r = warp + (uint32_t)i * 8u;
+      state[base + H->runoff[r] + lane] = cur[H->runswz[r] ^ swl];
     }
     __syncthreads();
+    base = nbase;
   }
 }
 
@@ -616,9 +606,10 @@ struct Planner {
       std::vector<int> incl, next;
       bool any_nd = false;
       uint32_t nd_count = 0;
+      uint64_t diag_touched = 0;
       // conservative size of the encoded program: op + matrix, and a flush
       // per target (op, lane/warp/register tables, slot and its non-local terms)
-      size_t bytes = 4096;
+      size_t bytes = 4096 + 3072;
       const size_t flush_bytes = 48 + 16 * (32 + 8 + 16) + 32 + 32 * (size_t)n;
       for (int gi : rem) {
         const PGate& g = G[gi];
@@ -629,6 +620,7 @@ struct Planner {
         }
         if (g.kind == PG_DIAG) {
           incl.push_back(gi);
+          diag_touched |= g.touched;
           continue;
         }
         const uint64_t need = targets(g);
@@ -638,8 +630,7 @@ struct Planner {
         while (tm) {
           const int t = __builtin_ctzll(tm);
           tm &= tm - 1;
-          c += 4.0;  // a flush of the target, if pending
-          (void)t;
+          if (poly.pending((uint32_t)t) || ((diag_touched >> t) & 1ULL)) c += 4.0;  // a flush
         }
         const size_t gb = 48 + 16 * 16 + flush_bytes * (size_t)__builtin_popcountll(need);
         const bool fits = (uint32_t)__builtin_popcountll(ns) <= M && nd_count < max_ops &&
@@ -834,9 +825,21 @@ int encode_sweep(const PSweep& sw, const std::vector<PGate>& G, uint32_t RB, Blo
       return fail(DQ_ERR_INTERNAL, "no bank-conflict-free thread layout");
     int rix[kMaxM], tix[kMaxM];
     for (int i = 0; i < kMaxM; ++i) rix[i] = tix[i] = -1;
-    for (uint32_t b = 0; b < RB; ++b) { sp.rpos[b] = regs[b]; rix[regs[b]] = (int)b; }
-    for (uint32_t b = RB; b < 4; ++b) sp.rpos[b] = 0;
-    for (int i = 0; i < kSwTB; ++i) { sp.tpos[i] = tb[i]; tix[tb[i]] = i; }
+    for (uint32_t b = 0; b < RB; ++b) { sp.V[b] = swz(1u << regs[b]); rix[regs[b]] = (int)b; }
+    for (uint32_t b = RB; b < 4; ++b) sp.V[b] = 0;
+    for (int i = 0; i < kSwTB; ++i) tix[tb[i]] = i;
+    for (uint32_t ln = 0; ln < 32; ++ln) {
+      uint32_t e = 0;
+      for (int i = 0; i < 5; ++i)
+        if ((ln >> i) & 1u) e |= 1u << tb[i];
+      sp.lanesw[ln] = swz(e);
+    }
+    for (uint32_t wp = 0; wp < 8; ++wp) {
+      uint32_t e = 0;
+      for (int i = 0; i < 3; ++i)
+        if ((wp >> i) & 1u) e |= 1u << tb[5 + i];
+      sp.warpsw[wp] = swz(e);
+    }
     sp.op_begin = (uint32_t)O.size();
     for (size_t oi = ph.ob; oi < ph.oe; ++oi) {
       const POp& op = sw.ops[oi];
@@ -891,7 +894,6 @@ int encode_sweep(const PSweep& sw, const std::vector<PGate>& G, uint32_t RB, Blo
             hasF = true;
           } else {
             wthr[tix[pl]] = wthr[tix[pl]] * pr.second;
-            so.flags |= 1u << tix[pl];
           }
         }
         so.slot = add_slot(op.wlin, nl);
@@ -970,10 +972,12 @@ int encode_sweep(const PSweep& sw, const std::vector<PGate>& G, uint32_t RB, Blo
   if (SL.size() > (size_t)kMaxSlots) return fail(DQ_ERR_INTERNAL, "too many per-tile slots");
 
   for (const SwPhase& sp : P) {
-    for (int i = 0; i < kSwTB; ++i)
-      if (sp.tpos[i] >= m) return fail(DQ_ERR_INTERNAL, "thread bit outside the tile");
+    for (int i = 0; i < 32; ++i)
+      if (sp.lanesw[i] >= (1u << m)) return fail(DQ_ERR_INTERNAL, "thread index outside the tile");
+    for (int i = 0; i < 8; ++i)
+      if (sp.warpsw[i] >= (1u << m)) return fail(DQ_ERR_INTERNAL, "thread index outside the tile");
     for (uint32_t b = 0; b < RB; ++b)
-      if (sp.rpos[b] >= m) return fail(DQ_ERR_INTERNAL, "register bit outside the tile");
+      if (sp.V[b] >= (1u << m)) return fail(DQ_ERR_INTERNAL, "register bit outside the tile");
   }
   for (const SwOp& so : O)
     if (((so.type <= OP_U2 || so.type == OP_U1H || so.type == OP_FLUSH_R) && so.b0 >= RB) ||
@@ -983,6 +987,13 @@ int encode_sweep(const PSweep& sw, const std::vector<PGate>& G, uint32_t RB, Blo
   SwHeader h{};
   h.m = m;
   h.rb = RB;
+  for (uint32_t r = 0; r < (1u << (m - 5)); ++r) {
+    uint64_t off = 0;
+    for (uint32_t b = 0; b + 5 < m; ++b)
+      if ((r >> b) & 1u) off |= 1ULL << sw.local[5 + b];
+    h.runoff[r] = off;
+    h.runswz[r] = swz(r << 5);
+  }
   h.nphase = (uint32_t)P.size();
   h.nslots = (uint32_t)SL.size();
   for (uint32_t k = 0; k < m; ++k) h.local_pos[k] = sw.local[k];
@@ -1288,6 +1299,14 @@ int fused_run_segment(double2* amp, uint32_t n, std::vector<PGate>& G, Planner& 
   std::vector<size_t> offs(sweeps.size());
   for (size_t i = 0; i < sweeps.size(); ++i) DQ_TRY(encode_sweep(sweeps[i], G, pl.RB, blob, &offs[i]));
   blob.align16();
+  if (fw.plan_out) {  // plan-only: hand the programs back instead of running them
+    const size_t base = fw.plan_out->size();
+    fw.plan_out->insert(fw.plan_out->end(), blob.buf.begin(), blob.buf.end());
+    for (size_t o : offs) fw.plan_offs->push_back(base + o);
+    fw.plan_rb = pl.RB;
+    prof->sweeps += sweeps.size();
+    return DQ_OK;
+  }
   // the pinned staging buffer may still feed an earlier copy
   DQ_CUDA_TRY(cudaStreamSynchronize(st));
   DQ_TRY(ensure_capacity(fw, blob.buf.size(), st));
@@ -1395,6 +1414,7 @@ int fused_run(double2* amp, uint32_t n, const dq_inst* prog, uint64_t ninst, con
         return fail(DQ_ERR_UNSUPPORTED, "unsupported generic gate");
       case DQ_MEASURE:
       case DQ_RESET: {
+        if (fw.plan_out) return fail(DQ_ERR_INVALID_ARG, "plan-only mode takes unitary programs");
         DQ_TRY(flush_segment());
         int out = 0;
         DQ_TRY(hooks.measure(perm[in.q[0]], &out));
@@ -1419,6 +1439,7 @@ int fused_run(double2* amp, uint32_t n, const dq_inst* prog, uint64_t ninst, con
       continue;
     }
     G.resize(before);
+    if (fw.plan_out) return fail(DQ_ERR_INVALID_ARG, "plan-only mode: gate not representable");
     // not representable in a sweep: flush, then the exact per-gate kernel
     DQ_TRY(flush_segment());
     GateOp op;
@@ -1434,7 +1455,7 @@ int fused_run(double2* amp, uint32_t n, const dq_inst* prog, uint64_t ninst, con
     DQ_TRY(hooks.exact_gate(op));
   }
   DQ_TRY(flush_segment());
-  if (timing) {
+  if (timing && !fw.plan_out) {
     DQ_CUDA_TRY(cudaStreamSynchronize(st));
     double t = 0;
     for (size_t i = 0; i + 1 < fw.events.size(); i += 2) {

@@ -24,6 +24,10 @@
 namespace dq {
 
 struct FusedWork {
+  // plan-only mode (no GPU work): encoded sweep programs are appended here
+  std::vector<uint8_t>* plan_out = nullptr;
+  std::vector<uint64_t>* plan_offs = nullptr;
+  uint32_t plan_rb = 0;
   uint8_t* d_blob = nullptr;
   size_t d_cap = 0;
   uint8_t* h_blob = nullptr;  // pinned staging

@@ -223,6 +223,16 @@ DQ_API int dq_sample_key(dq_state_t h, const uint32_t* qubits, uint32_t k, const
 DQ_API int dq_inner(dq_state_t h, const double* other, uint64_t len, double* re, double* im);
 DQ_API int dq_norm_sqr(dq_state_t h, double* out);
 
+/* ---- planner inspection (host only, no GPU needed) -------------------------
+ * Runs the fused-sweep planner of dq_run (DQ_EXEC_FUSED) on a unitary
+ * program of n qubits and writes the encoded sweep programs instead of
+ * launching them.  out receives: u32 magic 0x4C505144 ("DQPL"), u32 nsweeps,
+ * u32 register bits, u32 0, u32 perm[64] (logical -> physical after the
+ * program), u64 offset[nsweeps] into the blob, then the blob.  *len is the
+ * byte count needed (call with cap = 0 to size the buffer). */
+DQ_API int dq_debug_plan(uint32_t n, const dq_inst* prog, uint64_t ninst, const dq_run_opts* opts,
+                         uint8_t* out, uint64_t cap, uint64_t* len);
+
 /* ---- RNG (host side; same stream the device uses) ------------------------
  * ChaCha8Rng::seed_from_u64(seed) (rand_chacha 0.3.1 / rand_core 0.6.4),
  * gen::<f64>() (rand 0.8.5): the draws at positions [skip, skip + count). */

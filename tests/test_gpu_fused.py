@@ -43,7 +43,7 @@ def random_state(n, seed):
     return v / np.linalg.norm(v)
 
 
-@pytest.mark.parametrize("n,depth,seed", [(9, 300, 1), (10, 300, 2), (12, 400, 3), (13, 400, 4),
+@pytest.mark.parametrize("n,depth,seed", [(10, 300, 1), (11, 300, 2), (12, 400, 3), (13, 400, 4),
                                           (14, 400, 5), (16, 300, 6), (17, 200, 7)])
 def test_random_circuits_fused(gpu, n, depth, seed):
     prog = prog_of(random_circuit(100 + seed, n, depth))
@@ -67,7 +67,7 @@ def test_fusion_widths_and_budgets(gpu, width, max_cost):
     assert np.max(np.abs(st.download() - want)) < ATOL
 
 
-@pytest.mark.parametrize("n", [9, 13, 16])
+@pytest.mark.parametrize("n", [10, 13, 16])
 def test_qft_relabel_probabilities_and_state(gpu, n):
     c = qft_with_x(n, 5)
     prog = prog_of(c)
@@ -108,7 +108,7 @@ def swap_heavy(n, seed, depth=200):
     return JsonCircuit(n, insts)
 
 
-@pytest.mark.parametrize("n,seed", [(9, 1), (12, 2), (14, 3), (16, 4)])
+@pytest.mark.parametrize("n,seed", [(10, 1), (12, 2), (14, 3), (16, 4)])
 def test_swap_relabeling(gpu, n, seed):
     prog = prog_of(swap_heavy(n, seed))
     init = random_state(n, seed)
@@ -143,7 +143,7 @@ def measured(n, seed, layers=8):
     return JsonCircuit(n, insts, ncbits=6)
 
 
-@pytest.mark.parametrize("n,seed", [(9, 0), (11, 1), (13, 2), (15, 3)])
+@pytest.mark.parametrize("n,seed", [(10, 0), (11, 1), (13, 2), (15, 3)])
 def test_measure_reset_conditional_fused(gpu, n, seed):
     prog = prog_of(measured(n, seed))
     for rseed in (seed, 77 + seed):

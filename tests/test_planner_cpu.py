@@ -1,0 +1,89 @@
+"""The fused-sweep planner and encoder on the CPU (no GPU).
+
+dq_debug_plan runs the real planner/encoder of the engine and returns the
+encoded sweep programs; tests/_sweep_emu.py executes them like the kernel
+does.  The result must match the oracle within the fused path's 1e-12
+amplitude tolerance.
+"""
+import numpy as np
+import pytest
+
+import _oracle
+from _circuits import JsonCircuit, brickwork_u3_cx, g, gate, hea_ansatz, qft_with_x, random_circuit
+from _sweep_emu import canonical, emulate
+from dqsim_bosonic_b200 import _native as nat
+from dqsim_bosonic_b200.circuit import decode_circuit_json, encode
+
+ATOL = 1e-12
+
+
+def prog_of(c):
+    return encode(decode_circuit_json(c.model_dump_json()))
+
+
+def random_state(n, seed):
+    rng = np.random.default_rng(seed)
+    v = rng.normal(size=1 << n) + 1j * rng.normal(size=1 << n)
+    return v / np.linalg.norm(v)
+
+
+def check(c, seed=0, opts=None):
+    prog = prog_of(c)
+    n = prog.num_qubits
+    init = random_state(n, seed)
+    want, _, rc, _ = _oracle.run(prog, 0, init)
+    assert rc == 0
+    got, perm, ns = emulate(prog, init, opts)
+    got = canonical(got, perm)
+    err = np.max(np.abs(got - want))
+    assert err < ATOL, f"max error {err} over {ns} sweeps"
+    return ns
+
+
+@pytest.mark.parametrize("n,depth,seed", [(10, 120, 1), (11, 120, 2), (12, 150, 3), (13, 150, 4),
+                                          (14, 120, 5)])
+def test_random_circuits_planned(engine_lib, n, depth, seed):
+    check(random_circuit(200 + seed, n, depth), seed)
+
+
+@pytest.mark.parametrize("width", [10, 11, 12])
+@pytest.mark.parametrize("max_cost", [0, 6, 30])
+def test_widths_and_budgets_planned(engine_lib, width, max_cost):
+    opts = nat.RunOpts(0, nat.EXEC_FUSED, width, 0, 0, max_cost)
+    check(random_circuit(31 * width + max_cost, 13, 120), width, opts)
+
+
+@pytest.mark.parametrize("n", [10, 12, 14])
+def test_qft_planned(engine_lib, n):
+    ns = check(qft_with_x(n, 3))
+    assert ns >= 1
+
+
+def test_hea_planned(engine_lib):
+    c, _ = hea_ansatz(13, 3, 4)
+    check(c)
+
+
+def test_brickwork_planned(engine_lib):
+    check(brickwork_u3_cx(13, 8, 2))
+
+
+def test_single_gate_kinds_planned(engine_lib):
+    n = 12
+    rng = np.random.default_rng(9)
+    from _circuits import UNITARY_KINDS, random_gate
+
+    for kind in UNITARY_KINDS:
+        if kind in ("u0",):
+            continue
+        insts = [random_gate(rng, n, kind) for _ in range(6)]
+        check(JsonCircuit(n, insts), 3)
+
+
+def test_remote_and_swap_planned(engine_lib):
+    n = 12
+    insts = [g("h", q) for q in range(n)]
+    insts += [gate("remote_link_psi_minus", [3, 9]), g("swap", 0, 11), g("cswap", 2, 5, 10),
+              gate("nonlocal_cz", [1, 7]), g("rxx", 4, 8, 0.3), gate("remote_link_phi_plus", [6, 0]),
+              g("swap", 3, 4), g("cp", 11, 0, 0.9), g("rzz", 5, 6, 1.1)]
+    check(JsonCircuit(n, insts), 2)
