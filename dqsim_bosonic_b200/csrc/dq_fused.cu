@@ -80,10 +80,11 @@ struct SwPhase {
   uint32_t V[4];               // swizzled local index of each register bit
   uint32_t op_begin, op_end, pad0, pad1;
 };
+// 32 bytes, read as two 128-bit words: w0 = type | b0 << 8 | b1 << 16 | creg << 24,
+// w1 = ctl_thr | flags << 8 | slot << 16, data = first DATA entry, cnl = non-local controls
 struct SwOp {
-  uint32_t type, b0, b1, creg;
-  uint32_t ctl_thr, slot, data, flags;
-  uint64_t cnl, pad;
+  uint32_t w0, w1, data, pad;
+  uint64_t cnl, pad2;
 };
 struct SwSlot {
   uint32_t count, start, pad0, pad1;
@@ -102,6 +103,7 @@ static_assert(sizeof(SwOp) % 16 == 0 && sizeof(SwSlot) % 16 == 0 && sizeof(SwSlo
 // a thread target).
 constexpr uint32_t FL_THR = 1u;
 constexpr uint32_t FL_REG = 2u;
+constexpr uint32_t FL_PRE = 4u;   // 1q op: flush its target first (data = 4 matrix entries, then flush tables)
 
 // ---- device helpers -------------------------------------------------------------------
 
@@ -126,59 +128,41 @@ __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
 
-template <int RB, int B>
-__device__ __forceinline__ void u1_gen(double2 (&a)[1 << RB], const double2* __restrict__ D,
-                                       uint32_t creg) {
-  const double2 u00 = D[0], u01 = D[1], u10 = D[2], u11 = D[3];
-#pragma unroll
-  for (int j = 0; j < (1 << RB); ++j) {
-    if (j & (1 << B)) continue;
-    if ((j & creg) != creg) continue;
-    const int k = j | (1 << B);
-    const double2 x = a[j], y = a[k];
-    a[j] = cmac2_f(u00, x, u01, y);
-    a[k] = cmac2_f(u10, x, u11, y);
+// One-qubit op on register bit B, optionally preceded by the flush of B
+// (amplitudes with bit B set times W * F[compress(j)]).  KIND: 0 general
+// 2x2, 1 real 2x2, 2 [[1,1],[1,-1]], 3 X.  Controls only occur without a
+// pre-flush (the planner fuses flushes into uncontrolled ops only).
+template <int RB, int B, int KIND, bool PRE>
+__device__ __forceinline__ void u1_op(double2 (&a)[1 << RB], const double2* __restrict__ D,
+                                      uint32_t creg, double2 W, const double2* __restrict__ F) {
+  double2 u00, u01, u10, u11;
+  if (KIND <= 1) {
+    u00 = D[0]; u01 = D[1]; u10 = D[2]; u11 = D[3];
   }
-}
-
-template <int RB, int B>
-__device__ __forceinline__ void u1_real(double2 (&a)[1 << RB], const double2* __restrict__ D,
-                                        uint32_t creg) {
-  const double u00 = D[0].x, u01 = D[1].x, u10 = D[2].x, u11 = D[3].x;
 #pragma unroll
   for (int j = 0; j < (1 << RB); ++j) {
     if (j & (1 << B)) continue;
-    if ((j & creg) != creg) continue;
+    if (!PRE && (j & creg) != creg) continue;
     const int k = j | (1 << B);
-    const double2 x = a[j], y = a[k];
-    a[j] = make_double2(fma(u00, x.x, u01 * y.x), fma(u00, x.y, u01 * y.y));
-    a[k] = make_double2(fma(u10, x.x, u11 * y.x), fma(u10, x.y, u11 * y.y));
-  }
-}
-
-// [[1, 1], [1, -1]] (a Hadamard whose 1/sqrt(2) is applied by a later SCALE)
-template <int RB, int B>
-__device__ __forceinline__ void u1_had(double2 (&a)[1 << RB]) {
-#pragma unroll
-  for (int j = 0; j < (1 << RB); ++j) {
-    if (j & (1 << B)) continue;
-    const int k = j | (1 << B);
-    const double2 x = a[j], y = a[k];
-    a[j] = make_double2(x.x + y.x, x.y + y.y);
-    a[k] = make_double2(x.x - y.x, x.y - y.y);
-  }
-}
-
-template <int RB, int B>
-__device__ __forceinline__ void u1_x(double2 (&a)[1 << RB], uint32_t creg) {
-#pragma unroll
-  for (int j = 0; j < (1 << RB); ++j) {
-    if (j & (1 << B)) continue;
-    if ((j & creg) != creg) continue;
-    const int k = j | (1 << B);
-    const double2 t = a[j];
-    a[j] = a[k];
-    a[k] = t;
+    const double2 x = a[j];
+    double2 y = a[k];
+    if (PRE) {
+      const int idx = ((k >> (B + 1)) << B) | (k & ((1 << B) - 1));
+      y = cmul_f(y, F ? cmul_f(W, F[idx]) : W);
+    }
+    if (KIND == 0) {
+      a[j] = cmac2_f(u00, x, u01, y);
+      a[k] = cmac2_f(u10, x, u11, y);
+    } else if (KIND == 1) {
+      a[j] = make_double2(fma(u00.x, x.x, u01.x * y.x), fma(u00.x, x.y, u01.x * y.y));
+      a[k] = make_double2(fma(u10.x, x.x, u11.x * y.x), fma(u10.x, x.y, u11.x * y.y));
+    } else if (KIND == 2) {
+      a[j] = make_double2(x.x + y.x, x.y + y.y);
+      a[k] = make_double2(x.x - y.x, x.y - y.y);
+    } else {
+      a[j] = y;
+      a[k] = x;
+    }
   }
 }
 
@@ -222,7 +206,7 @@ __device__ __forceinline__ void flush_reg(double2 (&a)[1 << RB], double2 W,
 }
 
 #define DQ_SW_CASES1(FN, ...)                                          \
-  switch (op.b0) {                                                     \
+  switch (b0) {                                                        \
     case 0: FN<RB, 0>(__VA_ARGS__); break;                             \
     case 1: if (RB > 1) FN<RB, (RB > 1 ? 1 : 0)>(__VA_ARGS__); break;  \
     case 2: if (RB > 2) FN<RB, (RB > 2 ? 2 : 0)>(__VA_ARGS__); break;  \
@@ -230,46 +214,62 @@ __device__ __forceinline__ void flush_reg(double2 (&a)[1 << RB], double2 W,
     default: break;                                                    \
   }
 
+#define DQ_SW_U1(KIND, PRE)                                                                  \
+  switch (b0) {                                                                              \
+    case 0: u1_op<RB, 0, KIND, PRE>(a, D, creg, W, F); break;                                \
+    case 1: if (RB > 1) u1_op<RB, (RB > 1 ? 1 : 0), KIND, PRE>(a, D, creg, W, F); break;     \
+    case 2: if (RB > 2) u1_op<RB, (RB > 2 ? 2 : 0), KIND, PRE>(a, D, creg, W, F); break;     \
+    case 3: if (RB > 3) u1_op<RB, (RB > 3 ? 3 : 0), KIND, PRE>(a, D, creg, W, F); break;     \
+    default: break;                                                                          \
+  }
+
 template <int RB>
-__device__ __forceinline__ void u2_dispatch(double2 (&a)[1 << RB], const SwOp& op,
-                                            const double2* __restrict__ D) {
-#define DQ_U2C(X, Y)                                                                     \
-  if (op.b0 == X && op.b1 == Y) {                                                        \
-    if (RB > X && RB > Y) u2_gen<RB, (RB > X ? X : 0), (RB > Y ? Y : 1)>(a, D, op.creg); \
-    return;                                                                              \
+__device__ __forceinline__ void u2_dispatch(double2 (&a)[1 << RB], uint32_t b0, uint32_t b1,
+                                            uint32_t creg, const double2* __restrict__ D) {
+#define DQ_U2C(X, Y)                                                                      \
+  if (b0 == X && b1 == Y) {                                                               \
+    if (RB > X && RB > Y) u2_gen<RB, (RB > X ? X : 0), (RB > Y ? Y : 1)>(a, D, creg);     \
+    return;                                                                               \
   }
   DQ_U2C(0, 1) DQ_U2C(0, 2) DQ_U2C(0, 3) DQ_U2C(1, 2) DQ_U2C(1, 3) DQ_U2C(2, 3)
 #undef DQ_U2C
 }
 
 template <int RB>
-__device__ __forceinline__ void exec_op(const SwOp& op, double2 (&a)[1 << RB],
+__device__ __forceinline__ void exec_op(const uint4 o0, const uint4 o1, double2 (&a)[1 << RB],
                                         const double2* __restrict__ DATA,
                                         const double2* __restrict__ slots, uint32_t tid,
                                         uint64_t base) {
-  if ((base & op.cnl) != op.cnl) return;
-  if ((tid & op.ctl_thr) != op.ctl_thr) return;
-  const double2* D = DATA + op.data;
-  switch (op.type) {
-    case OP_U1: DQ_SW_CASES1(u1_gen, a, D, op.creg); break;
-    case OP_U1R: DQ_SW_CASES1(u1_real, a, D, op.creg); break;
-    case OP_U1H: DQ_SW_CASES1(u1_had, a); break;
-    case OP_U1X: DQ_SW_CASES1(u1_x, a, op.creg); break;
-    case OP_U2: u2_dispatch<RB>(a, op, D); break;
-    case OP_FLUSH_R:
-    case OP_FLUSH_T: {
-      if (op.type == OP_FLUSH_T && !((tid >> op.b0) & 1u)) break;
-      double2 W = slots[op.slot];
-      const double2* F = D;
-      if (op.flags & FL_THR) {
-        W = cmul_f(W, cmul_f(D[tid & 31u], D[32 + (tid >> 5)]));
-        F = D + 40;
-      }
-      if (!(op.flags & FL_REG)) F = nullptr;
-      if (op.type == OP_FLUSH_R) {
-        if (F) { DQ_SW_CASES1(flush_reg, a, W, F); }
-        else { DQ_SW_CASES1(flush_reg, a, W, nullptr); }
-      } else if (F) {
+  const uint32_t type = o0.x & 0xffu, b0 = (o0.x >> 8) & 0xffu, b1 = (o0.x >> 16) & 0xffu;
+  const uint32_t creg = o0.x >> 24, ctl = o0.y & 0xffu, flags = (o0.y >> 8) & 0xffu;
+  const uint32_t slot = o0.y >> 16;
+  const uint64_t cnl = ((uint64_t)o1.y << 32) | o1.x;
+  if ((base & cnl) != cnl) return;
+  if ((tid & ctl) != ctl) return;
+  const double2* D = DATA + o0.z;
+  // flush factors (FLUSH ops and pre-flushed one-qubit ops)
+  double2 W = make_double2(1.0, 0.0);
+  const double2* F = nullptr;
+  const bool is_u1 = type == OP_U1 || type == OP_U1R || type == OP_U1H || type == OP_U1X;
+  if ((flags & FL_PRE) || type == OP_FLUSH_R || type == OP_FLUSH_T || type == OP_GPHASE) {
+    W = slots[slot];
+    const double2* T = is_u1 ? D + 4 : D;
+    if (flags & FL_THR) {
+      W = cmul_f(W, cmul_f(T[tid & 31u], T[32 + (tid >> 5)]));
+      T += 40;
+    }
+    if (flags & FL_REG) F = T;
+  }
+  switch (type) {
+    case OP_U1: if (flags & FL_PRE) { DQ_SW_U1(0, true) } else { DQ_SW_U1(0, false) } break;
+    case OP_U1R: if (flags & FL_PRE) { DQ_SW_U1(1, true) } else { DQ_SW_U1(1, false) } break;
+    case OP_U1H: if (flags & FL_PRE) { DQ_SW_U1(2, true) } else { DQ_SW_U1(2, false) } break;
+    case OP_U1X: if (flags & FL_PRE) { DQ_SW_U1(3, true) } else { DQ_SW_U1(3, false) } break;
+    case OP_U2: u2_dispatch<RB>(a, b0, b1, creg, D); break;
+    case OP_FLUSH_R: DQ_SW_CASES1(flush_reg, a, W, F); break;
+    case OP_FLUSH_T:
+      if (!((tid >> b0) & 1u)) break;
+      if (F) {
 #pragma unroll
         for (int j = 0; j < (1 << RB); ++j) a[j] = cmul_f(a[j], cmul_f(W, F[j]));
       } else {
@@ -277,13 +277,10 @@ __device__ __forceinline__ void exec_op(const SwOp& op, double2 (&a)[1 << RB],
         for (int j = 0; j < (1 << RB); ++j) a[j] = cmul_f(a[j], W);
       }
       break;
-    }
-    case OP_GPHASE: {
-      const double2 W = slots[op.slot];
+    case OP_GPHASE:
 #pragma unroll
       for (int j = 0; j < (1 << RB); ++j) a[j] = cmul_f(a[j], W);
       break;
-    }
     case OP_SCALE: {
       const double f = D[0].x;
 #pragma unroll
@@ -377,8 +374,23 @@ __global__ void __launch_bounds__(kSwThreads, 1)
           if ((j >> b) & 1) x ^= V[b];
         a[j] = cur[x];
       }
-      const uint32_t oe = P.op_end;
-      for (uint32_t o = P.op_begin; o < oe; ++o) exec_op<RB>(OPS[o], a, DATA, slots, tid, base);
+      const uint32_t ob = P.op_begin, oe = P.op_end;
+      const uint4* OP4 = reinterpret_cast<const uint4*>(OPS);
+      uint4 c0 = make_uint4(0, 0, 0, 0), c1 = c0;
+      if (ob < oe) {
+        c0 = OP4[2 * ob];
+        c1 = OP4[2 * ob + 1];
+      }
+      for (uint32_t o = ob; o < oe; ++o) {
+        uint4 n0 = c0, n1 = c1;
+        if (o + 1 < oe) {  // next descriptor in flight while this op runs
+          n0 = OP4[2 * o + 2];
+          n1 = OP4[2 * o + 3];
+        }
+        exec_op<RB>(c0, c1, a, DATA, slots, tid, base);
+        c0 = n0;
+        c1 = n1;
+      }
       const uint32_t pt2 = opaque(pt);
 #pragma unroll
       for (int b = 0; b < RB; ++b) V[b] = opaque(V[b]);
@@ -792,8 +804,12 @@ int encode_sweep(const PSweep& sw, const std::vector<PGate>& G, uint32_t RB, Blo
   }
 
   double scale = 1.0;  // product of the deferred Hadamard factors
+  struct EncOp {
+    uint32_t type = 0, b0 = 0, b1 = 0, creg = 0, ctl_thr = 0, flags = 0, slot = 0, data = 0;
+    uint64_t cnl = 0;
+  };
   std::vector<SwPhase> P;
-  std::vector<SwOp> O;
+  std::vector<EncOp> O;
   std::vector<SwSlot> SL;
   std::vector<SwSlotEnt> SE;
   std::vector<double2> D;
@@ -841,14 +857,88 @@ int encode_sweep(const PSweep& sw, const std::vector<PGate>& G, uint32_t RB, Blo
       sp.warpsw[wp] = swz(e);
     }
     sp.op_begin = (uint32_t)O.size();
+    // flush of a register target: per-tile slot, thread/register factor tables
+    auto encode_flush = [&](const POp& op, EncOp& so) {
+      const int l = lidx[op.q];
+      std::vector<std::pair<uint64_t, hc>> nl;
+      hc wthr[kSwTB];
+      for (int i = 0; i < kSwTB; ++i) wthr[i] = hc{1, 0};
+      hc wreg[5];
+      for (int i = 0; i < 5; ++i) wreg[i] = hc{1, 0};
+      bool hasF = false;
+      for (auto& pr : op.partners) {
+        const int pl = lidx[pr.first];
+        if (pl < 0) {
+          nl.push_back({1ULL << pr.first, pr.second});
+        } else if (rix[pl] >= 0) {
+          wreg[rix[pl]] = wreg[rix[pl]] * pr.second;
+          hasF = true;
+        } else {
+          wthr[tix[pl]] = wthr[tix[pl]] * pr.second;
+        }
+      }
+      so.slot = add_slot(op.wlin, nl);
+      const bool reg_target = rix[l] >= 0;
+      bool thr = false;
+      for (int i = 0; i < kSwTB; ++i)
+        if (!(wthr[i].re == 1.0 && wthr[i].im == 0.0)) thr = true;
+      if (thr) {
+        so.flags |= FL_THR;
+        for (uint32_t ln = 0; ln < 32; ++ln) {  // lane factor: thread bits 0..4
+          hc f{1, 0};
+          for (int i = 0; i < 5; ++i)
+            if ((ln >> i) & 1u) f = f * wthr[i];
+          D.push_back(d2(f));
+        }
+        for (uint32_t wp = 0; wp < 8; ++wp) {   // warp factor: thread bits 5..7
+          hc f{1, 0};
+          for (int i = 0; i < 3; ++i)
+            if ((wp >> i) & 1u) f = f * wthr[5 + i];
+          D.push_back(d2(f));
+        }
+      }
+      if (hasF) {
+        so.flags |= FL_REG;
+        if (reg_target) {
+          const uint32_t B = (uint32_t)rix[l];
+          for (uint32_t idx = 0; idx < (1u << (RB - 1)); ++idx) {
+            const uint32_t j = ((idx >> B) << (B + 1)) | (idx & ((1u << B) - 1));
+            hc f{1, 0};
+            for (uint32_t b = 0; b < RB; ++b)
+              if (b != B && ((j >> b) & 1u)) f = f * wreg[b];
+            D.push_back(d2(f));
+          }
+        } else {
+          for (uint32_t j = 0; j < (1u << RB); ++j) {
+            hc f{1, 0};
+            for (uint32_t b = 0; b < RB; ++b)
+              if ((j >> b) & 1u) f = f * wreg[b];
+            D.push_back(d2(f));
+          }
+        }
+      }
+    };
+    auto is_u1_type = [](uint32_t t) {
+      return t == OP_U1 || t == OP_U1R || t == OP_U1X || t == OP_U1H;
+    };
     for (size_t oi = ph.ob; oi < ph.oe; ++oi) {
       const POp& op = sw.ops[oi];
-      SwOp so{};
+      EncOp so{};
       so.type = op.type;
-      if (op.type == OP_U1 || op.type == OP_U1R || op.type == OP_U1X || op.type == OP_U2 ||
-          op.type == OP_U1H) {
-        const PGate& g = G[op.gate];
-        if (op.type == OP_U1H) scale = scale * g.u[0].re;
+      // a flush of a register bit right before an uncontrolled one-qubit op on
+      // the same qubit travels inside that op (FL_PRE)
+      const POp* pre = nullptr;
+      if ((op.type == OP_FLUSH_R || op.type == OP_FLUSH_T) && oi + 1 < ph.oe &&
+          is_u1_type(sw.ops[oi + 1].type) && G[sw.ops[oi + 1].gate].ctrl == 0 &&
+          G[sw.ops[oi + 1].gate].t0 == op.q && rix[lidx[op.q]] >= 0) {
+        pre = &op;
+        ++oi;
+      }
+      const POp& cur = sw.ops[oi];
+      so.type = cur.type;
+      if (is_u1_type(cur.type) || cur.type == OP_U2) {
+        const PGate& g = G[cur.gate];
+        if (cur.type == OP_U1H) scale = scale * g.u[0].re;
         // controls: register bits, thread bits, non-local
         uint64_t cm = g.ctrl;
         while (cm) {
@@ -860,7 +950,7 @@ int encode_sweep(const PSweep& sw, const std::vector<PGate>& G, uint32_t RB, Blo
           else so.ctl_thr |= 1u << tix[l];
         }
         so.data = (uint32_t)D.size();
-        if (op.type == OP_U2) {
+        if (cur.type == OP_U2) {
           int r0 = rix[lidx[g.t0]], r1 = rix[lidx[g.t1]];
           hc mm[16];
           for (int i = 0; i < 16; ++i) mm[i] = g.u[i];
@@ -876,27 +966,15 @@ int encode_sweep(const PSweep& sw, const std::vector<PGate>& G, uint32_t RB, Blo
         } else {
           so.b0 = (uint32_t)rix[lidx[g.t0]];
           for (int i = 0; i < 4; ++i) D.push_back(d2(g.u[i]));
-        }
-      } else if (op.type == OP_FLUSH_R || op.type == OP_FLUSH_T) {
-        const int l = lidx[op.q];
-        std::vector<std::pair<uint64_t, hc>> nl;
-        hc wthr[kSwTB];
-        for (int i = 0; i < kSwTB; ++i) wthr[i] = hc{1, 0};
-        hc wreg[5];
-        for (int i = 0; i < 5; ++i) wreg[i] = hc{1, 0};
-        bool hasF = false;
-        for (auto& pr : op.partners) {
-          const int pl = lidx[pr.first];
-          if (pl < 0) {
-            nl.push_back({1ULL << pr.first, pr.second});
-          } else if (rix[pl] >= 0) {
-            wreg[rix[pl]] = wreg[rix[pl]] * pr.second;
-            hasF = true;
-          } else {
-            wthr[tix[pl]] = wthr[tix[pl]] * pr.second;
+          if (pre) {
+            so.flags |= FL_PRE;
+            encode_flush(*pre, so);
           }
         }
-        so.slot = add_slot(op.wlin, nl);
+      } else if (cur.type == OP_FLUSH_R || cur.type == OP_FLUSH_T) {
+        const int l = lidx[cur.q];
+        so.data = (uint32_t)D.size();
+        encode_flush(cur, so);
         if (rix[l] >= 0) {
           so.type = OP_FLUSH_R;
           so.b0 = (uint32_t)rix[l];
@@ -904,47 +982,8 @@ int encode_sweep(const PSweep& sw, const std::vector<PGate>& G, uint32_t RB, Blo
           so.type = OP_FLUSH_T;
           so.b0 = (uint32_t)tix[l];
         }
-        so.data = (uint32_t)D.size();
-        bool thr = false;
-        for (int i = 0; i < kSwTB; ++i)
-          if (!(wthr[i].re == 1.0 && wthr[i].im == 0.0)) thr = true;
-        if (thr) {
-          so.flags |= FL_THR;
-          for (uint32_t ln = 0; ln < 32; ++ln) {  // lane factor: thread bits 0..4
-            hc f{1, 0};
-            for (int i = 0; i < 5; ++i)
-              if ((ln >> i) & 1u) f = f * wthr[i];
-            D.push_back(d2(f));
-          }
-          for (uint32_t wp = 0; wp < 8; ++wp) {   // warp factor: thread bits 5..7
-            hc f{1, 0};
-            for (int i = 0; i < 3; ++i)
-              if ((wp >> i) & 1u) f = f * wthr[5 + i];
-            D.push_back(d2(f));
-          }
-        }
-        if (hasF) {
-          so.flags |= FL_REG;
-          if (so.type == OP_FLUSH_R) {
-            const uint32_t B = so.b0;
-            for (uint32_t idx = 0; idx < (1u << (RB - 1)); ++idx) {
-              const uint32_t j = ((idx >> B) << (B + 1)) | (idx & ((1u << B) - 1));
-              hc f{1, 0};
-              for (uint32_t b = 0; b < RB; ++b)
-                if (b != B && ((j >> b) & 1u)) f = f * wreg[b];
-              D.push_back(d2(f));
-            }
-          } else {
-            for (uint32_t j = 0; j < (1u << RB); ++j) {
-              hc f{1, 0};
-              for (uint32_t b = 0; b < RB; ++b)
-                if ((j >> b) & 1u) f = f * wreg[b];
-              D.push_back(d2(f));
-            }
-          }
-        }
-      } else if (op.type == OP_GPHASE) {
-        so.slot = add_slot(op.gcst, op.gterms);
+      } else if (cur.type == OP_GPHASE) {
+        so.slot = add_slot(cur.gcst, cur.gterms);
       }
       O.push_back(so);
     }
@@ -959,7 +998,7 @@ int encode_sweep(const PSweep& sw, const std::vector<PGate>& G, uint32_t RB, Blo
           break;
         }
       if (!folded) {
-        SwOp so{};
+        EncOp so{};
         so.type = OP_SCALE;
         so.data = (uint32_t)D.size();
         D.push_back(make_double2(scale, 0.0));
@@ -979,11 +1018,20 @@ int encode_sweep(const PSweep& sw, const std::vector<PGate>& G, uint32_t RB, Blo
     for (uint32_t b = 0; b < RB; ++b)
       if (sp.V[b] >= (1u << m)) return fail(DQ_ERR_INTERNAL, "register bit outside the tile");
   }
-  for (const SwOp& so : O)
+  for (const EncOp& so : O)
     if (((so.type <= OP_U2 || so.type == OP_U1H || so.type == OP_FLUSH_R) && so.b0 >= RB) ||
         (so.type == OP_FLUSH_T && so.b0 >= (uint32_t)kSwTB) || (so.type == OP_U2 && so.b1 >= RB) ||
-        so.slot >= SL.size() + (SL.empty() ? 1 : 0) || so.data > D.size())
+        so.slot >= SL.size() + (SL.empty() ? 1 : 0) || so.data > D.size() || so.slot > 0xffffu ||
+        so.creg > 0xffu || so.ctl_thr > 0xffu || so.flags > 0xffu)
       return fail(DQ_ERR_INTERNAL, "op encoding out of range");
+  std::vector<SwOp> OP(O.size());
+  for (size_t i = 0; i < O.size(); ++i) {
+    const EncOp& e = O[i];
+    OP[i].w0 = e.type | (e.b0 << 8) | (e.b1 << 16) | (e.creg << 24);
+    OP[i].w1 = e.ctl_thr | (e.flags << 8) | (e.slot << 16);
+    OP[i].data = e.data;
+    OP[i].cnl = e.cnl;
+  }
   SwHeader h{};
   h.m = m;
   h.rb = RB;
@@ -999,7 +1047,7 @@ int encode_sweep(const PSweep& sw, const std::vector<PGate>& G, uint32_t RB, Blo
   for (uint32_t k = 0; k < m; ++k) h.local_pos[k] = sw.local[k];
   const size_t hoff = blob.put(&h, 1);
   const size_t po = blob.put(P.data(), P.size());
-  const size_t oo = O.empty() ? blob.align16() : blob.put(O.data(), O.size());
+  const size_t oo = OP.empty() ? blob.align16() : blob.put(OP.data(), OP.size());
   const size_t so = SL.empty() ? blob.align16() : blob.put(SL.data(), SL.size());
   const size_t eo = SE.empty() ? blob.align16() : blob.put(SE.data(), SE.size());
   const size_t dd = D.empty() ? blob.align16() : blob.put(D.data(), D.size());

@@ -18,7 +18,7 @@ import numpy as np
 from dqsim_bosonic_b200 import _native as nat
 
 OP_U1, OP_U1R, OP_U1X, OP_U2, OP_FLUSH_R, OP_FLUSH_T, OP_GPHASE, OP_U1H, OP_SCALE = range(9)
-FL_THR, FL_REG = 1, 2
+FL_THR, FL_REG, FL_PRE = 1, 2, 4
 THREADS, TB, MAXM, MAXRUNS = 256, 8, 12, 128
 SWZ_G = {3: 3, 4: 5, 5: 6, 6: 7, 7: 3, 8: 5, 9: 6, 10: 7, 11: 1}
 
@@ -107,7 +107,7 @@ def run_sweep(state: np.ndarray, n: int, blob: bytes) -> None:
         assert X.max() < T
         a = smem[:, X]                                                             # tiles x threads x R
         for o in range(ob, oe):
-            _exec(blob, off_op + 48 * o, off_data, a, slots, base, tid, rb)
+            _exec(blob, off_op + 32 * o, off_data, a, slots, base, tid, rb)
         smem[:, X] = a
     state[gidx.reshape(ntiles, -1).astype(np.int64)] = smem[:, sidx.reshape(-1)]
 
@@ -121,8 +121,10 @@ def _xor_bits(j, V):
 
 
 def _exec(blob, oo, off_data, a, slots, base, tid, rb):
-    typ, b0, b1, creg, ctl_thr, slot, data, flags = struct.unpack_from("<8I", blob, oo)
-    cnl = np.uint64(struct.unpack_from("<Q", blob, oo + 32)[0])
+    w0, w1, data = struct.unpack_from("<3I", blob, oo)
+    typ, b0, b1, creg = w0 & 0xFF, (w0 >> 8) & 0xFF, (w0 >> 16) & 0xFF, w0 >> 24
+    ctl_thr, flags, slot = w1 & 0xFF, (w1 >> 8) & 0xFF, w1 >> 16
+    cnl = np.uint64(struct.unpack_from("<Q", blob, oo + 16)[0])
     R = 1 << rb
     tmask = ((base & cnl) == cnl)[:, None]                     # tiles x 1
     hmask = ((tid & ctl_thr) == ctl_thr)[None, :]              # 1 x threads
@@ -132,6 +134,23 @@ def _exec(blob, oo, off_data, a, slots, base, tid, rb):
     def upd(j, v):
         a[:, :, j] = np.where(act, v, a[:, :, j])
 
+    def flush_factors(T):
+        W = np.broadcast_to(slots[:, slot][:, None], act.shape).copy()
+        if flags & FL_THR:
+            lt = _c2(blob, T, 32)
+            wt = _c2(blob, T + 16 * 32, 8)
+            W = W * (lt[tid & 31] * wt[tid >> 5])[None, :]
+            T = T + 16 * 40
+        return W, T
+
+    if flags & FL_PRE:
+        W, Fo = flush_factors(D + 16 * 4)
+        F = _c2(blob, Fo, 1 << (rb - 1)) if flags & FL_REG else None
+        for j in range(R):
+            if not (j >> b0) & 1:
+                continue
+            idx = ((j >> (b0 + 1)) << b0) | (j & ((1 << b0) - 1))
+            upd(j, a[:, :, j] * (W * (F[idx] if F is not None else 1.0)))
     if typ in (OP_U1, OP_U1R, OP_U1H, OP_U1X):
         if typ == OP_U1H:
             u = np.array([1, 1, 1, -1], dtype=np.complex128)
@@ -158,13 +177,7 @@ def _exec(blob, oo, off_data, a, slots, base, tid, rb):
             for r in range(4):
                 upd(idx[r], sum(u[r, c] * v[c] for c in range(4)))
     elif typ in (OP_FLUSH_R, OP_FLUSH_T):
-        W = np.broadcast_to(slots[:, slot][:, None], act.shape).copy()
-        Fo = D
-        if flags & FL_THR:
-            lt = _c2(blob, D, 32)
-            wt = _c2(blob, D + 16 * 32, 8)
-            W = W * (lt[tid & 31] * wt[tid >> 5])[None, :]
-            Fo = D + 16 * 40
+        W, Fo = flush_factors(D)
         if typ == OP_FLUSH_T:
             act = act & ((tid >> b0) & 1).astype(bool)[None, :]
         if typ == OP_FLUSH_R:
