@@ -27,6 +27,7 @@
 // whose bits are set in this tile's base index) is computed once per tile.
 #include <cuda_runtime.h>
 #include <stdio.h>
+#include <stdlib.h>
 #include <string.h>
 
 #include <algorithm>
@@ -41,11 +42,14 @@ namespace dq {
 
 namespace {
 
-constexpr int kSwThreads = 256;
-constexpr int kSwTB = 8;      // thread bits (5 lane + 3 warp)
+// Thread geometry: TB thread bits (5 lane + TB-5 warp bits), 2^TB threads per
+// CTA.  TB = 7: 128 threads, two CTAs per SM (their phases overlap); TB = 8:
+// 256 threads, one CTA per SM.
+constexpr int kMaxTB = 8;
 constexpr int kMaxM = 12;
 constexpr int kMaxSlots = 128;
-constexpr int kMaxProg = 64 * 1024;   // bytes of one sweep program (staged in shared memory)
+// bytes of one sweep program (staged in shared memory next to two tile buffers)
+__host__ __device__ constexpr int max_prog(int tb) { return tb >= 8 ? 64 * 1024 : 40 * 1024; }
 
 enum : uint32_t { OP_U1 = 0, OP_U1R, OP_U1X, OP_U2, OP_FLUSH_R, OP_FLUSH_T, OP_GPHASE, OP_U1H,
                   OP_SCALE };
@@ -294,14 +298,17 @@ __device__ __forceinline__ void exec_op(const uint4 o0, const uint4 o1, double2 
 // One persistent CTA per SM walks tiles blockIdx.x, + gridDim.x, ...: the
 // next tile is prefetched (cp.async into the second buffer) while the
 // current one is computed.
-template <int RB>
-__global__ void __launch_bounds__(kSwThreads, 1)
+template <int TB, int RB>
+__global__ void __launch_bounds__(1 << TB, (TB == 7 ? 2 : 1))
     k_sweep(double2* __restrict__ state, const uint8_t* __restrict__ gprog, uint32_t prog_bytes,
             uint32_t ntiles) {
+  constexpr int kSwThreads = 1 << TB;
+  constexpr int kSwTB = TB;
   constexpr int M = kSwTB + RB;
   constexpr int T = 1 << M;
   constexpr int R = 1 << RB;
   constexpr int NI = 1 << (M - kSwTB);  // runs of 32 per warp
+  constexpr uint32_t NW = 1u << (TB - 5);  // warps
   extern __shared__ __align__(16) unsigned char smraw[];
   double2* buf0 = reinterpret_cast<double2*>(smraw);
   double2* buf1 = buf0 + T;
@@ -331,7 +338,7 @@ __global__ void __launch_bounds__(kSwThreads, 1)
   auto load_tile = [&](uint64_t base, double2* dst) {
 #pragma unroll
     for (int i = 0; i < NI; ++i) {
-      const uint32_t r = warp + (uint32_t)i * 8u;
+      const uint32_t r = warp + (uint32_t)i * NW;
       cp_async16(&dst[H->runswz[r] ^ swl], state + (base + H->runoff[r] + lane));
     }
     cp_async_commit();
@@ -407,7 +414,7 @@ __global__ void __launch_bounds__(kSwThreads, 1)
 
 #pragma unroll
     for (int i = 0; i < NI; ++i) {
-      const uint32_t r = warp + (uint32_t)i * 8u;
+      const uint32_t r = warp + (uint32_t)i * NW;
       state[base + H->runoff[r] + lane] = cur[H->runswz[r] ^ swl];
     }
     __syncthreads();
@@ -584,7 +591,7 @@ struct Blob {
 };
 
 struct Planner {
-  uint32_t n = 0, M = 12, RB = 5;
+  uint32_t n = 0, M = 12, RB = 5, TB = 8;
   double budget = 48.0;
   uint32_t max_ops = 40;    // non-diagonal gates per sweep (bounds the staged program)
   bool single_tile = false;
@@ -646,7 +653,7 @@ struct Planner {
         }
         const size_t gb = 48 + 16 * 16 + flush_bytes * (size_t)__builtin_popcountll(need);
         const bool fits = (uint32_t)__builtin_popcountll(ns) <= M && nd_count < max_ops &&
-                          bytes + gb <= (size_t)kMaxProg - 8192;
+                          bytes + gb <= (size_t)max_prog((int)TB) - 8192;
         const bool afford = single_tile || !any_nd || cost + c <= budget;
         if (!fits || !afford) {
           next.push_back(gi);
@@ -754,8 +761,9 @@ bool order_thread_bits(std::vector<uint32_t>& tb) {
 }
 
 // Encode a planned sweep into the device blob format.
-int encode_sweep(const PSweep& sw, const std::vector<PGate>& G, uint32_t RB, Blob& blob,
-                 size_t* offset) {
+int encode_sweep(const PSweep& sw, const std::vector<PGate>& G, uint32_t TBn, uint32_t RB,
+                 Blob& blob, size_t* offset) {
+  const int kSwTB = (int)TBn;
   const uint32_t m = (uint32_t)sw.local.size();
   if (m != kSwTB + RB) return fail(DQ_ERR_INTERNAL, "sweep local set size mismatch");
   int lidx[64];
@@ -852,7 +860,7 @@ int encode_sweep(const PSweep& sw, const std::vector<PGate>& G, uint32_t RB, Blo
     }
     for (uint32_t wp = 0; wp < 8; ++wp) {
       uint32_t e = 0;
-      for (int i = 0; i < 3; ++i)
+      for (int i = 0; i + 5 < kSwTB; ++i)
         if ((wp >> i) & 1u) e |= 1u << tb[5 + i];
       sp.warpsw[wp] = swz(e);
     }
@@ -861,7 +869,7 @@ int encode_sweep(const PSweep& sw, const std::vector<PGate>& G, uint32_t RB, Blo
     auto encode_flush = [&](const POp& op, EncOp& so) {
       const int l = lidx[op.q];
       std::vector<std::pair<uint64_t, hc>> nl;
-      hc wthr[kSwTB];
+      hc wthr[kMaxTB];
       for (int i = 0; i < kSwTB; ++i) wthr[i] = hc{1, 0};
       hc wreg[5];
       for (int i = 0; i < 5; ++i) wreg[i] = hc{1, 0};
@@ -890,9 +898,9 @@ int encode_sweep(const PSweep& sw, const std::vector<PGate>& G, uint32_t RB, Blo
             if ((ln >> i) & 1u) f = f * wthr[i];
           D.push_back(d2(f));
         }
-        for (uint32_t wp = 0; wp < 8; ++wp) {   // warp factor: thread bits 5..7
+        for (uint32_t wp = 0; wp < 8; ++wp) {   // warp factor: thread bits 5..TB-1
           hc f{1, 0};
-          for (int i = 0; i < 3; ++i)
+          for (int i = 0; i + 5 < kSwTB; ++i)
             if ((wp >> i) & 1u) f = f * wthr[5 + i];
           D.push_back(d2(f));
         }
@@ -1060,7 +1068,7 @@ int encode_sweep(const PSweep& sw, const std::vector<PGate>& G, uint32_t RB, Blo
   blob.align16();
   hp = reinterpret_cast<SwHeader*>(blob.buf.data() + hoff);
   hp->prog_bytes = (uint32_t)(blob.buf.size() - hoff);
-  if (hp->prog_bytes > (uint32_t)kMaxProg) return fail(DQ_ERR_INTERNAL, "sweep program too large");
+  if (hp->prog_bytes > (uint32_t)max_prog(kSwTB)) return fail(DQ_ERR_INTERNAL, "sweep program too large");
   *offset = hoff;
   return DQ_OK;
 }
@@ -1200,37 +1208,51 @@ bool convert_inst(const dq_inst& in, const uint32_t* perm, std::vector<PGate>& o
   }
 }
 
-template <int RB>
+template <int TB, int RB>
 int launch_sweep_rb(double2* amp, uint32_t n, const uint8_t* dblob, uint32_t prog_bytes,
                     cudaStream_t st) {
-  constexpr int M = kSwTB + RB;
-  const size_t smem_max = sizeof(double2) * (2 * (1u << M) + kMaxSlots) + kMaxProg;
+  constexpr int M = TB + RB;
+  const size_t smem_max = sizeof(double2) * (2 * (1u << M) + kMaxSlots) + max_prog(TB);
   const size_t smem = sizeof(double2) * (2 * (1u << M) + kMaxSlots) + prog_bytes;
   static uint64_t attr_done = 0;  // one bit per device
+  static int per_sm[64];
   int dev = 0;
   DQ_CUDA_TRY(cudaGetDevice(&dev));
   if (!((attr_done >> (dev & 63)) & 1ULL)) {
-    DQ_CUDA_TRY(cudaFuncSetAttribute(k_sweep<RB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    DQ_CUDA_TRY(cudaFuncSetAttribute(k_sweep<TB, RB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)smem_max));
+    int b = 1;
+    DQ_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_sweep<TB, RB>, 1 << TB, smem_max));
+    per_sm[dev & 63] = b < 1 ? 1 : b;
     attr_done |= 1ULL << (dev & 63);
   }
   int sms = 148;
   DQ_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
   const uint64_t tiles = 1ULL << (n - M);
-  const unsigned grid = (unsigned)std::min<uint64_t>(tiles, (uint64_t)sms);
-  k_sweep<RB><<<grid, kSwThreads, smem, st>>>(amp, dblob, prog_bytes, (uint32_t)tiles);
+  const unsigned grid = (unsigned)std::min<uint64_t>(tiles, (uint64_t)sms * per_sm[dev & 63]);
+  k_sweep<TB, RB><<<grid, 1 << TB, smem, st>>>(amp, dblob, prog_bytes, (uint32_t)tiles);
   DQ_CUDA_TRY(cudaGetLastError());
   return DQ_OK;
 }
 
-int launch_sweep(double2* amp, uint32_t n, uint32_t RB, const uint8_t* dblob, uint32_t prog_bytes,
-                 cudaStream_t st) {
-  switch (RB) {
-    case 2: return launch_sweep_rb<2>(amp, n, dblob, prog_bytes, st);
-    case 3: return launch_sweep_rb<3>(amp, n, dblob, prog_bytes, st);
-    case 4: return launch_sweep_rb<4>(amp, n, dblob, prog_bytes, st);
-    default: return fail(DQ_ERR_INTERNAL, "unsupported register width");
+int launch_sweep(double2* amp, uint32_t n, uint32_t TB, uint32_t RB, const uint8_t* dblob,
+                 uint32_t prog_bytes, cudaStream_t st) {
+  if (TB == 8) {
+    switch (RB) {
+      case 2: return launch_sweep_rb<8, 2>(amp, n, dblob, prog_bytes, st);
+      case 3: return launch_sweep_rb<8, 3>(amp, n, dblob, prog_bytes, st);
+      case 4: return launch_sweep_rb<8, 4>(amp, n, dblob, prog_bytes, st);
+      default: break;
+    }
+  } else if (TB == 7) {
+    switch (RB) {
+      case 2: return launch_sweep_rb<7, 2>(amp, n, dblob, prog_bytes, st);
+      case 3: return launch_sweep_rb<7, 3>(amp, n, dblob, prog_bytes, st);
+      case 4: return launch_sweep_rb<7, 4>(amp, n, dblob, prog_bytes, st);
+      default: break;
+    }
   }
+  return fail(DQ_ERR_INTERNAL, "unsupported sweep geometry");
 }
 
 int ensure_capacity(FusedWork& fw, size_t bytes, cudaStream_t st) {
@@ -1345,7 +1367,8 @@ int fused_run_segment(double2* amp, uint32_t n, std::vector<PGate>& G, Planner& 
   if (sweeps.empty()) return DQ_OK;
   Blob blob;
   std::vector<size_t> offs(sweeps.size());
-  for (size_t i = 0; i < sweeps.size(); ++i) DQ_TRY(encode_sweep(sweeps[i], G, pl.RB, blob, &offs[i]));
+  for (size_t i = 0; i < sweeps.size(); ++i)
+    DQ_TRY(encode_sweep(sweeps[i], G, pl.TB, pl.RB, blob, &offs[i]));
   blob.align16();
   if (fw.plan_out) {  // plan-only: hand the programs back instead of running them
     const size_t base = fw.plan_out->size();
@@ -1368,7 +1391,7 @@ int fused_run_segment(double2* amp, uint32_t n, std::vector<PGate>& G, Planner& 
       cudaEventRecord(e0, st);
     }
     const SwHeader* hh = reinterpret_cast<const SwHeader*>(blob.buf.data() + offs[i]);
-    DQ_TRY(launch_sweep(amp, n, pl.RB, fw.d_blob + offs[i], hh->prog_bytes, st));
+    DQ_TRY(launch_sweep(amp, n, pl.TB, pl.RB, fw.d_blob + offs[i], hh->prog_bytes, st));
     if (timing) {
       cudaEventRecord(e1, st);
       fw.events.push_back(e0);
@@ -1386,11 +1409,18 @@ int fused_run(double2* amp, uint32_t n, const dq_inst* prog, uint64_t ninst, con
   (void)device;
   Planner pl;
   pl.n = n;
-  uint32_t M = 12;
-  if (o.fusion_width >= (int)kFusedMinQubits && o.fusion_width <= kMaxM) M = (uint32_t)o.fusion_width;
+  // thread geometry: DQSIM_SWEEP_TB=8 selects one 256-thread CTA per SM
+  static const uint32_t tb_env = []() {
+    const char* e = getenv("DQSIM_SWEEP_TB");
+    return (e && atoi(e) == 8) ? 8u : 7u;
+  }();
+  const uint32_t TB = tb_env;
+  uint32_t M = TB + 4;  // 16 amplitudes per thread
+  if (o.fusion_width >= (int)(TB + 2) && o.fusion_width <= (int)(TB + 4)) M = (uint32_t)o.fusion_width;
   if (M > n) M = n;
   pl.M = M;
-  pl.RB = M - kSwTB;
+  pl.TB = TB;
+  pl.RB = M - TB;
   pl.single_tile = (M == n);
   if (o.max_cost > 0) pl.budget = (double)o.max_cost;
   Poly poly;
