@@ -127,6 +127,7 @@ SIGNATURES = [
     ("dq_measure_p1", ctypes.c_int, [_P, _U32, _DP]),
     ("dq_collapse", ctypes.c_int, [_P, _U32, ctypes.c_int, ctypes.c_double]),
     ("dq_measure", ctypes.c_int, [_P, _U32, ctypes.c_double, ctypes.POINTER(ctypes.c_int), _DP]),
+    ("dq_measure_p1_noalloc", ctypes.c_int, [_P, _U32, _U32, _P, _P]),
     ("dq_run", ctypes.c_int, [_P, _P, _U64, _P, _U64, _U64, _P, _U64, ctypes.POINTER(RunOpts),
                               ctypes.POINTER(Profile)]),
     ("dq_marginal_probs", ctypes.c_int, [_P, _P, _U32, _P]),

@@ -506,6 +506,8 @@ int launch_gate(double2* s, uint32_t n, const GateOp& op, cudaStream_t st, int d
   return DQ_OK;
 }
 
+unsigned p1_reduction_blocks(uint32_t n, int device) { return red_blocks(1ULL << (n - 1), device); }
+
 int launch_p1(const double2* s, uint32_t n, uint32_t q, Scratch& sc, double* d_out,
               cudaStream_t st, int device) {
   const uint64_t count = 1ULL << (n - 1);

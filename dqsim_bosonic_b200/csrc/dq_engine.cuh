@@ -24,6 +24,8 @@ constexpr int kRedThreads = 512;
 int launch_gate(double2* s, uint32_t n, const GateOp& op, cudaStream_t st, int device,
                 uint64_t* launches);
 
+// Number of per-block partial sums the p1 reduction of an n-qubit state uses.
+unsigned p1_reduction_blocks(uint32_t n, int device);
 // p1 = sum over amplitudes with bit q set (device value in *d_out).
 int launch_p1(const double2* s, uint32_t n, uint32_t q, Scratch& sc, double* d_out,
               cudaStream_t st, int device);
