@@ -16,7 +16,7 @@ kernel's own achieved HBM bandwidth (its bytes per launch / its measured
 launch time) against the measured copy peak.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                  [--workload qft30|brickwork20]
+                  [--workload qftN|brickwork20]
 """
 from __future__ import annotations
 
@@ -52,10 +52,13 @@ def peak_hbm():
 # ---- workloads ---------------------------------------------------------------------------
 
 def workload(name: str):
-    if name == "qft30":
-        return _circuits.qft_with_x(30, 1234), {"workload": "qft30_fp64", "num_qubits": 30,
-                                                 "state_bytes": 16 * 2**30,
-                                                 "circuit": "x(seeded half) + QFT + swap network"}
+    if name.startswith("qft") and name[3:].isdigit():
+        n = int(name[3:])
+        if not 10 <= n <= 33:
+            raise SystemExit("qftN needs 10 <= N <= 33")
+        return _circuits.qft_with_x(n, 1234), {"workload": f"qft{n}_fp64", "num_qubits": n,
+                                                "state_bytes": 16 * 2**n,
+                                                "circuit": "x(seeded half) + QFT + swap network"}
     if name == "brickwork20":
         return _circuits.brickwork_u3_cx(20, 20, 1234), {"workload": "brickwork20_fp64",
                                                           "num_qubits": 20,
