@@ -450,9 +450,28 @@ def dominant_kernel_roofline(st, prog, exec_mode, stream, dev):
         name = "k_phase (cp, quarter of the state)"
         nbytes = 2 * 16 * (2 ** n) * 0.25
     achieved = nbytes / (ms * 1e-3) / 1e9
+    traffic, tsrc = None, None
+    if exec_mode == nat.EXEC_FUSED:
+        traffic, tsrc = sweep_traffic(n)
     return {"kernel": name, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak, "peak_source": src, "bytes_per_launch": nbytes,
-            "launch_ms": ms, "traffic": None}
+            "launch_ms": ms, "traffic": traffic, "traffic_source": tsrc}
+
+
+def sweep_traffic(n: int):
+    """DRAM bytes per sweep launch from the committed ncu capture, scaled to n qubits.
+
+    The capture (26 qubits, 1 GiB state) is small enough for a full ncu set; a sweep's
+    traffic scales with the 2^n amplitudes it streams."""
+    f = ROOT / "profiles" / "k_sweep_qft26.md"
+    try:
+        for line in f.read_text().splitlines():
+            if line.startswith("traffic_bytes_per_launch_at_26q"):
+                b26 = float(line.split("=")[1])
+                return b26 * 2.0 ** (n - 26), "ncu dram__bytes_read+write of k_sweep at 26 qubits x 2^(n-26)"
+    except OSError:
+        pass
+    return None, None
 
 
 def fused_sweep_timing(st, prog, stream, reps):

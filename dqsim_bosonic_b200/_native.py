@@ -57,7 +57,8 @@ INST_DTYPE = np.dtype(
     align=True,
 )
 COND_DTYPE = np.dtype([("creg_base", "<u8"), ("creg_size", "<u8"), ("creg_value", "<u8")], align=True)
-assert INST_DTYPE.itemsize == 88 and COND_DTYPE.itemsize == 24
+PAULI_DTYPE = np.dtype([("coeff", "<f8"), ("xmask", "<u8"), ("zmask", "<u8")], align=True)
+assert INST_DTYPE.itemsize == 88 and COND_DTYPE.itemsize == 24 and PAULI_DTYPE.itemsize == 24
 
 
 class RunOpts(ctypes.Structure):
@@ -135,6 +136,9 @@ SIGNATURES = [
     ("dq_sample_key", ctypes.c_int, [_P, _P, _U32, _P, _U64, _P, ctypes.POINTER(_U64)]),
     ("dq_inner", ctypes.c_int, [_P, _P, _U64, _DP, _DP]),
     ("dq_norm_sqr", ctypes.c_int, [_P, _DP]),
+    ("dq_expval_pauli", ctypes.c_int, [_P, _P, _U64, _DP]),
+    ("dq_adjoint", ctypes.c_int, [_P, _P, _U64, _P, _U64, _P, _U64, ctypes.POINTER(RunOpts), _DP,
+                                  _P]),
     ("dq_debug_plan", ctypes.c_int, [_U32, _P, _U64, ctypes.POINTER(RunOpts), _P, _U64,
                                      ctypes.POINTER(_U64)]),
     ("dq_rng_f64", ctypes.c_int, [_U64, _U64, _U64, _P]),

@@ -22,6 +22,7 @@
 #include "dq_engine.cuh"
 #include "dq_fused.cuh"
 #include "dq_gates.hpp"
+#include "dq_handle.cuh"
 #include "dq_rng.cuh"
 
 namespace dq {
@@ -37,6 +38,7 @@ namespace {
 std::mutex g_cache_mu;
 std::map<std::pair<int, size_t>, std::vector<void*>> g_cache;
 constexpr size_t kMaxCachedPerKey = 2;
+}  // namespace
 
 int cache_alloc(int device, size_t bytes, void** out) {
   {
@@ -78,42 +80,12 @@ void cache_free(int device, size_t bytes, void* p) {
   }
 }
 
-struct DeviceGuard {
-  int prev = -1;
-  explicit DeviceGuard(int dev) {
-    cudaGetDevice(&prev);
-    if (prev != dev) cudaSetDevice(dev);
-  }
-  ~DeviceGuard() {
-    int cur = -1;
-    cudaGetDevice(&cur);
-    if (prev >= 0 && cur != prev) cudaSetDevice(prev);
-  }
-};
-}  // namespace
-
 }  // namespace dq
 
-struct dq_state_s {
-  int device = 0;
-  uint32_t n = 0;
-  uint64_t len = 0;
-  size_t bytes = 0;
-  double2* amp = nullptr;
-  cudaStream_t stream = nullptr;
-  dq::Scratch sc;
-  dq::FusedWork fw;
-  // perm[l] = physical bit position holding logical qubit l (fused runs
-  // relabel swap gates instead of moving data)
-  uint32_t perm[64];
-  bool permuted = false;
-};
 
 using namespace dq;
 
-namespace {
-
-constexpr uint32_t kMaxQubits = 34;
+namespace dq {
 
 int check_handle(dq_state_t h) {
   if (!h || !h->amp) return fail(DQ_ERR_INVALID_ARG, "null or destroyed state handle");
@@ -357,7 +329,7 @@ int exec_inst(RunCtx& c, const dq_inst& in) {
   return do_gate_op(c, op, gate_qubit_count(in.kind) == 1 ? 0 : 1);
 }
 
-}  // namespace
+}  // namespace dq
 
 // =========================================================================
 // extern "C"

@@ -13,6 +13,7 @@
 
 #include "dq_common.cuh"
 #include "dq_engine.cuh"
+#include "dq_reduce.cuh"
 #include "dq_rng.cuh"
 
 namespace dq {
@@ -138,60 +139,6 @@ int launch_dense_k(double2* s, uint32_t n, const Gate& g, cudaStream_t st) {
   const uint64_t count = 1ULL << (n - K);
   k_dense<K><<<blocks_for(count, kThreads), kThreads, 0, st>>>(s, count, P);
   return DQ_OK;
-}
-
-// ---- reductions ------------------------------------------------------------------
-
-__device__ __forceinline__ double warp_sum(double v) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v = __dadd_rn(v, __shfl_down_sync(0xffffffffu, v, o));
-  return v;
-}
-
-// Sum over the block; the result is valid in thread 0.  Fixed tree order.
-__device__ double block_sum(double v) {
-  __shared__ double sh[32];
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  v = warp_sum(v);
-  __syncthreads();
-  if (lane == 0) sh[w] = v;
-  __syncthreads();
-  v = 0.0;
-  if (w == 0) {
-    v = (lane < (int)(blockDim.x >> 5)) ? sh[lane] : 0.0;
-    v = warp_sum(v);
-  }
-  return v;
-}
-
-// Writes this block's partial(s); the last block to finish sums all partials
-// in index order (deterministic for a fixed grid) into out[0..W).
-template <int W>
-__device__ void finish_partials(const double (&v)[W], double* partial, unsigned* counter,
-                                double* out) {
-  __shared__ bool last;
-  double tot[W];
-#pragma unroll
-  for (int c = 0; c < W; ++c) tot[c] = block_sum(v[c]);
-  if (threadIdx.x == 0) {
-#pragma unroll
-    for (int c = 0; c < W; ++c) partial[c * gridDim.x + blockIdx.x] = tot[c];
-    __threadfence();
-    const unsigned t = atomicAdd(counter, 1u);
-    last = (t == gridDim.x - 1);
-  }
-  __syncthreads();
-  if (!last) return;
-  __threadfence();
-#pragma unroll
-  for (int c = 0; c < W; ++c) {
-    double a = 0.0;
-    for (unsigned i = threadIdx.x; i < gridDim.x; i += blockDim.x)
-      a = __dadd_rn(a, __ldcg(partial + c * gridDim.x + i));
-    a = block_sum(a);
-    if (threadIdx.x == 0) out[c] = a;
-  }
-  if (threadIdx.x == 0) *counter = 0u;
 }
 
 __global__ void k_p1(const double2* __restrict__ s, uint64_t count, uint32_t q,
@@ -507,6 +454,7 @@ int launch_gate(double2* s, uint32_t n, const GateOp& op, cudaStream_t st, int d
 }
 
 unsigned p1_reduction_blocks(uint32_t n, int device) { return red_blocks(1ULL << (n - 1), device); }
+unsigned reduction_blocks(uint64_t items, int device) { return red_blocks(items, device); }
 
 int launch_p1(const double2* s, uint32_t n, uint32_t q, Scratch& sc, double* d_out,
               cudaStream_t st, int device) {

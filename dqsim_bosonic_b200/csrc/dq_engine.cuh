@@ -26,6 +26,8 @@ int launch_gate(double2* s, uint32_t n, const GateOp& op, cudaStream_t st, int d
 
 // Number of per-block partial sums the p1 reduction of an n-qubit state uses.
 unsigned p1_reduction_blocks(uint32_t n, int device);
+// Grid of a reduction kernel over `items` work items (at most kPartials / 4 blocks).
+unsigned reduction_blocks(uint64_t items, int device);
 // p1 = sum over amplitudes with bit q set (device value in *d_out).
 int launch_p1(const double2* s, uint32_t n, uint32_t q, Scratch& sc, double* d_out,
               cudaStream_t st, int device);

@@ -241,6 +241,38 @@ DQ_API int dq_sample_key(dq_state_t h, const uint32_t* qubits, uint32_t k, const
 DQ_API int dq_inner(dq_state_t h, const double* other, uint64_t len, double* re, double* im);
 DQ_API int dq_norm_sqr(dq_state_t h, double* out);
 
+/* ---- observables and adjoint differentiation --------------------------------
+ * No counterpart in the reference engine (it has no gradients); the
+ * observable convention matches its state layout (qubit q = bit q).
+ * A Pauli term is coeff * P with P = prod over qubits q of X_q^x(q) Z_q^z(q)
+ * where x(q), z(q) are bits of xmask, zmask, except that a qubit with both
+ * bits set carries Y_q = i X_q Z_q.  coeff is real: sum_t terms is Hermitian. */
+typedef struct dq_pauli_term {
+  double coeff;
+  uint64_t xmask; /* qubits carrying X or Y */
+  uint64_t zmask; /* qubits carrying Z or Y */
+} dq_pauli_term;
+
+/* <psi|H|psi> of the handle's state for H = sum of terms (nterms <= 65536). */
+DQ_API int dq_expval_pauli(dq_state_t h, const dq_pauli_term* terms, uint64_t nterms, double* out);
+
+/* Adjoint gradient of E = <psi|H|psi>, psi = U_prog |psi0>, where psi0 is the
+ * state the handle holds on entry.  prog must be unitary: gates only, no
+ * measure/reset/conditions (barrier/id are skipped).  param_index[4*i + j] is
+ * the entry of grad[nparams] that parameter p[j] of instruction i feeds
+ * (-1 = held fixed); grad receives the sum over all slots feeding an entry.
+ * Differentiable kinds: rx ry rz p u1 u2 u3 u crx cry crz cp cu1 cu3 cu rxx rzz;
+ * a slot of any other kind must be -1.  opts selects the forward pass
+ * (DQ_EXEC_FUSED or DQ_EXEC_PER_GATE; semantics must be DQ_SEM_SIMULATE).
+ * The backward pass walks the program in reverse, uncomputing psi with the
+ * inverse gates alongside lambda = H psi (no stored intermediate states; one
+ * extra state-sized buffer).  On return the handle holds psi0 again, up to
+ * rounding.  param_index may be NULL when nparams == 0 (E only). */
+DQ_API int dq_adjoint(dq_state_t h, const dq_inst* prog, uint64_t ninst,
+                      const int32_t* param_index, uint64_t nparams,
+                      const dq_pauli_term* terms, uint64_t nterms,
+                      const dq_run_opts* opts, double* expval, double* grad);
+
 /* ---- planner inspection (host only, no GPU needed) -------------------------
  * Runs the fused-sweep planner of dq_run (DQ_EXEC_FUSED) on a unitary
  * program of n qubits and writes the encoded sweep programs instead of

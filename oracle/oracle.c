@@ -748,3 +748,38 @@ int or_run_shots(uint32_t n, const dq_inst* prog, uint64_t ninst, const dq_cond*
   if (failed) *failed = fail_all;
   return rc_all;
 }
+
+/* <psi|H|psi> for H = sum_t coeff_t * P_t (dq_pauli_term convention of
+ * include/dqsim_cuda.h: P = i^{ny} X^x Z^z, Y on qubits with both bits).
+ * No reference counterpart (the reference has no observables); used as the
+ * checker of the engine's observables and, through or_run, of its adjoint
+ * gradients (parameter shift and finite differences on the CPU).  Plain
+ * ascending loops; terms are summed in the order given. */
+double or_expval_pauli(const double* st_, uint32_t n, const dq_pauli_term* terms,
+                       uint64_t nterms) {
+  const cpx* st = (const cpx*)st_;
+  const uint64_t len = 1ULL << n;
+  double total = 0.0;
+  for (uint64_t t = 0; t < nterms; ++t) {
+    const uint64_t x = terms[t].xmask, z = terms[t].zmask;
+    const int ny = __builtin_popcountll(x & z) & 3;
+    double re = 0.0, im = 0.0; /* sum_j conj(psi_j) (X^x Z^z psi)_j */
+    for (uint64_t j = 0; j < len; ++j) {
+      const uint64_t src = j ^ x;
+      const double sgn = (__builtin_popcountll(src & z) & 1) ? -1.0 : 1.0;
+      const cpx a = st[j], b = st[src];
+      re += sgn * (a.re * b.re + a.im * b.im);
+      im += sgn * (a.re * b.im - a.im * b.re);
+    }
+    /* multiply by i^ny and keep the real part */
+    double v;
+    switch (ny) {
+      case 0: v = re; break;
+      case 1: v = -im; break;
+      case 2: v = -re; break;
+      default: v = im; break;
+    }
+    total += terms[t].coeff * v;
+  }
+  return total;
+}

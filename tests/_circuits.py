@@ -185,3 +185,34 @@ def hea_ansatz(n: int, layers: int, seed: int):
         for q in range(n):
             insts.append(g("rzz", q, (q + 1) % n, float(params[k]))); k += 1
     return JsonCircuit(n, insts), params
+
+
+def hea_param_circuit(n: int, layers: int, seed: int, ham_seed: int = 5, ring: bool = True):
+    """The hardware-efficient ansatz as a ParamCircuit: per layer ry then rz on
+    every qubit, then rzz on the ring (i, i+1 mod n); angles ~ U[-pi, pi).
+    H = sum_i a_i Z_i Z_{i+1} + sum_i b_i X_i, a, b ~ N(0, 1).
+    Returns (circuit, theta, observable)."""
+    from dqsim_bosonic_b200.adjoint import Param, ParamCircuit, PauliSum
+
+    rng = np.random.default_rng(seed)
+    theta = rng.uniform(-math.pi, math.pi, size=layers * 3 * n)
+    c = ParamCircuit(n)
+    k = 0
+    pairs = [(q, (q + 1) % n) for q in range(n if ring else n - 1)]
+    for _ in range(layers):
+        for q in range(n):
+            c.ry(q, Param(k)); k += 1
+        for q in range(n):
+            c.rz(q, Param(k)); k += 1
+        for a, b in pairs:
+            c.rzz(a, b, Param(k)); k += 1
+    theta = theta[:k]
+    hr = np.random.default_rng(ham_seed)
+    a = hr.normal(size=len(pairs))
+    b = hr.normal(size=n)
+    H = PauliSum()
+    for (i, j), ai in zip(pairs, a):
+        H.add(float(ai), {i: "Z", j: "Z"})
+    for i, bi in enumerate(b):
+        H.add(float(bi), {i: "X"})
+    return c, theta, H

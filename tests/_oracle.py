@@ -48,6 +48,7 @@ def lib():
             "or_run": (ctypes.c_int, [P, U32, P, U64, P, U64, P, U64, P]),
             "or_run_shots": (ctypes.c_int, [U32, P, U64, P, U64, U64, U64, P, U64, P]),
             "or_fuse_export": (U64, [P, U64, U32, P, P, P]),
+            "or_expval_pauli": (ctypes.c_double, [P, U32, P, U64]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -169,3 +170,72 @@ def fuse(prog):
     mat = np.empty((cap, 4), dtype=np.complex128)
     nf = lib().or_fuse_export(_p(prog.insts), prog.ninst, n, _p(inst), _p(qub), _p(mat))
     return inst[:nf], qub[:nf], mat[:nf]
+
+
+def expval_pauli(state: np.ndarray, terms: np.ndarray) -> float:
+    """<psi|H|psi> on the CPU for a PAULI_DTYPE term array."""
+    st = np.ascontiguousarray(state, dtype=np.complex128)
+    t = np.ascontiguousarray(terms)
+    n = int(st.size).bit_length() - 1
+    return float(lib().or_expval_pauli(_p(st), n, _p(t), len(t)))
+
+
+def run_unitary(insts: np.ndarray, n: int, init: np.ndarray | None = None) -> np.ndarray:
+    """Final state of a unitary dq_inst program on the CPU (from |0> or init)."""
+    st = np.zeros(1 << n, dtype=np.complex128)
+    if init is None:
+        st[0] = 1.0
+    else:
+        st[:] = init
+    cb = np.full(1, -1, dtype=np.int32)
+    failed = ctypes.c_int64(-1)
+    a = np.ascontiguousarray(insts)
+    rc = lib().or_run(_p(st), n, _p(a), len(a), None, 0, _p(cb), 1, ctypes.byref(failed))
+    if rc != 0:
+        raise RuntimeError(f"oracle run failed: {rc}")
+    return st
+
+
+def expval_program(insts: np.ndarray, n: int, terms: np.ndarray) -> float:
+    return expval_pauli(run_unitary(insts, n), terms)
+
+
+# Shift rules restated for the checker: two-term rule for generators with a
+# single eigenvalue gap of 1 (rx/ry/rz/rxx/rzz, phases, u3 angles), four-term
+# rule (gaps 1/2 and 1) for controlled rotations.
+_R2 = ((0.5, np.pi / 2), (-0.5, -np.pi / 2))
+_d1 = (np.sqrt(2) + 1) / (4 * np.sqrt(2))
+_d2 = (np.sqrt(2) - 1) / (4 * np.sqrt(2))
+_R4 = ((_d1, np.pi / 2), (-_d1, -np.pi / 2), (-_d2, 3 * np.pi / 2), (_d2, -3 * np.pi / 2))
+
+
+def param_shift(circuit, theta, terms: np.ndarray, occurrences=None) -> np.ndarray:
+    """Parameter-shift gradient with every forward run on the oracle."""
+    base = circuit.bind(theta)
+    n = circuit.num_qubits
+    occ = circuit.occurrences()
+    grad = np.zeros(circuit.num_params)
+    for o in (range(len(occ)) if occurrences is None else occurrences):
+        i, j, p = occ[o]
+        kind = circuit.ops[i][0]
+        rule = _R4 if (kind in ("crx", "cry", "crz") or (kind in ("cu3", "cu") and j == 0)) else _R2
+        g = 0.0
+        for c, s in rule:
+            a = base.copy()
+            a[i]["p"][j] += s
+            g += c * expval_program(a, n, terms)
+        grad[p.index] += p.scale * g
+    return grad
+
+
+def finite_difference(circuit, theta, terms: np.ndarray, h: float = 1e-6, entries=None) -> np.ndarray:
+    """Central differences of <H> in theta on the oracle."""
+    th = np.asarray(theta, dtype=np.float64).copy()
+    n = circuit.num_qubits
+    out = np.zeros(th.size)
+    for k in (range(th.size) if entries is None else entries):
+        tp = th.copy(); tp[k] += h
+        tm = th.copy(); tm[k] -= h
+        out[k] = (expval_program(circuit.bind(tp), n, terms) -
+                  expval_program(circuit.bind(tm), n, terms)) / (2 * h)
+    return out
