@@ -89,6 +89,46 @@ class Profile(ctypes.Structure):
     ]
 
 
+class TrajOpts(ctypes.Structure):
+    _fields_ = [
+        ("threads", ctypes.c_int32),
+        ("max_cluster", ctypes.c_int32),
+        ("local_bits", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
+    ]
+
+
+class TrajStats(ctypes.Structure):
+    _fields_ = [
+        ("boundary_draws", ctypes.c_uint64),
+        ("failed_inst", ctypes.c_int64),
+        ("kernel_ms", ctypes.c_double),
+        ("prepare_ms", ctypes.c_double),
+        ("engine_ms", ctypes.c_double),
+        ("cluster_span", ctypes.c_uint32),
+        ("clusters", ctypes.c_uint32),
+        ("threads", ctypes.c_uint32),
+        ("local_bits", ctypes.c_uint32),
+        ("launches", ctypes.c_uint32),
+        ("engine_items", ctypes.c_uint32),
+    ]
+
+
+class BatchItem(ctypes.Structure):
+    _fields_ = [
+        ("n", ctypes.c_uint32),
+        ("reserved", ctypes.c_uint32),
+        ("prog", ctypes.c_void_p),
+        ("ninst", ctypes.c_uint64),
+        ("conds", ctypes.c_void_p),
+        ("nconds", ctypes.c_uint64),
+        ("seed", ctypes.c_uint64),
+        ("cbits_out", ctypes.c_void_p),
+        ("ncbits", ctypes.c_uint64),
+        ("state_out", ctypes.c_void_p),
+    ]
+
+
 class EngineError(RuntimeError):
     """A non-OK status returned by the engine."""
 
@@ -136,6 +176,11 @@ SIGNATURES = [
     ("dq_sample_key", ctypes.c_int, [_P, _P, _U32, _P, _U64, _P, ctypes.POINTER(_U64)]),
     ("dq_inner", ctypes.c_int, [_P, _P, _U64, _DP, _DP]),
     ("dq_norm_sqr", ctypes.c_int, [_P, _DP]),
+    ("dq_run_trajectories", ctypes.c_int, [ctypes.c_int, _U32, _P, _U64, _P, _U64, _U64, _U64,
+                                           _U64, _P, _U64, ctypes.POINTER(TrajOpts),
+                                           ctypes.POINTER(TrajStats)]),
+    ("dq_run_batch", ctypes.c_int, [ctypes.c_int, _P, _U64, ctypes.POINTER(TrajOpts),
+                                    ctypes.POINTER(TrajStats)]),
     ("dq_expval_pauli", ctypes.c_int, [_P, _P, _U64, _DP]),
     ("dq_adjoint", ctypes.c_int, [_P, _P, _U64, _P, _U64, _P, _U64, ctypes.POINTER(RunOpts), _DP,
                                   _P]),

@@ -1,0 +1,969 @@
+// dq_traj.cu — batched shot trajectories in one persistent launch.
+//
+// simulate_shots (statevector/simulator.rs:216-322) runs every shot as its
+// own trajectory: a fresh |0..0> state, the fused program (types.rs:248-293,
+// run_fused_par 870-884, run_instruction_par 638-864), mid-circuit measure /
+// reset / conditionals, and ChaCha8Rng::seed_from_u64(base_seed + i).  Here
+// each trajectory lives entirely in shared memory: a thread-block cluster of
+// 2^cb CTAs holds one 2^n-amplitude state (2^(n-cb) amplitudes per CTA, at
+// most 8192 = 128 KiB), so n <= 16 with clusters of up to 8 CTAs.  Gates on
+// the low n-cb qubits touch one CTA's shared memory; gates on the top cb
+// qubits pair elements across CTAs through distributed shared memory.  A
+// measurement reduces p1 per CTA (fixed order), exchanges the cluster's
+// partials, draws the outcome from the device ChaCha8 stream and collapses
+// in place.  Each cluster loops over trajectories until all shots are done;
+// the state never touches HBM, only the classical registers are written out.
+//
+// Arithmetic is the exact per-gate arithmetic of dq_engine.cu (num-complex
+// order, no FMA, zero matrix entries skipped), so amplitudes match the
+// oracle's sequential shot bit for bit; p1 is summed in a different order,
+// which can only change an outcome when the draw lies within rounding of
+// p1 — such draws (|r - p1| < 1e-12) are counted and reported.
+#include <cooperative_groups.h>
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+
+#include <string.h>
+
+#include <algorithm>
+#include <chrono>
+#include <string>
+#include <vector>
+
+#include "dq_common.cuh"
+#include "dq_gates.hpp"
+#include "dq_handle.cuh"
+#include "dq_rng.cuh"
+
+namespace cg = cooperative_groups;
+
+namespace dq {
+namespace {
+
+constexpr uint32_t kLocalBitsMax = 13;  // 8192 amplitudes = 128 KiB per CTA
+constexpr uint32_t kTrajMaxQubits = 16;
+constexpr uint32_t kTrajMaxCbits = 1024;
+
+enum TOpType : uint8_t {
+  T_NOP = 0, T_ONEQ, T_PHASE, T_XPERM, T_SWAP, T_DIAG, T_DENSE, T_MEASURE, T_RESET, T_FAIL
+};
+
+struct TOp {
+  uint8_t type;
+  uint8_t k;        // DIAG / DENSE: qubit count
+  uint8_t t1, t2;   // target(s)
+  uint32_t cond_first, cond_count;
+  int32_t cbit;     // MEASURE: classical bit; FAIL: unused
+  uint32_t mat;     // offset into the matrix pool (double2 units)
+  uint32_t remote;  // touches cluster qubits or needs a cluster reduction
+  uint64_t ctrl;    // control mask (all must be 1)
+  uint8_t q[8];     // DIAG / DENSE qubits, q[0] = MSB of the matrix index
+  int64_t inst;     // original instruction index (-1: a fused 2x2)
+};
+static_assert(sizeof(TOp) == 48, "TOp layout");
+
+struct TProg {         // one program of a launch
+  uint32_t ops_off, nops;
+  uint32_t n, lb;       // qubits; amplitudes per CTA = 2^lb
+  uint32_t ncbits, pad;
+  uint64_t base_seed;   // shot s draws from seed_from_u64(base_seed + s) (wrapping)
+  uint64_t cbits_off;   // shot s writes cbits_out[cbits_off + s * ncbits ...]
+  double2* state_out;   // device: final state of shot s at + s * 2^n, or null
+};
+struct TItem {          // one trajectory: a shot of a program
+  uint32_t prog, pad;
+  uint64_t shot;
+};
+struct TrajParams {
+  const TOp* ops;
+  const double2* pool;
+  const dq_cond* conds;
+  const TProg* progs;
+  const TItem* items;
+  int32_t* cbits_out;
+  unsigned long long* queue;     // work queue: next item index
+  unsigned long long* boundary;  // draws within 1e-12 of p1
+  long long* failed;             // lowest (prog << 40 | instruction) that failed
+  uint64_t nitems;
+};
+
+__device__ __forceinline__ uint32_t ins0(uint32_t k, uint32_t p) {
+  return ((k >> p) << (p + 1)) | (k & ((1u << p) - 1u));
+}
+
+// Fixed-order block sum, result broadcast to every thread.
+template <int THREADS>
+__device__ double block_sum_all(double v, double* sh) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = __dadd_rn(v, __shfl_down_sync(0xffffffffu, v, o));
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  __syncthreads();
+  if (lane == 0) sh[w] = v;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double a = 0.0;
+    for (int i = 0; i < THREADS / 32; ++i) a = __dadd_rn(a, sh[i]);
+    sh[32] = a;
+  }
+  __syncthreads();
+  return sh[32];
+}
+
+template <int THREADS>
+__global__ void __launch_bounds__(THREADS) k_traj(const TrajParams P) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  __shared__ double s_bcast[2];
+  __shared__ int s_skip[2];  // double-buffered by op parity: one barrier per op suffices
+  __shared__ unsigned long long s_item;
+
+  cg::cluster_group cl = cg::this_cluster();
+  const uint32_t C = cl.num_blocks(), rank = cl.block_rank();
+  const uint32_t tid = threadIdx.x;
+  auto sync_all = [&](bool cluster) {
+    if (cluster && C > 1) cl.sync(); else __syncthreads();
+  };
+
+  for (;;) {
+    // rank 0 takes the next trajectory from the queue and shares it
+    if (rank == 0 && tid == 0) s_item = atomicAdd(P.queue, 1ULL);
+    sync_all(true);
+    const unsigned long long item = (rank == 0) ? s_item : *cl.map_shared_rank(&s_item, 0);
+    if (item >= P.nitems) {
+      sync_all(true);  // no CTA leaves while another still reads its shared memory
+      break;
+    }
+    const TItem it = P.items[item];
+    const TProg pg = P.progs[it.prog];
+    const uint32_t lb = pg.lb, L = 1u << lb;
+    double2* sm = reinterpret_cast<double2*>(smraw);
+    double* red = reinterpret_cast<double*>(sm + L);    // [0..32]: block sums, [40]: CTA partial
+    int32_t* cb = reinterpret_cast<int32_t*>(red + 48);  // classical bits
+    const uint64_t gbase = (uint64_t)rank << lb;
+    const uint64_t lmask = (uint64_t)L - 1;
+    auto elem = [&](uint64_t g) -> double2* {
+      const uint32_t r = (uint32_t)(g >> lb);
+      double2* base = (r == rank) ? sm : cl.map_shared_rank(sm, r);
+      return base + (g & lmask);
+    };
+
+    uint32_t key[8];
+    seed_key_from_u64(pg.base_seed + it.shot, key);
+    uint64_t draws = 0;
+    for (uint32_t i = tid; i < L; i += THREADS) sm[i] = make_double2(0.0, 0.0);
+    for (uint32_t i = tid; i < pg.ncbits; i += THREADS) cb[i] = -1;
+    if (rank == 0 && tid == 0) sm[0] = make_double2(1.0, 0.0);
+    bool last_cluster = true;
+    sync_all(true);
+
+    for (uint32_t oi = 0; oi < pg.nops; ++oi) {
+      const TOp op = P.ops[pg.ops_off + oi];
+      // conditions (little-endian register value, unwritten bits read as 0)
+      if (op.cond_count) {
+        if (tid == 0) {
+          int ok = 1;
+          for (uint32_t c = 0; c < op.cond_count && ok; ++c) {
+            const dq_cond cd = P.conds[op.cond_first + c];
+            uint64_t actual = 0;
+            for (uint64_t b = 0; b < cd.creg_size; ++b) {
+              const uint64_t idx = cd.creg_base + b;
+              const int32_t v = (idx < pg.ncbits) ? cb[idx] : 0;
+              actual |= (uint64_t)(v > 0 ? v : 0) << b;
+            }
+            if (actual != cd.creg_value) ok = 0;
+          }
+          s_skip[oi & 1] = !ok;
+        }
+        __syncthreads();
+        if (s_skip[oi & 1]) continue;
+      }
+      const bool remote = op.remote && C > 1;
+      if (remote && !last_cluster) cl.sync();
+
+      switch (op.type) {
+        case T_ONEQ:
+        case T_XPERM: {
+          const uint32_t t = op.t1;
+          const uint64_t hi_ctrl = op.ctrl & ~lmask;
+          const uint64_t lo_ctrl = op.ctrl & lmask;
+          double2 u[4];
+          if (op.type == T_ONEQ)
+            for (int i = 0; i < 4; ++i) u[i] = P.pool[op.mat + i];
+          // local zero-insertion positions: target (if local) and local controls
+          uint32_t pos[9];
+          int np = 0;
+          uint64_t m = lo_ctrl | (t < lb ? (1ULL << t) : 0ULL);
+          while (m) {
+            const uint32_t b = __ffsll((long long)m) - 1;
+            pos[np++] = b;
+            m &= m - 1;
+          }
+          const uint32_t count = L >> np;
+          if (t < lb) {
+            if ((gbase & hi_ctrl) != hi_ctrl) break;
+            const uint32_t tb = 1u << t;
+            for (uint32_t k = tid; k < count; k += THREADS) {
+              uint32_t o = k;
+              for (int p = 0; p < np; ++p) o = ins0(o, pos[p]);
+              o |= (uint32_t)lo_ctrl;
+              double2* pa = sm + o;
+              double2* pb = sm + (o | tb);
+              const double2 a = *pa, b = *pb;
+              if (op.type == T_ONEQ) {
+                *pa = cadd_x(cmul_x(u[0], a), cmul_x(u[1], b));
+                *pb = cadd_x(cmul_x(u[2], a), cmul_x(u[3], b));
+              } else {
+                *pa = b;
+                *pb = a;
+              }
+            }
+          } else {
+            const uint32_t tbr = 1u << (t - lb);
+            const uint32_t r0 = rank & ~tbr, r1 = rank | tbr;
+            if ((((uint64_t)r0 << lb) & hi_ctrl) != hi_ctrl) break;
+            double2* b0 = (r0 == rank) ? sm : cl.map_shared_rank(sm, r0);
+            double2* b1 = (r1 == rank) ? sm : cl.map_shared_rank(sm, r1);
+            const uint32_t half = count > 1 ? count >> 1 : 1;
+            uint32_t lo, hi;
+            if (rank == r0) { lo = 0; hi = half; } else { lo = half; hi = count > 1 ? count : half; }
+            for (uint32_t k = lo + tid; k < hi; k += THREADS) {
+              uint32_t o = k;
+              for (int p = 0; p < np; ++p) o = ins0(o, pos[p]);
+              o |= (uint32_t)lo_ctrl;
+              double2* pa = b0 + o;
+              double2* pb = b1 + o;
+              const double2 a = *pa, b = *pb;
+              if (op.type == T_ONEQ) {
+                *pa = cadd_x(cmul_x(u[0], a), cmul_x(u[1], b));
+                *pb = cadd_x(cmul_x(u[2], a), cmul_x(u[3], b));
+              } else {
+                *pa = b;
+                *pb = a;
+              }
+            }
+          }
+          break;
+        }
+        case T_PHASE: {
+          const uint64_t need = op.ctrl | (1ULL << op.t1);
+          const uint64_t hi = need & ~lmask, lo = need & lmask;
+          if ((gbase & hi) != hi) break;
+          const double2 e = P.pool[op.mat];
+          uint32_t pos[9];
+          int np = 0;
+          uint64_t m = lo;
+          while (m) {
+            const uint32_t b = __ffsll((long long)m) - 1;
+            pos[np++] = b;
+            m &= m - 1;
+          }
+          const uint32_t count = L >> np;
+          for (uint32_t k = tid; k < count; k += THREADS) {
+            uint32_t o = k;
+            for (int p = 0; p < np; ++p) o = ins0(o, pos[p]);
+            o |= (uint32_t)lo;
+            sm[o] = cmul_x(e, sm[o]);
+          }
+          break;
+        }
+        case T_DIAG: {
+          const uint32_t kq = op.k;
+          for (uint32_t o = tid; o < L; o += THREADS) {
+            const uint64_t g = gbase | o;
+            uint32_t idx = 0;
+            for (uint32_t b = 0; b < kq; ++b) idx = (idx << 1) | (uint32_t)((g >> op.q[b]) & 1ULL);
+            const double2 d = P.pool[op.mat + idx];
+            if (d.x == 1.0 && d.y == 0.0) continue;
+            sm[o] = cmul_x(d, sm[o]);
+          }
+          break;
+        }
+        case T_SWAP: {
+          // pairs (i: t1 = 1, t2 = 0) <-> (j = i ^ both); the CTA owning i does the pair
+          const uint64_t b1 = 1ULL << op.t1, b2 = 1ULL << op.t2;
+          const uint64_t fixed1 = op.ctrl | b1;  // bits that must be 1 in i
+          const uint64_t gate = op.ctrl | b1 | b2;
+          const uint64_t hi_one = fixed1 & ~lmask, hi_zero = b2 & ~lmask;
+          if ((gbase & hi_one) != hi_one || (gbase & hi_zero) != 0) break;
+          uint32_t pos[10];
+          int np = 0;
+          uint64_t m = gate & lmask;
+          while (m) {
+            const uint32_t b = __ffsll((long long)m) - 1;
+            pos[np++] = b;
+            m &= m - 1;
+          }
+          const uint32_t count = L >> np;
+          const uint32_t lo_one = (uint32_t)(fixed1 & lmask);
+          for (uint32_t k = tid; k < count; k += THREADS) {
+            uint32_t o = k;
+            for (int p = 0; p < np; ++p) o = ins0(o, pos[p]);
+            o |= lo_one;
+            const uint64_t gi = gbase | o, gj = gi ^ b1 ^ b2;
+            double2* pi = sm + o;
+            double2* pj = elem(gj);
+            const double2 a = *pi, b = *pj;
+            *pi = b;
+            *pj = a;
+          }
+          break;
+        }
+        case T_DENSE: {
+          const uint32_t kq = op.k, D = 1u << kq;
+          uint64_t gm = 0;
+          for (uint32_t b = 0; b < kq; ++b) gm |= 1ULL << op.q[b];
+          if ((gbase & gm & ~lmask) != 0) break;  // group base must have the gate bits zero
+          uint32_t pos[8];
+          int np = 0;
+          uint64_t m = gm & lmask;
+          while (m) {
+            const uint32_t b = __ffsll((long long)m) - 1;
+            pos[np++] = b;
+            m &= m - 1;
+          }
+          const uint32_t count = L >> np;
+          for (uint32_t k = tid; k < count; k += THREADS) {
+            uint32_t o = k;
+            for (int p = 0; p < np; ++p) o = ins0(o, pos[p]);
+            const uint64_t base = gbase | o;
+            double2 v[32];
+            double2* ptr[32];
+            for (uint32_t j = 0; j < D; ++j) {
+              uint64_t off = 0;
+              for (uint32_t b = 0; b < kq; ++b)
+                if ((j >> (kq - 1 - b)) & 1u) off |= 1ULL << op.q[b];
+              ptr[j] = elem(base | off);
+              v[j] = *ptr[j];
+            }
+            for (uint32_t r = 0; r < D; ++r) {
+              double2 acc = make_double2(0.0, 0.0);
+              for (uint32_t c = 0; c < D; ++c) {
+                const double2 uu = P.pool[op.mat + r * D + c];
+                if (uu.x != 0.0 || uu.y != 0.0) acc = cadd_x(acc, cmul_x(uu, v[c]));
+              }
+              *ptr[r] = acc;
+            }
+          }
+          break;
+        }
+        case T_MEASURE:
+        case T_RESET: {
+          const uint32_t q = op.t1;
+          const uint64_t qb = 1ULL << q;
+          double part = 0.0;
+          if (q < lb) {
+            for (uint32_t k = tid; k < L / 2; k += THREADS)
+              part = __dadd_rn(part, norm_sqr_x(sm[ins0(k, q) | (uint32_t)qb]));
+          } else if (gbase & qb) {
+            for (uint32_t o = tid; o < L; o += THREADS) part = __dadd_rn(part, norm_sqr_x(sm[o]));
+          }
+          const double cta = block_sum_all<THREADS>(part, red);
+          if (tid == 0) red[40] = cta;
+          if (C > 1) cl.sync(); else __syncthreads();
+          if (tid == 0) {
+            double p1 = 0.0;
+            for (uint32_t r = 0; r < C; ++r) {
+              const double* pr = (r == rank) ? red : cl.map_shared_rank(red, r);
+              p1 = __dadd_rn(p1, pr[40]);
+            }
+            const double rr = chacha8_draw(key, draws);
+            const int o = rr < p1 ? 1 : 0;
+            double norm;
+            if (o == 1) {
+              norm = sqrt(p1);
+              if (norm < 1e-15) norm = 1e-15;
+            } else {
+              double t = 1.0 - p1;
+              if (t < 0.0) t = 0.0;
+              norm = sqrt(t);
+              if (norm < 1e-15) norm = 1e-15;
+            }
+            if (rank == 0 && fabs(rr - p1) < 1e-12) atomicAdd(P.boundary, 1ULL);
+            s_bcast[0] = (double)o;
+            s_bcast[1] = norm;
+            if (op.type == T_MEASURE) cb[op.cbit] = o;
+          }
+          ++draws;
+          __syncthreads();
+          const int o = (int)s_bcast[0];
+          const double norm = s_bcast[1];
+          for (uint32_t i = tid; i < L; i += THREADS) {
+            const bool set = ((gbase | i) & qb) != 0;
+            if (set != (o == 1)) {
+              sm[i] = make_double2(0.0, 0.0);
+            } else {
+              const double2 a = sm[i];
+              sm[i] = make_double2(__ddiv_rn(a.x, norm), __ddiv_rn(a.y, norm));
+            }
+          }
+          if (op.type == T_RESET && o == 1) {
+            // X on q: an exact exchange of the two halves
+            if (C > 1) cl.sync(); else __syncthreads();
+            if (q < lb) {
+              for (uint32_t k = tid; k < L / 2; k += THREADS) {
+                const uint32_t a0 = ins0(k, q), a1 = a0 | (uint32_t)qb;
+                const double2 x = sm[a0];
+                sm[a0] = sm[a1];
+                sm[a1] = x;
+              }
+            } else {
+              const uint32_t tbr = 1u << (q - lb);
+              if (!(rank & tbr)) {
+                double2* other = cl.map_shared_rank(sm, rank | tbr);
+                for (uint32_t i = tid; i < L; i += THREADS) {
+                  const double2 x = sm[i];
+                  sm[i] = other[i];
+                  other[i] = x;
+                }
+              }
+            }
+          }
+          break;
+        }
+        case T_FAIL:
+          if (tid == 0 && rank == 0) atomicMin(P.failed, ((long long)it.prog << 40) | op.inst);
+          break;
+        default:
+          break;
+      }
+      sync_all(remote);
+      last_cluster = remote || C == 1;
+      if (op.type == T_FAIL) break;
+    }
+    // classical bits and (optionally) the final state out; the next
+    // trajectory re-initialises after a cluster barrier
+    if (rank == 0)
+      for (uint32_t i = tid; i < pg.ncbits; i += THREADS)
+        P.cbits_out[pg.cbits_off + it.shot * pg.ncbits + i] = cb[i];
+    if (pg.state_out) {
+      double2* dst = pg.state_out + (it.shot << pg.n) + gbase;
+      for (uint32_t i = tid; i < L; i += THREADS) dst[i] = sm[i];
+    }
+    sync_all(true);
+  }
+}
+
+// ---- host side ---------------------------------------------------------------
+
+struct Encoded {
+  std::vector<TOp> ops;
+  std::vector<double2> pool;
+};
+
+uint32_t push_mat(Encoded& e, const hc* m, uint32_t count) {
+  const uint32_t off = (uint32_t)e.pool.size();
+  for (uint32_t i = 0; i < count; ++i) e.pool.push_back(make_double2(m[i].re, m[i].im));
+  return off;
+}
+
+TOp blank_op(int64_t inst, const dq_inst* in) {
+  TOp t{};
+  t.inst = inst;
+  t.cbit = -1;
+  if (in) {
+    t.cond_first = in->cond_first;
+    t.cond_count = in->cond_count;
+  }
+  return t;
+}
+
+void encode_gateop(Encoded& e, const GateOp& g, TOp t) {
+  switch (g.cls) {
+    case GC_ONE_Q:
+      t.type = T_ONEQ;
+      t.t1 = (uint8_t)g.target;
+      t.ctrl = g.ctrl_mask;
+      t.mat = push_mat(e, g.u, 4);
+      break;
+    case GC_PHASE:
+      t.type = T_PHASE;
+      t.t1 = (uint8_t)g.target;
+      t.ctrl = g.ctrl_mask;
+      t.mat = push_mat(e, g.u, 1);
+      break;
+    case GC_XPERM:
+      t.type = T_XPERM;
+      t.t1 = (uint8_t)g.target;
+      t.ctrl = g.ctrl_mask;
+      break;
+    case GC_SWAP:
+      t.type = T_SWAP;
+      t.t1 = (uint8_t)g.target;
+      t.t2 = (uint8_t)g.target2;
+      t.ctrl = g.ctrl_mask;
+      break;
+    case GC_DIAG: {
+      t.type = T_DIAG;
+      t.k = (uint8_t)g.dense.k;
+      for (uint32_t b = 0; b < g.dense.k; ++b) t.q[b] = (uint8_t)g.dense.qubits[b];
+      const uint32_t D = 1u << g.dense.k;
+      std::vector<hc> d(D);
+      for (uint32_t i = 0; i < D; ++i) d[i] = g.dense.m[i * D + i];
+      t.mat = push_mat(e, d.data(), D);
+      break;
+    }
+    case GC_DENSE: {
+      t.type = T_DENSE;
+      t.k = (uint8_t)g.dense.k;
+      for (uint32_t b = 0; b < g.dense.k; ++b) t.q[b] = (uint8_t)g.dense.qubits[b];
+      const uint32_t D = 1u << g.dense.k;
+      t.mat = push_mat(e, g.dense.m, D * D);
+      break;
+    }
+    default:
+      t.type = T_NOP;
+      break;
+  }
+  e.ops.push_back(t);
+}
+
+// The fused shot program (fuse_program) as device ops, appended to e.
+int encode_program(const dq_inst* prog, uint64_t ninst, uint32_t n, uint32_t cond_base,
+                   Encoded& e) {
+  const std::vector<FusedEntry> fused = fuse_program(prog, ninst, n);
+  for (const FusedEntry& f : fused) {
+    if (f.inst < 0) {
+      GateOp g;
+      classify_1q(f.m, f.qubit, 0, g);
+      encode_gateop(e, g, blank_op(-1, nullptr));
+      continue;
+    }
+    const dq_inst& in = prog[f.inst];
+    TOp t = blank_op(f.inst, &in);
+    t.cond_first += cond_base;
+    switch (in.kind) {
+      case DQ_ID: case DQ_U0: case DQ_BARRIER: case DQ_CLASSICAL: case DQ_G_NOOP:
+      case DQ_G_OPAQUE:  // a no-op in the shot path (run_instruction_par)
+        continue;
+      case DQ_G_UNSUPPORTED:
+        t.type = T_FAIL;
+        e.ops.push_back(t);
+        continue;
+      case DQ_MEASURE:
+        t.type = T_MEASURE;
+        t.t1 = (uint8_t)in.q[0];
+        t.cbit = (int32_t)in.cbit;
+        e.ops.push_back(t);
+        continue;
+      case DQ_RESET:
+        t.type = T_RESET;
+        t.t1 = (uint8_t)in.q[0];
+        e.ops.push_back(t);
+        continue;
+      default:
+        break;
+    }
+    GateOp g;
+    if (!inst_to_op(in, g)) return fail(DQ_ERR_INTERNAL, "instruction kind without a matrix");
+    encode_gateop(e, g, t);
+  }
+  return DQ_OK;
+}
+
+void mark_remote(TOp* ops, size_t count, uint32_t lb) {
+  const uint64_t lmask = (1ULL << lb) - 1;
+  for (size_t i = 0; i < count; ++i) {
+    TOp& t = ops[i];
+    uint64_t touched = 0;
+    switch (t.type) {
+      case T_ONEQ: case T_XPERM: touched = 1ULL << t.t1; break;
+      case T_SWAP: touched = (1ULL << t.t1) | (1ULL << t.t2); break;
+      case T_DENSE:
+        for (uint32_t b = 0; b < t.k; ++b) touched |= 1ULL << t.q[b];
+        break;
+      case T_MEASURE: case T_RESET: t.remote = 1; continue;
+      default: break;
+    }
+    t.remote = (touched & ~lmask) ? 1u : 0u;
+  }
+}
+
+// All programs and trajectories of one launch (one cluster span).
+struct LaunchSet {
+  Encoded enc;
+  std::vector<dq_cond> conds;
+  std::vector<TProg> progs;
+  std::vector<TItem> items;
+  uint32_t C = 1;
+  uint32_t max_lb = 1, max_ncbits = 0;
+};
+
+int add_program(LaunchSet& ls, const dq_inst* prog, uint64_t ninst, const dq_cond* conds,
+                uint64_t nconds, uint32_t n, uint32_t lb, uint64_t base_seed, uint64_t cbits_off,
+                uint32_t ncbits, double2* state_out) {
+  TProg pg{};
+  pg.ops_off = (uint32_t)ls.enc.ops.size();
+  const uint32_t cond_base = (uint32_t)ls.conds.size();
+  for (uint64_t c = 0; c < nconds; ++c) ls.conds.push_back(conds[c]);
+  DQ_TRY(encode_program(prog, ninst, n, cond_base, ls.enc));
+  pg.nops = (uint32_t)(ls.enc.ops.size() - pg.ops_off);
+  mark_remote(ls.enc.ops.data() + pg.ops_off, pg.nops, lb);
+  pg.n = n;
+  pg.lb = lb;
+  pg.ncbits = ncbits;
+  pg.base_seed = base_seed;
+  pg.cbits_off = cbits_off;
+  pg.state_out = state_out;
+  ls.progs.push_back(pg);
+  ls.max_lb = std::max(ls.max_lb, lb);
+  ls.max_ncbits = std::max(ls.max_ncbits, ncbits);
+  return DQ_OK;
+}
+
+template <int THREADS>
+int launch_traj(const TrajParams& P, uint32_t C, size_t smem, int device, cudaStream_t st,
+                uint32_t* clusters_out) {
+  DQ_CUDA_TRY(cudaFuncSetAttribute(k_traj<THREADS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)smem));
+  cudaLaunchConfig_t cfg{};
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = C;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.blockDim = dim3(THREADS, 1, 1);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  int max_clusters = 0;
+  cfg.gridDim = dim3(C, 1, 1);
+  cudaError_t e = cudaOccupancyMaxActiveClusters(&max_clusters, (void*)k_traj<THREADS>, &cfg);
+  if (e != cudaSuccess || max_clusters < 1) {
+    cudaGetLastError();
+    return fail(DQ_ERR_UNSUPPORTED, std::string("trajectory kernel does not fit: cluster of ") +
+                                        std::to_string(C) + " CTAs x " + std::to_string(smem) +
+                                        " B shared memory");
+  }
+  uint64_t ncl = std::min<uint64_t>((uint64_t)max_clusters, P.nitems);
+  if (ncl < 1) ncl = 1;
+  cfg.gridDim = dim3((unsigned)(ncl * C), 1, 1);
+  DQ_CUDA_TRY(cudaLaunchKernelEx(&cfg, k_traj<THREADS>, P));
+  *clusters_out = (uint32_t)ncl;
+  return DQ_OK;
+}
+
+// Device buffers of one launch, freed on scope exit.
+struct LaunchBuffers {
+  TOp* ops = nullptr;
+  double2* pool = nullptr;
+  dq_cond* conds = nullptr;
+  TProg* progs = nullptr;
+  TItem* items = nullptr;
+  unsigned long long* ctr = nullptr;  // [0] queue, [1] boundary, [2] failed
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  cudaStream_t st = nullptr;
+  ~LaunchBuffers() {
+    if (st) cudaStreamSynchronize(st);
+    if (ops) cudaFree(ops);
+    if (pool) cudaFree(pool);
+    if (conds) cudaFree(conds);
+    if (progs) cudaFree(progs);
+    if (items) cudaFree(items);
+    if (ctr) cudaFree(ctr);
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+  }
+};
+
+template <class T>
+int upload(T** dst, const std::vector<T>& v, cudaStream_t st) {
+  const size_t bytes = sizeof(T) * std::max<size_t>(v.size(), 1);
+  DQ_CUDA_TRY(cudaMalloc((void**)dst, bytes));
+  if (!v.empty())
+    DQ_CUDA_TRY(cudaMemcpyAsync(*dst, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice, st));
+  return DQ_OK;
+}
+
+// Runs every item of ls in one persistent launch; cbits land in d_cbits.
+int run_launch(LaunchSet& ls, int threads, int device, cudaStream_t st, int32_t* d_cbits,
+               dq_traj_stats* acc) {
+  if (ls.items.empty()) return DQ_OK;
+  if (ls.enc.pool.empty()) ls.enc.pool.push_back(make_double2(0, 0));
+  LaunchBuffers b;
+  b.st = st;
+  DQ_TRY(upload(&b.ops, ls.enc.ops, st));
+  DQ_TRY(upload(&b.pool, ls.enc.pool, st));
+  DQ_TRY(upload(&b.conds, ls.conds, st));
+  DQ_TRY(upload(&b.progs, ls.progs, st));
+  DQ_TRY(upload(&b.items, ls.items, st));
+  DQ_CUDA_TRY(cudaMalloc((void**)&b.ctr, 3 * sizeof(unsigned long long)));
+  const unsigned long long init[3] = {0ULL, 0ULL, 0x7fffffffffffffffULL};
+  DQ_CUDA_TRY(cudaMemcpyAsync(b.ctr, init, sizeof(init), cudaMemcpyHostToDevice, st));
+  DQ_CUDA_TRY(cudaEventCreate(&b.e0));
+  DQ_CUDA_TRY(cudaEventCreate(&b.e1));
+  TrajParams P{};
+  P.ops = b.ops;
+  P.pool = b.pool;
+  P.conds = b.conds;
+  P.progs = b.progs;
+  P.items = b.items;
+  P.cbits_out = d_cbits;
+  P.queue = b.ctr;
+  P.boundary = b.ctr + 1;
+  P.failed = reinterpret_cast<long long*>(b.ctr + 2);
+  P.nitems = ls.items.size();
+  const size_t smem = sizeof(double2) * (1u << ls.max_lb) + sizeof(double) * 48 +
+                      sizeof(int32_t) * std::max<uint32_t>(ls.max_ncbits, 1);
+  uint32_t clusters = 0;
+  DQ_CUDA_TRY(cudaEventRecord(b.e0, st));
+  if (threads == 128) DQ_TRY(launch_traj<128>(P, ls.C, smem, device, st, &clusters));
+  else if (threads == 256) DQ_TRY(launch_traj<256>(P, ls.C, smem, device, st, &clusters));
+  else DQ_TRY(launch_traj<512>(P, ls.C, smem, device, st, &clusters));
+  DQ_CUDA_TRY(cudaEventRecord(b.e1, st));
+  unsigned long long ctr[3];
+  DQ_CUDA_TRY(cudaMemcpyAsync(ctr, b.ctr, sizeof(ctr), cudaMemcpyDeviceToHost, st));
+  DQ_CUDA_TRY(cudaStreamSynchronize(st));
+  float ms = 0.f;
+  DQ_CUDA_TRY(cudaEventElapsedTime(&ms, b.e0, b.e1));
+  acc->boundary_draws += ctr[1];
+  const long long f = (long long)ctr[2];
+  if (f != 0x7fffffffffffffffLL && (acc->failed_inst < 0 || f < acc->failed_inst))
+    acc->failed_inst = f;
+  acc->kernel_ms += ms;
+  acc->cluster_span = std::max(acc->cluster_span, ls.C);
+  acc->clusters = clusters;
+  acc->threads = (uint32_t)threads;
+  acc->local_bits = std::max(acc->local_bits, ls.max_lb);
+  acc->launches += 1;
+  return DQ_OK;
+}
+
+int check_opts(const dq_traj_opts* opts, int* threads, uint32_t* max_span, uint32_t* force_lb) {
+  dq_traj_opts o{};
+  if (opts) o = *opts;
+  *threads = o.threads ? o.threads : 256;
+  if (*threads != 128 && *threads != 256 && *threads != 512)
+    return fail(DQ_ERR_INVALID_ARG, "threads must be 128, 256 or 512");
+  *max_span = o.max_cluster ? (uint32_t)o.max_cluster : 8u;
+  if (*max_span != 1 && *max_span != 2 && *max_span != 4 && *max_span != 8)
+    return fail(DQ_ERR_INVALID_ARG, "max_cluster must be 1, 2, 4 or 8");
+  *force_lb = 0;
+  if (o.local_bits) {
+    if (o.local_bits < 1 || (uint32_t)o.local_bits > kLocalBitsMax)
+      return fail(DQ_ERR_INVALID_ARG, "local_bits must be in 1..13");
+    *force_lb = (uint32_t)o.local_bits;
+  }
+  return DQ_OK;
+}
+
+// Amplitudes per CTA (2^lb) and cluster span for an n-qubit trajectory.
+int geometry(uint32_t n, uint32_t max_span, uint32_t force_lb, uint32_t* lb, uint32_t* C) {
+  *lb = std::min(n, force_lb ? force_lb : kLocalBitsMax);
+  // a smaller max_span needs more amplitudes per CTA than 2^13: not possible
+  *C = 1u << (n - *lb);
+  if (*C > max_span)
+    return fail(DQ_ERR_INVALID_ARG, "a " + std::to_string(n) + "-qubit trajectory needs " +
+                                        std::to_string(*C) + " CTAs per cluster, more than max_cluster");
+  return DQ_OK;
+}
+
+double ms_since(std::chrono::steady_clock::time_point t0) {
+  return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+}
+
+void init_stats(dq_traj_stats* s) {
+  memset(s, 0, sizeof(*s));
+  s->failed_inst = -1;
+}
+
+}  // namespace
+}  // namespace dq
+
+using namespace dq;
+
+extern "C" {
+
+int dq_run_trajectories(int device, uint32_t n, const dq_inst* prog, uint64_t ninst,
+                        const dq_cond* conds, uint64_t nconds, uint64_t base_seed, uint64_t shot0,
+                        uint64_t shots, int32_t* cbits_out, uint64_t ncbits,
+                        const dq_traj_opts* opts, dq_traj_stats* stats) {
+  dq_traj_stats acc;
+  init_stats(&acc);
+  if (stats) *stats = acc;
+  if (n < 1 || n > kTrajMaxQubits)
+    return fail(DQ_ERR_INVALID_ARG, "dq_run_trajectories: n must be in 1..16");
+  if (ninst && !prog) return fail(DQ_ERR_INVALID_ARG, "null program");
+  if (shots && ncbits && !cbits_out) return fail(DQ_ERR_INVALID_ARG, "null cbits output");
+  if (ncbits > kTrajMaxCbits) return fail(DQ_ERR_INVALID_ARG, "at most 1024 classical bits");
+  if (shots > (1ULL << 40)) return fail(DQ_ERR_INVALID_ARG, "too many shots");
+  for (uint64_t i = 0; i < ninst; ++i) DQ_TRY(validate_inst(prog[i], n, nconds, ncbits, conds, i));
+  int threads;
+  uint32_t max_span, force_lb, lb, C;
+  DQ_TRY(check_opts(opts, &threads, &max_span, &force_lb));
+  DQ_TRY(geometry(n, max_span, force_lb, &lb, &C));
+  const auto t0 = std::chrono::steady_clock::now();
+  LaunchSet ls;
+  ls.C = C;
+  DQ_TRY(add_program(ls, prog, ninst, conds, nconds, n, lb, base_seed + shot0, 0,
+                     (uint32_t)ncbits, nullptr));
+  ls.items.resize(shots);
+  for (uint64_t s = 0; s < shots; ++s) ls.items[s] = TItem{0, 0, s};
+  acc.prepare_ms = ms_since(t0);
+
+  DeviceGuard g(device);
+  cudaStream_t st = nullptr;
+  DQ_CUDA_TRY(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+  int32_t* d_out = nullptr;
+  const size_t out_bytes = sizeof(int32_t) * (size_t)shots * ncbits;
+  int rc = DQ_OK;
+  cudaError_t e = cudaMalloc((void**)&d_out, std::max<size_t>(out_bytes, 4));
+  if (e != cudaSuccess) rc = fail(DQ_ERR_OOM, std::string("cudaMalloc(cbits): ") + cudaGetErrorString(e));
+  if (rc == DQ_OK) rc = run_launch(ls, threads, device, st, d_out, &acc);
+  if (rc == DQ_OK && out_bytes) {
+    e = cudaMemcpyAsync(cbits_out, d_out, out_bytes, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) rc = fail(DQ_ERR_CUDA, std::string("copy cbits: ") + cudaGetErrorString(e));
+  }
+  cudaStreamSynchronize(st);
+  if (d_out) cudaFree(d_out);
+  cudaStreamDestroy(st);
+  if (acc.failed_inst >= 0) acc.failed_inst &= (1LL << 40) - 1;
+  if (stats) *stats = acc;
+  DQ_TRY(rc);
+  if (acc.failed_inst >= 0)
+    return fail(DQ_ERR_UNSUPPORTED, "instruction " + std::to_string(acc.failed_inst) +
+                                        ": unsupported generic gate reached in a trajectory");
+  return DQ_OK;
+}
+
+int dq_run_batch(int device, const dq_batch_item* items, uint64_t nitems,
+                 const dq_traj_opts* opts, dq_traj_stats* stats) {
+  dq_traj_stats acc;
+  init_stats(&acc);
+  if (stats) *stats = acc;
+  if (nitems && !items) return fail(DQ_ERR_INVALID_ARG, "null items");
+  int threads;
+  uint32_t max_span, force_lb;
+  DQ_TRY(check_opts(opts, &threads, &max_span, &force_lb));
+  for (uint64_t k = 0; k < nitems; ++k) {
+    const dq_batch_item& it = items[k];
+    const std::string pre = "item " + std::to_string(k) + ": ";
+    if (it.n < 1 || it.n > kMaxQubits) return fail(DQ_ERR_INVALID_ARG, pre + "n must be in 1..34");
+    if (it.ninst && !it.prog) return fail(DQ_ERR_INVALID_ARG, pre + "null program");
+    if (it.ncbits && !it.cbits_out) return fail(DQ_ERR_INVALID_ARG, pre + "null cbits output");
+    if (it.ncbits > kTrajMaxCbits) return fail(DQ_ERR_INVALID_ARG, pre + "at most 1024 classical bits");
+    for (uint64_t i = 0; i < it.ninst; ++i) {
+      const int rc = validate_inst(it.prog[i], it.n, it.nconds, it.ncbits, it.conds, i);
+      if (rc != DQ_OK) return fail(rc, pre + dq_last_error());
+    }
+  }
+  DeviceGuard g(device);
+  const auto t0 = std::chrono::steady_clock::now();
+  // resident items grouped by cluster span; the rest run on the HBM engine
+  LaunchSet sets[4];
+  for (int c = 0; c < 4; ++c) sets[c].C = 1u << c;
+  std::vector<std::vector<uint64_t>> members(4);
+  std::vector<uint64_t> engine_items;
+  for (uint64_t k = 0; k < nitems; ++k) {
+    const uint32_t n = items[k].n;
+    if (n > kTrajMaxQubits) {
+      engine_items.push_back(k);
+      continue;
+    }
+    uint32_t lb, C;
+    DQ_TRY(geometry(n, max_span, force_lb, &lb, &C));
+    members[__builtin_ctz(C)].push_back(k);
+  }
+  // per set: state outputs packed into one device buffer, cbits likewise
+  struct Out { uint64_t item, state_off, cbits_off; };
+  std::vector<Out> outs[4];
+  uint64_t state_amps[4] = {0, 0, 0, 0}, cbit_words[4] = {0, 0, 0, 0};
+  for (int c = 0; c < 4; ++c) {
+    // costliest first (longest-processing-time order for the work queue)
+    std::vector<uint64_t>& m = members[c];
+    std::stable_sort(m.begin(), m.end(), [&](uint64_t a, uint64_t b) {
+      return (items[a].ninst << items[a].n) > (items[b].ninst << items[b].n);
+    });
+    for (uint64_t k : m) {
+      Out o{k, items[k].state_out ? state_amps[c] : ~0ULL, cbit_words[c]};
+      if (items[k].state_out) state_amps[c] += 1ULL << items[k].n;
+      cbit_words[c] += items[k].ncbits;
+      outs[c].push_back(o);
+    }
+  }
+  acc.prepare_ms = ms_since(t0);
+
+  cudaStream_t st = nullptr;
+  DQ_CUDA_TRY(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+  int rc = DQ_OK;
+  for (int c = 0; c < 4 && rc == DQ_OK; ++c) {
+    if (outs[c].empty()) continue;
+    double2* d_states = nullptr;
+    int32_t* d_cbits = nullptr;
+    cudaError_t e = cudaMalloc((void**)&d_states, sizeof(double2) * std::max<uint64_t>(state_amps[c], 1));
+    if (e == cudaSuccess) e = cudaMalloc((void**)&d_cbits, sizeof(int32_t) * std::max<uint64_t>(cbit_words[c], 1));
+    if (e != cudaSuccess) rc = fail(DQ_ERR_OOM, std::string("cudaMalloc(batch outputs): ") + cudaGetErrorString(e));
+    const auto tp = std::chrono::steady_clock::now();
+    LaunchSet& ls = sets[c];
+    for (const Out& o : outs[c]) {
+      if (rc != DQ_OK) break;
+      const dq_batch_item& it = items[o.item];
+      uint32_t lb, C;
+      geometry(it.n, max_span, force_lb, &lb, &C);
+      const uint32_t pi = (uint32_t)ls.progs.size();
+      rc = add_program(ls, it.prog, it.ninst, it.conds, it.nconds, it.n, lb, it.seed, o.cbits_off,
+                       (uint32_t)it.ncbits, o.state_off == ~0ULL ? nullptr : d_states + o.state_off);
+      ls.items.push_back(TItem{pi, 0, 0});
+    }
+    acc.prepare_ms += ms_since(tp);
+    if (rc == DQ_OK) rc = run_launch(ls, threads, device, st, d_cbits, &acc);
+    for (const Out& o : outs[c]) {
+      if (rc != DQ_OK) break;
+      const dq_batch_item& it = items[o.item];
+      if (it.state_out)
+        e = cudaMemcpyAsync(it.state_out, d_states + o.state_off, sizeof(double2) << it.n,
+                            cudaMemcpyDeviceToHost, st);
+      if (e == cudaSuccess && it.ncbits)
+        e = cudaMemcpyAsync(it.cbits_out, d_cbits + o.cbits_off, sizeof(int32_t) * it.ncbits,
+                            cudaMemcpyDeviceToHost, st);
+      if (e != cudaSuccess) rc = fail(DQ_ERR_CUDA, std::string("copy batch outputs: ") + cudaGetErrorString(e));
+    }
+    cudaStreamSynchronize(st);
+    if (d_states) cudaFree(d_states);
+    if (d_cbits) cudaFree(d_cbits);
+    if (rc == DQ_OK && acc.failed_inst >= 0) {
+      // map (program << 40 | instruction) back to the caller's item index
+      const uint64_t pi = (uint64_t)acc.failed_inst >> 40;
+      const uint64_t inst = (uint64_t)acc.failed_inst & ((1ULL << 40) - 1);
+      acc.failed_inst = (int64_t)((outs[c][pi].item << 40) | inst);
+      rc = fail(DQ_ERR_UNSUPPORTED, "item " + std::to_string(outs[c][pi].item) + ", instruction " +
+                                        std::to_string(inst) + ": unsupported generic gate");
+    }
+  }
+  // large states: the HBM engine, one state per size reused across items
+  dq_state_t h = nullptr;
+  for (uint64_t k : engine_items) {
+    if (rc != DQ_OK) break;
+    const dq_batch_item& it = items[k];
+    if (h && h->n != it.n) {
+      dq_state_destroy(h);
+      h = nullptr;
+    }
+    if (!h) rc = dq_state_create(it.n, device, &h);
+    else rc = dq_state_reset(h);
+    if (rc != DQ_OK) break;
+    std::vector<int32_t> cb(std::max<uint64_t>(it.ncbits, 1), -1);
+    dq_run_opts o{};
+    o.semantics = DQ_SEM_SHOTS;
+    o.exec = DQ_EXEC_FUSED;
+    dq_profile prof{};
+    const auto te = std::chrono::steady_clock::now();
+    rc = dq_run(h, it.prog, it.ninst, it.conds, it.nconds, it.seed, cb.data(), it.ncbits, &o, &prof);
+    acc.engine_ms += ms_since(te);
+    acc.boundary_draws += prof.boundary_draws;
+    if (rc != DQ_OK) {
+      acc.failed_inst = (int64_t)((k << 40) | (uint64_t)std::max<int64_t>(prof.failed_inst, 0));
+      break;
+    }
+    if (it.ncbits) memcpy(it.cbits_out, cb.data(), sizeof(int32_t) * it.ncbits);
+    if (it.state_out) rc = dq_state_download(h, it.state_out, 1ULL << it.n);
+    acc.engine_items += 1;
+  }
+  if (h) dq_state_destroy(h);
+  cudaStreamDestroy(st);
+  if (stats) *stats = acc;
+  return rc;
+}
+
+}  // extern "C"

@@ -241,6 +241,65 @@ DQ_API int dq_sample_key(dq_state_t h, const uint32_t* qubits, uint32_t k, const
 DQ_API int dq_inner(dq_state_t h, const double* other, uint64_t len, double* re, double* im);
 DQ_API int dq_norm_sqr(dq_state_t h, double* out);
 
+/* ---- batched shot trajectories ----------------------------------------------
+ * simulate_shots (statevector/simulator.rs:216-322) for states of up to 16
+ * qubits in one persistent launch: each trajectory (shot s, seed
+ * base_seed + shot0 + s, wrapping) runs the fused shot program
+ * (types.rs:248-293, run_instruction_par 638-864) on a state held in the
+ * shared memory of a thread-block cluster (2^local_bits amplitudes per CTA).
+ * cbits_out[s * ncbits + b] receives the shot's classical bits (-1 = never
+ * written).  Outcomes match the per-shot dq_run (DQ_SEM_SHOTS) except for
+ * draws within 1e-12 of p1, counted in boundary_draws.  ncbits <= 1024. */
+typedef struct dq_traj_opts {
+  int32_t threads;     /* threads per CTA: 128, 256 or 512 (0 = 256) */
+  int32_t max_cluster; /* most CTAs per trajectory: 1, 2, 4 or 8 (0 = 8) */
+  int32_t local_bits;  /* amplitudes per CTA = 2^local_bits, 1..13 (0 = min(n, 13)) */
+  int32_t reserved;
+} dq_traj_opts;
+
+typedef struct dq_traj_stats {
+  uint64_t boundary_draws;
+  int64_t failed_inst;   /* -1, or the instruction that failed (unsupported gate);
+                            dq_run_batch: item << 40 | instruction */
+  double kernel_ms;      /* device time of the resident launches (CUDA events) */
+  double prepare_ms;     /* host time fusing and encoding the programs */
+  double engine_ms;      /* dq_run_batch: host time of items run on the HBM engine */
+  uint32_t cluster_span; /* CTAs per trajectory (largest used) */
+  uint32_t clusters;     /* clusters resident in the last launch */
+  uint32_t threads;
+  uint32_t local_bits;   /* amplitudes per CTA = 2^local_bits (largest used) */
+  uint32_t launches;     /* resident launches */
+  uint32_t engine_items; /* dq_run_batch: items with n > 16 (HBM engine) */
+} dq_traj_stats;
+
+DQ_API int dq_run_trajectories(int device, uint32_t n, const dq_inst* prog, uint64_t ninst,
+                               const dq_cond* conds, uint64_t nconds, uint64_t base_seed,
+                               uint64_t shot0, uint64_t shots, int32_t* cbits_out,
+                               uint64_t ncbits, const dq_traj_opts* opts, dq_traj_stats* stats);
+
+/* A ragged batch of independent circuits, each one trajectory of the shot
+ * semantics above.  Items of up to 16 qubits run resident in shared memory,
+ * grouped into one persistent launch per cluster span (1, 2, 4, 8 CTAs),
+ * costliest first from a device work queue; larger items run on the HBM
+ * engine (dq_run, DQ_SEM_SHOTS, DQ_EXEC_FUSED) one after another.  Outputs go
+ * to the caller's host buffers: the classical bits and, when state_out is
+ * non-NULL, the final 2^n complex128 amplitudes. */
+typedef struct dq_batch_item {
+  uint32_t n;
+  uint32_t reserved;
+  const dq_inst* prog;
+  uint64_t ninst;
+  const dq_cond* conds;
+  uint64_t nconds;
+  uint64_t seed;          /* ChaCha8Rng::seed_from_u64(seed) for its outcomes */
+  int32_t* cbits_out;     /* ncbits entries, or NULL when ncbits == 0 */
+  uint64_t ncbits;
+  double* state_out;      /* 2^n interleaved complex128, or NULL */
+} dq_batch_item;
+
+DQ_API int dq_run_batch(int device, const dq_batch_item* items, uint64_t nitems,
+                        const dq_traj_opts* opts, dq_traj_stats* stats);
+
 /* ---- observables and adjoint differentiation --------------------------------
  * No counterpart in the reference engine (it has no gradients); the
  * observable convention matches its state layout (qubit q = bit q).
