@@ -282,6 +282,8 @@ def main():
     ap.add_argument("--workload", default="qft30")
     ap.add_argument("--exec", default=None, choices=[None, "fused", "per_gate"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the trajectory-batch and adjoint-gradient sections")
     args = ap.parse_args()
 
     from dqsim_bosonic_b200.circuit import decode_circuit_json, encode
@@ -408,6 +410,10 @@ def main():
         "gpu_launches": int(launches),
         "clocks": clk.summary(),
     }
+    if not args.no_extras:
+        line["trajectories"] = trajectory_section(dev, cpu=d.rank == 0 and d.world == 1
+                                                  and not args.no_cpu_baseline)
+        line["adjoint"] = adjoint_section(dev)
     if d.rank == 0 and d.world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         b, t, desc = cpu_sample_time(prog, threads, 20.0)
@@ -417,6 +423,134 @@ def main():
     if d.rank == 0:
         print(json.dumps(line), flush=True)
     d.close()
+
+
+def trajectory_section(dev: int, cpu: bool) -> dict:
+    """4096 shots of the 16-qubit trajectory workload (12 layers of u3 + cx
+    brickwork, measure / conditional x / reset after every third layer) in one
+    persistent launch replayed from a CUDA graph, against per-shot launches of
+    the plain per-gate kernels on the same GPU and the oracle on the host."""
+    from dqsim_bosonic_b200 import StatevectorSimulator
+    from dqsim_bosonic_b200 import _native as nat
+    from dqsim_bosonic_b200.batch import TrajectoryPlan, TrajectoryTuner
+    from dqsim_bosonic_b200.circuit import decode_circuit_json, encode
+    from dqsim_bosonic_b200.statevector import run_program
+
+    shots, base_seed = 4096, 7
+    circ = _circuits.trajectory_circuit(16, 12, seed=7)
+    prog = encode(decode_circuit_json(circ.model_dump_json()))
+    tuner = TrajectoryTuner(trial_shots=512)
+    opts = tuner.choose(prog, dev)
+    plan = TrajectoryPlan(prog, shots, dev, opts=opts)
+    for _ in range(2):
+        plan.run(base_seed)
+    ms = []
+    for _ in range(5):
+        bits, st = plan.run(base_seed)
+        ms.append(st.kernel_ms)
+    kernel_ms = float(np.median(ms))
+    # per-shot launches of the exact per-gate kernels (HBM-resident state)
+    state = nat.State(16, dev)
+    k = 16
+    run_program(state, prog, base_seed, nat.SEM_SHOTS, nat.EXEC_PER_GATE)
+    t0 = time.perf_counter()
+    for i in range(k):
+        state.reset()
+        run_program(state, prog, base_seed + i, nat.SEM_SHOTS, nat.EXEC_PER_GATE)
+    per_shot_ms = (time.perf_counter() - t0) * 1e3 / k
+    state.release()
+    # e2e through the public API (JSON circuit in, counts out)
+    sim = StatevectorSimulator(seed=base_seed, device=dev)
+    sim.simulate_shots(circ, shots)
+    t0 = time.perf_counter()
+    sim.simulate_shots(circ, shots)
+    e2e_ms = (time.perf_counter() - t0) * 1e3
+    out = {
+        "workload": "4096 shots x 16 qubits, 12 layers u3+cx brickwork, measure/cond-x/reset "
+                    "every 3rd layer (base_seed 7)",
+        "kernel_ms": kernel_ms,
+        "shots_per_s": shots / (kernel_ms * 1e-3),
+        "e2e_ms": e2e_ms,
+        "e2e_path": "StatevectorSimulator.simulate_shots(circuit, 4096)",
+        "per_shot_launches_ms": per_shot_ms * shots,
+        "per_shot_launches_note": f"plain per-gate kernels, one shot at a time; {k} shots timed, x{shots // k}",
+        "speedup_vs_per_shot_launches": per_shot_ms * shots / kernel_ms,
+        "geometry": {"threads": int(opts.threads or 256), "local_bits": int(st.local_bits),
+                     "cluster_span": int(st.cluster_span), "clusters": int(st.clusters)},
+        "boundary_draws": int(st.boundary_draws),
+        "hbm_bytes": 0,
+    }
+    if cpu:
+        import _oracle as orc
+
+        threads = os.cpu_count() or 1
+        orc.set_threads(threads)
+        m = 256
+        t0 = time.perf_counter()
+        want, rc, _ = orc.run_shots(prog, base_seed, m)
+        cpu_s = time.perf_counter() - t0
+        orc.set_threads(1)
+        bad = int(np.sum(np.any(bits[:m] != want, axis=1)))
+        out["cpu_baseline"] = {"shots_per_s": m / cpu_s, "cores": threads, "kind": "port",
+                               "sample": f"{m} shots on the oracle (sequential per shot)"}
+        out["parity"] = {"shots_checked": m, "mismatches": bad,
+                         "allowed_boundary_draws": int(st.boundary_draws)}
+    plan.release()
+    return out
+
+
+def adjoint_section(dev: int) -> dict:
+    """24-qubit hardware-efficient ansatz, 16 layers (1152 parameters),
+    H = sum a_i Z_i Z_{i+1} + sum b_i X_i: adjoint gradient vs GPU parameter
+    shift (2 forward runs per parameter with the plain per-gate kernels)."""
+    from dqsim_bosonic_b200.adjoint import adjoint_gradient, expectation, parameter_shift_gradient
+
+    c, theta, H = _circuits.hea_param_circuit(24, 16, seed=1)
+    adjoint_gradient(c, theta, H, device=dev)
+    reps, times, tms = 3, [], []
+    for _ in range(reps):
+        tm = {}
+        t0 = time.perf_counter()
+        e, g = adjoint_gradient(c, theta, H, device=dev, timing=tm)
+        times.append(time.perf_counter() - t0)
+        tms.append(tm)
+    t_adj = float(np.median(times))
+    tm = tms[int(np.argsort(times)[len(times) // 2])]
+    fwd = {}
+    for ex in ("per_gate", "fused"):
+        expectation(c, theta, H, device=dev, exec=ex)
+        t0 = time.perf_counter()
+        for _ in range(2):
+            expectation(c, theta, H, device=dev, exec=ex)
+        fwd[ex] = (time.perf_counter() - t0) / 2
+    P = theta.size
+    sub = list(range(0, P, P // 8))[:8]
+    ps = parameter_shift_gradient(c, theta, H, device=dev, exec="per_gate", occurrences=sub)
+    err = float(np.max(np.abs(g[sub] - ps[sub])))
+    n = c.num_qubits
+    back_bytes = len(c.ops) * 64.0 * 2 ** n
+    peak, src = peak_hbm()
+    achieved = back_bytes / (tm["backward_ms"] * 1e-3) / 1e9
+    ps_s = 2 * P * fwd["per_gate"]
+    return {
+        "workload": "hea24: 16 layers (ry, rz on all qubits, rzz ring), 1152 params; "
+                    "H = sum a_i Z_i Z_i+1 + sum b_i X_i",
+        "ms_per_gradient": t_adj * 1e3,
+        "grads_per_s": 1.0 / t_adj,
+        "phases_ms": tm,
+        "expval": e,
+        "param_shift_ms_per_gradient": ps_s * 1e3,
+        "param_shift_note": "2 x 1152 forward runs (plain per-gate kernels) + <H>; forward timed, x2P",
+        "speedup_vs_param_shift": ps_s / t_adj,
+        "param_shift_fused_forward_ms_per_gradient": 2 * P * fwd["fused"] * 1e3,
+        "speedup_vs_fused_param_shift": 2 * P * fwd["fused"] / t_adj,
+        "max_abs_diff_vs_param_shift": err,
+        "params_checked": len(sub),
+        "backward_roofline": {"kernel": "k_adj_1q / k_adj_2q (per gate, psi and lambda)",
+                              "bound": "hbm", "bytes": back_bytes, "achieved": achieved,
+                              "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                              "peak_source": src},
+    }
 
 
 def dominant_kernel_roofline(st, prog, exec_mode, stream, dev):

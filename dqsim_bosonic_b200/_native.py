@@ -179,11 +179,15 @@ SIGNATURES = [
     ("dq_run_trajectories", ctypes.c_int, [ctypes.c_int, _U32, _P, _U64, _P, _U64, _U64, _U64,
                                            _U64, _P, _U64, ctypes.POINTER(TrajOpts),
                                            ctypes.POINTER(TrajStats)]),
+    ("dq_traj_plan_create", ctypes.c_int, [ctypes.c_int, _U32, _P, _U64, _P, _U64, _U64, _U64,
+                                           ctypes.POINTER(TrajOpts), ctypes.POINTER(_P)]),
+    ("dq_traj_plan_run", ctypes.c_int, [_P, _U64, _P, ctypes.POINTER(TrajStats)]),
+    ("dq_traj_plan_destroy", ctypes.c_int, [_P]),
     ("dq_run_batch", ctypes.c_int, [ctypes.c_int, _P, _U64, ctypes.POINTER(TrajOpts),
                                     ctypes.POINTER(TrajStats)]),
     ("dq_expval_pauli", ctypes.c_int, [_P, _P, _U64, _DP]),
     ("dq_adjoint", ctypes.c_int, [_P, _P, _U64, _P, _U64, _P, _U64, ctypes.POINTER(RunOpts), _DP,
-                                  _P]),
+                                  _P, _P]),
     ("dq_debug_plan", ctypes.c_int, [_U32, _P, _U64, ctypes.POINTER(RunOpts), _P, _U64,
                                      ctypes.POINTER(_U64)]),
     ("dq_rng_f64", ctypes.c_int, [_U64, _U64, _U64, _P]),

@@ -22,6 +22,8 @@ from __future__ import annotations
 import ctypes
 import math
 import re
+import threading
+from concurrent.futures import ThreadPoolExecutor
 from dataclasses import dataclass
 
 import numpy as np
@@ -34,6 +36,7 @@ __all__ = [
     "ParamCircuit",
     "expectation",
     "adjoint_gradient",
+    "adjoint_gradient_batch",
     "parameter_shift_gradient",
     "AdjointExpectation",
     "expval",
@@ -247,15 +250,19 @@ class ParamCircuit:
 
 # ---- engine calls ------------------------------------------------------------------------------
 
-_states: dict[tuple[int, int], nat.State] = {}
+_states: dict[tuple[int, int, int], nat.State] = {}
+_states_lock = threading.Lock()
 
 
-def _state(n: int, device: int) -> nat.State:
-    st = _states.get((n, device))
-    if st is None:
-        st = nat.State(n, device)
-        _states[(n, device)] = st
-    return st
+def _state(n: int, device: int, slot: int = 0) -> nat.State:
+    """A cached engine state per (qubits, device, worker slot)."""
+    key = (n, device, slot)
+    with _states_lock:
+        st = _states.get(key)
+        if st is None:
+            st = nat.State(n, device)
+            _states[key] = st
+        return st
 
 
 def _exec_mode(exec: str) -> int:
@@ -294,25 +301,64 @@ def _forward_expval(n, insts, terms, device, mode) -> float:
 
 
 def adjoint_gradient(circuit: ParamCircuit, theta, observable: PauliSum, *, device: int = 0,
-                     exec: str = "fused") -> tuple[float, np.ndarray]:
-    """``(E, dE/dtheta)`` from one forward and one adjoint (reverse) pass."""
+                     exec: str = "fused", timing: dict | None = None,
+                     _slot: int = 0) -> tuple[float, np.ndarray]:
+    """``(E, dE/dtheta)`` from one forward and one adjoint (reverse) pass.
+
+    ``timing``: a dict that receives the device milliseconds of the forward
+    pass, of lambda = H psi and of the backward pass."""
     terms = _check_observable(circuit, observable)
     th = np.asarray(theta, dtype=np.float64).reshape(-1)
     insts = circuit.bind(th)
     occ = circuit.occurrences()
     slots = circuit.param_slots()
-    st = _state(circuit.num_qubits, device)
+    st = _state(circuit.num_qubits, device, _slot)
     st.reset()
     opts = nat.RunOpts(nat.SEM_SIMULATE, _exec_mode(exec), 0, 0, 0, 0)
     e = ctypes.c_double(0.0)
     g_occ = np.zeros(max(1, len(occ)), dtype=np.float64)
+    phases = np.zeros(3, dtype=np.float64)
     nat.check(nat.lib().dq_adjoint(st.handle, nat.ptr(insts), len(insts), nat.ptr(slots), len(occ),
                                    nat.ptr(terms), len(terms), ctypes.byref(opts), ctypes.byref(e),
-                                   nat.ptr(g_occ)), "dq_adjoint")
+                                   nat.ptr(g_occ), nat.ptr(phases) if timing is not None else None),
+              "dq_adjoint")
+    if timing is not None:
+        timing.update(forward_ms=float(phases[0]), observable_ms=float(phases[1]),
+                      backward_ms=float(phases[2]))
     grad = np.zeros(circuit.num_params, dtype=np.float64)
     for o, (_, _, p) in enumerate(occ):
         grad[p.index] += p.scale * g_occ[o]
     return e.value, grad
+
+
+def adjoint_gradient_batch(circuit: ParamCircuit, thetas, observable: PauliSum, *,
+                           device: int = 0, exec: str = "fused", workers: int = 4):
+    """``(E[B], dE/dtheta[B, P])`` for a batch of parameter sets.
+
+    Each set runs the adjoint pass on its own engine state; ``workers`` sets
+    are in flight at once on separate CUDA streams (one host thread each; the
+    engine calls release the GIL), which keeps the GPU busy when one set's
+    state is small enough to be launch-bound."""
+    th = np.asarray(thetas, dtype=np.float64)
+    if th.ndim != 2:
+        raise ValueError("thetas must be 2-D: (sets, parameters)")
+    B = th.shape[0]
+    es = np.empty(B)
+    gs = np.empty((B, circuit.num_params))
+    workers = max(1, min(int(workers), B))
+
+    def run(w):
+        for b in range(w, B, workers):
+            es[b], gs[b] = adjoint_gradient(circuit, th[b], observable, device=device, exec=exec,
+                                            _slot=w)
+
+    if workers == 1:
+        run(0)
+    else:
+        with ThreadPoolExecutor(max_workers=workers) as ex:
+            for f in [ex.submit(run, w) for w in range(workers)]:
+                f.result()
+    return es, gs
 
 
 # shift rules: (coefficient, shift) pairs; df/dx = sum c * f(x + s)
@@ -384,15 +430,12 @@ class AdjointExpectation:
 
             class _Fn(torch.autograd.Function):
                 @staticmethod
-                def forward(ctx, theta, circuit, observable, device, exec):
+                def forward(ctx, theta, circuit, observable, device, exec, workers):
                     th = theta.detach().to("cpu", torch.float64).numpy()
                     batched = th.ndim == 2
                     rows = th if batched else th[None, :]
-                    es = np.empty(rows.shape[0])
-                    gs = np.empty(rows.shape)
-                    for b in range(rows.shape[0]):
-                        es[b], gs[b] = adjoint_gradient(circuit, rows[b], observable,
-                                                        device=device, exec=exec)
+                    es, gs = adjoint_gradient_batch(circuit, rows, observable, device=device,
+                                                    exec=exec, workers=workers)
                     grad = torch.from_numpy(gs if batched else gs[0]).to(theta.device, theta.dtype)
                     ctx.save_for_backward(grad)
                     ctx.batched = batched
@@ -404,13 +447,14 @@ class AdjointExpectation:
                 def backward(ctx, grad_out):
                     (grad,) = ctx.saved_tensors
                     g = grad_out.unsqueeze(-1) * grad if ctx.batched else grad_out * grad
-                    return g, None, None, None, None
+                    return g, None, None, None, None, None
 
             cls._fn = _Fn
         return cls._fn
 
 
 def expval(theta, circuit: ParamCircuit, observable: PauliSum, *, device: int = 0,
-           exec: str = "fused"):
-    """Differentiable ``<H>`` (torch tensor in, torch tensor out)."""
-    return AdjointExpectation.function().apply(theta, circuit, observable, device, exec)
+           exec: str = "fused", workers: int = 4):
+    """Differentiable ``<H>`` (torch tensor in, torch tensor out); a 2-D
+    ``theta`` is a batch of parameter sets run ``workers`` at a time."""
+    return AdjointExpectation.function().apply(theta, circuit, observable, device, exec, workers)

@@ -9,6 +9,8 @@
   programs run shot by shot on the HBM engine (``dq_run``).
 * :func:`run_batch` — a ragged batch of independent circuits, one trajectory
   each (``dq_run_batch``), optionally returning every final state.
+* :class:`TrajectoryPlan` — a shot batch captured once as a CUDA graph and
+  replayed with new seeds.
 * :class:`TrajectoryTuner` — picks the launch geometry (threads per CTA,
   amplitudes per CTA, cluster span) by timing the candidates once per program
   shape.
@@ -111,6 +113,47 @@ def run_batch(progs, seeds, device: int = 0, *, want_states: bool = False, opts=
     nat.check(nat.lib().dq_run_batch(int(device), ctypes.addressof(items), len(progs),
                                      ctypes.byref(o), ctypes.byref(st)), "dq_run_batch")
     return cbits, (states if want_states else None), st
+
+
+class TrajectoryPlan:
+    """A shot batch of one program captured as a CUDA graph and replayed.
+
+    ``run(base_seed)`` replays the graph (seed upload, counter reset, the
+    persistent launch, result copies) and returns (cbits, TrajStats) for shots
+    ``base_seed + s``, s < shots."""
+
+    def __init__(self, prog, shots: int, device: int = 0, *, opts=None):
+        self.prog = prog
+        self.shots = int(shots)
+        self.device = int(device)
+        h = ctypes.c_void_p()
+        o = opts if opts is not None else _opts()
+        nat.check(nat.lib().dq_traj_plan_create(
+            self.device, prog.num_qubits, nat.ptr(prog.insts), prog.ninst,
+            nat.ptr(prog.conds) if prog.conds.size else None, prog.conds.size, self.shots,
+            prog.cbit_space, ctypes.byref(o), ctypes.byref(h)), "dq_traj_plan_create")
+        self._h = h
+
+    def run(self, base_seed: int):
+        if self._h is None:
+            raise ValueError("plan was released")
+        out = np.empty((self.shots, self.prog.cbit_space), dtype=np.int32)
+        st = nat.TrajStats()
+        nat.check(nat.lib().dq_traj_plan_run(self._h, base_seed & _U64,
+                                             nat.ptr(out) if out.size else None,
+                                             ctypes.byref(st)), "dq_traj_plan_run")
+        return out, st
+
+    def release(self) -> None:
+        if getattr(self, "_h", None) is not None:
+            nat.lib().dq_traj_plan_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.release()
+        except Exception:
+            pass
 
 
 class TrajectoryTuner:

@@ -493,7 +493,7 @@ int dq_expval_pauli(dq_state_t h, const dq_pauli_term* terms, uint64_t nterms, d
 
 int dq_adjoint(dq_state_t h, const dq_inst* prog, uint64_t ninst, const int32_t* param_index,
                uint64_t nparams, const dq_pauli_term* terms, uint64_t nterms,
-               const dq_run_opts* opts, double* expval, double* grad) {
+               const dq_run_opts* opts, double* expval, double* grad, double* phase_ms) {
   DQ_TRY(check_handle(h));
   if (!expval || (nparams && !grad)) return fail(DQ_ERR_INVALID_ARG, "null output");
   uint64_t nslots = 0;
@@ -505,10 +505,25 @@ int dq_adjoint(dq_state_t h, const dq_inst* prog, uint64_t ninst, const int32_t*
     return fail(DQ_ERR_INVALID_ARG, "dq_adjoint runs with DQ_SEM_SIMULATE semantics");
   o.profile = 0;
   DeviceGuard g(h->device);
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  if (phase_ms)
+    for (auto& e : ev) DQ_CUDA_TRY(cudaEventCreate(&e));
+  struct EvGuard {
+    cudaEvent_t* e;
+    ~EvGuard() {
+      for (int i = 0; i < 4; ++i)
+        if (e[i]) cudaEventDestroy(e[i]);
+    }
+  } evg{ev};
+  auto mark = [&](int i) {
+    if (ev[i]) cudaEventRecord(ev[i], h->stream);
+  };
 
   // forward pass
+  mark(0);
   DQ_TRY(dq_run(h, prog, ninst, nullptr, 0, 0, nullptr, 0, &o, nullptr));
   DQ_TRY(canonicalize(h));
+  mark(1);
 
   DeviceTerms t;
   DQ_TRY(upload_terms(terms, nterms, h->n, h->stream, &t));
@@ -521,6 +536,7 @@ int dq_adjoint(dq_state_t h, const dq_inst* prog, uint64_t ninst, const int32_t*
     if (e != cudaSuccess) rc = fail(DQ_ERR_OOM, std::string("cudaMallocAsync: ") + cudaGetErrorString(e));
   }
   if (rc == DQ_OK) rc = launch_pauli(h, lam, t, slots + nslots);
+  mark(2);
 
   // backward pass: slots are numbered in program order
   uint64_t slot = nslots;
@@ -559,6 +575,7 @@ int dq_adjoint(dq_state_t h, const dq_inst* prog, uint64_t ninst, const int32_t*
     }
   }
 
+  mark(3);
   std::vector<double> host(nslots + 1, 0.0);
   if (rc == DQ_OK) {
     cudaError_t e = cudaMemcpyAsync(host.data(), slots, sizeof(double) * (nslots + 1),
@@ -573,6 +590,12 @@ int dq_adjoint(dq_state_t h, const dq_inst* prog, uint64_t ninst, const int32_t*
     cache_free(h->device, h->bytes, lam);
   }
   DQ_TRY(rc);
+  if (phase_ms)
+    for (int i = 0; i < 3; ++i) {
+      float ms = 0.f;
+      DQ_CUDA_TRY(cudaEventElapsedTime(&ms, ev[i], ev[i + 1]));
+      phase_ms[i] = ms;
+    }
   *expval = host[nslots];
   for (uint64_t p = 0; p < nparams; ++p) grad[p] = 0.0;
   uint64_t s = 0;

@@ -31,6 +31,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -1214,22 +1215,28 @@ int launch_sweep_rb(double2* amp, uint32_t n, const uint8_t* dblob, uint32_t pro
   constexpr int M = TB + RB;
   const size_t smem_max = sizeof(double2) * (2 * (1u << M) + kMaxSlots) + max_prog(TB);
   const size_t smem = sizeof(double2) * (2 * (1u << M) + kMaxSlots) + prog_bytes;
-  static uint64_t attr_done = 0;  // one bit per device
-  static int per_sm[64];
+  // per device, once: opt-in shared memory and resident CTAs per SM (the
+  // mutex makes the first launches from concurrent host threads safe)
+  static std::mutex mu;
+  static int per_sm[64];  // 0 = not yet configured
   int dev = 0;
   DQ_CUDA_TRY(cudaGetDevice(&dev));
-  if (!((attr_done >> (dev & 63)) & 1ULL)) {
-    DQ_CUDA_TRY(cudaFuncSetAttribute(k_sweep<TB, RB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)smem_max));
-    int b = 1;
-    DQ_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_sweep<TB, RB>, 1 << TB, smem_max));
-    per_sm[dev & 63] = b < 1 ? 1 : b;
-    attr_done |= 1ULL << (dev & 63);
+  int resident;
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    if (per_sm[dev & 63] == 0) {
+      DQ_CUDA_TRY(cudaFuncSetAttribute(k_sweep<TB, RB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem_max));
+      int b = 1;
+      DQ_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_sweep<TB, RB>, 1 << TB, smem_max));
+      per_sm[dev & 63] = b < 1 ? 1 : b;
+    }
+    resident = per_sm[dev & 63];
   }
   int sms = 148;
   DQ_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
   const uint64_t tiles = 1ULL << (n - M);
-  const unsigned grid = (unsigned)std::min<uint64_t>(tiles, (uint64_t)sms * per_sm[dev & 63]);
+  const unsigned grid = (unsigned)std::min<uint64_t>(tiles, (uint64_t)sms * resident);
   k_sweep<TB, RB><<<grid, 1 << TB, smem, st>>>(amp, dblob, prog_bytes, (uint32_t)tiles);
   DQ_CUDA_TRY(cudaGetLastError());
   return DQ_OK;
@@ -1340,13 +1347,17 @@ int materialize_perm(double2* amp, uint32_t n, uint32_t* perm, cudaStream_t st, 
     }
     for (uint32_t k = 0; k < P.m; ++k) P.tauL[k] = (uint32_t)li[tau[P.L[k]]];
     const size_t smem = sizeof(double2) * 2 * ((1u << P.m) + ((1u << P.m) >> 4));
+    static std::mutex mu;
     static uint64_t attr_done = 0;  // one bit per device
     int dev = 0;
     DQ_CUDA_TRY(cudaGetDevice(&dev));
-    if (!((attr_done >> (dev & 63)) & 1ULL)) {
-      DQ_CUDA_TRY(cudaFuncSetAttribute(k_permute_pairs, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)(sizeof(double2) * 2 * (4096 + 256))));
-      attr_done |= 1ULL << (dev & 63);
+    {
+      std::lock_guard<std::mutex> lk(mu);
+      if (!((attr_done >> (dev & 63)) & 1ULL)) {
+        DQ_CUDA_TRY(cudaFuncSetAttribute(k_permute_pairs, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)(sizeof(double2) * 2 * (4096 + 256))));
+        attr_done |= 1ULL << (dev & 63);
+      }
     }
     const uint64_t tiles = 1ULL << (n - P.m);
     k_permute_pairs<<<(unsigned)tiles, 256, smem, st>>>(amp, P);

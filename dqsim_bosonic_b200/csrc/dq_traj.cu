@@ -610,37 +610,62 @@ int add_program(LaunchSet& ls, const dq_inst* prog, uint64_t ninst, const dq_con
   return DQ_OK;
 }
 
-template <int THREADS>
-int launch_traj(const TrajParams& P, uint32_t C, size_t smem, int device, cudaStream_t st,
-                uint32_t* clusters_out) {
-  DQ_CUDA_TRY(cudaFuncSetAttribute(k_traj<THREADS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   (int)smem));
+// Launch geometry of k_traj: opt-in shared memory, cluster dimension and as
+// many clusters as can be resident at once (capped by the item count).
+struct TrajLaunch {
   cudaLaunchConfig_t cfg{};
   cudaLaunchAttribute attr[1];
-  attr[0].id = cudaLaunchAttributeClusterDimension;
-  attr[0].val.clusterDim.x = C;
-  attr[0].val.clusterDim.y = 1;
-  attr[0].val.clusterDim.z = 1;
-  cfg.blockDim = dim3(THREADS, 1, 1);
-  cfg.dynamicSmemBytes = smem;
-  cfg.stream = st;
-  cfg.attrs = attr;
-  cfg.numAttrs = 1;
+  int threads = 256;
+  uint32_t clusters = 0;
+};
+
+template <int THREADS>
+int config_traj_t(uint32_t C, size_t smem, uint64_t nitems, TrajLaunch* L) {
+  DQ_CUDA_TRY(cudaFuncSetAttribute(k_traj<THREADS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)smem));
+  L->attr[0].id = cudaLaunchAttributeClusterDimension;
+  L->attr[0].val.clusterDim.x = C;
+  L->attr[0].val.clusterDim.y = 1;
+  L->attr[0].val.clusterDim.z = 1;
+  L->cfg.blockDim = dim3(THREADS, 1, 1);
+  L->cfg.dynamicSmemBytes = smem;
+  L->cfg.attrs = L->attr;
+  L->cfg.numAttrs = 1;
+  L->cfg.gridDim = dim3(C, 1, 1);
   int max_clusters = 0;
-  cfg.gridDim = dim3(C, 1, 1);
-  cudaError_t e = cudaOccupancyMaxActiveClusters(&max_clusters, (void*)k_traj<THREADS>, &cfg);
+  cudaError_t e = cudaOccupancyMaxActiveClusters(&max_clusters, (void*)k_traj<THREADS>, &L->cfg);
   if (e != cudaSuccess || max_clusters < 1) {
     cudaGetLastError();
     return fail(DQ_ERR_UNSUPPORTED, std::string("trajectory kernel does not fit: cluster of ") +
                                         std::to_string(C) + " CTAs x " + std::to_string(smem) +
                                         " B shared memory");
   }
-  uint64_t ncl = std::min<uint64_t>((uint64_t)max_clusters, P.nitems);
+  uint64_t ncl = std::min<uint64_t>((uint64_t)max_clusters, nitems);
   if (ncl < 1) ncl = 1;
-  cfg.gridDim = dim3((unsigned)(ncl * C), 1, 1);
-  DQ_CUDA_TRY(cudaLaunchKernelEx(&cfg, k_traj<THREADS>, P));
-  *clusters_out = (uint32_t)ncl;
+  L->cfg.gridDim = dim3((unsigned)(ncl * C), 1, 1);
+  L->threads = THREADS;
+  L->clusters = (uint32_t)ncl;
   return DQ_OK;
+}
+
+int config_traj(int threads, uint32_t C, size_t smem, uint64_t nitems, TrajLaunch* L) {
+  if (threads == 128) return config_traj_t<128>(C, smem, nitems, L);
+  if (threads == 256) return config_traj_t<256>(C, smem, nitems, L);
+  return config_traj_t<512>(C, smem, nitems, L);
+}
+
+int launch_traj(TrajLaunch& L, const TrajParams& P, cudaStream_t st) {
+  L.cfg.stream = st;
+  L.cfg.attrs = L.attr;
+  if (L.threads == 128) DQ_CUDA_TRY(cudaLaunchKernelEx(&L.cfg, k_traj<128>, P));
+  else if (L.threads == 256) DQ_CUDA_TRY(cudaLaunchKernelEx(&L.cfg, k_traj<256>, P));
+  else DQ_CUDA_TRY(cudaLaunchKernelEx(&L.cfg, k_traj<512>, P));
+  return DQ_OK;
+}
+
+size_t traj_smem(const LaunchSet& ls) {
+  return sizeof(double2) * (1u << ls.max_lb) + sizeof(double) * 48 +
+         sizeof(int32_t) * std::max<uint32_t>(ls.max_ncbits, 1);
 }
 
 // Device buffers of one launch, freed on scope exit.
@@ -653,6 +678,7 @@ struct LaunchBuffers {
   unsigned long long* ctr = nullptr;  // [0] queue, [1] boundary, [2] failed
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   cudaStream_t st = nullptr;
+  bool own_st = false;  // destroy st with the buffers
   ~LaunchBuffers() {
     if (st) cudaStreamSynchronize(st);
     if (ops) cudaFree(ops);
@@ -663,6 +689,7 @@ struct LaunchBuffers {
     if (ctr) cudaFree(ctr);
     if (e0) cudaEventDestroy(e0);
     if (e1) cudaEventDestroy(e1);
+    if (own_st && st) cudaStreamDestroy(st);
   }
 };
 
@@ -703,13 +730,12 @@ int run_launch(LaunchSet& ls, int threads, int device, cudaStream_t st, int32_t*
   P.boundary = b.ctr + 1;
   P.failed = reinterpret_cast<long long*>(b.ctr + 2);
   P.nitems = ls.items.size();
-  const size_t smem = sizeof(double2) * (1u << ls.max_lb) + sizeof(double) * 48 +
-                      sizeof(int32_t) * std::max<uint32_t>(ls.max_ncbits, 1);
-  uint32_t clusters = 0;
+  (void)device;
+  TrajLaunch L;
+  DQ_TRY(config_traj(threads, ls.C, traj_smem(ls), P.nitems, &L));
+  const uint32_t clusters = L.clusters;
   DQ_CUDA_TRY(cudaEventRecord(b.e0, st));
-  if (threads == 128) DQ_TRY(launch_traj<128>(P, ls.C, smem, device, st, &clusters));
-  else if (threads == 256) DQ_TRY(launch_traj<256>(P, ls.C, smem, device, st, &clusters));
-  else DQ_TRY(launch_traj<512>(P, ls.C, smem, device, st, &clusters));
+  DQ_TRY(launch_traj(L, P, st));
   DQ_CUDA_TRY(cudaEventRecord(b.e1, st));
   unsigned long long ctr[3];
   DQ_CUDA_TRY(cudaMemcpyAsync(ctr, b.ctr, sizeof(ctr), cudaMemcpyDeviceToHost, st));
@@ -769,6 +795,32 @@ void init_stats(dq_traj_stats* s) {
 
 }  // namespace
 }  // namespace dq
+
+// A trajectory batch captured once as a CUDA graph (seed upload, counter
+// reset, the persistent launch, result copies) and replayed per call.
+struct dq_traj_plan_s {
+  int device = 0;
+  uint64_t shots = 0, ncbits = 0;
+  dq::LaunchBuffers buf;
+  int32_t* d_cbits = nullptr;
+  int32_t* h_cbits = nullptr;            // pinned
+  uint64_t* h_seed = nullptr;            // pinned: base seed of the next replay
+  unsigned long long* h_ctr = nullptr;   // pinned: [0..3) initial, [3..6) results
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  dq::TrajLaunch L;
+  dq::TrajParams P{};
+  dq_traj_stats geom{};
+  ~dq_traj_plan_s() {
+    if (buf.st) cudaStreamSynchronize(buf.st);
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    if (d_cbits) cudaFree(d_cbits);
+    if (h_cbits) cudaFreeHost(h_cbits);
+    if (h_seed) cudaFreeHost(h_seed);
+    if (h_ctr) cudaFreeHost(h_ctr);
+  }
+};
 
 using namespace dq;
 
@@ -964,6 +1016,143 @@ int dq_run_batch(int device, const dq_batch_item* items, uint64_t nitems,
   cudaStreamDestroy(st);
   if (stats) *stats = acc;
   return rc;
+}
+
+int dq_traj_plan_create(int device, uint32_t n, const dq_inst* prog, uint64_t ninst,
+                        const dq_cond* conds, uint64_t nconds, uint64_t shots, uint64_t ncbits,
+                        const dq_traj_opts* opts, dq_traj_plan_t* out) {
+  if (!out) return fail(DQ_ERR_INVALID_ARG, "null output plan");
+  *out = nullptr;
+  if (n < 1 || n > kTrajMaxQubits) return fail(DQ_ERR_INVALID_ARG, "plan: n must be in 1..16");
+  if (ninst && !prog) return fail(DQ_ERR_INVALID_ARG, "null program");
+  if (ncbits > kTrajMaxCbits) return fail(DQ_ERR_INVALID_ARG, "at most 1024 classical bits");
+  if (shots < 1 || shots > (1ULL << 40)) return fail(DQ_ERR_INVALID_ARG, "shots must be in 1..2^40");
+  for (uint64_t i = 0; i < ninst; ++i) DQ_TRY(validate_inst(prog[i], n, nconds, ncbits, conds, i));
+  int threads;
+  uint32_t max_span, force_lb, lb, C;
+  DQ_TRY(check_opts(opts, &threads, &max_span, &force_lb));
+  DQ_TRY(geometry(n, max_span, force_lb, &lb, &C));
+  LaunchSet ls;
+  ls.C = C;
+  DQ_TRY(add_program(ls, prog, ninst, conds, nconds, n, lb, 0, 0, (uint32_t)ncbits, nullptr));
+  ls.items.resize(shots);
+  for (uint64_t s = 0; s < shots; ++s) ls.items[s] = TItem{0, 0, s};
+  if (ls.enc.pool.empty()) ls.enc.pool.push_back(make_double2(0, 0));
+
+  DeviceGuard g(device);
+  dq_traj_plan_t p = new (std::nothrow) dq_traj_plan_s();
+  if (!p) return fail(DQ_ERR_OOM, "host allocation failed");
+  p->device = device;
+  p->shots = shots;
+  p->ncbits = ncbits;
+  auto bail = [&](int rc) {
+    delete p;
+    return rc;
+  };
+  const size_t out_bytes = sizeof(int32_t) * (size_t)shots * ncbits;
+  int rc = DQ_OK;
+  auto cu = [&](cudaError_t e, const char* what) {
+    if (e != cudaSuccess && rc == DQ_OK) {
+      cudaGetLastError();
+      rc = fail(e == cudaErrorMemoryAllocation ? DQ_ERR_OOM : DQ_ERR_CUDA,
+                std::string(what) + ": " + cudaGetErrorString(e));
+    }
+  };
+  cu(cudaStreamCreateWithFlags(&p->buf.st, cudaStreamNonBlocking), "cudaStreamCreate");
+  if (rc != DQ_OK) return bail(rc);
+  p->buf.own_st = true;
+  cudaStream_t st = p->buf.st;
+  if ((rc = upload(&p->buf.ops, ls.enc.ops, st)) != DQ_OK) return bail(rc);
+  if ((rc = upload(&p->buf.pool, ls.enc.pool, st)) != DQ_OK) return bail(rc);
+  if ((rc = upload(&p->buf.conds, ls.conds, st)) != DQ_OK) return bail(rc);
+  if ((rc = upload(&p->buf.progs, ls.progs, st)) != DQ_OK) return bail(rc);
+  if ((rc = upload(&p->buf.items, ls.items, st)) != DQ_OK) return bail(rc);
+  cu(cudaMalloc((void**)&p->buf.ctr, 3 * sizeof(unsigned long long)), "cudaMalloc(counters)");
+  cu(cudaMalloc((void**)&p->d_cbits, std::max<size_t>(out_bytes, 4)), "cudaMalloc(cbits)");
+  cu(cudaMallocHost((void**)&p->h_cbits, std::max<size_t>(out_bytes, 4)), "cudaMallocHost(cbits)");
+  cu(cudaMallocHost((void**)&p->h_seed, sizeof(uint64_t)), "cudaMallocHost(seed)");
+  cu(cudaMallocHost((void**)&p->h_ctr, 6 * sizeof(unsigned long long)), "cudaMallocHost(counters)");
+  cu(cudaEventCreate(&p->buf.e0), "cudaEventCreate");
+  cu(cudaEventCreate(&p->buf.e1), "cudaEventCreate");
+  if (rc != DQ_OK) return bail(rc);
+  p->h_ctr[0] = 0;
+  p->h_ctr[1] = 0;
+  p->h_ctr[2] = 0x7fffffffffffffffULL;
+  p->h_seed[0] = 0;
+  TrajParams& P = p->P;
+  P.ops = p->buf.ops;
+  P.pool = p->buf.pool;
+  P.conds = p->buf.conds;
+  P.progs = p->buf.progs;
+  P.items = p->buf.items;
+  P.cbits_out = p->d_cbits;
+  P.queue = p->buf.ctr;
+  P.boundary = p->buf.ctr + 1;
+  P.failed = reinterpret_cast<long long*>(p->buf.ctr + 2);
+  P.nitems = shots;
+  if ((rc = config_traj(threads, C, traj_smem(ls), shots, &p->L)) != DQ_OK) return bail(rc);
+  cu(cudaStreamSynchronize(st), "cudaStreamSynchronize");
+  if (rc != DQ_OK) return bail(rc);
+  // capture: seed -> program table, counters reset, launch, results back
+  cu(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
+  if (rc != DQ_OK) return bail(rc);
+  cu(cudaMemcpyAsync(&p->buf.progs[0].base_seed, p->h_seed, sizeof(uint64_t),
+                     cudaMemcpyHostToDevice, st), "capture seed copy");
+  cu(cudaMemcpyAsync(p->buf.ctr, p->h_ctr, 3 * sizeof(unsigned long long), cudaMemcpyHostToDevice,
+                     st), "capture counter reset");
+  if (rc == DQ_OK) rc = launch_traj(p->L, P, st);
+  if (out_bytes)
+    cu(cudaMemcpyAsync(p->h_cbits, p->d_cbits, out_bytes, cudaMemcpyDeviceToHost, st),
+       "capture cbits copy");
+  cu(cudaMemcpyAsync(p->h_ctr + 3, p->buf.ctr, 3 * sizeof(unsigned long long),
+                     cudaMemcpyDeviceToHost, st), "capture counter copy");
+  cudaGraph_t graph = nullptr;
+  const cudaError_t ee = cudaStreamEndCapture(st, &graph);
+  p->graph = graph;
+  cu(ee, "cudaStreamEndCapture");
+  if (rc == DQ_OK) cu(cudaGraphInstantiate(&p->exec, p->graph, 0), "cudaGraphInstantiate");
+  if (rc != DQ_OK) return bail(rc);
+  p->geom.cluster_span = C;
+  p->geom.clusters = p->L.clusters;
+  p->geom.threads = (uint32_t)threads;
+  p->geom.local_bits = lb;
+  p->geom.launches = 1;
+  *out = p;
+  return DQ_OK;
+}
+
+int dq_traj_plan_run(dq_traj_plan_t p, uint64_t base_seed, int32_t* cbits_out,
+                     dq_traj_stats* stats) {
+  if (!p || !p->exec) return fail(DQ_ERR_INVALID_ARG, "null or destroyed plan");
+  const size_t out_bytes = sizeof(int32_t) * (size_t)p->shots * p->ncbits;
+  if (out_bytes && !cbits_out) return fail(DQ_ERR_INVALID_ARG, "null cbits output");
+  DeviceGuard g(p->device);
+  cudaStream_t st = p->buf.st;
+  p->h_seed[0] = base_seed;
+  DQ_CUDA_TRY(cudaEventRecord(p->buf.e0, st));
+  DQ_CUDA_TRY(cudaGraphLaunch(p->exec, st));
+  DQ_CUDA_TRY(cudaEventRecord(p->buf.e1, st));
+  DQ_CUDA_TRY(cudaStreamSynchronize(st));
+  float ms = 0.f;
+  DQ_CUDA_TRY(cudaEventElapsedTime(&ms, p->buf.e0, p->buf.e1));
+  if (out_bytes) memcpy(cbits_out, p->h_cbits, out_bytes);
+  dq_traj_stats s = p->geom;
+  s.boundary_draws = p->h_ctr[4];
+  const long long f = (long long)p->h_ctr[5];
+  s.failed_inst = f == 0x7fffffffffffffffLL ? -1 : (f & ((1LL << 40) - 1));
+  s.kernel_ms = ms;
+  if (stats) *stats = s;
+  if (s.failed_inst >= 0)
+    return fail(DQ_ERR_UNSUPPORTED, "instruction " + std::to_string(s.failed_inst) +
+                                        ": unsupported generic gate reached in a trajectory");
+  return DQ_OK;
+}
+
+int dq_traj_plan_destroy(dq_traj_plan_t p) {
+  if (!p) return DQ_OK;
+  DeviceGuard g(p->device);
+  delete p;
+  return DQ_OK;
 }
 
 }  // extern "C"

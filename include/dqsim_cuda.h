@@ -277,6 +277,18 @@ DQ_API int dq_run_trajectories(int device, uint32_t n, const dq_inst* prog, uint
                                uint64_t shot0, uint64_t shots, int32_t* cbits_out,
                                uint64_t ncbits, const dq_traj_opts* opts, dq_traj_stats* stats);
 
+/* The same batch captured once as a CUDA graph (seed upload, counter reset,
+ * the persistent launch and the result copies) and replayed per call with a
+ * new base seed: shot s of a replay uses seed base_seed + s.  kernel_ms in
+ * the stats is the device time of the whole replay. */
+typedef struct dq_traj_plan_s* dq_traj_plan_t;
+DQ_API int dq_traj_plan_create(int device, uint32_t n, const dq_inst* prog, uint64_t ninst,
+                               const dq_cond* conds, uint64_t nconds, uint64_t shots,
+                               uint64_t ncbits, const dq_traj_opts* opts, dq_traj_plan_t* out);
+DQ_API int dq_traj_plan_run(dq_traj_plan_t plan, uint64_t base_seed, int32_t* cbits_out,
+                            dq_traj_stats* stats);
+DQ_API int dq_traj_plan_destroy(dq_traj_plan_t plan);
+
 /* A ragged batch of independent circuits, each one trajectory of the shot
  * semantics above.  Items of up to 16 qubits run resident in shared memory,
  * grouped into one persistent launch per cluster span (1, 2, 4, 8 CTAs),
@@ -326,11 +338,14 @@ DQ_API int dq_expval_pauli(dq_state_t h, const dq_pauli_term* terms, uint64_t nt
  * The backward pass walks the program in reverse, uncomputing psi with the
  * inverse gates alongside lambda = H psi (no stored intermediate states; one
  * extra state-sized buffer).  On return the handle holds psi0 again, up to
- * rounding.  param_index may be NULL when nparams == 0 (E only). */
+ * rounding.  param_index may be NULL when nparams == 0 (E only).  phase_ms,
+ * when non-NULL, receives the device time (ms) of the forward pass, of
+ * lambda = H psi, and of the backward pass. */
 DQ_API int dq_adjoint(dq_state_t h, const dq_inst* prog, uint64_t ninst,
                       const int32_t* param_index, uint64_t nparams,
                       const dq_pauli_term* terms, uint64_t nterms,
-                      const dq_run_opts* opts, double* expval, double* grad);
+                      const dq_run_opts* opts, double* expval, double* grad,
+                      double* phase_ms);
 
 /* ---- planner inspection (host only, no GPU needed) -------------------------
  * Runs the fused-sweep planner of dq_run (DQ_EXEC_FUSED) on a unitary

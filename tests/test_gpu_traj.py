@@ -13,6 +13,7 @@ import _oracle as orc
 from _circuits import JsonCircuit, cond, g
 from dqsim_bosonic_b200 import _native as nat
 from dqsim_bosonic_b200.batch import (
+    TrajectoryPlan,
     TrajectoryTuner,
     _opts,
     run_batch,
@@ -151,3 +152,16 @@ def test_rejects_bad_arguments(gpu):
         trajectories_resident(prog, 1, 4, opts=_opts(256, 1, 0))  # needs 2 CTAs
     with pytest.raises(ValueError):
         trajectories_resident(prog, 1, 4, opts=_opts(100, 0, 0))
+
+
+def test_graph_plan_replays_match(gpu):
+    prog = prog_of(_circuits.trajectory_circuit(15, 6, seed=4))
+    plan = TrajectoryPlan(prog, 96)
+    for seed in (3, 1000, 3):
+        got, st = plan.run(seed)
+        want, st2 = trajectories_resident(prog, seed, 96)
+        assert st.cluster_span == st2.cluster_span == 4
+        if st.boundary_draws == 0 and st2.boundary_draws == 0:
+            assert (got == want).all()
+        assert st.kernel_ms > 0.0
+    plan.release()
