@@ -284,6 +284,10 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the trajectory-batch and adjoint-gradient sections")
+    ap.add_argument("--adam-steps", type=int, default=2,
+                    help="timed Adam steps of the 512-set batched adjoint (0 = skip)")
+    ap.add_argument("--adjoint31", action="store_true",
+                    help="add the 31-qubit adjoint pass with its finite-difference check")
     args = ap.parse_args()
 
     from dqsim_bosonic_b200.circuit import decode_circuit_json, encode
@@ -412,8 +416,12 @@ def main():
     }
     if not args.no_extras:
         line["trajectories"] = trajectory_section(dev, cpu=d.rank == 0 and d.world == 1
-                                                  and not args.no_cpu_baseline)
+                                                  and not args.no_cpu_baseline, d=d)
         line["adjoint"] = adjoint_section(dev)
+        if args.adam_steps > 0:
+            line["adjoint_batch"] = adjoint_batch_section(dev, args.adam_steps)
+    if args.adjoint31:
+        line["adjoint31"] = adjoint31_section(dev)
     if d.rank == 0 and d.world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         b, t, desc = cpu_sample_time(prog, threads, 20.0)
@@ -425,30 +433,46 @@ def main():
     d.close()
 
 
-def trajectory_section(dev: int, cpu: bool) -> dict:
+def trajectory_section(dev: int, cpu: bool, d=None) -> dict:
     """4096 shots of the 16-qubit trajectory workload (12 layers of u3 + cx
     brickwork, measure / conditional x / reset after every third layer) in one
     persistent launch replayed from a CUDA graph, against per-shot launches of
-    the plain per-gate kernels on the same GPU and the oracle on the host."""
+    the plain per-gate kernels on the same GPU and the oracle on the host.
+    With N ranks every rank runs 4096 shots of its own slice of the global
+    shot range (weak scaling: seeds base + global shot index) and the counts
+    are merged with one all-reduce of the outcome histogram."""
     from dqsim_bosonic_b200 import StatevectorSimulator
     from dqsim_bosonic_b200 import _native as nat
     from dqsim_bosonic_b200.batch import TrajectoryPlan, TrajectoryTuner
     from dqsim_bosonic_b200.circuit import decode_circuit_json, encode
     from dqsim_bosonic_b200.statevector import run_program
 
+    from dqsim_bosonic_b200.circuit import format_cbits
+    from dqsim_bosonic_b200.dist import merge_counts, shard_range
+
+    world = d.world if d is not None else 1
+    rank = d.rank if d is not None else 0
     shots, base_seed = 4096, 7
     circ = _circuits.trajectory_circuit(16, 12, seed=7)
     prog = encode(decode_circuit_json(circ.model_dump_json()))
     tuner = TrajectoryTuner(trial_shots=512)
     opts = tuner.choose(prog, dev)
     plan = TrajectoryPlan(prog, shots, dev, opts=opts)
+    lo, _ = shard_range(shots * world, rank, world)
     for _ in range(2):
-        plan.run(base_seed)
+        plan.run(base_seed + lo)
     ms = []
     for _ in range(5):
-        bits, st = plan.run(base_seed)
+        bits, st = plan.run(base_seed + lo)
         ms.append(st.kernel_ms)
     kernel_ms = float(np.median(ms))
+    if d is not None:
+        kernel_ms = d.max(kernel_ms)
+    local = {}
+    for row in bits:
+        k = format_cbits(row, prog.num_cbits)
+        local[k] = local.get(k, 0) + 1
+    merged = merge_counts(local, prog.num_cbits)
     # per-shot launches of the exact per-gate kernels (HBM-resident state)
     state = nat.State(16, dev)
     k = 16
@@ -466,10 +490,12 @@ def trajectory_section(dev: int, cpu: bool) -> dict:
     sim.simulate_shots(circ, shots)
     e2e_ms = (time.perf_counter() - t0) * 1e3
     out = {
-        "workload": "4096 shots x 16 qubits, 12 layers u3+cx brickwork, measure/cond-x/reset "
-                    "every 3rd layer (base_seed 7)",
+        "workload": "4096 shots x 16 qubits per GPU, 12 layers u3+cx brickwork, "
+                    "measure/cond-x/reset every 3rd layer (base_seed 7)",
         "kernel_ms": kernel_ms,
-        "shots_per_s": shots / (kernel_ms * 1e-3),
+        "shots_per_s": shots * world / (kernel_ms * 1e-3),
+        "ranks": world,
+        "merged_counts": merged,
         "e2e_ms": e2e_ms,
         "e2e_path": "StatevectorSimulator.simulate_shots(circuit, 4096)",
         "per_shot_launches_ms": per_shot_ms * shots,
@@ -551,6 +577,67 @@ def adjoint_section(dev: int) -> dict:
                               "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                               "peak_source": src},
     }
+
+
+def adjoint_batch_section(dev: int, adam_steps: int, workers: int = 4) -> dict:
+    """512 parameter sets of the 20-qubit, 8-layer ansatz (480 parameters
+    each) through the torch autograd function, driving Adam (lr 0.01) on the
+    sum of the energies.  Times `adam_steps` steps after one warm-up step."""
+    import torch
+
+    from dqsim_bosonic_b200.adjoint import expval
+
+    c, theta, H = _circuits.hea_param_circuit(20, 8, seed=1)
+    B = 512
+    rng = np.random.default_rng(11)
+    t = torch.tensor(rng.uniform(-math.pi, math.pi, size=(B, c.num_params)), requires_grad=True)
+    opt = torch.optim.Adam([t], lr=0.01)
+
+    def step():
+        opt.zero_grad()
+        e = expval(t, c, H, device=dev, workers=workers)
+        e.sum().backward()
+        opt.step()
+        return e.detach()
+
+    e0 = step()
+    t0 = time.perf_counter()
+    for _ in range(adam_steps):
+        e = step()
+    dt = (time.perf_counter() - t0) / max(adam_steps, 1)
+    return {
+        "workload": "512 parameter sets x hea20 (8 layers, 480 params), Adam lr 0.01 on sum <H>",
+        "s_per_adam_step": dt,
+        "gradients_per_s": B / dt,
+        "adam_steps_timed": adam_steps,
+        "projected_s_for_50_steps": 50 * dt,
+        "mean_energy_first": float(e0.mean()),
+        "mean_energy_last": float(e.mean()),
+        "workers": workers,
+    }
+
+
+def adjoint31_section(dev: int, fd_params: int = 32) -> dict:
+    """One adjoint pass at 31 qubits (4 layers, 372 parameters; psi and lambda
+    = 64 GiB in HBM), gradient checked by central differences (h = 1e-6) on a
+    seeded subset of parameters."""
+    from dqsim_bosonic_b200.adjoint import adjoint_gradient, expectation
+
+    c, theta, H = _circuits.hea_param_circuit(31, 4, seed=1)
+    tm = {}
+    t0 = time.perf_counter()
+    e, g = adjoint_gradient(c, theta, H, device=dev, timing=tm)
+    t_adj = time.perf_counter() - t0
+    sub = sorted(np.random.default_rng(0).choice(theta.size, size=fd_params, replace=False).tolist())
+    h = 1e-6
+    fd = []
+    for k in sub:
+        tp = theta.copy(); tp[k] += h
+        tmn = theta.copy(); tmn[k] -= h
+        fd.append((expectation(c, tp, H, device=dev) - expectation(c, tmn, H, device=dev)) / (2 * h))
+    err = float(np.max(np.abs(np.array(fd) - g[sub])))
+    return {"workload": "hea31: 4 layers, 372 params", "s_per_gradient": t_adj, "phases_ms": tm,
+            "expval": e, "fd_params": len(sub), "fd_h": h, "max_abs_diff_vs_fd": err}
 
 
 def dominant_kernel_roofline(st, prog, exec_mode, stream, dev):
