@@ -26,6 +26,7 @@
 #include <string>
 #include <vector>
 
+#include "dq_adjsweep.cuh"
 #include "dq_common.cuh"
 #include "dq_engine.cuh"
 #include "dq_gates.hpp"
@@ -270,6 +271,28 @@ bool block_derivs(const dq_inst& in, hc u[4], hc d[4][4], int* np) {
   }
 }
 
+// The 4x4 of rxx / rzz and its derivative.
+bool rxx_rzz_deriv(const dq_inst& in, hc m[16], hc dm[16]) {
+  if (in.kind != DQ_RXX && in.kind != DQ_RZZ) return false;
+  Gate g;
+  matrix_nq(in, g);
+  for (int i = 0; i < 16; ++i) {
+    m[i] = g.m[i];
+    dm[i] = hc{0, 0};
+  }
+  if (in.kind == DQ_RZZ) {
+    dm[0] = hc{0, -0.5} * g.m[0];
+    dm[5] = hc{0, 0.5} * g.m[5];
+    dm[10] = hc{0, 0.5} * g.m[10];
+    dm[15] = hc{0, -0.5} * g.m[15];
+  } else {
+    const double cv = cos(in.p[0] / 2.0), sv = sin(in.p[0] / 2.0);
+    for (int i : {0, 5, 10, 15}) dm[i] = hc{-sv / 2.0, 0};
+    for (int i : {3, 6, 9, 12}) dm[i] = hc{0, -cv / 2.0};
+  }
+  return true;
+}
+
 bool is_controlled_block(int kind) {
   switch (kind) {
     case DQ_CRX: case DQ_CRY: case DQ_CRZ: case DQ_CU1: case DQ_CP: case DQ_CU3: case DQ_CU:
@@ -433,22 +456,9 @@ int launch_adj(dq_state_t h, double2* lam, const dq_inst& in, double* d_out) {
     DQ_CUDA_TRY(cudaGetLastError());
     return DQ_OK;
   }
-  if (in.kind != DQ_RXX && in.kind != DQ_RZZ)
-    return fail(DQ_ERR_INTERNAL, "kind without derivative");
   Gate g;
-  matrix_nq(in, g);
   hc dm[16];
-  for (int i = 0; i < 16; ++i) dm[i] = hc{0, 0};
-  if (in.kind == DQ_RZZ) {
-    dm[0] = hc{0, -0.5} * g.m[0];
-    dm[5] = hc{0, 0.5} * g.m[5];
-    dm[10] = hc{0, 0.5} * g.m[10];
-    dm[15] = hc{0, -0.5} * g.m[15];
-  } else {
-    const double cv = cos(in.p[0] / 2.0), sv = sin(in.p[0] / 2.0);
-    for (int i : {0, 5, 10, 15}) dm[i] = hc{-sv / 2.0, 0};
-    for (int i : {3, 6, 9, 12}) dm[i] = hc{0, -cv / 2.0};
-  }
+  if (!rxx_rzz_deriv(in, g.m, dm)) return fail(DQ_ERR_INTERNAL, "kind without derivative");
   Adj2Args a{};
   for (int r = 0; r < 4; ++r)
     for (int c = 0; c < 4; ++c) {
@@ -468,6 +478,13 @@ int launch_adj(dq_state_t h, double2* lam, const dq_inst& in, double* d_out) {
 }
 
 }  // namespace
+
+bool adjoint_block_derivs(const dq_inst& in, hc u[4], hc d[4][4], int* np) {
+  return block_derivs(in, u, d, np);
+}
+bool adjoint_rxx_rzz_deriv(const dq_inst& in, hc m[16], hc dm[16]) { return rxx_rzz_deriv(in, m, dm); }
+bool adjoint_controlled_block(int kind) { return is_controlled_block(kind); }
+
 }  // namespace dq
 
 using namespace dq;
@@ -539,8 +556,14 @@ int dq_adjoint(dq_state_t h, const dq_inst* prog, uint64_t ninst, const int32_t*
   mark(2);
 
   // backward pass: slots are numbered in program order
+  const bool fused_back = o.exec == DQ_EXEC_FUSED;
+  if (fused_back && rc == DQ_OK) {
+    AdjSweepStats ss;
+    rc = adjoint_backward_fused(h->amp, lam, h->n, prog, ninst, param_index, nslots, slots,
+                                h->stream, h->device, &ss);
+  }
   uint64_t slot = nslots;
-  for (uint64_t r = ninst; rc == DQ_OK && r-- > 0;) {
+  for (uint64_t r = ninst; !fused_back && rc == DQ_OK && r-- > 0;) {
     const dq_inst& in = prog[r];
     if (is_noop_kind(in.kind)) continue;
     int nd = 0;

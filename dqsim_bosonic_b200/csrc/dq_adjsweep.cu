@@ -1,0 +1,835 @@
+// dq_adjsweep.cu — the adjoint backward pass as fused tile sweeps.
+//
+// The per-gate backward (dq_adjoint.cu) streams psi and lambda through HBM
+// once per gate (64 B per amplitude per gate).  Here a sweep loads a tile of
+// 2^m amplitudes of both vectors into shared memory (the tile spans the m
+// "local" qubits: bits 0..4 for coalescing plus up to m - 5 chosen ones),
+// applies a run of gates in reverse program order to both, reduces every
+// gate's gradient terms, and writes the tile back: 64 B per amplitude per
+// sweep instead of per gate.  A gate can join the current sweep when
+//   * it is diagonal (any qubits: a non-local bit is constant over a tile), or
+//   * its non-diagonal qubits (a one-qubit target, both qubits of a dense
+//     two-qubit gate) are local — the planner widens the local set up to m.
+// Gates of three or more qubits end the sweep and are undone by the exact
+// per-gate kernels on both vectors (they carry no trainable parameter).
+//
+// Ops (all act on psi and lambda; V = U^dagger, D_j = dU/dtheta_j):
+//   A_ONE   2x2 on a local target; optional local control mask; optional
+//           non-local selector bit choosing between two matrix variants
+//           (controlled gates with a non-local control: variant 0 = I).
+//   A_TWO   dense 4x4 on two local qubits (rxx, swap-like, psi+-, phi+).
+//   A_DIAG  diagonal on up to two qubits, local or not, applied elementwise.
+// Gradient terms: Re sum conj(lambda_k) (D_j psi_{k-1}) with psi_{k-1} = V psi_k,
+// summed per thread, reduced per warp into shared slots [slot][warp], per CTA
+// in warp order, and over CTAs in CTA order by k_adj_slots: deterministic for
+// a fixed grid.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+#include <string.h>
+
+#include <algorithm>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "dq_adjsweep.cuh"
+#include "dq_common.cuh"
+#include "dq_engine.cuh"
+#include "dq_gates.hpp"
+
+namespace dq {
+namespace {
+
+constexpr int kAThreads = 256;
+constexpr int kAWarps = kAThreads / 32;
+constexpr uint32_t kAMaxLocal = 11;
+constexpr uint32_t kAMaxOps = 192;
+constexpr uint32_t kAMaxSlots = 192;
+
+enum AType : uint8_t { A_ONE = 1, A_TWO = 2, A_DIAG = 3, A_DRUN = 4 };
+constexpr uint32_t kADiagRun = 16;  // diagonal ops applied in one elementwise pass
+
+struct AOp {
+  uint8_t type;
+  uint8_t np;        // derivative matrices (gradient slots) of the op
+  uint8_t lt, lt2;   // A_ONE: local target bit; A_TWO: local bits of the 4x4 MSB / LSB
+  int8_t sel;        // A_ONE: non-local selector position (-1: none)
+  uint8_t skip0;     // A_ONE with selector: variant 0 is the identity with no derivatives
+  uint8_t dq[2];     // A_DIAG: qubit encodings (bit 7: local; low 7 bits: local bit or global position)
+  uint8_t ndq;       // A_DIAG: 1 or 2 qubits (dq[0] = MSB of the diagonal index)
+  uint8_t cnt;       // A_DRUN: number of A_DIAG ops that follow it
+  uint8_t pad[2];
+  uint32_t lctrl;    // A_ONE: local control mask (tile offset bits)
+  uint32_t slot;     // first sweep-local gradient slot
+  uint32_t mat;      // offset of the op's matrices in the pool (double2 units)
+};
+static_assert(sizeof(AOp) == 24, "AOp layout");
+
+struct ASweepHdr {
+  uint32_t n, m, nops, nslots;
+  uint64_t ntiles;
+  uint32_t lpos[kAMaxLocal];  // local bit positions, ascending
+  uint32_t npos_cnt;
+  uint32_t npos[64];          // non-local bit positions, ascending
+};
+
+__device__ __forceinline__ double2 cfma2(double2 a, double2 b, double2 acc) {
+  return make_double2(fma(a.x, b.x, fma(-a.y, b.y, acc.x)), fma(a.x, b.y, fma(a.y, b.x, acc.y)));
+}
+__device__ __forceinline__ double2 cmul2(double2 a, double2 b) {
+  return make_double2(fma(a.x, b.x, -a.y * b.y), fma(a.x, b.y, a.y * b.x));
+}
+__device__ __forceinline__ double redot(double2 l, double2 w, double acc) {
+  return fma(l.x, w.x, fma(l.y, w.y, acc));
+}
+__device__ __forceinline__ uint32_t ins0a(uint32_t k, uint32_t p) {
+  return ((k >> p) << (p + 1)) | (k & ((1u << p) - 1u));
+}
+
+__device__ __forceinline__ double warp_sum_d(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  return v;
+}
+
+template <int NP>
+__device__ __forceinline__ void flush_acc(const double (&acc)[4], double* accw, uint32_t slot) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+  for (int j = 0; j < NP; ++j) {
+    const double v = warp_sum_d(acc[j]);
+    if (lane == 0) accw[(slot + j) * kAWarps + w] += v;
+  }
+}
+
+template <int NP>
+__device__ __noinline__ void op_one(double2* sp, double2* sl, const AOp& op, const double2* pool, uint32_t m,
+                       uint64_t base, double* accw) {
+  int var = 0;
+  if (op.sel >= 0) var = (int)((base >> op.sel) & 1ULL);
+  if (var == 0 && op.skip0) return;
+  const double2* mt = pool + op.mat + (uint32_t)var * (4u + 4u * NP);
+  double2 v[4], d[NP > 0 ? NP : 1][4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) v[i] = mt[i];
+#pragma unroll
+  for (int j = 0; j < NP; ++j)
+#pragma unroll
+    for (int i = 0; i < 4; ++i) d[j][i] = mt[4 + 4 * j + i];
+  // zero-insertion positions: target and local controls, ascending
+  uint32_t pos[12];
+  int npos = 0;
+  uint32_t mask = op.lctrl | (1u << op.lt);
+  while (mask) {
+    const uint32_t b = __ffs(mask) - 1;
+    pos[npos++] = b;
+    mask &= mask - 1;
+  }
+  const uint32_t count = (1u << m) >> npos;
+  const uint32_t tb = 1u << op.lt;
+  const bool plain = op.lctrl == 0;
+  double acc[4] = {0.0, 0.0, 0.0, 0.0};
+  for (uint32_t k = threadIdx.x; k < count; k += kAThreads) {
+    uint32_t o;
+    if (plain) {
+      o = ins0a(k, op.lt);
+    } else {
+      o = k;
+      for (int p = 0; p < npos; ++p) o = ins0a(o, pos[p]);
+      o |= op.lctrl;
+    }
+    const uint32_t o1 = o | tb;
+    const double2 a0 = sp[o], a1 = sp[o1], b0 = sl[o], b1 = sl[o1];
+    const double2 p0 = cfma2(v[1], a1, cmul2(v[0], a0));
+    const double2 p1 = cfma2(v[3], a1, cmul2(v[2], a0));
+    sp[o] = p0;
+    sp[o1] = p1;
+#pragma unroll
+    for (int j = 0; j < NP; ++j) {
+      const double2 w0 = cfma2(d[j][1], p1, cmul2(d[j][0], p0));
+      const double2 w1 = cfma2(d[j][3], p1, cmul2(d[j][2], p0));
+      acc[j] = redot(b0, w0, redot(b1, w1, acc[j]));
+    }
+    sl[o] = cfma2(v[1], b1, cmul2(v[0], b0));
+    sl[o1] = cfma2(v[3], b1, cmul2(v[2], b0));
+  }
+  flush_acc<NP>(acc, accw, op.slot);
+}
+
+template <int NP>
+__device__ __noinline__ void op_two(double2* sp, double2* sl, const AOp& op, const double2* pool, uint32_t m,
+                       double* accw) {
+  const double2* mt = pool + op.mat;
+  const uint32_t ba = 1u << op.lt, bb = 1u << op.lt2;
+  const uint32_t p0 = min((uint32_t)op.lt, (uint32_t)op.lt2), p1 = max((uint32_t)op.lt, (uint32_t)op.lt2);
+  const uint32_t count = (1u << m) >> 2;
+  double acc[4] = {0.0, 0.0, 0.0, 0.0};
+  for (uint32_t k = threadIdx.x; k < count; k += kAThreads) {
+    const uint32_t b = ins0a(ins0a(k, p0), p1);
+    const uint32_t idx[4] = {b, b | bb, b | ba, b | ba | bb};
+    double2 x[4], y[4], p[4];
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      x[r] = sp[idx[r]];
+      y[r] = sl[idx[r]];
+    }
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      double2 s = make_double2(0.0, 0.0);
+#pragma unroll
+      for (int c = 0; c < 4; ++c) s = cfma2(mt[r * 4 + c], x[c], s);
+      p[r] = s;
+    }
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      sp[idx[r]] = p[r];
+      double2 s = make_double2(0.0, 0.0);
+#pragma unroll
+      for (int c = 0; c < 4; ++c) s = cfma2(mt[r * 4 + c], y[c], s);
+#pragma unroll
+      for (int j = 0; j < NP; ++j) {
+        double2 w = make_double2(0.0, 0.0);
+#pragma unroll
+        for (int c = 0; c < 4; ++c) w = cfma2(mt[16 * (j + 1) + r * 4 + c], p[c], w);
+        acc[j] = redot(y[r], w, acc[j]);
+      }
+      sl[idx[r]] = s;
+    }
+  }
+  flush_acc<NP>(acc, accw, op.slot);
+}
+
+template <int NP>
+__device__ __noinline__ void op_diag(double2* sp, double2* sl, const AOp& op, const double2* pool, uint32_t m,
+                        uint64_t base, double* accw) {
+  // entry index bits: for each diag qubit, its bit from the tile offset (local)
+  // or from the tile base (non-local)
+  const double2* mt = pool + op.mat;  // [4 entries: v], then [NP][4]: d
+  uint32_t lmask[2] = {0, 0}, fixed = 0;
+  for (uint32_t a = 0; a < op.ndq; ++a) {
+    const uint32_t e = op.dq[a];
+    const uint32_t shift = op.ndq - 1 - a;  // dq[0] is the MSB
+    if (e & 0x80u) lmask[a] = 1u << (e & 0x7fu);
+    else fixed |= (uint32_t)((base >> (e & 0x7fu)) & 1ULL) << shift;
+  }
+  double2 v[4], d[NP > 0 ? NP : 1][4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) v[i] = mt[i];
+#pragma unroll
+  for (int j = 0; j < NP; ++j)
+#pragma unroll
+    for (int i = 0; i < 4; ++i) d[j][i] = mt[4 + 4 * j + i];
+  const uint32_t L = 1u << m;
+  const uint32_t sh0 = op.ndq == 2 ? 1u : 0u;
+  double acc[4] = {0.0, 0.0, 0.0, 0.0};
+  for (uint32_t o = threadIdx.x; o < L; o += kAThreads) {
+    uint32_t e = fixed;
+    if (lmask[0] && (o & lmask[0])) e |= 1u << sh0;
+    if (lmask[1] && (o & lmask[1])) e |= 1u;
+    const double2 a = sp[o], b = sl[o];
+    const double2 p = cmul2(v[e], a);
+    sp[o] = p;
+#pragma unroll
+    for (int j = 0; j < NP; ++j) acc[j] = redot(b, cmul2(d[j][e], p), acc[j]);
+    sl[o] = cmul2(v[e], b);
+  }
+  flush_acc<NP>(acc, accw, op.slot);
+}
+
+// One diagonal op staged in shared memory for a run.
+struct DSub {
+  double2 v[4];
+  double2 d[4];
+  uint32_t lm0, lm1;  // local bit masks of the MSB / LSB qubit (0: not local)
+  uint32_t fixed;     // index bits from non-local qubits (tile constant)
+  uint32_t b0;        // value of the MSB in the entry index (2 or 1)
+  uint32_t np, slot;
+  uint32_t pad[2];
+};
+
+// A run of diagonal ops: each element goes through all of them in order
+// (they commute with nothing in between, so the order is the program's).
+__device__ __noinline__ void op_drun(double2* sp, double2* sl, const AOp* sub, uint32_t cnt,
+                                     const double2* pool, uint32_t m, uint64_t base, double* accw,
+                                     DSub* ds) {
+  if (threadIdx.x < cnt) {
+    const AOp op = sub[threadIdx.x];
+    DSub& D = ds[threadIdx.x];
+    D.lm0 = D.lm1 = D.fixed = 0;
+    D.b0 = op.ndq == 2 ? 2u : 1u;
+    for (uint32_t a = 0; a < op.ndq; ++a) {
+      const uint32_t e = op.dq[a];
+      const uint32_t bitv = (a == 0) ? D.b0 : 1u;
+      if (e & 0x80u) {
+        if (a == 0) D.lm0 = 1u << (e & 0x7fu);
+        else D.lm1 = 1u << (e & 0x7fu);
+      } else if ((base >> (e & 0x7fu)) & 1ULL) {
+        D.fixed |= bitv;
+      }
+    }
+    const double2* mt = pool + op.mat;
+    for (int i = 0; i < 4; ++i) D.v[i] = mt[i];
+    for (int i = 0; i < 4; ++i) D.d[i] = op.np ? mt[4 + i] : make_double2(0.0, 0.0);
+    D.np = op.np;
+    D.slot = op.slot;
+  }
+  __syncthreads();
+  const uint32_t L = 1u << m;
+  double acc[kADiagRun];
+#pragma unroll
+  for (int u = 0; u < (int)kADiagRun; ++u) acc[u] = 0.0;
+  for (uint32_t o = threadIdx.x; o < L; o += kAThreads) {
+    double2 a = sp[o], b = sl[o];
+#pragma unroll
+    for (int u = 0; u < (int)kADiagRun; ++u) {
+      if (u < (int)cnt) {
+        const DSub& D = ds[u];
+        const uint32_t e = D.fixed | ((o & D.lm0) ? D.b0 : 0u) | ((o & D.lm1) ? 1u : 0u);
+        const double2 vv = D.v[e];
+        const double2 p = cmul2(vv, a);
+        if (D.np) acc[u] = redot(b, cmul2(D.d[e], p), acc[u]);
+        b = cmul2(vv, b);
+        a = p;
+      }
+    }
+    sp[o] = a;
+    sl[o] = b;
+  }
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+  for (int u = 0; u < (int)kADiagRun; ++u) {
+    if (u < (int)cnt && ds[u].np) {
+      const double v = warp_sum_d(acc[u]);
+      if (lane == 0) accw[ds[u].slot * kAWarps + w] += v;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kAThreads, 2)
+    k_adj_sweep(double2* __restrict__ psi, double2* __restrict__ lam, const ASweepHdr* __restrict__ hp,
+                const AOp* __restrict__ ops, const double2* __restrict__ pool, double* partial) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  __shared__ ASweepHdr H;
+  __shared__ uint64_t hi_tab[64];
+  __shared__ DSub dsub[kADiagRun];
+  if (threadIdx.x == 0) H = *hp;
+  __syncthreads();
+  const uint32_t m = H.m, L = 1u << m;
+  double2* sp = reinterpret_cast<double2*>(smraw);
+  double2* sl = sp + L;
+  double* accw = reinterpret_cast<double*>(sl + L);
+  for (uint32_t i = threadIdx.x; i < H.nslots * kAWarps; i += kAThreads) accw[i] = 0.0;
+  // offset bits above the 5 contiguous ones -> global bits
+  const uint32_t lo_bits = m < 5 ? m : 5;
+  const uint32_t nhi = m - lo_bits;
+  for (uint32_t hv = threadIdx.x; hv < (1u << nhi); hv += kAThreads) {
+    uint64_t g = 0;
+    for (uint32_t b = 0; b < nhi; ++b)
+      if (hv >> b & 1u) g |= 1ULL << H.lpos[lo_bits + b];
+    hi_tab[hv] = g;
+  }
+  __syncthreads();
+  const uint32_t lo_mask = (1u << lo_bits) - 1u;
+
+  for (uint64_t t = blockIdx.x; t < H.ntiles; t += gridDim.x) {
+    uint64_t base = 0;
+    for (uint32_t b = 0; b < H.npos_cnt; ++b)
+      if (t >> b & 1ULL) base |= 1ULL << H.npos[b];
+    for (uint32_t o = threadIdx.x; o < L; o += kAThreads) {
+      const uint64_t g = base | (o & lo_mask) | hi_tab[o >> lo_bits];
+      sp[o] = psi[g];
+      sl[o] = lam[g];
+    }
+    __syncthreads();
+    for (uint32_t i = 0; i < H.nops; ++i) {
+      const AOp op = ops[i];
+      if (op.type == A_DRUN) {
+        op_drun(sp, sl, ops + i + 1, op.cnt, pool, m, base, accw, dsub);
+        i += op.cnt;
+        __syncthreads();
+        continue;
+      }
+      switch (op.type) {
+        case A_ONE:
+          switch (op.np) {
+            case 0: op_one<0>(sp, sl, op, pool, m, base, accw); break;
+            case 1: op_one<1>(sp, sl, op, pool, m, base, accw); break;
+            case 2: op_one<2>(sp, sl, op, pool, m, base, accw); break;
+            case 3: op_one<3>(sp, sl, op, pool, m, base, accw); break;
+            default: op_one<4>(sp, sl, op, pool, m, base, accw); break;
+          }
+          break;
+        case A_TWO:
+          if (op.np) op_two<1>(sp, sl, op, pool, m, accw);
+          else op_two<0>(sp, sl, op, pool, m, accw);
+          break;
+        default:
+          if (op.np) op_diag<1>(sp, sl, op, pool, m, base, accw);
+          else op_diag<0>(sp, sl, op, pool, m, base, accw);
+          break;
+      }
+      __syncthreads();
+    }
+    for (uint32_t o = threadIdx.x; o < L; o += kAThreads) {
+      const uint64_t g = base | (o & lo_mask) | hi_tab[o >> lo_bits];
+      psi[g] = sp[o];
+      lam[g] = sl[o];
+    }
+    __syncthreads();
+  }
+  for (uint32_t s = threadIdx.x; s < H.nslots; s += kAThreads) {
+    double a = 0.0;
+    for (int w = 0; w < kAWarps; ++w) a += accw[s * kAWarps + w];
+    partial[(size_t)s * gridDim.x + blockIdx.x] = a;
+  }
+}
+
+// out[map[s]] = sum over CTAs (in order) of partial[s][cta]
+__global__ void k_adj_slots(const double* partial, uint32_t nslots, uint32_t ctas,
+                            const uint32_t* map, double* out) {
+  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nslots) return;
+  double a = 0.0;
+  for (uint32_t c = 0; c < ctas; ++c) a += partial[(size_t)s * ctas + c];
+  out[map[s]] = a;
+}
+
+// ---- host planner ----------------------------------------------------------------------------
+
+inline hc cjh(hc z) { return hc{z.re, -z.im}; }
+
+// One gate of the reversed program, classified for the sweep.
+struct AGate {
+  int64_t inst;
+  int kind;  // 0: one-qubit, 1: controlled one-qubit, 2: diagonal (<= 2 qubits), 3: dense 2q, 4: per-gate
+  uint32_t t = 0, c = 0;      // target / control (kind 0, 1)
+  uint32_t qa = 0, qb = 0;    // diagonal / dense qubits (qa = MSB)
+  uint32_t nq = 0;            // diagonal: 1 or 2
+  hc u[4];                    // kind 0/1: 2x2 (block)
+  hc du[4][4];                // derivatives of the 2x2 (block)
+  hc dg[4], ddg[4][4];        // kind 2: diagonal and its derivatives
+  hc m4[16], dm4[16];         // kind 3: 4x4 and its derivative
+  int np = 0;                 // active derivatives
+  uint32_t slot0 = 0;         // first global slot
+};
+
+bool diag2(const hc u[4]) { return is_zero(u[1]) && is_zero(u[2]); }
+
+}  // namespace
+
+// Implemented in dq_adjoint.cu: 2x2 block + derivatives of a (controlled)
+// one-qubit parametrised kind; derivatives of rxx / rzz.
+bool adjoint_block_derivs(const dq_inst& in, hc u[4], hc d[4][4], int* np);
+bool adjoint_rxx_rzz_deriv(const dq_inst& in, hc m[16], hc dm[16]);
+bool adjoint_controlled_block(int kind);
+
+namespace {
+
+int classify_gate(const dq_inst& in, const int32_t* pidx, uint64_t r, uint32_t slot0, AGate& g) {
+  g.inst = (int64_t)r;
+  g.slot0 = slot0;
+  int active[4] = {0, 0, 0, 0};
+  int nact = 0;
+  if (pidx)
+    for (int j = 0; j < 4; ++j)
+      if (pidx[4 * r + j] >= 0) active[nact++] = j;
+  hc u[4], d[4][4];
+  int np = 0;
+  const bool param_block = adjoint_block_derivs(in, u, d, &np);
+  if (param_block || matrix_1q(in.kind, in.p, u)) {
+    const bool ctl = param_block ? adjoint_controlled_block(in.kind) : false;
+    for (int i = 0; i < 4; ++i) g.u[i] = u[i];
+    g.np = nact;
+    for (int a = 0; a < nact; ++a)
+      for (int i = 0; i < 4; ++i) g.du[a][i] = d[active[a]][i];
+    // diagonal only if the matrix and every active derivative are (ry(0) is
+    // the identity, its derivative is not diagonal)
+    bool dg = diag2(u);
+    for (int a = 0; a < nact; ++a) dg = dg && diag2(g.du[a]);
+    if (!ctl) {
+      g.t = (uint32_t)in.q[0];
+      if (dg) {
+        g.kind = 2;
+        g.nq = 1;
+        g.qa = g.t;
+        g.dg[0] = u[0];
+        g.dg[1] = u[3];
+        for (int a = 0; a < nact; ++a) {
+          g.ddg[a][0] = g.du[a][0];
+          g.ddg[a][1] = g.du[a][3];
+        }
+      } else {
+        g.kind = 0;
+      }
+      return DQ_OK;
+    }
+    g.c = (uint32_t)in.q[0];
+    g.t = (uint32_t)in.q[1];
+    if (dg) {  // controlled diagonal: a two-qubit diagonal (c = MSB)
+      g.kind = 2;
+      g.nq = 2;
+      g.qa = g.c;
+      g.qb = g.t;
+      g.dg[0] = R(1); g.dg[1] = R(1); g.dg[2] = u[0]; g.dg[3] = u[3];
+      for (int a = 0; a < nact; ++a) {
+        g.ddg[a][0] = R(0); g.ddg[a][1] = R(0);
+        g.ddg[a][2] = g.du[a][0]; g.ddg[a][3] = g.du[a][3];
+      }
+    } else {
+      g.kind = 1;
+    }
+    return DQ_OK;
+  }
+  if (nact > 0 && !(in.kind == DQ_RXX || in.kind == DQ_RZZ))
+    return fail(DQ_ERR_INTERNAL, "parameter slot on a kind without a derivative");
+  Gate gt;
+  if (!matrix_nq(in, gt)) return fail(DQ_ERR_INTERNAL, "instruction kind without a matrix");
+  if (gt.k > 2) {
+    g.kind = 4;
+    return DQ_OK;
+  }
+  hc dm[16];
+  for (int i = 0; i < 16; ++i) dm[i] = R(0);
+  if (nact) adjoint_rxx_rzz_deriv(in, gt.m, dm);
+  g.np = nact;
+  GateOp op;
+  classify(gt, op);
+  g.qa = gt.qubits[0];
+  g.qb = gt.qubits[1];
+  if (nact == 0 && (op.cls == GC_ONE_Q || op.cls == GC_PHASE || op.cls == GC_XPERM)) {
+    // controlled one-qubit without a trainable parameter (rxx / rzz at
+    // special angles with an active slot keep their 4x4 and derivative)
+    g.c = gt.qubits[0];
+    g.t = gt.qubits[1];
+    for (int i = 0; i < 4; ++i) g.u[i] = hc{0, 0};
+    g.u[0] = gt.m[10]; g.u[1] = gt.m[11]; g.u[2] = gt.m[14]; g.u[3] = gt.m[15];
+    if (diag2(g.u)) {
+      g.kind = 2;
+      g.nq = 2;
+      g.qa = g.c;
+      g.qb = g.t;
+      g.dg[0] = R(1); g.dg[1] = R(1); g.dg[2] = g.u[0]; g.dg[3] = g.u[3];
+    } else {
+      g.kind = 1;
+    }
+    return DQ_OK;
+  }
+  bool dgn = true;
+  for (int r2 = 0; r2 < 4; ++r2)
+    for (int c2 = 0; c2 < 4; ++c2)
+      if (r2 != c2 && (!is_zero(gt.m[r2 * 4 + c2]) || (nact && !is_zero(dm[r2 * 4 + c2]))))
+        dgn = false;
+  if (dgn) {
+    g.kind = 2;
+    g.nq = 2;
+    for (int i = 0; i < 4; ++i) {
+      g.dg[i] = gt.m[i * 5];
+      if (nact) g.ddg[0][i] = dm[i * 5];
+    }
+    return DQ_OK;
+  }
+  g.kind = 3;
+  for (int i = 0; i < 16; ++i) {
+    g.m4[i] = gt.m[i];
+    g.dm4[i] = dm[i];
+  }
+  return DQ_OK;
+}
+
+struct ASweepPlan {
+  uint64_t Lmask = 0;
+  std::vector<AGate> gates;  // reverse program order
+};
+
+// Qubits a gate needs local.
+uint64_t need_local(const AGate& g) {
+  switch (g.kind) {
+    case 0: case 1: return 1ULL << g.t;
+    case 3: return (1ULL << g.qa) | (1ULL << g.qb);
+    default: return 0;
+  }
+}
+
+void push_mats(std::vector<double2>& pool, const hc* m, int count) {
+  for (int i = 0; i < count; ++i) pool.push_back(make_double2(m[i].re, m[i].im));
+}
+
+// Encodes one sweep's ops given its final local set.
+int encode_asweep(const ASweepPlan& sp, uint32_t n, ASweepHdr& hdr, std::vector<AOp>& ops,
+                  std::vector<double2>& pool, std::vector<uint32_t>& slot_map) {
+  memset(&hdr, 0, sizeof(hdr));
+  hdr.n = n;
+  uint32_t lidx[64];
+  uint32_t m = 0;
+  for (uint32_t q = 0; q < n; ++q) {
+    if (sp.Lmask >> q & 1ULL) {
+      lidx[q] = m;
+      hdr.lpos[m++] = q;
+    } else {
+      hdr.npos[hdr.npos_cnt++] = q;
+    }
+  }
+  hdr.m = m;
+  hdr.ntiles = 1ULL << (n - m);
+  uint32_t slot = 0;
+  for (const AGate& g : sp.gates) {
+    AOp op{};
+    op.np = (uint8_t)g.np;
+    op.slot = slot;
+    op.sel = -1;
+    op.mat = (uint32_t)pool.size();
+    for (int a = 0; a < g.np; ++a) slot_map.push_back(g.slot0 + (uint32_t)a);
+    slot += (uint32_t)g.np;
+    if (g.kind == 0 || g.kind == 1) {
+      op.type = A_ONE;
+      op.lt = (uint8_t)lidx[g.t];
+      const hc v[4] = {cjh(g.u[0]), cjh(g.u[2]), cjh(g.u[1]), cjh(g.u[3])};
+      if (g.kind == 1 && !(sp.Lmask >> g.c & 1ULL)) {
+        // non-local control: variant 0 (control 0) is the identity
+        op.sel = (int8_t)g.c;
+        op.skip0 = 1;
+        const hc id[4] = {R(1), R(0), R(0), R(1)};
+        push_mats(pool, id, 4);
+        for (int a = 0; a < g.np; ++a) {
+          const hc z[4] = {R(0), R(0), R(0), R(0)};
+          push_mats(pool, z, 4);
+        }
+      } else if (g.kind == 1) {
+        op.lctrl = 1u << lidx[g.c];
+      }
+      push_mats(pool, v, 4);
+      for (int a = 0; a < g.np; ++a) push_mats(pool, g.du[a], 4);
+    } else if (g.kind == 3) {
+      op.type = A_TWO;
+      op.lt = (uint8_t)lidx[g.qa];
+      op.lt2 = (uint8_t)lidx[g.qb];
+      hc v[16];
+      for (int r = 0; r < 4; ++r)
+        for (int c = 0; c < 4; ++c) v[r * 4 + c] = cjh(g.m4[c * 4 + r]);
+      push_mats(pool, v, 16);
+      if (g.np) push_mats(pool, g.dm4, 16);
+    } else {
+      op.type = A_DIAG;
+      op.ndq = (uint8_t)g.nq;
+      const uint32_t qs[2] = {g.qa, g.qb};
+      for (uint32_t a = 0; a < g.nq; ++a)
+        op.dq[a] = (sp.Lmask >> qs[a] & 1ULL) ? (uint8_t)(0x80u | lidx[qs[a]]) : (uint8_t)qs[a];
+      hc v[4] = {R(1), R(1), R(1), R(1)};
+      const uint32_t D = 1u << g.nq;
+      for (uint32_t i = 0; i < D; ++i) v[i] = cjh(g.dg[i]);
+      push_mats(pool, v, 4);
+      for (int a = 0; a < g.np; ++a) {
+        hc dd[4] = {R(0), R(0), R(0), R(0)};
+        for (uint32_t i = 0; i < D; ++i) dd[i] = g.ddg[a][i];
+        push_mats(pool, dd, 4);
+      }
+    }
+    ops.push_back(op);
+  }
+  // runs of consecutive diagonal ops become one A_DRUN header + the ops
+  std::vector<AOp> grouped;
+  for (size_t i = 0; i < ops.size();) {
+    if (ops[i].type != A_DIAG) {
+      grouped.push_back(ops[i++]);
+      continue;
+    }
+    size_t j = i;
+    while (j < ops.size() && ops[j].type == A_DIAG && j - i < kADiagRun) ++j;
+    AOp h{};
+    h.type = A_DRUN;
+    h.cnt = (uint8_t)(j - i);
+    grouped.push_back(h);
+    for (size_t k = i; k < j; ++k) grouped.push_back(ops[k]);
+    i = j;
+  }
+  ops.swap(grouped);
+  hdr.nops = (uint32_t)ops.size();
+  hdr.nslots = slot;
+  return DQ_OK;
+}
+
+int sweep_ctas(int device) {
+  static std::mutex mu;
+  static int per_sm[64];
+  std::lock_guard<std::mutex> lk(mu);
+  if (per_sm[device & 63] == 0) {
+    const size_t smem_max = sizeof(double2) * 2 * (1u << kAMaxLocal) + sizeof(double) * kAMaxSlots * kAWarps;
+    DQ_CUDA_TRY(cudaFuncSetAttribute(k_adj_sweep, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)smem_max));
+    int b = 1;
+    DQ_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_adj_sweep, kAThreads, smem_max));
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    per_sm[device & 63] = std::max(1, b) * sms;
+  }
+  return per_sm[device & 63];
+}
+
+}  // namespace
+
+int adjoint_backward_fused(double2* psi, double2* lam, uint32_t n, const dq_inst* prog,
+                           uint64_t ninst, const int32_t* pidx, uint64_t nslots, double* d_slots,
+                           cudaStream_t st, int device, AdjSweepStats* stats) {
+  // global slot numbering: program order, parameter order within a gate
+  std::vector<uint32_t> first_slot(ninst + 1, 0);
+  for (uint64_t i = 0; i < ninst; ++i) {
+    uint32_t c = 0;
+    if (pidx)
+      for (int j = 0; j < 4; ++j) c += pidx[4 * i + j] >= 0;
+    first_slot[i + 1] = first_slot[i] + c;
+  }
+  if (first_slot[ninst] != nslots) return fail(DQ_ERR_INTERNAL, "slot count mismatch");
+  const uint32_t m_max = std::min<uint32_t>(n, kAMaxLocal);
+  const uint32_t lo = std::min<uint32_t>(n, 5);
+  const uint64_t lo_mask = (1ULL << lo) - 1;
+  // segments: sweeps and per-gate instructions, in backward order
+  struct Seg {
+    bool sweep;
+    ASweepPlan plan;
+    int64_t inst;
+  };
+  std::vector<Seg> segs;
+  ASweepPlan cur;
+  cur.Lmask = lo_mask;
+  uint32_t cur_slots = 0;
+  auto close = [&]() {
+    if (!cur.gates.empty()) {
+      // widen the local set to m_max with the lowest unused qubits (more
+      // work per tile, fewer tiles; the set only needs to contain the gates')
+      for (uint32_t q = 0; q < n && (uint32_t)__builtin_popcountll(cur.Lmask) < m_max; ++q)
+        cur.Lmask |= 1ULL << q;
+      segs.push_back(Seg{true, cur, -1});
+    }
+    cur = ASweepPlan();
+    cur.Lmask = lo_mask;
+    cur_slots = 0;
+  };
+  for (uint64_t r = ninst; r-- > 0;) {
+    const dq_inst& in = prog[r];
+    if (in.kind == DQ_ID || in.kind == DQ_U0 || in.kind == DQ_BARRIER || in.kind == DQ_CLASSICAL ||
+        in.kind == DQ_G_NOOP)
+      continue;
+    AGate g;
+    DQ_TRY(classify_gate(in, pidx, r, first_slot[r], g));
+    if (g.kind == 4) {
+      close();
+      segs.push_back(Seg{false, ASweepPlan(), (int64_t)r});
+      continue;
+    }
+    const uint64_t need = need_local(g);
+    const uint64_t widened = cur.Lmask | need;
+    if ((uint32_t)__builtin_popcountll(widened) > m_max || cur.gates.size() >= kAMaxOps ||
+        cur_slots + (uint32_t)g.np > kAMaxSlots) {
+      close();
+    }
+    cur.Lmask |= need;
+    cur.gates.push_back(g);
+    cur_slots += (uint32_t)g.np;
+  }
+  close();
+
+  const int ctas_max = sweep_ctas(device);
+  if (ctas_max <= 0) return DQ_ERR_CUDA;
+  // device buffers for all sweeps at once
+  std::vector<ASweepHdr> hdrs;
+  std::vector<AOp> ops;
+  std::vector<double2> pool;
+  std::vector<uint32_t> slot_map;
+  struct SweepRef {
+    size_t hdr, op0, slot0;
+    uint32_t nslots;
+    unsigned grid;
+  };
+  std::vector<SweepRef> refs;
+  size_t max_partial = 1;
+  for (const Seg& s : segs) {
+    if (!s.sweep) continue;
+    ASweepHdr hdr;
+    const size_t op0 = ops.size(), sl0 = slot_map.size();
+    std::vector<AOp> o;
+    DQ_TRY(encode_asweep(s.plan, n, hdr, o, pool, slot_map));
+    for (AOp& a : o) ops.push_back(a);
+    const unsigned grid = (unsigned)std::min<uint64_t>(hdr.ntiles, (uint64_t)ctas_max);
+    refs.push_back(SweepRef{hdrs.size(), op0, sl0, hdr.nslots, grid});
+    max_partial = std::max(max_partial, (size_t)hdr.nslots * grid);
+    hdrs.push_back(hdr);
+  }
+  if (pool.empty()) pool.push_back(make_double2(0, 0));
+  if (slot_map.empty()) slot_map.push_back(0);
+  if (ops.empty()) ops.push_back(AOp{});
+  if (hdrs.empty()) hdrs.push_back(ASweepHdr{});
+  ASweepHdr* d_hdr = nullptr;
+  AOp* d_ops = nullptr;
+  double2* d_pool = nullptr;
+  uint32_t* d_map = nullptr;
+  double* d_part = nullptr;
+  int rc = DQ_OK;
+  auto cu = [&](cudaError_t e, const char* what) {
+    if (e != cudaSuccess && rc == DQ_OK) {
+      cudaGetLastError();
+      rc = fail(e == cudaErrorMemoryAllocation ? DQ_ERR_OOM : DQ_ERR_CUDA,
+                std::string(what) + ": " + cudaGetErrorString(e));
+    }
+  };
+  cu(cudaMallocAsync((void**)&d_hdr, sizeof(ASweepHdr) * hdrs.size(), st), "cudaMallocAsync(hdr)");
+  cu(cudaMallocAsync((void**)&d_ops, sizeof(AOp) * ops.size(), st), "cudaMallocAsync(ops)");
+  cu(cudaMallocAsync((void**)&d_pool, sizeof(double2) * pool.size(), st), "cudaMallocAsync(pool)");
+  cu(cudaMallocAsync((void**)&d_map, sizeof(uint32_t) * slot_map.size(), st), "cudaMallocAsync(map)");
+  cu(cudaMallocAsync((void**)&d_part, sizeof(double) * max_partial, st), "cudaMallocAsync(partials)");
+  if (rc == DQ_OK) {
+    cu(cudaMemcpyAsync(d_hdr, hdrs.data(), sizeof(ASweepHdr) * hdrs.size(), cudaMemcpyHostToDevice, st), "copy");
+    cu(cudaMemcpyAsync(d_ops, ops.data(), sizeof(AOp) * ops.size(), cudaMemcpyHostToDevice, st), "copy");
+    cu(cudaMemcpyAsync(d_pool, pool.data(), sizeof(double2) * pool.size(), cudaMemcpyHostToDevice, st), "copy");
+    cu(cudaMemcpyAsync(d_map, slot_map.data(), sizeof(uint32_t) * slot_map.size(), cudaMemcpyHostToDevice, st), "copy");
+  }
+  size_t si = 0;
+  uint64_t sweeps = 0, pergate = 0;
+  for (const Seg& s : segs) {
+    if (rc != DQ_OK) break;
+    if (!s.sweep) {
+      GateOp op;
+      const dq_inst& in = prog[s.inst];
+      hc u4[4];
+      (void)u4;
+      Gate gt;
+      if (!matrix_nq(in, gt)) {
+        rc = fail(DQ_ERR_INTERNAL, "instruction kind without a matrix");
+        break;
+      }
+      const uint32_t D = 1u << gt.k;
+      std::vector<hc> t(gt.m, gt.m + D * D);
+      for (uint32_t r = 0; r < D; ++r)
+        for (uint32_t c = 0; c < D; ++c) gt.m[r * D + c] = cjh(t[c * D + r]);
+      classify(gt, op);
+      rc = launch_gate(psi, n, op, st, device, nullptr);
+      if (rc == DQ_OK) rc = launch_gate(lam, n, op, st, device, nullptr);
+      ++pergate;
+      continue;
+    }
+    const SweepRef& ref = refs[si++];
+    const ASweepHdr& hdr = hdrs[ref.hdr];
+    const size_t smem = sizeof(double2) * 2 * (1u << hdr.m) + sizeof(double) * std::max<uint32_t>(hdr.nslots, 1) * kAWarps;
+    k_adj_sweep<<<ref.grid, kAThreads, smem, st>>>(psi, lam, d_hdr + ref.hdr, d_ops + ref.op0, d_pool,
+                                                    d_part);
+    cu(cudaGetLastError(), "k_adj_sweep");
+    if (ref.nslots && rc == DQ_OK) {
+      k_adj_slots<<<(ref.nslots + 127) / 128, 128, 0, st>>>(d_part, ref.nslots, ref.grid,
+                                                            d_map + ref.slot0, d_slots);
+      cu(cudaGetLastError(), "k_adj_slots");
+    }
+    ++sweeps;
+  }
+  if (d_hdr) cudaFreeAsync(d_hdr, st);
+  if (d_ops) cudaFreeAsync(d_ops, st);
+  if (d_pool) cudaFreeAsync(d_pool, st);
+  if (d_map) cudaFreeAsync(d_map, st);
+  if (d_part) cudaFreeAsync(d_part, st);
+  if (stats) {
+    stats->sweeps = sweeps;
+    stats->pergate = pergate;
+  }
+  return rc;
+}
+
+}  // namespace dq

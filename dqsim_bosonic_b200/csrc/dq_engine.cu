@@ -246,17 +246,33 @@ __global__ void k_marg_thread(const double2* __restrict__ s, uint64_t nj, uint64
   out[j] = acc;
 }
 
+// One block sums segment `seg` of output j.  Indices whose bits above the
+// lowest marginal qubit c agree form runs of 2^c consecutive amplitudes, so a
+// run's base index is computed once and the run is streamed with four
+// independent partial sums (combined in a fixed order: deterministic).
 __global__ void k_marg_seg(const double2* __restrict__ s, uint64_t nterms, uint32_t nseg,
                            MargParams P, double* __restrict__ partial) {
   const uint64_t j = blockIdx.x / nseg;
   const uint32_t seg = blockIdx.x % nseg;
-  const uint64_t per = (nterms + nseg - 1) / nseg;
+  const uint64_t per = nterms / nseg;  // nseg is a power of two dividing nterms
   const uint64_t r0 = (uint64_t)seg * per;
-  const uint64_t r1 = min(nterms, r0 + per);
   const uint64_t jb = deposit_j(j, P);
-  double acc = 0.0;
-  for (uint64_t r = r0 + threadIdx.x; r < r1; r += blockDim.x)
-    acc = __dadd_rn(acc, norm_sqr_x(s[insert_zeros(r, P.rest.p, P.rest.np) | jb]));
+  const uint32_t c = P.rest.np ? P.rest.p[0] : 63u;
+  const uint64_t run = c >= 63u ? per : (per < (1ULL << c) ? per : (1ULL << c));
+  const uint32_t bd = blockDim.x;
+  double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+  for (uint64_t rb = r0; rb < r0 + per; rb += run) {
+    const double2* src = s + (insert_zeros(rb, P.rest.p, P.rest.np) | jb);
+    uint64_t off = threadIdx.x;
+    for (; off + 3ULL * bd < run; off += 4ULL * bd) {
+      a0 = __dadd_rn(a0, norm_sqr_x(src[off]));
+      a1 = __dadd_rn(a1, norm_sqr_x(src[off + bd]));
+      a2 = __dadd_rn(a2, norm_sqr_x(src[off + 2ULL * bd]));
+      a3 = __dadd_rn(a3, norm_sqr_x(src[off + 3ULL * bd]));
+    }
+    for (; off < run; off += bd) a0 = __dadd_rn(a0, norm_sqr_x(src[off]));
+  }
+  double acc = __dadd_rn(__dadd_rn(a0, a1), __dadd_rn(a2, a3));
   acc = block_sum(acc);
   if (threadIdx.x == 0) partial[blockIdx.x] = acc;
 }
@@ -521,11 +537,11 @@ int launch_marginal(const double2* s, uint32_t n, const uint32_t* qubits, uint32
   if (nterms <= 64 || nj >= (uint64_t)sms * 1024) {
     k_marg_thread<<<blocks_for(nj, kThreads), kThreads, 0, st>>>(s, nj, nterms, P, d_out);
   } else {
-    uint64_t target_blocks = (uint64_t)sms * 8;
-    uint64_t nseg = (target_blocks + nj - 1) / nj;
-    const uint64_t max_seg = (nterms + kRedThreads - 1) / kRedThreads;
-    if (nseg > max_seg) nseg = max_seg;
-    if (nseg < 1) nseg = 1;
+    // a power of two number of segments per output (dividing nterms), about
+    // 8 blocks per SM in total, each segment at least one block's worth
+    const uint64_t target_blocks = (uint64_t)sms * 8;
+    uint64_t nseg = 1;
+    while (nj * nseg * 2 <= target_blocks && nseg * 2 * kRedThreads <= nterms) nseg <<= 1;
     while (nj * nseg > (uint64_t)kPartials && nseg > 1) nseg >>= 1;
     double* partial = sc.d_partial;
     double* tmp = nullptr;

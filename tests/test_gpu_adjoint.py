@@ -193,3 +193,55 @@ def test_batched_adjoint_matches_single_sets_and_drives_adam(gpu):
         opt.step()
         energies.append(e.detach().clone())
     assert energies[-1].sum() < energies[0].sum()
+
+
+def mixed_param_circuit(n, depth, seed):
+    """Random gates of every kind the ParamCircuit takes (three- to
+    five-qubit gates included), every angle of the parametrised ones
+    trainable."""
+    from dqsim_bosonic_b200.adjoint import _PARAM_COUNT, _QUBITS
+
+    rng = np.random.default_rng(seed)
+    kinds = [k for k, q in _QUBITS.items() if q <= n]
+    c = ParamCircuit(n)
+    k = 0
+    for _ in range(depth):
+        kind = kinds[rng.integers(len(kinds))]
+        qs = [int(v) for v in rng.permutation(n)[:_QUBITS[kind]]]
+        npar = _PARAM_COUNT.get(kind, 0)
+        c.add(kind, qs, [Param(k + j) for j in range(npar)])
+        k += npar
+    theta = rng.uniform(-np.pi, np.pi, size=k)
+    return c, theta
+
+
+@pytest.mark.parametrize("n,seed", [(13, 1), (16, 2), (7, 3)])
+def test_fused_backward_matches_per_gate_backward(gpu, n, seed):
+    c, theta = mixed_param_circuit(n, 160, seed)
+    H = random_observable(n, 12, seed=seed + 10)
+    e1, g1 = adjoint_gradient(c, theta, H, exec="fused")
+    e2, g2 = adjoint_gradient(c, theta, H, exec="per_gate")
+    assert abs(e1 - e2) < 1e-12
+    assert np.max(np.abs(g1 - g2)) < 1e-11, np.max(np.abs(g1 - g2))
+    sub = list(range(0, theta.size, max(1, theta.size // 12)))
+    ps = orc.param_shift(c, theta, H.array(), occurrences=sub)
+    assert np.max(np.abs(g1[sub] - ps[sub])) < TOL_SHIFT
+    from dqsim_bosonic_b200 import adjoint as adj
+
+    v = adj._state(n, 0).download()
+    assert abs(v[0] - 1.0) < 1e-10 and np.max(np.abs(v[1:])) < 1e-10
+
+
+@pytest.mark.parametrize("angle", [0.0, np.pi, -np.pi / 2])
+def test_special_angles_keep_their_derivatives(gpu, angle):
+    # at these angles some gates are diagonal or the identity while their
+    # derivatives are not: the fused planner must not treat them as diagonal
+    c, theta = every_kind_circuit(12)
+    theta = np.full_like(theta, angle)
+    H = random_observable(12, 10, seed=4)
+    e1, g1 = adjoint_gradient(c, theta, H, exec="fused")
+    e2, g2 = adjoint_gradient(c, theta, H, exec="per_gate")
+    assert abs(e1 - e2) < 1e-12
+    ps = orc.param_shift(c, theta, H.array())
+    assert np.max(np.abs(g1 - ps)) < TOL_SHIFT
+    assert np.max(np.abs(g2 - ps)) < TOL_SHIFT
