@@ -44,8 +44,18 @@ def trajectories_resident(prog, base_seed: int, shots: int, device: int = 0, *, 
                                base_seed & _U64, int(shot0), int(shots),
                                nat.ptr(out) if out.size else None, prog.cbit_space,
                                ctypes.byref(o), ctypes.byref(st))
-    nat.check(rc, "dq_run_trajectories")
+    _check_traj(rc, prog, st, "dq_run_trajectories")
     return out, st
+
+
+def _check_traj(rc: int, prog, st, what: str) -> None:
+    """Unsupported generic gates surface as the shot path's RuntimeError
+    with the reference's message; other failures as in nat.check."""
+    if rc == nat.DQ_ERR_UNSUPPORTED and st.failed_inst >= 0:
+        from .statevector import _unsupported_message
+
+        raise RuntimeError(_unsupported_message(prog, st.failed_inst & ((1 << 40) - 1)))
+    nat.check(rc, what)
 
 
 def run_trajectories(prog, base_seed: int, shots: int, device: int, want_times: bool = False,
@@ -110,8 +120,15 @@ def run_batch(progs, seeds, device: int = 0, *, want_states: bool = False, opts=
         it.state_out = nat.ptr(sv) if sv is not None else None
     st = nat.TrajStats()
     o = opts if opts is not None else _opts()
-    nat.check(nat.lib().dq_run_batch(int(device), ctypes.addressof(items), len(progs),
-                                     ctypes.byref(o), ctypes.byref(st)), "dq_run_batch")
+    rc = nat.lib().dq_run_batch(int(device), ctypes.addressof(items), len(progs),
+                                ctypes.byref(o), ctypes.byref(st))
+    if rc == nat.DQ_ERR_UNSUPPORTED and st.failed_inst >= 0:
+        from .statevector import _unsupported_message
+
+        k = st.failed_inst >> 40
+        raise RuntimeError(f"batch item {k}: " +
+                           _unsupported_message(progs[k], st.failed_inst & ((1 << 40) - 1)))
+    nat.check(rc, "dq_run_batch")
     return cbits, (states if want_states else None), st
 
 
@@ -139,9 +156,9 @@ class TrajectoryPlan:
             raise ValueError("plan was released")
         out = np.empty((self.shots, self.prog.cbit_space), dtype=np.int32)
         st = nat.TrajStats()
-        nat.check(nat.lib().dq_traj_plan_run(self._h, base_seed & _U64,
-                                             nat.ptr(out) if out.size else None,
-                                             ctypes.byref(st)), "dq_traj_plan_run")
+        rc = nat.lib().dq_traj_plan_run(self._h, base_seed & _U64,
+                                        nat.ptr(out) if out.size else None, ctypes.byref(st))
+        _check_traj(rc, self.prog, st, "dq_traj_plan_run")
         return out, st
 
     def release(self) -> None:

@@ -47,7 +47,8 @@ constexpr uint32_t kAMaxLocal = 11;
 constexpr uint32_t kAMaxOps = 192;
 constexpr uint32_t kAMaxSlots = 192;
 
-enum AType : uint8_t { A_ONE = 1, A_TWO = 2, A_DIAG = 3, A_DRUN = 4 };
+enum AType : uint8_t { A_ONE = 1, A_TWO = 2, A_DIAG = 3, A_DRUN = 4, A_PHASE = 5 };
+constexpr uint32_t kAPhaseOps = 16;  // ops of one register phase
 constexpr uint32_t kADiagRun = 16;  // diagonal ops applied in one elementwise pass
 
 struct AOp {
@@ -306,6 +307,134 @@ __device__ __noinline__ void op_drun(double2* sp, double2* sl, const AOp* sub, u
   }
 }
 
+// One op of a register phase staged in shared memory.
+struct PSub {
+  double2 v[4];      // one-qubit: U^dagger; diagonal: conj(diag)
+  double2 d[4][4];   // derivatives (one-qubit: np 2x2; diagonal: d[0] = diag)
+  uint32_t kind;     // 0: one-qubit on phase bit pb; 1: diagonal
+  uint32_t pb;       // one-qubit: index of the target among the phase bits
+  uint32_t np, slot;
+  uint32_t lm0, lm1, fixed, b0;  // diagonal: as in DSub
+};
+
+template <int PB>
+__device__ __forceinline__ void phase_one(double2 (&a)[8], double2 (&b)[8], const PSub& P,
+                                          double (&acc)[4]) {
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    if (i & (1 << PB)) continue;
+    const int j = i | (1 << PB);
+    const double2 a0 = a[i], a1 = a[j], b0 = b[i], b1 = b[j];
+    const double2 p0 = cfma2(P.v[1], a1, cmul2(P.v[0], a0));
+    const double2 p1 = cfma2(P.v[3], a1, cmul2(P.v[2], a0));
+    a[i] = p0;
+    a[j] = p1;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      if (q < (int)P.np) {
+        const double2 w0 = cfma2(P.d[q][1], p1, cmul2(P.d[q][0], p0));
+        const double2 w1 = cfma2(P.d[q][3], p1, cmul2(P.d[q][2], p0));
+        acc[q] = redot(b0, w0, redot(b1, w1, acc[q]));
+      }
+    }
+    b[i] = cfma2(P.v[1], b1, cmul2(P.v[0], b0));
+    b[j] = cfma2(P.v[3], b1, cmul2(P.v[2], b0));
+  }
+}
+
+// A register phase: every thread holds the 8 amplitudes of psi and lambda
+// that differ in the phase's three local bits and applies the phase's
+// one-qubit ops (on those bits) and diagonal ops (on any qubits) in order.
+// Each op's gradient terms are reduced per warp right after the op (all
+// lanes take part: the group loop runs the same trip count on every thread).
+__device__ __noinline__ void op_phase(double2* sp, double2* sl, const AOp& hdr, const AOp* sub,
+                                      const double2* pool, uint32_t m, uint64_t base,
+                                      double* accw, PSub* ps) {
+  const uint32_t cnt = hdr.cnt;
+  const uint32_t pbits[3] = {hdr.lt, hdr.lt2, (uint32_t)hdr.dq[0]};
+  if (threadIdx.x < cnt) {
+    const AOp op = sub[threadIdx.x];
+    PSub& P = ps[threadIdx.x];
+    const double2* mt = pool + op.mat;
+    P.np = op.np;
+    P.slot = op.slot;
+    if (op.type == A_ONE) {
+      P.kind = 0;
+      P.pb = op.lt == pbits[0] ? 0u : (op.lt == pbits[1] ? 1u : 2u);
+      for (int i = 0; i < 4; ++i) P.v[i] = mt[i];
+      for (uint32_t q = 0; q < op.np; ++q)
+        for (int i = 0; i < 4; ++i) P.d[q][i] = mt[4 + 4 * q + i];
+    } else {
+      P.kind = 1;
+      P.lm0 = P.lm1 = P.fixed = 0;
+      P.b0 = op.ndq == 2 ? 2u : 1u;
+      for (uint32_t a = 0; a < op.ndq; ++a) {
+        const uint32_t e = op.dq[a];
+        const uint32_t bitv = (a == 0) ? P.b0 : 1u;
+        if (e & 0x80u) {
+          if (a == 0) P.lm0 = 1u << (e & 0x7fu);
+          else P.lm1 = 1u << (e & 0x7fu);
+        } else if ((base >> (e & 0x7fu)) & 1ULL) {
+          P.fixed |= bitv;
+        }
+      }
+      for (int i = 0; i < 4; ++i) P.v[i] = mt[i];
+      for (int i = 0; i < 4; ++i) P.d[0][i] = op.np ? mt[4 + i] : make_double2(0.0, 0.0);
+    }
+  }
+  __syncthreads();
+  const uint32_t groups = (1u << m) >> 3;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  for (uint32_t g0 = 0; g0 < groups; g0 += kAThreads) {
+    const uint32_t g = g0 + threadIdx.x;
+    const bool valid = g < groups;
+    const uint32_t ob = ins0a(ins0a(ins0a(valid ? g : 0u, pbits[0]), pbits[1]), pbits[2]);
+    uint32_t off[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+      off[i] = ob | ((i & 1) ? 1u << pbits[0] : 0u) | ((i & 2) ? 1u << pbits[1] : 0u) |
+               ((i & 4) ? 1u << pbits[2] : 0u);
+    double2 a[8], b[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      a[i] = valid ? sp[off[i]] : make_double2(0.0, 0.0);
+      b[i] = valid ? sl[off[i]] : make_double2(0.0, 0.0);
+    }
+#pragma unroll 1
+    for (uint32_t u = 0; u < cnt; ++u) {
+      const PSub& P = ps[u];
+      double acc[4] = {0.0, 0.0, 0.0, 0.0};
+      if (P.kind == 0) {
+        if (P.pb == 0) phase_one<0>(a, b, P, acc);
+        else if (P.pb == 1) phase_one<1>(a, b, P, acc);
+        else phase_one<2>(a, b, P, acc);
+      } else {
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+          const uint32_t o = off[i];
+          const uint32_t e = P.fixed | ((o & P.lm0) ? P.b0 : 0u) | ((o & P.lm1) ? 1u : 0u);
+          const double2 vv = P.v[e];
+          const double2 p = cmul2(vv, a[i]);
+          if (P.np) acc[0] = redot(b[i], cmul2(P.d[0][e], p), acc[0]);
+          b[i] = cmul2(vv, b[i]);
+          a[i] = p;
+        }
+      }
+      for (uint32_t q = 0; q < P.np; ++q) {
+        const double v = warp_sum_d(acc[q]);
+        if (lane == 0) accw[(P.slot + q) * kAWarps + w] += v;
+      }
+    }
+    if (valid) {
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        sp[off[i]] = a[i];
+        sl[off[i]] = b[i];
+      }
+    }
+  }
+}
+
 __global__ void __launch_bounds__(kAThreads, 2)
     k_adj_sweep(double2* __restrict__ psi, double2* __restrict__ lam, const ASweepHdr* __restrict__ hp,
                 const AOp* __restrict__ ops, const double2* __restrict__ pool, double* partial) {
@@ -313,6 +442,7 @@ __global__ void __launch_bounds__(kAThreads, 2)
   __shared__ ASweepHdr H;
   __shared__ uint64_t hi_tab[64];
   __shared__ DSub dsub[kADiagRun];
+  __shared__ PSub psub[kAPhaseOps];
   if (threadIdx.x == 0) H = *hp;
   __syncthreads();
   const uint32_t m = H.m, L = 1u << m;
@@ -346,6 +476,12 @@ __global__ void __launch_bounds__(kAThreads, 2)
       const AOp op = ops[i];
       if (op.type == A_DRUN) {
         op_drun(sp, sl, ops + i + 1, op.cnt, pool, m, base, accw, dsub);
+        i += op.cnt;
+        __syncthreads();
+        continue;
+      }
+      if (op.type == A_PHASE) {
+        op_phase(sp, sl, op, ops + i + 1, pool, m, base, accw, psub);
         i += op.cnt;
         __syncthreads();
         continue;
@@ -627,9 +763,67 @@ int encode_asweep(const ASweepPlan& sp, uint32_t n, ASweepHdr& hdr, std::vector<
     }
     ops.push_back(op);
   }
+  // register phases: maximal runs of uncontrolled one-qubit ops (targets
+  // within three local bits) and diagonal ops, with at least one one-qubit op
+  if (m >= 3) {
+    std::vector<AOp> phased;
+    size_t i = 0;
+    while (i < ops.size()) {
+      const AOp& o = ops[i];
+      const bool one = o.type == A_ONE && o.lctrl == 0 && o.sel < 0;
+      if (!one && o.type != A_DIAG) {
+        phased.push_back(ops[i++]);
+        continue;
+      }
+      uint32_t bits[3];
+      uint32_t nb = 0;
+      size_t j = i;
+      uint32_t nones = 0;
+      while (j < ops.size() && j - i < kAPhaseOps) {
+        const AOp& q = ops[j];
+        if (q.type == A_DIAG) { ++j; continue; }
+        if (!(q.type == A_ONE && q.lctrl == 0 && q.sel < 0)) break;
+        bool have = false;
+        for (uint32_t b = 0; b < nb; ++b) have = have || bits[b] == q.lt;
+        if (!have) {
+          if (nb == 3) break;
+          bits[nb++] = q.lt;
+        }
+        ++nones;
+        ++j;
+      }
+      if (nones == 0) {  // diagonal ops only: left to the diagonal runs
+        for (size_t k = i; k < j; ++k) phased.push_back(ops[k]);
+        i = j;
+        continue;
+      }
+      // three distinct phase bits: fill with other local bits
+      for (uint32_t b = 0; nb < 3 && b < m; ++b) {
+        bool have = false;
+        for (uint32_t c = 0; c < nb; ++c) have = have || bits[c] == b;
+        if (!have) bits[nb++] = b;
+      }
+      std::sort(bits, bits + 3);
+      AOp h{};
+      h.type = A_PHASE;
+      h.cnt = (uint8_t)(j - i);
+      h.lt = (uint8_t)bits[0];
+      h.lt2 = (uint8_t)bits[1];
+      h.dq[0] = (uint8_t)bits[2];
+      phased.push_back(h);
+      for (size_t k = i; k < j; ++k) phased.push_back(ops[k]);
+      i = j;
+    }
+    ops.swap(phased);
+  }
   // runs of consecutive diagonal ops become one A_DRUN header + the ops
   std::vector<AOp> grouped;
   for (size_t i = 0; i < ops.size();) {
+    if (ops[i].type == A_PHASE) {
+      const size_t e = i + 1 + ops[i].cnt;
+      for (; i < e; ++i) grouped.push_back(ops[i]);
+      continue;
+    }
     if (ops[i].type != A_DIAG) {
       grouped.push_back(ops[i++]);
       continue;

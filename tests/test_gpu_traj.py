@@ -139,8 +139,10 @@ def test_ragged_batch_states_and_cbits(gpu):
 def test_unsupported_gate_reached(gpu):
     circ = JsonCircuit(5, [g("h", 0), _circuits.gate("mystery_gate", [0, 1])])
     prog = prog_of(circ)
-    with pytest.raises(nat.UnsupportedGate):
+    with pytest.raises(RuntimeError, match='Unsupported generic gate: "mystery_gate"'):
         trajectories_resident(prog, 1, 4)
+    with pytest.raises(RuntimeError, match='batch item 1: Unsupported generic gate'):
+        run_batch([prog_of(JsonCircuit(3, [g("h", 0)])), prog], [1, 2])
 
 
 def test_rejects_bad_arguments(gpu):
