@@ -50,7 +50,9 @@ constexpr int kMaxTB = 8;
 constexpr int kMaxM = 12;
 constexpr int kMaxSlots = 128;
 // bytes of one sweep program (staged in shared memory next to two tile buffers)
-__host__ __device__ constexpr int max_prog(int tb) { return tb >= 8 ? 64 * 1024 : 40 * 1024; }
+// Largest staged sweep program for a tile of 2^m amplitudes: what is left of
+// shared memory next to two tile buffers at the CTAs per SM the geometry runs.
+__host__ __device__ constexpr int max_prog(int m) { return m >= 12 ? 64 * 1024 : 40 * 1024; }
 
 enum : uint32_t { OP_U1 = 0, OP_U1R, OP_U1X, OP_U2, OP_FLUSH_R, OP_FLUSH_T, OP_GPHASE, OP_U1H,
                   OP_SCALE };
@@ -299,8 +301,12 @@ __device__ __forceinline__ void exec_op(const uint4 o0, const uint4 o1, double2 
 // One persistent CTA per SM walks tiles blockIdx.x, + gridDim.x, ...: the
 // next tile is prefetched (cp.async into the second buffer) while the
 // current one is computed.
-template <int TB, int RB>
-__global__ void __launch_bounds__(1 << TB, (TB == 7 ? 2 : 1))
+// S tile buffers form a cp.async pipeline with S - 1 tiles prefetched while
+// the current one is computed.  S = 2: two CTAs per SM whenever a tile is at
+// most 2^11 amplitudes; S = 1 (128 threads): no prefetch, three CTAs per SM
+// overlap each other's loads instead.
+template <int TB, int RB, int S>
+__global__ void __launch_bounds__(1 << TB, (S == 1 && TB == 7 ? 3 : (TB + RB <= 11 ? 2 : 1)))
     k_sweep(double2* __restrict__ state, const uint8_t* __restrict__ gprog, uint32_t prog_bytes,
             uint32_t ntiles) {
   constexpr int kSwThreads = 1 << TB;
@@ -311,9 +317,8 @@ __global__ void __launch_bounds__(1 << TB, (TB == 7 ? 2 : 1))
   constexpr int NI = 1 << (M - kSwTB);  // runs of 32 per warp
   constexpr uint32_t NW = 1u << (TB - 5);  // warps
   extern __shared__ __align__(16) unsigned char smraw[];
-  double2* buf0 = reinterpret_cast<double2*>(smraw);
-  double2* buf1 = buf0 + T;
-  double2* slots = buf1 + T;
+  double2* bufs = reinterpret_cast<double2*>(smraw);  // S tiles
+  double2* slots = bufs + S * T;
   uint8_t* prog = reinterpret_cast<uint8_t*>(slots + kMaxSlots);
   const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
 
@@ -335,26 +340,30 @@ __global__ void __launch_bounds__(1 << TB, (TB == 7 ? 2 : 1))
     for (int k = 0; k < M; ++k) b = insert_zero(b, H->local_pos[k]);
     return b;
   };
-  // run r = warp + 8 i: all of a tile's 2^(m-5) runs of 32 amplitudes
-  auto load_tile = [&](uint64_t base, double2* dst) {
+  // run r = warp + 8 i: all of a tile's 2^(m-5) runs of 32 amplitudes; one
+  // commit group per call (empty past the last tile, so the group count is
+  // uniform)
+  auto load_tile = [&](uint32_t t, double2* dst) {
+    if (t < ntiles) {
+      const uint64_t b = tile_base(t);
 #pragma unroll
-    for (int i = 0; i < NI; ++i) {
-      const uint32_t r = warp + (uint32_t)i * NW;
-      cp_async16(&dst[H->runswz[r] ^ swl], state + (base + H->runoff[r] + lane));
+      for (int i = 0; i < NI; ++i) {
+        const uint32_t r = warp + (uint32_t)i * NW;
+        cp_async16(&dst[H->runswz[r] ^ swl], state + (b + H->runoff[r] + lane));
+      }
     }
     cp_async_commit();
   };
 
   uint32_t tile = blockIdx.x;
-  uint64_t base = (tile < ntiles) ? tile_base(tile) : 0;
-  if (tile < ntiles) load_tile(base, buf0);
+#pragma unroll
+  for (int k = 0; k < S - 1; ++k) load_tile(tile + (uint32_t)k * gridDim.x, bufs + k * T);
   for (uint32_t it = 0; tile < ntiles; ++it, tile += gridDim.x) {
-    double2* cur = (it & 1u) ? buf1 : buf0;
-    double2* nxt = (it & 1u) ? buf0 : buf1;
-    const uint32_t ntile = tile + gridDim.x;
-    const bool has_next = ntile < ntiles;
-    const uint64_t nbase = has_next ? tile_base(ntile) : 0;
-    if (has_next) load_tile(nbase, nxt);
+    double2* cur = bufs + (it % S) * T;
+    // tile it + S - 1 goes into the buffer that tile it - 1 used (stored and
+    // released by the barrier that ended the previous iteration)
+    load_tile(tile + (uint32_t)(S - 1) * gridDim.x, bufs + ((it + S - 1) % S) * T);
+    const uint64_t base = tile_base(tile);
     for (uint32_t s = tid; s < nslots; s += kSwThreads) {
       double2 w = SL[s].w0;
       const uint32_t c = SL[s].count, st = SL[s].start;
@@ -364,7 +373,7 @@ __global__ void __launch_bounds__(1 << TB, (TB == 7 ? 2 : 1))
       }
       slots[s] = w;
     }
-    if (has_next) cp_async_wait<1>(); else cp_async_wait<0>();
+    cp_async_wait<S - 1>();  // this tile's group is complete; S - 1 newer may be pending
     __syncthreads();
 
     for (uint32_t p = 0; p < nph; ++p) {
@@ -419,8 +428,8 @@ __global__ void __launch_bounds__(1 << TB, (TB == 7 ? 2 : 1))
       state[base + H->runoff[r] + lane] = cur[H->runswz[r] ^ swl];
     }
     __syncthreads();
-    base = nbase;
   }
+  cp_async_wait<0>();
 }
 
 // ---- relabel materialisation: paired-tile involution of bit positions ------------
@@ -654,7 +663,7 @@ struct Planner {
         }
         const size_t gb = 48 + 16 * 16 + flush_bytes * (size_t)__builtin_popcountll(need);
         const bool fits = (uint32_t)__builtin_popcountll(ns) <= M && nd_count < max_ops &&
-                          bytes + gb <= (size_t)max_prog((int)TB) - 8192;
+                          bytes + gb <= (size_t)max_prog((int)M) - 8192;
         const bool afford = single_tile || !any_nd || cost + c <= budget;
         if (!fits || !afford) {
           next.push_back(gi);
@@ -1069,7 +1078,7 @@ int encode_sweep(const PSweep& sw, const std::vector<PGate>& G, uint32_t TBn, ui
   blob.align16();
   hp = reinterpret_cast<SwHeader*>(blob.buf.data() + hoff);
   hp->prog_bytes = (uint32_t)(blob.buf.size() - hoff);
-  if (hp->prog_bytes > (uint32_t)max_prog(kSwTB)) return fail(DQ_ERR_INTERNAL, "sweep program too large");
+  if (hp->prog_bytes > (uint32_t)max_prog((int)m)) return fail(DQ_ERR_INTERNAL, "sweep program too large");
   *offset = hoff;
   return DQ_OK;
 }
@@ -1209,12 +1218,12 @@ bool convert_inst(const dq_inst& in, const uint32_t* perm, std::vector<PGate>& o
   }
 }
 
-template <int TB, int RB>
-int launch_sweep_rb(double2* amp, uint32_t n, const uint8_t* dblob, uint32_t prog_bytes,
-                    cudaStream_t st) {
+template <int TB, int RB, int S>
+int launch_sweep_s(double2* amp, uint32_t n, const uint8_t* dblob, uint32_t prog_bytes,
+                   cudaStream_t st) {
   constexpr int M = TB + RB;
-  const size_t smem_max = sizeof(double2) * (2 * (1u << M) + kMaxSlots) + max_prog(TB);
-  const size_t smem = sizeof(double2) * (2 * (1u << M) + kMaxSlots) + prog_bytes;
+  const size_t smem_max = sizeof(double2) * (S * (1u << M) + kMaxSlots) + max_prog(M);
+  const size_t smem = sizeof(double2) * (S * (1u << M) + kMaxSlots) + prog_bytes;
   // per device, once: opt-in shared memory and resident CTAs per SM (the
   // mutex makes the first launches from concurrent host threads safe)
   static std::mutex mu;
@@ -1225,10 +1234,11 @@ int launch_sweep_rb(double2* amp, uint32_t n, const uint8_t* dblob, uint32_t pro
   {
     std::lock_guard<std::mutex> lk(mu);
     if (per_sm[dev & 63] == 0) {
-      DQ_CUDA_TRY(cudaFuncSetAttribute(k_sweep<TB, RB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)smem_max));
+      DQ_CUDA_TRY(cudaFuncSetAttribute(k_sweep<TB, RB, S>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_max));
       int b = 1;
-      DQ_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_sweep<TB, RB>, 1 << TB, smem_max));
+      DQ_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_sweep<TB, RB, S>, 1 << TB,
+                                                                smem_max));
       per_sm[dev & 63] = b < 1 ? 1 : b;
     }
     resident = per_sm[dev & 63];
@@ -1237,9 +1247,24 @@ int launch_sweep_rb(double2* amp, uint32_t n, const uint8_t* dblob, uint32_t pro
   DQ_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
   const uint64_t tiles = 1ULL << (n - M);
   const unsigned grid = (unsigned)std::min<uint64_t>(tiles, (uint64_t)sms * resident);
-  k_sweep<TB, RB><<<grid, 1 << TB, smem, st>>>(amp, dblob, prog_bytes, (uint32_t)tiles);
+  k_sweep<TB, RB, S><<<grid, 1 << TB, smem, st>>>(amp, dblob, prog_bytes, (uint32_t)tiles);
   DQ_CUDA_TRY(cudaGetLastError());
   return DQ_OK;
+}
+
+template <int TB, int RB>
+int launch_sweep_rb(double2* amp, uint32_t n, const uint8_t* dblob, uint32_t prog_bytes,
+                    cudaStream_t st) {
+  // default: single-buffered tiles, three 128-thread CTAs per SM (measured
+  // faster than two double-buffered CTAs: the extra warps hide more of the
+  // per-op latency than the prefetch saves); DQSIM_SWEEP_STAGES=2 selects
+  // double buffering
+  static const int stages = [] {
+    const char* e = getenv("DQSIM_SWEEP_STAGES");
+    return (e && atoi(e) == 2) ? 2 : 1;
+  }();
+  if (TB == 7 && stages == 1) return launch_sweep_s<7, RB, 1>(amp, n, dblob, prog_bytes, st);
+  return launch_sweep_s<TB, RB, 2>(amp, n, dblob, prog_bytes, st);
 }
 
 int launch_sweep(double2* amp, uint32_t n, uint32_t TB, uint32_t RB, const uint8_t* dblob,
