@@ -88,6 +88,27 @@ __device__ __forceinline__ uint32_t ins0a(uint32_t k, uint32_t p) {
   return ((k >> p) << (p + 1)) | (k & ((1u << p) - 1u));
 }
 
+// Shared-memory layout of a tile: element o lives at swz(o).  The low three
+// index bits are XORed with a fold of the higher ones, so eight threads whose
+// elements differ only in higher bits (register phases over low qubits,
+// strided pairs) hit eight different 128-byte bank rows.  A bijection on
+// [0, 2^m) for every m.
+__device__ __forceinline__ uint32_t swz(uint32_t o) {
+  return o ^ (((o >> 3) ^ (o >> 6) ^ (o >> 9)) & 7u);
+}
+
+__device__ __forceinline__ void cp_async16a(void* smem, const void* gmem) {
+  const uint32_t sa = (uint32_t)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+
+// x[e] for a run-time e in 0..3 without indexing a local array
+__device__ __forceinline__ double2 sel4(const double2 (&x)[4], uint32_t e) {
+  const double2 lo = (e & 1u) ? x[1] : x[0];
+  const double2 hi = (e & 1u) ? x[3] : x[2];
+  return (e & 2u) ? hi : lo;
+}
+
 __device__ __forceinline__ double warp_sum_d(double v) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
@@ -140,7 +161,8 @@ __device__ __noinline__ void op_one(double2* sp, double2* sl, const AOp& op, con
       for (int p = 0; p < npos; ++p) o = ins0a(o, pos[p]);
       o |= op.lctrl;
     }
-    const uint32_t o1 = o | tb;
+    const uint32_t o1 = swz(o | tb);
+    o = swz(o);
     const double2 a0 = sp[o], a1 = sp[o1], b0 = sl[o], b1 = sl[o1];
     const double2 p0 = cfma2(v[1], a1, cmul2(v[0], a0));
     const double2 p1 = cfma2(v[3], a1, cmul2(v[2], a0));
@@ -168,7 +190,7 @@ __device__ __noinline__ void op_two(double2* sp, double2* sl, const AOp& op, con
   double acc[4] = {0.0, 0.0, 0.0, 0.0};
   for (uint32_t k = threadIdx.x; k < count; k += kAThreads) {
     const uint32_t b = ins0a(ins0a(k, p0), p1);
-    const uint32_t idx[4] = {b, b | bb, b | ba, b | ba | bb};
+    const uint32_t idx[4] = {swz(b), swz(b | bb), swz(b | ba), swz(b | ba | bb)};
     double2 x[4], y[4], p[4];
 #pragma unroll
     for (int r = 0; r < 4; ++r) {
@@ -228,12 +250,13 @@ __device__ __noinline__ void op_diag(double2* sp, double2* sl, const AOp& op, co
     uint32_t e = fixed;
     if (lmask[0] && (o & lmask[0])) e |= 1u << sh0;
     if (lmask[1] && (o & lmask[1])) e |= 1u;
-    const double2 a = sp[o], b = sl[o];
+    const uint32_t so = swz(o);
+    const double2 a = sp[so], b = sl[so];
     const double2 p = cmul2(v[e], a);
-    sp[o] = p;
+    sp[so] = p;
 #pragma unroll
     for (int j = 0; j < NP; ++j) acc[j] = redot(b, cmul2(d[j][e], p), acc[j]);
-    sl[o] = cmul2(v[e], b);
+    sl[so] = cmul2(v[e], b);
   }
   flush_acc<NP>(acc, accw, op.slot);
 }
@@ -241,7 +264,7 @@ __device__ __noinline__ void op_diag(double2* sp, double2* sl, const AOp& op, co
 // One diagonal op staged in shared memory for a run.
 struct DSub {
   double2 v[4];
-  double2 d[4];
+  double2 d[4];       // v[e] * dU[e]: the gradient weight of entry e
   uint32_t lm0, lm1;  // local bit masks of the MSB / LSB qubit (0: not local)
   uint32_t fixed;     // index bits from non-local qubits (tile constant)
   uint32_t b0;        // value of the MSB in the entry index (2 or 1)
@@ -271,38 +294,64 @@ __device__ __noinline__ void op_drun(double2* sp, double2* sl, const AOp* sub, u
     }
     const double2* mt = pool + op.mat;
     for (int i = 0; i < 4; ++i) D.v[i] = mt[i];
-    for (int i = 0; i < 4; ++i) D.d[i] = op.np ? mt[4 + i] : make_double2(0.0, 0.0);
+    for (int i = 0; i < 4; ++i)
+      D.d[i] = op.np ? cmul2(mt[i], mt[4 + i]) : make_double2(0.0, 0.0);
     D.np = op.np;
     D.slot = op.slot;
   }
   __syncthreads();
+  // Every entry of a unitary diagonal has modulus 1, so z = conj(lambda) psi
+  // is the same before every op of the run, and op k's gradient term is
+  // Re(conj(lambda_k) dU_k V_k psi_k) = Re(z (V_k dU_k)[e]); psi and lambda
+  // then take the product of the run's phases once.  Ops are the outer loop
+  // (their parameters sit in registers), each thread's 8 elements the inner.
   const uint32_t L = 1u << m;
-  double acc[kADiagRun];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  for (uint32_t o0 = 0; o0 < L; o0 += 8u * kAThreads) {
+    uint32_t oo[8];
+    double2 z[8], ph[8];
 #pragma unroll
-  for (int u = 0; u < (int)kADiagRun; ++u) acc[u] = 0.0;
-  for (uint32_t o = threadIdx.x; o < L; o += kAThreads) {
-    double2 a = sp[o], b = sl[o];
+    for (int i = 0; i < 8; ++i) {
+      oo[i] = o0 + threadIdx.x + (uint32_t)i * kAThreads;
+      double2 zz = make_double2(0.0, 0.0);
+      if (oo[i] < L) {
+        const uint32_t so = swz(oo[i]);
+        const double2 a = sp[so], b = sl[so];
+        zz = make_double2(fma(b.x, a.x, b.y * a.y), fma(b.x, a.y, -b.y * a.x));
+      }
+      z[i] = zz;
+      ph[i] = make_double2(1.0, 0.0);
+    }
+#pragma unroll 1
+    for (uint32_t u = 0; u < cnt; ++u) {
+      double2 v[4], dw[4];
 #pragma unroll
-    for (int u = 0; u < (int)kADiagRun; ++u) {
-      if (u < (int)cnt) {
-        const DSub& D = ds[u];
-        const uint32_t e = D.fixed | ((o & D.lm0) ? D.b0 : 0u) | ((o & D.lm1) ? 1u : 0u);
-        const double2 vv = D.v[e];
-        const double2 p = cmul2(vv, a);
-        if (D.np) acc[u] = redot(b, cmul2(D.d[e], p), acc[u]);
-        b = cmul2(vv, b);
-        a = p;
+      for (int k = 0; k < 4; ++k) {
+        v[k] = ds[u].v[k];
+        dw[k] = ds[u].d[k];
+      }
+      const uint32_t fixed = ds[u].fixed, lm0 = ds[u].lm0, lm1 = ds[u].lm1, b0 = ds[u].b0;
+      const uint32_t np = ds[u].np;
+      double acc = 0.0;
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        const uint32_t e = fixed | ((oo[i] & lm0) ? b0 : 0u) | ((oo[i] & lm1) ? 1u : 0u);
+        ph[i] = cmul2(sel4(v, e), ph[i]);
+        const double2 wv = sel4(dw, e);
+        acc = fma(z[i].x, wv.x, fma(-z[i].y, wv.y, acc));
+      }
+      if (np) {
+        const double t = warp_sum_d(acc);
+        if (lane == 0) accw[ds[u].slot * kAWarps + w] += t;
       }
     }
-    sp[o] = a;
-    sl[o] = b;
-  }
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
 #pragma unroll
-  for (int u = 0; u < (int)kADiagRun; ++u) {
-    if (u < (int)cnt && ds[u].np) {
-      const double v = warp_sum_d(acc[u]);
-      if (lane == 0) accw[ds[u].slot * kAWarps + w] += v;
+    for (int i = 0; i < 8; ++i) {
+      if (oo[i] < L) {
+        const uint32_t so = swz(oo[i]);
+        sp[so] = cmul2(ph[i], sp[so]);
+        sl[so] = cmul2(ph[i], sl[so]);
+      }
     }
   }
 }
@@ -397,8 +446,8 @@ __device__ __noinline__ void op_phase(double2* sp, double2* sl, const AOp& hdr, 
     double2 a[8], b[8];
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
-      a[i] = valid ? sp[off[i]] : make_double2(0.0, 0.0);
-      b[i] = valid ? sl[off[i]] : make_double2(0.0, 0.0);
+      a[i] = valid ? sp[swz(off[i])] : make_double2(0.0, 0.0);
+      b[i] = valid ? sl[swz(off[i])] : make_double2(0.0, 0.0);
     }
 #pragma unroll 1
     for (uint32_t u = 0; u < cnt; ++u) {
@@ -428,8 +477,8 @@ __device__ __noinline__ void op_phase(double2* sp, double2* sl, const AOp& hdr, 
     if (valid) {
 #pragma unroll
       for (int i = 0; i < 8; ++i) {
-        sp[off[i]] = a[i];
-        sl[off[i]] = b[i];
+        sp[swz(off[i])] = a[i];
+        sl[swz(off[i])] = b[i];
       }
     }
   }
@@ -466,11 +515,15 @@ __global__ void __launch_bounds__(kAThreads, 2)
     uint64_t base = 0;
     for (uint32_t b = 0; b < H.npos_cnt; ++b)
       if (t >> b & 1ULL) base |= 1ULL << H.npos[b];
+    // all of the tile's copies in flight at once (cp.async straight into the
+    // swizzled layout), then one wait
     for (uint32_t o = threadIdx.x; o < L; o += kAThreads) {
       const uint64_t g = base | (o & lo_mask) | hi_tab[o >> lo_bits];
-      sp[o] = psi[g];
-      sl[o] = lam[g];
+      cp_async16a(sp + swz(o), psi + g);
+      cp_async16a(sl + swz(o), lam + g);
     }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
     __syncthreads();
     for (uint32_t i = 0; i < H.nops; ++i) {
       const AOp op = ops[i];
@@ -509,8 +562,8 @@ __global__ void __launch_bounds__(kAThreads, 2)
     }
     for (uint32_t o = threadIdx.x; o < L; o += kAThreads) {
       const uint64_t g = base | (o & lo_mask) | hi_tab[o >> lo_bits];
-      psi[g] = sp[o];
-      lam[g] = sl[o];
+      psi[g] = sp[swz(o)];
+      lam[g] = sl[swz(o)];
     }
     __syncthreads();
   }
