@@ -92,6 +92,17 @@ __device__ __forceinline__ uint32_t ins0(uint32_t k, uint32_t p) {
   return ((k >> p) << (p + 1)) | (k & ((1u << p) - 1u));
 }
 
+// Shared-memory layout of a trajectory slice: logical element o lives at
+// tswz(o).  The low three index bits are XORed with a fold of the higher ones
+// so that eight threads touching elements that differ only in higher bits
+// (pairs of a low target, strided controls) use eight different bank rows.
+// The same bijection in every CTA keeps distributed-shared-memory accesses
+// consistent; summation orders follow logical indices, so results are
+// unchanged.
+__device__ __forceinline__ uint32_t tswz(uint32_t o) {
+  return o ^ (((o >> 3) ^ (o >> 6) ^ (o >> 9) ^ (o >> 12)) & 7u);
+}
+
 // Fixed-order block sum, result broadcast to every thread.
 template <int THREADS>
 __device__ double block_sum_all(double v, double* sh) {
@@ -144,7 +155,7 @@ __global__ void __launch_bounds__(THREADS) k_traj(const TrajParams P) {
     auto elem = [&](uint64_t g) -> double2* {
       const uint32_t r = (uint32_t)(g >> lb);
       double2* base = (r == rank) ? sm : cl.map_shared_rank(sm, r);
-      return base + (g & lmask);
+      return base + tswz((uint32_t)(g & lmask));
     };
 
     uint32_t key[8];
@@ -206,8 +217,8 @@ __global__ void __launch_bounds__(THREADS) k_traj(const TrajParams P) {
               uint32_t o = k;
               for (int p = 0; p < np; ++p) o = ins0(o, pos[p]);
               o |= (uint32_t)lo_ctrl;
-              double2* pa = sm + o;
-              double2* pb = sm + (o | tb);
+              double2* pa = sm + tswz(o);
+              double2* pb = sm + tswz(o | tb);
               const double2 a = *pa, b = *pb;
               if (op.type == T_ONEQ) {
                 *pa = cadd_x(cmul_x(u[0], a), cmul_x(u[1], b));
@@ -230,8 +241,8 @@ __global__ void __launch_bounds__(THREADS) k_traj(const TrajParams P) {
               uint32_t o = k;
               for (int p = 0; p < np; ++p) o = ins0(o, pos[p]);
               o |= (uint32_t)lo_ctrl;
-              double2* pa = b0 + o;
-              double2* pb = b1 + o;
+              double2* pa = b0 + tswz(o);
+              double2* pb = b1 + tswz(o);
               const double2 a = *pa, b = *pb;
               if (op.type == T_ONEQ) {
                 *pa = cadd_x(cmul_x(u[0], a), cmul_x(u[1], b));
@@ -262,7 +273,7 @@ __global__ void __launch_bounds__(THREADS) k_traj(const TrajParams P) {
             uint32_t o = k;
             for (int p = 0; p < np; ++p) o = ins0(o, pos[p]);
             o |= (uint32_t)lo;
-            sm[o] = cmul_x(e, sm[o]);
+            sm[tswz(o)] = cmul_x(e, sm[tswz(o)]);
           }
           break;
         }
@@ -274,7 +285,7 @@ __global__ void __launch_bounds__(THREADS) k_traj(const TrajParams P) {
             for (uint32_t b = 0; b < kq; ++b) idx = (idx << 1) | (uint32_t)((g >> op.q[b]) & 1ULL);
             const double2 d = P.pool[op.mat + idx];
             if (d.x == 1.0 && d.y == 0.0) continue;
-            sm[o] = cmul_x(d, sm[o]);
+            sm[tswz(o)] = cmul_x(d, sm[tswz(o)]);
           }
           break;
         }
@@ -300,7 +311,7 @@ __global__ void __launch_bounds__(THREADS) k_traj(const TrajParams P) {
             for (int p = 0; p < np; ++p) o = ins0(o, pos[p]);
             o |= lo_one;
             const uint64_t gi = gbase | o, gj = gi ^ b1 ^ b2;
-            double2* pi = sm + o;
+            double2* pi = sm + tswz(o);
             double2* pj = elem(gj);
             const double2 a = *pi, b = *pj;
             *pi = b;
@@ -353,9 +364,9 @@ __global__ void __launch_bounds__(THREADS) k_traj(const TrajParams P) {
           double part = 0.0;
           if (q < lb) {
             for (uint32_t k = tid; k < L / 2; k += THREADS)
-              part = __dadd_rn(part, norm_sqr_x(sm[ins0(k, q) | (uint32_t)qb]));
+              part = __dadd_rn(part, norm_sqr_x(sm[tswz(ins0(k, q) | (uint32_t)qb)]));
           } else if (gbase & qb) {
-            for (uint32_t o = tid; o < L; o += THREADS) part = __dadd_rn(part, norm_sqr_x(sm[o]));
+            for (uint32_t o = tid; o < L; o += THREADS) part = __dadd_rn(part, norm_sqr_x(sm[tswz(o)]));
           }
           const double cta = block_sum_all<THREADS>(part, red);
           if (tid == 0) red[40] = cta;
@@ -390,10 +401,10 @@ __global__ void __launch_bounds__(THREADS) k_traj(const TrajParams P) {
           for (uint32_t i = tid; i < L; i += THREADS) {
             const bool set = ((gbase | i) & qb) != 0;
             if (set != (o == 1)) {
-              sm[i] = make_double2(0.0, 0.0);
+              sm[tswz(i)] = make_double2(0.0, 0.0);
             } else {
-              const double2 a = sm[i];
-              sm[i] = make_double2(__ddiv_rn(a.x, norm), __ddiv_rn(a.y, norm));
+              const double2 a = sm[tswz(i)];
+              sm[tswz(i)] = make_double2(__ddiv_rn(a.x, norm), __ddiv_rn(a.y, norm));
             }
           }
           if (op.type == T_RESET && o == 1) {
@@ -402,9 +413,9 @@ __global__ void __launch_bounds__(THREADS) k_traj(const TrajParams P) {
             if (q < lb) {
               for (uint32_t k = tid; k < L / 2; k += THREADS) {
                 const uint32_t a0 = ins0(k, q), a1 = a0 | (uint32_t)qb;
-                const double2 x = sm[a0];
-                sm[a0] = sm[a1];
-                sm[a1] = x;
+                const double2 x = sm[tswz(a0)];
+                sm[tswz(a0)] = sm[tswz(a1)];
+                sm[tswz(a1)] = x;
               }
             } else {
               const uint32_t tbr = 1u << (q - lb);
@@ -437,7 +448,7 @@ __global__ void __launch_bounds__(THREADS) k_traj(const TrajParams P) {
         P.cbits_out[pg.cbits_off + it.shot * pg.ncbits + i] = cb[i];
     if (pg.state_out) {
       double2* dst = pg.state_out + (it.shot << pg.n) + gbase;
-      for (uint32_t i = tid; i < L; i += THREADS) dst[i] = sm[i];
+      for (uint32_t i = tid; i < L; i += THREADS) dst[i] = sm[tswz(i)];
     }
     sync_all(true);
   }
