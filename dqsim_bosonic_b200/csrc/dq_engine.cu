@@ -246,12 +246,17 @@ __global__ void k_marg_thread(const double2* __restrict__ s, uint64_t nj, uint64
   out[j] = acc;
 }
 
-// One block sums segment `seg` of output j.  Indices whose bits above the
-// lowest marginal qubit c agree form runs of 2^c consecutive amplitudes, so a
-// run's base index is computed once and the run is streamed with four
-// independent partial sums (combined in a fixed order: deterministic).
+// One block sums segment `seg` of output j.  When the lowest marginal qubit
+// c leaves runs of at least a block of consecutive amplitudes (indices whose
+// bits above c agree), a run's base index is computed once and the run is
+// streamed.  Otherwise (marginal qubits at low positions, e.g. after a
+// relabeling) every thread takes terms r = r0 + tid, + blockDim, ... and
+// finds the index from shared tables that deposit 7 bits of r at a time.
+// Four independent partial sums per thread, combined in a fixed order, then a
+// fixed-order block sum: deterministic.
 __global__ void k_marg_seg(const double2* __restrict__ s, uint64_t nterms, uint32_t nseg,
                            MargParams P, double* __restrict__ partial) {
+  __shared__ uint64_t tab[5][128];
   const uint64_t j = blockIdx.x / nseg;
   const uint32_t seg = blockIdx.x % nseg;
   const uint64_t per = nterms / nseg;  // nseg is a power of two dividing nterms
@@ -261,16 +266,41 @@ __global__ void k_marg_seg(const double2* __restrict__ s, uint64_t nterms, uint3
   const uint64_t run = c >= 63u ? per : (per < (1ULL << c) ? per : (1ULL << c));
   const uint32_t bd = blockDim.x;
   double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
-  for (uint64_t rb = r0; rb < r0 + per; rb += run) {
-    const double2* src = s + (insert_zeros(rb, P.rest.p, P.rest.np) | jb);
-    uint64_t off = threadIdx.x;
-    for (; off + 3ULL * bd < run; off += 4ULL * bd) {
-      a0 = __dadd_rn(a0, norm_sqr_x(src[off]));
-      a1 = __dadd_rn(a1, norm_sqr_x(src[off + bd]));
-      a2 = __dadd_rn(a2, norm_sqr_x(src[off + 2ULL * bd]));
-      a3 = __dadd_rn(a3, norm_sqr_x(src[off + 3ULL * bd]));
+  if (run >= bd) {
+    for (uint64_t rb = r0; rb < r0 + per; rb += run) {
+      const double2* src = s + (insert_zeros(rb, P.rest.p, P.rest.np) | jb);
+      uint64_t off = threadIdx.x;
+      for (; off + 3ULL * bd < run; off += 4ULL * bd) {
+        a0 = __dadd_rn(a0, norm_sqr_x(src[off]));
+        a1 = __dadd_rn(a1, norm_sqr_x(src[off + bd]));
+        a2 = __dadd_rn(a2, norm_sqr_x(src[off + 2ULL * bd]));
+        a3 = __dadd_rn(a3, norm_sqr_x(src[off + 3ULL * bd]));
+      }
+      for (; off < run; off += bd) a0 = __dadd_rn(a0, norm_sqr_x(src[off]));
     }
-    for (; off < run; off += bd) a0 = __dadd_rn(a0, norm_sqr_x(src[off]));
+  } else {
+    // deposit tables: tab[g][v] = index bits of the term v << 7g
+    uint32_t bits = 0;
+    while (bits < 64 && (1ULL << bits) < nterms) ++bits;
+    const uint32_t ntab = min((bits + 6) / 7, 5u);  // nterms <= 2^34 needs at most 5
+    for (uint32_t i = threadIdx.x; i < ntab * 128u; i += bd)
+      tab[i >> 7][i & 127u] = insert_zeros((uint64_t)(i & 127u) << (7u * (i >> 7)), P.rest.p,
+                                           P.rest.np);
+    __syncthreads();
+    auto index = [&](uint64_t r) {
+      uint64_t x = jb;
+      for (uint32_t g = 0; g < ntab; ++g) x |= tab[g][(r >> (7u * g)) & 127u];
+      return x;
+    };
+    uint64_t e = threadIdx.x;
+    for (; e + 3ULL * bd < per; e += 4ULL * bd) {
+      const uint64_t r = r0 + e;
+      a0 = __dadd_rn(a0, norm_sqr_x(s[index(r)]));
+      a1 = __dadd_rn(a1, norm_sqr_x(s[index(r + bd)]));
+      a2 = __dadd_rn(a2, norm_sqr_x(s[index(r + 2ULL * bd)]));
+      a3 = __dadd_rn(a3, norm_sqr_x(s[index(r + 3ULL * bd)]));
+    }
+    for (; e < per; e += bd) a0 = __dadd_rn(a0, norm_sqr_x(s[index(r0 + e)]));
   }
   double acc = __dadd_rn(__dadd_rn(a0, a1), __dadd_rn(a2, a3));
   acc = block_sum(acc);
