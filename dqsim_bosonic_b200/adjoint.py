@@ -306,7 +306,8 @@ def adjoint_gradient(circuit: ParamCircuit, theta, observable: PauliSum, *, devi
     """``(E, dE/dtheta)`` from one forward and one adjoint (reverse) pass.
 
     ``timing``: a dict that receives the device milliseconds of the forward
-    pass, of lambda = H psi and of the backward pass."""
+    pass, of lambda = H psi and of the backward pass, and the number of fused
+    backward sweeps."""
     terms = _check_observable(circuit, observable)
     th = np.asarray(theta, dtype=np.float64).reshape(-1)
     insts = circuit.bind(th)
@@ -317,14 +318,14 @@ def adjoint_gradient(circuit: ParamCircuit, theta, observable: PauliSum, *, devi
     opts = nat.RunOpts(nat.SEM_SIMULATE, _exec_mode(exec), 0, 0, 0, 0)
     e = ctypes.c_double(0.0)
     g_occ = np.zeros(max(1, len(occ)), dtype=np.float64)
-    phases = np.zeros(3, dtype=np.float64)
+    phases = np.zeros(4, dtype=np.float64)
     nat.check(nat.lib().dq_adjoint(st.handle, nat.ptr(insts), len(insts), nat.ptr(slots), len(occ),
                                    nat.ptr(terms), len(terms), ctypes.byref(opts), ctypes.byref(e),
                                    nat.ptr(g_occ), nat.ptr(phases) if timing is not None else None),
               "dq_adjoint")
     if timing is not None:
         timing.update(forward_ms=float(phases[0]), observable_ms=float(phases[1]),
-                      backward_ms=float(phases[2]))
+                      backward_ms=float(phases[2]), backward_sweeps=int(phases[3]))
     grad = np.zeros(circuit.num_params, dtype=np.float64)
     for o, (_, _, p) in enumerate(occ):
         grad[p.index] += p.scale * g_occ[o]

@@ -557,11 +557,10 @@ int dq_adjoint(dq_state_t h, const dq_inst* prog, uint64_t ninst, const int32_t*
 
   // backward pass: slots are numbered in program order
   const bool fused_back = o.exec == DQ_EXEC_FUSED;
-  if (fused_back && rc == DQ_OK) {
-    AdjSweepStats ss;
+  AdjSweepStats ss;
+  if (fused_back && rc == DQ_OK)
     rc = adjoint_backward_fused(h->amp, lam, h->n, prog, ninst, param_index, nslots, slots,
                                 h->stream, h->device, &ss);
-  }
   uint64_t slot = nslots;
   for (uint64_t r = ninst; !fused_back && rc == DQ_OK && r-- > 0;) {
     const dq_inst& in = prog[r];
@@ -619,6 +618,7 @@ int dq_adjoint(dq_state_t h, const dq_inst* prog, uint64_t ninst, const int32_t*
       DQ_CUDA_TRY(cudaEventElapsedTime(&ms, ev[i], ev[i + 1]));
       phase_ms[i] = ms;
     }
+  if (phase_ms) phase_ms[3] = (double)ss.sweeps;
   *expval = host[nslots];
   for (uint64_t p = 0; p < nparams; ++p) grad[p] = 0.0;
   uint64_t s = 0;

@@ -339,8 +339,9 @@ DQ_API int dq_expval_pauli(dq_state_t h, const dq_pauli_term* terms, uint64_t nt
  * inverse gates alongside lambda = H psi (no stored intermediate states; one
  * extra state-sized buffer).  On return the handle holds psi0 again, up to
  * rounding.  param_index may be NULL when nparams == 0 (E only).  phase_ms,
- * when non-NULL, receives the device time (ms) of the forward pass, of
- * lambda = H psi, and of the backward pass. */
+ * when non-NULL, receives 4 values: the device time (ms) of the forward pass,
+ * of lambda = H psi and of the backward pass, then the number of fused
+ * backward sweeps (0 with DQ_EXEC_PER_GATE). */
 DQ_API int dq_adjoint(dq_state_t h, const dq_inst* prog, uint64_t ninst,
                       const int32_t* param_index, uint64_t nparams,
                       const dq_pauli_term* terms, uint64_t nterms,
