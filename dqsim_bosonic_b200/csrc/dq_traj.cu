@@ -167,8 +167,21 @@ __global__ void __launch_bounds__(THREADS) k_traj(const TrajParams P) {
     bool last_cluster = true;
     sync_all(true);
 
+    // the next op's descriptor and one-qubit matrix are loaded while the
+    // current op runs (global loads, otherwise a round trip before every op)
+    TOp nxt{};
+    double2 nu[4] = {};
+    auto fetch = [&](uint32_t k) {
+      nxt = P.ops[pg.ops_off + k];
+      if (nxt.type == T_ONEQ)
+        for (int i = 0; i < 4; ++i) nu[i] = P.pool[nxt.mat + i];
+    };
+    if (pg.nops) fetch(0);
     for (uint32_t oi = 0; oi < pg.nops; ++oi) {
-      const TOp op = P.ops[pg.ops_off + oi];
+      const TOp op = nxt;
+      double2 u[4];
+      for (int i = 0; i < 4; ++i) u[i] = nu[i];
+      if (oi + 1 < pg.nops) fetch(oi + 1);
       // conditions (little-endian register value, unwritten bits read as 0)
       if (op.cond_count) {
         if (tid == 0) {
@@ -197,9 +210,6 @@ __global__ void __launch_bounds__(THREADS) k_traj(const TrajParams P) {
           const uint32_t t = op.t1;
           const uint64_t hi_ctrl = op.ctrl & ~lmask;
           const uint64_t lo_ctrl = op.ctrl & lmask;
-          double2 u[4];
-          if (op.type == T_ONEQ)
-            for (int i = 0; i < 4; ++i) u[i] = P.pool[op.mat + i];
           // local zero-insertion positions: target (if local) and local controls
           uint32_t pos[9];
           int np = 0;
