@@ -85,7 +85,9 @@ struct SwPhase {
   uint32_t lanesw[32];         // swizzled local index of the lane bits (thread bits 0..4)
   uint32_t warpsw[8];          // swizzled local index of the warp bits (thread bits 5..7)
   uint32_t V[4];               // swizzled local index of each register bit
-  uint32_t op_begin, op_end, pad0, pad1;
+  uint32_t op_begin, op_end;
+  uint32_t xload;              // XORed into every load address: X gates folded into the load
+  uint32_t pad1;
 };
 // 32 bytes, read as two 128-bit words: w0 = type | b0 << 8 | b1 << 16 | creg << 24,
 // w1 = ctl_thr | flags << 8 | slot << 16, data = first DATA entry, cnl = non-local controls
@@ -379,13 +381,14 @@ __global__ void __launch_bounds__(1 << TB, (S == 1 && TB == 7 ? 3 : (TB + RB <= 
     for (uint32_t p = 0; p < nph; ++p) {
       const SwPhase& P = PH[p];
       const uint32_t pt = P.lanesw[lane] ^ P.warpsw[warp];
+      const uint32_t ptl = pt ^ P.xload;
       uint32_t V[RB];
 #pragma unroll
       for (int b = 0; b < RB; ++b) V[b] = P.V[b];
       double2 a[R];
 #pragma unroll
       for (int j = 0; j < R; ++j) {
-        uint32_t x = pt;
+        uint32_t x = ptl;
 #pragma unroll
         for (int b = 0; b < RB; ++b)
           if ((j >> b) & 1) x ^= V[b];
@@ -939,6 +942,12 @@ int encode_sweep(const PSweep& sw, const std::vector<PGate>& G, uint32_t TBn, ui
     auto is_u1_type = [](uint32_t t) {
       return t == OP_U1 || t == OP_U1R || t == OP_U1X || t == OP_U1H;
     };
+    // An uncontrolled X on a register bit that no earlier op of the phase
+    // involves (as target, control or, conservatively, any flush) commutes to
+    // the front of the phase and becomes part of the load: element j is read
+    // from the address of j with that bit flipped (the swizzled addresses are
+    // XOR-linear).  involved: register bits touched so far in this phase.
+    uint32_t involved = 0;
     for (size_t oi = ph.ob; oi < ph.oe; ++oi) {
       const POp& op = sw.ops[oi];
       EncOp so{};
@@ -954,6 +963,15 @@ int encode_sweep(const PSweep& sw, const std::vector<PGate>& G, uint32_t TBn, ui
       }
       const POp& cur = sw.ops[oi];
       so.type = cur.type;
+      if (!pre && cur.type == OP_U1X && G[cur.gate].ctrl == 0) {
+        const uint32_t b = (uint32_t)rix[lidx[G[cur.gate].t0]];
+        if (!((involved >> b) & 1u)) {
+          sp.xload ^= sp.V[b];
+          continue;
+        }
+      }
+      if (pre || cur.type == OP_FLUSH_R || cur.type == OP_FLUSH_T || cur.type == OP_GPHASE)
+        involved = ~0u;
       if (is_u1_type(cur.type) || cur.type == OP_U2) {
         const PGate& g = G[cur.gate];
         if (cur.type == OP_U1H) scale = scale * g.u[0].re;
@@ -1003,6 +1021,8 @@ int encode_sweep(const PSweep& sw, const std::vector<PGate>& G, uint32_t TBn, ui
       } else if (cur.type == OP_GPHASE) {
         so.slot = add_slot(cur.gcst, cur.gterms);
       }
+      if (is_u1_type(cur.type)) involved |= (1u << so.b0) | so.creg;
+      if (cur.type == OP_U2) involved |= (1u << so.b0) | (1u << so.b1) | so.creg;
       O.push_back(so);
     }
     if (&ph == &phases.back() && scale != 1.0) {

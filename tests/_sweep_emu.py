@@ -103,11 +103,11 @@ def run_sweep(state: np.ndarray, n: int, blob: bytes) -> None:
         lanesw = np.array(struct.unpack_from("<32I", blob, po), dtype=np.int64)
         warpsw = np.array(struct.unpack_from("<8I", blob, po + 128), dtype=np.int64)
         V = struct.unpack_from("<4I", blob, po + 160)[:rb]
-        ob, oe = struct.unpack_from("<2I", blob, po + 176)
+        ob, oe, xload = struct.unpack_from("<3I", blob, po + 176)
         pt = lanesw[tid & 31] ^ warpsw[tid >> 5]                                   # threads
         X = np.array([pt ^ _xor_bits(j, V) for j in range(R)]).T                   # threads x R
-        assert X.max() < T
-        a = smem[:, X]                                                             # tiles x threads x R
+        assert X.max() < T and (X ^ xload).max() < T
+        a = smem[:, X ^ xload]            # X gates folded into the load address   # tiles x threads x R
         for o in range(ob, oe):
             _exec(blob, off_op + 32 * o, off_data, a, slots, base, tid, rb)
         smem[:, X] = a

@@ -87,3 +87,25 @@ def test_remote_and_swap_planned(engine_lib):
               gate("nonlocal_cz", [1, 7]), g("rxx", 4, 8, 0.3), gate("remote_link_phi_plus", [6, 0]),
               g("swap", 3, 4), g("cp", 11, 0, 0.9), g("rzz", 5, 6, 1.1)]
     check(JsonCircuit(n, insts), 2)
+
+
+def test_leading_x_gates_fold_into_the_load():
+    """X gates that open a register phase cost nothing: they become a flip of
+    the phase's load address.  X after other ops on its qubit must stay an op."""
+    import struct
+
+    from _sweep_emu import plan
+
+    prog = prog_of(qft_with_x(12, 3))
+    blobs, _, _, _ = plan(prog)
+    m, rb, nphase, _ = struct.unpack_from("<4I", blobs[0], 0)
+    off_phase = struct.unpack_from("<I", blobs[0], 64)[0]
+    xloads = [struct.unpack_from("<I", blobs[0], off_phase + 192 * p + 184)[0] for p in range(nphase)]
+    assert any(xloads), "no X gate was folded"
+    # X before and after other gates on the same qubits, controls included
+    insts = []
+    for q in range(12):
+        insts += [g("x", q), g("h", q), g("x", q), g("ry", q, 0.3 + q), g("x", q)]
+    insts += [g("cx", 0, 5), g("x", 5), g("x", 0), g("cp", 3, 7, 0.7), g("x", 7)]
+    check(JsonCircuit(12, insts), seed=4)
+    check(JsonCircuit(12, insts[::-1]), seed=5)
