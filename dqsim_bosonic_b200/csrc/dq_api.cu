@@ -87,6 +87,32 @@ using namespace dq;
 
 namespace dq {
 
+// ---- handle shells --------------------------------------------------------------
+// Up to kMaxShells destroyed handles per device keep their stream, reduction
+// scratch, pinned buffer and fused-sweep buffers for the next dq_state_create.
+namespace {
+std::mutex g_shell_mu;
+std::vector<dq_state_t> g_shells[64];
+constexpr size_t kMaxShells = 8;
+}  // namespace
+
+dq_state_t take_shell(int device) {
+  std::lock_guard<std::mutex> lk(g_shell_mu);
+  auto& v = g_shells[device & 63];
+  if (v.empty()) return nullptr;
+  dq_state_t h = v.back();
+  v.pop_back();
+  return h;
+}
+
+bool put_shell(dq_state_t h) {
+  std::lock_guard<std::mutex> lk(g_shell_mu);
+  auto& v = g_shells[h->device & 63];
+  if (v.size() >= kMaxShells) return false;
+  v.push_back(h);
+  return true;
+}
+
 int check_handle(dq_state_t h) {
   if (!h || !h->amp) return fail(DQ_ERR_INVALID_ARG, "null or destroyed state handle");
   return DQ_OK;
@@ -364,6 +390,29 @@ int dq_state_create(uint32_t n, int device, dq_state_t* out) {
   if (ndev == 0) return fail(DQ_ERR_NO_DEVICE, "no CUDA device");
   if (device < 0 || device >= ndev) return fail(DQ_ERR_INVALID_ARG, "device index out of range");
   DeviceGuard g(device);
+  // a destroyed handle's shell (stream, scratch, pinned buffer, sweep program
+  // buffers) is reused: creating those costs milliseconds per simulate call
+  if (dq_state_t sh = take_shell(device)) {
+    sh->n = n;
+    sh->len = 1ULL << n;
+    sh->bytes = sizeof(double2) * sh->len;
+    void* p = nullptr;
+    const int rc = cache_alloc(device, sh->bytes, &p);
+    if (rc != DQ_OK) {
+      put_shell(sh);
+      return rc;
+    }
+    sh->amp = (double2*)p;
+    reset_perm(sh);
+    int rc2 = launch_set_basis(sh->amp, n, 0, sh->stream, device);
+    if (rc2 == DQ_OK) rc2 = sync_stream(sh);
+    if (rc2 != DQ_OK) {
+      dq_state_destroy(sh);
+      return rc2;
+    }
+    *out = sh;
+    return DQ_OK;
+  }
   dq_state_t h = new (std::nothrow) dq_state_s();
   if (!h) return fail(DQ_ERR_OOM, "host allocation failed");
   h->device = device;
@@ -415,8 +464,11 @@ int dq_state_destroy(dq_state_t h) {
   if (!h) return DQ_OK;
   DeviceGuard g(h->device);
   if (h->stream) cudaStreamSynchronize(h->stream);
-  fused_release(h->fw);
   if (h->amp) cache_free(h->device, h->bytes, h->amp);
+  h->amp = nullptr;
+  if (h->stream && h->sc.d_partial && h->sc.d_counter && h->sc.h_pinned && put_shell(h))
+    return DQ_OK;
+  fused_release(h->fw);
   if (h->sc.d_partial) cudaFree(h->sc.d_partial);
   if (h->sc.d_counter) cudaFree(h->sc.d_counter);
   if (h->sc.h_pinned) cudaFreeHost(h->sc.h_pinned);
