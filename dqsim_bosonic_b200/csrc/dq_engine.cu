@@ -307,6 +307,37 @@ __global__ void k_marg_seg(const double2* __restrict__ s, uint64_t nterms, uint3
   if (threadIdx.x == 0) partial[blockIdx.x] = acc;
 }
 
+// Marginal qubits all among the low 10 bits: block b streams the contiguous
+// chunk [b * chunk, (b + 1) * chunk) fully coalesced, thread t summing the
+// elements whose low 10 bits equal t; output j then adds, in ascending t, the
+// threads whose bits at the marginal positions spell j.  partial[j * gridDim.x + b].
+__global__ void __launch_bounds__(1024) k_marg_low(const double2* __restrict__ s, uint64_t chunk,
+                                                   MargParams P, double* __restrict__ partial) {
+  __shared__ double sh[1024];
+  const uint32_t t = threadIdx.x;
+  const double2* src = s + (uint64_t)blockIdx.x * chunk + t;
+  double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+  uint64_t i = 0;
+  for (; i + 3 * 1024 < chunk; i += 4 * 1024) {
+    a0 = __dadd_rn(a0, norm_sqr_x(src[i]));
+    a1 = __dadd_rn(a1, norm_sqr_x(src[i + 1024]));
+    a2 = __dadd_rn(a2, norm_sqr_x(src[i + 2048]));
+    a3 = __dadd_rn(a3, norm_sqr_x(src[i + 3072]));
+  }
+  for (; i < chunk; i += 1024) a0 = __dadd_rn(a0, norm_sqr_x(src[i]));
+  sh[t] = __dadd_rn(__dadd_rn(a0, a1), __dadd_rn(a2, a3));
+  __syncthreads();
+  const uint64_t nj = 1ULL << P.k;
+  if (t < nj) {
+    const uint32_t jb = (uint32_t)deposit_j(t, P);
+    const uint32_t nr = 1024u >> P.k;
+    double acc = 0.0;
+    for (uint32_t r = 0; r < nr; ++r)
+      acc = __dadd_rn(acc, sh[(uint32_t)insert_zeros(r, P.rest.p, P.rest.np) | jb]);
+    partial[(uint64_t)t * gridDim.x + blockIdx.x] = acc;
+  }
+}
+
 __global__ void k_marg_sum(const double* __restrict__ partial, uint64_t nj, uint32_t nseg,
                            double* __restrict__ out) {
   const uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
@@ -564,6 +595,20 @@ int launch_marginal(const double2* s, uint32_t n, const uint32_t* qubits, uint32
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
   // thread-per-output (exact reference order) when there are enough outputs
   // to fill the GPU or few terms per output
+  const uint32_t top = k ? P.rest.p[P.rest.np - 1] : 0;  // highest marginal position
+  if (k >= 1 && top < 10 && n >= 20 && nterms > 64) {
+    // all marginal qubits in the low 10 bits (e.g. after a relabeling)
+    uint32_t nb = 1;
+    while (nb * 2 <= (uint32_t)sms * 4 && (1ULL << n) / (nb * 2) >= 1024 * 4) nb *= 2;
+    const uint64_t chunk = (1ULL << n) / nb;
+    double* tmp = nullptr;
+    DQ_CUDA_TRY(cudaMallocAsync((void**)&tmp, sizeof(double) * nj * nb, st));
+    k_marg_low<<<nb, 1024, 0, st>>>(s, chunk, P, tmp);
+    k_marg_sum<<<blocks_for(nj, kThreads), kThreads, 0, st>>>(tmp, nj, nb, d_out);
+    DQ_CUDA_TRY(cudaFreeAsync(tmp, st));
+    DQ_CUDA_TRY(cudaGetLastError());
+    return DQ_OK;
+  }
   if (nterms <= 64 || nj >= (uint64_t)sms * 1024) {
     k_marg_thread<<<blocks_for(nj, kThreads), kThreads, 0, st>>>(s, nj, nterms, P, d_out);
   } else {

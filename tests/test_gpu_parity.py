@@ -178,7 +178,7 @@ def test_marginal_large_reduction(gpu):
     from dqsim_bosonic_b200.statevector import SimulationResult
 
     res = SimulationResult(st, n, {}, None)
-    for qs in ([19], [0, 10], [3, 17, 8], list(range(10))):
+    for qs in ([19], [0, 10], [3, 17, 8], list(range(10)), [7, 0, 3], [9, 1]):
         want = _oracle.marginal(init, qs)
         got = res.probability_array(qs)
         assert np.max(np.abs(got - want)) < ATOL
