@@ -77,7 +77,9 @@ struct SwHeader {
   uint32_t m, rb, nphase, nslots;
   uint32_t local_pos[kMaxM];
   uint32_t off_phase, off_op, off_slot, off_slotent;
-  uint32_t off_data, prog_bytes, pad1, pad2;
+  uint32_t off_data, prog_bytes;
+  uint32_t tile_xload;         // XORed into every tile-load address: X gates opening the sweep
+  uint32_t pad2;
   uint64_t runoff[kMaxRuns];   // physical offset of run r (local bits 5..m-1 = r)
   uint32_t runswz[kMaxRuns];   // swizzled shared-memory index of run r's first element
 };
@@ -351,7 +353,7 @@ __global__ void __launch_bounds__(1 << TB, (S == 1 && TB == 7 ? 3 : (TB + RB <= 
 #pragma unroll
       for (int i = 0; i < NI; ++i) {
         const uint32_t r = warp + (uint32_t)i * NW;
-        cp_async16(&dst[H->runswz[r] ^ swl], state + (b + H->runoff[r] + lane));
+        cp_async16(&dst[H->runswz[r] ^ swl ^ H->tile_xload], state + (b + H->runoff[r] + lane));
       }
     }
     cp_async_commit();
@@ -774,14 +776,40 @@ bool order_thread_bits(std::vector<uint32_t>& tb) {
 }
 
 // Encode a planned sweep into the device blob format.
-int encode_sweep(const PSweep& sw, const std::vector<PGate>& G, uint32_t TBn, uint32_t RB,
+int encode_sweep(const PSweep& sw_in, const std::vector<PGate>& G, uint32_t TBn, uint32_t RB,
                  Blob& blob, size_t* offset) {
   const int kSwTB = (int)TBn;
-  const uint32_t m = (uint32_t)sw.local.size();
+  const uint32_t m = (uint32_t)sw_in.local.size();
   if (m != kSwTB + RB) return fail(DQ_ERR_INTERNAL, "sweep local set size mismatch");
   int lidx[64];
   for (int i = 0; i < 64; ++i) lidx[i] = -1;
-  for (uint32_t k = 0; k < m; ++k) lidx[sw.local[k]] = (int)k;
+  for (uint32_t k = 0; k < m; ++k) lidx[sw_in.local[k]] = (int)k;
+
+  // Uncontrolled X gates on local bits that no earlier op of the sweep
+  // involves (as target or control; any flush or global phase stops the scan
+  // for good) commute to the front of the sweep and fold into the tile load:
+  // element e is stored at the shared-memory slot of e with those bits
+  // flipped (the swizzled layout is XOR-linear), so they cost nothing.
+  PSweep sw;
+  sw.local = sw_in.local;
+  uint32_t tile_xload = 0;
+  {
+    uint64_t involved = 0;
+    bool stopped = false;
+    for (const POp& op : sw_in.ops) {
+      if (!stopped && op.type == OP_U1X && op.gate >= 0 && G[op.gate].ctrl == 0) {
+        const uint32_t t = G[op.gate].t0;
+        if (!((involved >> t) & 1ULL) && lidx[t] >= 0) {
+          tile_xload ^= swz(1u << (uint32_t)lidx[t]);
+          continue;
+        }
+      }
+      if (op.type == OP_FLUSH_R || op.type == OP_FLUSH_T || op.type == OP_GPHASE) stopped = true;
+      if (op.gate >= 0) involved |= (1ULL << G[op.gate].t0) | G[op.gate].ctrl |
+                                    (op.type == OP_U2 ? (1ULL << G[op.gate].t1) : 0ULL);
+      sw.ops.push_back(op);
+    }
+  }
 
   // phases: consecutive ops whose register needs fit RB register bits
   struct PhaseTmp {
@@ -850,6 +878,7 @@ int encode_sweep(const PSweep& sw, const std::vector<PGate>& G, uint32_t TBn, ui
     return (uint32_t)SL.size() - 1;
   };
 
+  uint32_t carry_xload = 0;
   for (const PhaseTmp& ph : phases) {
     SwPhase sp{};
     std::vector<uint32_t> regs = ph.regs;
@@ -1044,6 +1073,13 @@ int encode_sweep(const PSweep& sw, const std::vector<PGate>& G, uint32_t TBn, ui
       }
     }
     sp.op_end = (uint32_t)O.size();
+    sp.xload ^= carry_xload;
+    carry_xload = 0;
+    if (sp.op_end == sp.op_begin && &ph != &phases.back()) {
+      // no op left (all folded): its flips move to the next phase's load
+      carry_xload = sp.xload;
+      continue;
+    }
     P.push_back(sp);
   }
   if (SL.size() > (size_t)kMaxSlots) return fail(DQ_ERR_INTERNAL, "too many per-tile slots");
@@ -1082,6 +1118,7 @@ int encode_sweep(const PSweep& sw, const std::vector<PGate>& G, uint32_t TBn, ui
   }
   h.nphase = (uint32_t)P.size();
   h.nslots = (uint32_t)SL.size();
+  h.tile_xload = tile_xload;
   for (uint32_t k = 0; k < m; ++k) h.local_pos[k] = sw.local[k];
   const size_t hoff = blob.put(&h, 1);
   const size_t po = blob.put(P.data(), P.size());

@@ -63,7 +63,8 @@ def run_sweep(state: np.ndarray, n: int, blob: bytes) -> None:
     """Apply one encoded sweep to state (complex128, modified in place)."""
     m, rb, nphase, nslots = struct.unpack_from("<4I", blob, 0)
     local = list(struct.unpack_from(f"<{MAXM}I", blob, 16))[:m]
-    off_phase, off_op, off_slot, off_slotent, off_data, prog_bytes = struct.unpack_from("<6I", blob, 64)
+    off_phase, off_op, off_slot, off_slotent, off_data, prog_bytes, tile_xload = struct.unpack_from(
+        "<7I", blob, 64)
     nruns = 1 << (m - 5)
     runoff = np.array(struct.unpack_from(f"<{MAXRUNS}Q", blob, 96)[:nruns], dtype=np.uint64)
     runswz = np.array(struct.unpack_from(f"<{MAXRUNS}I", blob, 96 + 8 * MAXRUNS)[:nruns], dtype=np.int64)
@@ -84,7 +85,8 @@ def run_sweep(state: np.ndarray, n: int, blob: bytes) -> None:
     gidx = base[:, None, None] + runoff[None, :, None] + lane[None, None, :]      # tiles x runs x 32
     sidx = (runswz[:, None] ^ swl[None, :])                                       # runs x 32
     smem = np.zeros((ntiles, T), dtype=np.complex128)
-    smem[:, sidx.reshape(-1)] = state[gidx.reshape(ntiles, -1).astype(np.int64)]
+    # X gates opening the sweep are folded into the load: element e lands at the slot of e ^ flips
+    smem[:, sidx.reshape(-1) ^ tile_xload] = state[gidx.reshape(ntiles, -1).astype(np.int64)]
     # per-tile slots
     slots = np.ones((ntiles, max(nslots, 1)), dtype=np.complex128)
     for s in range(nslots):
