@@ -19,6 +19,11 @@
 //           (controlled gates with a non-local control: variant 0 = I).
 //   A_TWO   dense 4x4 on two local qubits (rxx, swap-like, psi+-, phi+).
 //   A_DIAG  diagonal on up to two qubits, local or not, applied elementwise.
+//   A_DRUN  header of a run of 4..64 A_DIAG ops applied in one pass: their
+//           gradients from a Walsh-Hadamard transform of conj(lambda) psi,
+//           their phases as one quadratic phase polynomial (op_drun).
+//   A_PHASE header of 2..16 uncontrolled one-qubit ops on three local bits,
+//           applied to 8 amplitudes held in registers per thread (op_phase).
 // Gradient terms: Re sum conj(lambda_k) (D_j psi_{k-1}) with psi_{k-1} = V psi_k,
 // summed per thread, reduced per warp into shared slots [slot][warp], per CTA
 // in warp order, and over CTAs in CTA order by k_adj_slots: deterministic for
@@ -49,7 +54,8 @@ constexpr uint32_t kAMaxSlots = 192;
 
 enum AType : uint8_t { A_ONE = 1, A_TWO = 2, A_DIAG = 3, A_DRUN = 4, A_PHASE = 5 };
 constexpr uint32_t kAPhaseOps = 16;  // ops of one register phase
-constexpr uint32_t kADiagRun = 16;  // diagonal ops applied in one elementwise pass
+constexpr uint32_t kADiagRun = 64;  // diagonal ops applied in one elementwise pass
+constexpr uint32_t kADiagRunMin = 4;  // shorter runs stay single A_DIAG ops
 
 struct AOp {
   uint8_t type;
@@ -59,9 +65,9 @@ struct AOp {
   uint8_t skip0;     // A_ONE with selector: variant 0 is the identity with no derivatives
   uint8_t dq[2];     // A_DIAG: qubit encodings (bit 7: local; low 7 bits: local bit or global position)
   uint8_t ndq;       // A_DIAG: 1 or 2 qubits (dq[0] = MSB of the diagonal index)
-  uint8_t cnt;       // A_DRUN: number of A_DIAG ops that follow it
+  uint8_t cnt;       // A_DRUN / A_PHASE: number of ops that follow it
   uint8_t pad[2];
-  uint32_t lctrl;    // A_ONE: local control mask (tile offset bits)
+  uint32_t lctrl;    // A_ONE: local control mask (tile offset bits); A_DIAG: run record (pool offset)
   uint32_t slot;     // first sweep-local gradient slot
   uint32_t mat;      // offset of the op's matrices in the pool (double2 units)
 };
@@ -252,140 +258,253 @@ __device__ __noinline__ void op_diag(double2* sp, double2* sl, const AOp& op, co
     if (lmask[1] && (o & lmask[1])) e |= 1u;
     const uint32_t so = swz(o);
     const double2 a = sp[so], b = sl[so];
-    const double2 p = cmul2(v[e], a);
+    const double2 ve = sel4(v, e);
+    const double2 p = cmul2(ve, a);
     sp[so] = p;
 #pragma unroll
-    for (int j = 0; j < NP; ++j) acc[j] = redot(b, cmul2(d[j][e], p), acc[j]);
-    sl[so] = cmul2(v[e], b);
+    for (int j = 0; j < NP; ++j) acc[j] = redot(b, cmul2(sel4(d[j], e), p), acc[j]);
+    sl[so] = cmul2(ve, b);
   }
   flush_acc<NP>(acc, accw, op.slot);
 }
 
-// One diagonal op staged in shared memory for a run.
-struct DSub {
-  double2 v[4];
-  double2 d[4];       // v[e] * dU[e]: the gradient weight of entry e
-  uint32_t lm0, lm1;  // local bit masks of the MSB / LSB qubit (0: not local)
-  uint32_t fixed;     // index bits from non-local qubits (tile constant)
-  uint32_t b0;        // value of the MSB in the entry index (2 or 1)
-  uint32_t np, slot;
-  uint32_t pad[2];
+// One diagonal op of a run, staged in shared memory for the current tile.
+// The op's diagonal V over its entry index e = 2 b0 + b1 (b0: the MSB qubit;
+// a one-qubit op has b1 = 0) has modulus one, so it is exp(i theta(b0, b1))
+// with theta = al + be b0 + ga b1 + de b0 b1.  For this tile each qubit bit
+// is a constant (non-local qubit, or absent), a bit of threadIdx.x, or one
+// of the three register bits of the run's element layout (o = tid + 256 i).
+struct DRec {
+  double al, be, ga, de;
+  uint32_t k0, k1;  // 0: constant, 1: thread bit, 2: register bit
+  uint32_t p0, p1;  // constant value / bit of threadIdx.x / register bit
 };
 
-// A run of diagonal ops: each element goes through all of them in order
-// (they commute with nothing in between, so the order is the program's).
-__device__ __noinline__ void op_drun(double2* sp, double2* sl, const AOp* sub, uint32_t cnt,
-                                     const double2* pool, uint32_t m, uint64_t base, double* accw,
-                                     DSub* ds) {
-  if (threadIdx.x < cnt) {
-    const AOp op = sub[threadIdx.x];
-    DSub& D = ds[threadIdx.x];
-    D.lm0 = D.lm1 = D.fixed = 0;
-    D.b0 = op.ndq == 2 ? 2u : 1u;
-    for (uint32_t a = 0; a < op.ndq; ++a) {
-      const uint32_t e = op.dq[a];
-      const uint32_t bitv = (a == 0) ? D.b0 : 1u;
-      if (e & 0x80u) {
-        if (a == 0) D.lm0 = 1u << (e & 0x7fu);
-        else D.lm1 = 1u << (e & 0x7fu);
-      } else if ((base >> (e & 0x7fu)) & 1ULL) {
-        D.fixed |= bitv;
-      }
+__device__ __forceinline__ void drec_stage(DRec& D, const AOp& op, const double2* pool, uint64_t base) {
+  const double2* rec = pool + op.lctrl;
+  D.al = rec[0].x;
+  D.be = rec[0].y;
+  D.ga = rec[1].x;
+  D.de = rec[1].y;
+  uint32_t k[2] = {0, 0}, p[2] = {0, 0};
+  for (uint32_t a = 0; a < op.ndq; ++a) {
+    const uint32_t e = op.dq[a];
+    if (e & 0x80u) {
+      const uint32_t bp = e & 0x7fu;
+      k[a] = bp >= 8 ? 2u : 1u;
+      p[a] = bp >= 8 ? bp - 8 : bp;
+    } else {
+      p[a] = (uint32_t)((base >> (e & 0x7fu)) & 1ULL);
     }
-    const double2* mt = pool + op.mat;
-    for (int i = 0; i < 4; ++i) D.v[i] = mt[i];
-    for (int i = 0; i < 4; ++i)
-      D.d[i] = op.np ? cmul2(mt[i], mt[4 + i]) : make_double2(0.0, 0.0);
-    D.np = op.np;
-    D.slot = op.slot;
   }
+  D.k0 = k[0]; D.k1 = k[1];
+  D.p0 = p[0]; D.p1 = p[1];
+}
+
+__device__ __forceinline__ void gadd(double& g0, double& g1, double& g2, uint32_t r, double v) {
+  if (r == 0) g0 += v;
+  else if (r == 1) g1 += v;
+  else g2 += v;
+}
+
+// A run of diagonal ops in one elementwise pass.  Every diagonal entry has
+// modulus one, so z = conj(lambda) psi is the same before every op of the
+// run and op k's gradient term is
+//   Re sum_x z_x w_k[e_k(x)],   w_k = V_k dU_k  (entrywise).
+// Expanding w_k in the Walsh basis of its two index bits,
+//   w_k[2 b0 + b1] = sum_S what_k[S] (-1)^(b0 S0 + b1 S1),
+// turns the sum into four Walsh-Hadamard coefficients of z: a warp takes the
+// transform of its own 256 elements over the 8 bits that vary inside it
+// (3 register bits, 5 lane bits; the 3 warp bits and non-local bits are
+// constants that give a sign), after which each lane serves one op.  The run's
+// total phase is exp(i theta(x)) with theta a quadratic polynomial in the
+// index bits: each thread folds the ops into its constant, the linear terms of
+// its three register bits and their pairwise products, and one sincos per
+// element applies it to psi and lambda.  The host writes per op
+// rec[0] = (al, be), rec[1] = (ga, de), rec[2 + S] = what[S] at pool + lctrl.
+__device__ __noinline__ void op_drun(double2* sp, double2* sl, const AOp& hdr, const AOp* sub,
+                                     const double2* pool, uint32_t m, uint64_t base, double* accw,
+                                     DRec* ds) {
+  const uint32_t cnt = hdr.cnt;
+  for (uint32_t j = threadIdx.x; j < cnt; j += kAThreads) drec_stage(ds[j], sub[j], pool, base);
   __syncthreads();
-  // Every entry of a unitary diagonal has modulus 1, so z = conj(lambda) psi
-  // is the same before every op of the run, and op k's gradient term is
-  // Re(conj(lambda_k) dU_k V_k psi_k) = Re(z (V_k dU_k)[e]); psi and lambda
-  // then take the product of the run's phases once.  Ops are the outer loop
-  // (their parameters sit in registers), each thread's 8 elements the inner.
   const uint32_t L = 1u << m;
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  for (uint32_t o0 = 0; o0 < L; o0 += 8u * kAThreads) {
-    uint32_t oo[8];
-    double2 z[8], ph[8];
+  const uint32_t tid = threadIdx.x;
+  const int lane = tid & 31, w = tid >> 5;
+  if (hdr.np) {
+    double2 z[8];
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
-      oo[i] = o0 + threadIdx.x + (uint32_t)i * kAThreads;
+      const uint32_t o = tid + (uint32_t)i * kAThreads;
       double2 zz = make_double2(0.0, 0.0);
-      if (oo[i] < L) {
-        const uint32_t so = swz(oo[i]);
+      if (o < L) {
+        const uint32_t so = swz(o);
         const double2 a = sp[so], b = sl[so];
         zz = make_double2(fma(b.x, a.x, b.y * a.y), fma(b.x, a.y, -b.y * a.x));
       }
       z[i] = zz;
-      ph[i] = make_double2(1.0, 0.0);
     }
-#pragma unroll 1
-    for (uint32_t u = 0; u < cnt; ++u) {
-      double2 v[4], dw[4];
+    // Walsh-Hadamard transform over the register bits, then the lane bits:
+    // afterwards lane l, register r holds sum_x z_x (-1)^popc(x & M) over the
+    // warp's elements, M = l | r << 8
 #pragma unroll
-      for (int k = 0; k < 4; ++k) {
-        v[k] = ds[u].v[k];
-        dw[k] = ds[u].d[k];
-      }
-      const uint32_t fixed = ds[u].fixed, lm0 = ds[u].lm0, lm1 = ds[u].lm1, b0 = ds[u].b0;
-      const uint32_t np = ds[u].np;
-      double acc = 0.0;
+    for (int s = 1; s < 8; s <<= 1)
+#pragma unroll
+      for (int i = 0; i < 8; ++i)
+        if (!(i & s)) {
+          const double2 u = z[i], v = z[i | s];
+          z[i] = make_double2(u.x + v.x, u.y + v.y);
+          z[i | s] = make_double2(u.x - v.x, u.y - v.y);
+        }
+#pragma unroll
+    for (int s = 1; s < 32; s <<= 1) {
+      const bool up = (lane & s) != 0;
 #pragma unroll
       for (int i = 0; i < 8; ++i) {
-        const uint32_t e = fixed | ((oo[i] & lm0) ? b0 : 0u) | ((oo[i] & lm1) ? 1u : 0u);
-        ph[i] = cmul2(sel4(v, e), ph[i]);
-        const double2 wv = sel4(dw, e);
-        acc = fma(z[i].x, wv.x, fma(-z[i].y, wv.y, acc));
-      }
-      if (np) {
-        const double t = warp_sum_d(acc);
-        if (lane == 0) accw[ds[u].slot * kAWarps + w] += t;
+        const double px = __shfl_xor_sync(0xffffffffu, z[i].x, s);
+        const double py = __shfl_xor_sync(0xffffffffu, z[i].y, s);
+        z[i] = up ? make_double2(px - z[i].x, py - z[i].y) : make_double2(z[i].x + px, z[i].y + py);
       }
     }
+    for (uint32_t c0 = 0; c0 < cnt; c0 += 32) {
+      const uint32_t j = c0 + (uint32_t)lane;
+      double contrib = 0.0;
+      uint32_t slot = 0xffffffffu;
+      uint32_t src[4] = {0, 0, 0, 0}, reg[4] = {0, 0, 0, 0};
+      double2 wh[4];
+      if (j < cnt && sub[j].np) {
+        const AOp op = sub[j];
+        const DRec& D = ds[j];
+        slot = op.slot;
+        const double2* rec = pool + op.lctrl;
+        uint32_t lm[2], rm[2], cv[2];
+        const uint32_t kk[2] = {D.k0, D.k1}, pp[2] = {D.p0, D.p1};
 #pragma unroll
-    for (int i = 0; i < 8; ++i) {
-      if (oo[i] < L) {
-        const uint32_t so = swz(oo[i]);
-        sp[so] = cmul2(ph[i], sp[so]);
-        sl[so] = cmul2(ph[i], sl[so]);
+        for (int a = 0; a < 2; ++a) {
+          lm[a] = (kk[a] == 1 && pp[a] < 5) ? 1u << pp[a] : 0u;
+          rm[a] = kk[a] == 2 ? 1u << pp[a] : 0u;
+          cv[a] = kk[a] == 0 ? pp[a] : ((kk[a] == 1 && pp[a] >= 5) ? (tid >> pp[a]) & 1u : 0u);
+        }
+#pragma unroll
+        for (int S = 0; S < 4; ++S) {
+          const uint32_t s0 = (uint32_t)S >> 1, s1 = (uint32_t)S & 1u;
+          double2 v = rec[2 + S];
+          if ((s0 & cv[0]) ^ (s1 & cv[1])) v = make_double2(-v.x, -v.y);
+          wh[S] = v;
+          src[S] = (s0 ? lm[0] : 0u) | (s1 ? lm[1] : 0u);
+          reg[S] = (s0 ? rm[0] : 0u) | (s1 ? rm[1] : 0u);
+        }
+      } else {
+#pragma unroll
+        for (int S = 0; S < 4; ++S) wh[S] = make_double2(0.0, 0.0);
       }
+#pragma unroll
+      for (int S = 0; S < 4; ++S) {
+        double2 pz = make_double2(0.0, 0.0);
+#pragma unroll
+        for (int r = 0; r < 8; ++r) {
+          const double px = __shfl_sync(0xffffffffu, z[r].x, (int)src[S]);
+          const double py = __shfl_sync(0xffffffffu, z[r].y, (int)src[S]);
+          if (reg[S] == (uint32_t)r) pz = make_double2(px, py);
+        }
+        contrib = fma(wh[S].x, pz.x, fma(-wh[S].y, pz.y, contrib));
+      }
+      // the warp's terms in op order: deterministic slot sums
+      const uint32_t nk = cnt - c0 < 32u ? cnt - c0 : 32u;
+      for (uint32_t u = 0; u < nk; ++u) {
+        const double t = __shfl_sync(0xffffffffu, contrib, (int)u);
+        const uint32_t s = __shfl_sync(0xffffffffu, slot, (int)u);
+        if (lane == 0 && s != 0xffffffffu) accw[s * kAWarps + w] += t;
+      }
+    }
+  }
+  // the run's phase polynomial for this thread's eight elements
+  double T = 0.0, G0 = 0.0, G1 = 0.0, G2 = 0.0, H01 = 0.0, H02 = 0.0, H12 = 0.0;
+#pragma unroll 2
+  for (uint32_t u = 0; u < cnt; ++u) {
+    const DRec& D = ds[u];
+    const bool r0 = D.k0 == 2, r1 = D.k1 == 2;
+    const bool c0 = D.k0 == 1 ? ((tid >> D.p0) & 1u) != 0 : D.p0 != 0;
+    const bool c1 = D.k1 == 1 ? ((tid >> D.p1) & 1u) != 0 : D.p1 != 0;
+    if (!r0 && !r1) {
+      T += D.al + (c0 ? D.be : 0.0) + (c1 ? D.ga : 0.0) + ((c0 && c1) ? D.de : 0.0);
+    } else if (r0 && !r1) {
+      T += D.al + (c1 ? D.ga : 0.0);
+      gadd(G0, G1, G2, D.p0, D.be + (c1 ? D.de : 0.0));
+    } else if (!r0 && r1) {
+      T += D.al + (c0 ? D.be : 0.0);
+      gadd(G0, G1, G2, D.p1, D.ga + (c0 ? D.de : 0.0));
+    } else {
+      T += D.al;
+      gadd(G0, G1, G2, D.p0, D.be);
+      gadd(G0, G1, G2, D.p1, D.ga);
+      gadd(H01, H02, H12, D.p0 + D.p1 - 1u, D.de);
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    const uint32_t o = tid + (uint32_t)i * kAThreads;
+    if (o < L) {
+      double ang = T;
+      if (i & 1) ang += G0;
+      if (i & 2) ang += G1;
+      if (i & 4) ang += G2;
+      if ((i & 3) == 3) ang += H01;
+      if ((i & 5) == 5) ang += H02;
+      if ((i & 6) == 6) ang += H12;
+      double sn, cs;
+      sincos(ang, &sn, &cs);
+      const double2 ph = make_double2(cs, sn);
+      const uint32_t so = swz(o);
+      sp[so] = cmul2(ph, sp[so]);
+      sl[so] = cmul2(ph, sl[so]);
     }
   }
 }
 
 // One op of a register phase staged in shared memory.
 struct PSub {
-  double2 v[4];      // one-qubit: U^dagger; diagonal: conj(diag)
-  double2 d[4][4];   // derivatives (one-qubit: np 2x2; diagonal: d[0] = diag)
-  uint32_t kind;     // 0: one-qubit on phase bit pb; 1: diagonal
-  uint32_t pb;       // one-qubit: index of the target among the phase bits
+  double2 v[4];      // U^dagger
+  double2 d[4][4];   // np derivatives
+  uint32_t pb;       // index of the target among the phase bits
   uint32_t np, slot;
-  uint32_t lm0, lm1, fixed, b0;  // diagonal: as in DSub
+  uint32_t pad;
 };
+
+template <int PB>
+__device__ __forceinline__ int pair_lo(int k) {  // k-th index with bit PB clear
+  return PB == 0 ? 2 * k : (PB == 1 ? (k & 1) | ((k & 2) << 1) : k);
+}
 
 template <int PB>
 __device__ __forceinline__ void phase_one(double2 (&a)[8], double2 (&b)[8], const PSub& P,
                                           double (&acc)[4]) {
 #pragma unroll
-  for (int i = 0; i < 8; ++i) {
-    if (i & (1 << PB)) continue;
-    const int j = i | (1 << PB);
-    const double2 a0 = a[i], a1 = a[j], b0 = b[i], b1 = b[j];
-    const double2 p0 = cfma2(P.v[1], a1, cmul2(P.v[0], a0));
-    const double2 p1 = cfma2(P.v[3], a1, cmul2(P.v[2], a0));
-    a[i] = p0;
-    a[j] = p1;
+  for (int k = 0; k < 4; ++k) {
+    const int i = pair_lo<PB>(k), j = i | (1 << PB);
+    const double2 a0 = a[i], a1 = a[j];
+    a[i] = cfma2(P.v[1], a1, cmul2(P.v[0], a0));
+    a[j] = cfma2(P.v[3], a1, cmul2(P.v[2], a0));
+  }
+  // gradient terms per pair against the old lambda, summed as a tree
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      if (q < (int)P.np) {
-        const double2 w0 = cfma2(P.d[q][1], p1, cmul2(P.d[q][0], p0));
-        const double2 w1 = cfma2(P.d[q][3], p1, cmul2(P.d[q][2], p0));
-        acc[q] = redot(b0, w0, redot(b1, w1, acc[q]));
+  for (int q = 0; q < 4; ++q) {
+    if (q < (int)P.np) {
+      double t[4];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const int i = pair_lo<PB>(k), j = i | (1 << PB);
+        const double2 w0 = cfma2(P.d[q][1], a[j], cmul2(P.d[q][0], a[i]));
+        const double2 w1 = cfma2(P.d[q][3], a[j], cmul2(P.d[q][2], a[i]));
+        t[k] = redot(b[i], w0, b[j].x * w1.x + b[j].y * w1.y);
       }
+      acc[q] = (t[0] + t[1]) + (t[2] + t[3]);
     }
+  }
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const int i = pair_lo<PB>(k), j = i | (1 << PB);
+    const double2 b0 = b[i], b1 = b[j];
     b[i] = cfma2(P.v[1], b1, cmul2(P.v[0], b0));
     b[j] = cfma2(P.v[3], b1, cmul2(P.v[2], b0));
   }
@@ -393,12 +512,11 @@ __device__ __forceinline__ void phase_one(double2 (&a)[8], double2 (&b)[8], cons
 
 // A register phase: every thread holds the 8 amplitudes of psi and lambda
 // that differ in the phase's three local bits and applies the phase's
-// one-qubit ops (on those bits) and diagonal ops (on any qubits) in order.
-// Each op's gradient terms are reduced per warp right after the op (all
-// lanes take part: the group loop runs the same trip count on every thread).
+// uncontrolled one-qubit ops (on those bits) in order.  Each op's gradient
+// terms are reduced per warp right after the op (all lanes take part: the
+// group loop runs the same trip count on every thread).
 __device__ __noinline__ void op_phase(double2* sp, double2* sl, const AOp& hdr, const AOp* sub,
-                                      const double2* pool, uint32_t m, uint64_t base,
-                                      double* accw, PSub* ps) {
+                                      const double2* pool, uint32_t m, double* accw, PSub* ps) {
   const uint32_t cnt = hdr.cnt;
   const uint32_t pbits[3] = {hdr.lt, hdr.lt2, (uint32_t)hdr.dq[0]};
   if (threadIdx.x < cnt) {
@@ -407,29 +525,10 @@ __device__ __noinline__ void op_phase(double2* sp, double2* sl, const AOp& hdr, 
     const double2* mt = pool + op.mat;
     P.np = op.np;
     P.slot = op.slot;
-    if (op.type == A_ONE) {
-      P.kind = 0;
-      P.pb = op.lt == pbits[0] ? 0u : (op.lt == pbits[1] ? 1u : 2u);
-      for (int i = 0; i < 4; ++i) P.v[i] = mt[i];
-      for (uint32_t q = 0; q < op.np; ++q)
-        for (int i = 0; i < 4; ++i) P.d[q][i] = mt[4 + 4 * q + i];
-    } else {
-      P.kind = 1;
-      P.lm0 = P.lm1 = P.fixed = 0;
-      P.b0 = op.ndq == 2 ? 2u : 1u;
-      for (uint32_t a = 0; a < op.ndq; ++a) {
-        const uint32_t e = op.dq[a];
-        const uint32_t bitv = (a == 0) ? P.b0 : 1u;
-        if (e & 0x80u) {
-          if (a == 0) P.lm0 = 1u << (e & 0x7fu);
-          else P.lm1 = 1u << (e & 0x7fu);
-        } else if ((base >> (e & 0x7fu)) & 1ULL) {
-          P.fixed |= bitv;
-        }
-      }
-      for (int i = 0; i < 4; ++i) P.v[i] = mt[i];
-      for (int i = 0; i < 4; ++i) P.d[0][i] = op.np ? mt[4 + i] : make_double2(0.0, 0.0);
-    }
+    P.pb = op.lt == pbits[0] ? 0u : (op.lt == pbits[1] ? 1u : 2u);
+    for (int i = 0; i < 4; ++i) P.v[i] = mt[i];
+    for (uint32_t q = 0; q < op.np; ++q)
+      for (int i = 0; i < 4; ++i) P.d[q][i] = mt[4 + 4 * q + i];
   }
   __syncthreads();
   const uint32_t groups = (1u << m) >> 3;
@@ -453,22 +552,9 @@ __device__ __noinline__ void op_phase(double2* sp, double2* sl, const AOp& hdr, 
     for (uint32_t u = 0; u < cnt; ++u) {
       const PSub& P = ps[u];
       double acc[4] = {0.0, 0.0, 0.0, 0.0};
-      if (P.kind == 0) {
-        if (P.pb == 0) phase_one<0>(a, b, P, acc);
-        else if (P.pb == 1) phase_one<1>(a, b, P, acc);
-        else phase_one<2>(a, b, P, acc);
-      } else {
-#pragma unroll
-        for (int i = 0; i < 8; ++i) {
-          const uint32_t o = off[i];
-          const uint32_t e = P.fixed | ((o & P.lm0) ? P.b0 : 0u) | ((o & P.lm1) ? 1u : 0u);
-          const double2 vv = P.v[e];
-          const double2 p = cmul2(vv, a[i]);
-          if (P.np) acc[0] = redot(b[i], cmul2(P.d[0][e], p), acc[0]);
-          b[i] = cmul2(vv, b[i]);
-          a[i] = p;
-        }
-      }
+      if (P.pb == 0) phase_one<0>(a, b, P, acc);
+      else if (P.pb == 1) phase_one<1>(a, b, P, acc);
+      else phase_one<2>(a, b, P, acc);
       for (uint32_t q = 0; q < P.np; ++q) {
         const double v = warp_sum_d(acc[q]);
         if (lane == 0) accw[(P.slot + q) * kAWarps + w] += v;
@@ -490,7 +576,7 @@ __global__ void __launch_bounds__(kAThreads, 2)
   extern __shared__ __align__(16) unsigned char smraw[];
   __shared__ ASweepHdr H;
   __shared__ uint64_t hi_tab[64];
-  __shared__ DSub dsub[kADiagRun];
+  __shared__ DRec drec[kADiagRun];
   __shared__ PSub psub[kAPhaseOps];
   if (threadIdx.x == 0) H = *hp;
   __syncthreads();
@@ -528,13 +614,13 @@ __global__ void __launch_bounds__(kAThreads, 2)
     for (uint32_t i = 0; i < H.nops; ++i) {
       const AOp op = ops[i];
       if (op.type == A_DRUN) {
-        op_drun(sp, sl, ops + i + 1, op.cnt, pool, m, base, accw, dsub);
+        op_drun(sp, sl, op, ops + i + 1, pool, m, base, accw, drec);
         i += op.cnt;
         __syncthreads();
         continue;
       }
       if (op.type == A_PHASE) {
-        op_phase(sp, sl, op, ops + i + 1, pool, m, base, accw, psub);
+        op_phase(sp, sl, op, ops + i + 1, pool, m, accw, psub);
         i += op.cnt;
         __syncthreads();
         continue;
@@ -633,8 +719,10 @@ int classify_gate(const dq_inst& in, const int32_t* pidx, uint64_t r, uint32_t s
     for (int a = 0; a < nact; ++a)
       for (int i = 0; i < 4; ++i) g.du[a][i] = d[active[a]][i];
     // diagonal only if the matrix and every active derivative are (ry(0) is
-    // the identity, its derivative is not diagonal)
-    bool dg = diag2(u);
+    // the identity, its derivative is not diagonal) and at most one
+    // parameter is active (u3(0, phi, lambda) with both angles trainable
+    // stays a 2x2 op, which carries up to four derivatives)
+    bool dg = diag2(u) && nact <= 1;
     for (int a = 0; a < nact; ++a) dg = dg && diag2(g.du[a]);
     if (!ctl) {
       g.t = (uint32_t)in.q[0];
@@ -744,6 +832,32 @@ void push_mats(std::vector<double2>& pool, const hc* m, int count) {
   for (int i = 0; i < count; ++i) pool.push_back(make_double2(m[i].re, m[i].im));
 }
 
+// The record op_drun reads for a diagonal op: the angle polynomial of its
+// entries V[2 b0 + b1] = exp(i (al + be b0 + ga b1 + de b0 b1)) and the Walsh
+// coefficients what[2 S0 + S1] = 1/4 sum_e V[e] dU[e] (-1)^(b0 S0 + b1 S1).
+// A one-qubit diagonal (entry index b0) is the same with b1 = 0: its
+// coefficients with S1 = 1 vanish.
+void push_drun_record(std::vector<double2>& pool, const hc v[4], const hc dd[4], uint32_t nq) {
+  double th[4];
+  hc w[4];
+  for (int e = 0; e < 4; ++e) {
+    const int src = nq == 2 ? e : (e >> 1);
+    th[e] = std::atan2(v[src].im, v[src].re);
+    w[e] = hc{v[src].re * dd[src].re - v[src].im * dd[src].im, v[src].re * dd[src].im + v[src].im * dd[src].re};
+  }
+  pool.push_back(make_double2(th[0], th[2] - th[0]));
+  pool.push_back(make_double2(th[1] - th[0], th[3] - th[2] - th[1] + th[0]));
+  for (int S = 0; S < 4; ++S) {
+    double re = 0.0, im = 0.0;
+    for (int e = 0; e < 4; ++e) {
+      const bool neg = (((e >> 1) & (S >> 1)) ^ (e & S & 1)) != 0;
+      re += neg ? -w[e].re : w[e].re;
+      im += neg ? -w[e].im : w[e].im;
+    }
+    pool.push_back(make_double2(0.25 * re, 0.25 * im));
+  }
+}
+
 // Encodes one sweep's ops given its final local set.
 int encode_asweep(const ASweepPlan& sp, uint32_t n, ASweepHdr& hdr, std::vector<AOp>& ops,
                   std::vector<double2>& pool, std::vector<uint32_t>& slot_map) {
@@ -808,23 +922,27 @@ int encode_asweep(const ASweepPlan& sp, uint32_t n, ASweepHdr& hdr, std::vector<
       const uint32_t D = 1u << g.nq;
       for (uint32_t i = 0; i < D; ++i) v[i] = cjh(g.dg[i]);
       push_mats(pool, v, 4);
-      for (int a = 0; a < g.np; ++a) {
-        hc dd[4] = {R(0), R(0), R(0), R(0)};
-        for (uint32_t i = 0; i < D; ++i) dd[i] = g.ddg[a][i];
+      hc dd[4] = {R(0), R(0), R(0), R(0)};
+      if (g.np > 1) return fail(DQ_ERR_INTERNAL, "diagonal op with more than one derivative");
+      if (g.np) {
+        for (uint32_t i = 0; i < D; ++i) dd[i] = g.ddg[0][i];
         push_mats(pool, dd, 4);
       }
+      op.lctrl = (uint32_t)pool.size();
+      push_drun_record(pool, v, dd, g.nq);
     }
     ops.push_back(op);
   }
-  // register phases: maximal runs of uncontrolled one-qubit ops (targets
-  // within three local bits) and diagonal ops, with at least one one-qubit op
+  // register phases: maximal runs (two or more) of uncontrolled one-qubit ops
+  // whose targets fit three local bits; diagonal ops end a phase and go to
+  // the diagonal runs, which apply them far more cheaply
   if (m >= 3) {
     std::vector<AOp> phased;
     size_t i = 0;
     while (i < ops.size()) {
       const AOp& o = ops[i];
       const bool one = o.type == A_ONE && o.lctrl == 0 && o.sel < 0;
-      if (!one && o.type != A_DIAG) {
+      if (!one) {
         phased.push_back(ops[i++]);
         continue;
       }
@@ -834,7 +952,6 @@ int encode_asweep(const ASweepPlan& sp, uint32_t n, ASweepHdr& hdr, std::vector<
       uint32_t nones = 0;
       while (j < ops.size() && j - i < kAPhaseOps) {
         const AOp& q = ops[j];
-        if (q.type == A_DIAG) { ++j; continue; }
         if (!(q.type == A_ONE && q.lctrl == 0 && q.sel < 0)) break;
         bool have = false;
         for (uint32_t b = 0; b < nb; ++b) have = have || bits[b] == q.lt;
@@ -845,7 +962,7 @@ int encode_asweep(const ASweepPlan& sp, uint32_t n, ASweepHdr& hdr, std::vector<
         ++nones;
         ++j;
       }
-      if (nones == 0) {  // diagonal ops only: left to the diagonal runs
+      if (nones < 2) {  // a single op: the plain one-qubit pass
         for (size_t k = i; k < j; ++k) phased.push_back(ops[k]);
         i = j;
         continue;
@@ -883,10 +1000,13 @@ int encode_asweep(const ASweepPlan& sp, uint32_t n, ASweepHdr& hdr, std::vector<
     }
     size_t j = i;
     while (j < ops.size() && ops[j].type == A_DIAG && j - i < kADiagRun) ++j;
-    AOp h{};
-    h.type = A_DRUN;
-    h.cnt = (uint8_t)(j - i);
-    grouped.push_back(h);
+    if (j - i >= kADiagRunMin) {
+      AOp h{};
+      h.type = A_DRUN;
+      h.cnt = (uint8_t)(j - i);
+      for (size_t k = i; k < j; ++k) h.np = (uint8_t)(h.np | (ops[k].np ? 1 : 0));
+      grouped.push_back(h);
+    }
     for (size_t k = i; k < j; ++k) grouped.push_back(ops[k]);
     i = j;
   }

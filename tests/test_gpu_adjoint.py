@@ -245,3 +245,70 @@ def test_special_angles_keep_their_derivatives(gpu, angle):
     ps = orc.param_shift(c, theta, H.array())
     assert np.max(np.abs(g1 - ps)) < TOL_SHIFT
     assert np.max(np.abs(g2 - ps)) < TOL_SHIFT
+
+
+def diagonal_run_circuit(n, depth, seed):
+    """Layers of ry then long runs of diagonal gates (trainable and fixed) on
+    random qubits: low, middle and high bits, so a run mixes register, lane,
+    warp and non-local qubits and runs of more than 64 ops get split."""
+    rng = np.random.default_rng(seed)
+    c = ParamCircuit(n)
+    k = 0
+    diag1 = ["rz", "p", "u1", "z", "s", "t", "sdg"]
+    diag2 = ["rzz", "cp", "crz", "cu1", "cz"]
+    for layer in range(depth):
+        for q in range(n):
+            c.ry(q, Param(k)); k += 1
+        for _ in range(20 + 40 * layer):
+            if rng.random() < 0.5:
+                kind = diag1[rng.integers(len(diag1))]
+                qs = [int(rng.integers(n))]
+            else:
+                kind = diag2[rng.integers(len(diag2))]
+                qs = [int(v) for v in rng.permutation(n)[:2]]
+            npar = _PARAM_COUNT_T.get(kind, 0)
+            c.add(kind, qs, [Param(k + j) for j in range(npar)])
+            k += npar
+    theta = rng.uniform(-np.pi, np.pi, size=k)
+    return c, theta
+
+
+_PARAM_COUNT_T = {"rz": 1, "p": 1, "u1": 1, "rzz": 1, "cp": 1, "crz": 1, "cu1": 1}
+
+
+@pytest.mark.parametrize("n,seed", [(14, 5), (17, 6), (9, 7)])
+def test_long_diagonal_runs_match_per_gate_and_parameter_shift(gpu, n, seed):
+    c, theta = diagonal_run_circuit(n, 3, seed)
+    H = random_observable(n, 12, seed=seed + 20)
+    e1, g1 = adjoint_gradient(c, theta, H, exec="fused")
+    e2, g2 = adjoint_gradient(c, theta, H, exec="per_gate")
+    assert abs(e1 - e2) < 1e-12
+    assert np.max(np.abs(g1 - g2)) < 1e-11, np.max(np.abs(g1 - g2))
+    sub = list(range(0, theta.size, max(1, theta.size // 16)))
+    ps = orc.param_shift(c, theta, H.array(), occurrences=sub)
+    assert np.max(np.abs(g1[sub] - ps[sub])) < TOL_SHIFT
+
+
+def test_diagonal_gates_with_two_trainable_angles(gpu):
+    # u3(0, phi, lambda) and cu3(0, phi, lambda) are diagonal with two
+    # diagonal derivatives each: both must reach the gradient
+    n = 12
+    c = ParamCircuit(n)
+    k = 0
+    for q in range(n):
+        c.ry(q, Param(k)); k += 1
+    for q in range(n):
+        c.add("u3", [q], [0.0, Param(k), Param(k + 1)]); k += 2
+    for q in range(n - 1):
+        c.add("cu3", [q, q + 1], [0.0, Param(k), Param(k + 1)]); k += 2
+        c.add("cu", [q + 1, q], [0.0, Param(k), Param(k + 1), Param(k + 2)]); k += 3
+    for q in range(n):
+        c.rx(q, Param(k)); k += 1
+    theta = np.random.default_rng(3).uniform(-np.pi, np.pi, size=k)
+    H = random_observable(n, 10, seed=8)
+    e1, g1 = adjoint_gradient(c, theta, H, exec="fused")
+    e2, g2 = adjoint_gradient(c, theta, H, exec="per_gate")
+    assert abs(e1 - e2) < 1e-12
+    assert np.max(np.abs(g1 - g2)) < 1e-11
+    ps = orc.param_shift(c, theta, H.array())
+    assert np.max(np.abs(g1 - ps)) < TOL_SHIFT
