@@ -465,10 +465,11 @@ __device__ __noinline__ void op_drun(double2* sp, double2* sl, const AOp& hdr, c
 // One op of a register phase staged in shared memory.
 struct PSub {
   double2 v[4];      // U^dagger
-  double2 d[4][4];   // np derivatives
+  double2 d[4][4];   // np derivatives in the form D' = dU U^dagger (applied to psi before V)
   uint32_t pb;       // index of the target among the phase bits
+  uint32_t vk;       // 0: general V; 1: real V; 2: real diagonal, imaginary off-diagonal
   uint32_t np, slot;
-  uint32_t pad;
+  uint32_t tm[4];    // per derivative: bit 2e / 2e + 1 set if Re / Im of D'[e] is non-zero
 };
 
 template <int PB>
@@ -476,37 +477,70 @@ __device__ __forceinline__ int pair_lo(int k) {  // k-th index with bit PB clear
   return PB == 0 ? 2 * k : (PB == 1 ? (k & 1) | ((k & 2) << 1) : k);
 }
 
+// Re sum over the thread's pairs of conj(lambda) D' psi, term by term of D':
+// Re(D'[r][c] conj(l_r) p_c) = Re D' Re(conj(l_r) p_c) - Im D' Im(conj(l_r) p_c),
+// skipping the parts of D' that are zero (ry: two real entries, rx: two
+// imaginary ones).
 template <int PB>
-__device__ __forceinline__ void phase_one(double2 (&a)[8], double2 (&b)[8], const PSub& P,
-                                          double (&acc)[4]) {
+__device__ __forceinline__ double grad_terms(const double2 (&a)[8], const double2 (&b)[8], const double2* dp,
+                                             uint32_t tm) {
+  double s = 0.0;
 #pragma unroll
-  for (int k = 0; k < 4; ++k) {
-    const int i = pair_lo<PB>(k), j = i | (1 << PB);
-    const double2 a0 = a[i], a1 = a[j];
-    a[i] = cfma2(P.v[1], a1, cmul2(P.v[0], a0));
-    a[j] = cfma2(P.v[3], a1, cmul2(P.v[2], a0));
-  }
-  // gradient terms per pair against the old lambda, summed as a tree
-#pragma unroll
-  for (int q = 0; q < 4; ++q) {
-    if (q < (int)P.np) {
+  for (int e = 0; e < 4; ++e) {
+    const int r = e >> 1, c = e & 1;
+    if (tm & (1u << (2 * e))) {
       double t[4];
 #pragma unroll
       for (int k = 0; k < 4; ++k) {
         const int i = pair_lo<PB>(k), j = i | (1 << PB);
-        const double2 w0 = cfma2(P.d[q][1], a[j], cmul2(P.d[q][0], a[i]));
-        const double2 w1 = cfma2(P.d[q][3], a[j], cmul2(P.d[q][2], a[i]));
-        t[k] = redot(b[i], w0, b[j].x * w1.x + b[j].y * w1.y);
+        const double2 l = b[r ? j : i], p = a[c ? j : i];
+        t[k] = fma(l.x, p.x, l.y * p.y);
       }
-      acc[q] = (t[0] + t[1]) + (t[2] + t[3]);
+      s = fma(dp[e].x, (t[0] + t[1]) + (t[2] + t[3]), s);
+    }
+    if (tm & (2u << (2 * e))) {
+      double t[4];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const int i = pair_lo<PB>(k), j = i | (1 << PB);
+        const double2 l = b[r ? j : i], p = a[c ? j : i];
+        t[k] = fma(l.x, p.y, -l.y * p.x);
+      }
+      s = fma(-dp[e].y, (t[0] + t[1]) + (t[2] + t[3]), s);
     }
   }
+  return s;
+}
+
+// y = V x on one pair for the three shapes of V
+template <int VK>
+__device__ __forceinline__ void apply2(const double2* v, double2& x0, double2& x1) {
+  const double2 a0 = x0, a1 = x1;
+  if (VK == 1) {
+    x0 = make_double2(fma(v[1].x, a1.x, v[0].x * a0.x), fma(v[1].x, a1.y, v[0].x * a0.y));
+    x1 = make_double2(fma(v[3].x, a1.x, v[2].x * a0.x), fma(v[3].x, a1.y, v[2].x * a0.y));
+  } else if (VK == 2) {
+    x0 = make_double2(fma(-v[1].y, a1.y, v[0].x * a0.x), fma(v[1].y, a1.x, v[0].x * a0.y));
+    x1 = make_double2(fma(v[3].x, a1.x, -v[2].y * a0.y), fma(v[3].x, a1.y, v[2].y * a0.x));
+  } else {
+    x0 = cfma2(v[1], a1, cmul2(v[0], a0));
+    x1 = cfma2(v[3], a1, cmul2(v[2], a0));
+  }
+}
+
+template <int PB, int VK>
+__device__ __forceinline__ void phase_one(double2 (&a)[8], double2 (&b)[8], const PSub& P,
+                                          double (&acc)[4]) {
+  // gradient terms Re <lambda_k| dU U^dagger |psi_k> from the amplitudes
+  // before the op, then psi and lambda both take V = U^dagger
+#pragma unroll
+  for (int q = 0; q < 4; ++q)
+    if (q < (int)P.np) acc[q] = grad_terms<PB>(a, b, P.d[q], P.tm[q]);
 #pragma unroll
   for (int k = 0; k < 4; ++k) {
     const int i = pair_lo<PB>(k), j = i | (1 << PB);
-    const double2 b0 = b[i], b1 = b[j];
-    b[i] = cfma2(P.v[1], b1, cmul2(P.v[0], b0));
-    b[j] = cfma2(P.v[3], b1, cmul2(P.v[2], b0));
+    apply2<VK>(P.v, a[i], a[j]);
+    apply2<VK>(P.v, b[i], b[j]);
   }
 }
 
@@ -527,8 +561,20 @@ __device__ __noinline__ void op_phase(double2* sp, double2* sl, const AOp& hdr, 
     P.slot = op.slot;
     P.pb = op.lt == pbits[0] ? 0u : (op.lt == pbits[1] ? 1u : 2u);
     for (int i = 0; i < 4; ++i) P.v[i] = mt[i];
-    for (uint32_t q = 0; q < op.np; ++q)
-      for (int i = 0; i < 4; ++i) P.d[q][i] = mt[4 + 4 * q + i];
+    const bool real = mt[0].y == 0.0 && mt[1].y == 0.0 && mt[2].y == 0.0 && mt[3].y == 0.0;
+    const bool rxl = mt[0].y == 0.0 && mt[3].y == 0.0 && mt[1].x == 0.0 && mt[2].x == 0.0;
+    P.vk = real ? 1u : (rxl ? 2u : 0u);
+    // D' blocks follow the dU blocks (uncontrolled one-qubit ops only)
+    for (uint32_t q = 0; q < op.np; ++q) {
+      uint32_t tm = 0;
+      for (int i = 0; i < 4; ++i) {
+        const double2 dv = mt[4 + 4 * op.np + 4 * q + i];
+        P.d[q][i] = dv;
+        tm |= (dv.x != 0.0 ? 1u : 0u) << (2 * i);
+        tm |= (dv.y != 0.0 ? 2u : 0u) << (2 * i);
+      }
+      P.tm[q] = tm;
+    }
   }
   __syncthreads();
   const uint32_t groups = (1u << m) >> 3;
@@ -537,24 +583,31 @@ __device__ __noinline__ void op_phase(double2* sp, double2* sl, const AOp& hdr, 
     const uint32_t g = g0 + threadIdx.x;
     const bool valid = g < groups;
     const uint32_t ob = ins0a(ins0a(ins0a(valid ? g : 0u, pbits[0]), pbits[1]), pbits[2]);
-    uint32_t off[8];
-#pragma unroll
-    for (int i = 0; i < 8; ++i)
-      off[i] = ob | ((i & 1) ? 1u << pbits[0] : 0u) | ((i & 2) ? 1u << pbits[1] : 0u) |
-               ((i & 4) ? 1u << pbits[2] : 0u);
+    const uint32_t m0 = 1u << pbits[0], m1 = 1u << pbits[1], m2 = 1u << pbits[2];
+    auto off = [&](int i) {
+      return ob | ((i & 1) ? m0 : 0u) | ((i & 2) ? m1 : 0u) | ((i & 4) ? m2 : 0u);
+    };
     double2 a[8], b[8];
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
-      a[i] = valid ? sp[swz(off[i])] : make_double2(0.0, 0.0);
-      b[i] = valid ? sl[swz(off[i])] : make_double2(0.0, 0.0);
+      a[i] = valid ? sp[swz(off(i))] : make_double2(0.0, 0.0);
+      b[i] = valid ? sl[swz(off(i))] : make_double2(0.0, 0.0);
     }
 #pragma unroll 1
     for (uint32_t u = 0; u < cnt; ++u) {
       const PSub& P = ps[u];
       double acc[4] = {0.0, 0.0, 0.0, 0.0};
-      if (P.pb == 0) phase_one<0>(a, b, P, acc);
-      else if (P.pb == 1) phase_one<1>(a, b, P, acc);
-      else phase_one<2>(a, b, P, acc);
+      switch (P.pb * 3 + P.vk) {
+        case 0: phase_one<0, 0>(a, b, P, acc); break;
+        case 1: phase_one<0, 1>(a, b, P, acc); break;
+        case 2: phase_one<0, 2>(a, b, P, acc); break;
+        case 3: phase_one<1, 0>(a, b, P, acc); break;
+        case 4: phase_one<1, 1>(a, b, P, acc); break;
+        case 5: phase_one<1, 2>(a, b, P, acc); break;
+        case 6: phase_one<2, 0>(a, b, P, acc); break;
+        case 7: phase_one<2, 1>(a, b, P, acc); break;
+        default: phase_one<2, 2>(a, b, P, acc); break;
+      }
       for (uint32_t q = 0; q < P.np; ++q) {
         const double v = warp_sum_d(acc[q]);
         if (lane == 0) accw[(P.slot + q) * kAWarps + w] += v;
@@ -563,8 +616,8 @@ __device__ __noinline__ void op_phase(double2* sp, double2* sl, const AOp& hdr, 
     if (valid) {
 #pragma unroll
       for (int i = 0; i < 8; ++i) {
-        sp[swz(off[i])] = a[i];
-        sl[swz(off[i])] = b[i];
+        sp[swz(off(i))] = a[i];
+        sl[swz(off(i))] = b[i];
       }
     }
   }
@@ -832,6 +885,26 @@ void push_mats(std::vector<double2>& pool, const hc* m, int count) {
   for (int i = 0; i < count; ++i) pool.push_back(make_double2(m[i].re, m[i].im));
 }
 
+// D' = dU V (V = U^dagger, both 2x2 row-major): the derivative in the form
+// that acts on the amplitudes before the op.  Parts below 1e-14 of the
+// largest are rounding residue of exact zeros (ry: dU V = -i Y / 2) and are
+// stored as zeros, which the register phases skip.
+void push_dprime(std::vector<double2>& pool, const hc du[4], const hc v[4]) {
+  hc d[4];
+  double mx = 0.0;
+  for (int r = 0; r < 2; ++r)
+    for (int c = 0; c < 2; ++c) {
+      const hc x = du[2 * r] * v[c] + du[2 * r + 1] * v[2 + c];
+      d[2 * r + c] = x;
+      mx = std::max(mx, std::max(std::fabs(x.re), std::fabs(x.im)));
+    }
+  for (hc& x : d) {
+    if (std::fabs(x.re) <= 1e-14 * mx) x.re = 0.0;
+    if (std::fabs(x.im) <= 1e-14 * mx) x.im = 0.0;
+  }
+  push_mats(pool, d, 4);
+}
+
 // The record op_drun reads for a diagonal op: the angle polynomial of its
 // entries V[2 b0 + b1] = exp(i (al + be b0 + ga b1 + de b0 b1)) and the Walsh
 // coefficients what[2 S0 + S1] = 1/4 sum_e V[e] dU[e] (-1)^(b0 S0 + b1 S1).
@@ -903,6 +976,8 @@ int encode_asweep(const ASweepPlan& sp, uint32_t n, ASweepHdr& hdr, std::vector<
       }
       push_mats(pool, v, 4);
       for (int a = 0; a < g.np; ++a) push_mats(pool, g.du[a], 4);
+      if (g.kind == 0)
+        for (int a = 0; a < g.np; ++a) push_dprime(pool, g.du[a], v);
     } else if (g.kind == 3) {
       op.type = A_TWO;
       op.lt = (uint8_t)lidx[g.qa];
