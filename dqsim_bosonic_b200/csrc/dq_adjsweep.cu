@@ -583,15 +583,18 @@ __device__ __noinline__ void op_phase(double2* sp, double2* sl, const AOp& hdr, 
     const uint32_t g = g0 + threadIdx.x;
     const bool valid = g < groups;
     const uint32_t ob = ins0a(ins0a(ins0a(valid ? g : 0u, pbits[0]), pbits[1]), pbits[2]);
-    const uint32_t m0 = 1u << pbits[0], m1 = 1u << pbits[1], m2 = 1u << pbits[2];
+    // swz is linear over XOR and ob has the phase bits clear, so
+    // swz(ob | bits) = swz(ob) ^ swz(bits)
+    const uint32_t sb = swz(ob);
+    const uint32_t s0 = swz(1u << pbits[0]), s1 = swz(1u << pbits[1]), s2 = swz(1u << pbits[2]);
     auto off = [&](int i) {
-      return ob | ((i & 1) ? m0 : 0u) | ((i & 2) ? m1 : 0u) | ((i & 4) ? m2 : 0u);
+      return sb ^ ((i & 1) ? s0 : 0u) ^ ((i & 2) ? s1 : 0u) ^ ((i & 4) ? s2 : 0u);
     };
     double2 a[8], b[8];
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
-      a[i] = valid ? sp[swz(off(i))] : make_double2(0.0, 0.0);
-      b[i] = valid ? sl[swz(off(i))] : make_double2(0.0, 0.0);
+      a[i] = valid ? sp[off(i)] : make_double2(0.0, 0.0);
+      b[i] = valid ? sl[off(i)] : make_double2(0.0, 0.0);
     }
 #pragma unroll 1
     for (uint32_t u = 0; u < cnt; ++u) {
@@ -616,8 +619,8 @@ __device__ __noinline__ void op_phase(double2* sp, double2* sl, const AOp& hdr, 
     if (valid) {
 #pragma unroll
       for (int i = 0; i < 8; ++i) {
-        sp[swz(off(i))] = a[i];
-        sl[swz(off(i))] = b[i];
+        sp[off(i)] = a[i];
+        sl[off(i)] = b[i];
       }
     }
   }
