@@ -3,7 +3,7 @@
 // The per-gate backward (dq_adjoint.cu) streams psi and lambda through HBM
 // once per gate (64 B per amplitude per gate).  Here a sweep loads a tile of
 // 2^m amplitudes of both vectors into shared memory (the tile spans the m
-// "local" qubits: bits 0..4 for coalescing plus up to m - 5 chosen ones),
+// "local" qubits: bits 0..2 for coalescing plus up to m - 3 chosen ones),
 // applies a run of gates in reverse program order to both, reduces every
 // gate's gradient terms, and writes the tile back: 64 B per amplitude per
 // sweep instead of per gate.  A gate can join the current sweep when
@@ -49,6 +49,7 @@ namespace {
 constexpr int kAThreads = 256;
 constexpr int kAWarps = kAThreads / 32;
 constexpr uint32_t kAMaxLocal = 11;
+constexpr uint32_t kALoMin = 3;  // qubits 0..2 stay local: 128-byte runs per tile load
 constexpr uint32_t kAMaxOps = 192;
 constexpr uint32_t kAMaxSlots = 192;
 
@@ -631,7 +632,7 @@ __global__ void __launch_bounds__(kAThreads, 2)
                 const AOp* __restrict__ ops, const double2* __restrict__ pool, double* partial) {
   extern __shared__ __align__(16) unsigned char smraw[];
   __shared__ ASweepHdr H;
-  __shared__ uint64_t hi_tab[64];
+  __shared__ uint64_t hi_tab[1u << (kAMaxLocal - kALoMin)];
   __shared__ DRec drec[kADiagRun];
   __shared__ PSub psub[kAPhaseOps];
   if (threadIdx.x == 0) H = *hp;
@@ -642,7 +643,10 @@ __global__ void __launch_bounds__(kAThreads, 2)
   double* accw = reinterpret_cast<double*>(sl + L);
   for (uint32_t i = threadIdx.x; i < H.nslots * kAWarps; i += kAThreads) accw[i] = 0.0;
   // offset bits above the 5 contiguous ones -> global bits
-  const uint32_t lo_bits = m < 5 ? m : 5;
+  // local bits 0 .. lo_bits-1 are qubits 0 .. lo_bits-1: runs of 2^lo_bits
+  // consecutive amplitudes (at least 128 B)
+  uint32_t lo_bits = 0;
+  while (lo_bits < m && lo_bits < 5 && H.lpos[lo_bits] == lo_bits) ++lo_bits;
   const uint32_t nhi = m - lo_bits;
   for (uint32_t hv = threadIdx.x; hv < (1u << nhi); hv += kAThreads) {
     uint64_t g = 0;
@@ -1126,7 +1130,7 @@ int adjoint_backward_fused(double2* psi, double2* lam, uint32_t n, const dq_inst
   }
   if (first_slot[ninst] != nslots) return fail(DQ_ERR_INTERNAL, "slot count mismatch");
   const uint32_t m_max = std::min<uint32_t>(n, kAMaxLocal);
-  const uint32_t lo = std::min<uint32_t>(n, 5);
+  const uint32_t lo = std::min<uint32_t>(n, kALoMin);
   const uint64_t lo_mask = (1ULL << lo) - 1;
   // segments: sweeps and per-gate instructions, in backward order
   struct Seg {
