@@ -715,19 +715,24 @@ def sweep_traffic(n: int):
 
 
 def fused_sweep_timing(st, prog, stream, reps):
-    """Average duration of one fused sweep, from CUDA events around every
-    sweep launch on the state's stream (dq_run_opts.time_sweeps)."""
+    """Average duration and algorithmic bytes of one fused sweep, from CUDA
+    events around every sweep launch on the state's stream
+    (dq_run_opts.time_sweeps).  Every sweep reads and writes the state
+    (2 x 16 B per amplitude) except the first one after a reset, which
+    generates its input from the basis index and only writes (16 B)."""
     from dqsim_bosonic_b200 import _native as nat
     from dqsim_bosonic_b200.statevector import run_program
 
-    tot, cnt = 0.0, 0
+    tot, cnt, runs = 0.0, 0, 0
     for _ in range(reps):
         st.reset()
         _, prof = run_program(st, prog, 7, nat.SEM_SIMULATE, nat.EXEC_FUSED, time_sweeps=True)
         tot += prof.sweep_time
         cnt += int(prof.sweeps)
+        runs += 1 if prof.sweeps else 0
     n = prog.num_qubits
-    return "k_sweep (fused tile sweep)", 2 * 16 * (2 ** n), tot / max(cnt, 1) * 1e3
+    nbytes = (2 * cnt - runs) * 16 * (2 ** n) / max(cnt, 1)
+    return "k_sweep (fused tile sweep)", nbytes, tot / max(cnt, 1) * 1e3
 
 
 if __name__ == "__main__":

@@ -511,7 +511,7 @@ int dq_expval_pauli(dq_state_t h, const dq_pauli_term* terms, uint64_t nterms, d
 int dq_adjoint(dq_state_t h, const dq_inst* prog, uint64_t ninst, const int32_t* param_index,
                uint64_t nparams, const dq_pauli_term* terms, uint64_t nterms,
                const dq_run_opts* opts, double* expval, double* grad, double* phase_ms) {
-  DQ_TRY(check_handle(h));
+  DQ_TRY(check_handle_lazy(h));  // the forward dq_run starts from a lazy basis state
   if (!expval || (nparams && !grad)) return fail(DQ_ERR_INVALID_ARG, "null output");
   uint64_t nslots = 0;
   DQ_TRY(check_program(h, prog, ninst, param_index, nparams, &nslots));

@@ -113,9 +113,22 @@ bool put_shell(dq_state_t h) {
   return true;
 }
 
-int check_handle(dq_state_t h) {
+int check_handle_lazy(dq_state_t h) {
   if (!h || !h->amp) return fail(DQ_ERR_INVALID_ARG, "null or destroyed state handle");
   return DQ_OK;
+}
+
+int materialize_basis(dq_state_t h) {
+  if (h->lazy_basis < 0) return DQ_OK;
+  DeviceGuard g(h->device);
+  DQ_TRY(launch_set_basis(h->amp, h->n, (uint64_t)h->lazy_basis, h->stream, h->device));
+  h->lazy_basis = -1;
+  return DQ_OK;
+}
+
+int check_handle(dq_state_t h) {
+  DQ_TRY(check_handle_lazy(h));
+  return materialize_basis(h);
 }
 
 int sync_stream(dq_state_t h) {
@@ -130,6 +143,7 @@ void reset_perm(dq_state_t h) {
 
 // Make the physical layout canonical (perm = identity).
 int canonicalize(dq_state_t h) {
+  DQ_TRY(materialize_basis(h));
   if (!h->permuted) return DQ_OK;
   DQ_TRY(materialize_perm(h->amp, h->n, h->perm, h->stream, nullptr));
   h->permuted = false;
@@ -404,12 +418,7 @@ int dq_state_create(uint32_t n, int device, dq_state_t* out) {
     }
     sh->amp = (double2*)p;
     reset_perm(sh);
-    int rc2 = launch_set_basis(sh->amp, n, 0, sh->stream, device);
-    if (rc2 == DQ_OK) rc2 = sync_stream(sh);
-    if (rc2 != DQ_OK) {
-      dq_state_destroy(sh);
-      return rc2;
-    }
+    sh->lazy_basis = 0;  // |0...0>, written by the first sweep or on first use
     *out = sh;
     return DQ_OK;
   }
@@ -450,12 +459,12 @@ int dq_state_create(uint32_t n, int device, dq_state_t* out) {
   if (e != cudaSuccess) return cleanup(DQ_ERR_CUDA, "cudaMemset(counters)", e);
   e = cudaMallocHost((void**)&h->sc.h_pinned, sizeof(double) * 64);
   if (e != cudaSuccess) return cleanup(DQ_ERR_OOM, "cudaMallocHost", e);
-  rc = launch_set_basis(h->amp, n, 0, h->stream, device);
-  if (rc == DQ_OK) rc = sync_stream(h);
+  rc = sync_stream(h);
   if (rc != DQ_OK) {
     dq_state_destroy(h);
     return rc;
   }
+  h->lazy_basis = 0;  // |0...0>, written by the first sweep or on first use
   *out = h;
   return DQ_OK;
 }
@@ -486,18 +495,18 @@ int dq_state_num_qubits(dq_state_t h, uint32_t* n) {
 }
 
 int dq_state_set_basis(dq_state_t h, uint64_t index) {
-  DQ_TRY(check_handle(h));
+  DQ_TRY(check_handle_lazy(h));
   if (index >= h->len) return fail(DQ_ERR_INVALID_ARG, "basis index out of range");
-  DeviceGuard g(h->device);
-  DQ_TRY(launch_set_basis(h->amp, h->n, index, h->stream, h->device));
   reset_perm(h);
-  return sync_stream(h);
+  h->lazy_basis = (int64_t)index;
+  return DQ_OK;
 }
 
 int dq_state_reset(dq_state_t h) { return dq_state_set_basis(h, 0); }
 
 int dq_state_upload(dq_state_t h, const double* amps, uint64_t len) {
-  DQ_TRY(check_handle(h));
+  DQ_TRY(check_handle_lazy(h));
+  h->lazy_basis = -1;
   if (!amps || len != h->len) return fail(DQ_ERR_INVALID_ARG, "upload length must be 2^n amplitudes");
   DeviceGuard g(h->device);
   DQ_CUDA_TRY(cudaMemcpyAsync(h->amp, amps, h->bytes, cudaMemcpyHostToDevice, h->stream));
@@ -515,8 +524,9 @@ int dq_state_download(dq_state_t h, double* amps, uint64_t len) {
 }
 
 int dq_state_copy(dq_state_t dst, dq_state_t src) {
-  DQ_TRY(check_handle(dst));
+  DQ_TRY(check_handle_lazy(dst));
   DQ_TRY(check_handle(src));
+  dst->lazy_basis = -1;
   if (dst->n != src->n) return fail(DQ_ERR_INVALID_ARG, "state sizes differ");
   DeviceGuard g(dst->device);
   {
@@ -679,7 +689,7 @@ int dq_measure(dq_state_t h, uint32_t qubit, double r, int* outcome, double* p1_
 int dq_run(dq_state_t h, const dq_inst* prog, uint64_t ninst, const dq_cond* conds,
            uint64_t nconds, uint64_t seed, int32_t* cbits, uint64_t ncbits,
            const dq_run_opts* opts, dq_profile* prof) {
-  DQ_TRY(check_handle(h));
+  DQ_TRY(check_handle_lazy(h));
   if (ninst && !prog) return fail(DQ_ERR_INVALID_ARG, "null program");
   if (ncbits && !cbits) return fail(DQ_ERR_INVALID_ARG, "null cbits");
   dq_run_opts o{};
@@ -706,8 +716,15 @@ int dq_run(dq_state_t h, const dq_inst* prog, uint64_t ninst, const dq_cond* con
   const bool fused = o.exec == DQ_EXEC_FUSED && !o.profile && h->n >= kFusedMinQubits;
   if (fused) {
     FusedHooks hooks;
-    hooks.measure = [&c](uint32_t q, int* out) { return do_measure(c, q, out); };
-    hooks.exact_gate = [&c](const GateOp& op) { return do_gate_op(c, op, 0); };
+    hooks.measure = [&c, h](uint32_t q, int* out) {
+      DQ_TRY(materialize_basis(h));
+      return do_measure(c, q, out);
+    };
+    hooks.exact_gate = [&c, h](const GateOp& op) {
+      DQ_TRY(materialize_basis(h));
+      return do_gate_op(c, op, 0);
+    };
+    hooks.lazy_basis = &h->lazy_basis;
     hooks.cbits = cbits;
     hooks.ncbits = ncbits;
     hooks.conds = conds;

@@ -312,7 +312,7 @@ __device__ __forceinline__ void exec_op(const uint4 o0, const uint4 o1, double2 
 template <int TB, int RB, int S>
 __global__ void __launch_bounds__(1 << TB, (S == 1 && TB == 7 ? 3 : (TB + RB <= 11 ? 2 : 1)))
     k_sweep(double2* __restrict__ state, const uint8_t* __restrict__ gprog, uint32_t prog_bytes,
-            uint32_t ntiles) {
+            uint32_t ntiles, long long synth) {
   constexpr int kSwThreads = 1 << TB;
   constexpr int kSwTB = TB;
   constexpr int M = kSwTB + RB;
@@ -346,14 +346,20 @@ __global__ void __launch_bounds__(1 << TB, (S == 1 && TB == 7 ? 3 : (TB + RB <= 
   };
   // run r = warp + 8 i: all of a tile's 2^(m-5) runs of 32 amplitudes; one
   // commit group per call (empty past the last tile, so the group count is
-  // uniform)
+  // uniform).  synth >= 0: the state is the basis vector |synth> not yet
+  // written to memory, so the tile is generated instead of read.
   auto load_tile = [&](uint32_t t, double2* dst) {
     if (t < ntiles) {
       const uint64_t b = tile_base(t);
 #pragma unroll
       for (int i = 0; i < NI; ++i) {
         const uint32_t r = warp + (uint32_t)i * NW;
-        cp_async16(&dst[H->runswz[r] ^ swl ^ H->tile_xload], state + (b + H->runoff[r] + lane));
+        const uint64_t g = b + H->runoff[r] + lane;
+        double2* d = &dst[H->runswz[r] ^ swl ^ H->tile_xload];
+        if (synth >= 0)
+          *d = make_double2(g == (uint64_t)synth ? 1.0 : 0.0, 0.0);
+        else
+          cp_async16(d, state + g);
       }
     }
     cp_async_commit();
@@ -1277,7 +1283,7 @@ bool convert_inst(const dq_inst& in, const uint32_t* perm, std::vector<PGate>& o
 
 template <int TB, int RB, int S>
 int launch_sweep_s(double2* amp, uint32_t n, const uint8_t* dblob, uint32_t prog_bytes,
-                   cudaStream_t st) {
+                   cudaStream_t st, long long synth) {
   constexpr int M = TB + RB;
   const size_t smem_max = sizeof(double2) * (S * (1u << M) + kMaxSlots) + max_prog(M);
   const size_t smem = sizeof(double2) * (S * (1u << M) + kMaxSlots) + prog_bytes;
@@ -1304,14 +1310,14 @@ int launch_sweep_s(double2* amp, uint32_t n, const uint8_t* dblob, uint32_t prog
   DQ_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
   const uint64_t tiles = 1ULL << (n - M);
   const unsigned grid = (unsigned)std::min<uint64_t>(tiles, (uint64_t)sms * resident);
-  k_sweep<TB, RB, S><<<grid, 1 << TB, smem, st>>>(amp, dblob, prog_bytes, (uint32_t)tiles);
+  k_sweep<TB, RB, S><<<grid, 1 << TB, smem, st>>>(amp, dblob, prog_bytes, (uint32_t)tiles, synth);
   DQ_CUDA_TRY(cudaGetLastError());
   return DQ_OK;
 }
 
 template <int TB, int RB>
 int launch_sweep_rb(double2* amp, uint32_t n, const uint8_t* dblob, uint32_t prog_bytes,
-                    cudaStream_t st) {
+                    cudaStream_t st, long long synth) {
   // default: single-buffered tiles, three 128-thread CTAs per SM (measured
   // faster than two double-buffered CTAs: the extra warps hide more of the
   // per-op latency than the prefetch saves); DQSIM_SWEEP_STAGES=2 selects
@@ -1320,24 +1326,24 @@ int launch_sweep_rb(double2* amp, uint32_t n, const uint8_t* dblob, uint32_t pro
     const char* e = getenv("DQSIM_SWEEP_STAGES");
     return (e && atoi(e) == 2) ? 2 : 1;
   }();
-  if (TB == 7 && stages == 1) return launch_sweep_s<7, RB, 1>(amp, n, dblob, prog_bytes, st);
-  return launch_sweep_s<TB, RB, 2>(amp, n, dblob, prog_bytes, st);
+  if (TB == 7 && stages == 1) return launch_sweep_s<7, RB, 1>(amp, n, dblob, prog_bytes, st, synth);
+  return launch_sweep_s<TB, RB, 2>(amp, n, dblob, prog_bytes, st, synth);
 }
 
 int launch_sweep(double2* amp, uint32_t n, uint32_t TB, uint32_t RB, const uint8_t* dblob,
-                 uint32_t prog_bytes, cudaStream_t st) {
+                 uint32_t prog_bytes, cudaStream_t st, long long synth) {
   if (TB == 8) {
     switch (RB) {
-      case 2: return launch_sweep_rb<8, 2>(amp, n, dblob, prog_bytes, st);
-      case 3: return launch_sweep_rb<8, 3>(amp, n, dblob, prog_bytes, st);
-      case 4: return launch_sweep_rb<8, 4>(amp, n, dblob, prog_bytes, st);
+      case 2: return launch_sweep_rb<8, 2>(amp, n, dblob, prog_bytes, st, synth);
+      case 3: return launch_sweep_rb<8, 3>(amp, n, dblob, prog_bytes, st, synth);
+      case 4: return launch_sweep_rb<8, 4>(amp, n, dblob, prog_bytes, st, synth);
       default: break;
     }
   } else if (TB == 7) {
     switch (RB) {
-      case 2: return launch_sweep_rb<7, 2>(amp, n, dblob, prog_bytes, st);
-      case 3: return launch_sweep_rb<7, 3>(amp, n, dblob, prog_bytes, st);
-      case 4: return launch_sweep_rb<7, 4>(amp, n, dblob, prog_bytes, st);
+      case 2: return launch_sweep_rb<7, 2>(amp, n, dblob, prog_bytes, st, synth);
+      case 3: return launch_sweep_rb<7, 3>(amp, n, dblob, prog_bytes, st, synth);
+      case 4: return launch_sweep_rb<7, 4>(amp, n, dblob, prog_bytes, st, synth);
       default: break;
     }
   }
@@ -1453,7 +1459,8 @@ int materialize_perm(double2* amp, uint32_t n, uint32_t* perm, cudaStream_t st, 
 // ---- program runner ------------------------------------------------------------------------
 
 int fused_run_segment(double2* amp, uint32_t n, std::vector<PGate>& G, Planner& pl, Poly& poly,
-                      FusedWork& fw, cudaStream_t st, bool timing, dq_profile* prof) {
+                      FusedWork& fw, cudaStream_t st, bool timing, dq_profile* prof,
+                      int64_t* lazy_basis) {
   std::vector<PSweep> sweeps;
   pl.plan(G, poly, sweeps);
   pl.final_flush(poly, sweeps);
@@ -1484,7 +1491,10 @@ int fused_run_segment(double2* amp, uint32_t n, std::vector<PGate>& G, Planner& 
       cudaEventRecord(e0, st);
     }
     const SwHeader* hh = reinterpret_cast<const SwHeader*>(blob.buf.data() + offs[i]);
-    DQ_TRY(launch_sweep(amp, n, pl.TB, pl.RB, fw.d_blob + offs[i], hh->prog_bytes, st));
+    // a pending basis state is consumed by the first sweep (it writes every amplitude)
+    const long long synth = (lazy_basis && *lazy_basis >= 0) ? (long long)*lazy_basis : -1;
+    DQ_TRY(launch_sweep(amp, n, pl.TB, pl.RB, fw.d_blob + offs[i], hh->prog_bytes, st, synth));
+    if (lazy_basis) *lazy_basis = -1;
     if (timing) {
       cudaEventRecord(e1, st);
       fw.events.push_back(e0);
@@ -1534,7 +1544,7 @@ int fused_run(double2* amp, uint32_t n, const dq_inst* prog, uint64_t ninst, con
   std::vector<PGate> G;
   auto flush_segment = [&]() -> int {
     if (G.empty() && poly.empty()) return DQ_OK;
-    int rc = fused_run_segment(amp, n, G, pl, poly, fw, st, timing, prof);
+    int rc = fused_run_segment(amp, n, G, pl, poly, fw, st, timing, prof, hooks.lazy_basis);
     G.clear();
     return rc;
   };

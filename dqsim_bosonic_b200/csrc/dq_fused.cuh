@@ -45,6 +45,9 @@ struct FusedHooks {
   int32_t* cbits = nullptr;
   uint64_t ncbits = 0;
   const dq_cond* conds = nullptr;
+  // the state's pending basis index (>= 0: memory not yet written): the first
+  // sweep synthesises its tiles from it and clears it
+  int64_t* lazy_basis = nullptr;
 };
 
 // perm[l] = physical position of logical qubit l; updated in place (swap

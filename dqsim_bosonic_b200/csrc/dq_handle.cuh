@@ -23,6 +23,11 @@ struct dq_state_s {
   // relabel swap gates instead of moving data)
   uint32_t perm[64];
   bool permuted = false;
+  // >= 0: the state is the physical basis vector |lazy_basis> but memory has
+  // not been written yet; the next fused sweep synthesises its input tiles
+  // from it (no read of the state, no reset pass), anything else writes it
+  // first (materialize_basis)
+  int64_t lazy_basis = -1;
 };
 
 namespace dq {
@@ -46,7 +51,9 @@ struct DeviceGuard {
 int cache_alloc(int device, size_t bytes, void** out);
 void cache_free(int device, size_t bytes, void* p);
 
-int check_handle(dq_state_t h);
+int check_handle(dq_state_t h);            // validates and materialises a lazy basis state
+int check_handle_lazy(dq_state_t h);       // validates only
+int materialize_basis(dq_state_t h);
 int sync_stream(dq_state_t h);
 // Make the physical layout canonical (undo a pending qubit relabeling).
 int canonicalize(dq_state_t h);
