@@ -176,37 +176,46 @@ def _decode_registers(v: Any, where: str) -> dict[str, Register]:
     return {k: _decode_register(r, f"{where}[{k!r}]") for k, r in v.items()}
 
 
-def decode_instruction(v: Any, where: str = "instruction") -> Instruction:
+def _where(where, name: str | None = None) -> str:
+    w = where() if callable(where) else where
+    return w if name is None else f"{w}.{name}"
+
+
+def decode_instruction(v: Any, where: Any = "instruction") -> Instruction:
+    """``where``: the instruction's path for error messages (a string, or a
+    callable producing it: formatted only when an error is raised)."""
     if not isinstance(v, dict):
-        raise CircuitDecodeError(f"invalid type for {where}: expected internally tagged enum")
+        raise CircuitDecodeError(f"invalid type for {_where(where)}: expected internally tagged enum")
     if "kind" not in v:
-        raise CircuitDecodeError(f"missing field `kind` in {where}")
+        raise CircuitDecodeError(f"missing field `kind` in {_where(where)}")
     kind = v["kind"]
     if not isinstance(kind, str) or kind not in _FIELDS:
-        raise CircuitDecodeError(f"unknown variant `{kind}` in {where}")
+        raise CircuitDecodeError(f"unknown variant `{kind}` in {_where(where)}")
     out: dict[str, Any] = {}
     cond = None
     op = None
     for name, typ in _FIELDS[kind]:
         if name not in v:
-            raise CircuitDecodeError(f"missing field `{name}` in {where} ({kind})")
+            raise CircuitDecodeError(f"missing field `{name}` in {_where(where)} ({kind})")
         val = v[name]
-        w = f"{where}.{name}"
+        tv = type(val)
         if typ == "u":
-            out[name] = _usize(val, w)
+            # fast path: a plain int in range (bool is not int here: type() is exact)
+            out[name] = val if tv is int and 0 <= val <= _U64_MAX else _usize(val, _where(where, name))
         elif typ == "f":
-            out[name] = _f64(val, w)
+            out[name] = val if tv is float and math.isfinite(val) else _f64(val, _where(where, name))
         elif typ == "s":
-            out[name] = _string(val, w)
+            out[name] = val if tv is str else _string(val, _where(where, name))
         elif typ == "fl":
             if not isinstance(val, list):
-                raise CircuitDecodeError(f"invalid type for {w}: expected a sequence")
-            out[name] = [_f64(x, w) for x in val]
+                raise CircuitDecodeError(f"invalid type for {_where(where, name)}: expected a sequence")
+            out[name] = [_f64(x, _where(where, name)) for x in val]
         elif typ == "ul":
             if not isinstance(val, list):
-                raise CircuitDecodeError(f"invalid type for {w}: expected a sequence")
-            out[name] = [_usize(x, w) for x in val]
+                raise CircuitDecodeError(f"invalid type for {_where(where, name)}: expected a sequence")
+            out[name] = [_usize(x, _where(where, name)) for x in val]
         elif typ == "cond":
+            w = _where(where, name)
             if not isinstance(val, dict):
                 raise CircuitDecodeError(f"invalid type for {w}: expected struct Condition")
             for f in ("creg_base", "creg_size", "creg_value"):
@@ -215,7 +224,7 @@ def decode_instruction(v: Any, where: str = "instruction") -> Instruction:
             cond = (_usize(val["creg_base"], w), _usize(val["creg_size"], w),
                     _usize(val["creg_value"], w))
         elif typ == "inst":
-            op = decode_instruction(val, w)
+            op = decode_instruction(val, _where(where, name))
     return Instruction(kind, out, cond, op)
 
 
@@ -231,7 +240,8 @@ def decode_circuit_obj(obj: Any) -> Circuit:
     insts = obj["instructions"]
     if not isinstance(insts, list):
         raise CircuitDecodeError("invalid type for instructions: expected a sequence")
-    return Circuit(qregs, cregs, [decode_instruction(x, f"instructions[{i}]") for i, x in enumerate(insts)])
+    return Circuit(qregs, cregs, [decode_instruction(x, lambda i=i: f"instructions[{i}]")
+                                  for i, x in enumerate(insts)])
 
 
 def _reject_constant(c: str):
@@ -268,15 +278,28 @@ class Program:
         return int(self.insts.shape[0])
 
 
-def _encode_one(inst: Instruction, rec, conds: list[tuple[int, int, int]], names: dict, idx: int,
-                chain: list[tuple[int, int, int]]) -> int:
-    """Fill rec from inst; returns the highest cbit index referenced (or -1)."""
+_NEG8 = (-1,) * MAX_INST_QUBITS
+_ZERO4 = (0.0, 0.0, 0.0, 0.0)
+_TWO_QUBIT_GENERIC = {KIND["g_phi_plus"], KIND["g_psi_minus"], KIND["g_psi_plus"], KIND["g_cz"],
+                      KIND["g_cx"]}
+# per kind: (dq kind, qubit field names, parameter field names)
+_SPEC = {
+    k: (KIND[k] if k in KIND else -1, tuple(n for n, t in v if t == "u" and n != "cbit"),
+        tuple(n for n, t in v if t == "f"))
+    for k, v in _FIELDS.items()
+}
+
+
+def _encode_one(inst: Instruction, conds: list[tuple[int, int, int]], names: dict, idx: int,
+                chain: list[tuple[int, int, int]]) -> tuple[tuple, int]:
+    """(dq_inst record as a tuple, highest cbit index referenced or -1)."""
     if inst.kind == "conditional":
-        return _encode_one(inst.op, rec, conds, names, idx, chain + [inst.condition])
+        return _encode_one(inst.op, conds, names, idx, chain + [inst.condition])
     max_cbit = -1
     f = inst.fields
-    rec["cbit"] = 0
-    rec["q"][:] = -1
+    cbit = 0
+    q = _NEG8
+    p = _ZERO4
     if inst.kind == "gate":
         lname = f["name"].lower()
         if lname in _GENERIC:
@@ -287,60 +310,60 @@ def _encode_one(inst: Instruction, rec, conds: list[tuple[int, int, int]], names
             kind = KIND["g_unsupported"]
         names[idx] = lname
         qs = f["qubits"]
-        rec["kind"] = kind
-        rec["nq"] = min(len(qs), MAX_INST_QUBITS)
-        if kind in (KIND["g_phi_plus"], KIND["g_psi_minus"], KIND["g_psi_plus"], KIND["g_cz"],
-                    KIND["g_cx"]):
+        nq = min(len(qs), MAX_INST_QUBITS)
+        if kind in _TWO_QUBIT_GENERIC:
             if len(qs) != 2:
                 raise ValueError(f"generic gate {f['name']!r} expects 2 qubits, got {len(qs)}")
-            rec["nq"] = 2
-        for i, qv in enumerate(qs[:MAX_INST_QUBITS]):
-            rec["q"][i] = qv if qv < (1 << 31) else -1
+            nq = 2
+        ql = [qv if qv < (1 << 31) else -1 for qv in qs[:MAX_INST_QUBITS]]
+        q = tuple(ql) + _NEG8[len(ql):]
     elif inst.kind in ("barrier", "classical"):
-        rec["kind"] = KIND[inst.kind]
-        rec["nq"] = 0
+        kind = KIND[inst.kind]
+        nq = 0
     else:
-        rec["kind"] = KIND[inst.kind]
-        spec = _FIELDS[inst.kind]
-        qn = [n for n, t in spec if t == "u" and n != "cbit"]
-        pn = [n for n, t in spec if t == "f"]
-        rec["nq"] = len(qn)
-        for i, n in enumerate(qn):
+        kind, qn, pn = _SPEC[inst.kind]
+        nq = len(qn)
+        ql = []
+        for n in qn:
             v = f[n]
             if v >= (1 << 31):
                 raise ValueError(f"qubit index {v} out of range")
-            rec["q"][i] = v
-        for i, n in enumerate(pn):
-            rec["p"][i] = f[n]
+            ql.append(v)
+        q = tuple(ql) + _NEG8[nq:]
+        if pn:
+            pl = [f[n] for n in pn]
+            p = tuple(pl) + _ZERO4[len(pl):]
         if inst.kind == "measure":
-            rec["cbit"] = f["cbit"]
-            max_cbit = f["cbit"]
+            cbit = f["cbit"]
+            max_cbit = cbit
+    cond_first = cond_count = 0
     if chain:
-        rec["cond_first"] = len(conds)
-        rec["cond_count"] = len(chain)
+        cond_first = len(conds)
+        cond_count = len(chain)
         for c in chain:
             if c[1] > 64:
                 raise ValueError("conditions wider than 64 classical bits are not supported")
             conds.append(c)
             if c[1] > 0:
                 max_cbit = max(max_cbit, c[0] + c[1] - 1)
-    else:
-        rec["cond_first"] = 0
-        rec["cond_count"] = 0
-    return max_cbit
+    return (kind, nq, q, cbit, p, cond_first, cond_count), max_cbit
 
 
 def encode(circuit: Circuit) -> Program:
     n = circuit.num_qubits()
-    insts = np.zeros(len(circuit.instructions), dtype=INST_DTYPE)
     conds: list[tuple[int, int, int]] = []
     names: dict[int, str] = {}
     max_cbit = -1
+    rows = []
     for i, inst in enumerate(circuit.instructions):
-        max_cbit = max(max_cbit, _encode_one(inst, insts[i], conds, names, i, []))
+        row, mc = _encode_one(inst, conds, names, i, [])
+        rows.append(row)
+        if mc > max_cbit:
+            max_cbit = mc
+    insts = np.array(rows, dtype=INST_DTYPE) if rows else np.zeros(0, dtype=INST_DTYPE)
     carr = np.zeros(len(conds), dtype=COND_DTYPE)
-    for i, (b, s, v) in enumerate(conds):
-        carr[i] = (b, s, v)
+    for i, (b, s_, v) in enumerate(conds):
+        carr[i] = (b, s_, v)
     ncb = circuit.num_cbits()
     space = max(ncb, max_cbit + 1, 1)
     if space > (1 << 26):
