@@ -209,7 +209,7 @@ __global__ void __launch_bounds__(THREADS) k_traj(const TrajParams P) {
         case T_XPERM: {
           const uint32_t t = op.t1;
           const uint64_t hi_ctrl = op.ctrl & ~lmask;
-          const uint64_t lo_ctrl = op.ctrl & lmask;
+          const uint32_t lo_ctrl = (uint32_t)(op.ctrl & lmask);
           // local zero-insertion positions: target (if local) and local controls
           uint32_t pos[9];
           int np = 0;
@@ -220,46 +220,60 @@ __global__ void __launch_bounds__(THREADS) k_traj(const TrajParams P) {
             m &= m - 1;
           }
           const uint32_t count = L >> np;
+          const uint32_t p0 = np > 0 ? pos[0] : 0u, p1 = np > 1 ? pos[1] : 0u;
+          // pair k -> swizzled index of its element with the target bit 0
+          auto index = [&](uint32_t k) -> uint32_t {
+            uint32_t o;
+            if (np == 1) {
+              o = ins0(k, p0);
+            } else if (np == 2) {
+              o = ins0(ins0(k, p0), p1);
+            } else {
+              o = k;
+              for (int p = 0; p < np; ++p) o = ins0(o, pos[p]);
+            }
+            return tswz(o | lo_ctrl);
+          };
+          double2 *A, *B;
+          uint32_t sx, lo, hi;
           if (t < lb) {
             if ((gbase & hi_ctrl) != hi_ctrl) break;
-            const uint32_t tb = 1u << t;
-            for (uint32_t k = tid; k < count; k += THREADS) {
-              uint32_t o = k;
-              for (int p = 0; p < np; ++p) o = ins0(o, pos[p]);
-              o |= (uint32_t)lo_ctrl;
-              double2* pa = sm + tswz(o);
-              double2* pb = sm + tswz(o | tb);
-              const double2 a = *pa, b = *pb;
-              if (op.type == T_ONEQ) {
-                *pa = cadd_x(cmul_x(u[0], a), cmul_x(u[1], b));
-                *pb = cadd_x(cmul_x(u[2], a), cmul_x(u[3], b));
-              } else {
-                *pa = b;
-                *pb = a;
-              }
-            }
+            A = B = sm;
+            sx = tswz(1u << t);  // tswz is linear over XOR: partner = index ^ tswz(target bit)
+            lo = 0;
+            hi = count;
           } else {
             const uint32_t tbr = 1u << (t - lb);
             const uint32_t r0 = rank & ~tbr, r1 = rank | tbr;
             if ((((uint64_t)r0 << lb) & hi_ctrl) != hi_ctrl) break;
-            double2* b0 = (r0 == rank) ? sm : cl.map_shared_rank(sm, r0);
-            double2* b1 = (r1 == rank) ? sm : cl.map_shared_rank(sm, r1);
+            A = (r0 == rank) ? sm : cl.map_shared_rank(sm, r0);
+            B = (r1 == rank) ? sm : cl.map_shared_rank(sm, r1);
+            sx = 0;
             const uint32_t half = count > 1 ? count >> 1 : 1;
-            uint32_t lo, hi;
             if (rank == r0) { lo = 0; hi = half; } else { lo = half; hi = count > 1 ? count : half; }
-            for (uint32_t k = lo + tid; k < hi; k += THREADS) {
-              uint32_t o = k;
-              for (int p = 0; p < np; ++p) o = ins0(o, pos[p]);
-              o |= (uint32_t)lo_ctrl;
-              double2* pa = b0 + tswz(o);
-              double2* pb = b1 + tswz(o);
-              const double2 a = *pa, b = *pb;
+          }
+          // four pairs per thread in flight: loads first, then the exact
+          // per-pair arithmetic (pairs are disjoint, so the order of the
+          // stores does not matter)
+          for (uint32_t k0 = lo + tid; k0 < hi; k0 += 4u * THREADS) {
+            uint32_t so[4];
+            double2 a[4], b[4];
+#pragma unroll
+            for (int v = 0; v < 4; ++v) {
+              const uint32_t k = k0 + (uint32_t)v * THREADS;
+              so[v] = index(k < hi ? k : k0);
+              a[v] = A[so[v]];
+              b[v] = B[so[v] ^ sx];
+            }
+#pragma unroll
+            for (int v = 0; v < 4; ++v) {
+              if (k0 + (uint32_t)v * THREADS >= hi) break;
               if (op.type == T_ONEQ) {
-                *pa = cadd_x(cmul_x(u[0], a), cmul_x(u[1], b));
-                *pb = cadd_x(cmul_x(u[2], a), cmul_x(u[3], b));
+                A[so[v]] = cadd_x(cmul_x(u[0], a[v]), cmul_x(u[1], b[v]));
+                B[so[v] ^ sx] = cadd_x(cmul_x(u[2], a[v]), cmul_x(u[3], b[v]));
               } else {
-                *pa = b;
-                *pb = a;
+                A[so[v]] = b[v];
+                B[so[v] ^ sx] = a[v];
               }
             }
           }
@@ -279,11 +293,30 @@ __global__ void __launch_bounds__(THREADS) k_traj(const TrajParams P) {
             m &= m - 1;
           }
           const uint32_t count = L >> np;
-          for (uint32_t k = tid; k < count; k += THREADS) {
-            uint32_t o = k;
-            for (int p = 0; p < np; ++p) o = ins0(o, pos[p]);
-            o |= (uint32_t)lo;
-            sm[tswz(o)] = cmul_x(e, sm[tswz(o)]);
+          const uint32_t p0 = np > 0 ? pos[0] : 0u, p1 = np > 1 ? pos[1] : 0u;
+          for (uint32_t k0 = tid; k0 < count; k0 += 4u * THREADS) {
+            uint32_t so[4];
+            double2 a[4];
+#pragma unroll
+            for (int v = 0; v < 4; ++v) {
+              const uint32_t k = k0 + (uint32_t)v * THREADS < count ? k0 + (uint32_t)v * THREADS : k0;
+              uint32_t o;
+              if (np == 1) {
+                o = ins0(k, p0);
+              } else if (np == 2) {
+                o = ins0(ins0(k, p0), p1);
+              } else {
+                o = k;
+                for (int p = 0; p < np; ++p) o = ins0(o, pos[p]);
+              }
+              so[v] = tswz(o | (uint32_t)lo);
+              a[v] = sm[so[v]];
+            }
+#pragma unroll
+            for (int v = 0; v < 4; ++v) {
+              if (k0 + (uint32_t)v * THREADS >= count) break;
+              sm[so[v]] = cmul_x(e, a[v]);
+            }
           }
           break;
         }
