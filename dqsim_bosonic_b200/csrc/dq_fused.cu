@@ -344,13 +344,20 @@ __global__ void __launch_bounds__(1 << TB, (S == 1 && TB == 7 ? 3 : (TB + RB <= 
     for (int k = 0; k < M; ++k) b = insert_zero(b, H->local_pos[k]);
     return b;
   };
+  // Tile bases advance by the grid stride without re-depositing: with the
+  // local positions filled with ones a carry runs across them, so
+  // deposit(t + g) = ((deposit(t) | lmask) + deposit(g)) & ~lmask.
+  uint64_t lmask = 0;
+#pragma unroll
+  for (int k = 0; k < M; ++k) lmask |= 1ULL << H->local_pos[k];
+  const uint64_t bstride = tile_base(gridDim.x);
+  auto advance = [&](uint64_t b) { return ((b | lmask) + bstride) & ~lmask; };
   // run r = warp + 8 i: all of a tile's 2^(m-5) runs of 32 amplitudes; one
   // commit group per call (empty past the last tile, so the group count is
   // uniform).  synth >= 0: the state is the basis vector |synth> not yet
   // written to memory, so the tile is generated instead of read.
-  auto load_tile = [&](uint32_t t, double2* dst) {
+  auto load_tile = [&](uint32_t t, uint64_t b, double2* dst) {
     if (t < ntiles) {
-      const uint64_t b = tile_base(t);
 #pragma unroll
       for (int i = 0; i < NI; ++i) {
         const uint32_t r = warp + (uint32_t)i * NW;
@@ -366,22 +373,50 @@ __global__ void __launch_bounds__(1 << TB, (S == 1 && TB == 7 ? 3 : (TB + RB <= 
   };
 
   uint32_t tile = blockIdx.x;
+  uint64_t base = tile_base(tile);  // this iteration's tile
+  uint64_t bpre = base;             // the newest prefetched tile
 #pragma unroll
-  for (int k = 0; k < S - 1; ++k) load_tile(tile + (uint32_t)k * gridDim.x, bufs + k * T);
+  for (int k = 0; k < S - 1; ++k) {
+    load_tile(tile + (uint32_t)k * gridDim.x, bpre, bufs + k * T);
+    bpre = advance(bpre);
+  }
   for (uint32_t it = 0; tile < ntiles; ++it, tile += gridDim.x) {
     double2* cur = bufs + (it % S) * T;
     // tile it + S - 1 goes into the buffer that tile it - 1 used (stored and
     // released by the barrier that ended the previous iteration)
-    load_tile(tile + (uint32_t)(S - 1) * gridDim.x, bufs + ((it + S - 1) % S) * T);
-    const uint64_t base = tile_base(tile);
-    for (uint32_t s = tid; s < nslots; s += kSwThreads) {
-      double2 w = SL[s].w0;
-      const uint32_t c = SL[s].count, st = SL[s].start;
-      for (uint32_t e = 0; e < c; ++e) {
-        const SwSlotEnt& E = SE[st + e];
-        if ((base & E.mask) == E.mask) w = cmul_f(w, E.w);
+    load_tile(tile + (uint32_t)(S - 1) * gridDim.x, bpre, bufs + ((it + S - 1) % S) * T);
+    bpre = advance(bpre);
+    // per-tile phase factors: few slots with many entries take a warp
+    // each (lane products, then a butterfly over the lanes); otherwise one
+    // thread per slot
+    if (nslots <= 4 * NW) {
+      for (uint32_t s = warp; s < nslots; s += NW) {
+        const uint32_t c = SL[s].count, st = SL[s].start;
+        double2 w = make_double2(1.0, 0.0);
+        for (uint32_t e = lane; e < c; e += 32) {
+          const SwSlotEnt& E = SE[st + e];
+          if ((base & E.mask) == E.mask) w = cmul_f(w, E.w);
+        }
+        if (c > 1) {
+#pragma unroll
+          for (int o = 16; o > 0; o >>= 1) {
+            const double2 q = make_double2(__shfl_xor_sync(0xffffffffu, w.x, o),
+                                           __shfl_xor_sync(0xffffffffu, w.y, o));
+            w = cmul_f(w, q);
+          }
+        }
+        if (lane == 0) slots[s] = cmul_f(SL[s].w0, w);
       }
-      slots[s] = w;
+    } else {
+      for (uint32_t s = tid; s < nslots; s += kSwThreads) {
+        double2 w = SL[s].w0;
+        const uint32_t c = SL[s].count, st = SL[s].start;
+        for (uint32_t e = 0; e < c; ++e) {
+          const SwSlotEnt& E = SE[st + e];
+          if ((base & E.mask) == E.mask) w = cmul_f(w, E.w);
+        }
+        slots[s] = w;
+      }
     }
     cp_async_wait<S - 1>();  // this tile's group is complete; S - 1 newer may be pending
     __syncthreads();
@@ -438,6 +473,7 @@ __global__ void __launch_bounds__(1 << TB, (S == 1 && TB == 7 ? 3 : (TB + RB <= 
       const uint32_t r = warp + (uint32_t)i * NW;
       state[base + H->runoff[r] + lane] = cur[H->runswz[r] ^ swl];
     }
+    base = advance(base);
     __syncthreads();
   }
   cp_async_wait<0>();
