@@ -25,8 +25,9 @@ The exchange of global position j with local position a is the one data-path
 collective: partner ranks r and r ^ 2^j swap the part of their shards whose
 local bit a differs from their rank bit j, 2^(n_l - 1) amplitudes on each
 side (blocks of 2^a contiguous amplitudes; the victim is taken from the top
-local positions so the blocks stay large), in place through a chunk buffer.  Measurement sums the ranks' partial p1 with one
-all-reduce and every rank draws the outcome from the same ChaCha8 stream
+local positions so the blocks stay large), in place through a chunk buffer.
+Measurement sums the ranks' partial p1 with one all-reduce and every rank
+draws the outcome from the same ChaCha8 stream
 (``simulate`` semantics: one f64 per measure / reset, in program order), so
 outcomes, classical bits and the collapse match a single-state run except
 where |r - p1| is at rounding level (counted in ``boundary_draws``).
