@@ -649,7 +649,10 @@ struct Blob {
 
 struct Planner {
   uint32_t n = 0, M = 12, RB = 5, TB = 8;
-  double budget = 48.0;
+  // FP64 work per amplitude one sweep may take on: at 30 qubits a sweep's
+  // compute stays cheaper than another pass over the state up to ~100
+  // (brickwork28 of u3 + cx: 255 ms at 48, 227 ms at 96, the same above)
+  double budget = 96.0;
   uint32_t max_ops = 40;    // non-diagonal gates per sweep (bounds the staged program)
   bool single_tile = false;
 
