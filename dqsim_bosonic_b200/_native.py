@@ -190,6 +190,7 @@ SIGNATURES = [
                                   _P, _P]),
     ("dq_debug_plan", ctypes.c_int, [_U32, _P, _U64, ctypes.POINTER(RunOpts), _P, _U64,
                                      ctypes.POINTER(_U64)]),
+    ("dq_block_merge", ctypes.c_int, [_P, _P, _U32, _P, _P, _U32, _P]),
     ("dq_rng_f64", ctypes.c_int, [_U64, _U64, _U64, _P]),
     ("dq_rng_seed_key", ctypes.c_int, [_U64, _P]),
     ("dq_chacha_block", ctypes.c_int, [_P, _U32, _P]),

@@ -57,6 +57,8 @@ int materialize_basis(dq_state_t h);
 int sync_stream(dq_state_t h);
 // Make the physical layout canonical (undo a pending qubit relabeling).
 int canonicalize(dq_state_t h);
+// Mark the layout canonical without moving data (the state is rewritten).
+void reset_perm(dq_state_t h);
 // Copy `count` device doubles to `out` through the handle's pinned buffer.
 int read_scalars(dq_state_t h, const double* d_src, int count, double* out);
 int gate_qubit_count(int kind);

@@ -348,6 +348,17 @@ DQ_API int dq_adjoint(dq_state_t h, const dq_inst* prog, uint64_t ninst,
                       const dq_run_opts* opts, double* expval, double* grad,
                       double* phase_ms);
 
+/* ---- p-block merge -----------------------------------------------------------
+ * merge_blocks (src/distributed/pblock/model.rs:35-57): the tensor product of
+ * block a (state of the ascending qubits a_qubits[0..na)) and block b into
+ * `out`, whose qubits are the ascending union of both lists (a qubit named in
+ * both takes one position).  out must have exactly that many qubits and be a
+ * third state; it is overwritten.  Amplitude i of out is a[la(i)] * b[lb(i)]
+ * with num-complex's multiplication (no FMA): bit-identical to the
+ * reference.  All three states must live on one device. */
+DQ_API int dq_block_merge(dq_state_t a, const uint32_t* a_qubits, uint32_t na, dq_state_t b,
+                          const uint32_t* b_qubits, uint32_t nb, dq_state_t out);
+
 /* ---- planner inspection (host only, no GPU needed) -------------------------
  * Runs the fused-sweep planner of dq_run (DQ_EXEC_FUSED) on a unitary
  * program of n qubits and writes the encoded sweep programs instead of

@@ -19,6 +19,7 @@
  *   src/monolithic/statevector/simulator.rs:386-632  run_instruction
  *   src/monolithic/statevector/simulator.rs:638-884  run_instruction_par / run_fused_par
  *   src/monolithic/statevector/simulator.rs:216-296  simulate_shots seeding
+ *   src/distributed/pblock/model.rs:35-57            merge_blocks (tensor-product merge)
  * and the third-party arithmetic the path depends on (not in the reference
  * tree; versions pinned by its Cargo.lock):
  *   rand_chacha 0.3.1  ChaCha8Rng: 8-round ChaCha block function, 64-bit block
@@ -782,4 +783,40 @@ double or_expval_pauli(const double* st_, uint32_t n, const dq_pauli_term* terms
     total += terms[t].coeff * v;
   }
   return total;
+}
+
+/* merge_blocks (src/distributed/pblock/model.rs:35-57): merged qubits = the
+ * ascending union of qa[0..na) and qb[0..nb) (both ascending); for every
+ * merged index i, a_local gathers the bits of i at the merged positions of
+ * a's qubits, likewise b_local; out[i] = a[a_local] * b[b_local] (num-complex
+ * multiplication).  out has 2^|union| entries; returns |union|. */
+uint32_t or_block_merge(const double* a_, const uint32_t* qa, uint32_t na, const double* b_,
+                        const uint32_t* qb, uint32_t nb, double* out_) {
+  uint32_t u[128];
+  uint32_t n = 0, i = 0, j = 0;
+  while (i < na || j < nb) {
+    if (j >= nb || (i < na && qa[i] < qb[j])) u[n++] = qa[i++];
+    else if (i >= na || qb[j] < qa[i]) u[n++] = qb[j++];
+    else { u[n++] = qa[i++]; ++j; }
+  }
+  const cpx* a = (const cpx*)a_;
+  const cpx* b = (const cpx*)b_;
+  cpx* out = (cpx*)out_;
+  uint32_t pa[64], pb[64];
+  for (uint32_t k = 0; k < na; ++k)
+    for (uint32_t p = 0; p < n; ++p)
+      if (u[p] == qa[k]) pa[k] = p;
+  for (uint32_t k = 0; k < nb; ++k)
+    for (uint32_t p = 0; p < n; ++p)
+      if (u[p] == qb[k]) pb[k] = p;
+  const uint64_t dim = 1ULL << n;
+  for (uint64_t x = 0; x < dim; ++x) {
+    uint64_t la = 0, lb = 0;
+    for (uint32_t k = 0; k < na; ++k)
+      if ((x >> pa[k]) & 1ULL) la |= 1ULL << k;
+    for (uint32_t k = 0; k < nb; ++k)
+      if ((x >> pb[k]) & 1ULL) lb |= 1ULL << k;
+    out[x] = cmul(a[la], b[lb]);
+  }
+  return n;
 }

@@ -49,6 +49,7 @@ def lib():
             "or_run_shots": (ctypes.c_int, [U32, P, U64, P, U64, U64, U64, P, U64, P]),
             "or_fuse_export": (U64, [P, U64, U32, P, P, P]),
             "or_expval_pauli": (ctypes.c_double, [P, U32, P, U64]),
+            "or_block_merge": (U32, [P, P, U32, P, P, U32, P]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -239,3 +240,17 @@ def finite_difference(circuit, theta, terms: np.ndarray, h: float = 1e-6, entrie
         out[k] = (expval_program(circuit.bind(tp), n, terms) -
                   expval_program(circuit.bind(tm), n, terms)) / (2 * h)
     return out
+
+
+def block_merge(a: np.ndarray, qa, b: np.ndarray, qb) -> tuple[np.ndarray, list[int]]:
+    """merge_blocks on the CPU: (merged state, merged qubits)."""
+    qa = np.ascontiguousarray(qa, dtype=np.uint32)
+    qb = np.ascontiguousarray(qb, dtype=np.uint32)
+    u = sorted(set(qa.tolist()) | set(qb.tolist()))
+    out = np.empty(1 << len(u), dtype=np.complex128)
+    a = np.ascontiguousarray(a, dtype=np.complex128)
+    b = np.ascontiguousarray(b, dtype=np.complex128)
+    n = lib().or_block_merge(_p(a), _p(qa) if qa.size else None, qa.size, _p(b),
+                             _p(qb) if qb.size else None, qb.size, _p(out))
+    assert n == len(u)
+    return out, u
