@@ -16,6 +16,7 @@
 // memory: for byte c of i with value v, tab[c][v] = (la part, lb part).
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <string>
 #include <vector>
 
@@ -130,7 +131,10 @@ int dq_block_merge(dq_state_t a, const uint32_t* a_qubits, uint32_t na, dq_state
   cudaError_t e = cudaMemcpyAsync(d_tab, tab.data(), sizeof(ulonglong2) * tab.size(),
                                   cudaMemcpyHostToDevice, out->stream);
   if (e == cudaSuccess) {
-    const unsigned grid = grid_for(out->len, 256, out->device);
+    // persistent CTAs: every CTA stages the gather tables once (up to 20 KB)
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, out->device);
+    const unsigned grid = std::min<unsigned>(grid_for(out->len, 256, out->device), (unsigned)sms * 8u);
     k_block_merge<<<grid, 256, 0, out->stream>>>(out->amp, out->len, a->amp, b->amp, d_tab, nbytes);
     e = cudaGetLastError();
   }
