@@ -418,6 +418,7 @@ def main():
         line["trajectories"] = trajectory_section(dev, cpu=d.rank == 0 and d.world == 1
                                                   and not args.no_cpu_baseline, d=d)
         line["adjoint"] = adjoint_section(dev)
+        line["pblock_merge"] = pblock_merge_section(dev)
         if args.adam_steps > 0:
             line["adjoint_batch"] = adjoint_batch_section(dev, args.adam_steps)
     if args.adjoint31:
@@ -634,6 +635,53 @@ def adjoint_batch_section(dev: int, adam_steps: int, workers: int = 4) -> dict:
         "mean_energy_last": float(e.mean()),
         "workers": workers,
     }
+
+
+def pblock_merge_section(dev: int) -> dict:
+    """The p-block merge of two 15-qubit blocks (even and odd qubits) into a
+    30-qubit block: dq_block_merge timed with CUDA events on the merged
+    state's stream; algorithmic bytes = the merged state written plus both
+    blocks read."""
+    import torch
+
+    from dqsim_bosonic_b200 import _native as nat
+
+    qa = np.arange(0, 30, 2, dtype=np.uint32)
+    qb = np.arange(1, 30, 2, dtype=np.uint32)
+    sa, sb, out = nat.State(15, dev), nat.State(15, dev), nat.State(30, dev)
+    rng = np.random.default_rng(3)
+    for s_ in (sa, sb):
+        v = rng.normal(size=1 << 15) + 1j * rng.normal(size=1 << 15)
+        s_.upload(v / np.linalg.norm(v))
+    _, sptr = out.device_ptr()
+    stream = torch.cuda.ExternalStream(sptr, device=f"cuda:{dev}")
+    L = nat.lib()
+
+    def merge():
+        nat.check(L.dq_block_merge(sa.handle, nat.ptr(qa), 15, sb.handle, nat.ptr(qb), 15, out.handle),
+                  "dq_block_merge")
+
+    for _ in range(3):
+        merge()
+    ms = []
+    for _ in range(5):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        merge()
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        ms.append(e0.elapsed_time(e1))
+    for s_ in (sa, sb, out):
+        s_.release()
+    t = float(np.median(ms))
+    nbytes = 16.0 * (2 ** 30 + 2 * 2 ** 15)
+    peak, src = peak_hbm()
+    achieved = nbytes / (t * 1e-3) / 1e9
+    return {"workload": "merge_blocks: 15 + 15 interleaved qubits -> 30-qubit block",
+            "ms": t, "bytes": nbytes,
+            "roofline": {"kernel": "k_block_merge", "bound": "hbm", "achieved": achieved, "peak": peak,
+                         "unit": "GB/s", "frac": achieved / peak, "peak_source": src}}
 
 
 def adjoint31_section(dev: int, fd_params: int = 32) -> dict:

@@ -55,6 +55,8 @@ constexpr uint32_t kAMaxSlots = 192;
 
 enum AType : uint8_t { A_ONE = 1, A_TWO = 2, A_DIAG = 3, A_DRUN = 4, A_PHASE = 5 };
 constexpr uint32_t kAPhaseOps = 16;  // ops of one register phase
+constexpr uint32_t kAPhaseStage = 32;  // phase ops of a sweep staged once per CTA, at most
+constexpr uint32_t kAMaxSweepOps = 2 * kAMaxOps;  // ops of a sweep, run and phase headers included
 constexpr uint32_t kADiagRun = 64;  // diagonal ops applied in one elementwise pass
 constexpr uint32_t kADiagRunMin = 4;  // shorter runs stay single A_DIAG ops
 
@@ -80,6 +82,9 @@ struct ASweepHdr {
   uint32_t lpos[kAMaxLocal];  // local bit positions, ascending
   uint32_t npos_cnt;
   uint32_t npos[64];          // non-local bit positions, ascending
+  uint32_t phase_ops;         // > 0: every register phase's op data is staged once per CTA
+                              // (phase header lctrl = its first PSub); 0: staged per tile
+  uint32_t pad;
 };
 
 __device__ __forceinline__ double2 cfma2(double2 a, double2 b, double2 acc) {
@@ -545,13 +550,9 @@ __device__ __forceinline__ void phase_one(double2 (&a)[8], double2 (&b)[8], cons
   }
 }
 
-// A register phase: every thread holds the 8 amplitudes of psi and lambda
-// that differ in the phase's three local bits and applies the phase's
-// uncontrolled one-qubit ops (on those bits) in order.  Each op's gradient
-// terms are reduced per warp right after the op (all lanes take part: the
-// group loop runs the same trip count on every thread).
-__device__ __noinline__ void op_phase(double2* sp, double2* sl, const AOp& hdr, const AOp* sub,
-                                      const double2* pool, uint32_t m, double* accw, PSub* ps) {
+// The op data of one register phase: threads < cnt fill ps[0 .. cnt).
+__device__ __forceinline__ void stage_phase(const AOp& hdr, const AOp* sub, const double2* pool,
+                                            PSub* ps) {
   const uint32_t cnt = hdr.cnt;
   const uint32_t pbits[3] = {hdr.lt, hdr.lt2, (uint32_t)hdr.dq[0]};
   if (threadIdx.x < cnt) {
@@ -577,7 +578,23 @@ __device__ __noinline__ void op_phase(double2* sp, double2* sl, const AOp& hdr, 
       P.tm[q] = tm;
     }
   }
-  __syncthreads();
+}
+
+// A register phase: every thread holds the 8 amplitudes of psi and lambda
+// that differ in the phase's three local bits and applies the phase's
+// uncontrolled one-qubit ops (on those bits) in order.  Each op's gradient
+// terms are reduced per warp right after the op (all lanes take part: the
+// group loop runs the same trip count on every thread).  staged: ps already
+// holds the phase's op data (staged once per CTA).
+__device__ __noinline__ void op_phase(double2* sp, double2* sl, const AOp& hdr, const AOp* sub,
+                                      const double2* pool, uint32_t m, double* accw, PSub* ps,
+                                      bool staged) {
+  const uint32_t cnt = hdr.cnt;
+  const uint32_t pbits[3] = {hdr.lt, hdr.lt2, (uint32_t)hdr.dq[0]};
+  if (!staged) {
+    stage_phase(hdr, sub, pool, ps);
+    __syncthreads();
+  }
   const uint32_t groups = (1u << m) >> 3;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   for (uint32_t g0 = 0; g0 < groups; g0 += kAThreads) {
@@ -641,7 +658,20 @@ __global__ void __launch_bounds__(kAThreads, 2)
   double2* sp = reinterpret_cast<double2*>(smraw);
   double2* sl = sp + L;
   double* accw = reinterpret_cast<double*>(sl + L);
+  // the sweep's ops, and (phase_ops > 0) every register phase's op data, in
+  // shared memory for the whole launch
+  AOp* sops = reinterpret_cast<AOp*>(accw + ((H.nslots ? H.nslots : 1u) * kAWarps + 1u) / 2u * 2u);
+  PSub* psall = reinterpret_cast<PSub*>(sops + (H.nops + 1u) / 2u * 2u);
   for (uint32_t i = threadIdx.x; i < H.nslots * kAWarps; i += kAThreads) accw[i] = 0.0;
+  for (uint32_t i = threadIdx.x; i < H.nops; i += kAThreads) sops[i] = ops[i];
+  __syncthreads();
+  if (H.phase_ops) {
+    for (uint32_t i = 0; i < H.nops; ++i) {
+      const AOp op = sops[i];
+      if (op.type == A_PHASE) stage_phase(op, sops + i + 1, pool, psall + op.lctrl);
+      if (op.type == A_PHASE || op.type == A_DRUN) i += op.cnt;
+    }
+  }
   // offset bits above the 5 contiguous ones -> global bits
   // local bits 0 .. lo_bits-1 are qubits 0 .. lo_bits-1: runs of 2^lo_bits
   // consecutive amplitudes (at least 128 B)
@@ -672,15 +702,16 @@ __global__ void __launch_bounds__(kAThreads, 2)
     asm volatile("cp.async.wait_group 0;\n" ::: "memory");
     __syncthreads();
     for (uint32_t i = 0; i < H.nops; ++i) {
-      const AOp op = ops[i];
+      const AOp op = sops[i];
       if (op.type == A_DRUN) {
-        op_drun(sp, sl, op, ops + i + 1, pool, m, base, accw, drec);
+        op_drun(sp, sl, op, sops + i + 1, pool, m, base, accw, drec);
         i += op.cnt;
         __syncthreads();
         continue;
       }
       if (op.type == A_PHASE) {
-        op_phase(sp, sl, op, ops + i + 1, pool, m, accw, psub);
+        op_phase(sp, sl, op, sops + i + 1, pool, m, accw, H.phase_ops ? psall + op.lctrl : psub,
+                 H.phase_ops != 0);
         i += op.cnt;
         __syncthreads();
         continue;
@@ -1093,9 +1124,32 @@ int encode_asweep(const ASweepPlan& sp, uint32_t n, ASweepHdr& hdr, std::vector<
     i = j;
   }
   ops.swap(grouped);
+  // register phases' op data staged once per CTA when it fits
+  uint32_t pops = 0;
+  for (size_t i = 0; i < ops.size(); ++i)
+    if (ops[i].type == A_PHASE) pops += ops[i].cnt;
+  if (pops <= kAPhaseStage) {
+    uint32_t b = 0;
+    for (size_t i = 0; i < ops.size(); ++i)
+      if (ops[i].type == A_PHASE) {
+        ops[i].lctrl = b;
+        b += ops[i].cnt;
+      }
+    hdr.phase_ops = pops;
+  }
   hdr.nops = (uint32_t)ops.size();
   hdr.nslots = slot;
+  if (hdr.nops > kAMaxSweepOps) return fail(DQ_ERR_INTERNAL, "too many ops in an adjoint sweep");
   return DQ_OK;
+}
+
+// Dynamic shared memory of a sweep: psi and lambda tiles, per-warp gradient
+// slots, the op list and the staged phase data (layout as in k_adj_sweep).
+size_t asweep_smem(uint32_t m, uint32_t nslots, uint32_t nops, uint32_t phase_ops) {
+  const size_t slots = ((size_t)(nslots ? nslots : 1) * kAWarps + 1) / 2 * 2;
+  const size_t nops2 = ((size_t)nops + 1) / 2 * 2;
+  return sizeof(double2) * 2 * (1u << m) + sizeof(double) * slots + sizeof(AOp) * nops2 +
+         sizeof(PSub) * phase_ops;
 }
 
 int sweep_ctas(int device) {
@@ -1103,7 +1157,7 @@ int sweep_ctas(int device) {
   static int per_sm[64];
   std::lock_guard<std::mutex> lk(mu);
   if (per_sm[device & 63] == 0) {
-    const size_t smem_max = sizeof(double2) * 2 * (1u << kAMaxLocal) + sizeof(double) * kAMaxSlots * kAWarps;
+    const size_t smem_max = asweep_smem(kAMaxLocal, kAMaxSlots, kAMaxSweepOps, kAPhaseStage);
     DQ_CUDA_TRY(cudaFuncSetAttribute(k_adj_sweep, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)smem_max));
     int b = 1;
@@ -1258,7 +1312,7 @@ int adjoint_backward_fused(double2* psi, double2* lam, uint32_t n, const dq_inst
     }
     const SweepRef& ref = refs[si++];
     const ASweepHdr& hdr = hdrs[ref.hdr];
-    const size_t smem = sizeof(double2) * 2 * (1u << hdr.m) + sizeof(double) * std::max<uint32_t>(hdr.nslots, 1) * kAWarps;
+    const size_t smem = asweep_smem(hdr.m, hdr.nslots, hdr.nops, hdr.phase_ops);
     k_adj_sweep<<<ref.grid, kAThreads, smem, st>>>(psi, lam, d_hdr + ref.hdr, d_ops + ref.op0, d_pool,
                                                     d_part);
     cu(cudaGetLastError(), "k_adj_sweep");
