@@ -415,13 +415,9 @@ __device__ __noinline__ void op_drun(double2* sp, double2* sl, const AOp& hdr, c
         }
         contrib = fma(wh[S].x, pz.x, fma(-wh[S].y, pz.y, contrib));
       }
-      // the warp's terms in op order: deterministic slot sums
-      const uint32_t nk = cnt - c0 < 32u ? cnt - c0 : 32u;
-      for (uint32_t u = 0; u < nk; ++u) {
-        const double t = __shfl_sync(0xffffffffu, contrib, (int)u);
-        const uint32_t s = __shfl_sync(0xffffffffu, slot, (int)u);
-        if (lane == 0 && s != 0xffffffffu) accw[s * kAWarps + w] += t;
-      }
+      // every gate of a sweep has slots of its own, so each lane adds its
+      // op's term to the warp's slot directly (one writer per slot and warp)
+      if (slot != 0xffffffffu) accw[slot * kAWarps + w] += contrib;
     }
   }
   // the run's phase polynomial for this thread's eight elements
