@@ -286,6 +286,8 @@ def main():
                     help="skip the trajectory-batch and adjoint-gradient sections")
     ap.add_argument("--adam-steps", type=int, default=2,
                     help="timed Adam steps of the 512-set batched adjoint (0 = skip)")
+    ap.add_argument("--merge-qubits", type=int, default=30,
+                    help="qubits of the merged block in the p-block merge section (even split)")
     ap.add_argument("--adjoint31", action="store_true",
                     help="add the 31-qubit adjoint pass with its finite-difference check")
     args = ap.parse_args()
@@ -420,7 +422,7 @@ def main():
         line["trajectories"] = trajectory_section(dev, cpu=d.rank == 0 and d.world == 1
                                                   and not args.no_cpu_baseline, d=d)
         line["adjoint"] = adjoint_section(dev)
-        line["pblock_merge"] = pblock_merge_section(dev)
+        line["pblock_merge"] = pblock_merge_section(dev, args.merge_qubits)
         if args.adam_steps > 0:
             line["adjoint_batch"] = adjoint_batch_section(dev, args.adam_steps)
     if args.adjoint31:
@@ -639,28 +641,29 @@ def adjoint_batch_section(dev: int, adam_steps: int, workers: int = 4) -> dict:
     }
 
 
-def pblock_merge_section(dev: int) -> dict:
-    """The p-block merge of two 15-qubit blocks (even and odd qubits) into a
-    30-qubit block: dq_block_merge timed with CUDA events on the merged
-    state's stream; algorithmic bytes = the merged state written plus both
-    blocks read."""
+def pblock_merge_section(dev: int, n: int = 30) -> dict:
+    """The p-block merge of two blocks on the even and the odd qubits into an
+    n-qubit block (n = 30: two 15-qubit blocks): dq_block_merge timed with
+    CUDA events on the merged state's stream; algorithmic bytes = the merged
+    state written plus both blocks read."""
     import torch
 
     from dqsim_bosonic_b200 import _native as nat
 
-    qa = np.arange(0, 30, 2, dtype=np.uint32)
-    qb = np.arange(1, 30, 2, dtype=np.uint32)
-    sa, sb, out = nat.State(15, dev), nat.State(15, dev), nat.State(30, dev)
+    qa = np.arange(0, n, 2, dtype=np.uint32)
+    qb = np.arange(1, n, 2, dtype=np.uint32)
+    na, nb = int(qa.size), int(qb.size)
+    sa, sb, out = nat.State(na, dev), nat.State(nb, dev), nat.State(n, dev)
     rng = np.random.default_rng(3)
-    for s_ in (sa, sb):
-        v = rng.normal(size=1 << 15) + 1j * rng.normal(size=1 << 15)
+    for s_, k in ((sa, na), (sb, nb)):
+        v = rng.normal(size=1 << k) + 1j * rng.normal(size=1 << k)
         s_.upload(v / np.linalg.norm(v))
     _, sptr = out.device_ptr()
     stream = torch.cuda.ExternalStream(sptr, device=f"cuda:{dev}")
     L = nat.lib()
 
     def merge():
-        nat.check(L.dq_block_merge(sa.handle, nat.ptr(qa), 15, sb.handle, nat.ptr(qb), 15, out.handle),
+        nat.check(L.dq_block_merge(sa.handle, nat.ptr(qa), na, sb.handle, nat.ptr(qb), nb, out.handle),
                   "dq_block_merge")
 
     for _ in range(3):
@@ -677,10 +680,10 @@ def pblock_merge_section(dev: int) -> dict:
     for s_ in (sa, sb, out):
         s_.release()
     t = float(np.median(ms))
-    nbytes = 16.0 * (2 ** 30 + 2 * 2 ** 15)
+    nbytes = 16.0 * (2 ** n + 2 ** na + 2 ** nb)
     peak, src = peak_hbm()
     achieved = nbytes / (t * 1e-3) / 1e9
-    return {"workload": "merge_blocks: 15 + 15 interleaved qubits -> 30-qubit block",
+    return {"workload": f"merge_blocks: {na} + {nb} interleaved qubits -> {n}-qubit block",
             "ms": t, "bytes": nbytes,
             "roofline": {"kernel": "k_block_merge", "bound": "hbm", "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": achieved / peak, "peak_source": src}}
