@@ -46,7 +46,8 @@ constexpr uint32_t kTrajMaxQubits = 16;
 constexpr uint32_t kTrajMaxCbits = 1024;
 
 enum TOpType : uint8_t {
-  T_NOP = 0, T_ONEQ, T_PHASE, T_XPERM, T_SWAP, T_DIAG, T_DENSE, T_MEASURE, T_RESET, T_FAIL
+  T_NOP = 0, T_ONEQ, T_PHASE, T_XPERM, T_SWAP, T_DIAG, T_DENSE, T_MEASURE, T_RESET, T_FAIL,
+  T_RPHASE  // header of k (>= 2) T_ONEQ / T_XPERM ops on the four local bits q[0..3]
 };
 
 struct TOp {
@@ -58,7 +59,7 @@ struct TOp {
   uint32_t mat;     // offset into the matrix pool (double2 units)
   uint32_t remote;  // touches cluster qubits or needs a cluster reduction
   uint64_t ctrl;    // control mask (all must be 1)
-  uint8_t q[8];     // DIAG / DENSE qubits, q[0] = MSB of the matrix index
+  uint8_t q[8];     // DIAG / DENSE qubits, q[0] = MSB of the matrix index; RPHASE: register bits
   int64_t inst;     // original instruction index (-1: a fused 2x2)
 };
 static_assert(sizeof(TOp) == 48, "TOp layout");
@@ -101,6 +102,34 @@ __device__ __forceinline__ uint32_t ins0(uint32_t k, uint32_t p) {
 // unchanged.
 __device__ __forceinline__ uint32_t tswz(uint32_t o) {
   return o ^ (((o >> 3) ^ (o >> 6) ^ (o >> 9) ^ (o >> 12)) & 7u);
+}
+
+// One op of a register phase on the 16 amplitudes a thread holds (register
+// index bit b = local qubit q[b] of the phase): the exact per-pair arithmetic
+// of the shared-memory path, for the pairs whose control bits (creg) are set.
+template <int RT>
+__device__ __forceinline__ void rphase_1q(double2 (&a)[16], const double2 (&u)[4], uint32_t creg) {
+#pragma unroll
+  for (int j = 0; j < 16; ++j) {
+    if (j & (1 << RT)) continue;
+    if (((uint32_t)j & creg) != creg) continue;
+    const int k = j | (1 << RT);
+    const double2 x = a[j], y = a[k];
+    a[j] = cadd_x(cmul_x(u[0], x), cmul_x(u[1], y));
+    a[k] = cadd_x(cmul_x(u[2], x), cmul_x(u[3], y));
+  }
+}
+template <int RT>
+__device__ __forceinline__ void rphase_x(double2 (&a)[16], uint32_t creg) {
+#pragma unroll
+  for (int j = 0; j < 16; ++j) {
+    if (j & (1 << RT)) continue;
+    if (((uint32_t)j & creg) != creg) continue;
+    const int k = j | (1 << RT);
+    const double2 x = a[j];
+    a[j] = a[k];
+    a[k] = x;
+  }
 }
 
 // Fixed-order block sum, result broadcast to every thread.
@@ -474,6 +503,62 @@ __global__ void __launch_bounds__(THREADS) k_traj(const TrajParams P) {
           }
           break;
         }
+        case T_RPHASE: {
+          // the next op.k ops act on the four local bits q[0..3] only: each
+          // thread holds the 16 amplitudes of a group in registers and applies
+          // them in program order (one shared-memory pass, one barrier)
+          const uint32_t cnt = op.k;
+          const uint32_t r0 = op.q[0], r1 = op.q[1], r2 = op.q[2], r3 = op.q[3];
+          const uint32_t s0 = tswz(1u << r0), s1 = tswz(1u << r1), s2 = tswz(1u << r2),
+                         s3 = tswz(1u << r3);
+          auto sidx = [&](uint32_t sb, int j) {
+            return sb ^ ((j & 1) ? s0 : 0u) ^ ((j & 2) ? s1 : 0u) ^ ((j & 4) ? s2 : 0u) ^
+                   ((j & 8) ? s3 : 0u);
+          };
+          const uint32_t groups = L >> 4;
+          for (uint32_t gi = tid; gi < groups; gi += THREADS) {
+            // tswz is linear over XOR and the group base has the register bits clear
+            const uint32_t sb = tswz(ins0(ins0(ins0(ins0(gi, r0), r1), r2), r3));
+            double2 a[16];
+#pragma unroll
+            for (int j = 0; j < 16; ++j) a[j] = sm[sidx(sb, j)];
+            for (uint32_t sidx_op = 0; sidx_op < cnt; ++sidx_op) {
+              const TOp so = P.ops[pg.ops_off + oi + 1 + sidx_op];
+              const uint32_t t = so.t1;
+              const uint32_t rt = t == r0 ? 0u : (t == r1 ? 1u : (t == r2 ? 2u : 3u));
+              uint32_t creg = 0;
+              if (so.ctrl) {
+                if ((so.ctrl >> r0) & 1ULL) creg |= 1u;
+                if ((so.ctrl >> r1) & 1ULL) creg |= 2u;
+                if ((so.ctrl >> r2) & 1ULL) creg |= 4u;
+                if ((so.ctrl >> r3) & 1ULL) creg |= 8u;
+              }
+              if (so.type == T_ONEQ) {
+                double2 uu[4];
+                for (int i = 0; i < 4; ++i) uu[i] = P.pool[so.mat + i];
+                switch (rt) {
+                  case 0: rphase_1q<0>(a, uu, creg); break;
+                  case 1: rphase_1q<1>(a, uu, creg); break;
+                  case 2: rphase_1q<2>(a, uu, creg); break;
+                  default: rphase_1q<3>(a, uu, creg); break;
+                }
+              } else {
+                switch (rt) {
+                  case 0: rphase_x<0>(a, creg); break;
+                  case 1: rphase_x<1>(a, creg); break;
+                  case 2: rphase_x<2>(a, creg); break;
+                  default: rphase_x<3>(a, creg); break;
+                }
+              }
+            }
+#pragma unroll
+            for (int j = 0; j < 16; ++j) sm[sidx(sb, j)] = a[j];
+          }
+          // continue after the phase's ops
+          oi += cnt;
+          if (oi + 1 < pg.nops) fetch(oi + 1);
+          break;
+        }
         case T_FAIL:
           if (tid == 0 && rank == 0) atomicMin(P.failed, ((long long)it.prog << 40) | op.inst);
           break;
@@ -632,6 +717,50 @@ void mark_remote(TOp* ops, size_t count, uint32_t lb) {
   }
 }
 
+// Register phases: maximal runs (two or more) of unconditional T_ONEQ /
+// T_XPERM ops whose targets and controls all lie within four local bits
+// become one T_RPHASE header followed by the ops (in program order).
+std::vector<TOp> group_phases(const std::vector<TOp>& ops, uint32_t lb) {
+  std::vector<TOp> out;
+  if (lb < 4) return ops;
+  const uint64_t lmask = (1ULL << lb) - 1;
+  auto bits_of = [](const TOp& t) { return t.ctrl | (1ULL << t.t1); };
+  auto eligible = [&](const TOp& t) {
+    return (t.type == T_ONEQ || t.type == T_XPERM) && t.cond_count == 0 && !t.remote &&
+           (bits_of(t) & ~lmask) == 0;
+  };
+  size_t i = 0;
+  while (i < ops.size()) {
+    if (!eligible(ops[i])) {
+      out.push_back(ops[i++]);
+      continue;
+    }
+    uint64_t set = bits_of(ops[i]);
+    size_t j = i + 1;
+    while (j < ops.size() && j - i < 255 && eligible(ops[j]) &&
+           __builtin_popcountll(set | bits_of(ops[j])) <= 4) {
+      set |= bits_of(ops[j]);
+      ++j;
+    }
+    if (j - i < 2 || __builtin_popcountll(set) > 4) {
+      out.push_back(ops[i++]);
+      continue;
+    }
+    for (uint32_t b = 0; b < lb && __builtin_popcountll(set) < 4; ++b) set |= 1ULL << b;
+    TOp h{};
+    h.type = T_RPHASE;
+    h.k = (uint8_t)(j - i);
+    h.inst = ops[i].inst;
+    int nb = 0;
+    for (uint32_t b = 0; b < lb; ++b)
+      if ((set >> b) & 1ULL) h.q[nb++] = (uint8_t)b;
+    out.push_back(h);
+    for (size_t k = i; k < j; ++k) out.push_back(ops[k]);
+    i = j;
+  }
+  return out;
+}
+
 // All programs and trajectories of one launch (one cluster span).
 struct LaunchSet {
   Encoded enc;
@@ -652,6 +781,13 @@ int add_program(LaunchSet& ls, const dq_inst* prog, uint64_t ninst, const dq_con
   DQ_TRY(encode_program(prog, ninst, n, cond_base, ls.enc));
   pg.nops = (uint32_t)(ls.enc.ops.size() - pg.ops_off);
   mark_remote(ls.enc.ops.data() + pg.ops_off, pg.nops, lb);
+  {
+    const std::vector<TOp> tail(ls.enc.ops.begin() + pg.ops_off, ls.enc.ops.end());
+    const std::vector<TOp> grouped = group_phases(tail, lb);
+    ls.enc.ops.resize(pg.ops_off);
+    ls.enc.ops.insert(ls.enc.ops.end(), grouped.begin(), grouped.end());
+    pg.nops = (uint32_t)grouped.size();
+  }
   pg.n = n;
   pg.lb = lb;
   pg.ncbits = ncbits;
