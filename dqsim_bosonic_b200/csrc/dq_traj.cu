@@ -240,16 +240,14 @@ __global__ void __launch_bounds__(THREADS) k_traj(const TrajParams P) {
           const uint64_t hi_ctrl = op.ctrl & ~lmask;
           const uint32_t lo_ctrl = (uint32_t)(op.ctrl & lmask);
           // local zero-insertion positions: target (if local) and local controls
-          uint32_t pos[9];
-          int np = 0;
-          uint64_t m = lo_ctrl | (t < lb ? (1ULL << t) : 0ULL);
-          while (m) {
-            const uint32_t b = __ffsll((long long)m) - 1;
-            pos[np++] = b;
-            m &= m - 1;
-          }
+          // local zero-insertion positions (the set bits of zmask, ascending;
+          // no array: a dynamically indexed one would live in local memory)
+          const uint64_t zmask = lo_ctrl | (t < lb ? (1ULL << t) : 0ULL);
+          const int np = __popcll((long long)zmask);
           const uint32_t count = L >> np;
-          const uint32_t p0 = np > 0 ? pos[0] : 0u, p1 = np > 1 ? pos[1] : 0u;
+          const uint32_t p0 = np > 0 ? (uint32_t)(__ffsll((long long)zmask) - 1) : 0u;
+          const uint64_t zm1 = zmask & (zmask - 1);
+          const uint32_t p1 = np > 1 ? (uint32_t)(__ffsll((long long)zm1) - 1) : 0u;
           // pair k -> swizzled index of its element with the target bit 0
           auto index = [&](uint32_t k) -> uint32_t {
             uint32_t o;
@@ -259,7 +257,7 @@ __global__ void __launch_bounds__(THREADS) k_traj(const TrajParams P) {
               o = ins0(ins0(k, p0), p1);
             } else {
               o = k;
-              for (int p = 0; p < np; ++p) o = ins0(o, pos[p]);
+              for (uint64_t mm = zmask; mm; mm &= mm - 1) o = ins0(o, (uint32_t)(__ffsll((long long)mm) - 1));
             }
             return tswz(o | lo_ctrl);
           };
@@ -313,16 +311,11 @@ __global__ void __launch_bounds__(THREADS) k_traj(const TrajParams P) {
           const uint64_t hi = need & ~lmask, lo = need & lmask;
           if ((gbase & hi) != hi) break;
           const double2 e = P.pool[op.mat];
-          uint32_t pos[9];
-          int np = 0;
-          uint64_t m = lo;
-          while (m) {
-            const uint32_t b = __ffsll((long long)m) - 1;
-            pos[np++] = b;
-            m &= m - 1;
-          }
+          const int np = __popcll((long long)lo);
           const uint32_t count = L >> np;
-          const uint32_t p0 = np > 0 ? pos[0] : 0u, p1 = np > 1 ? pos[1] : 0u;
+          const uint32_t p0 = np > 0 ? (uint32_t)(__ffsll((long long)lo) - 1) : 0u;
+          const uint64_t lo1 = lo & (lo - 1);
+          const uint32_t p1 = np > 1 ? (uint32_t)(__ffsll((long long)lo1) - 1) : 0u;
           for (uint32_t k0 = tid; k0 < count; k0 += 4u * THREADS) {
             uint32_t so[4];
             double2 a[4];
@@ -336,7 +329,7 @@ __global__ void __launch_bounds__(THREADS) k_traj(const TrajParams P) {
                 o = ins0(ins0(k, p0), p1);
               } else {
                 o = k;
-                for (int p = 0; p < np; ++p) o = ins0(o, pos[p]);
+                for (uint64_t mm = lo; mm; mm &= mm - 1) o = ins0(o, (uint32_t)(__ffsll((long long)mm) - 1));
               }
               so[v] = tswz(o | (uint32_t)lo);
               a[v] = sm[so[v]];
@@ -368,19 +361,12 @@ __global__ void __launch_bounds__(THREADS) k_traj(const TrajParams P) {
           const uint64_t gate = op.ctrl | b1 | b2;
           const uint64_t hi_one = fixed1 & ~lmask, hi_zero = b2 & ~lmask;
           if ((gbase & hi_one) != hi_one || (gbase & hi_zero) != 0) break;
-          uint32_t pos[10];
-          int np = 0;
-          uint64_t m = gate & lmask;
-          while (m) {
-            const uint32_t b = __ffsll((long long)m) - 1;
-            pos[np++] = b;
-            m &= m - 1;
-          }
-          const uint32_t count = L >> np;
+          const uint64_t zmask = gate & lmask;
+          const uint32_t count = L >> __popcll((long long)zmask);
           const uint32_t lo_one = (uint32_t)(fixed1 & lmask);
           for (uint32_t k = tid; k < count; k += THREADS) {
             uint32_t o = k;
-            for (int p = 0; p < np; ++p) o = ins0(o, pos[p]);
+            for (uint64_t mm = zmask; mm; mm &= mm - 1) o = ins0(o, (uint32_t)(__ffsll((long long)mm) - 1));
             o |= lo_one;
             const uint64_t gi = gbase | o, gj = gi ^ b1 ^ b2;
             double2* pi = sm + tswz(o);
@@ -396,18 +382,11 @@ __global__ void __launch_bounds__(THREADS) k_traj(const TrajParams P) {
           uint64_t gm = 0;
           for (uint32_t b = 0; b < kq; ++b) gm |= 1ULL << op.q[b];
           if ((gbase & gm & ~lmask) != 0) break;  // group base must have the gate bits zero
-          uint32_t pos[8];
-          int np = 0;
-          uint64_t m = gm & lmask;
-          while (m) {
-            const uint32_t b = __ffsll((long long)m) - 1;
-            pos[np++] = b;
-            m &= m - 1;
-          }
-          const uint32_t count = L >> np;
+          const uint64_t zmask = gm & lmask;
+          const uint32_t count = L >> __popcll((long long)zmask);
           for (uint32_t k = tid; k < count; k += THREADS) {
             uint32_t o = k;
-            for (int p = 0; p < np; ++p) o = ins0(o, pos[p]);
+            for (uint64_t mm = zmask; mm; mm &= mm - 1) o = ins0(o, (uint32_t)(__ffsll((long long)mm) - 1));
             const uint64_t base = gbase | o;
             double2 v[32];
             double2* ptr[32];
