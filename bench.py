@@ -21,6 +21,7 @@ launch time) against the measured copy peak.
 from __future__ import annotations
 
 import argparse
+import gc
 import json
 import math
 import os
@@ -382,14 +383,20 @@ def main():
     torch.cuda.synchronize(dev)
     d.barrier()
     e2e_t = []
+    # the interpreter's cyclic garbage collector stays off inside the timed
+    # host steps (as timeit does); it runs between them
+    gc.collect()
     for _ in range(args.steps):
         torch.cuda.synchronize(dev)
+        gc.disable()
         t0 = time.perf_counter()
         res = sim.simulate(circ)
         p = res.probability_array(top)
         torch.cuda.synchronize(dev)
         e2e_t.append(time.perf_counter() - t0)
+        gc.enable()
         del res
+        gc.collect()
     e2e_total = d.max(float(np.sum(e2e_t)))
     e2e_value = eff_bytes * args.steps * d.world / e2e_total / 1e9
 
