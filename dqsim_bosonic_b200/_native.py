@@ -98,6 +98,16 @@ class TrajOpts(ctypes.Structure):
     ]
 
 
+class MpsStats(ctypes.Structure):
+    _fields_ = [
+        ("svd_calls", ctypes.c_uint64),
+        ("kernel_ms", ctypes.c_double),
+        ("failed_inst", ctypes.c_int64),
+        ("capacity", ctypes.c_uint32),
+        ("replicas", ctypes.c_uint32),
+    ]
+
+
 class TrajStats(ctypes.Structure):
     _fields_ = [
         ("boundary_draws", ctypes.c_uint64),
@@ -191,6 +201,17 @@ SIGNATURES = [
     ("dq_debug_plan", ctypes.c_int, [_U32, _P, _U64, ctypes.POINTER(RunOpts), _P, _U64,
                                      ctypes.POINTER(_U64)]),
     ("dq_block_merge", ctypes.c_int, [_P, _P, _U32, _P, _P, _U32, _P]),
+    ("dq_mps_create", ctypes.c_int, [_U32, ctypes.c_int, _U32, ctypes.c_double, ctypes.POINTER(_P)]),
+    ("dq_mps_destroy", ctypes.c_int, [_P]),
+    ("dq_mps_run", ctypes.c_int, [_P, _P, _U64, _P, _U64, _U64, _P, _U64,
+                                  ctypes.POINTER(MpsStats)]),
+    ("dq_mps_apply_2q", ctypes.c_int, [_P, _U32, _U32, _P]),
+    ("dq_mps_reserve", ctypes.c_int, [_P, _U32]),
+    ("dq_mps_bond_dims", ctypes.c_int, [_P, _P]),
+    ("dq_mps_to_state", ctypes.c_int, [_P, _P]),
+    ("dq_mps_run_shots", ctypes.c_int, [ctypes.c_int, _U32, _U32, ctypes.c_double, _P, _U64, _P,
+                                        _U64, _U64, _U64, _U64, _P, _U64, _U32,
+                                        ctypes.POINTER(MpsStats)]),
     ("dq_rng_f64", ctypes.c_int, [_U64, _U64, _U64, _P]),
     ("dq_rng_seed_key", ctypes.c_int, [_U64, _P]),
     ("dq_chacha_block", ctypes.c_int, [_P, _U32, _P]),

@@ -1,0 +1,1105 @@
+// dq_mps.cu — matrix-product-state backend on the device.
+//
+// Restates the MPS simulator of the reference (src/monolithic/mps/simulator.rs):
+// one rank-3 tensor A_k[l][s][r] per qubit k, bond dimensions dims[0..n]
+// (dims[0] = dims[n] = 1), single-qubit gates contracted into one tensor
+// (apply_1q, :99-113), two-qubit gates as a chain of adjacent steps (apply_2q,
+// :115-135) whose every step contracts the two tensors with the 4x4 gate into
+// theta (2L x 2R), takes its SVD, truncates and splits it again
+// (apply_adjacent_2q, :137-236), measurement by p1 / draw / projection
+// (measure, project_qubit, :259-291) and reset = measure + X.
+//
+// B200 design: a batch of B independent MPS (one per shot; B = 1 for
+// `simulate`) lives in HBM with padded tensors (capacity `cap` per bond) and
+// per-replica bond dimensions on the device.  Every program operation is one
+// launch over the whole batch, one CTA per replica, so the host never reads a
+// bond dimension while the program runs:
+//   k_mps_1q       the 2x2 contraction of one site (exact num-complex order)
+//   k_mps_2q       FUSED adjacent step: theta build, one-sided (Hestenes)
+//                  Jacobi SVD in shared memory, descending sort, truncation
+//                  with the reference's keep / renormalisation rule, split
+//                  into the two new site tensors, new bond dimension
+//   k_mps_measure  p1 by a transfer-matrix contraction over the chain
+//                  (O(n chi^3) instead of the reference's 2^n statevector),
+//                  the replica's ChaCha8 draw, projection, reset flip, cbit
+//   k_mps_expand   to_statevector (:238-257) as a left-to-right contraction,
+//                  one launch per site, same summation order as the reference
+// Conditions are evaluated per replica on the device.  When a truncation
+// keeps more singular values than the capacity, the kernel flags it and the
+// host re-runs the (deterministic) program with a larger capacity.
+//
+// The SVD differs from nalgebra's (Golub-Kahan) in the gauge of U and V, so
+// site tensors are not bit-identical to the reference; everything a caller
+// can observe (statevector, probabilities, outcomes) is gauge-invariant and
+// held to a tolerance.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cfloat>
+#include <cmath>
+#include <string>
+#include <vector>
+
+#include "dq_common.cuh"
+#include "dq_gates.hpp"
+#include "dq_handle.cuh"
+#include "dq_rng.cuh"
+
+namespace dq {
+namespace {
+
+enum MpsOpKind : int32_t { M_1Q = 0, M_2Q = 1, M_MEAS = 2, M_RESET = 3, M_FAIL = 4 };
+
+struct MpsOp {
+  int32_t kind;
+  uint32_t q;            // site (M_2Q: left site of the bond q, q+1)
+  int32_t cbit;          // M_MEAS: classical bit written
+  uint32_t cond_first;   // condition chain (all must hold)
+  uint32_t cond_count;
+  int32_t inst;          // instruction index (error reports)
+  double2 u[16];         // M_1Q: 2x2 row-major in u[0..3]; M_2Q: 4x4 row-major
+};
+
+// Device view of a batch.
+struct MpsView {
+  double2* t;            // site k of replica b at t + (k * batch + b) * site_elems
+  uint32_t* dims;        // batch x (n + 1)
+  const uint32_t* key;   // batch x 8 ChaCha8 key words
+  unsigned long long* ctr;  // batch: draws consumed
+  int32_t* cbits;        // batch x ncb
+  const dq_cond* conds;
+  double2* scratch;      // batch x scratch_elems (global fallback of the SVD work area)
+  int* flags;            // [0] status, [1] first failing instruction, [2] capacity needed
+  unsigned long long* svd_calls;
+  uint64_t site_elems;   // cap * 2 * cap
+  uint64_t scratch_elems;
+  uint32_t n, batch, cap, ncb;
+};
+
+enum : int { F_OK = 0, F_UNSUPPORTED = 1, F_CAPACITY = 2 };
+
+constexpr int kMpsThreads = 256;
+constexpr int kMaxSweeps = 60;
+
+__device__ __forceinline__ double2* site(const MpsView& v, uint32_t k, uint32_t b) {
+  return v.t + ((uint64_t)k * v.batch + b) * v.site_elems;
+}
+
+__device__ __forceinline__ bool cond_ok(const MpsView& v, const MpsOp& op, uint32_t b) {
+  const int32_t* cb = v.cbits + (uint64_t)b * v.ncb;
+  for (uint32_t c = 0; c < op.cond_count; ++c) {
+    const dq_cond cd = v.conds[op.cond_first + c];
+    uint64_t actual = 0;
+    for (uint64_t i = 0; i < cd.creg_size; ++i) {
+      const uint64_t idx = cd.creg_base + i;
+      const uint64_t bit = (idx < v.ncb && cb[idx] > 0) ? (uint64_t)cb[idx] : 0;
+      actual |= bit << i;
+    }
+    if (actual != cd.creg_value) return false;
+  }
+  return true;
+}
+
+// new[l][o][r] = sum_i u[o][i] old[l][i][r], accumulated from zero in the
+// reference's order (apply_1q, simulator.rs:99-113).
+__device__ void site_1q(double2* a, uint32_t L, uint32_t R, uint32_t cap, const double2* u) {
+  const double2 zero = make_double2(0.0, 0.0);
+  for (uint32_t t = threadIdx.x; t < L * R; t += blockDim.x) {
+    const uint32_t l = t / R, r = t - (t / R) * R;
+    double2* p0 = a + (uint64_t)(l * 2) * cap + r;
+    double2* p1 = p0 + cap;
+    const double2 a0 = *p0, a1 = *p1;
+    *p0 = cadd_x(cadd_x(zero, cmul_x(u[0], a0)), cmul_x(u[1], a1));
+    *p1 = cadd_x(cadd_x(zero, cmul_x(u[2], a0)), cmul_x(u[3], a1));
+  }
+}
+
+__global__ void __launch_bounds__(kMpsThreads) k_mps_reset(MpsView v) {
+  const uint32_t b = blockIdx.x;
+  for (uint32_t k = 0; k < v.n; ++k) {
+    double2* a = site(v, k, b);
+    if (threadIdx.x == 0) a[0] = make_double2(1.0, 0.0);   // |0>: A[0][0][0] = 1
+    if (threadIdx.x == 1) a[v.cap] = make_double2(0.0, 0.0);  // A[0][1][0] = 0
+  }
+  for (uint32_t k = threadIdx.x; k <= v.n; k += blockDim.x) v.dims[(uint64_t)b * (v.n + 1) + k] = 1;
+  for (uint32_t c = threadIdx.x; c < v.ncb; c += blockDim.x) v.cbits[(uint64_t)b * v.ncb + c] = -1;
+  if (threadIdx.x == 0) v.ctr[b] = 0;
+}
+
+__global__ void __launch_bounds__(kMpsThreads) k_mps_1q(MpsView v, MpsOp op) {
+  const uint32_t b = blockIdx.x;
+  if (!cond_ok(v, op, b)) return;
+  const uint32_t* dm = v.dims + (uint64_t)b * (v.n + 1);
+  site_1q(site(v, op.q, b), dm[op.q], dm[op.q + 1], v.cap, op.u);
+}
+
+__device__ __forceinline__ double warp_sum(double x) {
+  for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+  return x;
+}
+
+// Work-area size (double2 elements) of the fused step at capacity cap:
+// G (rows x cols) + J (cols x cols) + sigma (cols doubles) + perm (cols u32).
+__host__ __device__ inline uint64_t svd_work_elems(uint32_t cap) {
+  const uint64_t c = 2ull * cap;
+  return c * c + c * c + c + (c + 1) / 2;
+}
+
+// Fused adjacent two-qubit step on bond (q, q+1) of every replica.
+//   theta[(l*2+o0)][(o1*R+r)] = sum_in u[o][in] sum_k A[l][in0][k] B[k][in1][r]
+// (apply_adjacent_2q, simulator.rs:148-171; same accumulation order).  The
+// SVD is one-sided Jacobi on G = theta (2R <= 2L) or G = theta^H (2R > 2L):
+// column pairs (p, q) of a round-robin tournament are rotated until every
+// pair is orthogonal to within rows * eps, J accumulating the rotations, so
+// G = W J^H with orthogonal columns W_j = sigma_j u_j.
+__global__ void __launch_bounds__(kMpsThreads) k_mps_2q(MpsView v, MpsOp op, uint32_t max_keep,
+                                                        double thr, int use_smem) {
+  extern __shared__ double2 smem[];
+  __shared__ int s_rot;
+  __shared__ uint32_t s_keep;
+  __shared__ double s_scale;
+  const uint32_t b = blockIdx.x;
+  if (!cond_ok(v, op, b)) return;
+  uint32_t* dm = v.dims + (uint64_t)b * (v.n + 1);
+  const uint32_t q = op.q, cap = v.cap;
+  const uint32_t L = dm[q], M = dm[q + 1], R = dm[q + 2];
+  const bool tr = R > L;
+  const uint32_t rows = tr ? 2 * R : 2 * L, cols = tr ? 2 * L : 2 * R;
+  double2* G = use_smem ? smem : v.scratch + (uint64_t)b * v.scratch_elems;
+  double2* J = G + (uint64_t)rows * cols;
+  double* sig = reinterpret_cast<double*>(J + (uint64_t)cols * cols);
+  uint32_t* perm = reinterpret_cast<uint32_t*>(sig + cols);
+  double2* A = site(v, q, b);
+  double2* B = site(v, q + 1, b);
+  const double2 zero = make_double2(0.0, 0.0);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
+
+  // ---- theta -> G (column-major) ---------------------------------------------
+  for (uint32_t t = tid; t < L * R; t += blockDim.x) {
+    const uint32_t l = t / R, r = t - (t / R) * R;
+    double2 in[4];
+    for (int i0 = 0; i0 < 2; ++i0)
+      for (int i1 = 0; i1 < 2; ++i1) {
+        double2 acc = zero;
+        const double2* ar = A + (uint64_t)(l * 2 + i0) * cap;
+        for (uint32_t k = 0; k < M; ++k)
+          acc = cadd_x(acc, cmul_x(ar[k], B[(uint64_t)(k * 2 + i1) * cap + r]));
+        in[i0 * 2 + i1] = acc;
+      }
+    for (int o0 = 0; o0 < 2; ++o0)
+      for (int o1 = 0; o1 < 2; ++o1) {
+        const int o = o0 * 2 + o1;
+        double2 acc = zero;
+        for (int i = 0; i < 4; ++i) acc = cadd_x(acc, cmul_x(op.u[o * 4 + i], in[i]));
+        const uint32_t row = l * 2 + o0, col = o1 * R + r;
+        if (!tr) G[(uint64_t)col * rows + row] = acc;
+        else G[(uint64_t)row * rows + col] = make_double2(acc.x, -acc.y);
+      }
+  }
+  for (uint32_t t = tid; t < cols * cols; t += blockDim.x)
+    J[t] = (t / cols == t % cols) ? make_double2(1.0, 0.0) : zero;
+  if (tid == 0) s_rot = 0;
+  __syncthreads();
+
+  // ---- one-sided Jacobi --------------------------------------------------------
+  const double tol = (double)rows * DBL_EPSILON;
+  const uint32_t np = cols / 2;
+  for (int sweep = 0; sweep < kMaxSweeps; ++sweep) {
+    for (uint32_t rd = 0; rd + 1 < cols; ++rd) {
+      for (uint32_t pi = warp; pi < np; pi += nw) {
+        uint32_t p, qq;
+        if (pi == 0) {
+          p = rd;
+          qq = cols - 1;
+        } else {
+          p = (rd + pi) % (cols - 1);
+          qq = (rd + (cols - 1) - pi) % (cols - 1);
+        }
+        double2* gp = G + (uint64_t)p * rows;
+        double2* gq = G + (uint64_t)qq * rows;
+        double al = 0.0, be = 0.0, gr = 0.0, gi = 0.0;
+        for (uint32_t i = lane; i < rows; i += 32) {
+          const double2 x = gp[i], y = gq[i];
+          al += x.x * x.x + x.y * x.y;
+          be += y.x * y.x + y.y * y.y;
+          gr += x.x * y.x + x.y * y.y;
+          gi += x.x * y.y - x.y * y.x;
+        }
+        al = warp_sum(al);
+        be = warp_sum(be);
+        gr = warp_sum(gr);
+        gi = warp_sum(gi);
+        const double ag = sqrt(gr * gr + gi * gi);
+        if (ag > 0.0 && ag > tol * sqrt(al) * sqrt(be)) {
+          if (lane == 0) s_rot = 1;
+          const double zeta = (be - al) / (2.0 * ag);
+          const double t = (zeta >= 0.0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+          const double c = 1.0 / sqrt(1.0 + t * t), s = c * t;
+          const double ex = gr / ag, ey = gi / ag;  // e^{i phi}, gamma = |gamma| e^{i phi}
+          // a_p' = c a_p - s e^{-i phi} a_q ;  a_q' = s e^{i phi} a_p + c a_q
+          for (uint32_t i = lane; i < rows; i += 32) {
+            const double2 x = gp[i], y = gq[i];
+            gp[i] = make_double2(c * x.x - s * (ex * y.x + ey * y.y), c * x.y - s * (ex * y.y - ey * y.x));
+            gq[i] = make_double2(s * (ex * x.x - ey * x.y) + c * y.x, s * (ex * x.y + ey * x.x) + c * y.y);
+          }
+          double2* jp = J + (uint64_t)p * cols;
+          double2* jq = J + (uint64_t)qq * cols;
+          for (uint32_t i = lane; i < cols; i += 32) {
+            const double2 x = jp[i], y = jq[i];
+            jp[i] = make_double2(c * x.x - s * (ex * y.x + ey * y.y), c * x.y - s * (ex * y.y - ey * y.x));
+            jq[i] = make_double2(s * (ex * x.x - ey * x.y) + c * y.x, s * (ex * x.y + ey * x.x) + c * y.y);
+          }
+        }
+      }
+      __syncthreads();
+    }
+    const int rot = s_rot;
+    __syncthreads();
+    if (!rot) break;
+    if (tid == 0) s_rot = 0;
+    __syncthreads();
+  }
+
+  // ---- singular values, descending order (ties by column index) ---------------
+  for (uint32_t j = warp; j < cols; j += nw) {
+    const double2* g = G + (uint64_t)j * rows;
+    double s = 0.0;
+    for (uint32_t i = lane; i < rows; i += 32) s += g[i].x * g[i].x + g[i].y * g[i].y;
+    s = warp_sum(s);
+    if (lane == 0) sig[j] = sqrt(s);
+  }
+  __syncthreads();
+  for (uint32_t j = tid; j < cols; j += blockDim.x) {
+    uint32_t rank = 0;
+    const double sj = sig[j];
+    for (uint32_t i = 0; i < cols; ++i) rank += (sig[i] > sj || (sig[i] == sj && i < j)) ? 1u : 0u;
+    perm[rank] = j;
+  }
+  __syncthreads();
+
+  // ---- truncation (simulator.rs:186-218) ----------------------------------------
+  if (tid == 0) {
+    uint32_t keep = 0;
+    for (uint32_t k = 0; k < cols; ++k) keep += sig[perm[k]] > thr ? 1u : 0u;
+    keep = keep > 1u ? keep : 1u;
+    if (max_keep) keep = keep < max_keep ? keep : max_keep;
+    double kept = 0.0, total = 0.0, disc = 0.0;
+    for (uint32_t k = 0; k < keep; ++k) kept += sig[perm[k]] * sig[perm[k]];
+    for (uint32_t k = 0; k < cols; ++k) total += sig[perm[k]] * sig[perm[k]];
+    for (uint32_t k = keep; k < cols; ++k) disc += sig[perm[k]] * sig[perm[k]];
+    kept = fmax(sqrt(kept), 1e-15);
+    total = sqrt(total);
+    s_scale = disc > 0.0 ? total / kept : 1.0;
+    s_keep = keep;
+    if (keep > cap) {
+      atomicMax(&v.flags[2], (int)keep);
+      atomicMax(&v.flags[0], F_CAPACITY);
+    } else {
+      atomicAdd(v.svd_calls, 1ull);
+    }
+  }
+  __syncthreads();
+  const uint32_t keep = s_keep;
+  if (keep > cap) return;
+  const double scale = s_scale;
+
+  // ---- split: A' = U[:, :keep], B' = (sigma * scale) V^H[:keep, :] -------------
+  for (uint32_t t = tid; t < L * 2 * keep; t += blockDim.x) {
+    const uint32_t row = t / keep, k = t - (t / keep) * keep;   // row = l*2 + s
+    const uint32_t j = perm[k];
+    double2 val;
+    if (tr) {
+      val = J[(uint64_t)j * cols + row];
+    } else {
+      const double sj = sig[j];
+      const double2 g = G[(uint64_t)j * rows + row];
+      val = sj > 0.0 ? make_double2(g.x / sj, g.y / sj) : zero;
+    }
+    A[(uint64_t)row * cap + k] = val;
+  }
+  for (uint32_t t = tid; t < keep * 2 * R; t += blockDim.x) {
+    const uint32_t k = t / (2 * R), col = t - (t / (2 * R)) * (2 * R);  // col = s*R + r
+    const uint32_t s = col / R, r = col - (col / R) * R;
+    const uint32_t j = perm[k];
+    const double sj = sig[j];
+    double2 vh;
+    if (tr) {
+      const double2 g = G[(uint64_t)j * rows + col];
+      vh = sj > 0.0 ? make_double2(g.x / sj, -g.y / sj) : zero;
+    } else {
+      const double2 x = J[(uint64_t)j * cols + col];
+      vh = make_double2(x.x, -x.y);
+    }
+    B[(uint64_t)(k * 2 + s) * cap + r] = cmul_x(make_double2(sj * scale, 0.0), vh);
+  }
+  if (tid == 0) dm[q + 1] = keep;
+}
+
+// p1 of qubit op.q by transfer matrices E_{j+1} = sum_s A_j[s]^H E_j A_j[s]
+// (s = 1 only at the measured site), then the draw, the projection
+// (project_qubit, simulator.rs:276-291), the reset flip and the cbit.
+__global__ void __launch_bounds__(kMpsThreads) k_mps_measure(MpsView v, MpsOp op, int use_smem) {
+  extern __shared__ double2 smem[];
+  __shared__ int s_out;
+  __shared__ double s_scale;
+  const uint32_t b = blockIdx.x;
+  if (!cond_ok(v, op, b)) return;
+  const uint32_t* dm = v.dims + (uint64_t)b * (v.n + 1);
+  const uint32_t cap = v.cap;
+  double2* E = use_smem ? smem : v.scratch + (uint64_t)b * v.scratch_elems;
+  double2* F = E + (uint64_t)cap * cap;
+  double2* E2 = F + (uint64_t)cap * cap;
+  const double2 zero = make_double2(0.0, 0.0);
+  const int tid = threadIdx.x;
+  if (tid == 0) E[0] = make_double2(1.0, 0.0);
+  __syncthreads();
+  for (uint32_t j = 0; j < v.n; ++j) {
+    const uint32_t Lj = dm[j], Rj = dm[j + 1];
+    const double2* A = site(v, j, b);
+    for (uint32_t t = tid; t < Rj * Rj; t += blockDim.x) E2[t] = zero;
+    for (int s = 0; s < 2; ++s) {
+      if (j == op.q && s == 0) continue;
+      __syncthreads();
+      // F[l][r'] = sum_l' E[l][l'] A[l'][s][r']
+      for (uint32_t t = tid; t < Lj * Rj; t += blockDim.x) {
+        const uint32_t l = t / Rj, rp = t - (t / Rj) * Rj;
+        double2 acc = zero;
+        for (uint32_t lp = 0; lp < Lj; ++lp) {
+          const double2 e = E[l * Lj + lp], a = A[(uint64_t)(lp * 2 + s) * cap + rp];
+          acc.x += e.x * a.x - e.y * a.y;
+          acc.y += e.x * a.y + e.y * a.x;
+        }
+        F[t] = acc;
+      }
+      __syncthreads();
+      // E2[r][r'] += sum_l conj(A[l][s][r]) F[l][r']
+      for (uint32_t t = tid; t < Rj * Rj; t += blockDim.x) {
+        const uint32_t r = t / Rj, rp = t - (t / Rj) * Rj;
+        double2 acc = E2[t];
+        for (uint32_t l = 0; l < Lj; ++l) {
+          const double2 a = A[(uint64_t)(l * 2 + s) * cap + r], f = F[l * Rj + rp];
+          acc.x += a.x * f.x + a.y * f.y;
+          acc.y += a.x * f.y - a.y * f.x;
+        }
+        E2[t] = acc;
+      }
+    }
+    __syncthreads();
+    for (uint32_t t = tid; t < Rj * Rj; t += blockDim.x) E[t] = E2[t];
+    __syncthreads();
+  }
+  if (tid == 0) {
+    double p1 = E[0].x;
+    p1 = fmin(fmax(p1, 0.0), 1.0);
+    const double r = chacha8_draw(v.key + (uint64_t)b * 8, v.ctr[b]);
+    v.ctr[b] += 1;
+    const int outcome = r < p1 ? 1 : 0;
+    const double prob = outcome ? p1 : 1.0 - p1;
+    s_out = outcome;
+    s_scale = prob > 0.0 ? 1.0 / sqrt(prob) : 0.0;
+    if (op.kind == M_MEAS && op.cbit >= 0) v.cbits[(uint64_t)b * v.ncb + op.cbit] = outcome;
+  }
+  __syncthreads();
+  const int outcome = s_out;
+  const double2 sc = make_double2(s_scale, 0.0);
+  double2* A = site(v, op.q, b);
+  const uint32_t L = dm[op.q], R = dm[op.q + 1];
+  for (uint32_t t = tid; t < L * 2 * R; t += blockDim.x) {
+    const uint32_t row = t / R, r = t - (t / R) * R;   // row = l*2 + s
+    double2* p = A + (uint64_t)row * cap + r;
+    *p = ((int)(row & 1u) == outcome) ? cmul_x(*p, sc) : zero;
+  }
+  if (op.kind == M_RESET && outcome == 1) {
+    __syncthreads();
+    const double2 xm[4] = {zero, make_double2(1.0, 0.0), make_double2(1.0, 0.0), zero};
+    site_1q(A, L, R, cap, xm);
+  }
+}
+
+__global__ void k_mps_fail(MpsView v, MpsOp op) {
+  const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= v.batch || !cond_ok(v, op, b)) return;
+  atomicMax(&v.flags[0], F_UNSUPPORTED);
+  atomicMin(&v.flags[1], op.inst);
+}
+
+// One site of to_statevector (simulator.rs:238-257): from W (2^k x Lk, row i
+// = basis bits of qubits 0..k-1) to W' (2^(k+1) x Rk): W'[i + s 2^k][r] =
+// sum_l W[i][l] A[l][s][r], accumulated from zero in ascending l.
+__global__ void __launch_bounds__(256) k_mps_expand(const double2* __restrict__ w,
+                                                    double2* __restrict__ wn,
+                                                    const double2* __restrict__ a, uint32_t k,
+                                                    uint32_t Lk, uint32_t Rk, uint32_t cap) {
+  const uint64_t total = (2ull << k) * Rk;
+  const uint64_t half = 1ull << k;
+  for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+       t += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t i2 = t / Rk;
+    const uint32_t r = (uint32_t)(t - i2 * Rk);
+    const uint64_t i = i2 & (half - 1);
+    const uint32_t s = (uint32_t)(i2 >> k);
+    double2 acc = make_double2(0.0, 0.0);
+    for (uint32_t l = 0; l < Lk; ++l)
+      acc = cadd_x(acc, cmul_x(w[i * Lk + l], a[(uint64_t)(l * 2 + s) * cap + r]));
+    wn[t] = acc;
+  }
+}
+
+// ---- host side -------------------------------------------------------------------
+
+bool is_two_qubit_kind(int kind) {
+  switch (kind) {
+    case DQ_CX: case DQ_CZ: case DQ_CY: case DQ_CH: case DQ_SWAP: case DQ_CSX: case DQ_CRX:
+    case DQ_CRY: case DQ_CRZ: case DQ_CU1: case DQ_CP: case DQ_CU3: case DQ_CU: case DQ_RXX:
+    case DQ_RZZ: case DQ_G_PHI_PLUS: case DQ_G_PSI_MINUS: case DQ_G_PSI_PLUS: case DQ_G_CZ:
+    case DQ_G_CX:
+      return true;
+    default:
+      return false;
+  }
+}
+
+void set_u(MpsOp& op, const hc* m, int count) {
+  for (int i = 0; i < count; ++i) op.u[i] = make_double2(m[i].re, m[i].im);
+}
+
+// reverse_2q_order (simulator.rs:561-579): the gate with its two qubits exchanged.
+void reverse_2q(const hc in[16], hc out[16]) {
+  for (int a0 = 0; a0 < 2; ++a0)
+    for (int b0 = 0; b0 < 2; ++b0)
+      for (int a1 = 0; a1 < 2; ++a1)
+        for (int b1 = 0; b1 < 2; ++b1)
+          out[(a0 * 2 + b0) * 4 + (a1 * 2 + b1)] = in[(b0 * 2 + a0) * 4 + (b1 * 2 + a1)];
+}
+
+}  // namespace
+}  // namespace dq
+
+using namespace dq;
+
+struct dq_mps_s {
+  int device = 0;
+  uint32_t n = 0;
+  uint32_t batch = 0;
+  uint32_t cap = 0;
+  uint32_t max_bond = 0;    // 0 = unbounded
+  double thr = 1e-12;
+  uint32_t ncb = 0;
+  cudaStream_t stream = nullptr;
+  double2* t = nullptr;
+  uint32_t* dims = nullptr;
+  uint32_t* key = nullptr;
+  unsigned long long* ctr = nullptr;
+  int32_t* cbits = nullptr;
+  dq_cond* conds = nullptr;
+  uint64_t conds_cap = 0;
+  double2* scratch = nullptr;
+  int* flags = nullptr;
+  unsigned long long* svd_calls = nullptr;
+  bool smem = true;
+  uint64_t scratch_elems = 0;
+};
+
+namespace {
+
+uint32_t bond_bound(uint32_t n, uint32_t max_bond) {
+  const uint32_t half = n / 2;
+  const uint64_t b = half >= 31 ? (1ull << 31) : (1ull << half);
+  uint64_t r = b < 1 ? 1 : b;
+  if (max_bond && max_bond < r) r = max_bond;
+  return (uint32_t)r;
+}
+
+void free_buffers(dq_mps_s* h) {
+  cudaFree(h->t);
+  cudaFree(h->dims);
+  cudaFree(h->key);
+  cudaFree(h->ctr);
+  cudaFree(h->cbits);
+  cudaFree(h->conds);
+  cudaFree(h->scratch);
+  cudaFree(h->flags);
+  cudaFree(h->svd_calls);
+  h->t = nullptr; h->dims = nullptr; h->key = nullptr; h->ctr = nullptr; h->cbits = nullptr;
+  h->conds = nullptr; h->scratch = nullptr; h->flags = nullptr; h->svd_calls = nullptr;
+  h->conds_cap = 0;
+  h->ncb = 0;
+}
+
+constexpr size_t kMaxSmem = 220 * 1024;
+// Largest bond capacity: one CTA's Jacobi SVD of a 2048 x 2048 theta takes
+// on the order of a second.
+constexpr uint32_t kMaxCapacity = 1024;
+
+int alloc_buffers(dq_mps_s* h, uint32_t batch, uint32_t cap, uint32_t ncb) {
+  free_buffers(h);
+  h->batch = batch;
+  h->cap = cap;
+  h->ncb = ncb ? ncb : 1;
+  const uint64_t site = 2ull * cap * cap;
+  h->scratch_elems = svd_work_elems(cap);
+  const size_t work_bytes = h->scratch_elems * sizeof(double2);
+  h->smem = work_bytes <= kMaxSmem;
+  DQ_CUDA_TRY(cudaMalloc((void**)&h->t, sizeof(double2) * site * h->n * batch));
+  DQ_CUDA_TRY(cudaMalloc((void**)&h->dims, sizeof(uint32_t) * (h->n + 1) * batch));
+  DQ_CUDA_TRY(cudaMalloc((void**)&h->key, sizeof(uint32_t) * 8 * batch));
+  DQ_CUDA_TRY(cudaMalloc((void**)&h->ctr, sizeof(unsigned long long) * batch));
+  DQ_CUDA_TRY(cudaMalloc((void**)&h->cbits, sizeof(int32_t) * h->ncb * batch));
+  DQ_CUDA_TRY(cudaMalloc((void**)&h->flags, sizeof(int) * 4));
+  DQ_CUDA_TRY(cudaMalloc((void**)&h->svd_calls, sizeof(unsigned long long)));
+  if (!h->smem) DQ_CUDA_TRY(cudaMalloc((void**)&h->scratch, work_bytes * batch));
+  if (h->smem) {
+    DQ_CUDA_TRY(cudaFuncSetAttribute(k_mps_2q, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)work_bytes));
+    DQ_CUDA_TRY(cudaFuncSetAttribute(k_mps_measure, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)work_bytes));
+  }
+  return DQ_OK;
+}
+
+MpsView view_of(const dq_mps_s* h) {
+  MpsView v;
+  v.t = h->t;
+  v.dims = h->dims;
+  v.key = h->key;
+  v.ctr = h->ctr;
+  v.cbits = h->cbits;
+  v.conds = h->conds;
+  v.scratch = h->scratch;
+  v.flags = h->flags;
+  v.svd_calls = h->svd_calls;
+  v.site_elems = 2ull * h->cap * h->cap;
+  v.scratch_elems = h->scratch_elems;
+  v.n = h->n;
+  v.batch = h->batch;
+  v.cap = h->cap;
+  v.ncb = h->ncb;
+  return v;
+}
+
+// Lowers the program into batch operations (run_instruction, simulator.rs:457-559).
+// Returns DQ_ERR_UNSUPPORTED with *failed set for an unconditional operation
+// the MPS simulator rejects; conditional ones become M_FAIL operations.
+int lower(uint32_t n, const dq_inst* prog, uint64_t ninst, const dq_cond* conds, uint64_t nconds,
+          uint64_t ncbits, std::vector<MpsOp>& ops, int64_t* failed) {
+  ops.clear();
+  for (uint64_t i = 0; i < ninst; ++i) {
+    const dq_inst& in = prog[i];
+    MpsOp op;
+    memset(&op, 0, sizeof(op));
+    op.cond_first = in.cond_first;
+    op.cond_count = in.cond_count;
+    op.inst = (int32_t)i;
+    op.cbit = -1;
+    const bool two = is_two_qubit_kind(in.kind);
+    if (!(two && in.nq == 2 && in.q[0] == in.q[1]))
+      DQ_TRY(validate_inst(in, n, nconds, ncbits, conds, i));
+    else if (in.q[0] < 0 || (uint32_t)in.q[0] >= n)
+      return fail(DQ_ERR_INVALID_ARG, "instruction " + std::to_string(i) + ": qubit out of range");
+    switch (in.kind) {
+      case DQ_ID: case DQ_U0: case DQ_BARRIER: case DQ_CLASSICAL: case DQ_G_NOOP: case DQ_G_OPAQUE:
+        continue;
+      case DQ_MEASURE: case DQ_RESET:
+        op.kind = in.kind == DQ_MEASURE ? M_MEAS : M_RESET;
+        op.q = (uint32_t)in.q[0];
+        op.cbit = in.kind == DQ_MEASURE ? (int32_t)in.cbit : -1;
+        ops.push_back(op);
+        continue;
+      default: break;
+    }
+    hc m[4];
+    if (matrix_1q(in.kind, in.p, m)) {
+      op.kind = M_1Q;
+      op.q = (uint32_t)in.q[0];
+      set_u(op, m, 4);
+      ops.push_back(op);
+      continue;
+    }
+    if (two) {
+      const uint32_t a = (uint32_t)in.q[0], bq = (uint32_t)in.q[1];
+      if (a == bq) continue;  // apply_2q returns early for a == b
+      static thread_local Gate g;
+      if (!matrix_nq(in, g) || g.k != 2) return fail(DQ_ERR_INTERNAL, "two-qubit kind without a 4x4 matrix");
+      hc swapm[16], gm[16];
+      {
+        dq_inst sw;
+        memset(&sw, 0, sizeof(sw));
+        sw.kind = DQ_SWAP;
+        sw.nq = 2;
+        static thread_local Gate gs;
+        matrix_nq(sw, gs);
+        for (int k = 0; k < 16; ++k) swapm[k] = gs.m[k];
+      }
+      const uint32_t lo = a < bq ? a : bq, hi = a < bq ? bq : a;
+      if (a < bq) for (int k = 0; k < 16; ++k) gm[k] = g.m[k];
+      else reverse_2q(g.m, gm);
+      MpsOp s = op;
+      s.kind = M_2Q;
+      set_u(s, swapm, 16);
+      for (uint32_t pos = hi - 1; pos > lo; --pos) {
+        s.q = pos;
+        ops.push_back(s);
+      }
+      MpsOp gop = op;
+      gop.kind = M_2Q;
+      gop.q = lo;
+      set_u(gop, gm, 16);
+      ops.push_back(gop);
+      for (uint32_t pos = lo + 1; pos < hi; ++pos) {
+        s.q = pos;
+        ops.push_back(s);
+      }
+      continue;
+    }
+    // generic names the MPS dispatcher rejects, and gates on three or more qubits
+    if (in.cond_count == 0) {
+      *failed = (int64_t)i;
+      return fail(DQ_ERR_UNSUPPORTED, "instruction " + std::to_string(i) + " is not supported by the MPS simulator");
+    }
+    op.kind = M_FAIL;
+    ops.push_back(op);
+  }
+  return DQ_OK;
+}
+
+int launch_ops(dq_mps_s* h, const std::vector<MpsOp>& ops) {
+  const MpsView v = view_of(h);
+  const size_t shm = h->smem ? h->scratch_elems * sizeof(double2) : 0;
+  const int use = h->smem ? 1 : 0;
+  for (const MpsOp& op : ops) {
+    switch (op.kind) {
+      case M_1Q: k_mps_1q<<<h->batch, kMpsThreads, 0, h->stream>>>(v, op); break;
+      case M_2Q:
+        k_mps_2q<<<h->batch, kMpsThreads, shm, h->stream>>>(v, op, h->max_bond, h->thr, use);
+        break;
+      case M_MEAS: case M_RESET:
+        k_mps_measure<<<h->batch, kMpsThreads, shm, h->stream>>>(v, op, use);
+        break;
+      case M_FAIL: k_mps_fail<<<(h->batch + 127) / 128, 128, 0, h->stream>>>(v, op); break;
+      default: return fail(DQ_ERR_INTERNAL, "bad MPS operation");
+    }
+  }
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return fail(DQ_ERR_CUDA, std::string("MPS launch: ") + cudaGetErrorString(e));
+  return DQ_OK;
+}
+
+// Runs `ops` on a batch whose replica b is seeded with seeds[b]; grows the
+// capacity and re-runs while a truncation overflows it.
+uint64_t replica_bytes(uint32_t n, uint32_t cap) {
+  const uint64_t work = svd_work_elems(cap) * sizeof(double2);
+  return (uint64_t)n * 2ull * cap * cap * sizeof(double2) + (work <= kMaxSmem ? 0 : work);
+}
+
+// Runs `ops` on a batch whose replica b is seeded with seeds[b]; grows the
+// capacity and re-runs while a truncation overflows it.  With batch > 1 and a
+// grown capacity whose buffers would exceed `budget` bytes, it returns with
+// *shrink set (and the new capacity recorded) so that the caller re-splits.
+int run_batch(dq_mps_s* h, const std::vector<MpsOp>& ops, const dq_cond* conds, uint64_t nconds,
+              const uint64_t* seeds, uint32_t batch, uint32_t ncb, int* status, int* failed_inst,
+              double* kernel_ms, uint64_t budget = 0, bool* shrink = nullptr) {
+  const uint32_t bound = bond_bound(h->n, h->max_bond);
+  if (shrink) *shrink = false;
+  for (;;) {
+    if (h->batch != batch || h->ncb != (ncb ? ncb : 1) || !h->t) DQ_TRY(alloc_buffers(h, batch, h->cap, ncb));
+    if (nconds > h->conds_cap) {
+      cudaFree(h->conds);
+      h->conds = nullptr;
+      DQ_CUDA_TRY(cudaMalloc((void**)&h->conds, sizeof(dq_cond) * nconds));
+      h->conds_cap = nconds;
+    }
+    if (nconds)
+      DQ_CUDA_TRY(cudaMemcpyAsync(h->conds, conds, sizeof(dq_cond) * nconds, cudaMemcpyHostToDevice, h->stream));
+    std::vector<uint32_t> keys((size_t)batch * 8);
+    for (uint32_t b = 0; b < batch; ++b) seed_key_from_u64(seeds[b], &keys[(size_t)b * 8]);
+    DQ_CUDA_TRY(cudaMemcpyAsync(h->key, keys.data(), sizeof(uint32_t) * keys.size(), cudaMemcpyHostToDevice,
+                                h->stream));
+    const int init_flags[4] = {F_OK, 0x7fffffff, 0, 0};
+    DQ_CUDA_TRY(cudaMemcpyAsync(h->flags, init_flags, sizeof(init_flags), cudaMemcpyHostToDevice, h->stream));
+    DQ_CUDA_TRY(cudaMemsetAsync(h->svd_calls, 0, sizeof(unsigned long long), h->stream));
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, h->stream);
+    k_mps_reset<<<batch, kMpsThreads, 0, h->stream>>>(view_of(h));
+    int rc = launch_ops(h, ops);
+    cudaEventRecord(e1, h->stream);
+    int fl[4] = {0, 0, 0, 0};
+    if (rc == DQ_OK) {
+      const cudaError_t e = cudaMemcpyAsync(fl, h->flags, sizeof(fl), cudaMemcpyDeviceToHost, h->stream);
+      const cudaError_t s = cudaStreamSynchronize(h->stream);
+      if (e != cudaSuccess || s != cudaSuccess)
+        rc = fail(DQ_ERR_CUDA, std::string("MPS run: ") + cudaGetErrorString(e != cudaSuccess ? e : s));
+    }
+    float ms = 0.f;
+    if (rc == DQ_OK) cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc != DQ_OK) return rc;
+    if (fl[0] == F_CAPACITY) {
+      uint32_t need = (uint32_t)fl[2];
+      uint32_t cap = h->cap;
+      while (cap < need) cap *= 2;
+      if (cap > bound) cap = bound;
+      if (cap <= h->cap) return fail(DQ_ERR_INTERNAL, "MPS bond dimension above its bound");
+      if (cap > kMaxCapacity)
+        return fail(DQ_ERR_INVALID_ARG, "bond dimension " + std::to_string(need) +
+                                            " exceeds the device MPS limit of " +
+                                            std::to_string(kMaxCapacity) + "; set max_bond_dimension");
+      if (shrink && batch > 1 && budget && replica_bytes(h->n, cap) * batch > budget) {
+        free_buffers(h);
+        h->cap = cap;
+        *shrink = true;
+        return DQ_OK;
+      }
+      DQ_TRY(alloc_buffers(h, batch, cap, ncb));
+      continue;
+    }
+    *status = fl[0];
+    *failed_inst = fl[1];
+    if (kernel_ms) *kernel_ms = ms;
+    return DQ_OK;
+  }
+}
+
+int check_mps(dq_mps_t h) {
+  if (!h || !h->stream) return fail(DQ_ERR_INVALID_ARG, "null or destroyed MPS handle");
+  return DQ_OK;
+}
+
+int new_handle(uint32_t n, int device, uint32_t max_bond, double thr, dq_mps_s** out) {
+  if (n == 0 || n > 64) return fail(DQ_ERR_INVALID_ARG, "MPS qubit count must be in [1, 64]");
+  if (!(thr >= 0.0) || !std::isfinite(thr))
+    return fail(DQ_ERR_INVALID_ARG, "truncation_threshold must be a finite non-negative float");
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) return fail(DQ_ERR_NO_DEVICE, "no CUDA device");
+  if (device < 0 || device >= count) return fail(DQ_ERR_INVALID_ARG, "bad device ordinal");
+  DeviceGuard g(device);
+  dq_mps_s* h = new dq_mps_s();
+  h->device = device;
+  h->n = n;
+  h->max_bond = max_bond;
+  h->thr = thr;
+  h->cap = std::min<uint32_t>(bond_bound(n, max_bond), 16u);
+  if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete h;
+    return fail(DQ_ERR_CUDA, "cudaStreamCreate failed");
+  }
+  *out = h;
+  return DQ_OK;
+}
+
+void destroy_handle(dq_mps_s* h) {
+  DeviceGuard g(h->device);
+  cudaStreamSynchronize(h->stream);
+  free_buffers(h);
+  cudaStreamDestroy(h->stream);
+  h->stream = nullptr;
+  delete h;
+}
+
+int map_status(int status, int failed, int64_t* out_failed) {
+  if (status == F_UNSUPPORTED) {
+    if (out_failed) *out_failed = failed;
+    return fail(DQ_ERR_UNSUPPORTED, "instruction " + std::to_string(failed) +
+                                        " is not supported by the MPS simulator");
+  }
+  if (status != F_OK) return fail(DQ_ERR_INTERNAL, "MPS run flagged status " + std::to_string(status));
+  return DQ_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int dq_mps_create(uint32_t n, int device, uint32_t max_bond, double truncation_threshold, dq_mps_t* out) {
+  clear_error();
+  if (!out) return fail(DQ_ERR_INVALID_ARG, "null output handle");
+  *out = nullptr;
+  dq_mps_s* h = nullptr;
+  DQ_TRY(new_handle(n, device, max_bond, truncation_threshold, &h));
+  DeviceGuard g(device);
+  int rc = alloc_buffers(h, 1, h->cap, 1);
+  if (rc == DQ_OK) {
+    const uint64_t seed = 0;
+    std::vector<MpsOp> none;
+    int st = 0, fi = 0;
+    rc = run_batch(h, none, nullptr, 0, &seed, 1, 1, &st, &fi, nullptr);
+  }
+  if (rc != DQ_OK) {
+    destroy_handle(h);
+    return rc;
+  }
+  *out = h;
+  return DQ_OK;
+}
+
+int dq_mps_destroy(dq_mps_t h) {
+  clear_error();
+  if (!h) return DQ_OK;
+  destroy_handle(h);
+  return DQ_OK;
+}
+
+int dq_mps_run(dq_mps_t h, const dq_inst* prog, uint64_t ninst, const dq_cond* conds, uint64_t nconds,
+               uint64_t seed, int32_t* cbits, uint64_t ncbits, dq_mps_stats* stats) {
+  clear_error();
+  DQ_TRY(check_mps(h));
+  if ((ninst && !prog) || (nconds && !conds) || (ncbits && !cbits))
+    return fail(DQ_ERR_INVALID_ARG, "null program, condition or cbit buffer");
+  if (ncbits > (1u << 26)) return fail(DQ_ERR_INVALID_ARG, "classical register array too large");
+  if (stats) memset(stats, 0, sizeof(*stats));
+  if (stats) stats->failed_inst = -1;
+  DeviceGuard g(h->device);
+  std::vector<MpsOp> ops;
+  int64_t failed = -1;
+  int rc = lower(h->n, prog, ninst, conds, nconds, ncbits, ops, &failed);
+  if (rc != DQ_OK) {
+    if (stats) stats->failed_inst = failed;
+    return rc;
+  }
+  int st = 0, fi = 0;
+  double ms = 0.0;
+  DQ_TRY(run_batch(h, ops, conds, nconds, &seed, 1, (uint32_t)ncbits, &st, &fi, &ms));
+  int64_t f64 = -1;
+  rc = map_status(st, fi, &f64);
+  if (stats) {
+    stats->failed_inst = f64;
+    stats->kernel_ms = ms;
+    stats->capacity = h->cap;
+    stats->replicas = 1;
+    unsigned long long calls = 0;
+    cudaMemcpy(&calls, h->svd_calls, sizeof(calls), cudaMemcpyDeviceToHost);
+    stats->svd_calls = calls;
+  }
+  if (rc != DQ_OK) return rc;
+  if (ncbits) DQ_CUDA_TRY(cudaMemcpy(cbits, h->cbits, sizeof(int32_t) * ncbits, cudaMemcpyDeviceToHost));
+  return DQ_OK;
+}
+
+int dq_mps_apply_2q(dq_mps_t h, uint32_t a, uint32_t b, const double* u) {
+  clear_error();
+  DQ_TRY(check_mps(h));
+  if (!u || a >= h->n || b >= h->n) return fail(DQ_ERR_INVALID_ARG, "bad qubit or null matrix");
+  if (a == b) return DQ_OK;
+  DeviceGuard g(h->device);
+  hc m[16], swapm[16], gm[16];
+  for (int k = 0; k < 16; ++k) m[k] = hc{u[2 * k], u[2 * k + 1]};
+  {
+    dq_inst sw;
+    memset(&sw, 0, sizeof(sw));
+    sw.kind = DQ_SWAP;
+    sw.nq = 2;
+    static thread_local Gate gs;
+    matrix_nq(sw, gs);
+    for (int k = 0; k < 16; ++k) swapm[k] = gs.m[k];
+  }
+  if (a < b) for (int k = 0; k < 16; ++k) gm[k] = m[k];
+  else reverse_2q(m, gm);
+  const uint32_t lo = a < b ? a : b, hi = a < b ? b : a;
+  std::vector<MpsOp> ops;
+  MpsOp op;
+  memset(&op, 0, sizeof(op));
+  op.kind = M_2Q;
+  op.cbit = -1;
+  op.inst = -1;
+  set_u(op, swapm, 16);
+  for (uint32_t pos = hi - 1; pos > lo; --pos) { op.q = pos; ops.push_back(op); }
+  MpsOp gop = op;
+  gop.q = lo;
+  set_u(gop, gm, 16);
+  ops.push_back(gop);
+  for (uint32_t pos = lo + 1; pos < hi; ++pos) { op.q = pos; ops.push_back(op); }
+  // Below the bond bound a step may overflow the capacity: run the steps one
+  // at a time, and on an overflow (the step wrote nothing) widen and redo it.
+  const uint32_t bound = bond_bound(h->n, h->max_bond);
+  const int init_flags[4] = {F_OK, 0x7fffffff, 0, 0};
+  if (h->cap >= bound) {
+    DQ_CUDA_TRY(cudaMemcpyAsync(h->flags, init_flags, sizeof(init_flags), cudaMemcpyHostToDevice, h->stream));
+    DQ_TRY(launch_ops(h, ops));
+    int fl[4];
+    DQ_CUDA_TRY(cudaMemcpyAsync(fl, h->flags, sizeof(fl), cudaMemcpyDeviceToHost, h->stream));
+    DQ_CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return map_status(fl[0], fl[1], nullptr);
+  }
+  for (size_t i = 0; i < ops.size();) {
+    DQ_CUDA_TRY(cudaMemcpyAsync(h->flags, init_flags, sizeof(init_flags), cudaMemcpyHostToDevice, h->stream));
+    DQ_TRY(launch_ops(h, std::vector<MpsOp>(1, ops[i])));
+    int fl[4];
+    DQ_CUDA_TRY(cudaMemcpyAsync(fl, h->flags, sizeof(fl), cudaMemcpyDeviceToHost, h->stream));
+    DQ_CUDA_TRY(cudaStreamSynchronize(h->stream));
+    if (fl[0] == F_CAPACITY) {
+      uint32_t cap = h->cap;
+      while (cap < (uint32_t)fl[2]) cap *= 2;
+      DQ_TRY(dq_mps_reserve(h, cap < bound ? cap : bound));
+      continue;
+    }
+    DQ_TRY(map_status(fl[0], fl[1], nullptr));
+    ++i;
+  }
+  return DQ_OK;
+}
+
+int dq_mps_reserve(dq_mps_t h, uint32_t capacity) {
+  clear_error();
+  DQ_TRY(check_mps(h));
+  const uint32_t bound = bond_bound(h->n, h->max_bond);
+  if (capacity == 0 || capacity > bound || capacity > kMaxCapacity)
+    return fail(DQ_ERR_INVALID_ARG, "capacity must be in [1, " +
+                                        std::to_string(std::min(bound, kMaxCapacity)) + "]");
+  if (capacity <= h->cap) return DQ_OK;
+  if (h->batch != 1) return fail(DQ_ERR_INVALID_ARG, "dq_mps_reserve takes a single-state handle");
+  DeviceGuard g(h->device);
+  // keep the current state: copy every site into the larger layout
+  const uint32_t old = h->cap, n = h->n;
+  std::vector<double2> host((size_t)n * 2 * old * old);
+  DQ_CUDA_TRY(cudaMemcpyAsync(host.data(), h->t, sizeof(double2) * host.size(), cudaMemcpyDeviceToHost, h->stream));
+  std::vector<uint32_t> dims(n + 1);
+  DQ_CUDA_TRY(cudaMemcpyAsync(dims.data(), h->dims, sizeof(uint32_t) * (n + 1), cudaMemcpyDeviceToHost, h->stream));
+  std::vector<unsigned long long> ctr(1);
+  DQ_CUDA_TRY(cudaMemcpyAsync(ctr.data(), h->ctr, sizeof(unsigned long long), cudaMemcpyDeviceToHost, h->stream));
+  std::vector<uint32_t> key(8);
+  DQ_CUDA_TRY(cudaMemcpyAsync(key.data(), h->key, sizeof(uint32_t) * 8, cudaMemcpyDeviceToHost, h->stream));
+  DQ_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  DQ_TRY(alloc_buffers(h, 1, capacity, h->ncb));
+  std::vector<double2> wide((size_t)n * 2 * capacity * capacity, make_double2(0.0, 0.0));
+  for (uint32_t k = 0; k < n; ++k)
+    for (uint32_t row = 0; row < 2 * old; ++row)
+      for (uint32_t r = 0; r < old; ++r)
+        wide[(size_t)k * 2 * capacity * capacity + (size_t)row * capacity + r] =
+            host[(size_t)k * 2 * old * old + (size_t)row * old + r];
+  DQ_CUDA_TRY(cudaMemcpyAsync(h->t, wide.data(), sizeof(double2) * wide.size(), cudaMemcpyHostToDevice, h->stream));
+  DQ_CUDA_TRY(cudaMemcpyAsync(h->dims, dims.data(), sizeof(uint32_t) * (n + 1), cudaMemcpyHostToDevice, h->stream));
+  DQ_CUDA_TRY(cudaMemcpyAsync(h->ctr, ctr.data(), sizeof(unsigned long long), cudaMemcpyHostToDevice, h->stream));
+  DQ_CUDA_TRY(cudaMemcpyAsync(h->key, key.data(), sizeof(uint32_t) * 8, cudaMemcpyHostToDevice, h->stream));
+  DQ_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return DQ_OK;
+}
+
+int dq_mps_bond_dims(dq_mps_t h, uint32_t* dims) {
+  clear_error();
+  DQ_TRY(check_mps(h));
+  if (!dims) return fail(DQ_ERR_INVALID_ARG, "null output");
+  DeviceGuard g(h->device);
+  DQ_CUDA_TRY(cudaMemcpyAsync(dims, h->dims, sizeof(uint32_t) * (h->n + 1), cudaMemcpyDeviceToHost, h->stream));
+  DQ_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return DQ_OK;
+}
+
+int dq_mps_to_state(dq_mps_t h, dq_state_t out) {
+  clear_error();
+  DQ_TRY(check_mps(h));
+  DQ_TRY(check_handle_lazy(out));
+  if (out->n != h->n) return fail(DQ_ERR_INVALID_ARG, "the state must have the MPS's qubit count");
+  if (out->device != h->device) return fail(DQ_ERR_INVALID_ARG, "the state must live on the MPS's device");
+  DeviceGuard g(h->device);
+  std::vector<uint32_t> dims(h->n + 1);
+  DQ_CUDA_TRY(cudaMemcpyAsync(dims.data(), h->dims, sizeof(uint32_t) * (h->n + 1), cudaMemcpyDeviceToHost, h->stream));
+  DQ_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  DQ_TRY(sync_stream(out));
+  out->lazy_basis = -1;
+  reset_perm(out);
+  // W_k lives in `out` when n - 1 - k is even, else in tmp (both 2^n amplitudes)
+  double2* tmp = nullptr;
+  const size_t bytes = sizeof(double2) * (size_t)out->len;
+  if (h->n > 1) DQ_CUDA_TRY(cudaMallocAsync((void**)&tmp, bytes, h->stream));
+  double2* one = nullptr;
+  DQ_CUDA_TRY(cudaMallocAsync((void**)&one, sizeof(double2), h->stream));
+  const double2 o = make_double2(1.0, 0.0);
+  cudaError_t e = cudaMemcpyAsync(one, &o, sizeof(o), cudaMemcpyHostToDevice, h->stream);
+  const double2* w = one;
+  for (uint32_t k = 0; k <= h->n; ++k)
+    if (dims[k] == 0 || dims[k] > h->cap || (k < h->n && (2ull << k) * dims[k + 1] > out->len) ||
+        ((k == 0 || k == h->n) && dims[k] != 1))
+      e = cudaErrorInvalidValue;
+  for (uint32_t k = 0; k < h->n && e == cudaSuccess; ++k) {
+    double2* wn = ((h->n - 1 - k) % 2 == 0) ? out->amp : tmp;
+    const uint64_t total = (2ull << k) * dims[k + 1];
+    const unsigned grid = grid_for(total, 256, h->device);
+    const double2* a = h->t + (uint64_t)k * h->batch * 2ull * h->cap * h->cap;
+    k_mps_expand<<<grid, 256, 0, h->stream>>>(w, wn, a, k, dims[k], dims[k + 1], h->cap);
+    e = cudaGetLastError();
+    w = wn;
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  cudaFreeAsync(one, h->stream);
+  if (tmp) cudaFreeAsync(tmp, h->stream);
+  cudaStreamSynchronize(h->stream);
+  if (e != cudaSuccess) return fail(DQ_ERR_CUDA, std::string("MPS to_statevector: ") + cudaGetErrorString(e));
+  return DQ_OK;
+}
+
+int dq_mps_run_shots(int device, uint32_t n, uint32_t max_bond, double truncation_threshold,
+                     const dq_inst* prog, uint64_t ninst, const dq_cond* conds, uint64_t nconds,
+                     uint64_t base_seed, uint64_t shot0, uint64_t shots, int32_t* cbits_out,
+                     uint64_t ncbits, uint32_t batch, dq_mps_stats* stats) {
+  clear_error();
+  if ((ninst && !prog) || (nconds && !conds) || (shots && ncbits && !cbits_out))
+    return fail(DQ_ERR_INVALID_ARG, "null program, condition or cbit buffer");
+  if (ncbits > (1u << 26)) return fail(DQ_ERR_INVALID_ARG, "classical register array too large");
+  if (stats) {
+    memset(stats, 0, sizeof(*stats));
+    stats->failed_inst = -1;
+  }
+  std::vector<MpsOp> ops;
+  int64_t failed = -1;
+  {
+    int rc = lower(n, prog, ninst, conds, nconds, ncbits, ops, &failed);
+    if (rc != DQ_OK) {
+      if (stats) stats->failed_inst = failed;
+      return rc;
+    }
+  }
+  if (shots == 0) return DQ_OK;
+  dq_mps_s* h = nullptr;
+  DQ_TRY(new_handle(n, device, max_bond, truncation_threshold, &h));
+  DeviceGuard g(device);
+  const uint32_t bmax = batch ? batch : 4096u;
+  // device memory for one batch: at most a quarter of the free memory
+  size_t free_b = 0, total_b = 0;
+  cudaMemGetInfo(&free_b, &total_b);
+  const uint64_t budget = std::max<uint64_t>(free_b / 4, 1ull << 28);
+  int rc = DQ_OK;
+  double total_ms = 0.0;
+  unsigned long long calls = 0;
+  std::vector<uint64_t> seeds;
+  for (uint64_t s0 = 0; s0 < shots && rc == DQ_OK;) {
+    const uint64_t fit = std::max<uint64_t>(budget / replica_bytes(n, h->cap), 1);
+    const uint32_t nb = (uint32_t)std::min<uint64_t>(std::min<uint64_t>(bmax, fit), shots - s0);
+    seeds.resize(nb);
+    for (uint32_t b = 0; b < nb; ++b) seeds[b] = base_seed + shot0 + s0 + b;  // wrapping
+    int st = 0, fi = 0;
+    double ms = 0.0;
+    bool shrink = false;
+    rc = run_batch(h, ops, conds, nconds, seeds.data(), nb, (uint32_t)ncbits, &st, &fi, &ms, budget,
+                   &shrink);
+    if (rc != DQ_OK) break;
+    if (shrink) continue;  // capacity grew: redo this chunk with fewer replicas
+    int64_t f64 = -1;
+    rc = map_status(st, fi, &f64);
+    if (rc != DQ_OK) {
+      if (stats) stats->failed_inst = f64;
+      break;
+    }
+    total_ms += ms;
+    unsigned long long c = 0;
+    cudaMemcpy(&c, h->svd_calls, sizeof(c), cudaMemcpyDeviceToHost);
+    calls += c;
+    if (ncbits) {
+      const cudaError_t e = cudaMemcpy(cbits_out + s0 * ncbits, h->cbits, sizeof(int32_t) * ncbits * nb,
+                                       cudaMemcpyDeviceToHost);
+      if (e != cudaSuccess) rc = fail(DQ_ERR_CUDA, std::string("MPS cbits: ") + cudaGetErrorString(e));
+    }
+    s0 += nb;
+  }
+  if (stats) {
+    stats->kernel_ms = total_ms;
+    stats->svd_calls = calls;
+    stats->capacity = h->cap;
+    stats->replicas = h->batch;
+  }
+  destroy_handle(h);
+  return rc;
+}
+
+}  // extern "C"

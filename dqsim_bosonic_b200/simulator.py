@@ -6,16 +6,19 @@ Restates ``src/simulator.rs:13-113`` (``simulate_monolithic``,
 option parsing and rejection, in the same order: the mode and options are
 checked before the circuit is touched).
 
-Only the ``state_vector`` mode is backed by this engine.  The MPS,
-stabilizer and p-block backends of the reference are not part of this
-build; selecting them parses the mode and options exactly like the
-reference, reads the circuit, and then raises ``NotImplementedError``.
+The ``state_vector`` and ``mps`` modes are backed by this engine (``mps``:
+``dqsim_bosonic_b200.mps``).  The stabilizer and p-block backends of the
+reference are not part of this build; selecting them parses the mode and
+options exactly like the reference, reads the circuit, and then raises
+``NotImplementedError``.
 Distributed circuits run here by lowering them with
 ``as_monolithic_circuit()`` and simulating the result.
 """
 from __future__ import annotations
 
 from typing import Any
+
+from .mps import MpsSimulator
 
 
 def _ascii_lower(s: str) -> str:
@@ -96,21 +99,6 @@ def _out_of_scope(backend: str) -> NotImplementedError:
         f"the {backend} backend is not part of the B200 statevector engine; "
         "use mode='state_vector' (distributed circuits: as_monolithic_circuit())"
     )
-
-
-class MpsSimulator:
-    """Placeholder for the reference's MPS backend (not built here)."""
-
-    def __init__(self, seed=None, max_bond_dimension=None, truncation_threshold=1e-12):
-        self.seed = seed
-
-    def simulate(self, circuit):
-        circuit.model_dump_json()
-        raise _out_of_scope("MPS")
-
-    def simulate_shots(self, circuit, shots=1000, profile=False):
-        circuit.model_dump_json()
-        raise _out_of_scope("MPS")
 
 
 class StabilizerSimulator:

@@ -359,6 +359,49 @@ DQ_API int dq_adjoint(dq_state_t h, const dq_inst* prog, uint64_t ninst,
 DQ_API int dq_block_merge(dq_state_t a, const uint32_t* a_qubits, uint32_t na, dq_state_t b,
                           const uint32_t* b_qubits, uint32_t nb, dq_state_t out);
 
+/* ---- matrix-product-state backend -----------------------------------------
+ * MpsSimulator (src/monolithic/mps/simulator.rs:293-455): one MPS per handle
+ * (dq_mps_create, max_bond = 0 for max_bond_dimension=None) or a batch of
+ * independent shots (dq_mps_run_shots).  dq_mps_run replaces the instruction
+ * loop of MpsSimulator::simulate (:316-344): the state restarts at |0...0>,
+ * the outcomes draw from ChaCha8Rng::seed_from_u64(seed), cbits as in dq_run.
+ * Two-qubit gates are chains of fused adjacent steps (contract, SVD, keep the
+ * singular values above truncation_threshold, at least 1, at most max_bond,
+ * renormalise: apply_adjacent_2q :137-236).  dq_mps_to_state writes
+ * to_statevector (:238-257) into a statevector handle of n qubits.
+ * dq_mps_run_shots replaces the shot loop of MpsSimulator::simulate_shots
+ * (:368-385): shot i is seeded base_seed + shot0 + i (wrapping), its cbits
+ * go to row i of cbits_out (shots x ncbits, -1 = never written); batch = 0
+ * picks the replicas per launch.  DQ_ERR_UNSUPPORTED (stats->failed_inst =
+ * the instruction) for gates on three or more qubits and unknown generic
+ * names, raised when such an instruction executes (:540-557). */
+typedef struct dq_mps_s* dq_mps_t;
+typedef struct dq_mps_stats {
+  uint64_t svd_calls;     /* two-qubit SVD steps executed, over all replicas */
+  double kernel_ms;       /* device time of the program's launches */
+  int64_t failed_inst;    /* DQ_ERR_UNSUPPORTED: index of the instruction */
+  uint32_t capacity;      /* bond-dimension capacity the run ended with */
+  uint32_t replicas;      /* replicas per launch */
+} dq_mps_stats;
+DQ_API int dq_mps_create(uint32_t n, int device, uint32_t max_bond, double truncation_threshold,
+                         dq_mps_t* out);
+DQ_API int dq_mps_destroy(dq_mps_t h);
+DQ_API int dq_mps_run(dq_mps_t h, const dq_inst* prog, uint64_t ninst, const dq_cond* conds,
+                      uint64_t nconds, uint64_t seed, int32_t* cbits, uint64_t ncbits,
+                      dq_mps_stats* stats);
+/* Mps::apply_2q (:115-135) on the current state: u = 4x4 row-major complex
+ * (interleaved re/im, 32 doubles), a = most significant qubit of the row. */
+DQ_API int dq_mps_apply_2q(dq_mps_t h, uint32_t a, uint32_t b, const double* u);
+/* Widen the bond capacity of a single-state handle, keeping its state. */
+DQ_API int dq_mps_reserve(dq_mps_t h, uint32_t capacity);
+DQ_API int dq_mps_bond_dims(dq_mps_t h, uint32_t* dims);   /* n + 1 entries */
+DQ_API int dq_mps_to_state(dq_mps_t h, dq_state_t out);
+DQ_API int dq_mps_run_shots(int device, uint32_t n, uint32_t max_bond, double truncation_threshold,
+                            const dq_inst* prog, uint64_t ninst, const dq_cond* conds,
+                            uint64_t nconds, uint64_t base_seed, uint64_t shot0, uint64_t shots,
+                            int32_t* cbits_out, uint64_t ncbits, uint32_t batch,
+                            dq_mps_stats* stats);
+
 /* ---- planner inspection (host only, no GPU needed) -------------------------
  * Runs the fused-sweep planner of dq_run (DQ_EXEC_FUSED) on a unitary
  * program of n qubits and writes the encoded sweep programs instead of

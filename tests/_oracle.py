@@ -254,3 +254,70 @@ def block_merge(a: np.ndarray, qa, b: np.ndarray, qb) -> tuple[np.ndarray, list[
                              _p(qb) if qb.size else None, qb.size, _p(out))
     assert n == len(u)
     return out, u
+
+
+def _load_mps_oracle():
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("oracle_mps", ORACLE_DIR / "mps.py")
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+_mps_mod = None
+
+
+def mps_module():
+    global _mps_mod
+    if _mps_mod is None:
+        _mps_mod = _load_mps_oracle()
+    return _mps_mod
+
+
+class _Draws:
+    """Sequential gen::<f64>() draws of ChaCha8Rng::seed_from_u64(seed)."""
+
+    def __init__(self, seed: int):
+        self.seed = seed
+        self.pos = 0
+        self.buf = np.zeros(0)
+        self.base = 0
+
+    def __call__(self) -> float:
+        if self.pos - self.base >= self.buf.size:
+            self.base = self.pos
+            self.buf = rng_f64(self.seed, self.pos, 256)
+        v = float(self.buf[self.pos - self.base])
+        self.pos += 1
+        return v
+
+
+def _mps_classify(rec):
+    from dqsim_bosonic_b200._native import KIND
+    kind = int(rec["kind"])
+    if kind in (KIND["id"], KIND["u0"], KIND["barrier"], KIND["classical"], KIND["g_noop"],
+                KIND["g_opaque"]):
+        return "noop", None
+    if kind == KIND["measure"]:
+        return "measure", None
+    if kind == KIND["reset"]:
+        return "reset", None
+    m = np.zeros(4, dtype=np.complex128)
+    p = np.ascontiguousarray(rec["p"], dtype=np.float64)
+    if lib().or_matrix_1q(kind, _p(p), _p(m)):
+        return "1q", m.reshape(2, 2)
+    big = np.zeros(32 * 32, dtype=np.complex128)
+    qs = np.zeros(8, dtype=np.uint32)
+    r = np.array([rec])
+    k = lib().or_matrix_nq(_p(r), _p(big), _p(qs))
+    if k == 2:
+        return "2q", big[:16].reshape(4, 4).copy()
+    return "fail", None
+
+
+def mps_run(prog, seed: int, max_bond=None, threshold: float = 1e-12):
+    """The MPS oracle over an encoded program: (statevector, cbits, bond dims, svd calls)."""
+    mod = mps_module()
+    mps, cbits = mod.run(prog.insts, prog.conds, prog.num_qubits, prog.cbit_space, _Draws(seed),
+                         _mps_classify, max_bond, threshold)
+    return mps.to_statevector(), cbits, mps.bond_dims(), mps.svd_calls
