@@ -430,6 +430,7 @@ def main():
                                                   and not args.no_cpu_baseline, d=d)
         line["adjoint"] = adjoint_section(dev)
         line["pblock_merge"] = pblock_merge_section(dev, args.merge_qubits)
+        line["mps"] = mps_section(dev, cpu=d.rank == 0 and d.world == 1 and not args.no_cpu_baseline)
         if args.adam_steps > 0:
             line["adjoint_batch"] = adjoint_batch_section(dev, args.adam_steps)
     if args.adjoint31:
@@ -694,6 +695,81 @@ def pblock_merge_section(dev: int, n: int = 30) -> dict:
             "ms": t, "bytes": nbytes,
             "roofline": {"kernel": "k_block_merge", "bound": "hbm", "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": achieved / peak, "peak_source": src}}
+
+
+def mps_section(dev: int, cpu: bool) -> dict:
+    """The MPS backend (MpsSimulator): (a) the 16-qubit trajectory workload
+    (12 layers of u3 + cx brickwork, measure / conditional x / reset every
+    third layer) as 4096 MPS shots with max_bond_dimension 16, one batch of
+    independent MPS per launch; (b) one `simulate` of the 20-qubit u3 + cx
+    brickwork (20 layers) with max_bond_dimension 64 (single MPS: the SVD
+    steps run one after another).  CPU baseline: the numpy MPS oracle
+    (oracle/mps.py, LAPACK SVD) on a sample, with its cbits / statevector
+    compared to the device's."""
+    from dqsim_bosonic_b200.circuit import decode_circuit_json, encode
+    from dqsim_bosonic_b200.mps import MpsHandle, run_mps_shots
+
+    out = {}
+    prog = encode(decode_circuit_json(_circuits.trajectory_circuit(16, 12, seed=7).model_dump_json()))
+    shots, chi = 4096, 16
+    run_mps_shots(prog, 7, 256, dev, chi, 1e-12)
+    walls, sts = [], []
+    for _ in range(3):
+        t0 = time.perf_counter()
+        bits, st = run_mps_shots(prog, 7, shots, dev, chi, 1e-12)
+        walls.append(time.perf_counter() - t0)
+        sts.append(st)
+    i = int(np.argsort(walls)[1])
+    wall, st = walls[i], sts[i]
+    traj = {"workload": "MPS shots: 16-qubit trajectory circuit, 12 layers, measure/cond/reset, "
+                        f"{shots} shots, max_bond_dimension {chi}",
+            "shots_per_s": shots / wall, "wall_ms": wall * 1e3, "kernel_ms": st.kernel_ms,
+            "svd_steps": int(st.svd_calls), "svd_steps_per_s": st.svd_calls / (st.kernel_ms * 1e-3),
+            "replicas_per_launch": int(st.replicas), "bond_capacity": int(st.capacity)}
+    if cpu:
+        import _oracle as orc
+
+        m = 16
+        t0 = time.perf_counter()
+        bad = 0
+        for k in range(m):
+            _, cb, _, _ = orc.mps_run(prog, 7 + k, max_bond=chi)
+            bad += int(cb[:prog.cbit_space].tolist() != bits[k].tolist())
+        cpu_s = time.perf_counter() - t0
+        traj["cpu_baseline"] = {"shots_per_s": m / cpu_s, "cores": 1, "kind": "port",
+                                "sample": f"{m} shots on the numpy MPS oracle (LAPACK SVD)"}
+        traj["parity"] = {"shots_checked": m, "cbit_mismatches": bad}
+    out["trajectories"] = traj
+
+    n, layers, chi1 = 20, 20, 64
+    prog1 = encode(decode_circuit_json(_circuits.brickwork_u3_cx(n, layers, seed=1234).model_dump_json()))
+    h = MpsHandle(n, dev, chi1, 1e-12)
+    h.run(prog1, 1)
+    ts = []
+    for _ in range(3):
+        t0 = time.perf_counter()
+        _, st1 = h.run(prog1, 1)
+        ts.append(time.perf_counter() - t0)
+    dims = h.bond_dims()
+    sv = h.to_state().download() if cpu else None
+    h.release()
+    single = {"workload": f"MpsSimulator.simulate: {n}-qubit u3+cx brickwork, {layers} layers, "
+                          f"max_bond_dimension {chi1}",
+              "wall_ms": float(np.median(ts)) * 1e3, "kernel_ms": st1.kernel_ms,
+              "svd_steps": int(st1.svd_calls), "us_per_svd_step": st1.kernel_ms * 1e3 / max(st1.svd_calls, 1),
+              "max_bond": int(max(dims))}
+    if cpu:
+        import _oracle as orc
+
+        t0 = time.perf_counter()
+        ref, _, rdims, _ = orc.mps_run(prog1, 1, max_bond=chi1)
+        cpu_s = time.perf_counter() - t0
+        single["cpu_baseline"] = {"wall_ms": cpu_s * 1e3, "cores": 1, "kind": "port",
+                                  "sample": "the same simulate on the numpy MPS oracle (LAPACK SVD)"}
+        single["parity"] = {"max_abs_amplitude_diff": float(np.max(np.abs(sv - ref))),
+                            "bond_dims_equal": rdims == dims}
+    out["simulate"] = single
+    return out
 
 
 def adjoint31_section(dev: int, fd_params: int = 32) -> dict:

@@ -138,22 +138,30 @@ __device__ __forceinline__ double warp_sum(double x) {
   return x;
 }
 
-// Work-area size (double2 elements) of the fused step at capacity cap:
-// G (rows x cols) + J (cols x cols) + sigma (cols doubles) + perm (cols u32).
+// Work area (double2 elements) of the fused step at capacity cap, in shared
+// memory when it fits: G (rows x cols <= 4 cap^2) + sigma (cols doubles) +
+// perm (cols u32).  The measurement kernel uses it for three cap x cap
+// transfer matrices.
 __host__ __device__ inline uint64_t svd_work_elems(uint32_t cap) {
   const uint64_t c = 2ull * cap;
-  return c * c + c * c + c + (c + 1) / 2;
+  return c * c + c + (c + 1) / 2;
 }
+// theta copy (row-major 2L x 2R <= 4 cap^2), always in global memory
+__host__ __device__ inline uint64_t theta_elems(uint32_t cap) { return 4ull * cap * cap; }
 
 // Fused adjacent two-qubit step on bond (q, q+1) of every replica.
 //   theta[(l*2+o0)][(o1*R+r)] = sum_in u[o][in] sum_k A[l][in0][k] B[k][in1][r]
 // (apply_adjacent_2q, simulator.rs:148-171; same accumulation order).  The
 // SVD is one-sided Jacobi on G = theta (2R <= 2L) or G = theta^H (2R > 2L):
-// column pairs (p, q) of a round-robin tournament are rotated until every
-// pair is orthogonal to within rows * eps, J accumulating the rotations, so
-// G = W J^H with orthogonal columns W_j = sigma_j u_j.
-__global__ void __launch_bounds__(kMpsThreads) k_mps_2q(MpsView v, MpsOp op, uint32_t max_keep,
-                                                        double thr, int use_smem) {
+// column pairs of a round-robin tournament (each round cols/2 disjoint pairs,
+// one warp per pair) are rotated until every pair is orthogonal to within
+// rows * eps, leaving G = W V^H with orthogonal columns W_j = sigma_j u_j.
+// V is never formed: with U = W / sigma the split tensors are
+//   2R <= 2L:  left = U,                       right = scale * U^H theta
+//   2R >  2L:  left = theta W / sigma^2,       right = scale * W^H
+// read from a copy of theta (global memory, L2-resident).
+__global__ void __launch_bounds__(1024) k_mps_2q(MpsView v, MpsOp op, uint32_t max_keep, double thr,
+                                                 int use_smem) {
   extern __shared__ double2 smem[];
   __shared__ int s_rot;
   __shared__ uint32_t s_keep;
@@ -165,16 +173,17 @@ __global__ void __launch_bounds__(kMpsThreads) k_mps_2q(MpsView v, MpsOp op, uin
   const uint32_t L = dm[q], M = dm[q + 1], R = dm[q + 2];
   const bool tr = R > L;
   const uint32_t rows = tr ? 2 * R : 2 * L, cols = tr ? 2 * L : 2 * R;
-  double2* G = use_smem ? smem : v.scratch + (uint64_t)b * v.scratch_elems;
-  double2* J = G + (uint64_t)rows * cols;
-  double* sig = reinterpret_cast<double*>(J + (uint64_t)cols * cols);
+  const uint32_t tw = 2 * R;   // theta row length
+  double2* TH = v.scratch + (uint64_t)b * v.scratch_elems;
+  double2* G = use_smem ? smem : TH + theta_elems(cap);
+  double* sig = reinterpret_cast<double*>(G + (uint64_t)rows * cols);
   uint32_t* perm = reinterpret_cast<uint32_t*>(sig + cols);
   double2* A = site(v, q, b);
   double2* B = site(v, q + 1, b);
   const double2 zero = make_double2(0.0, 0.0);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
 
-  // ---- theta -> G (column-major) ---------------------------------------------
+  // ---- theta -> TH (row-major) and G (column-major) ---------------------------
   for (uint32_t t = tid; t < L * R; t += blockDim.x) {
     const uint32_t l = t / R, r = t - (t / R) * R;
     double2 in[4];
@@ -192,12 +201,11 @@ __global__ void __launch_bounds__(kMpsThreads) k_mps_2q(MpsView v, MpsOp op, uin
         double2 acc = zero;
         for (int i = 0; i < 4; ++i) acc = cadd_x(acc, cmul_x(op.u[o * 4 + i], in[i]));
         const uint32_t row = l * 2 + o0, col = o1 * R + r;
+        TH[(uint64_t)row * tw + col] = acc;
         if (!tr) G[(uint64_t)col * rows + row] = acc;
         else G[(uint64_t)row * rows + col] = make_double2(acc.x, -acc.y);
       }
   }
-  for (uint32_t t = tid; t < cols * cols; t += blockDim.x)
-    J[t] = (t / cols == t % cols) ? make_double2(1.0, 0.0) : zero;
   if (tid == 0) s_rot = 0;
   __syncthreads();
 
@@ -241,13 +249,6 @@ __global__ void __launch_bounds__(kMpsThreads) k_mps_2q(MpsView v, MpsOp op, uin
             const double2 x = gp[i], y = gq[i];
             gp[i] = make_double2(c * x.x - s * (ex * y.x + ey * y.y), c * x.y - s * (ex * y.y - ey * y.x));
             gq[i] = make_double2(s * (ex * x.x - ey * x.y) + c * y.x, s * (ex * x.y + ey * x.x) + c * y.y);
-          }
-          double2* jp = J + (uint64_t)p * cols;
-          double2* jq = J + (uint64_t)qq * cols;
-          for (uint32_t i = lane; i < cols; i += 32) {
-            const double2 x = jp[i], y = jq[i];
-            jp[i] = make_double2(c * x.x - s * (ex * y.x + ey * y.y), c * x.y - s * (ex * y.y - ey * y.x));
-            jq[i] = make_double2(s * (ex * x.x - ey * x.y) + c * y.x, s * (ex * x.y + ey * x.x) + c * y.y);
           }
         }
       }
@@ -303,17 +304,29 @@ __global__ void __launch_bounds__(kMpsThreads) k_mps_2q(MpsView v, MpsOp op, uin
   if (keep > cap) return;
   const double scale = s_scale;
 
-  // ---- split: A' = U[:, :keep], B' = (sigma * scale) V^H[:keep, :] -------------
+  // ---- split ----------------------------------------------------------------------
   for (uint32_t t = tid; t < L * 2 * keep; t += blockDim.x) {
     const uint32_t row = t / keep, k = t - (t / keep) * keep;   // row = l*2 + s
     const uint32_t j = perm[k];
-    double2 val;
-    if (tr) {
-      val = J[(uint64_t)j * cols + row];
-    } else {
-      const double sj = sig[j];
-      const double2 g = G[(uint64_t)j * rows + row];
-      val = sj > 0.0 ? make_double2(g.x / sj, g.y / sj) : zero;
+    const double sj = sig[j];
+    double2 val = zero;
+    if (sj > 0.0) {
+      if (!tr) {
+        const double2 g = G[(uint64_t)j * rows + row];
+        val = make_double2(g.x / sj, g.y / sj);
+      } else {
+        // (theta W_j)[row] / sigma_j^2
+        const double2* th = TH + (uint64_t)row * tw;
+        const double2* w = G + (uint64_t)j * rows;
+        double re = 0.0, im = 0.0;
+        for (uint32_t c2 = 0; c2 < tw; ++c2) {
+          const double2 a = th[c2], x = w[c2];
+          re += a.x * x.x - a.y * x.y;
+          im += a.x * x.y + a.y * x.x;
+        }
+        const double s2 = sj * sj;
+        val = make_double2(re / s2, im / s2);
+      }
     }
     A[(uint64_t)row * cap + k] = val;
   }
@@ -322,15 +335,25 @@ __global__ void __launch_bounds__(kMpsThreads) k_mps_2q(MpsView v, MpsOp op, uin
     const uint32_t s = col / R, r = col - (col / R) * R;
     const uint32_t j = perm[k];
     const double sj = sig[j];
-    double2 vh;
-    if (tr) {
-      const double2 g = G[(uint64_t)j * rows + col];
-      vh = sj > 0.0 ? make_double2(g.x / sj, -g.y / sj) : zero;
-    } else {
-      const double2 x = J[(uint64_t)j * cols + col];
-      vh = make_double2(x.x, -x.y);
+    double2 val = zero;
+    if (sj > 0.0) {
+      if (tr) {
+        const double2 g = G[(uint64_t)j * rows + col];
+        val = make_double2(scale * g.x, -scale * g.y);
+      } else {
+        // scale * (U_j^H theta)[col], U_j = W_j / sigma_j
+        const double2* w = G + (uint64_t)j * rows;
+        double re = 0.0, im = 0.0;
+        for (uint32_t r2 = 0; r2 < rows; ++r2) {
+          const double2 x = w[r2], a = TH[(uint64_t)r2 * tw + col];
+          re += x.x * a.x + x.y * a.y;
+          im += x.x * a.y - x.y * a.x;
+        }
+        const double f = scale / sj;
+        val = make_double2(f * re, f * im);
+      }
     }
-    B[(uint64_t)(k * 2 + s) * cap + r] = cmul_x(make_double2(sj * scale, 0.0), vh);
+    B[(uint64_t)(k * 2 + s) * cap + r] = val;
   }
   if (tid == 0) dm[q + 1] = keep;
 }
@@ -346,7 +369,7 @@ __global__ void __launch_bounds__(kMpsThreads) k_mps_measure(MpsView v, MpsOp op
   if (!cond_ok(v, op, b)) return;
   const uint32_t* dm = v.dims + (uint64_t)b * (v.n + 1);
   const uint32_t cap = v.cap;
-  double2* E = use_smem ? smem : v.scratch + (uint64_t)b * v.scratch_elems;
+  double2* E = use_smem ? smem : v.scratch + (uint64_t)b * v.scratch_elems + theta_elems(v.cap);
   double2* F = E + (uint64_t)cap * cap;
   double2* E2 = F + (uint64_t)cap * cap;
   const double2 zero = make_double2(0.0, 0.0);
@@ -498,6 +521,7 @@ struct dq_mps_s {
   unsigned long long* svd_calls = nullptr;
   bool smem = true;
   uint64_t scratch_elems = 0;
+  size_t work_bytes = 0;
 };
 
 namespace {
@@ -537,9 +561,10 @@ int alloc_buffers(dq_mps_s* h, uint32_t batch, uint32_t cap, uint32_t ncb) {
   h->cap = cap;
   h->ncb = ncb ? ncb : 1;
   const uint64_t site = 2ull * cap * cap;
-  h->scratch_elems = svd_work_elems(cap);
-  const size_t work_bytes = h->scratch_elems * sizeof(double2);
+  const size_t work_bytes = svd_work_elems(cap) * sizeof(double2);
   h->smem = work_bytes <= kMaxSmem;
+  h->work_bytes = work_bytes;
+  h->scratch_elems = theta_elems(cap) + (h->smem ? 0 : svd_work_elems(cap));
   DQ_CUDA_TRY(cudaMalloc((void**)&h->t, sizeof(double2) * site * h->n * batch));
   DQ_CUDA_TRY(cudaMalloc((void**)&h->dims, sizeof(uint32_t) * (h->n + 1) * batch));
   DQ_CUDA_TRY(cudaMalloc((void**)&h->key, sizeof(uint32_t) * 8 * batch));
@@ -547,7 +572,7 @@ int alloc_buffers(dq_mps_s* h, uint32_t batch, uint32_t cap, uint32_t ncb) {
   DQ_CUDA_TRY(cudaMalloc((void**)&h->cbits, sizeof(int32_t) * h->ncb * batch));
   DQ_CUDA_TRY(cudaMalloc((void**)&h->flags, sizeof(int) * 4));
   DQ_CUDA_TRY(cudaMalloc((void**)&h->svd_calls, sizeof(unsigned long long)));
-  if (!h->smem) DQ_CUDA_TRY(cudaMalloc((void**)&h->scratch, work_bytes * batch));
+  DQ_CUDA_TRY(cudaMalloc((void**)&h->scratch, sizeof(double2) * h->scratch_elems * batch));
   if (h->smem) {
     DQ_CUDA_TRY(cudaFuncSetAttribute(k_mps_2q, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)work_bytes));
@@ -664,13 +689,16 @@ int lower(uint32_t n, const dq_inst* prog, uint64_t ninst, const dq_cond* conds,
 
 int launch_ops(dq_mps_s* h, const std::vector<MpsOp>& ops) {
   const MpsView v = view_of(h);
-  const size_t shm = h->smem ? h->scratch_elems * sizeof(double2) : 0;
+  const size_t shm = h->smem ? h->work_bytes : 0;
   const int use = h->smem ? 1 : 0;
+  // one SVD per CTA: wide CTAs when few replicas share the GPU (latency), 256
+  // threads and several CTAs per SM otherwise (throughput)
+  const int t2q = h->batch <= 2 * 148 ? 1024 : 256;
   for (const MpsOp& op : ops) {
     switch (op.kind) {
       case M_1Q: k_mps_1q<<<h->batch, kMpsThreads, 0, h->stream>>>(v, op); break;
       case M_2Q:
-        k_mps_2q<<<h->batch, kMpsThreads, shm, h->stream>>>(v, op, h->max_bond, h->thr, use);
+        k_mps_2q<<<h->batch, t2q, shm, h->stream>>>(v, op, h->max_bond, h->thr, use);
         break;
       case M_MEAS: case M_RESET:
         k_mps_measure<<<h->batch, kMpsThreads, shm, h->stream>>>(v, op, use);
@@ -688,7 +716,8 @@ int launch_ops(dq_mps_s* h, const std::vector<MpsOp>& ops) {
 // capacity and re-runs while a truncation overflows it.
 uint64_t replica_bytes(uint32_t n, uint32_t cap) {
   const uint64_t work = svd_work_elems(cap) * sizeof(double2);
-  return (uint64_t)n * 2ull * cap * cap * sizeof(double2) + (work <= kMaxSmem ? 0 : work);
+  return (uint64_t)n * 2ull * cap * cap * sizeof(double2) + theta_elems(cap) * sizeof(double2) +
+         (work <= kMaxSmem ? 0 : work);
 }
 
 // Runs `ops` on a batch whose replica b is seeded with seeds[b]; grows the
