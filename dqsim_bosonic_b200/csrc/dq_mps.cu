@@ -358,6 +358,210 @@ __global__ void __launch_bounds__(1024) k_mps_2q(MpsView v, MpsOp op, uint32_t m
   if (tid == 0) dm[q + 1] = keep;
 }
 
+// Warp-per-replica form of k_mps_2q for capacity <= 16 (theta at most
+// 32 x 32): kWarpsPer2q replicas per CTA, each warp with its own shared-memory
+// G, no block barriers.  The cols/2 pairs of a round are spread over groups
+// of lpp lanes (lpp = the largest power of two <= 32 / pairs); a group splits
+// the rows of its pair and reduces the four dot products with xor shuffles.
+constexpr int kWarpsPer2q = 4;
+constexpr uint32_t kWarpCap = 16;
+
+__host__ __device__ inline uint64_t warp_work_bytes(uint32_t cap) {
+  const uint64_t c = 2ull * cap;
+  const uint64_t b = c * (c + 1) * sizeof(double2) + c * sizeof(double) + c * sizeof(uint32_t);
+  return (b + 15) & ~15ull;  // keeps every warp's G 16-byte aligned
+}
+
+__global__ void __launch_bounds__(kWarpsPer2q * 32) k_mps_2q_warp(MpsView v, MpsOp op, uint32_t max_keep,
+                                                                  double thr) {
+  extern __shared__ double2 smem[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint32_t b = blockIdx.x * kWarpsPer2q + warp;
+  if (b >= v.batch || !cond_ok(v, op, b)) return;
+  const unsigned full = 0xffffffffu;
+  const uint32_t cap = v.cap;
+  uint32_t* dm = v.dims + (uint64_t)b * (v.n + 1);
+  const uint32_t q = op.q;
+  const uint32_t L = dm[q], M = dm[q + 1], R = dm[q + 2];
+  const bool tr = R > L;
+  const uint32_t rows = tr ? 2 * R : 2 * L, cols = tr ? 2 * L : 2 * R;
+  const uint32_t ld = rows + 1;  // padded column stride
+  const uint32_t tw = 2 * R;
+  double2* TH = v.scratch + (uint64_t)b * v.scratch_elems;
+  double2* G = reinterpret_cast<double2*>(reinterpret_cast<char*>(smem) + warp * warp_work_bytes(cap));
+  double* sig = reinterpret_cast<double*>(G + 2ull * cap * (2ull * cap + 1));
+  uint32_t* perm = reinterpret_cast<uint32_t*>(sig + 2 * cap);
+  double2* A = site(v, q, b);
+  double2* B = site(v, q + 1, b);
+  const double2 zero = make_double2(0.0, 0.0);
+
+  for (uint32_t t = lane; t < L * R; t += 32) {
+    const uint32_t l = t / R, r = t - (t / R) * R;
+    double2 in[4];
+    for (int i0 = 0; i0 < 2; ++i0)
+      for (int i1 = 0; i1 < 2; ++i1) {
+        double2 acc = zero;
+        const double2* ar = A + (uint64_t)(l * 2 + i0) * cap;
+        for (uint32_t k = 0; k < M; ++k)
+          acc = cadd_x(acc, cmul_x(ar[k], B[(uint64_t)(k * 2 + i1) * cap + r]));
+        in[i0 * 2 + i1] = acc;
+      }
+    for (int o0 = 0; o0 < 2; ++o0)
+      for (int o1 = 0; o1 < 2; ++o1) {
+        const int o = o0 * 2 + o1;
+        double2 acc = zero;
+        for (int i = 0; i < 4; ++i) acc = cadd_x(acc, cmul_x(op.u[o * 4 + i], in[i]));
+        const uint32_t row = l * 2 + o0, col = o1 * R + r;
+        TH[(uint64_t)row * tw + col] = acc;
+        if (!tr) G[col * ld + row] = acc;
+        else G[row * ld + col] = make_double2(acc.x, -acc.y);
+      }
+  }
+  __syncwarp();
+
+  const double tol = (double)rows * DBL_EPSILON;
+  const uint32_t np = cols / 2;
+  uint32_t lpp = 1;
+  while (lpp * 2 * np <= 32) lpp *= 2;
+  const uint32_t pi = (uint32_t)lane / lpp, h = (uint32_t)lane % lpp;
+  const bool active = pi < np;
+  for (int sweep = 0; sweep < kMaxSweeps; ++sweep) {
+    bool rot = false;
+    for (uint32_t rd = 0; rd + 1 < cols; ++rd) {
+      uint32_t p = 0, qq = 0;
+      if (active) {
+        if (pi == 0) {
+          p = rd;
+          qq = cols - 1;
+        } else {
+          p = (rd + pi) % (cols - 1);
+          qq = (rd + (cols - 1) - pi) % (cols - 1);
+        }
+      }
+      double2* gp = G + p * ld;
+      double2* gq = G + qq * ld;
+      double al = 0.0, be = 0.0, gr = 0.0, gi = 0.0;
+      if (active)
+        for (uint32_t i = h; i < rows; i += lpp) {
+          const double2 x = gp[i], y = gq[i];
+          al += x.x * x.x + x.y * x.y;
+          be += y.x * y.x + y.y * y.y;
+          gr += x.x * y.x + x.y * y.y;
+          gi += x.x * y.y - x.y * y.x;
+        }
+      for (uint32_t o = lpp / 2; o >= 1; o >>= 1) {
+        al += __shfl_xor_sync(full, al, o);
+        be += __shfl_xor_sync(full, be, o);
+        gr += __shfl_xor_sync(full, gr, o);
+        gi += __shfl_xor_sync(full, gi, o);
+      }
+      const double ag = sqrt(gr * gr + gi * gi);
+      if (active && ag > 0.0 && ag > tol * sqrt(al) * sqrt(be)) {
+        rot = true;
+        const double zeta = (be - al) / (2.0 * ag);
+        const double t = (zeta >= 0.0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+        const double c = 1.0 / sqrt(1.0 + t * t), s = c * t;
+        const double ex = gr / ag, ey = gi / ag;
+        for (uint32_t i = h; i < rows; i += lpp) {
+          const double2 x = gp[i], y = gq[i];
+          gp[i] = make_double2(c * x.x - s * (ex * y.x + ey * y.y), c * x.y - s * (ex * y.y - ey * y.x));
+          gq[i] = make_double2(s * (ex * x.x - ey * x.y) + c * y.x, s * (ex * x.y + ey * x.x) + c * y.y);
+        }
+      }
+      __syncwarp();
+    }
+    if (!__any_sync(full, rot)) break;
+  }
+
+  for (uint32_t j = lane; j < cols; j += 32) {
+    const double2* g = G + j * ld;
+    double sq = 0.0;
+    for (uint32_t i = 0; i < rows; ++i) sq += g[i].x * g[i].x + g[i].y * g[i].y;
+    sig[j] = sqrt(sq);
+  }
+  __syncwarp();
+  for (uint32_t j = lane; j < cols; j += 32) {
+    uint32_t rank = 0;
+    const double sj = sig[j];
+    for (uint32_t i = 0; i < cols; ++i) rank += (sig[i] > sj || (sig[i] == sj && i < j)) ? 1u : 0u;
+    perm[rank] = j;
+  }
+  __syncwarp();
+  uint32_t keep = 0;
+  double scale = 1.0;
+  if (lane == 0) {
+    for (uint32_t k = 0; k < cols; ++k) keep += sig[perm[k]] > thr ? 1u : 0u;
+    keep = keep > 1u ? keep : 1u;
+    if (max_keep) keep = keep < max_keep ? keep : max_keep;
+    double kept = 0.0, total = 0.0, disc = 0.0;
+    for (uint32_t k = 0; k < keep; ++k) kept += sig[perm[k]] * sig[perm[k]];
+    for (uint32_t k = 0; k < cols; ++k) total += sig[perm[k]] * sig[perm[k]];
+    for (uint32_t k = keep; k < cols; ++k) disc += sig[perm[k]] * sig[perm[k]];
+    kept = fmax(sqrt(kept), 1e-15);
+    total = sqrt(total);
+    scale = disc > 0.0 ? total / kept : 1.0;
+    if (keep > cap) {
+      atomicMax(&v.flags[2], (int)keep);
+      atomicMax(&v.flags[0], F_CAPACITY);
+    } else {
+      atomicAdd(v.svd_calls, 1ull);
+    }
+  }
+  keep = __shfl_sync(full, keep, 0);
+  scale = __shfl_sync(full, scale, 0);
+  if (keep > cap) return;
+
+  for (uint32_t t = lane; t < L * 2 * keep; t += 32) {
+    const uint32_t row = t / keep, k = t - (t / keep) * keep;
+    const uint32_t j = perm[k];
+    const double sj = sig[j];
+    double2 val = zero;
+    if (sj > 0.0) {
+      if (!tr) {
+        const double2 g = G[j * ld + row];
+        val = make_double2(g.x / sj, g.y / sj);
+      } else {
+        const double2* th = TH + (uint64_t)row * tw;
+        const double2* w = G + j * ld;
+        double re = 0.0, im = 0.0;
+        for (uint32_t c2 = 0; c2 < tw; ++c2) {
+          const double2 a = th[c2], x = w[c2];
+          re += a.x * x.x - a.y * x.y;
+          im += a.x * x.y + a.y * x.x;
+        }
+        const double s2 = sj * sj;
+        val = make_double2(re / s2, im / s2);
+      }
+    }
+    A[(uint64_t)row * cap + k] = val;
+  }
+  for (uint32_t t = lane; t < keep * 2 * R; t += 32) {
+    const uint32_t k = t / (2 * R), col = t - (t / (2 * R)) * (2 * R);
+    const uint32_t s = col / R, r = col - (col / R) * R;
+    const uint32_t j = perm[k];
+    const double sj = sig[j];
+    double2 val = zero;
+    if (sj > 0.0) {
+      if (tr) {
+        const double2 g = G[j * ld + col];
+        val = make_double2(scale * g.x, -scale * g.y);
+      } else {
+        const double2* w = G + j * ld;
+        double re = 0.0, im = 0.0;
+        for (uint32_t r2 = 0; r2 < rows; ++r2) {
+          const double2 x = w[r2], a = TH[(uint64_t)r2 * tw + col];
+          re += x.x * a.x + x.y * a.y;
+          im += x.x * a.y - x.y * a.x;
+        }
+        const double f = scale / sj;
+        val = make_double2(f * re, f * im);
+      }
+    }
+    B[(uint64_t)(k * 2 + s) * cap + r] = val;
+  }
+  if (lane == 0) dm[q + 1] = keep;
+}
+
 // p1 of qubit op.q by transfer matrices E_{j+1} = sum_s A_j[s]^H E_j A_j[s]
 // (s = 1 only at the measured site), then the draw, the projection
 // (project_qubit, simulator.rs:276-291), the reset flip and the cbit.
@@ -573,6 +777,9 @@ int alloc_buffers(dq_mps_s* h, uint32_t batch, uint32_t cap, uint32_t ncb) {
   DQ_CUDA_TRY(cudaMalloc((void**)&h->flags, sizeof(int) * 4));
   DQ_CUDA_TRY(cudaMalloc((void**)&h->svd_calls, sizeof(unsigned long long)));
   DQ_CUDA_TRY(cudaMalloc((void**)&h->scratch, sizeof(double2) * h->scratch_elems * batch));
+  if (cap <= kWarpCap)
+    DQ_CUDA_TRY(cudaFuncSetAttribute(k_mps_2q_warp, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)(kWarpsPer2q * warp_work_bytes(cap))));
   if (h->smem) {
     DQ_CUDA_TRY(cudaFuncSetAttribute(k_mps_2q, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)work_bytes));
@@ -694,11 +901,17 @@ int launch_ops(dq_mps_s* h, const std::vector<MpsOp>& ops) {
   // one SVD per CTA: wide CTAs when few replicas share the GPU (latency), 256
   // threads and several CTAs per SM otherwise (throughput)
   const int t2q = h->batch <= 2 * 148 ? 1024 : 256;
+  // many replicas of small bonds: one warp per replica
+  const bool warp2q = h->batch > 2 * 148 && h->cap <= kWarpCap;
   for (const MpsOp& op : ops) {
     switch (op.kind) {
       case M_1Q: k_mps_1q<<<h->batch, kMpsThreads, 0, h->stream>>>(v, op); break;
       case M_2Q:
-        k_mps_2q<<<h->batch, t2q, shm, h->stream>>>(v, op, h->max_bond, h->thr, use);
+        if (warp2q)
+          k_mps_2q_warp<<<(h->batch + kWarpsPer2q - 1) / kWarpsPer2q, kWarpsPer2q * 32,
+                          kWarpsPer2q * warp_work_bytes(h->cap), h->stream>>>(v, op, h->max_bond, h->thr);
+        else
+          k_mps_2q<<<h->batch, t2q, shm, h->stream>>>(v, op, h->max_bond, h->thr, use);
         break;
       case M_MEAS: case M_RESET:
         k_mps_measure<<<h->batch, kMpsThreads, shm, h->stream>>>(v, op, use);

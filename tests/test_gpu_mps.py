@@ -283,6 +283,18 @@ def test_shots_match_oracle_per_shot():
     assert counts == ref_counts
 
 
+@pytest.mark.parametrize("max_bond", [3, 16])
+def test_large_batch_warp_steps_match_oracle(max_bond):
+    # 600 replicas per launch: the one-warp-per-replica form of the fused step
+    c = trajectory_circuit(10, 9, seed=8)
+    prog = prog_of(c)
+    bits, st = run_mps_shots(prog, 5, 600, 0, max_bond, 1e-12)
+    assert st.replicas == 600 and st.capacity <= 16
+    for i in list(range(12)) + [299, 300, 599]:
+        _, rcb, _, _ = _oracle.mps_run(prog, 5 + i, max_bond=max_bond)
+        assert bits[i].tolist() == rcb.tolist(), i
+
+
 def test_shots_agree_with_statevector_distribution():
     c = JsonCircuit(4, [g("h", q) for q in range(4)] + [g("cx", 0, 3), g("cx", 1, 2), g("ry", 0, 0.6),
                                                       g("cx", 3, 1)] +
