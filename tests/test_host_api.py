@@ -211,3 +211,25 @@ def test_null_handle_and_bad_args_return_status(engine_lib):
     assert engine_lib.dq_rng_f64(1, 0, 4, None) == nat.DQ_ERR_INVALID_ARG
     blk = np.zeros(16, dtype=np.uint32)
     assert engine_lib.dq_chacha_block(blk.ctypes.data, 7, blk.ctypes.data) == nat.DQ_ERR_INVALID_ARG
+
+
+def test_mps_entry_points_reject_bad_arguments_without_a_gpu(engine_lib):
+    L = engine_lib
+    assert L.dq_mps_destroy(None) == 0
+    h = ctypes.c_void_p()
+    assert L.dq_mps_create(0, 0, 0, 1e-12, ctypes.byref(h)) == nat.DQ_ERR_INVALID_ARG
+    assert "qubit count" in nat.last_error()
+    assert L.dq_mps_create(4, 0, 0, -1.0, ctypes.byref(h)) == nat.DQ_ERR_INVALID_ARG
+    assert "truncation_threshold" in nat.last_error()
+    assert L.dq_mps_create(4, 0, 0, 1e-12, None) == nat.DQ_ERR_INVALID_ARG
+    st = nat.MpsStats()
+    assert L.dq_mps_run(None, None, 0, None, 0, 0, None, 0, ctypes.byref(st)) == nat.DQ_ERR_INVALID_ARG
+    assert L.dq_mps_bond_dims(None, None) == nat.DQ_ERR_INVALID_ARG
+    assert L.dq_mps_apply_2q(None, 0, 1, None) == nat.DQ_ERR_INVALID_ARG
+    # an unconditional gate on three qubits is rejected while lowering, before any device work
+    from dqsim_bosonic_b200.circuit import decode_circuit_json, encode
+    from _circuits import JsonCircuit, g
+    p = encode(decode_circuit_json(JsonCircuit(3, [g("h", 0), g("ccx", 0, 1, 2)]).model_dump_json()))
+    rc = L.dq_mps_run_shots(0, 3, 0, 1e-12, nat.ptr(p.insts), p.ninst, None, 0, 1, 0, 4, None, 0, 0,
+                            ctypes.byref(st))
+    assert rc == nat.DQ_ERR_UNSUPPORTED and st.failed_inst == 1
