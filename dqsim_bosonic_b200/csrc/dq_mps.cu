@@ -76,7 +76,7 @@ struct MpsView {
   uint32_t n, batch, cap, ncb;
 };
 
-enum : int { F_OK = 0, F_UNSUPPORTED = 1, F_CAPACITY = 2 };
+enum : int { MF_OK = 0, MF_UNSUPPORTED = 1, MF_CAPACITY = 2 };
 
 constexpr int kMpsThreads = 256;
 constexpr int kMaxSweeps = 60;
@@ -136,6 +136,29 @@ __global__ void __launch_bounds__(kMpsThreads) k_mps_1q(MpsView v, MpsOp op) {
 __device__ __forceinline__ double warp_sum(double x) {
   for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
   return x;
+}
+
+// Rotation of one column pair (p, q) with Gram entries alpha = |a_p|^2,
+// beta = |a_q|^2, gamma = a_p^H a_q = |gamma| e^{i phi}: false when the pair
+// is orthogonal to within tol.  Otherwise
+//   a_p' = c a_p - s e^{-i phi} a_q,   a_q' = s e^{i phi} a_p + c a_q
+// with t = sign(zeta) / (|zeta| + sqrt(1 + zeta^2)), zeta = (beta - alpha) /
+// (2 |gamma|), c = 1 / sqrt(1 + t^2), s = c t, which zeroes a_p'^H a_q'.  The
+// reciprocal square roots keep the dependent chain at four special-function
+// operations.
+__device__ __forceinline__ bool jacobi_rotation(double al, double be, double gr, double gi, double tol,
+                                                double& c, double& s, double& ex, double& ey) {
+  const double g2 = gr * gr + gi * gi;
+  if (!(g2 > 0.0)) return false;
+  const double inv = rsqrt(g2);
+  if (!(g2 * inv > tol * sqrt(al) * sqrt(be))) return false;
+  const double zeta = 0.5 * (be - al) * inv;
+  const double t = (zeta >= 0.0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+  c = rsqrt(1.0 + t * t);
+  s = c * t;
+  ex = gr * inv;
+  ey = gi * inv;
+  return true;
 }
 
 // Work area (double2 elements) of the fused step at capacity cap, in shared
@@ -237,14 +260,9 @@ __global__ void __launch_bounds__(1024) k_mps_2q(MpsView v, MpsOp op, uint32_t m
         be = warp_sum(be);
         gr = warp_sum(gr);
         gi = warp_sum(gi);
-        const double ag = sqrt(gr * gr + gi * gi);
-        if (ag > 0.0 && ag > tol * sqrt(al) * sqrt(be)) {
+        double c, s, ex, ey;
+        if (jacobi_rotation(al, be, gr, gi, tol, c, s, ex, ey)) {
           if (lane == 0) s_rot = 1;
-          const double zeta = (be - al) / (2.0 * ag);
-          const double t = (zeta >= 0.0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
-          const double c = 1.0 / sqrt(1.0 + t * t), s = c * t;
-          const double ex = gr / ag, ey = gi / ag;  // e^{i phi}, gamma = |gamma| e^{i phi}
-          // a_p' = c a_p - s e^{-i phi} a_q ;  a_q' = s e^{i phi} a_p + c a_q
           for (uint32_t i = lane; i < rows; i += 32) {
             const double2 x = gp[i], y = gq[i];
             gp[i] = make_double2(c * x.x - s * (ex * y.x + ey * y.y), c * x.y - s * (ex * y.y - ey * y.x));
@@ -294,7 +312,7 @@ __global__ void __launch_bounds__(1024) k_mps_2q(MpsView v, MpsOp op, uint32_t m
     s_keep = keep;
     if (keep > cap) {
       atomicMax(&v.flags[2], (int)keep);
-      atomicMax(&v.flags[0], F_CAPACITY);
+      atomicMax(&v.flags[0], MF_CAPACITY);
     } else {
       atomicAdd(v.svd_calls, 1ull);
     }
@@ -455,13 +473,9 @@ __global__ void __launch_bounds__(kWarpsPer2q * 32) k_mps_2q_warp(MpsView v, Mps
         gr += __shfl_xor_sync(full, gr, o);
         gi += __shfl_xor_sync(full, gi, o);
       }
-      const double ag = sqrt(gr * gr + gi * gi);
-      if (active && ag > 0.0 && ag > tol * sqrt(al) * sqrt(be)) {
+      double c, s, ex, ey;
+      if (active && jacobi_rotation(al, be, gr, gi, tol, c, s, ex, ey)) {
         rot = true;
-        const double zeta = (be - al) / (2.0 * ag);
-        const double t = (zeta >= 0.0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
-        const double c = 1.0 / sqrt(1.0 + t * t), s = c * t;
-        const double ex = gr / ag, ey = gi / ag;
         for (uint32_t i = h; i < rows; i += lpp) {
           const double2 x = gp[i], y = gq[i];
           gp[i] = make_double2(c * x.x - s * (ex * y.x + ey * y.y), c * x.y - s * (ex * y.y - ey * y.x));
@@ -502,7 +516,7 @@ __global__ void __launch_bounds__(kWarpsPer2q * 32) k_mps_2q_warp(MpsView v, Mps
     scale = disc > 0.0 ? total / kept : 1.0;
     if (keep > cap) {
       atomicMax(&v.flags[2], (int)keep);
-      atomicMax(&v.flags[0], F_CAPACITY);
+      atomicMax(&v.flags[0], MF_CAPACITY);
     } else {
       atomicAdd(v.svd_calls, 1ull);
     }
@@ -646,7 +660,7 @@ __global__ void __launch_bounds__(kMpsThreads) k_mps_measure(MpsView v, MpsOp op
 __global__ void k_mps_fail(MpsView v, MpsOp op) {
   const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= v.batch || !cond_ok(v, op, b)) return;
-  atomicMax(&v.flags[0], F_UNSUPPORTED);
+  atomicMax(&v.flags[0], MF_UNSUPPORTED);
   atomicMin(&v.flags[1], op.inst);
 }
 
@@ -956,7 +970,7 @@ int run_batch(dq_mps_s* h, const std::vector<MpsOp>& ops, const dq_cond* conds, 
     for (uint32_t b = 0; b < batch; ++b) seed_key_from_u64(seeds[b], &keys[(size_t)b * 8]);
     DQ_CUDA_TRY(cudaMemcpyAsync(h->key, keys.data(), sizeof(uint32_t) * keys.size(), cudaMemcpyHostToDevice,
                                 h->stream));
-    const int init_flags[4] = {F_OK, 0x7fffffff, 0, 0};
+    const int init_flags[4] = {MF_OK, 0x7fffffff, 0, 0};
     DQ_CUDA_TRY(cudaMemcpyAsync(h->flags, init_flags, sizeof(init_flags), cudaMemcpyHostToDevice, h->stream));
     DQ_CUDA_TRY(cudaMemsetAsync(h->svd_calls, 0, sizeof(unsigned long long), h->stream));
     cudaEvent_t e0, e1;
@@ -978,7 +992,7 @@ int run_batch(dq_mps_s* h, const std::vector<MpsOp>& ops, const dq_cond* conds, 
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     if (rc != DQ_OK) return rc;
-    if (fl[0] == F_CAPACITY) {
+    if (fl[0] == MF_CAPACITY) {
       uint32_t need = (uint32_t)fl[2];
       uint32_t cap = h->cap;
       while (cap < need) cap *= 2;
@@ -1041,12 +1055,12 @@ void destroy_handle(dq_mps_s* h) {
 }
 
 int map_status(int status, int failed, int64_t* out_failed) {
-  if (status == F_UNSUPPORTED) {
+  if (status == MF_UNSUPPORTED) {
     if (out_failed) *out_failed = failed;
     return fail(DQ_ERR_UNSUPPORTED, "instruction " + std::to_string(failed) +
                                         " is not supported by the MPS simulator");
   }
-  if (status != F_OK) return fail(DQ_ERR_INTERNAL, "MPS run flagged status " + std::to_string(status));
+  if (status != MF_OK) return fail(DQ_ERR_INTERNAL, "MPS run flagged status " + std::to_string(status));
   return DQ_OK;
 }
 
@@ -1155,7 +1169,7 @@ int dq_mps_apply_2q(dq_mps_t h, uint32_t a, uint32_t b, const double* u) {
   // Below the bond bound a step may overflow the capacity: run the steps one
   // at a time, and on an overflow (the step wrote nothing) widen and redo it.
   const uint32_t bound = bond_bound(h->n, h->max_bond);
-  const int init_flags[4] = {F_OK, 0x7fffffff, 0, 0};
+  const int init_flags[4] = {MF_OK, 0x7fffffff, 0, 0};
   if (h->cap >= bound) {
     DQ_CUDA_TRY(cudaMemcpyAsync(h->flags, init_flags, sizeof(init_flags), cudaMemcpyHostToDevice, h->stream));
     DQ_TRY(launch_ops(h, ops));
@@ -1170,7 +1184,7 @@ int dq_mps_apply_2q(dq_mps_t h, uint32_t a, uint32_t b, const double* u) {
     int fl[4];
     DQ_CUDA_TRY(cudaMemcpyAsync(fl, h->flags, sizeof(fl), cudaMemcpyDeviceToHost, h->stream));
     DQ_CUDA_TRY(cudaStreamSynchronize(h->stream));
-    if (fl[0] == F_CAPACITY) {
+    if (fl[0] == MF_CAPACITY) {
       uint32_t cap = h->cap;
       while (cap < (uint32_t)fl[2]) cap *= 2;
       DQ_TRY(dq_mps_reserve(h, cap < bound ? cap : bound));

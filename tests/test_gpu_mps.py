@@ -245,13 +245,23 @@ def test_truncation_matches_oracle(max_bond, thr):
     assert np.max(np.abs(sv - ref)) < 1e-9
 
 
-def test_capacity_growth_to_global_scratch_matches_oracle():
+def test_capacity_growth_to_global_work_area_matches_oracle():
     # bond dimension 64 at the middle of 12 qubits: the handle starts at
     # capacity 16 and re-runs at 32 and 64 (64: SVD work area in global memory)
     c = brickwork_u3_cx(12, 14, seed=3)
     sv, _, dims, st = device_run(c, SEED)
     ref, _, rdims, _ = _oracle.mps_run(prog_of(c), SEED)
     assert max(dims) == 64 and st.capacity == 64
+    assert dims == rdims
+    assert np.max(np.abs(sv - ref)) < 1e-12
+
+
+def test_bond_128_matches_oracle():
+    # capacity 128: theta up to 256 x 256
+    c = brickwork_u3_cx(14, 14, seed=4)
+    sv, _, dims, st = device_run(c, SEED)
+    ref, _, rdims, _ = _oracle.mps_run(prog_of(c), SEED)
+    assert max(dims) == 128 and st.capacity == 128
     assert dims == rdims
     assert np.max(np.abs(sv - ref)) < 1e-12
 
