@@ -384,9 +384,13 @@ __global__ void __launch_bounds__(1024) k_mps_2q(MpsView v, MpsOp op, uint32_t m
 constexpr int kWarpsPer2q = 4;
 constexpr uint32_t kWarpCap = 16;
 
+// Largest padded column stride: ld <= 2 cap + 4 when cap is a multiple of 4
+// (then 2 cap = 0 mod 8 and lpp >= 2), else <= 2 cap + 7.
+__host__ __device__ inline uint32_t warp_ld_max(uint32_t cap) { return 2 * cap + (cap % 4 == 0 ? 4 : 7); }
+
 __host__ __device__ inline uint64_t warp_work_bytes(uint32_t cap) {
   const uint64_t c = 2ull * cap;
-  const uint64_t b = c * (c + 1) * sizeof(double2) + c * sizeof(double) + c * sizeof(uint32_t);
+  const uint64_t b = c * warp_ld_max(cap) * sizeof(double2) + c * sizeof(double) + c * sizeof(uint32_t);
   return (b + 15) & ~15ull;  // keeps every warp's G 16-byte aligned
 }
 
@@ -403,11 +407,17 @@ __global__ void __launch_bounds__(kWarpsPer2q * 32) k_mps_2q_warp(MpsView v, Mps
   const uint32_t L = dm[q], M = dm[q + 1], R = dm[q + 2];
   const bool tr = R > L;
   const uint32_t rows = tr ? 2 * R : 2 * L, cols = tr ? 2 * L : 2 * R;
-  const uint32_t ld = rows + 1;  // padded column stride
+  const uint32_t np = cols / 2;
+  uint32_t lpp = 1;  // lanes per pair
+  while (lpp * 2 * np <= 32) lpp *= 2;
+  // Column stride ld = lpp (mod 8) for lpp < 8: the 8 lanes of a 16-byte access
+  // phase (8 / lpp pairs with consecutive columns, lpp rows each) then fall in
+  // 8 distinct groups of 4 banks.
+  const uint32_t ld = lpp < 8 ? rows + ((lpp + 8 - rows % 8) % 8) : rows;
   const uint32_t tw = 2 * R;
   double2* TH = v.scratch + (uint64_t)b * v.scratch_elems;
   double2* G = reinterpret_cast<double2*>(reinterpret_cast<char*>(smem) + warp * warp_work_bytes(cap));
-  double* sig = reinterpret_cast<double*>(G + 2ull * cap * (2ull * cap + 1));
+  double* sig = reinterpret_cast<double*>(G + 2ull * cap * warp_ld_max(cap));
   uint32_t* perm = reinterpret_cast<uint32_t*>(sig + 2 * cap);
   double2* A = site(v, q, b);
   double2* B = site(v, q + 1, b);
@@ -438,9 +448,6 @@ __global__ void __launch_bounds__(kWarpsPer2q * 32) k_mps_2q_warp(MpsView v, Mps
   __syncwarp();
 
   const double tol = (double)rows * DBL_EPSILON;
-  const uint32_t np = cols / 2;
-  uint32_t lpp = 1;
-  while (lpp * 2 * np <= 32) lpp *= 2;
   const uint32_t pi = (uint32_t)lane / lpp, h = (uint32_t)lane % lpp;
   const bool active = pi < np;
   for (int sweep = 0; sweep < kMaxSweeps; ++sweep) {
