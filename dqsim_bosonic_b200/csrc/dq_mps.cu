@@ -235,35 +235,48 @@ __global__ void __launch_bounds__(1024) k_mps_2q(MpsView v, MpsOp op, uint32_t m
   // ---- one-sided Jacobi --------------------------------------------------------
   const double tol = (double)rows * DBL_EPSILON;
   const uint32_t np = cols / 2;
+  // more pairs than warps: two lane groups of 16 lanes, one pair each, so that
+  // two of a warp's pairs run side by side (narrower groups would leave each
+  // lane a long serial run of loads)
+  const uint32_t ppw = (np + nw - 1) / nw;
+  const uint32_t lpp = ppw > 1 ? 16u : 32u;
+  const uint32_t gpw = 32 / lpp, g = (uint32_t)lane / lpp, h = (uint32_t)lane % lpp;
   for (int sweep = 0; sweep < kMaxSweeps; ++sweep) {
     for (uint32_t rd = 0; rd + 1 < cols; ++rd) {
-      for (uint32_t pi = warp; pi < np; pi += nw) {
-        uint32_t p, qq;
-        if (pi == 0) {
-          p = rd;
-          qq = cols - 1;
-        } else {
-          p = (rd + pi) % (cols - 1);
-          qq = (rd + (cols - 1) - pi) % (cols - 1);
+      for (uint32_t base = warp * gpw; base < np; base += nw * gpw) {
+        const uint32_t pi = base + g;
+        const bool active = pi < np;
+        uint32_t p = 0, qq = 0;
+        if (active) {
+          if (pi == 0) {
+            p = rd;
+            qq = cols - 1;
+          } else {
+            p = (rd + pi) % (cols - 1);
+            qq = (rd + (cols - 1) - pi) % (cols - 1);
+          }
         }
         double2* gp = G + (uint64_t)p * rows;
         double2* gq = G + (uint64_t)qq * rows;
         double al = 0.0, be = 0.0, gr = 0.0, gi = 0.0;
-        for (uint32_t i = lane; i < rows; i += 32) {
-          const double2 x = gp[i], y = gq[i];
-          al += x.x * x.x + x.y * x.y;
-          be += y.x * y.x + y.y * y.y;
-          gr += x.x * y.x + x.y * y.y;
-          gi += x.x * y.y - x.y * y.x;
+        if (active)
+          for (uint32_t i = h; i < rows; i += lpp) {
+            const double2 x = gp[i], y = gq[i];
+            al += x.x * x.x + x.y * x.y;
+            be += y.x * y.x + y.y * y.y;
+            gr += x.x * y.x + x.y * y.y;
+            gi += x.x * y.y - x.y * y.x;
+          }
+        for (uint32_t o = lpp / 2; o >= 1; o >>= 1) {
+          al += __shfl_xor_sync(0xffffffffu, al, o);
+          be += __shfl_xor_sync(0xffffffffu, be, o);
+          gr += __shfl_xor_sync(0xffffffffu, gr, o);
+          gi += __shfl_xor_sync(0xffffffffu, gi, o);
         }
-        al = warp_sum(al);
-        be = warp_sum(be);
-        gr = warp_sum(gr);
-        gi = warp_sum(gi);
         double c, s, ex, ey;
-        if (jacobi_rotation(al, be, gr, gi, tol, c, s, ex, ey)) {
-          if (lane == 0) s_rot = 1;
-          for (uint32_t i = lane; i < rows; i += 32) {
+        if (active && jacobi_rotation(al, be, gr, gi, tol, c, s, ex, ey)) {
+          if (h == 0) s_rot = 1;
+          for (uint32_t i = h; i < rows; i += lpp) {
             const double2 x = gp[i], y = gq[i];
             gp[i] = make_double2(c * x.x - s * (ex * y.x + ey * y.y), c * x.y - s * (ex * y.y - ey * y.x));
             gq[i] = make_double2(s * (ex * x.x - ey * x.y) + c * y.x, s * (ex * x.y + ey * x.x) + c * y.y);
