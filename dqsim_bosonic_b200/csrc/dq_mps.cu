@@ -677,6 +677,95 @@ __global__ void __launch_bounds__(kMpsThreads) k_mps_measure(MpsView v, MpsOp op
   }
 }
 
+// Warp-per-replica form of k_mps_measure for large batches of small bonds
+// (capacity <= 16): the three transfer matrices of a replica (3 x cap^2) live
+// in its warp's slice of shared memory; __syncwarp orders the phases.
+__host__ __device__ inline uint64_t warp_measure_bytes(uint32_t cap) {
+  return 3ull * cap * cap * sizeof(double2);
+}
+
+__global__ void __launch_bounds__(kWarpsPer2q * 32) k_mps_measure_warp(MpsView v, MpsOp op) {
+  extern __shared__ double2 smem[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint32_t b = blockIdx.x * kWarpsPer2q + warp;
+  if (b >= v.batch || !cond_ok(v, op, b)) return;
+  const unsigned full = 0xffffffffu;
+  const uint32_t* dm = v.dims + (uint64_t)b * (v.n + 1);
+  const uint32_t cap = v.cap;
+  double2* E = smem + (uint64_t)warp * 3 * cap * cap;
+  double2* F = E + (uint64_t)cap * cap;
+  double2* E2 = F + (uint64_t)cap * cap;
+  const double2 zero = make_double2(0.0, 0.0);
+  if (lane == 0) E[0] = make_double2(1.0, 0.0);
+  __syncwarp();
+  for (uint32_t j = 0; j < v.n; ++j) {
+    const uint32_t Lj = dm[j], Rj = dm[j + 1];
+    const double2* A = site(v, j, b);
+    for (uint32_t t = lane; t < Rj * Rj; t += 32) E2[t] = zero;
+    for (int s = 0; s < 2; ++s) {
+      if (j == op.q && s == 0) continue;
+      __syncwarp();
+      for (uint32_t t = lane; t < Lj * Rj; t += 32) {
+        const uint32_t l = t / Rj, rp = t - (t / Rj) * Rj;
+        double2 acc = zero;
+        for (uint32_t lp = 0; lp < Lj; ++lp) {
+          const double2 e = E[l * Lj + lp], a = A[(uint64_t)(lp * 2 + s) * cap + rp];
+          acc.x += e.x * a.x - e.y * a.y;
+          acc.y += e.x * a.y + e.y * a.x;
+        }
+        F[t] = acc;
+      }
+      __syncwarp();
+      for (uint32_t t = lane; t < Rj * Rj; t += 32) {
+        const uint32_t r = t / Rj, rp = t - (t / Rj) * Rj;
+        double2 acc = E2[t];
+        for (uint32_t l = 0; l < Lj; ++l) {
+          const double2 a = A[(uint64_t)(l * 2 + s) * cap + r], f = F[l * Rj + rp];
+          acc.x += a.x * f.x + a.y * f.y;
+          acc.y += a.x * f.y - a.y * f.x;
+        }
+        E2[t] = acc;
+      }
+    }
+    __syncwarp();
+    for (uint32_t t = lane; t < Rj * Rj; t += 32) E[t] = E2[t];
+    __syncwarp();
+  }
+  int outcome = 0;
+  double scale = 0.0;
+  if (lane == 0) {
+    double p1 = fmin(fmax(E[0].x, 0.0), 1.0);
+    const double r = chacha8_draw(v.key + (uint64_t)b * 8, v.ctr[b]);
+    v.ctr[b] += 1;
+    outcome = r < p1 ? 1 : 0;
+    const double prob = outcome ? p1 : 1.0 - p1;
+    scale = prob > 0.0 ? 1.0 / sqrt(prob) : 0.0;
+    if (op.kind == M_MEAS && op.cbit >= 0) v.cbits[(uint64_t)b * v.ncb + op.cbit] = outcome;
+  }
+  outcome = __shfl_sync(full, outcome, 0);
+  scale = __shfl_sync(full, scale, 0);
+  const double2 sc = make_double2(scale, 0.0);
+  double2* A = site(v, op.q, b);
+  const uint32_t L = dm[op.q], R = dm[op.q + 1];
+  for (uint32_t t = lane; t < L * 2 * R; t += 32) {
+    const uint32_t row = t / R, r = t - (t / R) * R;
+    double2* p = A + (uint64_t)row * cap + r;
+    *p = ((int)(row & 1u) == outcome) ? cmul_x(*p, sc) : zero;
+  }
+  if (op.kind == M_RESET && outcome == 1) {
+    __syncwarp();
+    const double2 x1 = make_double2(1.0, 0.0);
+    for (uint32_t t = lane; t < L * R; t += 32) {
+      const uint32_t l = t / R, r = t - (t / R) * R;
+      double2* p0 = A + (uint64_t)(l * 2) * cap + r;
+      double2* p1 = p0 + cap;
+      const double2 a0 = *p0, a1 = *p1;
+      *p0 = cadd_x(cadd_x(zero, cmul_x(zero, a0)), cmul_x(x1, a1));
+      *p1 = cadd_x(cadd_x(zero, cmul_x(x1, a0)), cmul_x(zero, a1));
+    }
+  }
+}
+
 __global__ void k_mps_fail(MpsView v, MpsOp op) {
   const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= v.batch || !cond_ok(v, op, b)) return;
@@ -811,6 +900,9 @@ int alloc_buffers(dq_mps_s* h, uint32_t batch, uint32_t cap, uint32_t ncb) {
   DQ_CUDA_TRY(cudaMalloc((void**)&h->flags, sizeof(int) * 4));
   DQ_CUDA_TRY(cudaMalloc((void**)&h->svd_calls, sizeof(unsigned long long)));
   DQ_CUDA_TRY(cudaMalloc((void**)&h->scratch, sizeof(double2) * h->scratch_elems * batch));
+  if (cap <= kWarpCap)
+    DQ_CUDA_TRY(cudaFuncSetAttribute(k_mps_measure_warp, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)(kWarpsPer2q * warp_measure_bytes(cap))));
   if (cap <= kWarpCap)
     DQ_CUDA_TRY(cudaFuncSetAttribute(k_mps_2q_warp, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)(kWarpsPer2q * warp_work_bytes(cap))));
@@ -948,7 +1040,11 @@ int launch_ops(dq_mps_s* h, const std::vector<MpsOp>& ops) {
           k_mps_2q<<<h->batch, t2q, shm, h->stream>>>(v, op, h->max_bond, h->thr, use);
         break;
       case M_MEAS: case M_RESET:
-        k_mps_measure<<<h->batch, kMpsThreads, shm, h->stream>>>(v, op, use);
+        if (warp2q)
+          k_mps_measure_warp<<<(h->batch + kWarpsPer2q - 1) / kWarpsPer2q, kWarpsPer2q * 32,
+                               kWarpsPer2q * warp_measure_bytes(h->cap), h->stream>>>(v, op);
+        else
+          k_mps_measure<<<h->batch, kMpsThreads, shm, h->stream>>>(v, op, use);
         break;
       case M_FAIL: k_mps_fail<<<(h->batch + 127) / 128, 128, 0, h->stream>>>(v, op); break;
       default: return fail(DQ_ERR_INTERNAL, "bad MPS operation");
