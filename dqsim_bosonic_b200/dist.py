@@ -104,11 +104,13 @@ def _collective_device(group=None):
 
 def simulate_shots_sharded(sim, circuit, shots: int, group=None) -> dict[str, int]:
     """``simulate_shots`` with the shots split across the process group; every
-    rank returns the merged counts (identical to a single-rank run)."""
+    rank returns the merged counts (identical to a single-rank run).  ``sim``
+    is a ``StatevectorSimulator`` or an ``MpsSimulator``."""
     import torch.distributed as dist
 
     from .batch import run_trajectories
     from .circuit import format_cbits
+    from .mps import MpsSimulator, run_mps_shots
     from .statevector import _entropy_u64, _parse
 
     rank = dist.get_rank(group) if dist.is_initialized() else 0
@@ -118,7 +120,11 @@ def simulate_shots_sharded(sim, circuit, shots: int, group=None) -> dict[str, in
     lo, hi = shard_range(shots, rank, world)
     counts: dict[str, int] = {}
     if hi > lo:
-        bits, _, _ = run_trajectories(prog, (base_seed + lo) & ((1 << 64) - 1), hi - lo, sim.device)
+        seed0 = (base_seed + lo) & ((1 << 64) - 1)
+        if isinstance(sim, MpsSimulator):  # MPS shots (mps/simulator.rs:368-385), same seeding
+            bits, _ = run_mps_shots(prog, seed0, hi - lo, sim.device, sim._max_bond, sim._threshold)
+        else:
+            bits, _, _ = run_trajectories(prog, seed0, hi - lo, sim.device)
         for row in bits:
             k = format_cbits(row, prog.num_cbits)
             counts[k] = counts.get(k, 0) + 1
