@@ -71,9 +71,11 @@ struct MpsView {
   double2* scratch;      // batch x scratch_elems (global fallback of the SVD work area)
   int* flags;            // [0] status, [1] first failing instruction, [2] capacity needed
   unsigned long long* svd_calls;
+  const MpsOp* ops;      // the program's operations; a launch runs ops[first + blockIdx.y]
   uint64_t site_elems;   // cap * 2 * cap
   uint64_t scratch_elems;
   uint32_t n, batch, cap, ncb;
+  uint32_t slots;        // scratch slots per replica (two-qubit steps per launch)
 };
 
 enum : int { MF_OK = 0, MF_UNSUPPORTED = 1, MF_CAPACITY = 2 };
@@ -126,7 +128,8 @@ __global__ void __launch_bounds__(kMpsThreads) k_mps_reset(MpsView v) {
   if (threadIdx.x == 0) v.ctr[b] = 0;
 }
 
-__global__ void __launch_bounds__(kMpsThreads) k_mps_1q(MpsView v, MpsOp op) {
+__global__ void __launch_bounds__(kMpsThreads) k_mps_1q(MpsView v, uint32_t first) {
+  const MpsOp& op = v.ops[first + blockIdx.y];
   const uint32_t b = blockIdx.x;
   if (!cond_ok(v, op, b)) return;
   const uint32_t* dm = v.dims + (uint64_t)b * (v.n + 1);
@@ -183,8 +186,9 @@ __host__ __device__ inline uint64_t theta_elems(uint32_t cap) { return 4ull * ca
 //   2R <= 2L:  left = U,                       right = scale * U^H theta
 //   2R >  2L:  left = theta W / sigma^2,       right = scale * W^H
 // read from a copy of theta (global memory, L2-resident).
-__global__ void __launch_bounds__(1024) k_mps_2q(MpsView v, MpsOp op, uint32_t max_keep, double thr,
+__global__ void __launch_bounds__(1024) k_mps_2q(MpsView v, uint32_t first, uint32_t max_keep, double thr,
                                                  int use_smem) {
+  const MpsOp& op = v.ops[first + blockIdx.y];
   extern __shared__ double2 smem[];
   __shared__ int s_rot;
   __shared__ uint32_t s_keep;
@@ -197,7 +201,7 @@ __global__ void __launch_bounds__(1024) k_mps_2q(MpsView v, MpsOp op, uint32_t m
   const bool tr = R > L;
   const uint32_t rows = tr ? 2 * R : 2 * L, cols = tr ? 2 * L : 2 * R;
   const uint32_t tw = 2 * R;   // theta row length
-  double2* TH = v.scratch + (uint64_t)b * v.scratch_elems;
+  double2* TH = v.scratch + ((uint64_t)b * v.slots + blockIdx.y) * v.scratch_elems;
   double2* G = use_smem ? smem : TH + theta_elems(cap);
   double* sig = reinterpret_cast<double*>(G + (uint64_t)rows * cols);
   uint32_t* perm = reinterpret_cast<uint32_t*>(sig + cols);
@@ -407,8 +411,9 @@ __host__ __device__ inline uint64_t warp_work_bytes(uint32_t cap) {
   return (b + 15) & ~15ull;  // keeps every warp's G 16-byte aligned
 }
 
-__global__ void __launch_bounds__(kWarpsPer2q * 32) k_mps_2q_warp(MpsView v, MpsOp op, uint32_t max_keep,
+__global__ void __launch_bounds__(kWarpsPer2q * 32) k_mps_2q_warp(MpsView v, uint32_t first, uint32_t max_keep,
                                                                   double thr) {
+  const MpsOp& op = v.ops[first + blockIdx.y];
   extern __shared__ double2 smem[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const uint32_t b = blockIdx.x * kWarpsPer2q + warp;
@@ -428,7 +433,7 @@ __global__ void __launch_bounds__(kWarpsPer2q * 32) k_mps_2q_warp(MpsView v, Mps
   // 8 distinct groups of 4 banks.
   const uint32_t ld = lpp < 8 ? rows + ((lpp + 8 - rows % 8) % 8) : rows;
   const uint32_t tw = 2 * R;
-  double2* TH = v.scratch + (uint64_t)b * v.scratch_elems;
+  double2* TH = v.scratch + ((uint64_t)b * v.slots + blockIdx.y) * v.scratch_elems;
   double2* G = reinterpret_cast<double2*>(reinterpret_cast<char*>(smem) + warp * warp_work_bytes(cap));
   double* sig = reinterpret_cast<double*>(G + 2ull * cap * warp_ld_max(cap));
   uint32_t* perm = reinterpret_cast<uint32_t*>(sig + 2 * cap);
@@ -599,7 +604,8 @@ __global__ void __launch_bounds__(kWarpsPer2q * 32) k_mps_2q_warp(MpsView v, Mps
 // p1 of qubit op.q by transfer matrices E_{j+1} = sum_s A_j[s]^H E_j A_j[s]
 // (s = 1 only at the measured site), then the draw, the projection
 // (project_qubit, simulator.rs:276-291), the reset flip and the cbit.
-__global__ void __launch_bounds__(kMpsThreads) k_mps_measure(MpsView v, MpsOp op, int use_smem) {
+__global__ void __launch_bounds__(kMpsThreads) k_mps_measure(MpsView v, uint32_t first, int use_smem) {
+  const MpsOp& op = v.ops[first];
   extern __shared__ double2 smem[];
   __shared__ int s_out;
   __shared__ double s_scale;
@@ -607,7 +613,7 @@ __global__ void __launch_bounds__(kMpsThreads) k_mps_measure(MpsView v, MpsOp op
   if (!cond_ok(v, op, b)) return;
   const uint32_t* dm = v.dims + (uint64_t)b * (v.n + 1);
   const uint32_t cap = v.cap;
-  double2* E = use_smem ? smem : v.scratch + (uint64_t)b * v.scratch_elems + theta_elems(v.cap);
+  double2* E = use_smem ? smem : v.scratch + (uint64_t)b * v.slots * v.scratch_elems + theta_elems(v.cap);
   double2* F = E + (uint64_t)cap * cap;
   double2* E2 = F + (uint64_t)cap * cap;
   const double2 zero = make_double2(0.0, 0.0);
@@ -684,7 +690,8 @@ __host__ __device__ inline uint64_t warp_measure_bytes(uint32_t cap) {
   return 3ull * cap * cap * sizeof(double2);
 }
 
-__global__ void __launch_bounds__(kWarpsPer2q * 32) k_mps_measure_warp(MpsView v, MpsOp op) {
+__global__ void __launch_bounds__(kWarpsPer2q * 32) k_mps_measure_warp(MpsView v, uint32_t first) {
+  const MpsOp& op = v.ops[first];
   extern __shared__ double2 smem[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const uint32_t b = blockIdx.x * kWarpsPer2q + warp;
@@ -766,7 +773,8 @@ __global__ void __launch_bounds__(kWarpsPer2q * 32) k_mps_measure_warp(MpsView v
   }
 }
 
-__global__ void k_mps_fail(MpsView v, MpsOp op) {
+__global__ void k_mps_fail(MpsView v, uint32_t first) {
+  const MpsOp& op = v.ops[first];
   const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= v.batch || !cond_ok(v, op, b)) return;
   atomicMax(&v.flags[0], MF_UNSUPPORTED);
@@ -849,6 +857,9 @@ struct dq_mps_s {
   bool smem = true;
   uint64_t scratch_elems = 0;
   size_t work_bytes = 0;
+  uint32_t slots = 1;        // two-qubit steps one launch may run per replica
+  void* ops = nullptr;       // device copy of the program's operations
+  size_t ops_cap = 0;
 };
 
 namespace {
@@ -871,6 +882,9 @@ void free_buffers(dq_mps_s* h) {
   cudaFree(h->scratch);
   cudaFree(h->flags);
   cudaFree(h->svd_calls);
+  cudaFree(h->ops);
+  h->ops = nullptr;
+  h->ops_cap = 0;
   h->t = nullptr; h->dims = nullptr; h->key = nullptr; h->ctr = nullptr; h->cbits = nullptr;
   h->conds = nullptr; h->scratch = nullptr; h->flags = nullptr; h->svd_calls = nullptr;
   h->conds_cap = 0;
@@ -882,9 +896,17 @@ constexpr size_t kMaxSmem = 220 * 1024;
 // on the order of a second.
 constexpr uint32_t kMaxCapacity = 1024;
 
+// Steps on disjoint bonds are independent: with few replicas, one launch runs
+// up to this many of them per replica (each with its own scratch slot).
+uint32_t slots_for(uint32_t n, uint32_t batch) {
+  if (batch > 2 * 148) return 1;
+  return std::max<uint32_t>(1, std::min<uint32_t>(n / 2, 32));
+}
+
 int alloc_buffers(dq_mps_s* h, uint32_t batch, uint32_t cap, uint32_t ncb) {
   free_buffers(h);
   h->batch = batch;
+  h->slots = slots_for(h->n, batch);
   h->cap = cap;
   h->ncb = ncb ? ncb : 1;
   const uint64_t site = 2ull * cap * cap;
@@ -899,7 +921,7 @@ int alloc_buffers(dq_mps_s* h, uint32_t batch, uint32_t cap, uint32_t ncb) {
   DQ_CUDA_TRY(cudaMalloc((void**)&h->cbits, sizeof(int32_t) * h->ncb * batch));
   DQ_CUDA_TRY(cudaMalloc((void**)&h->flags, sizeof(int) * 4));
   DQ_CUDA_TRY(cudaMalloc((void**)&h->svd_calls, sizeof(unsigned long long)));
-  DQ_CUDA_TRY(cudaMalloc((void**)&h->scratch, sizeof(double2) * h->scratch_elems * batch));
+  DQ_CUDA_TRY(cudaMalloc((void**)&h->scratch, sizeof(double2) * h->scratch_elems * h->slots * batch));
   if (cap <= kWarpCap)
     DQ_CUDA_TRY(cudaFuncSetAttribute(k_mps_measure_warp, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)(kWarpsPer2q * warp_measure_bytes(cap))));
@@ -926,6 +948,8 @@ MpsView view_of(const dq_mps_s* h) {
   v.scratch = h->scratch;
   v.flags = h->flags;
   v.svd_calls = h->svd_calls;
+  v.ops = static_cast<const MpsOp*>(h->ops);
+  v.slots = h->slots;
   v.site_elems = 2ull * h->cap * h->cap;
   v.scratch_elems = h->scratch_elems;
   v.n = h->n;
@@ -1020,7 +1044,21 @@ int lower(uint32_t n, const dq_inst* prog, uint64_t ninst, const dq_cond* conds,
   return DQ_OK;
 }
 
+// Groups consecutive operations into launches: a run of one-qubit gates, or
+// of two-qubit steps (at most `slots`), whose sites are pairwise disjoint
+// commutes exactly, so one launch (blockIdx.y = the operation) runs them all;
+// measurements, resets and failures are launches of their own.
 int launch_ops(dq_mps_s* h, const std::vector<MpsOp>& ops) {
+  if (ops.empty()) return DQ_OK;
+  if (ops.size() > h->ops_cap) {
+    cudaFree(h->ops);
+    h->ops = nullptr;
+    h->ops_cap = 0;
+    DQ_CUDA_TRY(cudaMalloc(&h->ops, sizeof(MpsOp) * ops.size()));
+    h->ops_cap = ops.size();
+  }
+  DQ_CUDA_TRY(cudaMemcpyAsync(h->ops, ops.data(), sizeof(MpsOp) * ops.size(), cudaMemcpyHostToDevice,
+                              h->stream));
   const MpsView v = view_of(h);
   const size_t shm = h->smem ? h->work_bytes : 0;
   const int use = h->smem ? 1 : 0;
@@ -1029,26 +1067,43 @@ int launch_ops(dq_mps_s* h, const std::vector<MpsOp>& ops) {
   const int t2q = h->batch <= 2 * 148 ? 1024 : 256;
   // many replicas of small bonds: one warp per replica
   const bool warp2q = h->batch > 2 * 148 && h->cap <= kWarpCap;
-  for (const MpsOp& op : ops) {
-    switch (op.kind) {
-      case M_1Q: k_mps_1q<<<h->batch, kMpsThreads, 0, h->stream>>>(v, op); break;
+  std::vector<uint8_t> used(h->n, 0);
+  for (size_t i = 0; i < ops.size();) {
+    const int kind = ops[i].kind;
+    size_t j = i;
+    if (kind == M_1Q || kind == M_2Q) {
+      std::fill(used.begin(), used.end(), 0);
+      const size_t limit = kind == M_2Q ? h->slots : 65535;
+      while (j < ops.size() && ops[j].kind == kind && j - i < limit) {
+        const uint32_t q = ops[j].q, q2 = kind == M_2Q ? q + 1 : q;
+        if (used[q] || used[q2]) break;
+        used[q] = used[q2] = 1;
+        ++j;
+      }
+    } else {
+      j = i + 1;
+    }
+    const uint32_t first = (uint32_t)i, count = (uint32_t)(j - i);
+    switch (kind) {
+      case M_1Q: k_mps_1q<<<dim3(h->batch, count), kMpsThreads, 0, h->stream>>>(v, first); break;
       case M_2Q:
         if (warp2q)
-          k_mps_2q_warp<<<(h->batch + kWarpsPer2q - 1) / kWarpsPer2q, kWarpsPer2q * 32,
-                          kWarpsPer2q * warp_work_bytes(h->cap), h->stream>>>(v, op, h->max_bond, h->thr);
+          k_mps_2q_warp<<<dim3((h->batch + kWarpsPer2q - 1) / kWarpsPer2q, count), kWarpsPer2q * 32,
+                          kWarpsPer2q * warp_work_bytes(h->cap), h->stream>>>(v, first, h->max_bond, h->thr);
         else
-          k_mps_2q<<<h->batch, t2q, shm, h->stream>>>(v, op, h->max_bond, h->thr, use);
+          k_mps_2q<<<dim3(h->batch, count), t2q, shm, h->stream>>>(v, first, h->max_bond, h->thr, use);
         break;
       case M_MEAS: case M_RESET:
         if (warp2q)
           k_mps_measure_warp<<<(h->batch + kWarpsPer2q - 1) / kWarpsPer2q, kWarpsPer2q * 32,
-                               kWarpsPer2q * warp_measure_bytes(h->cap), h->stream>>>(v, op);
+                               kWarpsPer2q * warp_measure_bytes(h->cap), h->stream>>>(v, first);
         else
-          k_mps_measure<<<h->batch, kMpsThreads, shm, h->stream>>>(v, op, use);
+          k_mps_measure<<<h->batch, kMpsThreads, shm, h->stream>>>(v, first, use);
         break;
-      case M_FAIL: k_mps_fail<<<(h->batch + 127) / 128, 128, 0, h->stream>>>(v, op); break;
+      case M_FAIL: k_mps_fail<<<(h->batch + 127) / 128, 128, 0, h->stream>>>(v, first); break;
       default: return fail(DQ_ERR_INTERNAL, "bad MPS operation");
     }
+    i = j;
   }
   const cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return fail(DQ_ERR_CUDA, std::string("MPS launch: ") + cudaGetErrorString(e));
@@ -1057,10 +1112,10 @@ int launch_ops(dq_mps_s* h, const std::vector<MpsOp>& ops) {
 
 // Runs `ops` on a batch whose replica b is seeded with seeds[b]; grows the
 // capacity and re-runs while a truncation overflows it.
-uint64_t replica_bytes(uint32_t n, uint32_t cap) {
+uint64_t replica_bytes(uint32_t n, uint32_t cap, uint32_t slots) {
   const uint64_t work = svd_work_elems(cap) * sizeof(double2);
-  return (uint64_t)n * 2ull * cap * cap * sizeof(double2) + theta_elems(cap) * sizeof(double2) +
-         (work <= kMaxSmem ? 0 : work);
+  return (uint64_t)n * 2ull * cap * cap * sizeof(double2) +
+         slots * (theta_elems(cap) * sizeof(double2) + (work <= kMaxSmem ? 0 : work));
 }
 
 // Runs `ops` on a batch whose replica b is seeded with seeds[b]; grows the
@@ -1118,7 +1173,7 @@ int run_batch(dq_mps_s* h, const std::vector<MpsOp>& ops, const dq_cond* conds, 
         return fail(DQ_ERR_INVALID_ARG, "bond dimension " + std::to_string(need) +
                                             " exceeds the device MPS limit of " +
                                             std::to_string(kMaxCapacity) + "; set max_bond_dimension");
-      if (shrink && batch > 1 && budget && replica_bytes(h->n, cap) * batch > budget) {
+      if (shrink && batch > 1 && budget && replica_bytes(h->n, cap, slots_for(h->n, batch)) * batch > budget) {
         free_buffers(h);
         h->cap = cap;
         *shrink = true;
@@ -1436,7 +1491,7 @@ int dq_mps_run_shots(int device, uint32_t n, uint32_t max_bond, double truncatio
   unsigned long long calls = 0;
   std::vector<uint64_t> seeds;
   for (uint64_t s0 = 0; s0 < shots && rc == DQ_OK;) {
-    const uint64_t fit = std::max<uint64_t>(budget / replica_bytes(n, h->cap), 1);
+    const uint64_t fit = std::max<uint64_t>(budget / replica_bytes(n, h->cap, 1), 1);
     const uint32_t nb = (uint32_t)std::min<uint64_t>(std::min<uint64_t>(bmax, fit), shots - s0);
     seeds.resize(nb);
     for (uint32_t b = 0; b < nb; ++b) seeds[b] = base_seed + shot0 + s0 + b;  // wrapping
