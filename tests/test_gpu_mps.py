@@ -364,3 +364,20 @@ def test_generic_gates_and_nested_conditionals_match_oracle():
         assert cb.tolist() == rcb.tolist()
         assert dims == rdims
         assert np.max(np.abs(sv - ref)) < 1e-12
+
+
+def test_shots_beyond_statevector_width_ghz40():
+    # 40 qubits (no statevector of that size exists): GHZ by h + a cx chain (bond
+    # dimension 2), then every qubit measured; each shot reads all zeros or all ones
+    n = 40
+    insts = [g("h", 0)] + [g("cx", i, i + 1) for i in range(n - 1)] + [g("measure", i, i) for i in range(n)]
+    c = JsonCircuit(n, insts, ncbits=n)
+    counts = MpsSimulator(seed=9).simulate_shots(c, 2000)
+    assert set(counts) <= {"0" * n, "1" * n}
+    assert sum(counts.values()) == 2000
+    assert 800 < counts.get("1" * n, 0) < 1200
+    # reset + conditional across the chain: flip qubit 39 back when qubit 0 read 1
+    insts2 = insts[:n] + [g("measure", 0, 0), cond(0, 1, 1, g("x", n - 1)), g("measure", n - 1, 1)]
+    c2 = JsonCircuit(n, insts2, ncbits=2)
+    counts2 = MpsSimulator(seed=9).simulate_shots(c2, 500)
+    assert set(counts2) <= {"00", "01"}
