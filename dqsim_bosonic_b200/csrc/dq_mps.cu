@@ -11,16 +11,20 @@
 //
 // B200 design: a batch of B independent MPS (one per shot; B = 1 for
 // `simulate`) lives in HBM with padded tensors (capacity `cap` per bond) and
-// per-replica bond dimensions on the device.  Every program operation is one
-// launch over the whole batch, one CTA per replica, so the host never reads a
-// bond dimension while the program runs:
+// per-replica bond dimensions on the device.  Every launch runs one program
+// operation, or a run of operations on pairwise disjoint sites (they commute
+// exactly; blockIdx.y selects the operation), over the whole batch, so the host
+// never reads a bond dimension while the program runs:
 //   k_mps_1q       the 2x2 contraction of one site (exact num-complex order)
-//   k_mps_2q       FUSED adjacent step: theta build, one-sided (Hestenes)
-//                  Jacobi SVD in shared memory, descending sort, truncation
-//                  with the reference's keep / renormalisation rule, split
-//                  into the two new site tensors, new bond dimension
+//   k_mps_2q       FUSED adjacent step, one CTA per replica: theta build,
+//                  one-sided (Hestenes) Jacobi SVD in shared memory (global
+//                  memory above capacity 32), descending sort, truncation with
+//                  the reference's keep / renormalisation rule, split into the
+//                  two new site tensors, new bond dimension
+//   k_mps_2q_warp  the same step with one warp per replica (large batches of
+//                  bonds <= 16)
 //   k_mps_measure  p1 by a transfer-matrix contraction over the chain
-//                  (O(n chi^3) instead of the reference's 2^n statevector),
+//   (and _warp)    (O(n chi^3) instead of the reference's 2^n statevector),
 //                  the replica's ChaCha8 draw, projection, reset flip, cbit
 //   k_mps_expand   to_statevector (:238-257) as a left-to-right contraction,
 //                  one launch per site, same summation order as the reference
