@@ -57,6 +57,11 @@ def test_mps_mode_accepts_supported_options_before_circuit_decoding():
         simulate_monolithic(object(), mode="mps", max_bond_dimension=1, truncation_threshold=1e-14)
 
 
+def test_mps_mode_accepts_none_bond_dimension_before_circuit_decoding():
+    with pytest.raises(AttributeError, match="model_dump_json"):
+        simulate_monolithic(object(), mode="mps", max_bond_dimension=None)
+
+
 def test_mps_mode_rejects_zero_bond_dimension():
     with pytest.raises(ValueError, match="max_bond_dimension"):
         simulate_monolithic(object(), mode="mps", max_bond_dimension=0)
