@@ -397,31 +397,46 @@ __global__ void __launch_bounds__(1024) k_mps_2q(MpsView v, uint32_t first, uint
   if (tid == 0) dm[q + 1] = keep;
 }
 
-// Warp-per-replica form of k_mps_2q for capacity <= 16 (theta at most
-// 32 x 32): kWarpsPer2q replicas per CTA, each warp with its own shared-memory
-// G, no block barriers.  The cols/2 pairs of a round are spread over groups
-// of lpp lanes (lpp = the largest power of two <= 32 / pairs); a group splits
-// the rows of its pair and reduces the four dot products with xor shuffles.
-constexpr int kWarpsPer2q = 4;
+// Batched form of k_mps_2q for capacity <= 16 (theta at most 32 x 32): two
+// warps (64 lanes) per replica, kRepsPer2q replicas per CTA, each replica with
+// its own shared-memory G and its own named barrier (id 1 + slot, 64 threads)
+// instead of block barriers.  The cols/2 pairs of a round are spread over
+// groups of lpp lanes (lpp = the largest power of two <= 64 / pairs, at most
+// 32, so a group never spans two warps); a group splits the rows of its pair
+// and reduces the four dot products with xor shuffles.  Every early return and
+// every loop exit depends only on values both warps hold (the replica's
+// condition, cols, the shared convergence flags, keep), so both warps reach
+// the same barriers.
+constexpr int kRepsPer2q = 4;
+constexpr int kLanesPerRep = 64;
+constexpr int kWarpsPer2q = kRepsPer2q * kLanesPerRep / 32;  // warps per CTA
 constexpr uint32_t kWarpCap = 16;
 
 // Largest padded column stride: ld <= 2 cap + 4 when cap is a multiple of 4
-// (then 2 cap = 0 mod 8 and lpp >= 2), else <= 2 cap + 7.
+// (then 2 cap = 0 mod 8 and lpp >= 4), else <= 2 cap + 7.
 __host__ __device__ inline uint32_t warp_ld_max(uint32_t cap) { return 2 * cap + (cap % 4 == 0 ? 4 : 7); }
 
 __host__ __device__ inline uint64_t warp_work_bytes(uint32_t cap) {
   const uint64_t c = 2ull * cap;
   const uint64_t b = c * warp_ld_max(cap) * sizeof(double2) + c * sizeof(double) + c * sizeof(uint32_t);
-  return (b + 15) & ~15ull;  // keeps every warp's G 16-byte aligned
+  return (b + 15) & ~15ull;  // keeps every replica's G 16-byte aligned
 }
+
+__device__ __forceinline__ void rep_sync(int id) { asm volatile("bar.sync %0, 64;" ::"r"(id) : "memory"); }
 
 __global__ void __launch_bounds__(kWarpsPer2q * 32) k_mps_2q_warp(MpsView v, uint32_t first, uint32_t max_keep,
                                                                   double thr) {
   const MpsOp& op = v.ops[first + blockIdx.y];
   extern __shared__ double2 smem[];
+  __shared__ int s_any[kRepsPer2q][2][2];   // [slot][sweep parity][warp]
+  __shared__ uint32_t s_keep[kRepsPer2q];
+  __shared__ double s_scale[kRepsPer2q];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const uint32_t b = blockIdx.x * kWarpsPer2q + warp;
-  if (b >= v.batch || !cond_ok(v, op, b)) return;
+  const int slot = warp / 2, wr = warp % 2;          // replica slot in the CTA, warp within it
+  const uint32_t tl = (uint32_t)(wr * 32 + lane);    // lane within the replica (0..63)
+  const int bar = 1 + slot;
+  const uint32_t b = blockIdx.x * kRepsPer2q + slot;
+  if (b >= v.batch || !cond_ok(v, op, b)) return;    // the same for both warps of the replica
   const unsigned full = 0xffffffffu;
   const uint32_t cap = v.cap;
   uint32_t* dm = v.dims + (uint64_t)b * (v.n + 1);
@@ -431,21 +446,21 @@ __global__ void __launch_bounds__(kWarpsPer2q * 32) k_mps_2q_warp(MpsView v, uin
   const uint32_t rows = tr ? 2 * R : 2 * L, cols = tr ? 2 * L : 2 * R;
   const uint32_t np = cols / 2;
   uint32_t lpp = 1;  // lanes per pair
-  while (lpp * 2 * np <= 32) lpp *= 2;
+  while (lpp < 32 && lpp * 2 * np <= (uint32_t)kLanesPerRep) lpp *= 2;
   // Column stride ld = lpp (mod 8) for lpp < 8: the 8 lanes of a 16-byte access
   // phase (8 / lpp pairs with consecutive columns, lpp rows each) then fall in
   // 8 distinct groups of 4 banks.
   const uint32_t ld = lpp < 8 ? rows + ((lpp + 8 - rows % 8) % 8) : rows;
   const uint32_t tw = 2 * R;
   double2* TH = v.scratch + ((uint64_t)b * v.slots + blockIdx.y) * v.scratch_elems;
-  double2* G = reinterpret_cast<double2*>(reinterpret_cast<char*>(smem) + warp * warp_work_bytes(cap));
+  double2* G = reinterpret_cast<double2*>(reinterpret_cast<char*>(smem) + slot * warp_work_bytes(cap));
   double* sig = reinterpret_cast<double*>(G + 2ull * cap * warp_ld_max(cap));
   uint32_t* perm = reinterpret_cast<uint32_t*>(sig + 2 * cap);
   double2* A = site(v, q, b);
   double2* B = site(v, q + 1, b);
   const double2 zero = make_double2(0.0, 0.0);
 
-  for (uint32_t t = lane; t < L * R; t += 32) {
+  for (uint32_t t = tl; t < L * R; t += kLanesPerRep) {
     const uint32_t l = t / R, r = t - (t / R) * R;
     double2 in[4];
     for (int i0 = 0; i0 < 2; ++i0)
@@ -467,10 +482,10 @@ __global__ void __launch_bounds__(kWarpsPer2q * 32) k_mps_2q_warp(MpsView v, uin
         else G[row * ld + col] = make_double2(acc.x, -acc.y);
       }
   }
-  __syncwarp();
+  rep_sync(bar);
 
   const double tol = (double)rows * DBL_EPSILON;
-  const uint32_t pi = (uint32_t)lane / lpp, h = (uint32_t)lane % lpp;
+  const uint32_t pi = tl / lpp, h = tl % lpp;
   const bool active = pi < np;
   for (int sweep = 0; sweep < kMaxSweeps; ++sweep) {
     bool rot = false;
@@ -511,28 +526,31 @@ __global__ void __launch_bounds__(kWarpsPer2q * 32) k_mps_2q_warp(MpsView v, uin
           gq[i] = make_double2(s * (ex * x.x - ey * x.y) + c * y.x, s * (ex * x.y + ey * x.x) + c * y.y);
         }
       }
-      __syncwarp();
+      rep_sync(bar);
     }
-    if (!__any_sync(full, rot)) break;
+    // both warps stop together: each posts its vote, the decision is the OR
+    const int vote = __any_sync(full, rot) ? 1 : 0;
+    if (lane == 0) s_any[slot][sweep & 1][wr] = vote;
+    rep_sync(bar);
+    if (!(s_any[slot][sweep & 1][0] | s_any[slot][sweep & 1][1])) break;
   }
 
-  for (uint32_t j = lane; j < cols; j += 32) {
+  for (uint32_t j = tl; j < cols; j += kLanesPerRep) {
     const double2* g = G + j * ld;
     double sq = 0.0;
     for (uint32_t i = 0; i < rows; ++i) sq += g[i].x * g[i].x + g[i].y * g[i].y;
     sig[j] = sqrt(sq);
   }
-  __syncwarp();
-  for (uint32_t j = lane; j < cols; j += 32) {
+  rep_sync(bar);
+  for (uint32_t j = tl; j < cols; j += kLanesPerRep) {
     uint32_t rank = 0;
     const double sj = sig[j];
     for (uint32_t i = 0; i < cols; ++i) rank += (sig[i] > sj || (sig[i] == sj && i < j)) ? 1u : 0u;
     perm[rank] = j;
   }
-  __syncwarp();
-  uint32_t keep = 0;
-  double scale = 1.0;
-  if (lane == 0) {
+  rep_sync(bar);
+  if (tl == 0) {
+    uint32_t keep = 0;
     for (uint32_t k = 0; k < cols; ++k) keep += sig[perm[k]] > thr ? 1u : 0u;
     keep = keep > 1u ? keep : 1u;
     if (max_keep) keep = keep < max_keep ? keep : max_keep;
@@ -542,7 +560,8 @@ __global__ void __launch_bounds__(kWarpsPer2q * 32) k_mps_2q_warp(MpsView v, uin
     for (uint32_t k = keep; k < cols; ++k) disc += sig[perm[k]] * sig[perm[k]];
     kept = fmax(sqrt(kept), 1e-15);
     total = sqrt(total);
-    scale = disc > 0.0 ? total / kept : 1.0;
+    s_scale[slot] = disc > 0.0 ? total / kept : 1.0;
+    s_keep[slot] = keep;
     if (keep > cap) {
       atomicMax(&v.flags[2], (int)keep);
       atomicMax(&v.flags[0], MF_CAPACITY);
@@ -550,11 +569,12 @@ __global__ void __launch_bounds__(kWarpsPer2q * 32) k_mps_2q_warp(MpsView v, uin
       atomicAdd(v.svd_calls, 1ull);
     }
   }
-  keep = __shfl_sync(full, keep, 0);
-  scale = __shfl_sync(full, scale, 0);
-  if (keep > cap) return;
+  rep_sync(bar);
+  const uint32_t keep = s_keep[slot];
+  const double scale = s_scale[slot];
+  if (keep > cap) return;  // the same for both warps
 
-  for (uint32_t t = lane; t < L * 2 * keep; t += 32) {
+  for (uint32_t t = tl; t < L * 2 * keep; t += kLanesPerRep) {
     const uint32_t row = t / keep, k = t - (t / keep) * keep;
     const uint32_t j = perm[k];
     const double sj = sig[j];
@@ -578,7 +598,7 @@ __global__ void __launch_bounds__(kWarpsPer2q * 32) k_mps_2q_warp(MpsView v, uin
     }
     A[(uint64_t)row * cap + k] = val;
   }
-  for (uint32_t t = lane; t < keep * 2 * R; t += 32) {
+  for (uint32_t t = tl; t < keep * 2 * R; t += kLanesPerRep) {
     const uint32_t k = t / (2 * R), col = t - (t / (2 * R)) * (2 * R);
     const uint32_t s = col / R, r = col - (col / R) * R;
     const uint32_t j = perm[k];
@@ -602,7 +622,7 @@ __global__ void __launch_bounds__(kWarpsPer2q * 32) k_mps_2q_warp(MpsView v, uin
     }
     B[(uint64_t)(k * 2 + s) * cap + r] = val;
   }
-  if (lane == 0) dm[q + 1] = keep;
+  if (tl == 0) dm[q + 1] = keep;
 }
 
 // p1 of qubit op.q by transfer matrices E_{j+1} = sum_s A_j[s]^H E_j A_j[s]
@@ -931,7 +951,7 @@ int alloc_buffers(dq_mps_s* h, uint32_t batch, uint32_t cap, uint32_t ncb) {
                                      (int)(kWarpsPer2q * warp_measure_bytes(cap))));
   if (cap <= kWarpCap)
     DQ_CUDA_TRY(cudaFuncSetAttribute(k_mps_2q_warp, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)(kWarpsPer2q * warp_work_bytes(cap))));
+                                     (int)(kRepsPer2q * warp_work_bytes(cap))));
   if (h->smem) {
     DQ_CUDA_TRY(cudaFuncSetAttribute(k_mps_2q, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)work_bytes));
@@ -1092,8 +1112,8 @@ int launch_ops(dq_mps_s* h, const std::vector<MpsOp>& ops) {
       case M_1Q: k_mps_1q<<<dim3(h->batch, count), kMpsThreads, 0, h->stream>>>(v, first); break;
       case M_2Q:
         if (warp2q)
-          k_mps_2q_warp<<<dim3((h->batch + kWarpsPer2q - 1) / kWarpsPer2q, count), kWarpsPer2q * 32,
-                          kWarpsPer2q * warp_work_bytes(h->cap), h->stream>>>(v, first, h->max_bond, h->thr);
+          k_mps_2q_warp<<<dim3((h->batch + kRepsPer2q - 1) / kRepsPer2q, count), kWarpsPer2q * 32,
+                          kRepsPer2q * warp_work_bytes(h->cap), h->stream>>>(v, first, h->max_bond, h->thr);
         else
           k_mps_2q<<<dim3(h->batch, count), t2q, shm, h->stream>>>(v, first, h->max_bond, h->thr, use);
         break;
