@@ -1220,8 +1220,8 @@ int check_mps(dq_mps_t h) {
 
 int new_handle(uint32_t n, int device, uint32_t max_bond, double thr, dq_mps_s** out) {
   if (n == 0 || n > 64) return fail(DQ_ERR_INVALID_ARG, "MPS qubit count must be in [1, 64]");
-  if (!(thr >= 0.0) || !std::isfinite(thr))
-    return fail(DQ_ERR_INVALID_ARG, "truncation_threshold must be a finite non-negative float");
+  // any threshold is accepted, as MpsSimulator::new does: a negative one keeps
+  // every singular value, NaN or +inf keeps one (s > thr is false)
   int count = 0;
   if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) return fail(DQ_ERR_NO_DEVICE, "no CUDA device");
   if (device < 0 || device >= count) return fail(DQ_ERR_INVALID_ARG, "bad device ordinal");

@@ -381,3 +381,19 @@ def test_shots_beyond_statevector_width_ghz40():
     c2 = JsonCircuit(n, insts2, ncbits=2)
     counts2 = MpsSimulator(seed=9).simulate_shots(c2, 500)
     assert set(counts2) <= {"00", "01"}
+
+
+def test_threshold_extremes_follow_the_keep_rule():
+    # negative: every singular value kept (exact state); NaN / +inf: one kept (bond 1)
+    c = brickwork_u3_cx(6, 4, seed=6)
+    prog = prog_of(c)
+    exact = _oracle.run(prog, SEED)[0]
+    _, _, edims, _ = _oracle.mps_run(prog, SEED, threshold=-1.0)
+    sv, _, dims, _ = device_run(c, SEED, thr=-1.0)
+    assert dims == edims == [1, 2, 4, 8, 4, 2, 1]
+    assert np.max(np.abs(sv - exact)) < 1e-12
+    for thr in (float("nan"), float("inf")):
+        sv1, _, d1, _ = device_run(c, SEED, thr=thr)
+        ref1, _, r1, _ = _oracle.mps_run(prog, SEED, threshold=thr)
+        assert d1 == r1 == [1] * 7
+        assert np.max(np.abs(sv1 - ref1)) < 1e-9
