@@ -293,13 +293,14 @@ def test_shots_match_oracle_per_shot():
     assert counts == ref_counts
 
 
-@pytest.mark.parametrize("max_bond", [3, 16])
-def test_large_batch_warp_steps_match_oracle(max_bond):
-    # 600 replicas per launch: the one-warp-per-replica form of the fused step
+@pytest.mark.parametrize("max_bond", [3, 16, 32])
+def test_large_batch_steps_match_oracle(max_bond):
+    # 600 replicas per launch: bonds <= 16 take the two-warps-per-replica form of
+    # the fused step, bond 32 the 256-thread CTA form
     c = trajectory_circuit(10, 9, seed=8)
     prog = prog_of(c)
     bits, st = run_mps_shots(prog, 5, 600, 0, max_bond, 1e-12)
-    assert st.replicas == 600 and st.capacity <= 16
+    assert st.replicas == 600 and st.capacity <= max(16, max_bond)
     for i in list(range(12)) + [299, 300, 599]:
         _, rcb, _, _ = _oracle.mps_run(prog, 5 + i, max_bond=max_bond)
         assert bits[i].tolist() == rcb.tolist(), i
