@@ -398,3 +398,26 @@ def test_threshold_extremes_follow_the_keep_rule():
         ref1, _, r1, _ = _oracle.mps_run(prog, SEED, threshold=thr)
         assert d1 == r1 == [1] * 7
         assert np.max(np.abs(sv1 - ref1)) < 1e-9
+
+
+def test_apply_2q_widens_a_live_handle():
+    # 10 qubits (bond bound 32, starting capacity 16): a brickwork run reaches bond 16,
+    # then long-range gates push a bond to 32, so dq_mps_apply_2q widens the live
+    # handle (dq_mps_reserve keeps its state) and redoes the overflowing step
+    c = brickwork_u3_cx(10, 6, seed=12)
+    prog = prog_of(c)
+    h = MpsHandle(10, 0, None, 1e-12)
+    h.run(prog, SEED)
+    mod = _oracle.mps_module()
+    ref, _ = mod.run(prog.insts, prog.conds, 10, prog.cbit_space, _oracle._Draws(SEED),
+                     _oracle._mps_classify)
+    swap = np.eye(4, dtype=np.complex128)[[0, 2, 1, 3]]
+    rng = np.random.default_rng(3)
+    for a, b in ((0, 9), (8, 1), (2, 7), (6, 3)):
+        u, _ = np.linalg.qr(rng.normal(size=(4, 4)) + 1j * rng.normal(size=(4, 4)))
+        h.apply_2q(a, b, u)
+        ref.apply_2q(a, b, u, swap)
+    assert max(h.bond_dims()) == 32
+    assert h.bond_dims() == ref.bond_dims()
+    assert np.max(np.abs(h.to_state().download() - ref.to_statevector())) < 1e-12
+    h.release()
