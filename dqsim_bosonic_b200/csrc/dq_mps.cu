@@ -707,9 +707,10 @@ __global__ void __launch_bounds__(kMpsThreads) k_mps_measure(MpsView v, uint32_t
   }
 }
 
-// Warp-per-replica form of k_mps_measure for large batches of small bonds
-// (capacity <= 16): the three transfer matrices of a replica (3 x cap^2) live
-// in its warp's slice of shared memory; __syncwarp orders the phases.
+// Batched form of k_mps_measure for capacity <= 16: two warps per replica
+// (joined by the replica's named barrier, as in k_mps_2q_warp), kRepsPer2q
+// replicas per CTA; the three transfer matrices of a replica (3 x cap^2) live in
+// its slice of shared memory.
 __host__ __device__ inline uint64_t warp_measure_bytes(uint32_t cap) {
   return 3ull * cap * cap * sizeof(double2);
 }
@@ -717,26 +718,30 @@ __host__ __device__ inline uint64_t warp_measure_bytes(uint32_t cap) {
 __global__ void __launch_bounds__(kWarpsPer2q * 32) k_mps_measure_warp(MpsView v, uint32_t first) {
   const MpsOp& op = v.ops[first];
   extern __shared__ double2 smem[];
+  __shared__ int s_out[kRepsPer2q];
+  __shared__ double s_sc[kRepsPer2q];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const uint32_t b = blockIdx.x * kWarpsPer2q + warp;
-  if (b >= v.batch || !cond_ok(v, op, b)) return;
-  const unsigned full = 0xffffffffu;
+  const int slot = warp / 2, wr = warp % 2;
+  const uint32_t tl = (uint32_t)(wr * 32 + lane);
+  const int bar = 1 + slot;
+  const uint32_t b = blockIdx.x * kRepsPer2q + slot;
+  if (b >= v.batch || !cond_ok(v, op, b)) return;  // the same for both warps of the replica
   const uint32_t* dm = v.dims + (uint64_t)b * (v.n + 1);
   const uint32_t cap = v.cap;
-  double2* E = smem + (uint64_t)warp * 3 * cap * cap;
+  double2* E = smem + (uint64_t)slot * 3 * cap * cap;
   double2* F = E + (uint64_t)cap * cap;
   double2* E2 = F + (uint64_t)cap * cap;
   const double2 zero = make_double2(0.0, 0.0);
-  if (lane == 0) E[0] = make_double2(1.0, 0.0);
-  __syncwarp();
+  if (tl == 0) E[0] = make_double2(1.0, 0.0);
+  rep_sync(bar);
   for (uint32_t j = 0; j < v.n; ++j) {
     const uint32_t Lj = dm[j], Rj = dm[j + 1];
     const double2* A = site(v, j, b);
-    for (uint32_t t = lane; t < Rj * Rj; t += 32) E2[t] = zero;
+    for (uint32_t t = tl; t < Rj * Rj; t += kLanesPerRep) E2[t] = zero;
     for (int s = 0; s < 2; ++s) {
       if (j == op.q && s == 0) continue;
-      __syncwarp();
-      for (uint32_t t = lane; t < Lj * Rj; t += 32) {
+      rep_sync(bar);
+      for (uint32_t t = tl; t < Lj * Rj; t += kLanesPerRep) {
         const uint32_t l = t / Rj, rp = t - (t / Rj) * Rj;
         double2 acc = zero;
         for (uint32_t lp = 0; lp < Lj; ++lp) {
@@ -746,8 +751,8 @@ __global__ void __launch_bounds__(kWarpsPer2q * 32) k_mps_measure_warp(MpsView v
         }
         F[t] = acc;
       }
-      __syncwarp();
-      for (uint32_t t = lane; t < Rj * Rj; t += 32) {
+      rep_sync(bar);
+      for (uint32_t t = tl; t < Rj * Rj; t += kLanesPerRep) {
         const uint32_t r = t / Rj, rp = t - (t / Rj) * Rj;
         double2 acc = E2[t];
         for (uint32_t l = 0; l < Lj; ++l) {
@@ -758,35 +763,34 @@ __global__ void __launch_bounds__(kWarpsPer2q * 32) k_mps_measure_warp(MpsView v
         E2[t] = acc;
       }
     }
-    __syncwarp();
-    for (uint32_t t = lane; t < Rj * Rj; t += 32) E[t] = E2[t];
-    __syncwarp();
+    rep_sync(bar);
+    for (uint32_t t = tl; t < Rj * Rj; t += kLanesPerRep) E[t] = E2[t];
+    rep_sync(bar);
   }
-  int outcome = 0;
-  double scale = 0.0;
-  if (lane == 0) {
-    double p1 = fmin(fmax(E[0].x, 0.0), 1.0);
+  if (tl == 0) {
+    const double p1 = fmin(fmax(E[0].x, 0.0), 1.0);
     const double r = chacha8_draw(v.key + (uint64_t)b * 8, v.ctr[b]);
     v.ctr[b] += 1;
-    outcome = r < p1 ? 1 : 0;
+    const int outcome = r < p1 ? 1 : 0;
     const double prob = outcome ? p1 : 1.0 - p1;
-    scale = prob > 0.0 ? 1.0 / sqrt(prob) : 0.0;
+    s_out[slot] = outcome;
+    s_sc[slot] = prob > 0.0 ? 1.0 / sqrt(prob) : 0.0;
     if (op.kind == M_MEAS && op.cbit >= 0) v.cbits[(uint64_t)b * v.ncb + op.cbit] = outcome;
   }
-  outcome = __shfl_sync(full, outcome, 0);
-  scale = __shfl_sync(full, scale, 0);
-  const double2 sc = make_double2(scale, 0.0);
+  rep_sync(bar);
+  const int outcome = s_out[slot];
+  const double2 sc = make_double2(s_sc[slot], 0.0);
   double2* A = site(v, op.q, b);
   const uint32_t L = dm[op.q], R = dm[op.q + 1];
-  for (uint32_t t = lane; t < L * 2 * R; t += 32) {
+  for (uint32_t t = tl; t < L * 2 * R; t += kLanesPerRep) {
     const uint32_t row = t / R, r = t - (t / R) * R;
     double2* p = A + (uint64_t)row * cap + r;
     *p = ((int)(row & 1u) == outcome) ? cmul_x(*p, sc) : zero;
   }
   if (op.kind == M_RESET && outcome == 1) {
-    __syncwarp();
+    rep_sync(bar);
     const double2 x1 = make_double2(1.0, 0.0);
-    for (uint32_t t = lane; t < L * R; t += 32) {
+    for (uint32_t t = tl; t < L * R; t += kLanesPerRep) {
       const uint32_t l = t / R, r = t - (t / R) * R;
       double2* p0 = A + (uint64_t)(l * 2) * cap + r;
       double2* p1 = p0 + cap;
@@ -948,7 +952,7 @@ int alloc_buffers(dq_mps_s* h, uint32_t batch, uint32_t cap, uint32_t ncb) {
   DQ_CUDA_TRY(cudaMalloc((void**)&h->scratch, sizeof(double2) * h->scratch_elems * h->slots * batch));
   if (cap <= kWarpCap)
     DQ_CUDA_TRY(cudaFuncSetAttribute(k_mps_measure_warp, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)(kWarpsPer2q * warp_measure_bytes(cap))));
+                                     (int)(kRepsPer2q * warp_measure_bytes(cap))));
   if (cap <= kWarpCap)
     DQ_CUDA_TRY(cudaFuncSetAttribute(k_mps_2q_warp, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)(kRepsPer2q * warp_work_bytes(cap))));
@@ -1119,8 +1123,8 @@ int launch_ops(dq_mps_s* h, const std::vector<MpsOp>& ops) {
         break;
       case M_MEAS: case M_RESET:
         if (warp2q)
-          k_mps_measure_warp<<<(h->batch + kWarpsPer2q - 1) / kWarpsPer2q, kWarpsPer2q * 32,
-                               kWarpsPer2q * warp_measure_bytes(h->cap), h->stream>>>(v, first);
+          k_mps_measure_warp<<<(h->batch + kRepsPer2q - 1) / kRepsPer2q, kWarpsPer2q * 32,
+                               kRepsPer2q * warp_measure_bytes(h->cap), h->stream>>>(v, first);
         else
           k_mps_measure<<<h->batch, kMpsThreads, shm, h->stream>>>(v, first, use);
         break;
