@@ -105,11 +105,16 @@ class ClockSampler:
     def __init__(self, device: int):
         self.device = device
         self.proc = None
-        self.path = ROOT / "gpurun_out" / f"clocks_dev{device}_{os.getpid()}.csv"
+        # raw samples go to $DQSIM_CLOCKS_DIR (default: the system temp directory);
+        # the JSON line carries their summary
+        import tempfile
+
+        base = Path(os.environ.get("DQSIM_CLOCKS_DIR", tempfile.gettempdir()))
+        self.path = base / f"dqsim_clocks_dev{device}_{os.getpid()}.csv"
 
     def __enter__(self):
         try:
-            self.path.parent.mkdir(exist_ok=True)
+            self.path.parent.mkdir(parents=True, exist_ok=True)
             self.fh = open(self.path, "w")
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
