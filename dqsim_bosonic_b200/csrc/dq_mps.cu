@@ -153,12 +153,21 @@ __device__ __forceinline__ double warp_sum(double x) {
 // (2 |gamma|), c = 1 / sqrt(1 + t^2), s = c t, which zeroes a_p'^H a_q'.  The
 // reciprocal square roots keep the dependent chain at four special-function
 // operations.
+//
+// A pair of negligible columns (both |a|^2 <= neg = (rows eps)^2 |theta|_F^2,
+// at the rounding level of theta) is left alone: their mutual directions carry
+// no information and rotating them again and again only delays convergence of
+// a rank-deficient theta.  A negligible column is still rotated against every
+// significant one, so it ends up orthogonal to the significant subspace (it
+// may be kept when the threshold keeps everything).
 __device__ __forceinline__ bool jacobi_rotation(double al, double be, double gr, double gi, double tol,
-                                                double& c, double& s, double& ex, double& ey) {
+                                                double neg, double& c, double& s, double& ex, double& ey) {
   const double g2 = gr * gr + gi * gi;
   if (!(g2 > 0.0)) return false;
+  if (al <= neg && be <= neg) return false;
+  const double nab = sqrt(al) * sqrt(be);
   const double inv = rsqrt(g2);
-  if (!(g2 * inv > tol * sqrt(al) * sqrt(be))) return false;
+  if (!(g2 * inv > tol * nab)) return false;
   const double zeta = 0.5 * (be - al) * inv;
   const double t = (zeta >= 0.0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
   c = rsqrt(1.0 + t * t);
@@ -197,6 +206,8 @@ __global__ void __launch_bounds__(1024) k_mps_2q(MpsView v, uint32_t first, uint
   __shared__ int s_rot;
   __shared__ uint32_t s_keep;
   __shared__ double s_scale;
+  __shared__ double s_part[32];
+  __shared__ double s_n2;
   const uint32_t b = blockIdx.x;
   if (!cond_ok(v, op, b)) return;
   uint32_t* dm = v.dims + (uint64_t)b * (v.n + 1);
@@ -215,6 +226,7 @@ __global__ void __launch_bounds__(1024) k_mps_2q(MpsView v, uint32_t first, uint
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
 
   // ---- theta -> TH (row-major) and G (column-major) ---------------------------
+  double n2loc = 0.0;  // |theta|_F^2, for the negligible-pair test
   for (uint32_t t = tid; t < L * R; t += blockDim.x) {
     const uint32_t l = t / R, r = t - (t / R) * R;
     double2 in[4];
@@ -233,15 +245,25 @@ __global__ void __launch_bounds__(1024) k_mps_2q(MpsView v, uint32_t first, uint
         for (int i = 0; i < 4; ++i) acc = cadd_x(acc, cmul_x(op.u[o * 4 + i], in[i]));
         const uint32_t row = l * 2 + o0, col = o1 * R + r;
         TH[(uint64_t)row * tw + col] = acc;
+        n2loc += acc.x * acc.x + acc.y * acc.y;
         if (!tr) G[(uint64_t)col * rows + row] = acc;
         else G[(uint64_t)row * rows + col] = make_double2(acc.x, -acc.y);
       }
   }
+  n2loc = warp_sum(n2loc);
+  if (lane == 0) s_part[warp] = n2loc;
   if (tid == 0) s_rot = 0;
+  __syncthreads();
+  if (tid == 0) {
+    double n2 = 0.0;
+    for (int w = 0; w < nw; ++w) n2 += s_part[w];
+    s_n2 = n2;
+  }
   __syncthreads();
 
   // ---- one-sided Jacobi --------------------------------------------------------
   const double tol = (double)rows * DBL_EPSILON;
+  const double neg = tol * tol * s_n2;
   const uint32_t np = cols / 2;
   // more pairs than warps: two lane groups of 16 lanes, one pair each, so that
   // two of a warp's pairs run side by side (narrower groups would leave each
@@ -282,7 +304,7 @@ __global__ void __launch_bounds__(1024) k_mps_2q(MpsView v, uint32_t first, uint
           gi += __shfl_xor_sync(0xffffffffu, gi, o);
         }
         double c, s, ex, ey;
-        if (active && jacobi_rotation(al, be, gr, gi, tol, c, s, ex, ey)) {
+        if (active && jacobi_rotation(al, be, gr, gi, tol, neg, c, s, ex, ey)) {
           if (h == 0) s_rot = 1;
           for (uint32_t i = h; i < rows; i += lpp) {
             const double2 x = gp[i], y = gq[i];
@@ -431,6 +453,7 @@ __global__ void __launch_bounds__(kWarpsPer2q * 32) k_mps_2q_warp(MpsView v, uin
   __shared__ int s_any[kRepsPer2q][2][2];   // [slot][sweep parity][warp]
   __shared__ uint32_t s_keep[kRepsPer2q];
   __shared__ double s_scale[kRepsPer2q];
+  __shared__ double s_n2[kRepsPer2q][2];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int slot = warp / 2, wr = warp % 2;          // replica slot in the CTA, warp within it
   const uint32_t tl = (uint32_t)(wr * 32 + lane);    // lane within the replica (0..63)
@@ -460,6 +483,7 @@ __global__ void __launch_bounds__(kWarpsPer2q * 32) k_mps_2q_warp(MpsView v, uin
   double2* B = site(v, q + 1, b);
   const double2 zero = make_double2(0.0, 0.0);
 
+  double n2loc = 0.0;  // |theta|_F^2, for the negligible-pair test
   for (uint32_t t = tl; t < L * R; t += kLanesPerRep) {
     const uint32_t l = t / R, r = t - (t / R) * R;
     double2 in[4];
@@ -478,13 +502,17 @@ __global__ void __launch_bounds__(kWarpsPer2q * 32) k_mps_2q_warp(MpsView v, uin
         for (int i = 0; i < 4; ++i) acc = cadd_x(acc, cmul_x(op.u[o * 4 + i], in[i]));
         const uint32_t row = l * 2 + o0, col = o1 * R + r;
         TH[(uint64_t)row * tw + col] = acc;
+        n2loc += acc.x * acc.x + acc.y * acc.y;
         if (!tr) G[col * ld + row] = acc;
         else G[row * ld + col] = make_double2(acc.x, -acc.y);
       }
   }
+  n2loc = warp_sum(n2loc);
+  if (lane == 0) s_n2[slot][wr] = n2loc;
   rep_sync(bar);
 
   const double tol = (double)rows * DBL_EPSILON;
+  const double neg = tol * tol * (s_n2[slot][0] + s_n2[slot][1]);
   const uint32_t pi = tl / lpp, h = tl % lpp;
   const bool active = pi < np;
   for (int sweep = 0; sweep < kMaxSweeps; ++sweep) {
@@ -518,7 +546,7 @@ __global__ void __launch_bounds__(kWarpsPer2q * 32) k_mps_2q_warp(MpsView v, uin
         gi += __shfl_xor_sync(full, gi, o);
       }
       double c, s, ex, ey;
-      if (active && jacobi_rotation(al, be, gr, gi, tol, c, s, ex, ey)) {
+      if (active && jacobi_rotation(al, be, gr, gi, tol, neg, c, s, ex, ey)) {
         rot = true;
         for (uint32_t i = h; i < rows; i += lpp) {
           const double2 x = gp[i], y = gq[i];
