@@ -381,7 +381,8 @@ def main():
                                exec="per_gate" if exec_mode == nat.EXEC_PER_GATE else "fused")
     n = prog.num_qubits
     top = list(range(n - 1, max(-1, n - 11), -1))
-    for _ in range(2):
+    # untimed warm-up of the host path (a freshly started box is noisy for a while)
+    for _ in range(max(5, args.warmup)):
         res = sim.simulate(circ)
         res.probability_array(top)
         del res
