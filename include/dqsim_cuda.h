@@ -392,7 +392,9 @@ DQ_API int dq_mps_run(dq_mps_t h, const dq_inst* prog, uint64_t ninst, const dq_
 /* Mps::apply_2q (:115-135) on the current state: u = 4x4 row-major complex
  * (interleaved re/im, 32 doubles), a = most significant qubit of the row. */
 DQ_API int dq_mps_apply_2q(dq_mps_t h, uint32_t a, uint32_t b, const double* u);
-/* Widen the bond capacity of a single-state handle, keeping its state. */
+/* Widen the bond capacity of a single-state handle, keeping its state, bond
+ * dimensions and RNG position (its classical bits are not kept: a later
+ * dq_mps_run starts them afresh). */
 DQ_API int dq_mps_reserve(dq_mps_t h, uint32_t capacity);
 DQ_API int dq_mps_bond_dims(dq_mps_t h, uint32_t* dims);   /* n + 1 entries */
 DQ_API int dq_mps_to_state(dq_mps_t h, dq_state_t out);
