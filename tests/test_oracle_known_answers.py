@@ -165,7 +165,7 @@ def test_fuse_flushes_before_touching_instruction():
 
 
 def test_golden_fixtures():
-    files = sorted(GOLDEN.glob("*.json"))
+    files = sorted(f for f in GOLDEN.glob("*.json") if not f.name.startswith("amp_"))
     assert files, "golden fixtures missing"
     for f in files:
         fx = json.loads(f.read_text())
