@@ -110,6 +110,9 @@ class SimulationResult:
         self._cbits = cbits
         self._profile = profile
         self.last_boundary_draws = 0
+        # host-side phase times (ms) of the call that made this result and of
+        # its latest probability query: parse, state, run, engine, query
+        self.timings: dict[str, float] = {}
 
     @property
     def statevector(self) -> np.ndarray:
@@ -130,10 +133,12 @@ class SimulationResult:
         return self._state
 
     def _marginal(self, qs: list[int]) -> np.ndarray:
+        t0 = time.perf_counter()
         out = np.empty(1 << len(qs), dtype=np.float64)
         q = np.asarray(qs, dtype=np.uint32)
         nat.check(nat.lib().dq_marginal_probs(self._state.handle, nat.ptr(q), len(qs), nat.ptr(out)),
                   "dq_marginal_probs")
+        self.timings["query_ms"] = (time.perf_counter() - t0) * 1e3
         return out
 
     def probability_array(self, qubits=None) -> np.ndarray:
@@ -246,16 +251,23 @@ class StatevectorSimulator:
 
     def simulate(self, circuit) -> SimulationResult:
         """Run the circuit and return a ``SimulationResult``."""
-        prog, _ = _parse(circuit)
+        prog, parse_s = _parse(circuit)
         seed = self._seed if self._seed is not None else _entropy_u64()
+        t0 = time.perf_counter()
         state = nat.State(prog.num_qubits, self.device)
+        t1 = time.perf_counter()
         exec_mode = nat.EXEC_PER_GATE if self._profile else self._exec
         cbits, prof = run_program(state, prog, seed, nat.SEM_SIMULATE, exec_mode, self.fusion_width,
                                   self._profile)
+        t2 = time.perf_counter()
         cb = {i: int(v) for i, v in enumerate(cbits.tolist()) if v >= 0}
         res = SimulationResult(state, prog.num_qubits, cb,
                                SimulationProfile(prof) if self._profile else None)
         res.last_boundary_draws = int(prof.boundary_draws)
+        # run_ms: the dq_run call (it returns once the state is final);
+        # engine_ms: the engine's own clock inside that call
+        res.timings = {"parse_ms": parse_s * 1e3, "state_ms": (t1 - t0) * 1e3,
+                       "run_ms": (t2 - t1) * 1e3, "engine_ms": float(prof.total_time) * 1e3}
         return res
 
     def simulate_shots(self, circuit, shots=1000, profile=False) -> dict[str, int]:
