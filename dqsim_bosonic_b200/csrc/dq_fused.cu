@@ -1,14 +1,8 @@
 // dq_fused.cu — the tile-sweep engine: planner (host) and sweep kernel (sm_100a).
 //
-// Kernel geometry.  A tile holds 2^m amplitudes (m = 7 + RB local qubits,
-// RB = register bits per thread, m <= 12, 64 KiB of FP64 complex at m = 12).
-// 128 threads per CTA, 3 CTAs per SM.  Local bit k of a tile is physical
-// qubit local_pos[k] (ascending); local bits 0..4 are qubits 0..4, so a tile
-// is made of 2^(m-5) runs of 32 consecutive amplitudes (512 B) that a warp
-// moves with one coalesced cp.async each.  In shared memory the element
-// index is XOR-swizzled (low 3 bits ^= a linear function of the high bits)
-// so that any 7 of the 12 local bits can serve as thread bits without bank
-// conflicts.
+// The device side (tile geometry, the encoded program layout, the per-op
+// register arithmetic and the per-CTA tile loop) is in dq_sweep.cuh.  The
+// default launch runs 128 threads per CTA, three CTAs per SM.
 //
 // A sweep is a list of phases.  In a phase each thread holds 2^RB amplitudes
 // in registers: the ones whose RB "register" local bits vary, at the thread
@@ -38,445 +32,37 @@
 #include "dq_common.cuh"
 #include "dq_fused.cuh"
 #include "dq_gates.hpp"
+#include "dq_sweep.cuh"
 
 namespace dq {
 
 namespace {
 
-// Thread geometry: TB thread bits (5 lane + TB-5 warp bits), 2^TB threads per
-// CTA.  TB = 7: 128 threads, two CTAs per SM (their phases overlap); TB = 8:
-// 256 threads, one CTA per SM.
-constexpr int kMaxTB = 8;
-constexpr int kMaxM = 12;
-constexpr int kMaxSlots = 128;
-// bytes of one sweep program (staged in shared memory next to two tile buffers)
-// Largest staged sweep program for a tile of 2^m amplitudes: what is left of
-// shared memory next to two tile buffers at the CTAs per SM the geometry runs.
-__host__ __device__ constexpr int max_prog(int m) { return m >= 12 ? 64 * 1024 : 40 * 1024; }
-
-enum : uint32_t { OP_U1 = 0, OP_U1R, OP_U1X, OP_U2, OP_FLUSH_R, OP_FLUSH_T, OP_GPHASE, OP_U1H,
-                  OP_SCALE };
-
-// swizzle vectors of local bits 3..11 (bits 0..2 map to themselves)
-__host__ __device__ constexpr uint32_t swz_g(int k) {
-  return k == 3 ? 3u : k == 4 ? 5u : k == 5 ? 6u : k == 6 ? 7u : k == 7 ? 3u : k == 8 ? 5u
-       : k == 9 ? 6u : k == 10 ? 7u : k == 11 ? 1u : 0u;
-}
-__host__ __device__ constexpr uint32_t swz_vec(int k) { return k < 3 ? (1u << k) : swz_g(k); }
-__host__ __device__ constexpr uint32_t swz(uint32_t e) {
-  uint32_t g = 0;
-  for (int k = 3; k < kMaxM; ++k)
-    if ((e >> k) & 1u) g ^= swz_g(k);
-  return e ^ g;
-}
-
-// ---- sweep program layout (copied verbatim into shared memory) ----------------
-constexpr int kMaxRuns = 1 << (kMaxM - 5);
-
-struct SwHeader {
-  uint32_t m, rb, nphase, nslots;
-  uint32_t local_pos[kMaxM];
-  uint32_t off_phase, off_op, off_slot, off_slotent;
-  uint32_t off_data, prog_bytes;
-  uint32_t tile_xload;         // XORed into every tile-load address: X gates opening the sweep
-  uint32_t pad2;
-  uint64_t runoff[kMaxRuns];   // physical offset of run r (local bits 5..m-1 = r)
-  uint32_t runswz[kMaxRuns];   // swizzled shared-memory index of run r's first element
-};
-struct SwPhase {
-  uint32_t lanesw[32];         // swizzled local index of the lane bits (thread bits 0..4)
-  uint32_t warpsw[8];          // swizzled local index of the warp bits (thread bits 5..7)
-  uint32_t V[4];               // swizzled local index of each register bit
-  uint32_t op_begin, op_end;
-  uint32_t xload;              // XORed into every load address: X gates folded into the load
-  uint32_t pad1;
-};
-// 32 bytes, read as two 128-bit words: w0 = type | b0 << 8 | b1 << 16 | creg << 24,
-// w1 = ctl_thr | flags << 8 | slot << 16, data = first DATA entry, cnl = non-local controls
-struct SwOp {
-  uint32_t w0, w1, data, pad;
-  uint64_t cnl, pad2;
-};
-struct SwSlot {
-  uint32_t count, start, pad0, pad1;
-  double2 w0;
-};
-struct SwSlotEnt {
-  uint64_t mask, pad;
-  double2 w;
-};
-static_assert(sizeof(SwHeader) % 16 == 0 && sizeof(SwPhase) % 16 == 0, "layout");
-static_assert(sizeof(SwOp) % 16 == 0 && sizeof(SwSlot) % 16 == 0 && sizeof(SwSlotEnt) % 16 == 0,
-              "layout");
-
-// FLUSH flags: thread-partner tables present (32 lane + 8 warp factors), then
-// a register-partner table (2^(RB-1) entries for a register target, 2^RB for
-// a thread target).
-constexpr uint32_t FL_THR = 1u;
-constexpr uint32_t FL_REG = 2u;
-constexpr uint32_t FL_PRE = 4u;   // 1q op: flush its target first (data = 4 matrix entries, then flush tables)
-
-// ---- device helpers -------------------------------------------------------------------
-
-// Hide a value's provenance from the optimiser so that addresses are
-// recomputed instead of being kept live (in registers) across a phase.
-__device__ __forceinline__ uint32_t opaque(uint32_t x) {
-  asm volatile("" : "+r"(x));
-  return x;
-}
-__device__ __forceinline__ uint64_t opaque64(uint64_t x) {
-  asm volatile("" : "+l"(x));
-  return x;
-}
-
-__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
-  const uint32_t sa = (uint32_t)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
-}
-
-// One-qubit op on register bit B, optionally preceded by the flush of B
-// (amplitudes with bit B set times W * F[compress(j)]).  KIND: 0 general
-// 2x2, 1 real 2x2, 2 [[1,1],[1,-1]], 3 X.  Controls only occur without a
-// pre-flush (the planner fuses flushes into uncontrolled ops only).
-template <int RB, int B, int KIND, bool PRE>
-__device__ __forceinline__ void u1_op(double2 (&a)[1 << RB], const double2* __restrict__ D,
-                                      uint32_t creg, double2 W, const double2* __restrict__ F) {
-  double2 u00, u01, u10, u11;
-  if (KIND <= 1) {
-    u00 = D[0]; u01 = D[1]; u10 = D[2]; u11 = D[3];
-  }
-#pragma unroll
-  for (int j = 0; j < (1 << RB); ++j) {
-    if (j & (1 << B)) continue;
-    if (!PRE && (j & creg) != creg) continue;
-    const int k = j | (1 << B);
-    const double2 x = a[j];
-    double2 y = a[k];
-    if (PRE) {
-      const int idx = ((k >> (B + 1)) << B) | (k & ((1 << B) - 1));
-      y = cmul_f(y, F ? cmul_f(W, F[idx]) : W);
-    }
-    if (KIND == 0) {
-      a[j] = cmac2_f(u00, x, u01, y);
-      a[k] = cmac2_f(u10, x, u11, y);
-    } else if (KIND == 1) {
-      a[j] = make_double2(fma(u00.x, x.x, u01.x * y.x), fma(u00.x, x.y, u01.x * y.y));
-      a[k] = make_double2(fma(u10.x, x.x, u11.x * y.x), fma(u10.x, x.y, u11.x * y.y));
-    } else if (KIND == 2) {
-      a[j] = make_double2(x.x + y.x, x.y + y.y);
-      a[k] = make_double2(x.x - y.x, x.y - y.y);
-    } else {
-      a[j] = y;
-      a[k] = x;
-    }
-  }
-}
-
-// dense 4x4 on register bits B0 (MSB of the gate index) and B1
-template <int RB, int B0, int B1>
-__device__ __forceinline__ void u2_gen(double2 (&a)[1 << RB], const double2* __restrict__ D,
-                                       uint32_t creg) {
-#pragma unroll
-  for (int j = 0; j < (1 << RB); ++j) {
-    if (j & ((1 << B0) | (1 << B1))) continue;
-    if ((j & creg) != creg) continue;
-    const int i0 = j, i1 = j | (1 << B1), i2 = j | (1 << B0), i3 = j | (1 << B0) | (1 << B1);
-    const double2 v0 = a[i0], v1 = a[i1], v2 = a[i2], v3 = a[i3];
-#pragma unroll
-    for (int r = 0; r < 4; ++r) {
-      const double2 s01 = cmac2_f(D[4 * r], v0, D[4 * r + 1], v1);
-      const double2 s23 = cmac2_f(D[4 * r + 2], v2, D[4 * r + 3], v3);
-      const double2 w = make_double2(s01.x + s23.x, s01.y + s23.y);
-      if (r == 0) a[i0] = w;
-      else if (r == 1) a[i1] = w;
-      else if (r == 2) a[i2] = w;
-      else a[i3] = w;
-    }
-  }
-}
-
-// flush on register bit B: a[j] *= W * F[compress(j)] for j with bit B set
-template <int RB, int B>
-__device__ __forceinline__ void flush_reg(double2 (&a)[1 << RB], double2 W,
-                                          const double2* __restrict__ F) {
-#pragma unroll
-  for (int j = 0; j < (1 << RB); ++j) {
-    if (!(j & (1 << B))) continue;
-    if (F) {
-      const int idx = ((j >> (B + 1)) << B) | (j & ((1 << B) - 1));
-      a[j] = cmul_f(a[j], cmul_f(W, F[idx]));
-    } else {
-      a[j] = cmul_f(a[j], W);
-    }
-  }
-}
-
-#define DQ_SW_CASES1(FN, ...)                                          \
-  switch (b0) {                                                        \
-    case 0: FN<RB, 0>(__VA_ARGS__); break;                             \
-    case 1: if (RB > 1) FN<RB, (RB > 1 ? 1 : 0)>(__VA_ARGS__); break;  \
-    case 2: if (RB > 2) FN<RB, (RB > 2 ? 2 : 0)>(__VA_ARGS__); break;  \
-    case 3: if (RB > 3) FN<RB, (RB > 3 ? 3 : 0)>(__VA_ARGS__); break;  \
-    default: break;                                                    \
-  }
-
-#define DQ_SW_U1(KIND, PRE)                                                                  \
-  switch (b0) {                                                                              \
-    case 0: u1_op<RB, 0, KIND, PRE>(a, D, creg, W, F); break;                                \
-    case 1: if (RB > 1) u1_op<RB, (RB > 1 ? 1 : 0), KIND, PRE>(a, D, creg, W, F); break;     \
-    case 2: if (RB > 2) u1_op<RB, (RB > 2 ? 2 : 0), KIND, PRE>(a, D, creg, W, F); break;     \
-    case 3: if (RB > 3) u1_op<RB, (RB > 3 ? 3 : 0), KIND, PRE>(a, D, creg, W, F); break;     \
-    default: break;                                                                          \
-  }
-
-template <int RB>
-__device__ __forceinline__ void u2_dispatch(double2 (&a)[1 << RB], uint32_t b0, uint32_t b1,
-                                            uint32_t creg, const double2* __restrict__ D) {
-#define DQ_U2C(X, Y)                                                                      \
-  if (b0 == X && b1 == Y) {                                                               \
-    if (RB > X && RB > Y) u2_gen<RB, (RB > X ? X : 0), (RB > Y ? Y : 1)>(a, D, creg);     \
-    return;                                                                               \
-  }
-  DQ_U2C(0, 1) DQ_U2C(0, 2) DQ_U2C(0, 3) DQ_U2C(1, 2) DQ_U2C(1, 3) DQ_U2C(2, 3)
-#undef DQ_U2C
-}
-
-template <int RB>
-__device__ __forceinline__ void exec_op(const uint4 o0, const uint4 o1, double2 (&a)[1 << RB],
-                                        const double2* __restrict__ DATA,
-                                        const double2* __restrict__ slots, uint32_t tid,
-                                        uint64_t base) {
-  const uint32_t type = o0.x & 0xffu, b0 = (o0.x >> 8) & 0xffu, b1 = (o0.x >> 16) & 0xffu;
-  const uint32_t creg = o0.x >> 24, ctl = o0.y & 0xffu, flags = (o0.y >> 8) & 0xffu;
-  const uint32_t slot = o0.y >> 16;
-  const uint64_t cnl = ((uint64_t)o1.y << 32) | o1.x;
-  if ((base & cnl) != cnl) return;
-  if ((tid & ctl) != ctl) return;
-  const double2* D = DATA + o0.z;
-  // flush factors (FLUSH ops and pre-flushed one-qubit ops)
-  double2 W = make_double2(1.0, 0.0);
-  const double2* F = nullptr;
-  const bool is_u1 = type == OP_U1 || type == OP_U1R || type == OP_U1H || type == OP_U1X;
-  if ((flags & FL_PRE) || type == OP_FLUSH_R || type == OP_FLUSH_T || type == OP_GPHASE) {
-    W = slots[slot];
-    const double2* T = is_u1 ? D + 4 : D;
-    if (flags & FL_THR) {
-      W = cmul_f(W, cmul_f(T[tid & 31u], T[32 + (tid >> 5)]));
-      T += 40;
-    }
-    if (flags & FL_REG) F = T;
-  }
-  switch (type) {
-    case OP_U1: if (flags & FL_PRE) { DQ_SW_U1(0, true) } else { DQ_SW_U1(0, false) } break;
-    case OP_U1R: if (flags & FL_PRE) { DQ_SW_U1(1, true) } else { DQ_SW_U1(1, false) } break;
-    case OP_U1H: if (flags & FL_PRE) { DQ_SW_U1(2, true) } else { DQ_SW_U1(2, false) } break;
-    case OP_U1X: if (flags & FL_PRE) { DQ_SW_U1(3, true) } else { DQ_SW_U1(3, false) } break;
-    case OP_U2: u2_dispatch<RB>(a, b0, b1, creg, D); break;
-    case OP_FLUSH_R: DQ_SW_CASES1(flush_reg, a, W, F); break;
-    case OP_FLUSH_T:
-      if (!((tid >> b0) & 1u)) break;
-      if (F) {
-#pragma unroll
-        for (int j = 0; j < (1 << RB); ++j) a[j] = cmul_f(a[j], cmul_f(W, F[j]));
-      } else {
-#pragma unroll
-        for (int j = 0; j < (1 << RB); ++j) a[j] = cmul_f(a[j], W);
-      }
-      break;
-    case OP_GPHASE:
-#pragma unroll
-      for (int j = 0; j < (1 << RB); ++j) a[j] = cmul_f(a[j], W);
-      break;
-    case OP_SCALE: {
-      const double f = D[0].x;
-#pragma unroll
-      for (int j = 0; j < (1 << RB); ++j) a[j] = make_double2(a[j].x * f, a[j].y * f);
-      break;
-    }
-    default: break;
-  }
-}
-
-// One persistent CTA per SM walks tiles blockIdx.x, + gridDim.x, ...: the
-// next tile is prefetched (cp.async into the second buffer) while the
-// current one is computed.
-// S tile buffers form a cp.async pipeline with S - 1 tiles prefetched while
-// the current one is computed.  S = 2: two CTAs per SM whenever a tile is at
-// most 2^11 amplitudes; S = 1 (128 threads): no prefetch, three CTAs per SM
-// overlap each other's loads instead.
-template <int TB, int RB, int S>
-__global__ void __launch_bounds__(1 << TB, (S == 1 && TB == 7 ? 3 : (TB + RB <= 11 ? 2 : 1)))
+// One persistent CTA per SM walks tiles blockIdx.x, + gridDim.x, ...
+// S = 1 (128 threads): no prefetch, three CTAs per SM overlap each other's
+// loads.  S = 2: the next tile's load is in flight while the current one is
+// computed.  PG: the sweep program is read where it lies in global memory (a
+// few KB, L1-resident after the first tile) instead of being staged in
+// shared memory, which leaves room for two tile buffers at three CTAs per SM.
+template <int TB, int RB, int S, bool PG, int RUNB>
+__global__ void __launch_bounds__(1 << TB, ((S == 1 || PG) && TB == 7 ? 3 : (TB + RB <= 11 ? 2 : 1)))
     k_sweep(double2* __restrict__ state, const uint8_t* __restrict__ gprog, uint32_t prog_bytes,
             uint32_t ntiles, long long synth) {
-  constexpr int kSwThreads = 1 << TB;
-  constexpr int kSwTB = TB;
-  constexpr int M = kSwTB + RB;
-  constexpr int T = 1 << M;
-  constexpr int R = 1 << RB;
-  constexpr int NI = 1 << (M - kSwTB);  // runs of 32 per warp
-  constexpr uint32_t NW = 1u << (TB - 5);  // warps
+  constexpr int T = 1 << (TB + RB);
   extern __shared__ __align__(16) unsigned char smraw[];
   double2* bufs = reinterpret_cast<double2*>(smraw);  // S tiles
   double2* slots = bufs + S * T;
-  uint8_t* prog = reinterpret_cast<uint8_t*>(slots + kMaxSlots);
-  const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
-
-  for (uint32_t i = tid * 16u; i < prog_bytes; i += kSwThreads * 16u)
-    *reinterpret_cast<uint4*>(prog + i) = __ldg(reinterpret_cast<const uint4*>(gprog + i));
-  __syncthreads();
-  const SwHeader* H = reinterpret_cast<const SwHeader*>(prog);
-  const SwPhase* PH = reinterpret_cast<const SwPhase*>(prog + H->off_phase);
-  const SwOp* OPS = reinterpret_cast<const SwOp*>(prog + H->off_op);
-  const SwSlot* SL = reinterpret_cast<const SwSlot*>(prog + H->off_slot);
-  const SwSlotEnt* SE = reinterpret_cast<const SwSlotEnt*>(prog + H->off_slotent);
-  const double2* DATA = reinterpret_cast<const double2*>(prog + H->off_data);
-  const uint32_t nph = H->nphase, nslots = H->nslots;
-  const uint32_t swl = swz(lane);  // lane part of a run element's index (bits 0..4)
-
-  auto tile_base = [&](uint32_t t) {
-    uint64_t b = t;
-#pragma unroll
-    for (int k = 0; k < M; ++k) b = insert_zero(b, H->local_pos[k]);
-    return b;
-  };
-  // Tile bases advance by the grid stride without re-depositing: with the
-  // local positions filled with ones a carry runs across them, so
-  // deposit(t + g) = ((deposit(t) | lmask) + deposit(g)) & ~lmask.
-  uint64_t lmask = 0;
-#pragma unroll
-  for (int k = 0; k < M; ++k) lmask |= 1ULL << H->local_pos[k];
-  const uint64_t bstride = tile_base(gridDim.x);
-  auto advance = [&](uint64_t b) { return ((b | lmask) + bstride) & ~lmask; };
-  // run r = warp + 8 i: all of a tile's 2^(m-5) runs of 32 amplitudes; one
-  // commit group per call (empty past the last tile, so the group count is
-  // uniform).  synth >= 0: the state is the basis vector |synth> not yet
-  // written to memory, so the tile is generated instead of read.
-  auto load_tile = [&](uint32_t t, uint64_t b, double2* dst) {
-    if (t < ntiles) {
-#pragma unroll
-      for (int i = 0; i < NI; ++i) {
-        const uint32_t r = warp + (uint32_t)i * NW;
-        const uint64_t g = b + H->runoff[r] + lane;
-        double2* d = &dst[H->runswz[r] ^ swl ^ H->tile_xload];
-        if (synth >= 0)
-          *d = make_double2(g == (uint64_t)synth ? 1.0 : 0.0, 0.0);
-        else
-          cp_async16(d, state + g);
-      }
-    }
-    cp_async_commit();
-  };
-
-  uint32_t tile = blockIdx.x;
-  uint64_t base = tile_base(tile);  // this iteration's tile
-  uint64_t bpre = base;             // the newest prefetched tile
-#pragma unroll
-  for (int k = 0; k < S - 1; ++k) {
-    load_tile(tile + (uint32_t)k * gridDim.x, bpre, bufs + k * T);
-    bpre = advance(bpre);
-  }
-  for (uint32_t it = 0; tile < ntiles; ++it, tile += gridDim.x) {
-    double2* cur = bufs + (it % S) * T;
-    // tile it + S - 1 goes into the buffer that tile it - 1 used (stored and
-    // released by the barrier that ended the previous iteration)
-    load_tile(tile + (uint32_t)(S - 1) * gridDim.x, bpre, bufs + ((it + S - 1) % S) * T);
-    bpre = advance(bpre);
-    // per-tile phase factors: few slots with many entries take a warp
-    // each (lane products, then a butterfly over the lanes); otherwise one
-    // thread per slot
-    if (nslots <= 4 * NW) {
-      for (uint32_t s = warp; s < nslots; s += NW) {
-        const uint32_t c = SL[s].count, st = SL[s].start;
-        double2 w = make_double2(1.0, 0.0);
-        for (uint32_t e = lane; e < c; e += 32) {
-          const SwSlotEnt& E = SE[st + e];
-          if ((base & E.mask) == E.mask) w = cmul_f(w, E.w);
-        }
-        if (c > 1) {
-#pragma unroll
-          for (int o = 16; o > 0; o >>= 1) {
-            const double2 q = make_double2(__shfl_xor_sync(0xffffffffu, w.x, o),
-                                           __shfl_xor_sync(0xffffffffu, w.y, o));
-            w = cmul_f(w, q);
-          }
-        }
-        if (lane == 0) slots[s] = cmul_f(SL[s].w0, w);
-      }
-    } else {
-      for (uint32_t s = tid; s < nslots; s += kSwThreads) {
-        double2 w = SL[s].w0;
-        const uint32_t c = SL[s].count, st = SL[s].start;
-        for (uint32_t e = 0; e < c; ++e) {
-          const SwSlotEnt& E = SE[st + e];
-          if ((base & E.mask) == E.mask) w = cmul_f(w, E.w);
-        }
-        slots[s] = w;
-      }
-    }
-    cp_async_wait<S - 1>();  // this tile's group is complete; S - 1 newer may be pending
+  const uint8_t* prog;
+  if (PG) {
+    prog = gprog;
+  } else {
+    uint8_t* sprog = reinterpret_cast<uint8_t*>(slots + kMaxSlots);
+    for (uint32_t i = threadIdx.x * 16u; i < prog_bytes; i += (1u << TB) * 16u)
+      *reinterpret_cast<uint4*>(sprog + i) = __ldg(reinterpret_cast<const uint4*>(gprog + i));
     __syncthreads();
-
-    for (uint32_t p = 0; p < nph; ++p) {
-      const SwPhase& P = PH[p];
-      const uint32_t pt = P.lanesw[lane] ^ P.warpsw[warp];
-      const uint32_t ptl = pt ^ P.xload;
-      uint32_t V[RB];
-#pragma unroll
-      for (int b = 0; b < RB; ++b) V[b] = P.V[b];
-      double2 a[R];
-#pragma unroll
-      for (int j = 0; j < R; ++j) {
-        uint32_t x = ptl;
-#pragma unroll
-        for (int b = 0; b < RB; ++b)
-          if ((j >> b) & 1) x ^= V[b];
-        a[j] = cur[x];
-      }
-      const uint32_t ob = P.op_begin, oe = P.op_end;
-      const uint4* OP4 = reinterpret_cast<const uint4*>(OPS);
-      uint4 c0 = make_uint4(0, 0, 0, 0), c1 = c0;
-      if (ob < oe) {
-        c0 = OP4[2 * ob];
-        c1 = OP4[2 * ob + 1];
-      }
-      for (uint32_t o = ob; o < oe; ++o) {
-        uint4 n0 = c0, n1 = c1;
-        if (o + 1 < oe) {  // next descriptor in flight while this op runs
-          n0 = OP4[2 * o + 2];
-          n1 = OP4[2 * o + 3];
-        }
-        exec_op<RB>(c0, c1, a, DATA, slots, tid, base);
-        c0 = n0;
-        c1 = n1;
-      }
-      const uint32_t pt2 = opaque(pt);
-#pragma unroll
-      for (int b = 0; b < RB; ++b) V[b] = opaque(V[b]);
-#pragma unroll
-      for (int j = 0; j < R; ++j) {
-        uint32_t x = pt2;
-#pragma unroll
-        for (int b = 0; b < RB; ++b)
-          if ((j >> b) & 1) x ^= V[b];
-        cur[x] = a[j];
-      }
-      __syncthreads();
-    }
-
-#pragma unroll
-    for (int i = 0; i < NI; ++i) {
-      const uint32_t r = warp + (uint32_t)i * NW;
-      state[base + H->runoff[r] + lane] = cur[H->runswz[r] ^ swl];
-    }
-    base = advance(base);
-    __syncthreads();
+    prog = sprog;
   }
-  cp_async_wait<0>();
+  sweep_tiles<TB, RB, S, RUNB>(state, prog, ntiles, synth, bufs, slots, blockIdx.x, gridDim.x);
 }
 
 // ---- relabel materialisation: paired-tile involution of bit positions ------------
@@ -655,6 +241,8 @@ struct Planner {
   double budget = 96.0;
   uint32_t max_ops = 40;    // non-diagonal gates per sweep (bounds the staged program)
   bool single_tile = false;
+  // qubits every tile holds (0..4: 512-byte runs; 0..2: 128-byte runs)
+  uint64_t pinned = 0x1FULL;
 
   // cost in FP64 instructions per amplitude
   double gate_cost(const PGate& g) const {
@@ -677,7 +265,7 @@ struct Planner {
   void plan(std::vector<PGate>& G, Poly& poly, std::vector<PSweep>& out) {
     std::vector<int> rem(G.size());
     for (size_t i = 0; i < G.size(); ++i) rem[i] = (int)i;
-    const uint64_t low_mask = single_tile ? ((n >= 64) ? ~0ULL : ((1ULL << n) - 1)) : 0x1FULL;
+    const uint64_t low_mask = single_tile ? ((n >= 64) ? ~0ULL : ((1ULL << n) - 1)) : pinned;
     while (!rem.empty()) {
       uint64_t S = low_mask;
       uint64_t blocked = 0;
@@ -767,7 +355,7 @@ struct Planner {
     if (poly.empty() && !poly.has_cst) return;
     if (sweeps.empty()) {
       PSweep sw;
-      uint64_t S = single_tile ? ((n >= 64) ? ~0ULL : ((1ULL << n) - 1)) : 0x1FULL;
+      uint64_t S = single_tile ? ((n >= 64) ? ~0ULL : ((1ULL << n) - 1)) : pinned;
       for (uint32_t q = 0; q < n && (uint32_t)__builtin_popcountll(S) < M; ++q)
         if (poly.pending(q)) S |= 1ULL << q;
       for (uint32_t q = 0; q < n && (uint32_t)__builtin_popcountll(S) < M; ++q) S |= 1ULL << q;
@@ -1154,12 +742,19 @@ int encode_sweep(const PSweep& sw_in, const std::vector<PGate>& G, uint32_t TBn,
   SwHeader h{};
   h.m = m;
   h.rb = RB;
-  for (uint32_t r = 0; r < (1u << (m - 5)); ++r) {
+  // runs of 2^run_bits: the sweep's lowest run_bits local bits are qubits 0..run_bits-1
+  uint32_t run_bits = 0;
+  while (run_bits < 5 && run_bits < m && sw.local[run_bits] == run_bits) ++run_bits;
+  run_bits = run_bits >= 5 ? 5u : 3u;
+  if (m < run_bits || sw.local[run_bits - 1] != run_bits - 1)
+    return fail(DQ_ERR_INTERNAL, "sweep local set lacks the pinned low qubits");
+  h.run_bits = run_bits;
+  for (uint32_t r = 0; r < (1u << (m - run_bits)); ++r) {
     uint64_t off = 0;
-    for (uint32_t b = 0; b + 5 < m; ++b)
-      if ((r >> b) & 1u) off |= 1ULL << sw.local[5 + b];
+    for (uint32_t b = 0; b + run_bits < m; ++b)
+      if ((r >> b) & 1u) off |= 1ULL << sw.local[run_bits + b];
     h.runoff[r] = off;
-    h.runswz[r] = swz(r << 5);
+    h.runswz[r] = swz(r << run_bits);
   }
   h.nphase = (uint32_t)P.size();
   h.nslots = (uint32_t)SL.size();
@@ -1320,12 +915,12 @@ bool convert_inst(const dq_inst& in, const uint32_t* perm, std::vector<PGate>& o
   }
 }
 
-template <int TB, int RB, int S>
-int launch_sweep_s(double2* amp, uint32_t n, const uint8_t* dblob, uint32_t prog_bytes,
+template <int TB, int RB, int S, bool PG, int RUNB>
+int launch_sweep_r(double2* amp, uint32_t n, const uint8_t* dblob, uint32_t prog_bytes,
                    cudaStream_t st, long long synth) {
   constexpr int M = TB + RB;
-  const size_t smem_max = sizeof(double2) * (S * (1u << M) + kMaxSlots) + max_prog(M);
-  const size_t smem = sizeof(double2) * (S * (1u << M) + kMaxSlots) + prog_bytes;
+  const size_t smem_max = sizeof(double2) * (S * (1u << M) + kMaxSlots) + (PG ? 0 : max_prog(M));
+  const size_t smem = sizeof(double2) * (S * (1u << M) + kMaxSlots) + (PG ? 0 : prog_bytes);
   // per device, once: opt-in shared memory and resident CTAs per SM (the
   // mutex makes the first launches from concurrent host threads safe)
   static std::mutex mu;
@@ -1336,10 +931,10 @@ int launch_sweep_s(double2* amp, uint32_t n, const uint8_t* dblob, uint32_t prog
   {
     std::lock_guard<std::mutex> lk(mu);
     if (per_sm[dev & 63] == 0) {
-      DQ_CUDA_TRY(cudaFuncSetAttribute(k_sweep<TB, RB, S>,
+      DQ_CUDA_TRY(cudaFuncSetAttribute(k_sweep<TB, RB, S, PG, RUNB>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_max));
       int b = 1;
-      DQ_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_sweep<TB, RB, S>, 1 << TB,
+      DQ_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_sweep<TB, RB, S, PG, RUNB>, 1 << TB,
                                                                 smem_max));
       per_sm[dev & 63] = b < 1 ? 1 : b;
     }
@@ -1349,40 +944,48 @@ int launch_sweep_s(double2* amp, uint32_t n, const uint8_t* dblob, uint32_t prog
   DQ_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
   const uint64_t tiles = 1ULL << (n - M);
   const unsigned grid = (unsigned)std::min<uint64_t>(tiles, (uint64_t)sms * resident);
-  k_sweep<TB, RB, S><<<grid, 1 << TB, smem, st>>>(amp, dblob, prog_bytes, (uint32_t)tiles, synth);
+  k_sweep<TB, RB, S, PG, RUNB><<<grid, 1 << TB, smem, st>>>(amp, dblob, prog_bytes, (uint32_t)tiles, synth);
   DQ_CUDA_TRY(cudaGetLastError());
   return DQ_OK;
 }
 
 template <int TB, int RB>
 int launch_sweep_rb(double2* amp, uint32_t n, const uint8_t* dblob, uint32_t prog_bytes,
-                    cudaStream_t st, long long synth) {
+                    cudaStream_t st, long long synth, uint32_t run_bits) {
   // default: single-buffered tiles, three 128-thread CTAs per SM (measured
   // faster than two double-buffered CTAs: the extra warps hide more of the
   // per-op latency than the prefetch saves); DQSIM_SWEEP_STAGES=2 selects
   // double buffering
+  // DQSIM_SWEEP_STAGES=3: double-buffered tiles with the program read from
+  // global memory (three CTAs per SM)
   static const int stages = [] {
     const char* e = getenv("DQSIM_SWEEP_STAGES");
-    return (e && atoi(e) == 2) ? 2 : 1;
+    return e ? atoi(e) : 1;
   }();
-  if (TB == 7 && stages == 1) return launch_sweep_s<7, RB, 1>(amp, n, dblob, prog_bytes, st, synth);
-  return launch_sweep_s<TB, RB, 2>(amp, n, dblob, prog_bytes, st, synth);
+  if (run_bits == 3) {
+    if (TB == 7 && stages == 3) return launch_sweep_r<7, RB, 2, true, 3>(amp, n, dblob, prog_bytes, st, synth);
+    if (TB == 7 && stages != 2) return launch_sweep_r<7, RB, 1, false, 3>(amp, n, dblob, prog_bytes, st, synth);
+    return launch_sweep_r<TB, RB, 2, false, 3>(amp, n, dblob, prog_bytes, st, synth);
+  }
+  if (TB == 7 && stages == 3) return launch_sweep_r<7, RB, 2, true, 5>(amp, n, dblob, prog_bytes, st, synth);
+  if (TB == 7 && stages != 2) return launch_sweep_r<7, RB, 1, false, 5>(amp, n, dblob, prog_bytes, st, synth);
+  return launch_sweep_r<TB, RB, 2, false, 5>(amp, n, dblob, prog_bytes, st, synth);
 }
 
 int launch_sweep(double2* amp, uint32_t n, uint32_t TB, uint32_t RB, const uint8_t* dblob,
-                 uint32_t prog_bytes, cudaStream_t st, long long synth) {
+                 uint32_t prog_bytes, cudaStream_t st, long long synth, uint32_t run_bits) {
   if (TB == 8) {
     switch (RB) {
-      case 2: return launch_sweep_rb<8, 2>(amp, n, dblob, prog_bytes, st, synth);
-      case 3: return launch_sweep_rb<8, 3>(amp, n, dblob, prog_bytes, st, synth);
-      case 4: return launch_sweep_rb<8, 4>(amp, n, dblob, prog_bytes, st, synth);
+      case 2: return launch_sweep_rb<8, 2>(amp, n, dblob, prog_bytes, st, synth, run_bits);
+      case 3: return launch_sweep_rb<8, 3>(amp, n, dblob, prog_bytes, st, synth, run_bits);
+      case 4: return launch_sweep_rb<8, 4>(amp, n, dblob, prog_bytes, st, synth, run_bits);
       default: break;
     }
   } else if (TB == 7) {
     switch (RB) {
-      case 2: return launch_sweep_rb<7, 2>(amp, n, dblob, prog_bytes, st, synth);
-      case 3: return launch_sweep_rb<7, 3>(amp, n, dblob, prog_bytes, st, synth);
-      case 4: return launch_sweep_rb<7, 4>(amp, n, dblob, prog_bytes, st, synth);
+      case 2: return launch_sweep_rb<7, 2>(amp, n, dblob, prog_bytes, st, synth, run_bits);
+      case 3: return launch_sweep_rb<7, 3>(amp, n, dblob, prog_bytes, st, synth, run_bits);
+      case 4: return launch_sweep_rb<7, 4>(amp, n, dblob, prog_bytes, st, synth, run_bits);
       default: break;
     }
   }
@@ -1532,7 +1135,8 @@ int fused_run_segment(double2* amp, uint32_t n, std::vector<PGate>& G, Planner& 
     const SwHeader* hh = reinterpret_cast<const SwHeader*>(blob.buf.data() + offs[i]);
     // a pending basis state is consumed by the first sweep (it writes every amplitude)
     const long long synth = (lazy_basis && *lazy_basis >= 0) ? (long long)*lazy_basis : -1;
-    DQ_TRY(launch_sweep(amp, n, pl.TB, pl.RB, fw.d_blob + offs[i], hh->prog_bytes, st, synth));
+    DQ_TRY(launch_sweep(amp, n, pl.TB, pl.RB, fw.d_blob + offs[i], hh->prog_bytes, st, synth,
+                        hh->run_bits));
     if (lazy_basis) *lazy_basis = -1;
     if (timing) {
       cudaEventRecord(e1, st);
@@ -1564,6 +1168,12 @@ int fused_run(double2* amp, uint32_t n, const dq_inst* prog, uint64_t ninst, con
   pl.TB = TB;
   pl.RB = M - TB;
   pl.single_tile = (M == n);
+  // DQSIM_SWEEP_PIN=3: tiles pin qubits 0..2 only (128-byte runs)
+  static const uint64_t pin_env = []() {
+    const char* e = getenv("DQSIM_SWEEP_PIN");
+    return (e && atoi(e) == 3) ? 0x7ULL : 0x1FULL;
+  }();
+  pl.pinned = pin_env;
   if (o.max_cost > 0) pl.budget = (double)o.max_cost;
   Poly poly;
   poly.init(n);
@@ -1622,6 +1232,14 @@ int fused_run(double2* amp, uint32_t n, const dq_inst* prog, uint64_t ninst, con
       ok = (actual == cd.creg_value);
     }
     if (!ok) continue;
+    // While the state is still a pending basis vector and nothing has been
+    // queued yet, an X gate is a flip of that basis index: exact, and it
+    // leaves every tile qubit free for the gates that follow.
+    if (in.kind == DQ_X && hooks.lazy_basis && *hooks.lazy_basis >= 0 && G.empty() &&
+        poly.empty() && !poly.has_cst) {
+      *hooks.lazy_basis ^= (int64_t)(1ULL << perm[in.q[0]]);
+      continue;
+    }
     switch (in.kind) {
       case DQ_ID: case DQ_U0: case DQ_BARRIER: case DQ_CLASSICAL: case DQ_G_NOOP:
         continue;

@@ -19,7 +19,7 @@ from dqsim_bosonic_b200 import _native as nat
 
 OP_U1, OP_U1R, OP_U1X, OP_U2, OP_FLUSH_R, OP_FLUSH_T, OP_GPHASE, OP_U1H, OP_SCALE = range(9)
 FL_THR, FL_REG, FL_PRE = 1, 2, 4
-MAXM, MAXRUNS = 12, 128
+MAXM, MAXRUNS = 12, 512
 SWZ_G = {3: 3, 4: 5, 5: 6, 6: 7, 7: 3, 8: 5, 9: 6, 10: 7, 11: 1}
 
 
@@ -63,9 +63,10 @@ def run_sweep(state: np.ndarray, n: int, blob: bytes) -> None:
     """Apply one encoded sweep to state (complex128, modified in place)."""
     m, rb, nphase, nslots = struct.unpack_from("<4I", blob, 0)
     local = list(struct.unpack_from(f"<{MAXM}I", blob, 16))[:m]
-    off_phase, off_op, off_slot, off_slotent, off_data, prog_bytes, tile_xload = struct.unpack_from(
-        "<7I", blob, 64)
-    nruns = 1 << (m - 5)
+    off_phase, off_op, off_slot, off_slotent, off_data, prog_bytes, tile_xload, run_bits = \
+        struct.unpack_from("<8I", blob, 64)
+    nruns = 1 << (m - run_bits)
+    run_len = 1 << run_bits
     runoff = np.array(struct.unpack_from(f"<{MAXRUNS}Q", blob, 96)[:nruns], dtype=np.uint64)
     runswz = np.array(struct.unpack_from(f"<{MAXRUNS}I", blob, 96 + 8 * MAXRUNS)[:nruns], dtype=np.int64)
     T, R = 1 << m, 1 << rb
@@ -79,11 +80,11 @@ def run_sweep(state: np.ndarray, n: int, blob: bytes) -> None:
         p = np.uint64(p)
         lowmask = (np.uint64(1) << p) - np.uint64(1)
         base = ((base >> p) << (p + np.uint64(1))) | (base & lowmask)
-    lane = np.arange(32, dtype=np.uint64)
-    swl = np.array([swz(int(x)) for x in range(32)], dtype=np.int64)
-    # gather: element (run r, lane) -> smem index runswz[r] ^ swz(lane)
-    gidx = base[:, None, None] + runoff[None, :, None] + lane[None, None, :]      # tiles x runs x 32
-    sidx = (runswz[:, None] ^ swl[None, :])                                       # runs x 32
+    lane = np.arange(run_len, dtype=np.uint64)
+    swl = np.array([swz(int(x)) for x in range(run_len)], dtype=np.int64)
+    # gather: element (run r, offset) -> smem index runswz[r] ^ swz(offset)
+    gidx = base[:, None, None] + runoff[None, :, None] + lane[None, None, :]      # tiles x runs x run_len
+    sidx = (runswz[:, None] ^ swl[None, :])                                       # runs x run_len
     smem = np.zeros((ntiles, T), dtype=np.complex128)
     # X gates opening the sweep are folded into the load: element e lands at the slot of e ^ flips
     smem[:, sidx.reshape(-1) ^ tile_xload] = state[gidx.reshape(ntiles, -1).astype(np.int64)]
