@@ -508,6 +508,8 @@ def main():
             line["adjoint_batch"] = adjoint_batch_section(dev, args.adam_steps)
     if not args.no_extras:
         line["distributed30"] = distributed30_section(dev, args.steps)
+        line["ragged"] = ragged_section(dev, cpu=d.rank == 0 and d.world == 1
+                                        and not args.no_cpu_baseline)
     if not args.no_extras and not args.no_adjoint31:
         line["adjoint31"] = adjoint31_section(dev)
     if "_cpu_job" in line.get("trajectories", {}):
@@ -847,6 +849,78 @@ def mps_section(dev: int, cpu: bool) -> dict:
         single["parity"] = {"max_abs_amplitude_diff": float(np.max(np.abs(sv - ref))),
                             "bond_dims_equal": rdims == dims}
     out["simulate"] = single
+    return out
+
+
+def ragged_section(dev: int, cpu: bool) -> dict:
+    """1024 independent u3 + cx brickwork circuits, n ~ U{10..22} qubits,
+    depth ~ U{5..40} layers (seed 99), one trajectory each through
+    dq_run_batch: ONE persistent launch (states of <= 16 qubits in cluster
+    shared memory, 17..22 qubits HBM-resident fused sweeps).  Against
+    per-circuit launches of the fused engine on the same GPU (a seeded sample
+    of 64 circuits, scaled to the batch) and, for parity, the final states of
+    a sample of items compared with the oracle."""
+    from dqsim_bosonic_b200 import _native as nat
+    from dqsim_bosonic_b200.batch import run_batch
+    from dqsim_bosonic_b200.circuit import decode_circuit_json, encode
+    from dqsim_bosonic_b200.statevector import run_program
+
+    circs = _circuits.ragged_batch(1024, 99)
+    progs = [encode(decode_circuit_json(c.model_dump_json())) for c in circs]
+    seeds = [99 + k for k in range(len(progs))]
+    ns = np.array([p.num_qubits for p in progs])
+    run_batch(progs, seeds, dev)  # warm-up (module load, allocations)
+    walls, sts = [], []
+    for _ in range(3):
+        t0 = time.perf_counter()
+        _, _, st = run_batch(progs, seeds, dev)
+        walls.append(time.perf_counter() - t0)
+        sts.append(st)
+    i = int(np.argsort(walls)[1])
+    wall, st = walls[i], sts[i]
+    # per-circuit launches of the fused engine (HBM state per circuit), sample scaled up
+    rng = np.random.default_rng(7)
+    sample = rng.choice(len(progs), size=64, replace=False)
+    states = {}
+    for k in sample:
+        p = progs[k]
+        s = states.get(p.num_qubits)
+        if s is None:
+            s = states[p.num_qubits] = nat.State(p.num_qubits, dev)
+        s.reset()
+        run_program(s, p, seeds[k], nat.SEM_SHOTS, nat.EXEC_FUSED)
+    per = 0.0
+    for k in sample:
+        p = progs[k]
+        s = states[p.num_qubits]
+        t0 = time.perf_counter()
+        s.reset()
+        run_program(s, p, seeds[k], nat.SEM_SHOTS, nat.EXEC_FUSED)
+        per += time.perf_counter() - t0
+    for s in states.values():
+        s.release()
+    per_batch_s = per * len(progs) / len(sample)
+    out = {"workload": "1024 u3+cx brickwork circuits, n ~ U{10..22}, depth ~ U{5..40} layers (seed 99)",
+           "items": len(progs), "qubit_histogram": {int(q): int((ns == q).sum()) for q in np.unique(ns)},
+           "wall_ms": wall * 1e3, "kernel_ms": st.kernel_ms, "items_per_s": len(progs) / wall,
+           "launches": int(st.launches), "hbm_items": int(st.hbm_items),
+           "engine_items": int(st.engine_items), "cluster_span": int(st.cluster_span),
+           "clusters": int(st.clusters),
+           "per_circuit_launches_s": per_batch_s,
+           "per_circuit_note": "one fused dq_run per circuit (64 sampled circuits, scaled to 1024)",
+           "speedup_vs_per_circuit": per_batch_s / wall}
+    if cpu:
+        import _oracle as orc
+
+        pick = [int(k) for k in np.argsort(ns * 1000 + np.arange(len(ns)))[:6]]
+        pick += [int(k) for k in np.flatnonzero((ns >= 17) & (ns <= 18))[:2]]
+        _, sv, _ = run_batch(progs, seeds, dev, want_states=pick)
+        worst = 0.0
+        for k in pick:
+            ref, _, rc, _ = orc.run(progs[k], 0)
+            worst = max(worst, float(np.max(np.abs(sv[k] - ref))))
+        out["parity"] = {"items_checked": len(pick), "qubits": [int(ns[k]) for k in pick],
+                         "max_abs_amplitude_diff": worst, "tolerance": 1e-12}
     return out
 
 

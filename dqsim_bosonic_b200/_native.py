@@ -121,6 +121,8 @@ class TrajStats(ctypes.Structure):
         ("local_bits", ctypes.c_uint32),
         ("launches", ctypes.c_uint32),
         ("engine_items", ctypes.c_uint32),
+        ("hbm_items", ctypes.c_uint32),
+        ("reserved", ctypes.c_uint32),
     ]
 
 

@@ -92,10 +92,14 @@ def run_trajectories(prog, base_seed: int, shots: int, device: int, want_times: 
     return out, times, 0.0
 
 
-def run_batch(progs, seeds, device: int = 0, *, want_states: bool = False, opts=None):
-    """Independent circuits, one trajectory each (shot semantics).
+def run_batch(progs, seeds, device: int = 0, *, want_states=False, opts=None):
+    """Independent circuits, one trajectory each (shot semantics), in one
+    persistent launch (``dq_run_batch``).
 
-    Returns (list of cbits arrays, list of final states or None, TrajStats)."""
+    ``want_states``: True for every item's final state, or a collection of
+    item indices to return the states of those items only.
+    Returns (list of cbits arrays, list of final states (None where not
+    requested) or None, TrajStats)."""
     progs = list(progs)
     seeds = [int(s) & _U64 for s in seeds]
     if len(seeds) != len(progs):
@@ -103,9 +107,11 @@ def run_batch(progs, seeds, device: int = 0, *, want_states: bool = False, opts=
     items = (nat.BatchItem * max(1, len(progs)))()
     cbits = []
     states = []
+    pick = None if isinstance(want_states, bool) else set(int(i) for i in want_states)
     for k, (p, s) in enumerate(zip(progs, seeds)):
         cb = np.full(p.cbit_space, -1, dtype=np.int32)
-        sv = np.empty(1 << p.num_qubits, dtype=np.complex128) if want_states else None
+        wanted = (k in pick) if pick is not None else bool(want_states)
+        sv = np.empty(1 << p.num_qubits, dtype=np.complex128) if wanted else None
         cbits.append(cb)
         states.append(sv)
         it = items[k]
@@ -129,7 +135,7 @@ def run_batch(progs, seeds, device: int = 0, *, want_states: bool = False, opts=
         raise RuntimeError(f"batch item {k}: " +
                            _unsupported_message(progs[k], st.failed_inst & ((1 << 40) - 1)))
     nat.check(rc, "dq_run_batch")
-    return cbits, (states if want_states else None), st
+    return cbits, (states if (pick is not None or want_states) else None), st
 
 
 class TrajectoryPlan:

@@ -65,6 +65,28 @@ __global__ void __launch_bounds__(1 << TB, ((S == 1 || PG) && TB == 7 ? 3 : (TB 
   sweep_tiles<TB, RB, S, RUNB>(state, prog, ntiles, synth, bufs, slots, blockIdx.x, gridDim.x);
 }
 
+// Sweep k of many states in one launch: job j's tiles are split into chunks
+// of chunk_tiles consecutive tiles and the CTAs take (job, chunk) work items
+// in order; double-buffered tiles, programs read from global memory.
+template <int TB, int RB, int RUNB>
+__global__ void __launch_bounds__(1 << TB, TB == 7 ? 3 : 2)
+    k_sweep_multi(const SweepJob* __restrict__ jobs, uint32_t njobs, uint32_t nchunks,
+                  uint32_t chunk_tiles, uint32_t ntiles) {
+  constexpr int T = 1 << (TB + RB);
+  extern __shared__ __align__(16) unsigned char smraw[];
+  double2* bufs = reinterpret_cast<double2*>(smraw);
+  double2* slots = bufs + 2 * T;
+  const uint64_t work = (uint64_t)njobs * nchunks;
+  for (uint64_t w = blockIdx.x; w < work; w += gridDim.x) {
+    const SweepJob J = jobs[w / nchunks];
+    const uint32_t c = (uint32_t)(w % nchunks);
+    const uint32_t t0 = c * chunk_tiles;
+    const uint32_t t1 = min(t0 + chunk_tiles, ntiles);
+    sweep_tiles<TB, RB, 2, RUNB>(J.state, J.prog, t1, J.synth, bufs, slots, t0, 1);
+    __syncthreads();
+  }
+}
+
 // ---- relabel materialisation: paired-tile involution of bit positions ------------
 //
 // A bit-position involution tau (tau(tau(p)) = p) moves amplitude i to tau(i).
@@ -992,6 +1014,39 @@ int launch_sweep(double2* amp, uint32_t n, uint32_t TB, uint32_t RB, const uint8
   return fail(DQ_ERR_INTERNAL, "unsupported sweep geometry");
 }
 
+template <int TB, int RB, int RUNB>
+int launch_sweep_multi_t(const SweepJob* d_jobs, uint32_t njobs, uint32_t n, cudaStream_t st) {
+  constexpr int M = TB + RB;
+  const size_t smem = sizeof(double2) * (2 * (1u << M) + kMaxSlots);
+  static std::mutex mu;
+  static int per_sm[64];
+  int dev = 0;
+  DQ_CUDA_TRY(cudaGetDevice(&dev));
+  int resident;
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    if (per_sm[dev & 63] == 0) {
+      DQ_CUDA_TRY(cudaFuncSetAttribute(k_sweep_multi<TB, RB, RUNB>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      int b = 1;
+      DQ_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_sweep_multi<TB, RB, RUNB>,
+                                                                1 << TB, smem));
+      per_sm[dev & 63] = b < 1 ? 1 : b;
+    }
+    resident = per_sm[dev & 63];
+  }
+  int sms = 148;
+  DQ_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  const uint32_t ntiles = 1u << (n - M);
+  const uint32_t chunk = std::min<uint32_t>(64, ntiles);
+  const uint32_t nchunks = (ntiles + chunk - 1) / chunk;
+  const uint64_t work = (uint64_t)njobs * nchunks;
+  const unsigned grid = (unsigned)std::min<uint64_t>(work, (uint64_t)sms * resident);
+  k_sweep_multi<TB, RB, RUNB><<<grid, 1 << TB, smem, st>>>(d_jobs, njobs, nchunks, chunk, ntiles);
+  DQ_CUDA_TRY(cudaGetLastError());
+  return DQ_OK;
+}
+
 int ensure_capacity(FusedWork& fw, size_t bytes, cudaStream_t st) {
   if (bytes <= fw.d_cap && bytes <= fw.h_cap) return DQ_OK;
   DQ_CUDA_TRY(cudaStreamSynchronize(st));
@@ -1117,6 +1172,10 @@ int fused_run_segment(double2* amp, uint32_t n, std::vector<PGate>& G, Planner& 
     fw.plan_out->insert(fw.plan_out->end(), blob.buf.begin(), blob.buf.end());
     for (size_t o : offs) fw.plan_offs->push_back(base + o);
     fw.plan_rb = pl.RB;
+    if (lazy_basis && *lazy_basis >= 0) {  // the first sweep generates the basis vector
+      fw.plan_synth = *lazy_basis;
+      *lazy_basis = -1;
+    }
     prof->sweeps += sweeps.size();
     return DQ_OK;
   }
@@ -1160,7 +1219,7 @@ int fused_run(double2* amp, uint32_t n, const dq_inst* prog, uint64_t ninst, con
     const char* e = getenv("DQSIM_SWEEP_TB");
     return (e && atoi(e) == 8) ? 8u : 7u;
   }();
-  const uint32_t TB = tb_env;
+  const uint32_t TB = fw.plan_tb ? fw.plan_tb : tb_env;
   uint32_t M = TB + 4;  // 16 amplitudes per thread
   if (o.fusion_width >= (int)(TB + 2) && o.fusion_width <= (int)(TB + 4)) M = (uint32_t)o.fusion_width;
   if (M > n) M = n;
@@ -1304,6 +1363,49 @@ int fused_run(double2* amp, uint32_t n, const dq_inst* prog, uint64_t ninst, con
     prof->sweep_time += t;
   }
   return DQ_OK;
+}
+
+int fused_plan(uint32_t n, const dq_inst* prog, uint64_t ninst, int semantics, uint32_t tb,
+               int fusion_width, int64_t lazy_basis, std::vector<uint8_t>* blob,
+               std::vector<uint64_t>* offs, uint32_t* perm, int64_t* synth, uint32_t* rb) {
+  if (n < kFusedMinQubits || n > 34) return fail(DQ_ERR_INVALID_ARG, "fused planning needs 10..34 qubits");
+  FusedWork fw;
+  fw.plan_out = blob;
+  fw.plan_offs = offs;
+  fw.plan_tb = tb;
+  FusedHooks hooks;
+  int64_t lazy = lazy_basis;
+  hooks.lazy_basis = lazy_basis >= 0 ? &lazy : nullptr;
+  dq_profile prof{};
+  prof.failed_inst = -1;
+  dq_run_opts o{};
+  o.semantics = semantics;
+  o.exec = DQ_EXEC_FUSED;
+  o.fusion_width = fusion_width;
+  DQ_TRY(fused_run(nullptr, n, prog, ninst, o, fw, nullptr, 0, hooks, &prof, perm));
+  *synth = offs->empty() ? (lazy_basis >= 0 ? lazy : -1) : fw.plan_synth;
+  *rb = fw.plan_rb;
+  return DQ_OK;
+}
+
+uint32_t sweep_run_bits(const uint8_t* prog) {
+  return reinterpret_cast<const SwHeader*>(prog)->run_bits;
+}
+
+int launch_sweep_multi(const SweepJob* d_jobs, uint32_t njobs, uint32_t n, uint32_t rb,
+                       uint32_t run_bits, cudaStream_t st) {
+  if (!njobs) return DQ_OK;
+  if (n < 7 + rb) return fail(DQ_ERR_INVALID_ARG, "state smaller than a tile");
+  const bool r3 = run_bits == 3;
+  switch (rb) {
+    case 2: return r3 ? launch_sweep_multi_t<7, 2, 3>(d_jobs, njobs, n, st)
+                      : launch_sweep_multi_t<7, 2, 5>(d_jobs, njobs, n, st);
+    case 3: return r3 ? launch_sweep_multi_t<7, 3, 3>(d_jobs, njobs, n, st)
+                      : launch_sweep_multi_t<7, 3, 5>(d_jobs, njobs, n, st);
+    case 4: return r3 ? launch_sweep_multi_t<7, 4, 3>(d_jobs, njobs, n, st)
+                      : launch_sweep_multi_t<7, 4, 5>(d_jobs, njobs, n, st);
+    default: return fail(DQ_ERR_INTERNAL, "unsupported multi-sweep geometry");
+  }
 }
 
 }  // namespace dq

@@ -28,6 +28,11 @@ struct FusedWork {
   std::vector<uint8_t>* plan_out = nullptr;
   std::vector<uint64_t>* plan_offs = nullptr;
   uint32_t plan_rb = 0;
+  // plan-only mode: thread bits of the kernel that will run the programs (0:
+  // the default launch geometry); out: the basis index the first planned sweep
+  // generates its tiles from (-1: it reads the state)
+  uint32_t plan_tb = 0;
+  int64_t plan_synth = -1;
   uint8_t* d_blob = nullptr;
   size_t d_cap = 0;
   uint8_t* h_blob = nullptr;  // pinned staging
@@ -63,5 +68,31 @@ int materialize_perm(double2* amp, uint32_t n, uint32_t* perm, cudaStream_t st,
 
 // Smallest register width the fused path runs (smaller states use per-gate kernels).
 constexpr uint32_t kFusedMinQubits = 10;
+
+// Plans a unitary program as fused sweeps without running anything: the
+// encoded programs are appended to *blob (their offsets to *offs), *rb is
+// the register bits of the geometry, perm is updated by the swaps, and
+// *synth receives the basis index the first sweep generates its tiles from
+// (lazy_basis >= 0: the program starts from that basis vector) or -1.
+// tb = 0: the default thread geometry; fusion_width 0: the default tile.
+int fused_plan(uint32_t n, const dq_inst* prog, uint64_t ninst, int semantics, uint32_t tb,
+               int fusion_width, int64_t lazy_basis, std::vector<uint8_t>* blob,
+               std::vector<uint64_t>* offs, uint32_t* perm, int64_t* synth, uint32_t* rb);
+
+// One sweep of one state in a multi-state launch.
+struct SweepJob {
+  double2* state;
+  const uint8_t* prog;  // device pointer to an encoded sweep program
+  long long synth;      // >= 0: generate the input from this basis index
+};
+
+// Runs one sweep of each of njobs states (all of n qubits, programs planned
+// with 7 thread bits, register width rb and the same run width run_bits) in
+// ONE launch; d_jobs is device memory.
+int launch_sweep_multi(const SweepJob* d_jobs, uint32_t njobs, uint32_t n, uint32_t rb,
+                       uint32_t run_bits, cudaStream_t st);
+
+// The run width (5 or 3) of an encoded sweep program in host memory.
+uint32_t sweep_run_bits(const uint8_t* prog);
 
 }  // namespace dq

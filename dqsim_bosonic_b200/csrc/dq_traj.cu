@@ -32,9 +32,11 @@
 #include <vector>
 
 #include "dq_common.cuh"
+#include "dq_fused.cuh"
 #include "dq_gates.hpp"
 #include "dq_handle.cuh"
 #include "dq_rng.cuh"
+#include "dq_sweep.cuh"
 
 namespace cg = cooperative_groups;
 
@@ -71,6 +73,17 @@ struct TProg {         // one program of a launch
   uint64_t base_seed;   // shot s draws from seed_from_u64(base_seed + s) (wrapping)
   uint64_t cbits_off;   // shot s writes cbits_out[cbits_off + s * ncbits ...]
   double2* state_out;   // device: final state of shot s at + s * 2^n, or null
+  // Items too large for a cluster's shared memory (batch items of 17+ qubits)
+  // keep their state in HBM at `hbm` and run as fused tile sweeps: sweeps
+  // [sweep_first, sweep_first + nsweeps) of the launch's sweep table, the
+  // first one generating its tiles from the basis index `synth`.
+  double2* hbm;
+  uint32_t sweep_first, nsweeps;
+  long long synth;
+};
+struct TSweep {          // one fused sweep of an HBM item
+  uint64_t off;          // byte offset of its program in the launch's sweep blob
+  uint32_t ntiles, run_bits;
 };
 struct TItem {          // one trajectory: a shot of a program
   uint32_t prog, pad;
@@ -87,6 +100,8 @@ struct TrajParams {
   unsigned long long* boundary;  // draws within 1e-12 of p1
   long long* failed;             // lowest (prog << 40 | instruction) that failed
   uint64_t nitems;
+  const uint8_t* sweep_blob;     // sweep programs of the HBM items (dq_sweep.cuh layout)
+  const TSweep* sweeps;
 };
 
 __device__ __forceinline__ uint32_t ins0(uint32_t k, uint32_t p) {
@@ -175,6 +190,36 @@ __global__ void __launch_bounds__(THREADS) k_traj(const TrajParams P) {
     }
     const TItem it = P.items[item];
     const TProg pg = P.progs[it.prog];
+    if (pg.hbm) {
+      // HBM item: the cluster's CTAs split the tiles of each sweep (tiles
+      // rank, rank + C, ...; 256 threads run the 8-thread-bit geometry the
+      // sweeps were planned for) with a cluster barrier between sweeps; the
+      // fence makes each sweep's stores visible to the CTAs of the next one.
+      if constexpr (THREADS == 256) {
+        double2* bufs = reinterpret_cast<double2*>(smraw);
+        double2* slots = bufs + (1u << 11);
+        if (pg.nsweeps == 0) {  // nothing but a basis state to write
+          const uint64_t len = 1ULL << pg.n;
+          for (uint64_t i = (uint64_t)rank * THREADS + tid; i < len; i += (uint64_t)C * THREADS)
+            pg.hbm[i] = make_double2(i == (uint64_t)pg.synth ? 1.0 : 0.0, 0.0);
+        }
+        for (uint32_t s = 0; s < pg.nsweeps; ++s) {
+          const TSweep sw = P.sweeps[pg.sweep_first + s];
+          const long long sy = s == 0 ? pg.synth : -1LL;
+          if (sw.run_bits == 3)
+            sweep_tiles<8, 3, 1, 3>(pg.hbm, P.sweep_blob + sw.off, sw.ntiles, sy, bufs, slots, rank, C);
+          else
+            sweep_tiles<8, 3, 1, 5>(pg.hbm, P.sweep_blob + sw.off, sw.ntiles, sy, bufs, slots, rank, C);
+          __threadfence();
+          cl.sync();
+        }
+      }
+      if (rank == 0)  // unitary items write no classical bit
+        for (uint32_t i = tid; i < pg.ncbits; i += THREADS)
+          P.cbits_out[pg.cbits_off + it.shot * pg.ncbits + i] = -1;
+      sync_all(true);
+      continue;
+    }
     const uint32_t lb = pg.lb, L = 1u << lb;
     double2* sm = reinterpret_cast<double2*>(smraw);
     double* red = reinterpret_cast<double*>(sm + L);    // [0..32]: block sums, [40]: CTA partial
@@ -746,9 +791,68 @@ struct LaunchSet {
   std::vector<dq_cond> conds;
   std::vector<TProg> progs;
   std::vector<TItem> items;
+  std::vector<uint8_t> blob;     // sweep programs of the HBM items
+  std::vector<TSweep> sweeps;
   uint32_t C = 1;
   uint32_t max_lb = 1, max_ncbits = 0;
 };
+
+// Largest batch item that runs as HBM-resident fused sweeps inside the
+// persistent launch (2^30 amplitudes = 16 GiB).
+constexpr uint32_t kHbmItemMaxQubits = 30;
+// Sweep geometry of HBM items: 8 thread bits (the 256-thread trajectory
+// CTA), 3 register bits, tiles of 2^11 amplitudes.
+constexpr uint32_t kHbmTB = 8, kHbmM = 11;
+
+// A unitary batch item planned as fused sweeps for the HBM path of k_traj.
+struct HbmPlan {
+  std::vector<uint8_t> blob;
+  std::vector<uint64_t> offs;
+  int64_t synth = -1;
+  uint32_t perm[64];
+};
+
+// Plans item `it` (shot semantics, from |0...0>) as sweeps of the HBM
+// geometry; false when the item has measurements, resets or conditions, or a
+// gate the sweep planner does not represent (such items run on the engine).
+bool plan_hbm_item(const dq_batch_item& it, HbmPlan* out) {
+  for (uint64_t i = 0; i < it.ninst; ++i) {
+    const dq_inst& in = it.prog[i];
+    if (in.cond_count || in.kind == DQ_MEASURE || in.kind == DQ_RESET || in.kind == DQ_G_UNSUPPORTED)
+      return false;
+  }
+  for (uint32_t l = 0; l < 64; ++l) out->perm[l] = l;
+  uint32_t rb = 0;
+  if (fused_plan(it.n, it.prog, it.ninst, DQ_SEM_SHOTS, kHbmTB, (int)kHbmM, 0, &out->blob, &out->offs,
+                 out->perm, &out->synth, &rb) != DQ_OK ||
+      (!out->offs.empty() && rb != kHbmM - kHbmTB)) {
+    clear_error();
+    return false;
+  }
+  return true;
+}
+
+// Adds a planned HBM item whose state lives at `hbm` (device, 2^n amplitudes).
+void add_hbm_program(LaunchSet& ls, const HbmPlan& pl, uint32_t n, uint64_t cbits_off,
+                     uint32_t ncbits, double2* hbm) {
+  while (ls.blob.size() % 16) ls.blob.push_back(0);
+  const uint64_t base = ls.blob.size();
+  ls.blob.insert(ls.blob.end(), pl.blob.begin(), pl.blob.end());
+  TProg pg{};
+  pg.n = n;
+  pg.lb = 12;  // the launch's shared memory holds the 2^11-amplitude tile and the slot factors
+  pg.ncbits = ncbits;
+  pg.cbits_off = cbits_off;
+  pg.hbm = hbm;
+  pg.sweep_first = (uint32_t)ls.sweeps.size();
+  pg.nsweeps = (uint32_t)pl.offs.size();
+  pg.synth = (long long)pl.synth;
+  for (uint64_t off : pl.offs)
+    ls.sweeps.push_back(TSweep{base + off, 1u << (n - kHbmM), sweep_run_bits(pl.blob.data() + off)});
+  ls.progs.push_back(pg);
+  ls.max_lb = std::max(ls.max_lb, pg.lb);
+  ls.max_ncbits = std::max(ls.max_ncbits, ncbits);
+}
 
 int add_program(LaunchSet& ls, const dq_inst* prog, uint64_t ninst, const dq_cond* conds,
                 uint64_t nconds, uint32_t n, uint32_t lb, uint64_t base_seed, uint64_t cbits_off,
@@ -844,6 +948,8 @@ struct LaunchBuffers {
   dq_cond* conds = nullptr;
   TProg* progs = nullptr;
   TItem* items = nullptr;
+  uint8_t* blob = nullptr;
+  TSweep* sweeps = nullptr;
   unsigned long long* ctr = nullptr;  // [0] queue, [1] boundary, [2] failed
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   cudaStream_t st = nullptr;
@@ -855,6 +961,8 @@ struct LaunchBuffers {
     if (conds) cudaFree(conds);
     if (progs) cudaFree(progs);
     if (items) cudaFree(items);
+    if (blob) cudaFree(blob);
+    if (sweeps) cudaFree(sweeps);
     if (ctr) cudaFree(ctr);
     if (e0) cudaEventDestroy(e0);
     if (e1) cudaEventDestroy(e1);
@@ -883,6 +991,8 @@ int run_launch(LaunchSet& ls, int threads, int device, cudaStream_t st, int32_t*
   DQ_TRY(upload(&b.conds, ls.conds, st));
   DQ_TRY(upload(&b.progs, ls.progs, st));
   DQ_TRY(upload(&b.items, ls.items, st));
+  DQ_TRY(upload(&b.blob, ls.blob, st));
+  DQ_TRY(upload(&b.sweeps, ls.sweeps, st));
   DQ_CUDA_TRY(cudaMalloc((void**)&b.ctr, 3 * sizeof(unsigned long long)));
   const unsigned long long init[3] = {0ULL, 0ULL, 0x7fffffffffffffffULL};
   DQ_CUDA_TRY(cudaMemcpyAsync(b.ctr, init, sizeof(init), cudaMemcpyHostToDevice, st));
@@ -899,6 +1009,8 @@ int run_launch(LaunchSet& ls, int threads, int device, cudaStream_t st, int32_t*
   P.boundary = b.ctr + 1;
   P.failed = reinterpret_cast<long long*>(b.ctr + 2);
   P.nitems = ls.items.size();
+  P.sweep_blob = b.blob;
+  P.sweeps = b.sweeps;
   (void)device;
   TrajLaunch L;
   DQ_TRY(config_traj(threads, ls.C, traj_smem(ls), P.nitems, &L));
@@ -1071,34 +1183,79 @@ int dq_run_batch(int device, const dq_batch_item* items, uint64_t nitems,
   }
   DeviceGuard g(device);
   const auto t0 = std::chrono::steady_clock::now();
-  // resident items grouped by cluster span; the rest run on the HBM engine
-  LaunchSet sets[4];
-  for (int c = 0; c < 4; ++c) sets[c].C = 1u << c;
-  std::vector<std::vector<uint64_t>> members(4);
-  std::vector<uint64_t> engine_items;
+  // One persistent launch takes every item it can: states of up to 16 qubits
+  // live in a cluster's shared memory; unitary items of 17..30 qubits keep
+  // their state in HBM and run as fused tile sweeps by one cluster each.
+  // Everything shares one cluster span (the widest any item needs).  Left
+  // for separate launches: items whose slice at that span would hold fewer
+  // than 16 amplitudes, and every resident item when local_bits is forced
+  // (grouped by span); left for the engine (one dq_run each): large items
+  // with measurements, resets or conditions.
+  std::vector<uint64_t> resident, hbm_items, engine_items;
+  std::vector<HbmPlan> plans;
   for (uint64_t k = 0; k < nitems; ++k) {
     const uint32_t n = items[k].n;
-    if (n > kTrajMaxQubits) {
-      engine_items.push_back(k);
+    if (n <= kTrajMaxQubits) {
+      resident.push_back(k);
       continue;
     }
+    HbmPlan pl;
+    if (threads == 256 && !force_lb && n <= kHbmItemMaxQubits && plan_hbm_item(items[k], &pl)) {
+      hbm_items.push_back(k);
+      plans.push_back(std::move(pl));
+    } else {
+      engine_items.push_back(k);
+    }
+  }
+  uint32_t Cmain = hbm_items.empty() ? 1u : std::min<uint32_t>(8u, max_span);
+  for (uint64_t k : resident) {
     uint32_t lb, C;
-    DQ_TRY(geometry(n, max_span, force_lb, &lb, &C));
-    members[__builtin_ctz(C)].push_back(k);
+    DQ_TRY(geometry(items[k].n, max_span, force_lb, &lb, &C));
+    if (!force_lb) Cmain = std::max(Cmain, C);
+  }
+  const uint32_t cbits_main = (uint32_t)__builtin_ctz(Cmain);
+  // set 0: the main launch (span Cmain); sets 1..4: spans 1, 2, 4, 8 for the rest
+  LaunchSet sets[5];
+  sets[0].C = Cmain;
+  for (int c = 0; c < 4; ++c) sets[1 + c].C = 1u << c;
+  std::vector<std::vector<uint64_t>> members(5);
+  std::vector<uint32_t> item_lb(nitems, 0);
+  for (uint64_t k : resident) {
+    const uint32_t n = items[k].n;
+    uint32_t lb, C;
+    geometry(n, max_span, force_lb, &lb, &C);
+    if (!force_lb && n >= cbits_main + 4) {
+      item_lb[k] = n - cbits_main;
+      members[0].push_back(k);
+    } else {
+      item_lb[k] = lb;
+      members[1 + __builtin_ctz(C)].push_back(k);
+    }
+  }
+  for (uint64_t h = 0; h < hbm_items.size(); ++h) members[0].push_back(hbm_items[h]);
+  std::vector<int64_t> plan_of(nitems, -1);
+  for (uint64_t h = 0; h < hbm_items.size(); ++h) plan_of[hbm_items[h]] = (int64_t)h;
+  // HBM item states: one device allocation
+  std::vector<uint64_t> hbm_off(hbm_items.size(), 0);
+  uint64_t hbm_amps = 0;
+  for (uint64_t h = 0; h < hbm_items.size(); ++h) {
+    hbm_off[h] = hbm_amps;
+    hbm_amps += 1ULL << items[hbm_items[h]].n;
   }
   // per set: state outputs packed into one device buffer, cbits likewise
   struct Out { uint64_t item, state_off, cbits_off; };
-  std::vector<Out> outs[4];
-  uint64_t state_amps[4] = {0, 0, 0, 0}, cbit_words[4] = {0, 0, 0, 0};
-  for (int c = 0; c < 4; ++c) {
+  std::vector<Out> outs[5];
+  uint64_t state_amps[5] = {0, 0, 0, 0, 0}, cbit_words[5] = {0, 0, 0, 0, 0};
+  for (int c = 0; c < 5; ++c) {
     // costliest first (longest-processing-time order for the work queue)
     std::vector<uint64_t>& m = members[c];
     std::stable_sort(m.begin(), m.end(), [&](uint64_t a, uint64_t b) {
       return (items[a].ninst << items[a].n) > (items[b].ninst << items[b].n);
     });
     for (uint64_t k : m) {
-      Out o{k, items[k].state_out ? state_amps[c] : ~0ULL, cbit_words[c]};
-      if (items[k].state_out) state_amps[c] += 1ULL << items[k].n;
+      const bool packed = items[k].state_out && plan_of[k] < 0;
+      Out o{k, packed ? state_amps[c] : ~0ULL, cbit_words[c]};
+      if (packed) state_amps[c] += 1ULL << items[k].n;
       cbit_words[c] += items[k].ncbits;
       outs[c].push_back(o);
     }
@@ -1108,7 +1265,15 @@ int dq_run_batch(int device, const dq_batch_item* items, uint64_t nitems,
   cudaStream_t st = nullptr;
   DQ_CUDA_TRY(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
   int rc = DQ_OK;
-  for (int c = 0; c < 4 && rc == DQ_OK; ++c) {
+  double2* d_hbm = nullptr;
+  if (hbm_amps) {
+    cudaError_t e = cudaMalloc((void**)&d_hbm, sizeof(double2) * hbm_amps);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      rc = fail(DQ_ERR_OOM, std::string("cudaMalloc(batch HBM states): ") + cudaGetErrorString(e));
+    }
+  }
+  for (int c = 0; c < 5 && rc == DQ_OK; ++c) {
     if (outs[c].empty()) continue;
     double2* d_states = nullptr;
     int32_t* d_cbits = nullptr;
@@ -1120,11 +1285,15 @@ int dq_run_batch(int device, const dq_batch_item* items, uint64_t nitems,
     for (const Out& o : outs[c]) {
       if (rc != DQ_OK) break;
       const dq_batch_item& it = items[o.item];
-      uint32_t lb, C;
-      geometry(it.n, max_span, force_lb, &lb, &C);
       const uint32_t pi = (uint32_t)ls.progs.size();
-      rc = add_program(ls, it.prog, it.ninst, it.conds, it.nconds, it.n, lb, it.seed, o.cbits_off,
-                       (uint32_t)it.ncbits, o.state_off == ~0ULL ? nullptr : d_states + o.state_off);
+      if (plan_of[o.item] >= 0) {
+        const uint64_t h = (uint64_t)plan_of[o.item];
+        add_hbm_program(ls, plans[h], it.n, o.cbits_off, (uint32_t)it.ncbits, d_hbm + hbm_off[h]);
+      } else {
+        rc = add_program(ls, it.prog, it.ninst, it.conds, it.nconds, it.n, item_lb[o.item], it.seed,
+                         o.cbits_off, (uint32_t)it.ncbits,
+                         o.state_off == ~0ULL ? nullptr : d_states + o.state_off);
+      }
       ls.items.push_back(TItem{pi, 0, 0});
     }
     acc.prepare_ms += ms_since(tp);
@@ -1132,9 +1301,22 @@ int dq_run_batch(int device, const dq_batch_item* items, uint64_t nitems,
     for (const Out& o : outs[c]) {
       if (rc != DQ_OK) break;
       const dq_batch_item& it = items[o.item];
-      if (it.state_out)
+      e = cudaSuccess;
+      if (plan_of[o.item] >= 0) {
+        // HBM item: undo its sweeps' qubit relabeling, then copy the state out
+        const uint64_t h = (uint64_t)plan_of[o.item];
+        if (it.state_out) {
+          uint64_t extra = 0;
+          rc = materialize_perm(d_hbm + hbm_off[h], it.n, plans[h].perm, st, &extra);
+          acc.launches += (uint32_t)extra;
+          if (rc != DQ_OK) break;
+          e = cudaMemcpyAsync(it.state_out, d_hbm + hbm_off[h], sizeof(double2) << it.n,
+                              cudaMemcpyDeviceToHost, st);
+        }
+      } else if (it.state_out) {
         e = cudaMemcpyAsync(it.state_out, d_states + o.state_off, sizeof(double2) << it.n,
                             cudaMemcpyDeviceToHost, st);
+      }
       if (e == cudaSuccess && it.ncbits)
         e = cudaMemcpyAsync(it.cbits_out, d_cbits + o.cbits_off, sizeof(int32_t) * it.ncbits,
                             cudaMemcpyDeviceToHost, st);
@@ -1152,6 +1334,8 @@ int dq_run_batch(int device, const dq_batch_item* items, uint64_t nitems,
                                         std::to_string(inst) + ": unsupported generic gate");
     }
   }
+  if (d_hbm) cudaFree(d_hbm);
+  acc.hbm_items = (uint32_t)hbm_items.size();
   // large states: the HBM engine, one state per size reused across items
   dq_state_t h = nullptr;
   for (uint64_t k : engine_items) {

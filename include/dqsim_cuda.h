@@ -268,8 +268,12 @@ typedef struct dq_traj_stats {
   uint32_t clusters;     /* clusters resident in the last launch */
   uint32_t threads;
   uint32_t local_bits;   /* amplitudes per CTA = 2^local_bits (largest used) */
-  uint32_t launches;     /* resident launches */
-  uint32_t engine_items; /* dq_run_batch: items with n > 16 (HBM engine) */
+  uint32_t launches;     /* persistent launches (plus relabeling passes of HBM items' outputs) */
+  uint32_t engine_items; /* dq_run_batch: items run one dq_run each (n > 16 with measurements,
+                            resets or conditions) */
+  uint32_t hbm_items;    /* dq_run_batch: unitary items of 17..30 qubits run inside the
+                            persistent launch as HBM-resident fused sweeps */
+  uint32_t reserved;
 } dq_traj_stats;
 
 DQ_API int dq_run_trajectories(int device, uint32_t n, const dq_inst* prog, uint64_t ninst,
@@ -290,12 +294,20 @@ DQ_API int dq_traj_plan_run(dq_traj_plan_t plan, uint64_t base_seed, int32_t* cb
 DQ_API int dq_traj_plan_destroy(dq_traj_plan_t plan);
 
 /* A ragged batch of independent circuits, each one trajectory of the shot
- * semantics above.  Items of up to 16 qubits run resident in shared memory,
- * grouped into one persistent launch per cluster span (1, 2, 4, 8 CTAs),
- * costliest first from a device work queue; larger items run on the HBM
- * engine (dq_run, DQ_SEM_SHOTS, DQ_EXEC_FUSED) one after another.  Outputs go
- * to the caller's host buffers: the classical bits and, when state_out is
- * non-NULL, the final 2^n complex128 amplitudes. */
+ * semantics above (the per-shot loop of statevector/simulator.rs:249-296
+ * over circuits of uneven size), in ONE persistent launch taken costliest
+ * first from a device work queue: items of up to 16 qubits keep their state
+ * in the shared memory of a thread-block cluster; unitary items of 17..30
+ * qubits keep it in HBM and run as fused tile sweeps (the planner of the
+ * fused engine, 2^11-amplitude tiles) by the CTAs of one cluster, with a
+ * cluster barrier between sweeps.  All items share the widest cluster span
+ * any of them needs.  Outside that launch: items whose shared-memory slice
+ * at that span would hold fewer than 16 amplitudes and, with a forced
+ * local_bits, every resident item (launches per cluster span), and large
+ * items with measurements, resets or conditions (the HBM engine, dq_run with
+ * DQ_SEM_SHOTS, one after another).  Outputs go to the caller's host
+ * buffers: the classical bits and, when state_out is non-NULL, the final 2^n
+ * complex128 amplitudes. */
 typedef struct dq_batch_item {
   uint32_t n;
   uint32_t reserved;

@@ -118,6 +118,18 @@ def brickwork_u3_cx(n: int = 20, layers: int = 20, seed: int = 1234) -> JsonCirc
     return JsonCircuit(n, insts)
 
 
+def ragged_batch(count: int = 1024, seed: int = 99, n_lo: int = 10, n_hi: int = 22,
+                 d_lo: int = 5, d_hi: int = 40) -> list:
+    """Independent u3 + cx brickwork circuits of uneven size: n ~ U{n_lo..n_hi}
+    qubits and depth ~ U{d_lo..d_hi} layers (each layer u3 on every qubit with
+    angles ~ U[0, 2pi), then cx on the brickwork pairs), seeded."""
+    rng = np.random.default_rng(seed)
+    ns = rng.integers(n_lo, n_hi + 1, size=count)
+    ds = rng.integers(d_lo, d_hi + 1, size=count)
+    return [brickwork_u3_cx(int(n), int(d), seed=int(seed) * 100003 + k)
+            for k, (n, d) in enumerate(zip(ns, ds))]
+
+
 def qft_with_x(n: int = 30, seed: int = 1234) -> JsonCircuit:
     """x on a seeded random subset (p = 0.5), then the textbook QFT with swaps."""
     rng = np.random.default_rng(seed)

@@ -122,7 +122,9 @@ def test_ragged_batch_states_and_cbits(gpu):
         progs.append(prog_of(circ))
         seeds.append(1000 + k)
     cbits, states, st = run_batch(progs, seeds, want_states=True)
-    assert st.engine_items == 2 and st.launches == 4
+    # 17 and 18 qubits: HBM items of the persistent launch when the sweep
+    # planner represents every gate, otherwise one engine run each
+    assert st.engine_items + st.hbm_items == 2
     for k, p in enumerate(progs):
         want_cb, rc, _ = orc.run_shots(p, seeds[k], 1)
         assert rc == 0
@@ -134,6 +136,47 @@ def test_ragged_batch_states_and_cbits(gpu):
             assert np.max(np.abs(states[k] - ref)) < 1e-12, k
         else:
             assert abs(np.vdot(states[k], states[k]).real - 1.0) < 1e-12
+
+
+def test_ragged_batch_is_one_launch(gpu):
+    """Resident (<= 16 qubits) and HBM-resident (17..19 qubits) items of a
+    ragged u3 + cx batch run in one persistent launch; every final state
+    matches the oracle within 1e-12."""
+    ns = [10, 11, 13, 14, 16, 17, 18, 19, 12, 15]
+    rng = np.random.default_rng(5)
+    progs = [prog_of(_circuits.brickwork_u3_cx(n, int(rng.integers(5, 16)), seed=40 + k))
+             for k, n in enumerate(ns)]
+    seeds = [7 + k for k in range(len(ns))]
+    cbits, states, st = run_batch(progs, seeds, want_states=True)
+    assert st.launches == 1 and st.engine_items == 0 and st.hbm_items == 3
+    assert st.cluster_span == 8
+    for k, p in enumerate(progs):
+        ref, _, rc, _ = orc.run(p, 0)
+        assert rc == 0
+        assert np.max(np.abs(states[k] - ref)) < 1e-12, (k, ns[k])
+
+
+def test_ragged_batch_hbm_item_with_swaps_and_x(gpu):
+    """An HBM item whose sweeps relabel qubits (swap) and open with X gates:
+    its state is put back in canonical order before it is copied out."""
+    n = 18
+    insts = [g("x", 3), g("x", 17), g("h", 0), g("swap", 0, 17), g("cx", 17, 5), g("swap", 2, 11),
+             g("u3", 11, 0.3, 0.2, 0.1), g("cp", 4, 16, 0.7), g("h", 16)]
+    progs = [prog_of(JsonCircuit(n, insts)), prog_of(_circuits.brickwork_u3_cx(12, 4, seed=3))]
+    cbits, states, st = run_batch(progs, [1, 2], want_states=True)
+    assert st.hbm_items == 1 and st.engine_items == 0
+    for k, p in enumerate(progs):
+        ref, _, rc, _ = orc.run(p, 0)
+        assert rc == 0
+        assert np.max(np.abs(states[k] - ref)) < 1e-12, k
+
+
+def test_ragged_batch_partial_state_outputs(gpu):
+    progs = [prog_of(_circuits.brickwork_u3_cx(n, 4, seed=n)) for n in (11, 17, 12)]
+    _, states, st = run_batch(progs, [1, 2, 3], want_states=[1])
+    assert states[0] is None and states[2] is None
+    ref, _, _, _ = orc.run(progs[1], 0)
+    assert np.max(np.abs(states[1] - ref)) < 1e-12
 
 
 def test_unsupported_gate_reached(gpu):
