@@ -691,13 +691,16 @@ def adjoint_section(dev: int) -> dict:
     }
 
 
-def adjoint_batch_section(dev: int, adam_steps: int, workers: int = 4) -> dict:
+def adjoint_batch_section(dev: int, adam_steps: int) -> dict:
     """512 parameter sets of the 20-qubit, 8-layer ansatz (480 parameters
     each) through the torch autograd function, driving Adam (lr 0.01) on the
-    sum of the energies.  Times `adam_steps` steps after one warm-up step."""
+    sum of the energies.  Every set's gradient comes from one batched adjoint
+    call per step (dq_adjoint_batch: each forward sweep, lambda = H psi and
+    each backward sweep is one launch over all 512 sets).  Times `adam_steps`
+    steps after one warm-up step."""
     import torch
 
-    from dqsim_bosonic_b200.adjoint import expval
+    from dqsim_bosonic_b200.adjoint import adjoint_gradient_batch, expval
 
     c, theta, H = _circuits.hea_param_circuit(20, 8, seed=1)
     B = 512
@@ -707,7 +710,7 @@ def adjoint_batch_section(dev: int, adam_steps: int, workers: int = 4) -> dict:
 
     def step():
         opt.zero_grad()
-        e = expval(t, c, H, device=dev, workers=workers)
+        e = expval(t, c, H, device=dev)
         e.sum().backward()
         opt.step()
         return e.detach()
@@ -717,6 +720,8 @@ def adjoint_batch_section(dev: int, adam_steps: int, workers: int = 4) -> dict:
     for _ in range(adam_steps):
         e = step()
     dt = (time.perf_counter() - t0) / max(adam_steps, 1)
+    st = {}
+    adjoint_gradient_batch(c, t.detach().numpy(), H, device=dev, stats=st)
     return {
         "workload": "512 parameter sets x hea20 (8 layers, 480 params), Adam lr 0.01 on sum <H>",
         "s_per_adam_step": dt,
@@ -725,7 +730,13 @@ def adjoint_batch_section(dev: int, adam_steps: int, workers: int = 4) -> dict:
         "projected_s_for_50_steps": 50 * dt,
         "mean_energy_first": float(e0.mean()),
         "mean_energy_last": float(e.mean()),
-        "workers": workers,
+        "launches_per_gradient_batch": int(st["launches"]),
+        "forward_sweeps": int(st["forward_sweeps"]),
+        "backward_sweeps": int(st["backward_sweeps"]),
+        "phases_ms": {"plan": st["plan_ms"], "forward": st["forward_ms"],
+                      "observable": st["observable_ms"], "backward": st["backward_ms"]},
+        "batched": bool(st["batched"]),
+        "set_groups": int(st["groups"]),
     }
 
 

@@ -126,6 +126,20 @@ class TrajStats(ctypes.Structure):
     ]
 
 
+class AdjointBatchStats(ctypes.Structure):
+    _fields_ = [
+        ("launches", ctypes.c_uint64),
+        ("forward_sweeps", ctypes.c_uint64),
+        ("backward_sweeps", ctypes.c_uint64),
+        ("plan_ms", ctypes.c_double),
+        ("forward_ms", ctypes.c_double),
+        ("observable_ms", ctypes.c_double),
+        ("backward_ms", ctypes.c_double),
+        ("batched", ctypes.c_uint32),
+        ("groups", ctypes.c_uint32),
+    ]
+
+
 class BatchItem(ctypes.Structure):
     _fields_ = [
         ("n", ctypes.c_uint32),
@@ -200,6 +214,8 @@ SIGNATURES = [
     ("dq_expval_pauli", ctypes.c_int, [_P, _P, _U64, _DP]),
     ("dq_adjoint", ctypes.c_int, [_P, _P, _U64, _P, _U64, _P, _U64, ctypes.POINTER(RunOpts), _DP,
                                   _P, _P]),
+    ("dq_adjoint_batch", ctypes.c_int, [ctypes.c_int, _U32, _P, _U64, _P, _U64, _P, _U64, _P, _U64,
+                                        _P, _P, ctypes.POINTER(AdjointBatchStats)]),
     ("dq_debug_plan", ctypes.c_int, [_U32, _P, _U64, ctypes.POINTER(RunOpts), _P, _U64,
                                      ctypes.POINTER(_U64)]),
     ("dq_block_merge", ctypes.c_int, [_P, _P, _U32, _P, _P, _U32, _P]),

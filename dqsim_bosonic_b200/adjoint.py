@@ -333,20 +333,27 @@ def adjoint_gradient(circuit: ParamCircuit, theta, observable: PauliSum, *, devi
 
 
 def adjoint_gradient_batch(circuit: ParamCircuit, thetas, observable: PauliSum, *,
-                           device: int = 0, exec: str = "fused", workers: int = 4):
+                           device: int = 0, exec: str = "fused", workers: int = 0,
+                           stats: dict | None = None):
     """``(E[B], dE/dtheta[B, P])`` for a batch of parameter sets.
 
-    Each set runs the adjoint pass on its own engine state; ``workers`` sets
-    are in flight at once on separate CUDA streams (one host thread each; the
-    engine calls release the GIL), which keeps the GPU busy when one set's
-    state is small enough to be launch-bound."""
+    Default (``workers = 0``, fused exec): one ``dq_adjoint_batch`` call runs
+    every set together -- each fused forward sweep, lambda = H psi and each
+    fused backward sweep is ONE launch over all sets.  ``workers > 0``: the
+    sets run one adjoint pass each, ``workers`` of them in flight at once on
+    separate engine states (host threads).  ``stats``: a dict that receives
+    the batched call's launch count, sweep counts and phase times."""
     th = np.asarray(thetas, dtype=np.float64)
     if th.ndim != 2:
         raise ValueError("thetas must be 2-D: (sets, parameters)")
     B = th.shape[0]
+    if th.shape[1] != circuit.num_params:
+        raise ValueError(f"thetas have {th.shape[1]} columns, the circuit {circuit.num_params}")
     es = np.empty(B)
     gs = np.empty((B, circuit.num_params))
-    workers = max(1, min(int(workers), B))
+    if workers <= 0 and _exec_mode(exec) == nat.EXEC_FUSED:
+        return _adjoint_batch_native(circuit, th, observable, device, stats)
+    workers = max(1, min(int(workers) if workers > 0 else 4, B))
 
     def run(w):
         for b in range(w, B, workers):
@@ -359,6 +366,33 @@ def adjoint_gradient_batch(circuit: ParamCircuit, thetas, observable: PauliSum, 
         with ThreadPoolExecutor(max_workers=workers) as ex:
             for f in [ex.submit(run, w) for w in range(workers)]:
                 f.result()
+    return es, gs
+
+
+def _adjoint_batch_native(circuit: ParamCircuit, th: np.ndarray, observable: PauliSum, device: int,
+                          stats: dict | None):
+    terms = _check_observable(circuit, observable)
+    B = th.shape[0]
+    insts = circuit.bind(th[0])
+    occ = circuit.occurrences()
+    slots = circuit.param_slots()
+    idx = np.array([p.index for (_, _, p) in occ], dtype=np.int64)
+    scale = np.array([p.scale for (_, _, p) in occ], dtype=np.float64)
+    shift = np.array([p.shift for (_, _, p) in occ], dtype=np.float64)
+    # value of every trainable occurrence in every set
+    vals = np.ascontiguousarray(th[:, idx] * scale + shift) if len(occ) else np.zeros((B, 1))
+    es = np.zeros(B, dtype=np.float64)
+    g_occ = np.zeros((B, max(1, len(occ))), dtype=np.float64)
+    st = nat.AdjointBatchStats()
+    nat.check(nat.lib().dq_adjoint_batch(int(device), circuit.num_qubits, nat.ptr(insts), len(insts),
+                                         nat.ptr(slots), len(occ), nat.ptr(vals), B, nat.ptr(terms),
+                                         len(terms), nat.ptr(es), nat.ptr(g_occ), ctypes.byref(st)),
+              "dq_adjoint_batch")
+    if stats is not None:
+        stats.update({name: getattr(st, name) for name, _ in nat.AdjointBatchStats._fields_})
+    gs = np.zeros((B, circuit.num_params), dtype=np.float64)
+    if len(occ):
+        np.add.at(gs.T, idx, (g_occ[:, :len(occ)] * scale).T)
     return es, gs
 
 
@@ -455,7 +489,8 @@ class AdjointExpectation:
 
 
 def expval(theta, circuit: ParamCircuit, observable: PauliSum, *, device: int = 0,
-           exec: str = "fused", workers: int = 4):
+           exec: str = "fused", workers: int = 0):
     """Differentiable ``<H>`` (torch tensor in, torch tensor out); a 2-D
-    ``theta`` is a batch of parameter sets run ``workers`` at a time."""
+    ``theta`` is a batch of parameter sets, run together by one batched
+    adjoint call (``workers > 0``: that many sets at a time on host threads)."""
     return AdjointExpectation.function().apply(theta, circuit, observable, device, exec, workers)

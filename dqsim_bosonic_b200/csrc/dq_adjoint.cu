@@ -22,13 +22,16 @@
 #include <stdint.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "dq_adjsweep.cuh"
 #include "dq_common.cuh"
 #include "dq_engine.cuh"
+#include "dq_fused.cuh"
 #include "dq_gates.hpp"
 #include "dq_handle.cuh"
 #include "dq_reduce.cuh"
@@ -54,10 +57,10 @@ __device__ __forceinline__ double2 cfma(double2 a, double2 b, double2 acc) {
 
 // lambda = H psi (when STORE) and E = Re <psi|H psi>.
 template <bool STORE>
-__global__ void k_pauli(const double2* __restrict__ psi, double2* __restrict__ lam, uint64_t len,
-                        const PauliGroup* __restrict__ groups, uint32_t ngroups,
-                        const PauliTerm* __restrict__ terms, double* partial, unsigned* counter,
-                        double* out) {
+__device__ __forceinline__ void pauli_body(const double2* __restrict__ psi, double2* __restrict__ lam,
+                                           uint64_t len, const PauliGroup* __restrict__ groups,
+                                           uint32_t ngroups, const PauliTerm* __restrict__ terms,
+                                           double* partial, unsigned* counter, double* out) {
   double e = 0.0;
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
   for (uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; j < len; j += stride) {
@@ -81,6 +84,26 @@ __global__ void k_pauli(const double2* __restrict__ psi, double2* __restrict__ l
   }
   double v[1] = {e};
   finish_partials<1>(v, partial, counter, out);
+}
+
+template <bool STORE>
+__global__ void k_pauli(const double2* __restrict__ psi, double2* __restrict__ lam, uint64_t len,
+                        const PauliGroup* __restrict__ groups, uint32_t ngroups,
+                        const PauliTerm* __restrict__ terms, double* partial, unsigned* counter,
+                        double* out) {
+  pauli_body<STORE>(psi, lam, len, groups, ngroups, terms, partial, counter, out);
+}
+
+// The same for B states in one launch: state b (blockIdx.y) at psi + b len,
+// its lambda at lam + b len, its reduction scratch at partial + b gridDim.x
+// and counter + b, its expectation value at out[b * out_stride].
+__global__ void k_pauli_multi(const double2* __restrict__ psi, double2* __restrict__ lam,
+                              uint64_t len, const PauliGroup* __restrict__ groups, uint32_t ngroups,
+                              const PauliTerm* __restrict__ terms, double* partial,
+                              unsigned* counter, double* out, uint64_t out_stride) {
+  const uint64_t b = blockIdx.y;
+  pauli_body<true>(psi + b * len, lam + b * len, len, groups, ngroups, terms,
+                   partial + b * gridDim.x, counter + b, out + b * out_stride);
 }
 
 // One parametrised 2x2 gate (controls: all set) on psi and lambda.
@@ -326,8 +349,8 @@ bool is_noop_kind(int kind) {
 }
 
 // Validates a unitary program and its parameter map; counts differentiated slots.
-int check_program(dq_state_t h, const dq_inst* prog, uint64_t ninst, const int32_t* pidx,
-                  uint64_t nparams, uint64_t* nslots) {
+int check_program_n(uint32_t n, const dq_inst* prog, uint64_t ninst, const int32_t* pidx,
+                    uint64_t nparams, uint64_t* nslots) {
   if (ninst && !prog) return fail(DQ_ERR_INVALID_ARG, "null program");
   if (nparams && !pidx) return fail(DQ_ERR_INVALID_ARG, "null param_index with nparams > 0");
   if (nparams > (1ULL << 31)) return fail(DQ_ERR_INVALID_ARG, "too many parameters");
@@ -339,7 +362,7 @@ int check_program(dq_state_t h, const dq_inst* prog, uint64_t ninst, const int32
       return fail(DQ_ERR_UNSUPPORTED, "instruction " + std::to_string(i) +
                                           ": adjoint differentiation needs a unitary program "
                                           "(gates only, no measure/reset/conditions)");
-    DQ_TRY(validate_inst(in, h->n, 0, 0, nullptr, i));
+    DQ_TRY(validate_inst(in, n, 0, 0, nullptr, i));
     if (!pidx) continue;
     const int np = diff_param_count(in.kind);
     for (int j = 0; j < 4; ++j) {
@@ -356,6 +379,11 @@ int check_program(dq_state_t h, const dq_inst* prog, uint64_t ninst, const int32
   }
   *nslots = s;
   return DQ_OK;
+}
+
+int check_program(dq_state_t h, const dq_inst* prog, uint64_t ninst, const int32_t* pidx,
+                  uint64_t nparams, uint64_t* nslots) {
+  return check_program_n(h->n, prog, ninst, pidx, nparams, nslots);
 }
 
 struct DeviceTerms {
@@ -630,6 +658,261 @@ int dq_adjoint(dq_state_t h, const dq_inst* prog, uint64_t ninst, const int32_t*
     }
   }
   return DQ_OK;
+}
+
+
+int dq_adjoint_batch(int device, uint32_t n, const dq_inst* prog, uint64_t ninst,
+                     const int32_t* param_index, uint64_t nparams, const double* values,
+                     uint64_t nsets, const dq_pauli_term* terms, uint64_t nterms, double* expvals,
+                     double* grads, dq_adjoint_batch_stats* stats) {
+  dq_adjoint_batch_stats acc{};
+  if (stats) *stats = acc;
+  if (n < 1 || n > kMaxQubits) return fail(DQ_ERR_INVALID_ARG, "nqubits must be in 1..34");
+  uint64_t nslots = 0;
+  DQ_TRY(check_program_n(n, prog, ninst, param_index, nparams, &nslots));
+  if (nsets && (!expvals || (nparams && (!grads || !values))))
+    return fail(DQ_ERR_INVALID_ARG, "null values or outputs");
+  if (nsets == 0) return DQ_OK;
+  int ndev = 0;
+  DQ_TRY(dq_device_count(&ndev));
+  if (device < 0 || device >= ndev) return fail(DQ_ERR_INVALID_ARG, "device index out of range");
+  DeviceGuard g(device);
+  const auto t0 = std::chrono::steady_clock::now();
+  // each set's program: the parameter slots replaced by its values
+  std::vector<std::vector<dq_inst>> progs(nsets);
+  for (uint64_t s = 0; s < nsets; ++s) {
+    progs[s].assign(prog, prog + ninst);
+    if (!param_index) continue;
+    for (uint64_t i = 0; i < ninst; ++i)
+      for (int j = 0; j < 4; ++j) {
+        const int32_t v = param_index[4 * i + j];
+        if (v >= 0) progs[s][i].p[j] = values[s * nparams + (uint64_t)v];
+      }
+  }
+  // plan every set on host threads: forward sweeps from |0...0>, backward sweeps
+  struct SetPlan {
+    std::vector<uint8_t> fblob;
+    std::vector<uint64_t> foffs;
+    uint32_t perm[64];
+    int64_t synth = -1;
+    uint32_t rb = 0;
+    ABatchSet back;
+    int rc = DQ_OK;
+  };
+  std::vector<SetPlan> plans(nsets);
+  bool batched = n >= kFusedMinQubits;
+  if (batched) {
+    const unsigned hw = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    const unsigned nt = (unsigned)std::min<uint64_t>(hw, nsets);
+    auto work = [&](unsigned t) {
+      for (uint64_t s = t; s < nsets; s += nt) {
+        SetPlan& P = plans[s];
+        for (uint32_t l = 0; l < 64; ++l) P.perm[l] = l;
+        P.rc = fused_plan(n, progs[s].data(), ninst, DQ_SEM_SIMULATE, 7, 0, 0, &P.fblob, &P.foffs,
+                          P.perm, &P.synth, &P.rb);
+        if (P.rc == DQ_OK)
+          P.rc = adjoint_backward_plan_set(n, progs[s].data(), ninst, param_index, nslots, &P.back);
+      }
+    };
+    std::vector<std::thread> th;
+    for (unsigned t = 1; t < nt; ++t) th.emplace_back(work, t);
+    work(0);
+    for (auto& x : th) x.join();
+    uint32_t rb = 0;
+    for (uint64_t s = 0; s < nsets; ++s)
+      if (!plans[s].foffs.empty()) rb = plans[s].rb;
+    for (uint64_t s = 0; s < nsets && batched; ++s)
+      if (plans[s].rc != DQ_OK || plans[s].back.sweeps() == 0 ||
+          (!plans[s].foffs.empty() && plans[s].rb != rb))
+        batched = false;
+    clear_error();
+  }
+  acc.plan_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  if (!batched) {
+    // set by set through dq_adjoint on one engine state
+    dq_state_t h = nullptr;
+    DQ_TRY(dq_state_create(n, device, &h));
+    dq_run_opts o{};
+    o.exec = DQ_EXEC_FUSED;
+    int rc = DQ_OK;
+    for (uint64_t s = 0; s < nsets && rc == DQ_OK; ++s) {
+      rc = dq_state_reset(h);
+      if (rc == DQ_OK)
+        rc = dq_adjoint(h, progs[s].data(), ninst, param_index, nparams, terms, nterms, &o,
+                        expvals + s, nparams ? grads + s * nparams : nullptr, nullptr);
+    }
+    dq_state_destroy(h);
+    acc.groups = (uint32_t)nsets;
+    if (stats) *stats = acc;
+    return rc;
+  }
+  uint32_t rb = 0;
+  for (uint64_t s = 0; s < nsets; ++s)
+    if (!plans[s].foffs.empty()) rb = plans[s].rb;
+  const uint64_t len = 1ULL << n;
+  // sets resident at a time: psi and lambda of each in about half the free memory
+  size_t freeb = 0, totalb = 0;
+  DQ_CUDA_TRY(cudaMemGetInfo(&freeb, &totalb));
+  const uint64_t per_set = 2 * sizeof(double2) * len + 64 * 1024;
+  const uint64_t G = std::max<uint64_t>(1, std::min<uint64_t>(nsets, (freeb / 2) / per_set));
+  cudaStream_t st = nullptr;
+  DQ_CUDA_TRY(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+  int rc = DQ_OK;
+  auto cu = [&](cudaError_t e, const char* what) {
+    if (e != cudaSuccess && rc == DQ_OK) {
+      cudaGetLastError();
+      rc = fail(e == cudaErrorMemoryAllocation ? DQ_ERR_OOM : DQ_ERR_CUDA,
+                std::string(what) + ": " + cudaGetErrorString(e));
+    }
+  };
+  DeviceTerms t;
+  rc = upload_terms(terms, nterms, n, st, &t);
+  double2 *psi = nullptr, *lam = nullptr;
+  double* slots = nullptr;
+  double* part = nullptr;
+  unsigned* ctr = nullptr;
+  uint8_t* fblob = nullptr;
+  SweepJob* d_jobs = nullptr;
+  const unsigned pblocks = reduction_blocks(len, device);
+  const uint64_t sl = nslots + 1;  // per set: gradient slots, then E
+  // all forward programs in one device buffer
+  std::vector<uint8_t> fall;
+  std::vector<uint64_t> fbase(nsets, 0);
+  size_t kf = 0, kb = 0;
+  for (uint64_t s = 0; s < nsets; ++s) {
+    while (fall.size() % 16) fall.push_back(0);
+    fbase[s] = fall.size();
+    fall.insert(fall.end(), plans[s].fblob.begin(), plans[s].fblob.end());
+    kf = std::max(kf, plans[s].foffs.size());
+    kb = std::max(kb, plans[s].back.sweeps());
+  }
+  if (fall.empty()) fall.push_back(0);
+  acc.forward_sweeps = kf;
+  acc.backward_sweeps = kb;
+  if (rc == DQ_OK) {
+    cu(cudaMalloc((void**)&psi, sizeof(double2) * len * G), "cudaMalloc(psi)");
+    cu(cudaMalloc((void**)&lam, sizeof(double2) * len * G), "cudaMalloc(lambda)");
+    cu(cudaMalloc((void**)&slots, sizeof(double) * sl * G), "cudaMalloc(slots)");
+    cu(cudaMalloc((void**)&part, sizeof(double) * pblocks * G), "cudaMalloc(partials)");
+    cu(cudaMalloc((void**)&ctr, sizeof(unsigned) * G), "cudaMalloc(counters)");
+    cu(cudaMalloc((void**)&fblob, fall.size()), "cudaMalloc(programs)");
+    cu(cudaMalloc((void**)&d_jobs, sizeof(SweepJob) * std::max<size_t>(1, kf * G)), "cudaMalloc(jobs)");
+  }
+  if (rc == DQ_OK) {
+    cu(cudaMemcpyAsync(fblob, fall.data(), fall.size(), cudaMemcpyHostToDevice, st), "copy programs");
+    cu(cudaMemsetAsync(ctr, 0, sizeof(unsigned) * G, st), "memset");
+  }
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  for (auto& e : ev) cu(cudaEventCreate(&e), "cudaEventCreate");
+  std::vector<double> host(sl * G);
+  for (uint64_t g0 = 0; g0 < nsets && rc == DQ_OK; g0 += G) {
+    const uint64_t g1 = std::min(nsets, g0 + G), ng = g1 - g0;
+    ++acc.groups;
+    // forward: sweep k of every set of the group in one launch per run width
+    struct Range { size_t begin, end; uint32_t run_bits; };
+    std::vector<SweepJob> jobs;
+    std::vector<Range> ranges;
+    for (size_t k = 0; k < kf; ++k)
+      for (uint32_t rbits : {5u, 3u}) {
+        const size_t b0 = jobs.size();
+        for (uint64_t s = g0; s < g1; ++s) {
+          if (k >= plans[s].foffs.size()) continue;
+          const uint8_t* hp = plans[s].fblob.data() + plans[s].foffs[k];
+          if (sweep_run_bits(hp) != rbits) continue;
+          jobs.push_back(SweepJob{psi + (s - g0) * len, fblob + fbase[s] + plans[s].foffs[k],
+                                  k == 0 ? (long long)plans[s].synth : -1LL});
+        }
+        if (jobs.size() > b0) ranges.push_back(Range{b0, jobs.size(), rbits});
+      }
+    if (!jobs.empty())
+      cu(cudaMemcpyAsync(d_jobs, jobs.data(), sizeof(SweepJob) * jobs.size(), cudaMemcpyHostToDevice, st),
+         "copy jobs");
+    cu(cudaEventRecord(ev[0], st), "event");
+    for (const Range& r : ranges) {
+      if (rc != DQ_OK) break;
+      rc = launch_sweep_multi(d_jobs + r.begin, (uint32_t)(r.end - r.begin), n, rb, r.run_bits, st);
+      ++acc.launches;
+    }
+    for (uint64_t s = g0; s < g1 && rc == DQ_OK; ++s) {
+      double2* ps = psi + (s - g0) * len;
+      if (plans[s].foffs.empty()) {  // no sweep: the state is a basis vector
+        rc = launch_set_basis(ps, n, (uint64_t)std::max<int64_t>(plans[s].synth, 0), st, device);
+        ++acc.launches;
+      }
+      uint64_t extra = 0;
+      if (rc == DQ_OK) rc = materialize_perm(ps, n, plans[s].perm, st, &extra);
+      acc.launches += extra;
+    }
+    cu(cudaEventRecord(ev[1], st), "event");
+    // lambda = H psi and E for every set of the group
+    if (rc == DQ_OK) {
+      k_pauli_multi<<<dim3(pblocks, (unsigned)ng), kRedThreads, 0, st>>>(
+          psi, lam, len, t.groups, t.ngroups, t.terms, part, ctr, slots + nslots, sl);
+      cu(cudaGetLastError(), "k_pauli_multi");
+      ++acc.launches;
+    }
+    cu(cudaEventRecord(ev[2], st), "event");
+    // backward: sweep k of every set of the group in one launch
+    if (rc == DQ_OK) {
+      std::vector<double2*> pp(ng), lp(ng);
+      std::vector<double*> sp(ng);
+      for (uint64_t s = 0; s < ng; ++s) {
+        pp[s] = psi + s * len;
+        lp[s] = lam + s * len;
+        sp[s] = slots + s * sl;
+      }
+      std::vector<ABatchSet> bs;
+      bs.reserve(ng);
+      for (uint64_t s = g0; s < g1; ++s) bs.push_back(std::move(plans[s].back));
+      uint64_t nl = 0;
+      rc = adjoint_backward_batch(pp.data(), lp.data(), bs, sp.data(), st, device, &nl);
+      acc.launches += nl;
+    }
+    cu(cudaEventRecord(ev[3], st), "event");
+    if (rc == DQ_OK)
+      cu(cudaMemcpyAsync(host.data(), slots, sizeof(double) * sl * ng, cudaMemcpyDeviceToHost, st),
+         "copy slots");
+    cu(cudaStreamSynchronize(st), "sync");
+    if (rc == DQ_OK) {
+      float a = 0.f, b = 0.f, c = 0.f;
+      cudaEventElapsedTime(&a, ev[0], ev[1]);
+      cudaEventElapsedTime(&b, ev[1], ev[2]);
+      cudaEventElapsedTime(&c, ev[2], ev[3]);
+      acc.forward_ms += a;
+      acc.observable_ms += b;
+      acc.backward_ms += c;
+      for (uint64_t s = g0; s < g1; ++s) {
+        const double* h = host.data() + (s - g0) * sl;
+        expvals[s] = h[nslots];
+        double* gr = nparams ? grads + s * nparams : nullptr;
+        for (uint64_t p = 0; p < nparams; ++p) gr[p] = 0.0;
+        uint64_t k = 0;
+        for (uint64_t i = 0; i < ninst; ++i) {
+          if (!param_index || is_noop_kind(prog[i].kind)) continue;
+          for (int j = 0; j < 4; ++j) {
+            const int32_t v = param_index[4 * i + j];
+            if (v >= 0) gr[v] += 2.0 * h[k++];
+          }
+        }
+      }
+    }
+  }
+  cudaStreamSynchronize(st);
+  for (auto& e : ev)
+    if (e) cudaEventDestroy(e);
+  free_terms(t, st);
+  cudaStreamSynchronize(st);
+  if (psi) cudaFree(psi);
+  if (lam) cudaFree(lam);
+  if (slots) cudaFree(slots);
+  if (part) cudaFree(part);
+  if (ctr) cudaFree(ctr);
+  if (fblob) cudaFree(fblob);
+  if (d_jobs) cudaFree(d_jobs);
+  cudaStreamDestroy(st);
+  acc.batched = 1;
+  if (stats) *stats = acc;
+  return rc;
 }
 
 }  // extern "C"

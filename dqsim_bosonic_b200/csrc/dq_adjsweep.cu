@@ -87,6 +87,19 @@ struct ASweepHdr {
   uint32_t pad;
 };
 
+// One sweep of one (psi, lambda) pair in a multi-job launch.
+struct AJob {
+  double2* psi;
+  double2* lam;
+  const ASweepHdr* hdr;
+  const AOp* ops;
+  const double2* pool;
+  double* partial;       // [slot][chunk]
+  const uint32_t* map;   // sweep-local slot -> index into out
+  double* out;           // the pair's gradient slots
+  uint32_t nslots, pad;
+};
+
 __device__ __forceinline__ double2 cfma2(double2 a, double2 b, double2 acc) {
   return make_double2(fma(a.x, b.x, fma(-a.y, b.y, acc.x)), fma(a.x, b.y, fma(a.y, b.x, acc.y)));
 }
@@ -640,9 +653,15 @@ __device__ __noinline__ void op_phase(double2* sp, double2* sl, const AOp& hdr, 
   }
 }
 
-__global__ void __launch_bounds__(kAThreads, 2)
-    k_adj_sweep(double2* __restrict__ psi, double2* __restrict__ lam, const ASweepHdr* __restrict__ hp,
-                const AOp* __restrict__ ops, const double2* __restrict__ pool, double* partial) {
+// One backward sweep over tiles t0, t0 + step, ... (< t1) of psi and lambda;
+// the CTA's gradient sums go to partial[slot * nparts + part].  Every thread
+// of the CTA calls it; the caller separates consecutive calls by a barrier.
+__device__ __forceinline__ void adj_sweep_body(double2* __restrict__ psi, double2* __restrict__ lam,
+                                               const ASweepHdr* __restrict__ hp,
+                                               const AOp* __restrict__ ops,
+                                               const double2* __restrict__ pool, double* partial,
+                                               uint32_t part, uint32_t nparts, uint64_t t0,
+                                               uint64_t t1, uint64_t step) {
   extern __shared__ __align__(16) unsigned char smraw[];
   __shared__ ASweepHdr H;
   __shared__ uint64_t hi_tab[1u << (kAMaxLocal - kALoMin)];
@@ -683,7 +702,7 @@ __global__ void __launch_bounds__(kAThreads, 2)
   __syncthreads();
   const uint32_t lo_mask = (1u << lo_bits) - 1u;
 
-  for (uint64_t t = blockIdx.x; t < H.ntiles; t += gridDim.x) {
+  for (uint64_t t = t0; t < t1 && t < H.ntiles; t += step) {
     uint64_t base = 0;
     for (uint32_t b = 0; b < H.npos_cnt; ++b)
       if (t >> b & 1ULL) base |= 1ULL << H.npos[b];
@@ -743,8 +762,42 @@ __global__ void __launch_bounds__(kAThreads, 2)
   for (uint32_t s = threadIdx.x; s < H.nslots; s += kAThreads) {
     double a = 0.0;
     for (int w = 0; w < kAWarps; ++w) a += accw[s * kAWarps + w];
-    partial[(size_t)s * gridDim.x + blockIdx.x] = a;
+    partial[(size_t)s * nparts + part] = a;
   }
+}
+
+__global__ void __launch_bounds__(kAThreads, 2)
+    k_adj_sweep(double2* __restrict__ psi, double2* __restrict__ lam, const ASweepHdr* __restrict__ hp,
+                const AOp* __restrict__ ops, const double2* __restrict__ pool, double* partial) {
+  adj_sweep_body(psi, lam, hp, ops, pool, partial, blockIdx.x, gridDim.x, blockIdx.x, ~0ULL,
+                 gridDim.x);
+}
+
+// Sweep k of many independent (psi, lambda) pairs in one launch: job j is
+// one parameter set's sweep, split into chunks of chunk_tiles consecutive
+// tiles; the CTAs take (job, chunk) work items in order.  Chunk c of job j
+// writes its sums to jobs[j].partial[slot * nchunks + c].
+__global__ void __launch_bounds__(kAThreads, 2)
+    k_adj_sweep_multi(const AJob* __restrict__ jobs, uint32_t njobs, uint32_t nchunks,
+                      uint64_t chunk_tiles) {
+  const uint64_t work = (uint64_t)njobs * nchunks;
+  for (uint64_t w = blockIdx.x; w < work; w += gridDim.x) {
+    const AJob J = jobs[w / nchunks];
+    const uint32_t c = (uint32_t)(w % nchunks);
+    adj_sweep_body(J.psi, J.lam, J.hdr, J.ops, J.pool, J.partial, c, nchunks, c * chunk_tiles,
+                   (c + 1) * chunk_tiles, 1);
+    __syncthreads();
+  }
+}
+
+// jobs[j].out[map[s]] = sum over chunks (in order) of jobs[j].partial[s][chunk]
+__global__ void k_adj_slots_multi(const AJob* __restrict__ jobs, uint32_t nchunks) {
+  const AJob J = jobs[blockIdx.y];
+  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= J.nslots) return;
+  double a = 0.0;
+  for (uint32_t c = 0; c < nchunks; ++c) a += J.partial[(size_t)s * nchunks + c];
+  J.out[J.map[s]] = a;
 }
 
 // out[map[s]] = sum over CTAs (in order) of partial[s][cta]
@@ -1165,11 +1218,16 @@ int sweep_ctas(int device) {
   return per_sm[device & 63];
 }
 
-}  // namespace
+// Segments of the backward pass in backward order: fused sweeps and the
+// instructions undone one at a time (three or more qubits).
+struct BackSeg {
+  bool sweep;
+  ASweepPlan plan;
+  int64_t inst;
+};
 
-int adjoint_backward_fused(double2* psi, double2* lam, uint32_t n, const dq_inst* prog,
-                           uint64_t ninst, const int32_t* pidx, uint64_t nslots, double* d_slots,
-                           cudaStream_t st, int device, AdjSweepStats* stats) {
+int plan_backward_segments(uint32_t n, const dq_inst* prog, uint64_t ninst, const int32_t* pidx,
+                           uint64_t nslots, std::vector<BackSeg>& segs) {
   // global slot numbering: program order, parameter order within a gate
   std::vector<uint32_t> first_slot(ninst + 1, 0);
   for (uint64_t i = 0; i < ninst; ++i) {
@@ -1182,13 +1240,6 @@ int adjoint_backward_fused(double2* psi, double2* lam, uint32_t n, const dq_inst
   const uint32_t m_max = std::min<uint32_t>(n, kAMaxLocal);
   const uint32_t lo = std::min<uint32_t>(n, kALoMin);
   const uint64_t lo_mask = (1ULL << lo) - 1;
-  // segments: sweeps and per-gate instructions, in backward order
-  struct Seg {
-    bool sweep;
-    ASweepPlan plan;
-    int64_t inst;
-  };
-  std::vector<Seg> segs;
   ASweepPlan cur;
   cur.Lmask = lo_mask;
   uint32_t cur_slots = 0;
@@ -1198,7 +1249,7 @@ int adjoint_backward_fused(double2* psi, double2* lam, uint32_t n, const dq_inst
       // work per tile, fewer tiles; the set only needs to contain the gates')
       for (uint32_t q = 0; q < n && (uint32_t)__builtin_popcountll(cur.Lmask) < m_max; ++q)
         cur.Lmask |= 1ULL << q;
-      segs.push_back(Seg{true, cur, -1});
+      segs.push_back(BackSeg{true, cur, -1});
     }
     cur = ASweepPlan();
     cur.Lmask = lo_mask;
@@ -1213,7 +1264,7 @@ int adjoint_backward_fused(double2* psi, double2* lam, uint32_t n, const dq_inst
     DQ_TRY(classify_gate(in, pidx, r, first_slot[r], g));
     if (g.kind == 4) {
       close();
-      segs.push_back(Seg{false, ASweepPlan(), (int64_t)r});
+      segs.push_back(BackSeg{false, ASweepPlan(), (int64_t)r});
       continue;
     }
     const uint64_t need = need_local(g);
@@ -1227,7 +1278,17 @@ int adjoint_backward_fused(double2* psi, double2* lam, uint32_t n, const dq_inst
     cur_slots += (uint32_t)g.np;
   }
   close();
+  return DQ_OK;
+}
 
+}  // namespace
+
+int adjoint_backward_fused(double2* psi, double2* lam, uint32_t n, const dq_inst* prog,
+                           uint64_t ninst, const int32_t* pidx, uint64_t nslots, double* d_slots,
+                           cudaStream_t st, int device, AdjSweepStats* stats) {
+  using Seg = BackSeg;
+  std::vector<Seg> segs;
+  DQ_TRY(plan_backward_segments(n, prog, ninst, pidx, nslots, segs));
   const int ctas_max = sweep_ctas(device);
   if (ctas_max <= 0) return DQ_ERR_CUDA;
   // device buffers for all sweeps at once
@@ -1328,6 +1389,173 @@ int adjoint_backward_fused(double2* psi, double2* lam, uint32_t n, const dq_inst
     stats->sweeps = sweeps;
     stats->pergate = pergate;
   }
+  return rc;
+}
+
+// ---- many parameter sets at once -------------------------------------------------------
+
+int adjoint_backward_plan_set(uint32_t n, const dq_inst* prog, uint64_t ninst, const int32_t* pidx,
+                              uint64_t nslots, ABatchSet* out) {
+  std::vector<BackSeg> segs;
+  DQ_TRY(plan_backward_segments(n, prog, ninst, pidx, nslots, segs));
+  ABatchSet s;
+  for (const BackSeg& g : segs) {
+    if (!g.sweep)
+      return fail(DQ_ERR_UNSUPPORTED, "a gate of three or more qubits: no batched backward sweep");
+    ASweepHdr hdr;
+    std::vector<AOp> o;
+    const size_t op0 = s.ops.size() / sizeof(AOp), sl0 = s.map.size();
+    DQ_TRY(encode_asweep(g.plan, n, hdr, o, s.pool, s.map));
+    s.ops.insert(s.ops.end(), reinterpret_cast<const uint8_t*>(o.data()),
+                 reinterpret_cast<const uint8_t*>(o.data() + o.size()));
+    s.op0.push_back(op0);
+    s.slot0.push_back(sl0);
+    s.nslots.push_back(hdr.nslots);
+    s.hdrs.insert(s.hdrs.end(), reinterpret_cast<const uint8_t*>(&hdr),
+                  reinterpret_cast<const uint8_t*>(&hdr + 1));
+  }
+  if (s.pool.empty()) s.pool.push_back(make_double2(0, 0));
+  *out = std::move(s);
+  return DQ_OK;
+}
+
+int adjoint_backward_batch(double2* const* psi, double2* const* lam, const std::vector<ABatchSet>& sets,
+                           double* const* d_slots, cudaStream_t st, int device, uint64_t* launches) {
+  const size_t B = sets.size();
+  if (!B) return DQ_OK;
+  // every set's headers, ops, pools and slot maps in four device arrays
+  std::vector<ASweepHdr> hdrs;
+  std::vector<AOp> ops;
+  std::vector<double2> pool;
+  std::vector<uint32_t> map;
+  std::vector<size_t> bh(B), bo(B), bp(B), bm(B);
+  size_t kmax = 0;
+  for (size_t b = 0; b < B; ++b) {
+    const ABatchSet& s = sets[b];
+    bh[b] = hdrs.size();
+    bo[b] = ops.size();
+    bp[b] = pool.size();
+    bm[b] = map.size();
+    for (size_t k = 0; k < s.sweeps(); ++k) {
+      ASweepHdr x;
+      memcpy(&x, s.hdrs.data() + k * sizeof(ASweepHdr), sizeof(x));
+      hdrs.push_back(x);
+    }
+    const size_t nops = s.ops.size() / sizeof(AOp);
+    ops.resize(bo[b] + nops);
+    if (nops) memcpy(ops.data() + bo[b], s.ops.data(), nops * sizeof(AOp));
+    pool.insert(pool.end(), s.pool.begin(), s.pool.end());
+    map.insert(map.end(), s.map.begin(), s.map.end());
+    kmax = std::max(kmax, s.sweeps());
+  }
+  if (hdrs.empty()) return DQ_OK;
+  if (ops.empty()) ops.push_back(AOp{});
+  if (map.empty()) map.push_back(0);
+  const int ctas = sweep_ctas(device);
+  if (ctas <= 0) return DQ_ERR_CUDA;
+  const uint64_t ntiles = hdrs[0].ntiles;
+  const uint64_t chunk_tiles = std::max<uint64_t>(1, std::min<uint64_t>(64, ntiles));
+  const uint32_t nchunks = (uint32_t)((ntiles + chunk_tiles - 1) / chunk_tiles);
+  // jobs of every sweep index (device pointers filled in once the arrays exist)
+  std::vector<AJob> jobs;
+  std::vector<size_t> job_hdr, job_ops, job_pool, job_map;
+  std::vector<size_t> job0(kmax + 1, 0);
+  std::vector<size_t> smem(kmax, 0);
+  std::vector<uint32_t> maxsl(kmax, 0);
+  size_t part_per_job = 1;
+  for (const ASweepHdr& h : hdrs) part_per_job = std::max<size_t>(part_per_job, (size_t)h.nslots * nchunks);
+  for (size_t k = 0; k < kmax; ++k) {
+    job0[k] = jobs.size();
+    for (size_t b = 0; b < B; ++b) {
+      const ABatchSet& s = sets[b];
+      if (k >= s.sweeps()) continue;
+      const ASweepHdr& h = hdrs[bh[b] + k];
+      if (h.ntiles != ntiles) return fail(DQ_ERR_INTERNAL, "batched sweeps of unequal tile counts");
+      AJob j{};
+      j.psi = psi[b];
+      j.lam = lam[b];
+      j.out = d_slots[b];
+      j.nslots = s.nslots[k];
+      jobs.push_back(j);
+      job_hdr.push_back(bh[b] + k);
+      job_ops.push_back(bo[b] + s.op0[k]);
+      job_pool.push_back(bp[b]);
+      job_map.push_back(bm[b] + s.slot0[k]);
+      smem[k] = std::max(smem[k], asweep_smem(h.m, h.nslots, h.nops, h.phase_ops));
+      maxsl[k] = std::max(maxsl[k], h.nslots);
+    }
+  }
+  job0[kmax] = jobs.size();
+  size_t max_jobs = 1;
+  for (size_t k = 0; k < kmax; ++k) max_jobs = std::max(max_jobs, job0[k + 1] - job0[k]);
+  ASweepHdr* d_hdr = nullptr;
+  AOp* d_ops = nullptr;
+  double2* d_pool = nullptr;
+  uint32_t* d_map = nullptr;
+  double* d_part = nullptr;
+  AJob* d_jobs = nullptr;
+  int rc = DQ_OK;
+  auto cu = [&](cudaError_t e, const char* what) {
+    if (e != cudaSuccess && rc == DQ_OK) {
+      cudaGetLastError();
+      rc = fail(e == cudaErrorMemoryAllocation ? DQ_ERR_OOM : DQ_ERR_CUDA,
+                std::string(what) + ": " + cudaGetErrorString(e));
+    }
+  };
+  cu(cudaMalloc((void**)&d_hdr, sizeof(ASweepHdr) * hdrs.size()), "cudaMalloc(hdr)");
+  cu(cudaMalloc((void**)&d_ops, sizeof(AOp) * ops.size()), "cudaMalloc(ops)");
+  cu(cudaMalloc((void**)&d_pool, sizeof(double2) * pool.size()), "cudaMalloc(pool)");
+  cu(cudaMalloc((void**)&d_map, sizeof(uint32_t) * map.size()), "cudaMalloc(map)");
+  cu(cudaMalloc((void**)&d_part, sizeof(double) * part_per_job * max_jobs), "cudaMalloc(partials)");
+  cu(cudaMalloc((void**)&d_jobs, sizeof(AJob) * std::max<size_t>(jobs.size(), 1)), "cudaMalloc(jobs)");
+  if (rc == DQ_OK) {
+    for (size_t k = 0; k < kmax; ++k)
+      for (size_t i = job0[k]; i < job0[k + 1]; ++i) {
+        AJob& j = jobs[i];
+        j.hdr = d_hdr + job_hdr[i];
+        j.ops = d_ops + job_ops[i];
+        j.pool = d_pool + job_pool[i];
+        j.map = d_map + job_map[i];
+        j.partial = d_part + (i - job0[k]) * part_per_job;
+      }
+    cu(cudaMemcpyAsync(d_hdr, hdrs.data(), sizeof(ASweepHdr) * hdrs.size(), cudaMemcpyHostToDevice, st), "copy");
+    cu(cudaMemcpyAsync(d_ops, ops.data(), sizeof(AOp) * ops.size(), cudaMemcpyHostToDevice, st), "copy");
+    cu(cudaMemcpyAsync(d_pool, pool.data(), sizeof(double2) * pool.size(), cudaMemcpyHostToDevice, st), "copy");
+    cu(cudaMemcpyAsync(d_map, map.data(), sizeof(uint32_t) * map.size(), cudaMemcpyHostToDevice, st), "copy");
+    cu(cudaMemcpyAsync(d_jobs, jobs.data(), sizeof(AJob) * jobs.size(), cudaMemcpyHostToDevice, st), "copy");
+  }
+  {
+    static std::mutex mu;
+    static uint64_t attr_done = 0;
+    std::lock_guard<std::mutex> lk(mu);
+    if (!((attr_done >> (device & 63)) & 1ULL)) {
+      const size_t smem_max = asweep_smem(kAMaxLocal, kAMaxSlots, kAMaxSweepOps, kAPhaseStage);
+      cu(cudaFuncSetAttribute(k_adj_sweep_multi, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)smem_max), "cudaFuncSetAttribute");
+      attr_done |= 1ULL << (device & 63);
+    }
+  }
+  for (size_t k = 0; k < kmax && rc == DQ_OK; ++k) {
+    const uint32_t nj = (uint32_t)(job0[k + 1] - job0[k]);
+    if (!nj) continue;
+    const uint64_t work = (uint64_t)nj * nchunks;
+    const unsigned grid = (unsigned)std::min<uint64_t>(work, (uint64_t)ctas);
+    k_adj_sweep_multi<<<grid, kAThreads, smem[k], st>>>(d_jobs + job0[k], nj, nchunks, chunk_tiles);
+    cu(cudaGetLastError(), "k_adj_sweep_multi");
+    if (launches) ++*launches;
+    if (maxsl[k] && rc == DQ_OK) {
+      k_adj_slots_multi<<<dim3((maxsl[k] + 127) / 128, nj), 128, 0, st>>>(d_jobs + job0[k], nchunks);
+      cu(cudaGetLastError(), "k_adj_slots_multi");
+      if (launches) ++*launches;
+    }
+  }
+  cudaStreamSynchronize(st);
+  if (d_hdr) cudaFree(d_hdr);
+  if (d_ops) cudaFree(d_ops);
+  if (d_pool) cudaFree(d_pool);
+  if (d_map) cudaFree(d_map);
+  if (d_part) cudaFree(d_part);
+  if (d_jobs) cudaFree(d_jobs);
   return rc;
 }
 

@@ -360,6 +360,36 @@ DQ_API int dq_adjoint(dq_state_t h, const dq_inst* prog, uint64_t ninst,
                       const dq_run_opts* opts, double* expval, double* grad,
                       double* phase_ms);
 
+/* Adjoint gradients of nsets parameter sets of one circuit at once (no
+ * counterpart in the reference, which has no gradients).  Set s runs `prog`
+ * from |0...0> on `nqubits` qubits with every parameter slot that
+ * param_index maps to p (param_index as in dq_adjoint) replaced by
+ * values[s * nparams + p]; its E_s goes to expvals[s] and
+ * dE_s/d(value p) to grads[s * nparams + p].  The sets share each launch:
+ * every fused forward sweep, lambda = H psi, and every fused backward sweep
+ * runs for all sets at once (one launch per sweep index; the sets' tiles are
+ * (set, chunk) work items), with the states of as many sets as fit in about
+ * half of the free device memory resident at a time.  Programs the batched
+ * sweeps cannot represent (gates of three or more qubits without a sweep
+ * form, fewer than 10 qubits) run set by set through dq_adjoint;
+ * stats->batched tells which path ran. */
+typedef struct dq_adjoint_batch_stats {
+  uint64_t launches;         /* kernel launches of the batched path */
+  uint64_t forward_sweeps;   /* sweep indices of the forward pass (largest set) */
+  uint64_t backward_sweeps;  /* sweep indices of the backward pass (largest set) */
+  double plan_ms;            /* host planning of all sets */
+  double forward_ms;         /* device time, all groups */
+  double observable_ms;
+  double backward_ms;
+  uint32_t batched;          /* 1: batched launches; 0: set by set */
+  uint32_t groups;           /* groups of sets resident at a time */
+} dq_adjoint_batch_stats;
+
+DQ_API int dq_adjoint_batch(int device, uint32_t nqubits, const dq_inst* prog, uint64_t ninst,
+                            const int32_t* param_index, uint64_t nparams, const double* values,
+                            uint64_t nsets, const dq_pauli_term* terms, uint64_t nterms,
+                            double* expvals, double* grads, dq_adjoint_batch_stats* stats);
+
 /* ---- p-block merge -----------------------------------------------------------
  * merge_blocks (src/distributed/pblock/model.rs:35-57): the tensor product of
  * block a (state of the ascending qubits a_qubits[0..na)) and block b into

@@ -195,6 +195,57 @@ def test_batched_adjoint_matches_single_sets_and_drives_adam(gpu):
     assert energies[-1].sum() < energies[0].sum()
 
 
+@pytest.mark.parametrize("n,layers,B", [(11, 2, 6), (14, 3, 9), (20, 1, 3)])
+def test_batched_launches_match_single_sets(gpu, n, layers, B):
+    """dq_adjoint_batch: every sweep index of every set in one launch; energies
+    and gradients equal the single-set adjoint pass within 1e-11."""
+    from dqsim_bosonic_b200.adjoint import adjoint_gradient_batch
+
+    c, _, H = _circuits.hea_param_circuit(n, layers, seed=3)
+    thetas = np.random.default_rng(n).uniform(-np.pi, np.pi, size=(B, c.num_params))
+    st = {}
+    es, gs = adjoint_gradient_batch(c, thetas, H, stats=st)
+    assert st["batched"] == 1 and st["groups"] == 1
+    # one launch per forward sweep, one for lambda = H psi, two per backward
+    # sweep (the sweep and its gradient reduction), independent of B
+    assert st["launches"] == st["forward_sweeps"] + 1 + 2 * st["backward_sweeps"]
+    for b in range(B):
+        e1, g1 = adjoint_gradient(c, thetas[b], H)
+        assert abs(es[b] - e1) < 1e-11
+        assert np.max(np.abs(gs[b] - g1)) < 1e-11
+
+
+def test_batched_shared_scaled_params_and_fallback(gpu):
+    from dqsim_bosonic_b200.adjoint import adjoint_gradient_batch
+
+    # shared and scaled parameters, a controlled rotation and a dense two-qubit gate
+    n = 12
+    c = ParamCircuit(n)
+    for q in range(n):
+        c.add("ry", [q], [Param(q % 5, scale=0.5, shift=0.1)])
+    c.add("crx", [0, 7], [Param(5)])
+    c.add("rxx", [3, 11], [Param(6, scale=-2.0)])
+    c.add("u3", [9], [Param(7), Param(8), 0.3])
+    c.add("rzz", [2, 10], [Param(0)])
+    H = random_observable(n, 6, 4)
+    thetas = np.random.default_rng(1).uniform(-np.pi, np.pi, size=(4, c.num_params))
+    st = {}
+    es, gs = adjoint_gradient_batch(c, thetas, H, stats=st)
+    assert st["batched"] == 1
+    for b in range(4):
+        e1, g1 = adjoint_gradient(c, thetas[b], H)
+        assert abs(es[b] - e1) < 1e-11 and np.max(np.abs(gs[b] - g1)) < 1e-11
+    # fewer than 10 qubits: the set-by-set path, same results
+    c2, _, H2 = _circuits.hea_param_circuit(6, 2, seed=2)
+    th2 = np.random.default_rng(2).uniform(-np.pi, np.pi, size=(3, c2.num_params))
+    st2 = {}
+    es2, gs2 = adjoint_gradient_batch(c2, th2, H2, stats=st2)
+    assert st2["batched"] == 0
+    for b in range(3):
+        e1, g1 = adjoint_gradient(c2, th2[b], H2)
+        assert abs(es2[b] - e1) < 1e-12 and np.max(np.abs(gs2[b] - g1)) < 1e-12
+
+
 def mixed_param_circuit(n, depth, seed):
     """Random gates of every kind the ParamCircuit takes (three- to
     five-qubit gates included), every angle of the parametrised ones
