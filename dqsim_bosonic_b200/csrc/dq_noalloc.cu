@@ -1,9 +1,9 @@
 // dq_noalloc.cu — the measurement probability p1 without any allocation.
 //
-// Some callers of this library cannot allocate device memory: code running
-// inside a CUDA graph capture (where cudaMalloc is not permitted), hosts that
-// own a fixed device-memory budget and hand the library pre-allocated buffers
-// only, and embedders whose allocator must not be bypassed.  For them
+// Some callers of this library cannot allocate device memory: hosts that own
+// a fixed device-memory budget and hand the library pre-allocated buffers
+// only, embedders whose allocator must not be bypassed, and code running in a
+// context where cudaMalloc is not permitted.  For them
 // dq_measure_p1_noalloc computes p1 = sum of |psi_i|^2 over the amplitudes
 // with a given qubit set, for a state vector the caller owns, writing the
 // result to a device location the caller owns.  Its only scratch (the
@@ -21,13 +21,19 @@
 namespace dq {
 namespace {
 
-// Room for kNoAllocPartials partial sums followed by the counter word.
+// Room for kNoAllocPartials partial sums followed by the counter word.  The
+// p1 reduction launches at most kPartials / 4 blocks (one partial sum each),
+// so every n the entry point accepts fits.
 constexpr int kNoAllocPartials = 1024;
 constexpr size_t kNoAllocScratchBytes = sizeof(double) * kNoAllocPartials + 256;
+static_assert(kPartials / 4 <= kNoAllocPartials, "the p1 grid can outgrow the static scratch");
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
-// Device address of g_noalloc_scratch, resolved once per device.
+// Device address of g_noalloc_scratch, resolved once per device ordinal and
+// kept for the life of the process: a device reset (cudaDeviceReset) or a
+// re-created primary context can load the module at another address, after
+// which the cached address is stale; do not reset a device this library uses.
 std::mutex g_mu;
 void* g_addr[64] = {};
 

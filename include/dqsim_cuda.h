@@ -195,20 +195,23 @@ DQ_API int dq_collapse(dq_state_t h, uint32_t qubit, int outcome, double p1);
 DQ_API int dq_measure(dq_state_t h, uint32_t qubit, double r, int* outcome, double* p1);
 
 /* dq_measure_p1_noalloc: the p1 reduction of dq_measure_p1 for callers that
- * cannot allocate device memory (code inside a CUDA graph capture, hosts
- * that own a fixed device-memory budget, embedders whose allocator must not
- * be bypassed).  No counterpart in the reference: the Rust engine's
- * measure_qubit sums on the CPU and has no device memory to manage.
+ * cannot allocate device memory (hosts that own a fixed device-memory
+ * budget, embedders whose allocator must not be bypassed, code running where
+ * cudaMalloc is not permitted).  No counterpart in the reference: the Rust
+ * engine's measure_qubit sums on the CPU and has no device memory to manage.
  * amps_device: a caller-owned device array of 2^n interleaved complex128
  * amplitudes on the current device; p1_device: caller-owned device double
  * that receives p1.  The call only enqueues work on `stream` (a
  * cudaStream_t, NULL = default stream) and returns; it allocates nothing.
  * Its scratch is a static device array of 1024 partial sums (8 KiB + a
- * counter) that every GPU loading the library keeps until exit; n is
- * limited to 1..34 and requests needing more partial sums are rejected.
- * The first call on a device resolves the array's address on that device,
- * so make it before any stream capture.  All calls share the one array:
- * calls that overlap on the GPU (other streams, other threads) race. */
+ * counter) that every GPU loading the library keeps until exit; the p1
+ * reduction never needs more than 1024 of them.  n is limited to 1..34, the
+ * engine's largest state (2^34 amplitudes = 256 GiB), and requests needing
+ * more partial sums than the array holds are rejected.  The first call on a
+ * device resolves the array's address on that device and keeps it for the
+ * process (a device reset makes it stale), so make that first call before
+ * any stream capture.  All calls share the one array: calls that overlap on
+ * the GPU (other streams, other threads) race. */
 DQ_API int dq_measure_p1_noalloc(const double* amps_device, uint32_t n, uint32_t qubit,
                                  double* p1_device, void* stream);
 

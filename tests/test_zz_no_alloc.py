@@ -1,8 +1,8 @@
 """The allocation-free p1 entry point (needs a B200).
 
 dq_measure_p1_noalloc serves callers that cannot allocate device memory:
-code running inside a CUDA graph capture, hosts with a fixed device-memory
-budget, embedders whose allocator must not be bypassed.  The test acts as
+hosts with a fixed device-memory budget, embedders whose allocator must not
+be bypassed, code running where cudaMalloc is not permitted.  The test acts as
 such a caller: it owns the state and the output buffer, calls the entry
 point through the C ABI twice in a row (the shared static scratch keeps the
 previous call's contents), and compares both results with dq_measure_p1.
