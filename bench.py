@@ -437,17 +437,22 @@ def main():
                                exec="per_gate" if exec_mode == nat.EXEC_PER_GATE else "fused")
     n = prog.num_qubits
     top = list(range(n - 1, max(-1, n - 11), -1))
-    # untimed warm-up of the host path (a freshly started box is noisy for a while)
+    # the interpreter's cyclic garbage collector stays off inside the timed
+    # host steps (as timeit does); it runs between them.  The untimed warm-up
+    # steps run exactly like the timed ones (a freshly started box is noisy
+    # for a while, and the first step after a collection was slow).
+    gc.collect()
     for _ in range(max(5, args.warmup)):
+        torch.cuda.synchronize(dev)
+        gc.disable()
         res = sim.simulate(circ)
         res.probabilities(top)
+        torch.cuda.synchronize(dev)
+        gc.enable()
         del res
-    torch.cuda.synchronize(dev)
+        gc.collect()
     d.barrier()
     e2e_t, phases = [], []
-    # the interpreter's cyclic garbage collector stays off inside the timed
-    # host steps (as timeit does); it runs between them
-    gc.collect()
     for _ in range(args.steps):
         torch.cuda.synchronize(dev)
         gc.disable()

@@ -809,20 +809,23 @@ int dq_adjoint_batch(int device, uint32_t n, const dq_inst* prog, uint64_t ninst
     const uint64_t g1 = std::min(nsets, g0 + G), ng = g1 - g0;
     ++acc.groups;
     // forward: sweep k of every set of the group in one launch per run width
-    struct Range { size_t begin, end; uint32_t run_bits; };
+    struct Range { size_t begin, end; uint32_t run_bits, max_bytes; };
     std::vector<SweepJob> jobs;
     std::vector<Range> ranges;
     for (size_t k = 0; k < kf; ++k)
       for (uint32_t rbits : {5u, 3u}) {
         const size_t b0 = jobs.size();
+        uint32_t mb = 0;
         for (uint64_t s = g0; s < g1; ++s) {
           if (k >= plans[s].foffs.size()) continue;
           const uint8_t* hp = plans[s].fblob.data() + plans[s].foffs[k];
           if (sweep_run_bits(hp) != rbits) continue;
+          const uint32_t pb = sweep_prog_bytes(hp);
+          mb = std::max(mb, pb);
           jobs.push_back(SweepJob{psi + (s - g0) * len, fblob + fbase[s] + plans[s].foffs[k],
-                                  k == 0 ? (long long)plans[s].synth : -1LL});
+                                  k == 0 ? (long long)plans[s].synth : -1LL, pb, 0});
         }
-        if (jobs.size() > b0) ranges.push_back(Range{b0, jobs.size(), rbits});
+        if (jobs.size() > b0) ranges.push_back(Range{b0, jobs.size(), rbits, mb});
       }
     if (!jobs.empty())
       cu(cudaMemcpyAsync(d_jobs, jobs.data(), sizeof(SweepJob) * jobs.size(), cudaMemcpyHostToDevice, st),
@@ -830,7 +833,8 @@ int dq_adjoint_batch(int device, uint32_t n, const dq_inst* prog, uint64_t ninst
     cu(cudaEventRecord(ev[0], st), "event");
     for (const Range& r : ranges) {
       if (rc != DQ_OK) break;
-      rc = launch_sweep_multi(d_jobs + r.begin, (uint32_t)(r.end - r.begin), n, rb, r.run_bits, st);
+      rc = launch_sweep_multi(d_jobs + r.begin, (uint32_t)(r.end - r.begin), n, rb, r.run_bits,
+                              r.max_bytes, st);
       ++acc.launches;
     }
     for (uint64_t s = g0; s < g1 && rc == DQ_OK; ++s) {

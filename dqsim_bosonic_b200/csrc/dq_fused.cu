@@ -41,33 +41,27 @@ namespace {
 // One persistent CTA per SM walks tiles blockIdx.x, + gridDim.x, ...
 // S = 1 (128 threads): no prefetch, three CTAs per SM overlap each other's
 // loads.  S = 2: the next tile's load is in flight while the current one is
-// computed.  PG: the sweep program is read where it lies in global memory (a
-// few KB, L1-resident after the first tile) instead of being staged in
-// shared memory, which leaves room for two tile buffers at three CTAs per SM.
-template <int TB, int RB, int S, bool PG, int RUNB>
-__global__ void __launch_bounds__(1 << TB, ((S == 1 || PG) && TB == 7 ? 3 : (TB + RB <= 11 ? 2 : 1)))
+// computed.  The sweep program is staged in shared memory once per launch
+// (read from global memory per op instead, QFT30 ran 38% slower).
+template <int TB, int RB, int S, int RUNB>
+__global__ void __launch_bounds__(1 << TB, (S == 1 && TB == 7 ? 3 : (TB + RB <= 11 ? 2 : 1)))
     k_sweep(double2* __restrict__ state, const uint8_t* __restrict__ gprog, uint32_t prog_bytes,
             uint32_t ntiles, long long synth) {
   constexpr int T = 1 << (TB + RB);
   extern __shared__ __align__(16) unsigned char smraw[];
   double2* bufs = reinterpret_cast<double2*>(smraw);  // S tiles
   double2* slots = bufs + S * T;
-  const uint8_t* prog;
-  if (PG) {
-    prog = gprog;
-  } else {
-    uint8_t* sprog = reinterpret_cast<uint8_t*>(slots + kMaxSlots);
-    for (uint32_t i = threadIdx.x * 16u; i < prog_bytes; i += (1u << TB) * 16u)
-      *reinterpret_cast<uint4*>(sprog + i) = __ldg(reinterpret_cast<const uint4*>(gprog + i));
-    __syncthreads();
-    prog = sprog;
-  }
-  sweep_tiles<TB, RB, S, RUNB>(state, prog, ntiles, synth, bufs, slots, blockIdx.x, gridDim.x);
+  uint8_t* sprog = reinterpret_cast<uint8_t*>(slots + kMaxSlots);
+  for (uint32_t i = threadIdx.x * 16u; i < prog_bytes; i += (1u << TB) * 16u)
+    *reinterpret_cast<uint4*>(sprog + i) = __ldg(reinterpret_cast<const uint4*>(gprog + i));
+  __syncthreads();
+  sweep_tiles<TB, RB, S, RUNB>(state, sprog, ntiles, synth, bufs, slots, blockIdx.x, gridDim.x);
 }
 
 // Sweep k of many states in one launch: job j's tiles are split into chunks
 // of chunk_tiles consecutive tiles and the CTAs take (job, chunk) work items
-// in order; double-buffered tiles, programs read from global memory.
+// in order; a CTA stages a job's program in shared memory when it moves to
+// that job (a few KB per chunk of 2 MB of tiles).
 template <int TB, int RB, int RUNB>
 __global__ void __launch_bounds__(1 << TB, TB == 7 ? 3 : 2)
     k_sweep_multi(const SweepJob* __restrict__ jobs, uint32_t njobs, uint32_t nchunks,
@@ -75,14 +69,23 @@ __global__ void __launch_bounds__(1 << TB, TB == 7 ? 3 : 2)
   constexpr int T = 1 << (TB + RB);
   extern __shared__ __align__(16) unsigned char smraw[];
   double2* bufs = reinterpret_cast<double2*>(smraw);
-  double2* slots = bufs + 2 * T;
+  double2* slots = bufs + T;
+  uint8_t* sprog = reinterpret_cast<uint8_t*>(slots + kMaxSlots);
   const uint64_t work = (uint64_t)njobs * nchunks;
+  uint64_t staged = ~0ULL;
   for (uint64_t w = blockIdx.x; w < work; w += gridDim.x) {
-    const SweepJob J = jobs[w / nchunks];
+    const uint64_t j = w / nchunks;
+    const SweepJob J = jobs[j];
+    if (j != staged) {
+      for (uint32_t i = threadIdx.x * 16u; i < J.prog_bytes; i += (1u << TB) * 16u)
+        *reinterpret_cast<uint4*>(sprog + i) = __ldg(reinterpret_cast<const uint4*>(J.prog + i));
+      __syncthreads();
+      staged = j;
+    }
     const uint32_t c = (uint32_t)(w % nchunks);
     const uint32_t t0 = c * chunk_tiles;
     const uint32_t t1 = min(t0 + chunk_tiles, ntiles);
-    sweep_tiles<TB, RB, 2, RUNB>(J.state, J.prog, t1, J.synth, bufs, slots, t0, 1);
+    sweep_tiles<TB, RB, 1, RUNB>(J.state, sprog, t1, J.synth, bufs, slots, t0, 1);
     __syncthreads();
   }
 }
@@ -265,6 +268,7 @@ struct Planner {
   bool single_tile = false;
   // qubits every tile holds (0..4: 512-byte runs; 0..2: 128-byte runs)
   uint64_t pinned = 0x1FULL;
+  bool pin_auto = false;
 
   // cost in FP64 instructions per amplitude
   double gate_cost(const PGate& g) const {
@@ -937,12 +941,12 @@ bool convert_inst(const dq_inst& in, const uint32_t* perm, std::vector<PGate>& o
   }
 }
 
-template <int TB, int RB, int S, bool PG, int RUNB>
+template <int TB, int RB, int S, int RUNB>
 int launch_sweep_r(double2* amp, uint32_t n, const uint8_t* dblob, uint32_t prog_bytes,
                    cudaStream_t st, long long synth) {
   constexpr int M = TB + RB;
-  const size_t smem_max = sizeof(double2) * (S * (1u << M) + kMaxSlots) + (PG ? 0 : max_prog(M));
-  const size_t smem = sizeof(double2) * (S * (1u << M) + kMaxSlots) + (PG ? 0 : prog_bytes);
+  const size_t smem_max = sizeof(double2) * (S * (1u << M) + kMaxSlots) + max_prog(M);
+  const size_t smem = sizeof(double2) * (S * (1u << M) + kMaxSlots) + prog_bytes;
   // per device, once: opt-in shared memory and resident CTAs per SM (the
   // mutex makes the first launches from concurrent host threads safe)
   static std::mutex mu;
@@ -953,10 +957,10 @@ int launch_sweep_r(double2* amp, uint32_t n, const uint8_t* dblob, uint32_t prog
   {
     std::lock_guard<std::mutex> lk(mu);
     if (per_sm[dev & 63] == 0) {
-      DQ_CUDA_TRY(cudaFuncSetAttribute(k_sweep<TB, RB, S, PG, RUNB>,
+      DQ_CUDA_TRY(cudaFuncSetAttribute(k_sweep<TB, RB, S, RUNB>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_max));
       int b = 1;
-      DQ_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_sweep<TB, RB, S, PG, RUNB>, 1 << TB,
+      DQ_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_sweep<TB, RB, S, RUNB>, 1 << TB,
                                                                 smem_max));
       per_sm[dev & 63] = b < 1 ? 1 : b;
     }
@@ -966,7 +970,7 @@ int launch_sweep_r(double2* amp, uint32_t n, const uint8_t* dblob, uint32_t prog
   DQ_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
   const uint64_t tiles = 1ULL << (n - M);
   const unsigned grid = (unsigned)std::min<uint64_t>(tiles, (uint64_t)sms * resident);
-  k_sweep<TB, RB, S, PG, RUNB><<<grid, 1 << TB, smem, st>>>(amp, dblob, prog_bytes, (uint32_t)tiles, synth);
+  k_sweep<TB, RB, S, RUNB><<<grid, 1 << TB, smem, st>>>(amp, dblob, prog_bytes, (uint32_t)tiles, synth);
   DQ_CUDA_TRY(cudaGetLastError());
   return DQ_OK;
 }
@@ -978,20 +982,16 @@ int launch_sweep_rb(double2* amp, uint32_t n, const uint8_t* dblob, uint32_t pro
   // faster than two double-buffered CTAs: the extra warps hide more of the
   // per-op latency than the prefetch saves); DQSIM_SWEEP_STAGES=2 selects
   // double buffering
-  // DQSIM_SWEEP_STAGES=3: double-buffered tiles with the program read from
-  // global memory (three CTAs per SM)
   static const int stages = [] {
     const char* e = getenv("DQSIM_SWEEP_STAGES");
     return e ? atoi(e) : 1;
   }();
   if (run_bits == 3) {
-    if (TB == 7 && stages == 3) return launch_sweep_r<7, RB, 2, true, 3>(amp, n, dblob, prog_bytes, st, synth);
-    if (TB == 7 && stages != 2) return launch_sweep_r<7, RB, 1, false, 3>(amp, n, dblob, prog_bytes, st, synth);
-    return launch_sweep_r<TB, RB, 2, false, 3>(amp, n, dblob, prog_bytes, st, synth);
+    if (TB == 7 && stages != 2) return launch_sweep_r<7, RB, 1, 3>(amp, n, dblob, prog_bytes, st, synth);
+    return launch_sweep_r<TB, RB, 2, 3>(amp, n, dblob, prog_bytes, st, synth);
   }
-  if (TB == 7 && stages == 3) return launch_sweep_r<7, RB, 2, true, 5>(amp, n, dblob, prog_bytes, st, synth);
-  if (TB == 7 && stages != 2) return launch_sweep_r<7, RB, 1, false, 5>(amp, n, dblob, prog_bytes, st, synth);
-  return launch_sweep_r<TB, RB, 2, false, 5>(amp, n, dblob, prog_bytes, st, synth);
+  if (TB == 7 && stages != 2) return launch_sweep_r<7, RB, 1, 5>(amp, n, dblob, prog_bytes, st, synth);
+  return launch_sweep_r<TB, RB, 2, 5>(amp, n, dblob, prog_bytes, st, synth);
 }
 
 int launch_sweep(double2* amp, uint32_t n, uint32_t TB, uint32_t RB, const uint8_t* dblob,
@@ -1015,9 +1015,11 @@ int launch_sweep(double2* amp, uint32_t n, uint32_t TB, uint32_t RB, const uint8
 }
 
 template <int TB, int RB, int RUNB>
-int launch_sweep_multi_t(const SweepJob* d_jobs, uint32_t njobs, uint32_t n, cudaStream_t st) {
+int launch_sweep_multi_t(const SweepJob* d_jobs, uint32_t njobs, uint32_t n, uint32_t max_bytes,
+                         cudaStream_t st) {
   constexpr int M = TB + RB;
-  const size_t smem = sizeof(double2) * (2 * (1u << M) + kMaxSlots);
+  const size_t smem_max = sizeof(double2) * ((1u << M) + kMaxSlots) + max_prog(M);
+  const size_t smem = sizeof(double2) * ((1u << M) + kMaxSlots) + max_bytes;
   static std::mutex mu;
   static int per_sm[64];
   int dev = 0;
@@ -1027,10 +1029,10 @@ int launch_sweep_multi_t(const SweepJob* d_jobs, uint32_t njobs, uint32_t n, cud
     std::lock_guard<std::mutex> lk(mu);
     if (per_sm[dev & 63] == 0) {
       DQ_CUDA_TRY(cudaFuncSetAttribute(k_sweep_multi<TB, RB, RUNB>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_max));
       int b = 1;
       DQ_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_sweep_multi<TB, RB, RUNB>,
-                                                                1 << TB, smem));
+                                                                1 << TB, smem_max));
       per_sm[dev & 63] = b < 1 ? 1 : b;
     }
     resident = per_sm[dev & 63];
@@ -1159,8 +1161,26 @@ int fused_run_segment(double2* amp, uint32_t n, std::vector<PGate>& G, Planner& 
                       FusedWork& fw, cudaStream_t st, bool timing, dq_profile* prof,
                       int64_t* lazy_basis) {
   std::vector<PSweep> sweeps;
-  pl.plan(G, poly, sweeps);
-  pl.final_flush(poly, sweeps);
+  if (pl.pin_auto && !pl.single_tile) {
+    // plan with qubits 0..4 pinned and with 0..2 pinned; the wider tile
+    // choice wins only when it saves at least a tenth of the sweeps (its
+    // 128-byte runs cost a little more per sweep)
+    Poly poly3 = poly;
+    std::vector<PSweep> sweeps3;
+    pl.pinned = 0x1FULL;
+    pl.plan(G, poly, sweeps);
+    pl.final_flush(poly, sweeps);
+    pl.pinned = 0x7ULL;
+    pl.plan(G, poly3, sweeps3);
+    pl.final_flush(poly3, sweeps3);
+    if (10 * sweeps3.size() <= 9 * sweeps.size()) {
+      sweeps.swap(sweeps3);
+      poly = poly3;
+    }
+  } else {
+    pl.plan(G, poly, sweeps);
+    pl.final_flush(poly, sweeps);
+  }
   if (sweeps.empty()) return DQ_OK;
   Blob blob;
   std::vector<size_t> offs(sweeps.size());
@@ -1227,12 +1247,16 @@ int fused_run(double2* amp, uint32_t n, const dq_inst* prog, uint64_t ninst, con
   pl.TB = TB;
   pl.RB = M - TB;
   pl.single_tile = (M == n);
-  // DQSIM_SWEEP_PIN=3: tiles pin qubits 0..2 only (128-byte runs)
-  static const uint64_t pin_env = []() {
+  // Pinned tile qubits: 0..4 (512-byte runs) or 0..2 (128-byte runs, two
+  // more tile qubits free); by default each segment of 20+ qubits is planned
+  // both ways and keeps the one with clearly fewer sweeps.
+  // DQSIM_SWEEP_PIN=5 / 3 forces one.
+  static const int pin_env = []() {
     const char* e = getenv("DQSIM_SWEEP_PIN");
-    return (e && atoi(e) == 3) ? 0x7ULL : 0x1FULL;
+    return e ? atoi(e) : 0;
   }();
-  pl.pinned = pin_env;
+  pl.pinned = pin_env == 3 ? 0x7ULL : 0x1FULL;
+  pl.pin_auto = pin_env == 0 && n >= 20;
   if (o.max_cost > 0) pl.budget = (double)o.max_cost;
   Poly poly;
   poly.init(n);
@@ -1392,18 +1416,23 @@ uint32_t sweep_run_bits(const uint8_t* prog) {
   return reinterpret_cast<const SwHeader*>(prog)->run_bits;
 }
 
+uint32_t sweep_prog_bytes(const uint8_t* prog) {
+  return reinterpret_cast<const SwHeader*>(prog)->prog_bytes;
+}
+
 int launch_sweep_multi(const SweepJob* d_jobs, uint32_t njobs, uint32_t n, uint32_t rb,
-                       uint32_t run_bits, cudaStream_t st) {
+                       uint32_t run_bits, uint32_t max_bytes, cudaStream_t st) {
   if (!njobs) return DQ_OK;
   if (n < 7 + rb) return fail(DQ_ERR_INVALID_ARG, "state smaller than a tile");
+  if (max_bytes > (uint32_t)max_prog(7 + (int)rb)) return fail(DQ_ERR_INTERNAL, "sweep program too large");
   const bool r3 = run_bits == 3;
   switch (rb) {
-    case 2: return r3 ? launch_sweep_multi_t<7, 2, 3>(d_jobs, njobs, n, st)
-                      : launch_sweep_multi_t<7, 2, 5>(d_jobs, njobs, n, st);
-    case 3: return r3 ? launch_sweep_multi_t<7, 3, 3>(d_jobs, njobs, n, st)
-                      : launch_sweep_multi_t<7, 3, 5>(d_jobs, njobs, n, st);
-    case 4: return r3 ? launch_sweep_multi_t<7, 4, 3>(d_jobs, njobs, n, st)
-                      : launch_sweep_multi_t<7, 4, 5>(d_jobs, njobs, n, st);
+    case 2: return r3 ? launch_sweep_multi_t<7, 2, 3>(d_jobs, njobs, n, max_bytes, st)
+                      : launch_sweep_multi_t<7, 2, 5>(d_jobs, njobs, n, max_bytes, st);
+    case 3: return r3 ? launch_sweep_multi_t<7, 3, 3>(d_jobs, njobs, n, max_bytes, st)
+                      : launch_sweep_multi_t<7, 3, 5>(d_jobs, njobs, n, max_bytes, st);
+    case 4: return r3 ? launch_sweep_multi_t<7, 4, 3>(d_jobs, njobs, n, max_bytes, st)
+                      : launch_sweep_multi_t<7, 4, 5>(d_jobs, njobs, n, max_bytes, st);
     default: return fail(DQ_ERR_INTERNAL, "unsupported multi-sweep geometry");
   }
 }

@@ -84,15 +84,17 @@ struct SweepJob {
   double2* state;
   const uint8_t* prog;  // device pointer to an encoded sweep program
   long long synth;      // >= 0: generate the input from this basis index
+  uint32_t prog_bytes, pad;
 };
 
 // Runs one sweep of each of njobs states (all of n qubits, programs planned
-// with 7 thread bits, register width rb and the same run width run_bits) in
-// ONE launch; d_jobs is device memory.
+// with 7 thread bits, register width rb and the same run width run_bits, none
+// longer than max_bytes) in ONE launch; d_jobs is device memory.
 int launch_sweep_multi(const SweepJob* d_jobs, uint32_t njobs, uint32_t n, uint32_t rb,
-                       uint32_t run_bits, cudaStream_t st);
+                       uint32_t run_bits, uint32_t max_bytes, cudaStream_t st);
 
-// The run width (5 or 3) of an encoded sweep program in host memory.
+// The run width (5 or 3) and the size of an encoded sweep program in host memory.
 uint32_t sweep_run_bits(const uint8_t* prog);
+uint32_t sweep_prog_bytes(const uint8_t* prog);
 
 }  // namespace dq

@@ -84,6 +84,7 @@ struct TProg {         // one program of a launch
 struct TSweep {          // one fused sweep of an HBM item
   uint64_t off;          // byte offset of its program in the launch's sweep blob
   uint32_t ntiles, run_bits;
+  uint32_t prog_bytes, pad;
 };
 struct TItem {          // one trajectory: a shot of a program
   uint32_t prog, pad;
@@ -195,9 +196,11 @@ __global__ void __launch_bounds__(THREADS) k_traj(const TrajParams P) {
       // rank, rank + C, ...; 256 threads run the 8-thread-bit geometry the
       // sweeps were planned for) with a cluster barrier between sweeps; the
       // fence makes each sweep's stores visible to the CTAs of the next one.
+      // Each sweep's program is staged in shared memory behind the tile.
       if constexpr (THREADS == 256) {
         double2* bufs = reinterpret_cast<double2*>(smraw);
         double2* slots = bufs + (1u << 11);
+        uint8_t* sprog = reinterpret_cast<uint8_t*>(slots + kMaxSlots);
         if (pg.nsweeps == 0) {  // nothing but a basis state to write
           const uint64_t len = 1ULL << pg.n;
           for (uint64_t i = (uint64_t)rank * THREADS + tid; i < len; i += (uint64_t)C * THREADS)
@@ -206,10 +209,14 @@ __global__ void __launch_bounds__(THREADS) k_traj(const TrajParams P) {
         for (uint32_t s = 0; s < pg.nsweeps; ++s) {
           const TSweep sw = P.sweeps[pg.sweep_first + s];
           const long long sy = s == 0 ? pg.synth : -1LL;
+          for (uint32_t i = tid * 16u; i < sw.prog_bytes; i += THREADS * 16u)
+            *reinterpret_cast<uint4*>(sprog + i) =
+                __ldg(reinterpret_cast<const uint4*>(P.sweep_blob + sw.off + i));
+          __syncthreads();
           if (sw.run_bits == 3)
-            sweep_tiles<8, 3, 1, 3>(pg.hbm, P.sweep_blob + sw.off, sw.ntiles, sy, bufs, slots, rank, C);
+            sweep_tiles<8, 3, 1, 3>(pg.hbm, sprog, sw.ntiles, sy, bufs, slots, rank, C);
           else
-            sweep_tiles<8, 3, 1, 5>(pg.hbm, P.sweep_blob + sw.off, sw.ntiles, sy, bufs, slots, rank, C);
+            sweep_tiles<8, 3, 1, 5>(pg.hbm, sprog, sw.ntiles, sy, bufs, slots, rank, C);
           __threadfence();
           cl.sync();
         }
@@ -840,7 +847,7 @@ void add_hbm_program(LaunchSet& ls, const HbmPlan& pl, uint32_t n, uint64_t cbit
   ls.blob.insert(ls.blob.end(), pl.blob.begin(), pl.blob.end());
   TProg pg{};
   pg.n = n;
-  pg.lb = 12;  // the launch's shared memory holds the 2^11-amplitude tile and the slot factors
+  pg.lb = 13;  // the launch's shared memory holds the tile, the slot factors and the program
   pg.ncbits = ncbits;
   pg.cbits_off = cbits_off;
   pg.hbm = hbm;
@@ -848,7 +855,8 @@ void add_hbm_program(LaunchSet& ls, const HbmPlan& pl, uint32_t n, uint64_t cbit
   pg.nsweeps = (uint32_t)pl.offs.size();
   pg.synth = (long long)pl.synth;
   for (uint64_t off : pl.offs)
-    ls.sweeps.push_back(TSweep{base + off, 1u << (n - kHbmM), sweep_run_bits(pl.blob.data() + off)});
+    ls.sweeps.push_back(TSweep{base + off, 1u << (n - kHbmM), sweep_run_bits(pl.blob.data() + off),
+                               sweep_prog_bytes(pl.blob.data() + off), 0});
   ls.progs.push_back(pg);
   ls.max_lb = std::max(ls.max_lb, pg.lb);
   ls.max_ncbits = std::max(ls.max_ncbits, ncbits);
