@@ -43,8 +43,10 @@ namespace {
 // loads.  S = 2: the next tile's load is in flight while the current one is
 // computed.  The sweep program is staged in shared memory once per launch
 // (read from global memory per op instead, QFT30 ran 38% slower).
-template <int TB, int RB, int S, int RUNB>
-__global__ void __launch_bounds__(1 << TB, (S == 1 && TB == 7 ? 3 : (TB + RB <= 11 ? 2 : 1)))
+// MINB: CTAs per SM the register budget is cut for (3: 168 registers; 4: 128,
+// with a little spilling).
+template <int TB, int RB, int S, int RUNB, int MINB>
+__global__ void __launch_bounds__(1 << TB, (S == 1 && TB == 7 ? MINB : (TB + RB <= 11 ? 2 : 1)))
     k_sweep(double2* __restrict__ state, const uint8_t* __restrict__ gprog, uint32_t prog_bytes,
             uint32_t ntiles, long long synth) {
   constexpr int T = 1 << (TB + RB);
@@ -941,36 +943,44 @@ bool convert_inst(const dq_inst& in, const uint32_t* perm, std::vector<PGate>& o
   }
 }
 
-template <int TB, int RB, int S, int RUNB>
+template <int TB, int RB, int S, int RUNB, int MINB>
 int launch_sweep_r(double2* amp, uint32_t n, const uint8_t* dblob, uint32_t prog_bytes,
                    cudaStream_t st, long long synth) {
   constexpr int M = TB + RB;
   const size_t smem_max = sizeof(double2) * (S * (1u << M) + kMaxSlots) + max_prog(M);
   const size_t smem = sizeof(double2) * (S * (1u << M) + kMaxSlots) + prog_bytes;
-  // per device, once: opt-in shared memory and resident CTAs per SM (the
-  // mutex makes the first launches from concurrent host threads safe)
+  // per device, once: opt-in shared memory; resident CTAs per SM for this
+  // launch's shared memory (programs are mostly far below the maximum), cached
+  // per 4 KB of program size (the mutex makes concurrent host threads safe)
   static std::mutex mu;
-  static int per_sm[64];  // 0 = not yet configured
+  static bool attr_done[64];
+  static int per_sm[64][17];  // 0 = not yet queried
   int dev = 0;
   DQ_CUDA_TRY(cudaGetDevice(&dev));
   int resident;
   {
     std::lock_guard<std::mutex> lk(mu);
-    if (per_sm[dev & 63] == 0) {
-      DQ_CUDA_TRY(cudaFuncSetAttribute(k_sweep<TB, RB, S, RUNB>,
+    if (!attr_done[dev & 63]) {
+      DQ_CUDA_TRY(cudaFuncSetAttribute(k_sweep<TB, RB, S, RUNB, MINB>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_max));
-      int b = 1;
-      DQ_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_sweep<TB, RB, S, RUNB>, 1 << TB,
-                                                                smem_max));
-      per_sm[dev & 63] = b < 1 ? 1 : b;
+      attr_done[dev & 63] = true;
     }
-    resident = per_sm[dev & 63];
+    const uint32_t bucket = std::min<uint32_t>(16, (prog_bytes + 4095) / 4096);
+    const size_t smem_b = std::min(smem_max, smem - prog_bytes + 4096 * (size_t)bucket);
+    int& r = per_sm[dev & 63][bucket];
+    if (r == 0) {
+      int b = 1;
+      DQ_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_sweep<TB, RB, S, RUNB, MINB>,
+                                                                1 << TB, smem_b));
+      r = b < 1 ? 1 : b;
+    }
+    resident = r;
   }
   int sms = 148;
   DQ_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
   const uint64_t tiles = 1ULL << (n - M);
   const unsigned grid = (unsigned)std::min<uint64_t>(tiles, (uint64_t)sms * resident);
-  k_sweep<TB, RB, S, RUNB><<<grid, 1 << TB, smem, st>>>(amp, dblob, prog_bytes, (uint32_t)tiles, synth);
+  k_sweep<TB, RB, S, RUNB, MINB><<<grid, 1 << TB, smem, st>>>(amp, dblob, prog_bytes, (uint32_t)tiles, synth);
   DQ_CUDA_TRY(cudaGetLastError());
   return DQ_OK;
 }
@@ -986,12 +996,20 @@ int launch_sweep_rb(double2* amp, uint32_t n, const uint8_t* dblob, uint32_t pro
     const char* e = getenv("DQSIM_SWEEP_STAGES");
     return e ? atoi(e) : 1;
   }();
-  if (run_bits == 3) {
-    if (TB == 7 && stages != 2) return launch_sweep_r<7, RB, 1, 3>(amp, n, dblob, prog_bytes, st, synth);
-    return launch_sweep_r<TB, RB, 2, 3>(amp, n, dblob, prog_bytes, st, synth);
+  // DQSIM_SWEEP_CTAS=4: registers cut for four 128-thread CTAs per SM
+  static const int ctas = [] {
+    const char* e = getenv("DQSIM_SWEEP_CTAS");
+    return (e && atoi(e) == 4) ? 4 : 3;
+  }();
+  if (TB == 7 && stages != 2) {
+    if (ctas == 4)
+      return run_bits == 3 ? launch_sweep_r<7, RB, 1, 3, 4>(amp, n, dblob, prog_bytes, st, synth)
+                           : launch_sweep_r<7, RB, 1, 5, 4>(amp, n, dblob, prog_bytes, st, synth);
+    return run_bits == 3 ? launch_sweep_r<7, RB, 1, 3, 3>(amp, n, dblob, prog_bytes, st, synth)
+                         : launch_sweep_r<7, RB, 1, 5, 3>(amp, n, dblob, prog_bytes, st, synth);
   }
-  if (TB == 7 && stages != 2) return launch_sweep_r<7, RB, 1, 5>(amp, n, dblob, prog_bytes, st, synth);
-  return launch_sweep_r<TB, RB, 2, 5>(amp, n, dblob, prog_bytes, st, synth);
+  return run_bits == 3 ? launch_sweep_r<TB, RB, 2, 3, 3>(amp, n, dblob, prog_bytes, st, synth)
+                       : launch_sweep_r<TB, RB, 2, 5, 3>(amp, n, dblob, prog_bytes, st, synth);
 }
 
 int launch_sweep(double2* amp, uint32_t n, uint32_t TB, uint32_t RB, const uint8_t* dblob,

@@ -29,6 +29,7 @@
 #include <algorithm>
 #include <chrono>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "dq_common.cuh"
@@ -196,10 +197,11 @@ __global__ void __launch_bounds__(THREADS) k_traj(const TrajParams P) {
       // rank, rank + C, ...; 256 threads run the 8-thread-bit geometry the
       // sweeps were planned for) with a cluster barrier between sweeps; the
       // fence makes each sweep's stores visible to the CTAs of the next one.
-      // Each sweep's program is staged in shared memory behind the tile.
+      // Each sweep's program is staged in shared memory behind two tile
+      // buffers (the next tile loads while the current one is computed).
       if constexpr (THREADS == 256) {
         double2* bufs = reinterpret_cast<double2*>(smraw);
-        double2* slots = bufs + (1u << 11);
+        double2* slots = bufs + 2 * (1u << 11);
         uint8_t* sprog = reinterpret_cast<uint8_t*>(slots + kMaxSlots);
         if (pg.nsweeps == 0) {  // nothing but a basis state to write
           const uint64_t len = 1ULL << pg.n;
@@ -214,9 +216,9 @@ __global__ void __launch_bounds__(THREADS) k_traj(const TrajParams P) {
                 __ldg(reinterpret_cast<const uint4*>(P.sweep_blob + sw.off + i));
           __syncthreads();
           if (sw.run_bits == 3)
-            sweep_tiles<8, 3, 1, 3>(pg.hbm, sprog, sw.ntiles, sy, bufs, slots, rank, C);
+            sweep_tiles<8, 3, 2, 3>(pg.hbm, sprog, sw.ntiles, sy, bufs, slots, rank, C);
           else
-            sweep_tiles<8, 3, 1, 5>(pg.hbm, sprog, sw.ntiles, sy, bufs, slots, rank, C);
+            sweep_tiles<8, 3, 2, 5>(pg.hbm, sprog, sw.ntiles, sy, bufs, slots, rank, C);
           __threadfence();
           cl.sync();
         }
@@ -1199,20 +1201,36 @@ int dq_run_batch(int device, const dq_batch_item* items, uint64_t nitems,
   // than 16 amplitudes, and every resident item when local_bits is forced
   // (grouped by span); left for the engine (one dq_run each): large items
   // with measurements, resets or conditions.
-  std::vector<uint64_t> resident, hbm_items, engine_items;
+  std::vector<uint64_t> resident, hbm_items, engine_items, large;
   std::vector<HbmPlan> plans;
   for (uint64_t k = 0; k < nitems; ++k) {
-    const uint32_t n = items[k].n;
-    if (n <= kTrajMaxQubits) {
-      resident.push_back(k);
-      continue;
-    }
-    HbmPlan pl;
-    if (threads == 256 && !force_lb && n <= kHbmItemMaxQubits && plan_hbm_item(items[k], &pl)) {
-      hbm_items.push_back(k);
-      plans.push_back(std::move(pl));
-    } else {
-      engine_items.push_back(k);
+    if (items[k].n <= kTrajMaxQubits) resident.push_back(k);
+    else large.push_back(k);
+  }
+  {
+    // plan the large items on host threads
+    std::vector<HbmPlan> lp(large.size());
+    std::vector<char> ok(large.size(), 0);
+    const bool hbm_ok = threads == 256 && !force_lb;
+    const unsigned hw = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    const unsigned nt = (unsigned)std::max<size_t>(1, std::min<size_t>(hw, large.size()));
+    auto work = [&](unsigned t) {
+      for (size_t i = t; i < large.size(); i += nt) {
+        const dq_batch_item& it = items[large[i]];
+        ok[i] = hbm_ok && it.n <= kHbmItemMaxQubits && plan_hbm_item(it, &lp[i]);
+      }
+    };
+    std::vector<std::thread> th;
+    for (unsigned t = 1; t < nt; ++t) th.emplace_back(work, t);
+    work(0);
+    for (auto& x : th) x.join();
+    for (size_t i = 0; i < large.size(); ++i) {
+      if (ok[i]) {
+        hbm_items.push_back(large[i]);
+        plans.push_back(std::move(lp[i]));
+      } else {
+        engine_items.push_back(large[i]);
+      }
     }
   }
   uint32_t Cmain = hbm_items.empty() ? 1u : std::min<uint32_t>(8u, max_span);
