@@ -790,8 +790,14 @@ int dq_adjoint_batch(int device, uint32_t n, const dq_inst* prog, uint64_t ninst
   acc.forward_sweeps = kf;
   acc.backward_sweeps = kb;
   if (rc == DQ_OK) {
-    cu(cudaMalloc((void**)&psi, sizeof(double2) * len * G), "cudaMalloc(psi)");
-    cu(cudaMalloc((void**)&lam, sizeof(double2) * len * G), "cudaMalloc(lambda)");
+    // psi and lambda of the group come from the engine's size-keyed buffer
+    // cache: repeated calls (an optimiser loop) do not pay cudaMalloc/cudaFree
+    void* pv = nullptr;
+    void* lv = nullptr;
+    rc = cache_alloc(device, sizeof(double2) * len * G, &pv);
+    if (rc == DQ_OK) rc = cache_alloc(device, sizeof(double2) * len * G, &lv);
+    psi = (double2*)pv;
+    lam = (double2*)lv;
     cu(cudaMalloc((void**)&slots, sizeof(double) * sl * G), "cudaMalloc(slots)");
     cu(cudaMalloc((void**)&part, sizeof(double) * pblocks * G), "cudaMalloc(partials)");
     cu(cudaMalloc((void**)&ctr, sizeof(unsigned) * G), "cudaMalloc(counters)");
@@ -906,8 +912,8 @@ int dq_adjoint_batch(int device, uint32_t n, const dq_inst* prog, uint64_t ninst
     if (e) cudaEventDestroy(e);
   free_terms(t, st);
   cudaStreamSynchronize(st);
-  if (psi) cudaFree(psi);
-  if (lam) cudaFree(lam);
+  if (psi) cache_free(device, sizeof(double2) * len * G, psi);
+  if (lam) cache_free(device, sizeof(double2) * len * G, lam);
   if (slots) cudaFree(slots);
   if (part) cudaFree(part);
   if (ctr) cudaFree(ctr);

@@ -43,10 +43,8 @@ namespace {
 // loads.  S = 2: the next tile's load is in flight while the current one is
 // computed.  The sweep program is staged in shared memory once per launch
 // (read from global memory per op instead, QFT30 ran 38% slower).
-// MINB: CTAs per SM the register budget is cut for (3: 168 registers; 4: 128,
-// with a little spilling).
-template <int TB, int RB, int S, int RUNB, int MINB>
-__global__ void __launch_bounds__(1 << TB, (S == 1 && TB == 7 ? MINB : (TB + RB <= 11 ? 2 : 1)))
+template <int TB, int RB, int S, int RUNB>
+__global__ void __launch_bounds__(1 << TB, (S == 1 && TB == 7 ? 3 : (TB + RB <= 11 ? 2 : 1)))
     k_sweep(double2* __restrict__ state, const uint8_t* __restrict__ gprog, uint32_t prog_bytes,
             uint32_t ntiles, long long synth) {
   constexpr int T = 1 << (TB + RB);
@@ -943,7 +941,7 @@ bool convert_inst(const dq_inst& in, const uint32_t* perm, std::vector<PGate>& o
   }
 }
 
-template <int TB, int RB, int S, int RUNB, int MINB>
+template <int TB, int RB, int S, int RUNB>
 int launch_sweep_r(double2* amp, uint32_t n, const uint8_t* dblob, uint32_t prog_bytes,
                    cudaStream_t st, long long synth) {
   constexpr int M = TB + RB;
@@ -961,7 +959,7 @@ int launch_sweep_r(double2* amp, uint32_t n, const uint8_t* dblob, uint32_t prog
   {
     std::lock_guard<std::mutex> lk(mu);
     if (!attr_done[dev & 63]) {
-      DQ_CUDA_TRY(cudaFuncSetAttribute(k_sweep<TB, RB, S, RUNB, MINB>,
+      DQ_CUDA_TRY(cudaFuncSetAttribute(k_sweep<TB, RB, S, RUNB>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_max));
       attr_done[dev & 63] = true;
     }
@@ -970,7 +968,7 @@ int launch_sweep_r(double2* amp, uint32_t n, const uint8_t* dblob, uint32_t prog
     int& r = per_sm[dev & 63][bucket];
     if (r == 0) {
       int b = 1;
-      DQ_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_sweep<TB, RB, S, RUNB, MINB>,
+      DQ_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_sweep<TB, RB, S, RUNB>,
                                                                 1 << TB, smem_b));
       r = b < 1 ? 1 : b;
     }
@@ -980,7 +978,7 @@ int launch_sweep_r(double2* amp, uint32_t n, const uint8_t* dblob, uint32_t prog
   DQ_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
   const uint64_t tiles = 1ULL << (n - M);
   const unsigned grid = (unsigned)std::min<uint64_t>(tiles, (uint64_t)sms * resident);
-  k_sweep<TB, RB, S, RUNB, MINB><<<grid, 1 << TB, smem, st>>>(amp, dblob, prog_bytes, (uint32_t)tiles, synth);
+  k_sweep<TB, RB, S, RUNB><<<grid, 1 << TB, smem, st>>>(amp, dblob, prog_bytes, (uint32_t)tiles, synth);
   DQ_CUDA_TRY(cudaGetLastError());
   return DQ_OK;
 }
@@ -996,20 +994,11 @@ int launch_sweep_rb(double2* amp, uint32_t n, const uint8_t* dblob, uint32_t pro
     const char* e = getenv("DQSIM_SWEEP_STAGES");
     return e ? atoi(e) : 1;
   }();
-  // DQSIM_SWEEP_CTAS=4: registers cut for four 128-thread CTAs per SM
-  static const int ctas = [] {
-    const char* e = getenv("DQSIM_SWEEP_CTAS");
-    return (e && atoi(e) == 4) ? 4 : 3;
-  }();
-  if (TB == 7 && stages != 2) {
-    if (ctas == 4)
-      return run_bits == 3 ? launch_sweep_r<7, RB, 1, 3, 4>(amp, n, dblob, prog_bytes, st, synth)
-                           : launch_sweep_r<7, RB, 1, 5, 4>(amp, n, dblob, prog_bytes, st, synth);
-    return run_bits == 3 ? launch_sweep_r<7, RB, 1, 3, 3>(amp, n, dblob, prog_bytes, st, synth)
-                         : launch_sweep_r<7, RB, 1, 5, 3>(amp, n, dblob, prog_bytes, st, synth);
-  }
-  return run_bits == 3 ? launch_sweep_r<TB, RB, 2, 3, 3>(amp, n, dblob, prog_bytes, st, synth)
-                       : launch_sweep_r<TB, RB, 2, 5, 3>(amp, n, dblob, prog_bytes, st, synth);
+  if (TB == 7 && stages != 2)
+    return run_bits == 3 ? launch_sweep_r<7, RB, 1, 3>(amp, n, dblob, prog_bytes, st, synth)
+                         : launch_sweep_r<7, RB, 1, 5>(amp, n, dblob, prog_bytes, st, synth);
+  return run_bits == 3 ? launch_sweep_r<TB, RB, 2, 3>(amp, n, dblob, prog_bytes, st, synth)
+                       : launch_sweep_r<TB, RB, 2, 5>(amp, n, dblob, prog_bytes, st, synth);
 }
 
 int launch_sweep(double2* amp, uint32_t n, uint32_t TB, uint32_t RB, const uint8_t* dblob,

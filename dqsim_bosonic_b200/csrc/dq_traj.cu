@@ -1293,11 +1293,11 @@ int dq_run_batch(int device, const dq_batch_item* items, uint64_t nitems,
   int rc = DQ_OK;
   double2* d_hbm = nullptr;
   if (hbm_amps) {
-    cudaError_t e = cudaMalloc((void**)&d_hbm, sizeof(double2) * hbm_amps);
-    if (e != cudaSuccess) {
-      cudaGetLastError();
-      rc = fail(DQ_ERR_OOM, std::string("cudaMalloc(batch HBM states): ") + cudaGetErrorString(e));
-    }
+    // from the engine's size-keyed buffer cache: a repeated batch does not
+    // pay cudaMalloc/cudaFree of its HBM states
+    void* p = nullptr;
+    rc = cache_alloc(device, sizeof(double2) * hbm_amps, &p);
+    d_hbm = (double2*)p;
   }
   for (int c = 0; c < 5 && rc == DQ_OK; ++c) {
     if (outs[c].empty()) continue;
@@ -1360,7 +1360,7 @@ int dq_run_batch(int device, const dq_batch_item* items, uint64_t nitems,
                                         std::to_string(inst) + ": unsupported generic gate");
     }
   }
-  if (d_hbm) cudaFree(d_hbm);
+  if (d_hbm) cache_free(device, sizeof(double2) * hbm_amps, d_hbm);
   acc.hbm_items = (uint32_t)hbm_items.size();
   // large states: the HBM engine, one state per size reused across items
   dq_state_t h = nullptr;
