@@ -396,7 +396,7 @@ def main():
         nonlocal launches
         st.reset()
         _, prof = run_program(st, prog, 7, nat.SEM_SIMULATE, exec_mode)
-        launches += 1 + int(prof.kernel_launches)
+        launches += int(prof.kernel_launches)
         return prof
 
     for _ in range(max(args.warmup, 3)):

@@ -11,6 +11,7 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <algorithm>
 #include <chrono>
 #include <map>
 #include <mutex>
@@ -133,6 +134,70 @@ int check_handle(dq_state_t h) {
 
 int sync_stream(dq_state_t h) {
   DQ_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return DQ_OK;
+}
+
+// Query outputs up to this size use the handle's kept buffers; larger ones a
+// temporary allocation (a 30-qubit marginal alone is 8 GiB).
+constexpr size_t kQueryKeepBytes = 64ULL << 20;
+
+// A device buffer for one query: the handle's kept buffer, or a temporary one
+// freed (after the stream drains) when the object goes out of scope.
+struct QueryBuffer {
+  dq_state_t h = nullptr;
+  void* tmp = nullptr;
+  void* ptr = nullptr;
+  ~QueryBuffer() {
+    if (tmp) {
+      cudaStreamSynchronize(h->stream);
+      cudaFree(tmp);
+    }
+  }
+  int get(dq_state_t hh, size_t bytes) {
+    h = hh;
+    if (bytes <= kQueryKeepBytes) {
+      DQ_TRY(ensure_query_buffers(h, bytes, 0));
+      ptr = h->q_dev;
+      return DQ_OK;
+    }
+    cudaError_t e = cudaMalloc(&tmp, bytes);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      tmp = nullptr;
+      return fail(DQ_ERR_OOM, std::string("cudaMalloc(query output): ") + cudaGetErrorString(e));
+    }
+    ptr = tmp;
+    return DQ_OK;
+  }
+};
+
+int ensure_query_buffers(dq_state_t h, size_t dev_bytes, size_t host_bytes) {
+  if (dev_bytes > h->q_dev_cap) {
+    DQ_TRY(sync_stream(h));
+    if (h->q_dev) cudaFree(h->q_dev);
+    h->q_dev = nullptr;
+    h->q_dev_cap = 0;
+    const size_t cap = std::max<size_t>(dev_bytes, 64 * 1024);
+    cudaError_t e = cudaMalloc(&h->q_dev, cap);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      return fail(DQ_ERR_OOM, std::string("cudaMalloc(query buffer): ") + cudaGetErrorString(e));
+    }
+    h->q_dev_cap = cap;
+  }
+  if (host_bytes > h->q_host_cap) {
+    DQ_TRY(sync_stream(h));
+    if (h->q_host) cudaFreeHost(h->q_host);
+    h->q_host = nullptr;
+    h->q_host_cap = 0;
+    const size_t cap = std::max<size_t>(host_bytes, 64 * 1024);
+    cudaError_t e = cudaMallocHost(&h->q_host, cap);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      return fail(DQ_ERR_OOM, std::string("cudaMallocHost(query buffer): ") + cudaGetErrorString(e));
+    }
+    h->q_host_cap = cap;
+  }
   return DQ_OK;
 }
 
@@ -478,6 +543,8 @@ int dq_state_destroy(dq_state_t h) {
   if (h->stream && h->sc.d_partial && h->sc.d_counter && h->sc.h_pinned && put_shell(h))
     return DQ_OK;
   fused_release(h->fw);
+  if (h->q_dev) cudaFree(h->q_dev);
+  if (h->q_host) cudaFreeHost(h->q_host);
   if (h->sc.d_partial) cudaFree(h->sc.d_partial);
   if (h->sc.d_counter) cudaFree(h->sc.d_counter);
   if (h->sc.h_pinned) cudaFreeHost(h->sc.h_pinned);
@@ -783,16 +850,19 @@ int dq_marginal_probs(dq_state_t h, const uint32_t* qubits, uint32_t k, double* 
   for (auto& q : mq) q = h->perm[q];
   qubits = mq.data();
   const uint64_t nj = 1ULL << k;
-  double* d = nullptr;
-  DQ_CUDA_TRY(cudaMallocAsync((void**)&d, sizeof(double) * nj, h->stream));
-  int rc = launch_marginal(h->amp, h->n, qubits, k, d, h->sc, h->stream, h->device);
-  if (rc == DQ_OK) {
-    cudaError_t e = cudaMemcpyAsync(out, d, sizeof(double) * nj, cudaMemcpyDeviceToHost, h->stream);
-    if (e != cudaSuccess) rc = fail(DQ_ERR_CUDA, cudaGetErrorString(e));
-  }
-  cudaFreeAsync(d, h->stream);
-  if (rc != DQ_OK) return rc;
-  return sync_stream(h);
+  // small outputs land in the handle's pinned buffer (then one memcpy), large
+  // ones go straight to the caller's memory
+  const bool staged = nj <= (1ULL << 16);
+  QueryBuffer qb;
+  DQ_TRY(qb.get(h, sizeof(double) * nj));
+  if (staged) DQ_TRY(ensure_query_buffers(h, 0, sizeof(double) * nj));
+  double* d = reinterpret_cast<double*>(qb.ptr);
+  DQ_TRY(launch_marginal(h->amp, h->n, qubits, k, d, h->sc, h->stream, h->device));
+  DQ_CUDA_TRY(cudaMemcpyAsync(staged ? h->q_host : (void*)out, d, sizeof(double) * nj,
+                              cudaMemcpyDeviceToHost, h->stream));
+  DQ_TRY(sync_stream(h));
+  if (staged) memcpy(out, h->q_host, sizeof(double) * nj);
+  return DQ_OK;
 }
 
 int dq_sample_key(dq_state_t h, const uint32_t* qubits, uint32_t k, const uint32_t* key8,
@@ -811,13 +881,15 @@ int dq_sample_key(dq_state_t h, const uint32_t* qubits, uint32_t k, const uint32
   for (auto& q : mq) q = h->perm[q];
   qubits = mq.data();
   const uint64_t nj = 1ULL << k;
-  double* cdf = nullptr;
-  uint32_t* idx = nullptr;
-  DQ_CUDA_TRY(cudaMallocAsync((void**)&cdf, sizeof(double) * nj, h->stream));
-  int rc = DQ_OK;
-  cudaError_t e = cudaMallocAsync((void**)&idx, sizeof(uint32_t) * (shots ? shots : 1), h->stream);
-  if (e != cudaSuccess) rc = fail(DQ_ERR_OOM, cudaGetErrorString(e));
-  if (rc == DQ_OK) rc = launch_marginal(h->amp, h->n, qubits, k, cdf, h->sc, h->stream, h->device);
+  // CDF and sampled indices in the handle's device query buffer (CDF first,
+  // indices 256-byte aligned after it)
+  const size_t cdf_bytes = (sizeof(double) * nj + 255) / 256 * 256;
+  QueryBuffer qb;
+  DQ_TRY(qb.get(h, cdf_bytes + sizeof(uint32_t) * (shots ? shots : 1)));
+  double* cdf = reinterpret_cast<double*>(qb.ptr);
+  uint32_t* idx = reinterpret_cast<uint32_t*>(reinterpret_cast<char*>(qb.ptr) + cdf_bytes);
+  int rc = launch_marginal(h->amp, h->n, qubits, k, cdf, h->sc, h->stream, h->device);
+  cudaError_t e = cudaSuccess;
   if (rc == DQ_OK) rc = launch_cdf(cdf, nj, h->stream, h->device);
   if (rc == DQ_OK) {
     e = cudaMemsetAsync(h->sc.d_ull, 0, sizeof(unsigned long long), h->stream);
@@ -834,8 +906,6 @@ int dq_sample_key(dq_state_t h, const uint32_t* qubits, uint32_t k, const uint32
                         cudaMemcpyDeviceToHost, h->stream);
     if (e != cudaSuccess) rc = fail(DQ_ERR_CUDA, cudaGetErrorString(e));
   }
-  cudaFreeAsync(cdf, h->stream);
-  cudaFreeAsync(idx, h->stream);
   if (rc != DQ_OK) return rc;
   DQ_TRY(sync_stream(h));
   memcpy(&nb, h->sc.h_pinned, sizeof(nb));

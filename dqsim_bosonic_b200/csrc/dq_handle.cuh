@@ -28,6 +28,12 @@ struct dq_state_s {
   // from it (no read of the state, no reset pass), anything else writes it
   // first (materialize_basis)
   int64_t lazy_basis = -1;
+  // query buffers (marginals, CDF, sampled indices): kept and grown as needed
+  // so that a query allocates nothing per call
+  void* q_dev = nullptr;
+  size_t q_dev_cap = 0;
+  void* q_host = nullptr;  // pinned
+  size_t q_host_cap = 0;
 };
 
 namespace dq {
@@ -61,6 +67,9 @@ int canonicalize(dq_state_t h);
 void reset_perm(dq_state_t h);
 // Copy `count` device doubles to `out` through the handle's pinned buffer.
 int read_scalars(dq_state_t h, const double* d_src, int count, double* out);
+// Grow the handle's query buffers to at least dev_bytes (device) and
+// host_bytes (pinned host); the stream is drained before a buffer is replaced.
+int ensure_query_buffers(dq_state_t h, size_t dev_bytes, size_t host_bytes);
 int gate_qubit_count(int kind);
 int validate_inst(const dq_inst& in, uint32_t n, uint64_t nconds, uint64_t ncbits,
                   const dq_cond* conds, uint64_t idx);
