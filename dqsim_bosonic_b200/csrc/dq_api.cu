@@ -853,11 +853,16 @@ int dq_marginal_probs(dq_state_t h, const uint32_t* qubits, uint32_t k, double* 
   // small outputs land in the handle's pinned buffer (then one memcpy), large
   // ones go straight to the caller's memory
   const bool staged = nj <= (1ULL << 16);
+  // output first, the reduction's partials 256-byte aligned after it
+  const size_t out_bytes = (sizeof(double) * nj + 255) / 256 * 256;
+  const size_t work_bytes = sizeof(double) * marginal_workspace(h->n, qubits, k, h->device);
   QueryBuffer qb;
-  DQ_TRY(qb.get(h, sizeof(double) * nj));
+  DQ_TRY(qb.get(h, out_bytes + work_bytes));
   if (staged) DQ_TRY(ensure_query_buffers(h, 0, sizeof(double) * nj));
   double* d = reinterpret_cast<double*>(qb.ptr);
-  DQ_TRY(launch_marginal(h->amp, h->n, qubits, k, d, h->sc, h->stream, h->device));
+  double* work = work_bytes ? reinterpret_cast<double*>(reinterpret_cast<char*>(qb.ptr) + out_bytes)
+                            : nullptr;
+  DQ_TRY(launch_marginal(h->amp, h->n, qubits, k, d, work, h->sc, h->stream, h->device));
   DQ_CUDA_TRY(cudaMemcpyAsync(staged ? h->q_host : (void*)out, d, sizeof(double) * nj,
                               cudaMemcpyDeviceToHost, h->stream));
   DQ_TRY(sync_stream(h));
@@ -881,16 +886,22 @@ int dq_sample_key(dq_state_t h, const uint32_t* qubits, uint32_t k, const uint32
   for (auto& q : mq) q = h->perm[q];
   qubits = mq.data();
   const uint64_t nj = 1ULL << k;
-  // CDF and sampled indices in the handle's device query buffer (CDF first,
-  // indices 256-byte aligned after it)
-  const size_t cdf_bytes = (sizeof(double) * nj + 255) / 256 * 256;
+  // CDF, sampled indices and the reductions' workspace in the handle's device
+  // query buffer, each part 256-byte aligned
+  auto align256 = [](size_t b) { return (b + 255) / 256 * 256; };
+  const size_t cdf_bytes = align256(sizeof(double) * nj);
+  const size_t idx_bytes = align256(sizeof(uint32_t) * (shots ? shots : 1));
+  const size_t work_bytes = sizeof(double) * std::max<uint64_t>(marginal_workspace(h->n, qubits, k, h->device),
+                                                                cdf_workspace(nj));
   QueryBuffer qb;
-  DQ_TRY(qb.get(h, cdf_bytes + sizeof(uint32_t) * (shots ? shots : 1)));
-  double* cdf = reinterpret_cast<double*>(qb.ptr);
-  uint32_t* idx = reinterpret_cast<uint32_t*>(reinterpret_cast<char*>(qb.ptr) + cdf_bytes);
-  int rc = launch_marginal(h->amp, h->n, qubits, k, cdf, h->sc, h->stream, h->device);
+  DQ_TRY(qb.get(h, cdf_bytes + idx_bytes + work_bytes));
+  char* base = reinterpret_cast<char*>(qb.ptr);
+  double* cdf = reinterpret_cast<double*>(base);
+  uint32_t* idx = reinterpret_cast<uint32_t*>(base + cdf_bytes);
+  double* work = reinterpret_cast<double*>(base + cdf_bytes + idx_bytes);
+  int rc = launch_marginal(h->amp, h->n, qubits, k, cdf, work, h->sc, h->stream, h->device);
   cudaError_t e = cudaSuccess;
-  if (rc == DQ_OK) rc = launch_cdf(cdf, nj, h->stream, h->device);
+  if (rc == DQ_OK) rc = launch_cdf(cdf, nj, work, h->stream, h->device);
   if (rc == DQ_OK) {
     e = cudaMemsetAsync(h->sc.d_ull, 0, sizeof(unsigned long long), h->stream);
     if (e != cudaSuccess) rc = fail(DQ_ERR_CUDA, cudaGetErrorString(e));

@@ -577,71 +577,108 @@ int launch_set_basis(double2* s, uint32_t n, uint64_t index, cudaStream_t st, in
   return DQ_OK;
 }
 
-int launch_marginal(const double2* s, uint32_t n, const uint32_t* qubits, uint32_t k,
-                    double* d_out, Scratch& sc, cudaStream_t st, int device) {
+namespace {
+
+// How one marginal query reduces: the kernel family, its partial count and the
+// workspace doubles the partials need beyond the handle scratch.
+struct MargPlan {
+  int kind = 0;        // 0 k_marg_low, 1 k_marg_thread, 2 k_marg_seg
+  uint64_t parts = 1;  // blocks of k_marg_low / segments per output of k_marg_seg
+  uint64_t work = 0;   // doubles of caller workspace (0: none needed)
   MargParams P{};
+};
+
+MargPlan plan_marginal(uint32_t n, const uint32_t* qubits, uint32_t k, int device) {
+  MargPlan m;
   uint64_t mask = 0;
   for (uint32_t b = 0; b < k; ++b) {
-    P.q[b] = qubits[b];
+    m.P.q[b] = qubits[b];
     mask |= 1ULL << qubits[b];
   }
-  P.k = k;
-  P.rest.np = 0;
-  for (uint32_t b = 0; b < 64 && P.rest.np < 32; ++b)
-    if (mask >> b & 1ULL) P.rest.p[P.rest.np++] = b;
+  m.P.k = k;
+  m.P.rest.np = 0;
+  for (uint32_t b = 0; b < 64 && m.P.rest.np < 32; ++b)
+    if (mask >> b & 1ULL) m.P.rest.p[m.P.rest.np++] = b;
   const uint64_t nj = 1ULL << k;
   const uint64_t nterms = 1ULL << (n - k);
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-  // thread-per-output (exact reference order) when there are enough outputs
-  // to fill the GPU or few terms per output
-  const uint32_t top = k ? P.rest.p[P.rest.np - 1] : 0;  // highest marginal position
+  const uint32_t top = k ? m.P.rest.p[m.P.rest.np - 1] : 0;  // highest marginal position
   if (k >= 1 && top < 10 && n >= 20 && nterms > 64) {
     // all marginal qubits in the low 10 bits (e.g. after a relabeling)
-    uint32_t nb = 1;
-    while (nb * 2 <= (uint32_t)sms * 4 && (1ULL << n) / (nb * 2) >= 1024 * 4) nb *= 2;
-    const uint64_t chunk = (1ULL << n) / nb;
-    double* tmp = nullptr;
-    DQ_CUDA_TRY(cudaMallocAsync((void**)&tmp, sizeof(double) * nj * nb, st));
-    k_marg_low<<<nb, 1024, 0, st>>>(s, chunk, P, tmp);
-    k_marg_sum<<<blocks_for(nj, kThreads), kThreads, 0, st>>>(tmp, nj, nb, d_out);
-    DQ_CUDA_TRY(cudaFreeAsync(tmp, st));
-    DQ_CUDA_TRY(cudaGetLastError());
-    return DQ_OK;
+    uint64_t nb = 1;
+    while (nb * 2 <= (uint64_t)sms * 4 && (1ULL << n) / (nb * 2) >= 1024 * 4) nb *= 2;
+    m.kind = 0;
+    m.parts = nb;
+    m.work = nj * nb;
+    return m;
   }
+  // thread-per-output (exact reference order) when there are enough outputs
+  // to fill the GPU or few terms per output
   if (nterms <= 64 || nj >= (uint64_t)sms * 1024) {
-    k_marg_thread<<<blocks_for(nj, kThreads), kThreads, 0, st>>>(s, nj, nterms, P, d_out);
-  } else {
-    // a power of two number of segments per output (dividing nterms), about
-    // 8 blocks per SM in total, each segment at least one block's worth
-    const uint64_t target_blocks = (uint64_t)sms * 8;
-    uint64_t nseg = 1;
-    while (nj * nseg * 2 <= target_blocks && nseg * 2 * kRedThreads <= nterms) nseg <<= 1;
-    while (nj * nseg > (uint64_t)kPartials && nseg > 1) nseg >>= 1;
-    double* partial = sc.d_partial;
-    double* tmp = nullptr;
-    if (nj * nseg > (uint64_t)kPartials) {
-      DQ_CUDA_TRY(cudaMallocAsync((void**)&tmp, sizeof(double) * nj * nseg, st));
-      partial = tmp;
-    }
-    k_marg_seg<<<(unsigned)(nj * nseg), kRedThreads, 0, st>>>(s, nterms, (uint32_t)nseg, P, partial);
-    k_marg_sum<<<blocks_for(nj, kThreads), kThreads, 0, st>>>(partial, nj, (uint32_t)nseg, d_out);
-    if (tmp) DQ_CUDA_TRY(cudaFreeAsync(tmp, st));
+    m.kind = 1;
+    return m;
   }
+  // a power of two number of segments per output (dividing nterms), about
+  // 8 blocks per SM in total, each segment at least one block's worth
+  const uint64_t target_blocks = (uint64_t)sms * 8;
+  uint64_t nseg = 1;
+  while (nj * nseg * 2 <= target_blocks && nseg * 2 * kRedThreads <= nterms) nseg <<= 1;
+  while (nj * nseg > (uint64_t)kPartials && nseg > 1) nseg >>= 1;
+  m.kind = 2;
+  m.parts = nseg;
+  m.work = nj * nseg > (uint64_t)kPartials ? nj * nseg : 0;
+  return m;
+}
+
+}  // namespace
+
+uint64_t marginal_workspace(uint32_t n, const uint32_t* qubits, uint32_t k, int device) {
+  return plan_marginal(n, qubits, k, device).work;
+}
+
+int launch_marginal(const double2* s, uint32_t n, const uint32_t* qubits, uint32_t k,
+                    double* d_out, double* d_work, Scratch& sc, cudaStream_t st, int device) {
+  const MargPlan m = plan_marginal(n, qubits, k, device);
+  const uint64_t nj = 1ULL << k;
+  double* tmp = nullptr;  // allocated here only when the caller gave no workspace
+  double* work = d_work;
+  if (m.work && !work) {
+    DQ_CUDA_TRY(cudaMallocAsync((void**)&tmp, sizeof(double) * m.work, st));
+    work = tmp;
+  }
+  if (m.kind == 0) {
+    k_marg_low<<<(unsigned)m.parts, 1024, 0, st>>>(s, (1ULL << n) / m.parts, m.P, work);
+    k_marg_sum<<<blocks_for(nj, kThreads), kThreads, 0, st>>>(work, nj, (uint32_t)m.parts, d_out);
+  } else if (m.kind == 1) {
+    k_marg_thread<<<blocks_for(nj, kThreads), kThreads, 0, st>>>(s, nj, 1ULL << (n - k), m.P, d_out);
+  } else {
+    double* partial = m.work ? work : sc.d_partial;
+    k_marg_seg<<<(unsigned)(nj * m.parts), kRedThreads, 0, st>>>(s, 1ULL << (n - k), (uint32_t)m.parts,
+                                                                  m.P, partial);
+    k_marg_sum<<<blocks_for(nj, kThreads), kThreads, 0, st>>>(partial, nj, (uint32_t)m.parts, d_out);
+  }
+  if (tmp) DQ_CUDA_TRY(cudaFreeAsync(tmp, st));
   DQ_CUDA_TRY(cudaGetLastError());
   return DQ_OK;
 }
 
-int launch_cdf(double* d, uint64_t len, cudaStream_t st, int device) {
+uint64_t cdf_workspace(uint64_t len) { return (len + kScanChunk - 1) / kScanChunk; }
+
+int launch_cdf(double* d, uint64_t len, double* d_work, cudaStream_t st, int device) {
   (void)device;
-  const uint64_t nb = (len + kScanChunk - 1) / kScanChunk;
-  double* sums = nullptr;
-  DQ_CUDA_TRY(cudaMallocAsync((void**)&sums, sizeof(double) * nb, st));
+  const uint64_t nb = cdf_workspace(len);
+  double* tmp = nullptr;  // allocated here only when the caller gave no workspace
+  double* sums = d_work;
+  if (!sums) {
+    DQ_CUDA_TRY(cudaMallocAsync((void**)&tmp, sizeof(double) * nb, st));
+    sums = tmp;
+  }
   k_scan_sums<<<(unsigned)nb, kScanThreads, 0, st>>>(d, len, sums);
   k_scan_offsets<<<1, kScanThreads, 0, st>>>(sums, nb);
   k_scan_apply<<<(unsigned)nb, kScanThreads, 0, st>>>(d, len, sums);
   k_set_last_one<<<1, 1, 0, st>>>(d, len);
-  DQ_CUDA_TRY(cudaFreeAsync(sums, st));
+  if (tmp) DQ_CUDA_TRY(cudaFreeAsync(tmp, st));
   DQ_CUDA_TRY(cudaGetLastError());
   return DQ_OK;
 }

@@ -36,11 +36,17 @@ int launch_collapse(double2* s, uint32_t n, uint32_t q, int outcome, double norm
                     cudaStream_t st, int device);
 int launch_set_basis(double2* s, uint32_t n, uint64_t index, cudaStream_t st, int device);
 
-// marginal probabilities into a device buffer d_out[2^k].
+// Device doubles of workspace a marginal over these (physical) qubits needs.
+uint64_t marginal_workspace(uint32_t n, const uint32_t* qubits, uint32_t k, int device);
+// marginal probabilities into a device buffer d_out[2^k]; d_work holds
+// marginal_workspace() doubles (nullptr: a stream-ordered temporary is used).
 int launch_marginal(const double2* s, uint32_t n, const uint32_t* qubits, uint32_t k,
-                    double* d_out, Scratch& sc, cudaStream_t st, int device);
-// in-place inclusive prefix sum of d[len] (deterministic order), last = 1.0.
-int launch_cdf(double* d, uint64_t len, cudaStream_t st, int device);
+                    double* d_out, double* d_work, Scratch& sc, cudaStream_t st, int device);
+// Device doubles of workspace launch_cdf needs for len entries.
+uint64_t cdf_workspace(uint64_t len);
+// in-place inclusive prefix sum of d[len] (deterministic order), last = 1.0;
+// d_work holds cdf_workspace(len) doubles (nullptr: a stream-ordered temporary).
+int launch_cdf(double* d, uint64_t len, double* d_work, cudaStream_t st, int device);
 // per-shot lower_bound in the CDF with device ChaCha8 draws.
 int launch_sample(const double* cdf, uint64_t len, const uint32_t key[8], uint64_t shots,
                   uint32_t* d_idx, unsigned long long* d_boundary, cudaStream_t st, int device);

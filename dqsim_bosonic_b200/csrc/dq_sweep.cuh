@@ -126,7 +126,9 @@ __device__ __forceinline__ void cp_async_wait() {
 // (amplitudes with bit B set times W * F[compress(j)]).  KIND: 0 general
 // 2x2, 1 real 2x2, 2 [[1,1],[1,-1]], 3 X.  Controls only occur without a
 // pre-flush (the planner fuses flushes into uncontrolled ops only).
-template <int RB, int B, int KIND, bool PRE>
+// PRE: 0 no flush; 1 flush by the per-thread factor W; 2 flush by W times the
+// register-partner table F (known at compile time, no per-pair select).
+template <int RB, int B, int KIND, int PRE>
 __device__ __forceinline__ void u1_op(double2 (&a)[1 << RB], const double2* __restrict__ D,
                                       uint32_t creg, double2 W, const double2* __restrict__ F) {
   double2 u00, u01, u10, u11;
@@ -136,13 +138,15 @@ __device__ __forceinline__ void u1_op(double2 (&a)[1 << RB], const double2* __re
 #pragma unroll
   for (int j = 0; j < (1 << RB); ++j) {
     if (j & (1 << B)) continue;
-    if (!PRE && (j & creg) != creg) continue;
+    if (PRE == 0 && (j & creg) != creg) continue;
     const int k = j | (1 << B);
     const double2 x = a[j];
     double2 y = a[k];
-    if (PRE) {
+    if (PRE == 2) {
       const int idx = ((k >> (B + 1)) << B) | (k & ((1 << B) - 1));
-      y = cmul_f(y, F ? cmul_f(W, F[idx]) : W);
+      y = cmul_f(y, cmul_f(W, F[idx]));
+    } else if (PRE == 1) {
+      y = cmul_f(y, W);
     }
     if (KIND == 0) {
       a[j] = cmac2_f(u00, x, u01, y);
@@ -255,10 +259,18 @@ __device__ __forceinline__ void exec_op(const uint4 o0, const uint4 o1, double2 
     if (flags & FL_REG) F = T;
   }
   switch (type) {
-    case OP_U1: if (flags & FL_PRE) { DQ_SW_U1(0, true) } else { DQ_SW_U1(0, false) } break;
-    case OP_U1R: if (flags & FL_PRE) { DQ_SW_U1(1, true) } else { DQ_SW_U1(1, false) } break;
-    case OP_U1H: if (flags & FL_PRE) { DQ_SW_U1(2, true) } else { DQ_SW_U1(2, false) } break;
-    case OP_U1X: if (flags & FL_PRE) { DQ_SW_U1(3, true) } else { DQ_SW_U1(3, false) } break;
+    case OP_U1:
+      if (!(flags & FL_PRE)) { DQ_SW_U1(0, 0) } else if (F) { DQ_SW_U1(0, 2) } else { DQ_SW_U1(0, 1) }
+      break;
+    case OP_U1R:
+      if (!(flags & FL_PRE)) { DQ_SW_U1(1, 0) } else if (F) { DQ_SW_U1(1, 2) } else { DQ_SW_U1(1, 1) }
+      break;
+    case OP_U1H:
+      if (!(flags & FL_PRE)) { DQ_SW_U1(2, 0) } else if (F) { DQ_SW_U1(2, 2) } else { DQ_SW_U1(2, 1) }
+      break;
+    case OP_U1X:
+      if (!(flags & FL_PRE)) { DQ_SW_U1(3, 0) } else if (F) { DQ_SW_U1(3, 2) } else { DQ_SW_U1(3, 1) }
+      break;
     case OP_U2: u2_dispatch<RB>(a, b0, b1, creg, D); break;
     case OP_FLUSH_R: DQ_SW_CASES1(flush_reg, a, W, F); break;
     case OP_FLUSH_T:
