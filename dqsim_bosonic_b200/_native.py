@@ -23,6 +23,7 @@ DQ_ERR_OOM = -3
 DQ_ERR_UNSUPPORTED = -4
 DQ_ERR_NO_DEVICE = -5
 DQ_ERR_INTERNAL = -6
+DQ_ERR_DECODE = -7
 
 # ---- instruction kinds (enum dq_kind) --------------------------------------------
 KIND_NAMES = [
@@ -155,6 +156,17 @@ class BatchItem(ctypes.Structure):
     ]
 
 
+class CircuitInfo(ctypes.Structure):
+    _fields_ = [
+        ("ninst", ctypes.c_uint64),
+        ("ncond", ctypes.c_uint64),
+        ("num_qubits", ctypes.c_uint64),
+        ("num_cbits", ctypes.c_uint64),
+        ("cbit_space", ctypes.c_uint64),
+        ("names_bytes", ctypes.c_uint64),
+    ]
+
+
 class EngineError(RuntimeError):
     """A non-OK status returned by the engine."""
 
@@ -178,6 +190,10 @@ SIGNATURES = [
     ("dq_abi_version", ctypes.c_int, []),
     ("dq_last_error", ctypes.c_char_p, []),
     ("dq_device_count", ctypes.c_int, [ctypes.POINTER(ctypes.c_int)]),
+    ("dq_circuit_decode", ctypes.c_int, [ctypes.c_char_p, _U64, ctypes.POINTER(_P),
+                                         ctypes.POINTER(CircuitInfo)]),
+    ("dq_circuit_export", ctypes.c_int, [_P, _P, _P, _P]),
+    ("dq_circuit_free", None, [_P]),
     ("dq_state_create", ctypes.c_int, [_U32, ctypes.c_int, ctypes.POINTER(_P)]),
     ("dq_state_destroy", ctypes.c_int, [_P]),
     ("dq_state_num_qubits", ctypes.c_int, [_P, ctypes.POINTER(_U32)]),

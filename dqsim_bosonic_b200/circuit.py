@@ -19,8 +19,10 @@ serde rules restated here:
 """
 from __future__ import annotations
 
+import ctypes
 import json
 import math
+import struct
 from dataclasses import dataclass, field
 from typing import Any
 
@@ -369,6 +371,53 @@ def encode(circuit: Circuit) -> Program:
     if space > (1 << 26):
         raise ValueError("classical register index too large")
     return Program(insts, carr, n, ncb, space, names)
+
+
+def _decode_native(text: str) -> Program | None:
+    """The library's decoder (``dq_circuit_decode``); None when it leaves the
+    text to :func:`decode_circuit_json` (an error to report, or a rare form)."""
+    from . import _native as nat
+
+    try:
+        raw = text.encode("utf-8")
+    except UnicodeEncodeError:  # lone surrogates in the text
+        return None
+    L = nat.lib()
+    handle = ctypes.c_void_p()
+    info = nat.CircuitInfo()
+    rc = L.dq_circuit_decode(raw, len(raw), ctypes.byref(handle), ctypes.byref(info))
+    if rc == nat.DQ_ERR_DECODE:
+        return None
+    nat.check(rc, "dq_circuit_decode")
+    try:
+        insts = np.empty(info.ninst, dtype=INST_DTYPE)
+        conds = np.empty(info.ncond, dtype=COND_DTYPE)
+        names = np.empty(info.names_bytes, dtype=np.uint8)
+        nat.check(L.dq_circuit_export(handle, nat.ptr(insts) if insts.size else None,
+                                      nat.ptr(conds) if conds.size else None,
+                                      nat.ptr(names) if names.size else None),
+                  "dq_circuit_export")
+    finally:
+        L.dq_circuit_free(handle)
+    gate_names: dict[int, str] = {}
+    buf = names.tobytes()
+    pos = 0
+    while pos < len(buf):
+        idx, ln = struct.unpack_from("<QQ", buf, pos)
+        gate_names[idx] = buf[pos + 16:pos + 16 + ln].decode("utf-8")
+        pos += 16 + ln
+    return Program(insts, conds, int(info.num_qubits), int(info.num_cbits), int(info.cbit_space),
+                   gate_names)
+
+
+def decode_program(text: str) -> Program:
+    """Circuit JSON -> ``Program``: the library's decoder for the well-formed
+    case, this module's decoder and encoder for everything it declines (same
+    result, and the reference's error messages)."""
+    prog = _decode_native(text)
+    if prog is not None:
+        return prog
+    return encode(decode_circuit_json(text))
 
 
 def circuit_json(circuit: Any) -> str:

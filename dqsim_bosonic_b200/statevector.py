@@ -18,7 +18,7 @@ from typing import Any
 import numpy as np
 
 from . import _native as nat
-from .circuit import CircuitDecodeError, Program, circuit_json, decode_circuit_json, encode, format_cbits
+from .circuit import CircuitDecodeError, Program, circuit_json, decode_program, format_cbits
 
 _U64 = (1 << 64) - 1
 
@@ -196,7 +196,7 @@ def _parse(circuit: Any) -> tuple[Program, float]:
     t0 = time.perf_counter()
     text = circuit_json(circuit)
     try:
-        prog = encode(decode_circuit_json(text))
+        prog = decode_program(text)
     except CircuitDecodeError as e:
         raise ValueError(f"Circuit JSON parse error: {e}") from None
     return prog, time.perf_counter() - t0

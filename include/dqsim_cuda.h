@@ -49,6 +49,7 @@ extern "C" {
 #define DQ_ERR_UNSUPPORTED (-4)    /* unsupported generic gate (NotImplemented) */
 #define DQ_ERR_NO_DEVICE (-5)      /* no CUDA device visible                  */
 #define DQ_ERR_INTERNAL (-6)       /* invariant violated inside the engine    */
+#define DQ_ERR_DECODE (-7)         /* circuit JSON left to the full decoder   */
 
 /* ---- instruction IR ------------------------------------------------------
  * One dq_inst per `Instruction` variant of the reference IR
@@ -115,6 +116,30 @@ typedef struct dq_cond {             /* `Condition` (src/types.rs:54-58)    */
   uint64_t creg_value;
 } dq_cond;
 
+/* ---- circuit JSON decoding ------------------------------------------------
+ * Replaces the serde decoding of `circuit.model_dump_json()` into the
+ * reference's `Circuit` (src/types.rs:8-135, called from
+ * statevector/simulator.rs:327-329) together with the host encoding into
+ * dq_inst / dq_cond records.  dq_circuit_decode takes the well-formed case;
+ * it returns DQ_ERR_DECODE for invalid JSON, a shape serde rejects, an encoder
+ * limit (qubit index >= 2^31, classical space > 2^26 bits, conditions wider
+ * than 64 bits, a two-qubit remote gate without two qubits) and a few rare
+ * legal forms (duplicate keys, lone surrogate escapes, non-ASCII gate names,
+ * numbers that under- or overflow), so that the caller's full decoder reports
+ * the exact error or result.  On DQ_OK, dq_circuit_export copies out
+ * info->ninst records, info->ncond conditions and info->names_bytes bytes of
+ * generic gate names ((uint64 instruction index, uint64 length, bytes)
+ * records, names lower-cased); dq_circuit_free releases the object. */
+typedef struct dq_circuit dq_circuit;
+typedef struct dq_circuit_info {
+  uint64_t ninst;
+  uint64_t ncond;
+  uint64_t num_qubits;   /* max(base + size) over qregs (types.rs:24-31)     */
+  uint64_t num_cbits;    /* max(base + size) over cregs (types.rs:33-38)     */
+  uint64_t cbit_space;   /* classical bits the run needs (>= 1, <= 2^26)     */
+  uint64_t names_bytes;
+} dq_circuit_info;
+
 /* ---- options and profile ------------------------------------------------ */
 enum dq_semantics {
   DQ_SEM_SIMULATE = 0,  /* run_instruction (simulate):  circuit-* unsupported */
@@ -156,6 +181,11 @@ typedef struct dq_state_s* dq_state_t;
 DQ_API int dq_abi_version(void);
 DQ_API const char* dq_last_error(void);
 DQ_API int dq_device_count(int* count);
+
+DQ_API int dq_circuit_decode(const char* json, uint64_t len, dq_circuit** out,
+                             dq_circuit_info* info);
+DQ_API int dq_circuit_export(const dq_circuit* c, dq_inst* insts, dq_cond* conds, uint8_t* names);
+DQ_API void dq_circuit_free(dq_circuit* c);
 
 /* ---- state lifecycle ----------------------------------------------------
  * Replaces `vec![C::new(0.0, 0.0); 1 << n]; state[0] = 1`
