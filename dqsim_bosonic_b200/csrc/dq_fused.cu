@@ -775,12 +775,15 @@ int encode_sweep(const PSweep& sw_in, const std::vector<PGate>& G, uint32_t TBn,
   if (m < run_bits || sw.local[run_bits - 1] != run_bits - 1)
     return fail(DQ_ERR_INTERNAL, "sweep local set lacks the pinned low qubits");
   h.run_bits = run_bits;
-  for (uint32_t r = 0; r < (1u << (m - run_bits)); ++r) {
+  const uint32_t nruns = 1u << (m - run_bits);
+  std::vector<uint64_t> runoff(nruns);
+  std::vector<uint32_t> runswz(nruns);
+  for (uint32_t r = 0; r < nruns; ++r) {
     uint64_t off = 0;
     for (uint32_t b = 0; b + run_bits < m; ++b)
       if ((r >> b) & 1u) off |= 1ULL << sw.local[run_bits + b];
-    h.runoff[r] = off;
-    h.runswz[r] = swz(r << run_bits);
+    runoff[r] = off;
+    runswz[r] = swz(r << run_bits);
   }
   h.nphase = (uint32_t)P.size();
   h.nslots = (uint32_t)SL.size();
@@ -792,7 +795,11 @@ int encode_sweep(const PSweep& sw_in, const std::vector<PGate>& G, uint32_t TBn,
   const size_t so = SL.empty() ? blob.align16() : blob.put(SL.data(), SL.size());
   const size_t eo = SE.empty() ? blob.align16() : blob.put(SE.data(), SE.size());
   const size_t dd = D.empty() ? blob.align16() : blob.put(D.data(), D.size());
+  const size_t ro = blob.put(runoff.data(), runoff.size());
+  const size_t rs = blob.put(runswz.data(), runswz.size());
   SwHeader* hp = reinterpret_cast<SwHeader*>(blob.buf.data() + hoff);
+  hp->off_runoff = (uint32_t)(ro - hoff);
+  hp->off_runswz = (uint32_t)(rs - hoff);
   hp->off_phase = (uint32_t)(po - hoff);
   hp->off_op = (uint32_t)(oo - hoff);
   hp->off_slot = (uint32_t)(so - hoff);

@@ -63,8 +63,10 @@ struct SwHeader {
   uint32_t off_data, prog_bytes;
   uint32_t tile_xload;         // XORed into every tile-load address: X gates opening the sweep
   uint32_t run_bits;           // 5 or 3
-  uint64_t runoff[kMaxRuns];   // physical offset of run r (local bits run_bits..m-1 = r)
-  uint32_t runswz[kMaxRuns];   // swizzled shared-memory index of run r's first element
+  // 2^(m - run_bits) entries each, stored after the header:
+  uint32_t off_runoff;         // u64 physical offset of run r (local bits run_bits..m-1 = r)
+  uint32_t off_runswz;         // u32 swizzled shared-memory index of run r's first element
+  uint32_t pad0, pad1;
 };
 struct SwPhase {
   uint32_t lanesw[32];         // swizzled local index of the lane bits (thread bits 0..4)
@@ -322,6 +324,8 @@ __device__ __forceinline__ void sweep_tiles(double2* __restrict__ state, const u
   const SwSlot* SL = reinterpret_cast<const SwSlot*>(prog + H->off_slot);
   const SwSlotEnt* SE = reinterpret_cast<const SwSlotEnt*>(prog + H->off_slotent);
   const double2* DATA = reinterpret_cast<const double2*>(prog + H->off_data);
+  const uint64_t* RUNOFF = reinterpret_cast<const uint64_t*>(prog + H->off_runoff);
+  const uint32_t* RUNSWZ = reinterpret_cast<const uint32_t*>(prog + H->off_runswz);
   const uint32_t nph = H->nphase, nslots = H->nslots;
   // element e = 32 c + lane of a tile (c: the warp's chunk) lies in run
   // e >> run_bits at offset e & (2^run_bits - 1)
@@ -357,8 +361,8 @@ __device__ __forceinline__ void sweep_tiles(double2* __restrict__ state, const u
 #pragma unroll
       for (int i = 0; i < NI; ++i) {
         const uint32_t r = ((warp + (uint32_t)i * NW) << cshift) + lane_run;
-        const uint64_t g = b + H->runoff[r] + lane_off;
-        double2* d = &dst[H->runswz[r] ^ swl ^ H->tile_xload];
+        const uint64_t g = b + RUNOFF[r] + lane_off;
+        double2* d = &dst[RUNSWZ[r] ^ swl ^ H->tile_xload];
         if (synth >= 0)
           *d = make_double2(g == (uint64_t)synth ? 1.0 : 0.0, 0.0);
         else
@@ -386,7 +390,7 @@ __device__ __forceinline__ void sweep_tiles(double2* __restrict__ state, const u
 #pragma unroll
       for (int i = 0; i < NI; ++i) {
         const uint32_t r = ((warp + (uint32_t)i * NW) << cshift) + lane_run;
-        state[base + H->runoff[r] + lane_off] = make_double2(0.0, 0.0);
+        state[base + RUNOFF[r] + lane_off] = make_double2(0.0, 0.0);
       }
       base = advance(base);
       continue;
@@ -476,7 +480,7 @@ __device__ __forceinline__ void sweep_tiles(double2* __restrict__ state, const u
 #pragma unroll
     for (int i = 0; i < NI; ++i) {
       const uint32_t r = ((warp + (uint32_t)i * NW) << cshift) + lane_run;
-      state[base + H->runoff[r] + lane_off] = cur[H->runswz[r] ^ swl];
+      state[base + RUNOFF[r] + lane_off] = cur[RUNSWZ[r] ^ swl];
     }
     base = advance(base);
     __syncthreads();

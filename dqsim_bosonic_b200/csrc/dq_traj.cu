@@ -45,6 +45,9 @@ namespace dq {
 namespace {
 
 constexpr uint32_t kLocalBitsMax = 13;  // 8192 amplitudes = 128 KiB per CTA
+// Tile bits of the fused sweeps that HBM-resident batch items run (2^12
+// amplitudes: 8 thread bits of the 256-thread CTA and 4 register bits).
+constexpr int kHbmTileBits = 12;
 constexpr uint32_t kTrajMaxQubits = 16;
 constexpr uint32_t kTrajMaxCbits = 1024;
 
@@ -201,7 +204,7 @@ __global__ void __launch_bounds__(THREADS) k_traj(const TrajParams P) {
       // buffers (the next tile loads while the current one is computed).
       if constexpr (THREADS == 256) {
         double2* bufs = reinterpret_cast<double2*>(smraw);
-        double2* slots = bufs + 2 * (1u << 11);
+        double2* slots = bufs + 2 * (1u << kHbmTileBits);
         uint8_t* sprog = reinterpret_cast<uint8_t*>(slots + kMaxSlots);
         if (pg.nsweeps == 0) {  // nothing but a basis state to write
           const uint64_t len = 1ULL << pg.n;
@@ -216,9 +219,9 @@ __global__ void __launch_bounds__(THREADS) k_traj(const TrajParams P) {
                 __ldg(reinterpret_cast<const uint4*>(P.sweep_blob + sw.off + i));
           __syncthreads();
           if (sw.run_bits == 3)
-            sweep_tiles<8, 3, 2, 3>(pg.hbm, sprog, sw.ntiles, sy, bufs, slots, rank, C);
+            sweep_tiles<8, kHbmTileBits - 8, 2, 3>(pg.hbm, sprog, sw.ntiles, sy, bufs, slots, rank, C);
           else
-            sweep_tiles<8, 3, 2, 5>(pg.hbm, sprog, sw.ntiles, sy, bufs, slots, rank, C);
+            sweep_tiles<8, kHbmTileBits - 8, 2, 5>(pg.hbm, sprog, sw.ntiles, sy, bufs, slots, rank, C);
           __threadfence();
           cl.sync();
         }
@@ -804,14 +807,16 @@ struct LaunchSet {
   std::vector<TSweep> sweeps;
   uint32_t C = 1;
   uint32_t max_lb = 1, max_ncbits = 0;
+  size_t hbm_smem = 0;           // shared memory the HBM items' sweeps need
 };
 
 // Largest batch item that runs as HBM-resident fused sweeps inside the
 // persistent launch (2^30 amplitudes = 16 GiB).
 constexpr uint32_t kHbmItemMaxQubits = 30;
 // Sweep geometry of HBM items: 8 thread bits (the 256-thread trajectory
-// CTA), 3 register bits, tiles of 2^11 amplitudes.
-constexpr uint32_t kHbmTB = 8, kHbmM = 11;
+// CTA), 4 register bits, tiles of 2^12 amplitudes (two tile buffers, the
+// slot factors and the staged program fit one CTA's shared memory).
+constexpr uint32_t kHbmTB = 8, kHbmM = kHbmTileBits;
 
 // A unitary batch item planned as fused sweeps for the HBM path of k_traj.
 struct HbmPlan {
@@ -849,16 +854,19 @@ void add_hbm_program(LaunchSet& ls, const HbmPlan& pl, uint32_t n, uint64_t cbit
   ls.blob.insert(ls.blob.end(), pl.blob.begin(), pl.blob.end());
   TProg pg{};
   pg.n = n;
-  pg.lb = 13;  // the launch's shared memory holds the tile, the slot factors and the program
+  pg.lb = 13;  // reported local bits; the HBM branch sizes its shared memory by hbm_smem
   pg.ncbits = ncbits;
   pg.cbits_off = cbits_off;
   pg.hbm = hbm;
   pg.sweep_first = (uint32_t)ls.sweeps.size();
   pg.nsweeps = (uint32_t)pl.offs.size();
   pg.synth = (long long)pl.synth;
-  for (uint64_t off : pl.offs)
+  for (uint64_t off : pl.offs) {
+    const uint32_t pb = sweep_prog_bytes(pl.blob.data() + off);
     ls.sweeps.push_back(TSweep{base + off, 1u << (n - kHbmM), sweep_run_bits(pl.blob.data() + off),
-                               sweep_prog_bytes(pl.blob.data() + off), 0});
+                               pb, 0});
+    ls.hbm_smem = std::max<size_t>(ls.hbm_smem, sizeof(double2) * (2 * (1u << kHbmM) + kMaxSlots) + pb);
+  }
   ls.progs.push_back(pg);
   ls.max_lb = std::max(ls.max_lb, pg.lb);
   ls.max_ncbits = std::max(ls.max_ncbits, ncbits);
@@ -947,8 +955,8 @@ int launch_traj(TrajLaunch& L, const TrajParams& P, cudaStream_t st) {
 }
 
 size_t traj_smem(const LaunchSet& ls) {
-  return sizeof(double2) * (1u << ls.max_lb) + sizeof(double) * 48 +
-         sizeof(int32_t) * std::max<uint32_t>(ls.max_ncbits, 1);
+  return std::max<size_t>(ls.hbm_smem, sizeof(double2) * (1u << ls.max_lb) + sizeof(double) * 48 +
+                                           sizeof(int32_t) * std::max<uint32_t>(ls.max_ncbits, 1));
 }
 
 // Device buffers of one launch, freed on scope exit.

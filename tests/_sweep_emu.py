@@ -19,7 +19,7 @@ from dqsim_bosonic_b200 import _native as nat
 
 OP_U1, OP_U1R, OP_U1X, OP_U2, OP_FLUSH_R, OP_FLUSH_T, OP_GPHASE, OP_U1H, OP_SCALE = range(9)
 FL_THR, FL_REG, FL_PRE = 1, 2, 4
-MAXM, MAXRUNS = 12, 512
+MAXM = 12
 SWZ_G = {3: 3, 4: 5, 5: 6, 6: 7, 7: 3, 8: 5, 9: 6, 10: 7, 11: 1}
 
 
@@ -67,8 +67,9 @@ def run_sweep(state: np.ndarray, n: int, blob: bytes) -> None:
         struct.unpack_from("<8I", blob, 64)
     nruns = 1 << (m - run_bits)
     run_len = 1 << run_bits
-    runoff = np.array(struct.unpack_from(f"<{MAXRUNS}Q", blob, 96)[:nruns], dtype=np.uint64)
-    runswz = np.array(struct.unpack_from(f"<{MAXRUNS}I", blob, 96 + 8 * MAXRUNS)[:nruns], dtype=np.int64)
+    off_runoff, off_runswz = struct.unpack_from("<2I", blob, 96)
+    runoff = np.array(struct.unpack_from(f"<{nruns}Q", blob, off_runoff), dtype=np.uint64)
+    runswz = np.array(struct.unpack_from(f"<{nruns}I", blob, off_runswz), dtype=np.int64)
     T, R = 1 << m, 1 << rb
     TB = m - rb
     THREADS = 1 << TB
