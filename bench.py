@@ -335,6 +335,33 @@ def run_reference_arm(args, wl_prog, cfg):
 
 # ---- our arm ------------------------------------------------------------------------------------------
 
+def profile_case(spec: str) -> None:
+    """One small case of one kernel (no JSON line): the command a profiler wraps."""
+    kind, *rest = spec.split(":")
+    if kind == "ragged":
+        from dqsim_bosonic_b200.batch import run_batch
+        from dqsim_bosonic_b200.circuit import decode_program
+
+        n, count = int(rest[0]), int(rest[1])
+        circs = _circuits.ragged_batch(1024, 99)
+        progs = [decode_program(c.model_dump_json()) for c in circs]
+        idx = [k for k, p in enumerate(progs) if p.num_qubits == n][:count]
+        for _ in range(2):
+            _, _, st = run_batch([progs[k] for k in idx], [99 + k for k in idx], 0)
+        print(f"ragged n={n} items={len(idx)} kernel_ms={st.kernel_ms:.3f} launches={st.launches}")
+    elif kind == "adjoint":
+        from dqsim_bosonic_b200.adjoint import adjoint_gradient
+
+        n = int(rest[0])
+        c, theta, H = _circuits.hea_param_circuit(n, 16, seed=1)
+        for _ in range(2):
+            tm = {}
+            adjoint_gradient(c, theta, H, device=0, timing=tm)
+        print(f"adjoint n={n} " + " ".join(f"{k}={v}" for k, v in tm.items()))
+    else:
+        raise SystemExit(f"unknown profile case {spec!r}")
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -352,7 +379,15 @@ def main():
                     help="qubits of the merged block in the p-block merge section (even split)")
     ap.add_argument("--no-adjoint31", action="store_true",
                     help="skip the 31-qubit adjoint pass with its finite-difference check")
+    ap.add_argument("--profile-case", default=None,
+                    help="run one small case of one kernel for a profiler and exit: "
+                         "ragged:<n>:<items> (run_batch over the first <items> items of <n> "
+                         "qubits of the 1024-circuit ragged set, twice) or adjoint:<n> "
+                         "(two adjoint gradients of the 16-layer ansatz on <n> qubits)")
     args = ap.parse_args()
+    if args.profile_case:
+        profile_case(args.profile_case)
+        return
 
     from dqsim_bosonic_b200.circuit import decode_circuit_json, encode
 

@@ -20,6 +20,8 @@
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdint.h>
+#include <stdio.h>
+#include <stdlib.h>
 
 #include <algorithm>
 #include <chrono>
@@ -678,6 +680,19 @@ int dq_adjoint_batch(int device, uint32_t n, const dq_inst* prog, uint64_t ninst
   if (device < 0 || device >= ndev) return fail(DQ_ERR_INVALID_ARG, "device index out of range");
   DeviceGuard g(device);
   const auto t0 = std::chrono::steady_clock::now();
+  // DQSIM_ADJOINT_TIMING=1: host phase times on stderr
+  static const bool timing = [] {
+    const char* e = getenv("DQSIM_ADJOINT_TIMING");
+    return e && atoi(e) != 0;
+  }();
+  auto tlast = t0;
+  auto mark = [&](const char* what) {
+    if (!timing) return;
+    const auto now = std::chrono::steady_clock::now();
+    fprintf(stderr, "[dq_adjoint_batch] %-18s %8.3f ms\n", what,
+            std::chrono::duration<double, std::milli>(now - tlast).count());
+    tlast = now;
+  };
   // each set's program: the parameter slots replaced by its values
   std::vector<std::vector<dq_inst>> progs(nsets);
   for (uint64_t s = 0; s < nsets; ++s) {
@@ -728,6 +743,7 @@ int dq_adjoint_batch(int device, uint32_t n, const dq_inst* prog, uint64_t ninst
     clear_error();
   }
   acc.plan_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  mark("programs+plan");
   if (!batched) {
     // set by set through dq_adjoint on one engine state
     dq_state_t h = nullptr;
@@ -775,18 +791,37 @@ int dq_adjoint_batch(int device, uint32_t n, const dq_inst* prog, uint64_t ninst
   SweepJob* d_jobs = nullptr;
   const unsigned pblocks = reduction_blocks(len, device);
   const uint64_t sl = nslots + 1;  // per set: gradient slots, then E
-  // all forward programs in one device buffer
-  std::vector<uint8_t> fall;
+  // all forward programs in one device buffer, staged in pinned host memory
+  // (recycled across calls) by host threads
   std::vector<uint64_t> fbase(nsets, 0);
-  size_t kf = 0, kb = 0;
+  size_t fall_bytes = 0, kf = 0, kb = 0;
   for (uint64_t s = 0; s < nsets; ++s) {
-    while (fall.size() % 16) fall.push_back(0);
-    fbase[s] = fall.size();
-    fall.insert(fall.end(), plans[s].fblob.begin(), plans[s].fblob.end());
+    fbase[s] = fall_bytes;
+    fall_bytes += (plans[s].fblob.size() + 15) / 16 * 16;
     kf = std::max(kf, plans[s].foffs.size());
     kb = std::max(kb, plans[s].back.sweeps());
   }
-  if (fall.empty()) fall.push_back(0);
+  fall_bytes = std::max<size_t>(fall_bytes, 16);
+  struct PinnedStage {
+    size_t bytes = 0;
+    void* p = nullptr;
+    ~PinnedStage() { pinned_free(bytes, p); }
+  } fall;
+  if (rc == DQ_OK) rc = pinned_alloc(fall_bytes, &fall.p);
+  if (rc == DQ_OK) {
+    fall.bytes = fall_bytes;
+    uint8_t* dst = static_cast<uint8_t*>(fall.p);
+    const unsigned hw = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    const unsigned nt = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(hw, nsets / 8 + 1));
+    auto work = [&](unsigned t) {
+      for (uint64_t s = t; s < nsets; s += nt)
+        if (!plans[s].fblob.empty()) memcpy(dst + fbase[s], plans[s].fblob.data(), plans[s].fblob.size());
+    };
+    std::vector<std::thread> th;
+    for (unsigned t = 1; t < nt; ++t) th.emplace_back(work, t);
+    work(0);
+    for (auto& x : th) x.join();
+  }
   acc.forward_sweeps = kf;
   acc.backward_sweeps = kb;
   if (rc == DQ_OK) {
@@ -798,19 +833,24 @@ int dq_adjoint_batch(int device, uint32_t n, const dq_inst* prog, uint64_t ninst
     if (rc == DQ_OK) rc = cache_alloc(device, sizeof(double2) * len * G, &lv);
     psi = (double2*)pv;
     lam = (double2*)lv;
-    cu(cudaMalloc((void**)&slots, sizeof(double) * sl * G), "cudaMalloc(slots)");
-    cu(cudaMalloc((void**)&part, sizeof(double) * pblocks * G), "cudaMalloc(partials)");
-    cu(cudaMalloc((void**)&ctr, sizeof(unsigned) * G), "cudaMalloc(counters)");
-    cu(cudaMalloc((void**)&fblob, fall.size()), "cudaMalloc(programs)");
-    cu(cudaMalloc((void**)&d_jobs, sizeof(SweepJob) * std::max<size_t>(1, kf * G)), "cudaMalloc(jobs)");
+    // the small buffers also from the cache: an optimiser loop repeats their sizes
+    void* p = nullptr;
+    if (rc == DQ_OK && (rc = cache_alloc(device, sizeof(double) * sl * G, &p)) == DQ_OK) slots = (double*)p;
+    if (rc == DQ_OK && (rc = cache_alloc(device, sizeof(double) * pblocks * G, &p)) == DQ_OK) part = (double*)p;
+    if (rc == DQ_OK && (rc = cache_alloc(device, sizeof(unsigned) * G, &p)) == DQ_OK) ctr = (unsigned*)p;
+    if (rc == DQ_OK && (rc = cache_alloc(device, fall_bytes, &p)) == DQ_OK) fblob = (uint8_t*)p;
+    if (rc == DQ_OK &&
+        (rc = cache_alloc(device, sizeof(SweepJob) * std::max<size_t>(1, kf * G), &p)) == DQ_OK)
+      d_jobs = (SweepJob*)p;
   }
   if (rc == DQ_OK) {
-    cu(cudaMemcpyAsync(fblob, fall.data(), fall.size(), cudaMemcpyHostToDevice, st), "copy programs");
+    cu(cudaMemcpyAsync(fblob, fall.p, fall_bytes, cudaMemcpyHostToDevice, st), "copy programs");
     cu(cudaMemsetAsync(ctr, 0, sizeof(unsigned) * G, st), "memset");
   }
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
   for (auto& e : ev) cu(cudaEventCreate(&e), "cudaEventCreate");
   std::vector<double> host(sl * G);
+  mark("setup");
   for (uint64_t g0 = 0; g0 < nsets && rc == DQ_OK; g0 += G) {
     const uint64_t g1 = std::min(nsets, g0 + G), ng = g1 - g0;
     ++acc.groups;
@@ -854,6 +894,7 @@ int dq_adjoint_batch(int device, uint32_t n, const dq_inst* prog, uint64_t ninst
       acc.launches += extra;
     }
     cu(cudaEventRecord(ev[1], st), "event");
+    mark("forward enqueue");
     // lambda = H psi and E for every set of the group
     if (rc == DQ_OK) {
       k_pauli_multi<<<dim3(pblocks, (unsigned)ng), kRedThreads, 0, st>>>(
@@ -875,14 +916,17 @@ int dq_adjoint_batch(int device, uint32_t n, const dq_inst* prog, uint64_t ninst
       bs.reserve(ng);
       for (uint64_t s = g0; s < g1; ++s) bs.push_back(std::move(plans[s].back));
       uint64_t nl = 0;
+      mark("observable enqueue");
       rc = adjoint_backward_batch(pp.data(), lp.data(), bs, sp.data(), st, device, &nl);
       acc.launches += nl;
+      mark("backward (host)");
     }
     cu(cudaEventRecord(ev[3], st), "event");
     if (rc == DQ_OK)
       cu(cudaMemcpyAsync(host.data(), slots, sizeof(double) * sl * ng, cudaMemcpyDeviceToHost, st),
          "copy slots");
     cu(cudaStreamSynchronize(st), "sync");
+    mark("sync");
     if (rc == DQ_OK) {
       float a = 0.f, b = 0.f, c = 0.f;
       cudaEventElapsedTime(&a, ev[0], ev[1]);
@@ -914,12 +958,13 @@ int dq_adjoint_batch(int device, uint32_t n, const dq_inst* prog, uint64_t ninst
   cudaStreamSynchronize(st);
   if (psi) cache_free(device, sizeof(double2) * len * G, psi);
   if (lam) cache_free(device, sizeof(double2) * len * G, lam);
-  if (slots) cudaFree(slots);
-  if (part) cudaFree(part);
-  if (ctr) cudaFree(ctr);
-  if (fblob) cudaFree(fblob);
-  if (d_jobs) cudaFree(d_jobs);
+  if (slots) cache_free(device, sizeof(double) * sl * G, slots);
+  if (part) cache_free(device, sizeof(double) * pblocks * G, part);
+  if (ctr) cache_free(device, sizeof(unsigned) * G, ctr);
+  if (fblob) cache_free(device, fall_bytes, fblob);
+  if (d_jobs) cache_free(device, sizeof(SweepJob) * std::max<size_t>(1, kf * G), d_jobs);
   cudaStreamDestroy(st);
+  mark("gradients+finish");
   acc.batched = 1;
   if (stats) *stats = acc;
   return rc;

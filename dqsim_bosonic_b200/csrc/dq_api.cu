@@ -81,6 +81,51 @@ void cache_free(int device, size_t bytes, void* p) {
   }
 }
 
+// Pinned host staging buffers, kept by size class (a power of two of at
+// least 1 MiB) so that repeated large uploads neither page-fault fresh host
+// memory nor pay cudaHostAlloc.
+std::mutex g_pinned_mu;
+std::map<size_t, std::vector<void*>> g_pinned;
+
+size_t pinned_class(size_t bytes) {
+  size_t c = 1ULL << 20;
+  while (c < bytes) c <<= 1;
+  return c;
+}
+
+int pinned_alloc(size_t bytes, void** out) {
+  const size_t c = pinned_class(bytes);
+  {
+    std::lock_guard<std::mutex> lk(g_pinned_mu);
+    auto it = g_pinned.find(c);
+    if (it != g_pinned.end() && !it->second.empty()) {
+      *out = it->second.back();
+      it->second.pop_back();
+      return DQ_OK;
+    }
+  }
+  cudaError_t e = cudaHostAlloc(out, c, cudaHostAllocDefault);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    *out = nullptr;
+    return fail(DQ_ERR_OOM, std::string("cudaHostAlloc(") + std::to_string(c) + " B): " +
+                                cudaGetErrorString(e));
+  }
+  return DQ_OK;
+}
+
+void pinned_free(size_t bytes, void* p) {
+  if (!p) return;
+  const size_t c = pinned_class(bytes);
+  std::lock_guard<std::mutex> lk(g_pinned_mu);
+  auto& v = g_pinned[c];
+  if (v.size() < kMaxCachedPerKey) {
+    v.push_back(p);
+  } else {
+    cudaFreeHost(p);
+  }
+}
+
 }  // namespace dq
 
 

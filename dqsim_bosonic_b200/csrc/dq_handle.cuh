@@ -56,6 +56,9 @@ struct DeviceGuard {
 // Device buffers of state size are recycled through a per-(device, size) cache.
 int cache_alloc(int device, size_t bytes, void** out);
 void cache_free(int device, size_t bytes, void* p);
+// Pinned host staging buffers (at least `bytes`), recycled by size class.
+int pinned_alloc(size_t bytes, void** out);
+void pinned_free(size_t bytes, void* p);
 
 int check_handle(dq_state_t h);            // validates and materialises a lazy basis state
 int check_handle_lazy(dq_state_t h);       // validates only

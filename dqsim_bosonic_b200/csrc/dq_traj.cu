@@ -24,6 +24,8 @@
 #include <math.h>
 #include <stdint.h>
 
+#include <stdio.h>
+#include <stdlib.h>
 #include <string.h>
 
 #include <algorithm>
@@ -804,6 +806,9 @@ struct LaunchSet {
   std::vector<TProg> progs;
   std::vector<TItem> items;
   std::vector<uint8_t> blob;     // sweep programs of the HBM items
+  // or, when set, the sweep programs staged in pinned host memory
+  const uint8_t* blob_host = nullptr;
+  size_t blob_host_bytes = 0;
   std::vector<TSweep> sweeps;
   uint32_t C = 1;
   uint32_t max_lb = 1, max_ncbits = 0;
@@ -846,12 +851,10 @@ bool plan_hbm_item(const dq_batch_item& it, HbmPlan* out) {
   return true;
 }
 
-// Adds a planned HBM item whose state lives at `hbm` (device, 2^n amplitudes).
-void add_hbm_program(LaunchSet& ls, const HbmPlan& pl, uint32_t n, uint64_t cbits_off,
-                     uint32_t ncbits, double2* hbm) {
-  while (ls.blob.size() % 16) ls.blob.push_back(0);
-  const uint64_t base = ls.blob.size();
-  ls.blob.insert(ls.blob.end(), pl.blob.begin(), pl.blob.end());
+// Adds a planned HBM item whose state lives at `hbm` (device, 2^n amplitudes)
+// and whose sweep programs sit at byte `base` of the set's program blob.
+void add_hbm_program(LaunchSet& ls, const HbmPlan& pl, uint64_t base, uint32_t n,
+                     uint64_t cbits_off, uint32_t ncbits, double2* hbm) {
   TProg pg{};
   pg.n = n;
   pg.lb = 13;  // reported local bits; the HBM branch sizes its shared memory by hbm_smem
@@ -870,6 +873,63 @@ void add_hbm_program(LaunchSet& ls, const HbmPlan& pl, uint32_t n, uint64_t cbit
   ls.progs.push_back(pg);
   ls.max_lb = std::max(ls.max_lb, pg.lb);
   ls.max_ncbits = std::max(ls.max_ncbits, ncbits);
+}
+
+// Op types whose `mat` indexes the matrix pool (push_mat in encode_gateop).
+bool op_uses_pool(uint8_t type) {
+  return type == T_ONEQ || type == T_PHASE || type == T_DIAG || type == T_DENSE;
+}
+
+// One program's ops and matrices, encoded on its own (matrix offsets into
+// its own pool, condition offsets from 0) so that programs can be encoded
+// on several host threads and appended to a launch set afterwards.
+struct ProgCode {
+  std::vector<TOp> ops;
+  std::vector<double2> pool;
+  int rc = DQ_OK;
+  std::string err;
+};
+
+void encode_prog_code(const dq_inst* prog, uint64_t ninst, uint32_t n, uint32_t lb, ProgCode& out) {
+  Encoded e;
+  out.rc = encode_program(prog, ninst, n, 0, e);
+  if (out.rc != DQ_OK) {
+    out.err = dq_last_error();
+    return;
+  }
+  mark_remote(e.ops.data(), e.ops.size(), lb);
+  out.ops = group_phases(e.ops, lb);
+  out.pool = std::move(e.pool);
+}
+
+// Appends a program encoded by encode_prog_code: the same records add_program
+// would write (matrix and condition offsets moved to the set's pools).
+int add_prog_code(LaunchSet& ls, const ProgCode& pc, const dq_cond* conds, uint64_t nconds,
+                  uint32_t n, uint32_t lb, uint64_t base_seed, uint64_t cbits_off, uint32_t ncbits,
+                  double2* state_out) {
+  if (pc.rc != DQ_OK) return fail(pc.rc, pc.err);
+  TProg pg{};
+  pg.ops_off = (uint32_t)ls.enc.ops.size();
+  const uint32_t pool_base = (uint32_t)ls.enc.pool.size();
+  const uint32_t cond_base = (uint32_t)ls.conds.size();
+  for (uint64_t c = 0; c < nconds; ++c) ls.conds.push_back(conds[c]);
+  ls.enc.pool.insert(ls.enc.pool.end(), pc.pool.begin(), pc.pool.end());
+  for (TOp t : pc.ops) {
+    if (op_uses_pool(t.type)) t.mat += pool_base;
+    if (t.cond_count) t.cond_first += cond_base;
+    ls.enc.ops.push_back(t);
+  }
+  pg.nops = (uint32_t)pc.ops.size();
+  pg.n = n;
+  pg.lb = lb;
+  pg.ncbits = ncbits;
+  pg.base_seed = base_seed;
+  pg.cbits_off = cbits_off;
+  pg.state_out = state_out;
+  ls.progs.push_back(pg);
+  ls.max_lb = std::max(ls.max_lb, lb);
+  ls.max_ncbits = std::max(ls.max_ncbits, ncbits);
+  return DQ_OK;
 }
 
 int add_program(LaunchSet& ls, const dq_inst* prog, uint64_t ninst, const dq_cond* conds,
@@ -1009,7 +1069,12 @@ int run_launch(LaunchSet& ls, int threads, int device, cudaStream_t st, int32_t*
   DQ_TRY(upload(&b.conds, ls.conds, st));
   DQ_TRY(upload(&b.progs, ls.progs, st));
   DQ_TRY(upload(&b.items, ls.items, st));
-  DQ_TRY(upload(&b.blob, ls.blob, st));
+  if (ls.blob_host) {
+    DQ_CUDA_TRY(cudaMalloc((void**)&b.blob, std::max<size_t>(ls.blob_host_bytes, 16)));
+    DQ_CUDA_TRY(cudaMemcpyAsync(b.blob, ls.blob_host, ls.blob_host_bytes, cudaMemcpyHostToDevice, st));
+  } else {
+    DQ_TRY(upload(&b.blob, ls.blob, st));
+  }
   DQ_TRY(upload(&b.sweeps, ls.sweeps, st));
   DQ_CUDA_TRY(cudaMalloc((void**)&b.ctr, 3 * sizeof(unsigned long long)));
   const unsigned long long init[3] = {0ULL, 0ULL, 0x7fffffffffffffffULL};
@@ -1201,6 +1266,19 @@ int dq_run_batch(int device, const dq_batch_item* items, uint64_t nitems,
   }
   DeviceGuard g(device);
   const auto t0 = std::chrono::steady_clock::now();
+  // DQSIM_BATCH_TIMING=1: host phase times on stderr
+  static const bool timing = [] {
+    const char* e = getenv("DQSIM_BATCH_TIMING");
+    return e && atoi(e) != 0;
+  }();
+  auto tlast = t0;
+  auto mark = [&](const char* what) {
+    if (!timing) return;
+    const auto now = std::chrono::steady_clock::now();
+    fprintf(stderr, "[dq_run_batch] %-14s %8.3f ms\n", what,
+            std::chrono::duration<double, std::milli>(now - tlast).count());
+    tlast = now;
+  };
   // One persistent launch takes every item it can: states of up to 16 qubits
   // live in a cluster's shared memory; unitary items of 17..30 qubits keep
   // their state in HBM and run as fused tile sweeps by one cluster each.
@@ -1241,6 +1319,7 @@ int dq_run_batch(int device, const dq_batch_item* items, uint64_t nitems,
       }
     }
   }
+  mark("plan large");
   uint32_t Cmain = hbm_items.empty() ? 1u : std::min<uint32_t>(8u, max_span);
   for (uint64_t k : resident) {
     uint32_t lb, C;
@@ -1294,7 +1373,62 @@ int dq_run_batch(int device, const dq_batch_item* items, uint64_t nitems,
       outs[c].push_back(o);
     }
   }
+  // encode the resident items on host threads (each into its own ops and
+  // matrix pool; appended to the launch sets in queue order below)
+  std::vector<ProgCode> codes(nitems);
+  {
+    std::vector<uint64_t> todo;
+    for (int c = 0; c < 5; ++c)
+      for (const Out& o : outs[c])
+        if (plan_of[o.item] < 0) todo.push_back(o.item);
+    const unsigned hw = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    const unsigned nt = (unsigned)std::max<size_t>(1, std::min<size_t>(hw, todo.size() / 8 + 1));
+    auto work = [&](unsigned t) {
+      for (size_t i = t; i < todo.size(); i += nt) {
+        const uint64_t k = todo[i];
+        encode_prog_code(items[k].prog, items[k].ninst, items[k].n, item_lb[k], codes[k]);
+      }
+    };
+    std::vector<std::thread> th;
+    for (unsigned t = 1; t < nt; ++t) th.emplace_back(work, t);
+    work(0);
+    for (auto& x : th) x.join();
+  }
+  // the HBM items' sweep programs, copied on host threads into one pinned
+  // staging buffer (recycled across calls) and uploaded with one copy
+  std::vector<uint64_t> hbm_blob_off(plans.size(), 0);
+  size_t hbm_blob_bytes = 0;
+  for (size_t h = 0; h < plans.size(); ++h) {
+    hbm_blob_off[h] = hbm_blob_bytes;
+    hbm_blob_bytes += (plans[h].blob.size() + 15) / 16 * 16;
+  }
+  // returned to the pool on every exit path; each set's copies are complete
+  // by then (run_launch synchronizes its stream, on errors too)
+  struct PinnedStage {
+    size_t bytes = 0;
+    void* p = nullptr;
+    ~PinnedStage() { pinned_free(bytes, p); }
+  } stage;
+  void* hbm_blob = nullptr;
+  if (hbm_blob_bytes) {
+    DQ_TRY(pinned_alloc(hbm_blob_bytes, &hbm_blob));
+    stage.bytes = hbm_blob_bytes;
+    stage.p = hbm_blob;
+    const unsigned hw = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    const unsigned nt = (unsigned)std::max<size_t>(1, std::min<size_t>(hw, plans.size() / 8 + 1));
+    auto work = [&](unsigned t) {
+      for (size_t h = t; h < plans.size(); h += nt)
+        memcpy(static_cast<uint8_t*>(hbm_blob) + hbm_blob_off[h], plans[h].blob.data(), plans[h].blob.size());
+    };
+    std::vector<std::thread> th;
+    for (unsigned t = 1; t < nt; ++t) th.emplace_back(work, t);
+    work(0);
+    for (auto& x : th) x.join();
+    sets[0].blob_host = static_cast<const uint8_t*>(hbm_blob);
+    sets[0].blob_host_bytes = hbm_blob_bytes;
+  }
   acc.prepare_ms = ms_since(t0);
+  mark("group+encode");
 
   cudaStream_t st = nullptr;
   DQ_CUDA_TRY(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
@@ -1322,16 +1456,21 @@ int dq_run_batch(int device, const dq_batch_item* items, uint64_t nitems,
       const uint32_t pi = (uint32_t)ls.progs.size();
       if (plan_of[o.item] >= 0) {
         const uint64_t h = (uint64_t)plan_of[o.item];
-        add_hbm_program(ls, plans[h], it.n, o.cbits_off, (uint32_t)it.ncbits, d_hbm + hbm_off[h]);
+        add_hbm_program(ls, plans[h], hbm_blob_off[h], it.n, o.cbits_off, (uint32_t)it.ncbits,
+                        d_hbm + hbm_off[h]);
       } else {
-        rc = add_program(ls, it.prog, it.ninst, it.conds, it.nconds, it.n, item_lb[o.item], it.seed,
-                         o.cbits_off, (uint32_t)it.ncbits,
-                         o.state_off == ~0ULL ? nullptr : d_states + o.state_off);
+        rc = add_prog_code(ls, codes[o.item], it.conds, it.nconds, it.n, item_lb[o.item], it.seed,
+                           o.cbits_off, (uint32_t)it.ncbits,
+                           o.state_off == ~0ULL ? nullptr : d_states + o.state_off);
       }
       ls.items.push_back(TItem{pi, 0, 0});
     }
     acc.prepare_ms += ms_since(tp);
+    mark("encode set");
+    const double k0 = acc.kernel_ms;
     if (rc == DQ_OK) rc = run_launch(ls, threads, device, st, d_cbits, &acc);
+    if (timing) fprintf(stderr, "[dq_run_batch] kernel         %8.3f ms\n", acc.kernel_ms - k0);
+    mark("launch set");
     for (const Out& o : outs[c]) {
       if (rc != DQ_OK) break;
       const dq_batch_item& it = items[o.item];
@@ -1359,6 +1498,7 @@ int dq_run_batch(int device, const dq_batch_item* items, uint64_t nitems,
     cudaStreamSynchronize(st);
     if (d_states) cudaFree(d_states);
     if (d_cbits) cudaFree(d_cbits);
+    mark("outputs");
     if (rc == DQ_OK && acc.failed_inst >= 0) {
       // map (program << 40 | instruction) back to the caller's item index
       const uint64_t pi = (uint64_t)acc.failed_inst >> 40;
@@ -1401,6 +1541,7 @@ int dq_run_batch(int device, const dq_batch_item* items, uint64_t nitems,
   }
   if (h) dq_state_destroy(h);
   cudaStreamDestroy(st);
+  mark("engine items");
   if (stats) *stats = acc;
   return rc;
 }
