@@ -731,6 +731,45 @@ int encode_sweep(const PSweep& sw_in, const std::vector<PGate>& G, uint32_t TBn,
         O.push_back(so);
       }
     }
+    // A phase made only of uncontrolled Hadamard-pattern ops on register bits
+    // 0, 1, ..., K-1 in that order (register bits are assigned in the order
+    // the phase's ops need them), optionally followed by the deferred scale,
+    // runs as straight-line code: an OP_HPHASE marker goes in front of them.
+    {
+      const size_t ob = sp.op_begin, oe = O.size();
+      size_t k = 0;
+      bool ok = oe > ob, sc = false;
+      for (size_t i = ob; i < oe && ok; ++i) {
+        const EncOp& x = O[i];
+        if (x.type == OP_SCALE && i + 1 == oe && i > ob) {
+          sc = true;
+          continue;
+        }
+        ok = x.type == OP_U1H && x.creg == 0 && x.ctl_thr == 0 && x.cnl == 0 && x.b0 == (uint32_t)k;
+        ++k;
+      }
+      if (ok && k >= 1 && k <= RB) {
+        for (size_t i = ob; i < ob + k; ++i) {
+          EncOp& x = O[i];
+          if (!(x.flags & FL_PRE) || !(x.flags & FL_REG)) continue;
+          // register-partner table entries equal to the entry of their low bits
+          const size_t f0 = x.data + 4 + ((x.flags & FL_THR) ? 40 : 0);
+          const uint32_t lowmask = (1u << x.b0) - 1u;
+          bool low = true;
+          for (uint32_t idx = 0; idx < (1u << (RB - 1)) && low; ++idx) {
+            const double2 u = D[f0 + idx], v = D[f0 + (idx & lowmask)];
+            low = u.x == v.x && u.y == v.y;
+          }
+          if (low) x.flags |= FL_LOWF;
+        }
+        EncOp hp{};
+        hp.type = OP_HPHASE;
+        hp.b1 = (uint32_t)k;
+        hp.flags = sc ? HPH_SCALE : 0u;
+        hp.data = sc ? O[oe - 1].data : 0u;
+        O.insert(O.begin() + (ptrdiff_t)ob, hp);
+      }
+    }
     sp.op_end = (uint32_t)O.size();
     sp.xload ^= carry_xload;
     carry_xload = 0;

@@ -34,7 +34,7 @@ constexpr int kMaxSlots = 128;
 __host__ __device__ constexpr int max_prog(int m) { return m >= 12 ? 64 * 1024 : 40 * 1024; }
 
 enum : uint32_t { OP_U1 = 0, OP_U1R, OP_U1X, OP_U2, OP_FLUSH_R, OP_FLUSH_T, OP_GPHASE, OP_U1H,
-                  OP_SCALE };
+                  OP_SCALE, OP_HPHASE };
 
 // swizzle vectors of local bits 3..11 (bits 0..2 map to themselves)
 __host__ __device__ constexpr uint32_t swz_g(int k) {
@@ -100,6 +100,14 @@ static_assert(sizeof(SwOp) % 16 == 0 && sizeof(SwSlot) % 16 == 0 && sizeof(SwSlo
 constexpr uint32_t FL_THR = 1u;
 constexpr uint32_t FL_REG = 2u;
 constexpr uint32_t FL_PRE = 4u;   // 1q op: flush its target first (data = 4 matrix entries, then flush tables)
+// U1H op inside an H phase: its register-partner table depends only on the
+// register bits below its target (entries 0 .. 2^b0 - 1 hold every value)
+constexpr uint32_t FL_LOWF = 8u;
+// OP_HPHASE marks a phase whose ops are K = b1 uncontrolled Hadamard-pattern
+// ops (OP_U1H) on register bits 0, 1, ..., K-1 in that order, optionally
+// followed by the deferred OP_SCALE (flags bit 0 set, data = the scale): the
+// kernel runs them as straight-line code instead of interpreting them.
+constexpr uint32_t HPH_SCALE = 1u;
 
 // ---- device helpers -------------------------------------------------------------------
 
@@ -233,6 +241,99 @@ __device__ __forceinline__ void u2_dispatch(double2 (&a)[1 << RB], uint32_t b0, 
   }
   DQ_U2C(0, 1) DQ_U2C(0, 2) DQ_U2C(0, 3) DQ_U2C(1, 2) DQ_U2C(1, 3) DQ_U2C(2, 3)
 #undef DQ_U2C
+}
+
+// ---- H phases: straight-line Hadamard-pattern ops ---------------------------------------
+// Op on register bit B: the upper amplitude y of each pair is multiplied by
+// its flush factor (PRE 1: W; PRE 2: W * F[idx], the W * F products formed
+// once per distinct F entry: 2^B of them when LOWF), then the butterfly
+// (x + y', x - y').  SC: the phase's deferred scale s folds into this op as
+// (s x + y', s x - y') with s already in W (PRE 0: y' = s y).
+template <int RB, int B, int PRE, bool LOWF, bool SC>
+__device__ __forceinline__ void hph_op(double2 (&a)[1 << RB], double2 W, const double2* __restrict__ F,
+                                       double s) {
+  constexpr int NF = (PRE == 2) ? (LOWF ? (1 << B) : (1 << (RB - 1))) : 1;
+  double2 WF[NF];
+  if (PRE == 2) {
+#pragma unroll
+    for (int i = 0; i < NF; ++i) WF[i] = cmul_f(W, F[i]);
+  }
+#pragma unroll
+  for (int j = 0; j < (1 << RB); ++j) {
+    if (j & (1 << B)) continue;
+    const int k = j | (1 << B);
+    const double2 x = a[j];
+    double2 y = a[k];
+    if (PRE == 2) {
+      const int idx = LOWF ? (k & ((1 << B) - 1)) : (((k >> (B + 1)) << B) | (k & ((1 << B) - 1)));
+      y = cmul_f(y, WF[idx]);
+    } else if (PRE == 1) {
+      y = cmul_f(y, W);
+    } else if (SC) {
+      y = make_double2(y.x * s, y.y * s);
+    }
+    if (SC) {
+      a[j] = make_double2(fma(x.x, s, y.x), fma(x.y, s, y.y));
+      a[k] = make_double2(fma(x.x, s, -y.x), fma(x.y, s, -y.y));
+    } else {
+      a[j] = make_double2(x.x + y.x, x.y + y.y);
+      a[k] = make_double2(x.x - y.x, x.y - y.y);
+    }
+  }
+}
+
+template <int RB, int B, bool SC>
+__device__ __forceinline__ void hph_flags(double2 (&a)[1 << RB], uint32_t fl, double2 W,
+                                          const double2* __restrict__ F, double s) {
+  if (!(fl & FL_PRE)) hph_op<RB, B, 0, false, SC>(a, W, F, s);
+  else if (!(fl & FL_REG)) hph_op<RB, B, 1, false, SC>(a, W, F, s);
+  else if (fl & FL_LOWF) hph_op<RB, B, 2, true, SC>(a, W, F, s);
+  else hph_op<RB, B, 2, false, SC>(a, W, F, s);
+}
+
+// sub-op I of K (register bit I), then the rest
+template <int RB, int K, int I>
+__device__ __forceinline__ void hph_run(double2 (&a)[1 << RB], const uint4* __restrict__ SUB,
+                                        const double2* __restrict__ DATA,
+                                        const double2* __restrict__ slots, uint32_t tid, double s,
+                                        bool sc) {
+  if constexpr (I < K) {
+    const uint4 o0 = SUB[2 * I];
+    const uint32_t fl = (o0.y >> 8) & 0xffu;
+    const double2* T = DATA + o0.z + 4;
+    double2 W = make_double2(1.0, 0.0);
+    if (fl & FL_PRE) {
+      W = slots[o0.y >> 16];
+      if (fl & FL_THR) {
+        W = cmul_f(W, cmul_f(T[tid & 31u], T[32 + (tid >> 5)]));
+        T += 40;
+      }
+    }
+    if (I == K - 1 && sc) {
+      W = make_double2(W.x * s, W.y * s);
+      hph_flags<RB, I, true>(a, fl, W, T, s);
+    } else {
+      hph_flags<RB, I, false>(a, fl, W, T, s);
+    }
+    hph_run<RB, K, I + 1>(a, SUB, DATA, slots, tid, s, sc);
+  }
+}
+
+// An OP_HPHASE marker (hdr) and its sub-ops at SUB (two uint4 per op).
+template <int RB>
+__device__ __forceinline__ void h_phase(const uint4 hdr, const uint4* __restrict__ SUB,
+                                        double2 (&a)[1 << RB], const double2* __restrict__ DATA,
+                                        const double2* __restrict__ slots, uint32_t tid) {
+  const uint32_t K = (hdr.x >> 16) & 0xffu;
+  const bool sc = ((hdr.y >> 8) & HPH_SCALE) != 0u;
+  const double s = sc ? DATA[hdr.z].x : 1.0;
+  switch (K) {
+    case 1: hph_run<RB, 1, 0>(a, SUB, DATA, slots, tid, s, sc); break;
+    case 2: if constexpr (RB >= 2) hph_run<RB, 2, 0>(a, SUB, DATA, slots, tid, s, sc); break;
+    case 3: if constexpr (RB >= 3) hph_run<RB, 3, 0>(a, SUB, DATA, slots, tid, s, sc); break;
+    case 4: if constexpr (RB >= 4) hph_run<RB, 4, 0>(a, SUB, DATA, slots, tid, s, sc); break;
+    default: break;
+  }
 }
 
 template <int RB>
@@ -453,15 +554,19 @@ __device__ __forceinline__ void sweep_tiles(double2* __restrict__ state, const u
         c0 = OP4[2 * ob];
         c1 = OP4[2 * ob + 1];
       }
-      for (uint32_t o = ob; o < oe; ++o) {
-        uint4 n0 = c0, n1 = c1;
-        if (o + 1 < oe) {  // next descriptor in flight while this op runs
-          n0 = OP4[2 * o + 2];
-          n1 = OP4[2 * o + 3];
+      if (ob < oe && (c0.x & 0xffu) == OP_HPHASE) {
+        h_phase<RB>(c0, OP4 + 2 * ob + 2, a, DATA, slots, tid);
+      } else {
+        for (uint32_t o = ob; o < oe; ++o) {
+          uint4 n0 = c0, n1 = c1;
+          if (o + 1 < oe) {  // next descriptor in flight while this op runs
+            n0 = OP4[2 * o + 2];
+            n1 = OP4[2 * o + 3];
+          }
+          exec_op<RB>(c0, c1, a, DATA, slots, tid, base);
+          c0 = n0;
+          c1 = n1;
         }
-        exec_op<RB>(c0, c1, a, DATA, slots, tid, base);
-        c0 = n0;
-        c1 = n1;
       }
       const uint32_t pt2 = opaque(pt);
 #pragma unroll

@@ -17,7 +17,7 @@ import numpy as np
 
 from dqsim_bosonic_b200 import _native as nat
 
-OP_U1, OP_U1R, OP_U1X, OP_U2, OP_FLUSH_R, OP_FLUSH_T, OP_GPHASE, OP_U1H, OP_SCALE = range(9)
+OP_U1, OP_U1R, OP_U1X, OP_U2, OP_FLUSH_R, OP_FLUSH_T, OP_GPHASE, OP_U1H, OP_SCALE, OP_HPHASE = range(10)
 FL_THR, FL_REG, FL_PRE = 1, 2, 4
 MAXM = 12
 SWZ_G = {3: 3, 4: 5, 5: 6, 6: 7, 7: 3, 8: 5, 9: 6, 10: 7, 11: 1}
@@ -207,6 +207,10 @@ def _exec(blob, oo, off_data, a, slots, base, tid, rb):
         f = _c2(blob, D, 1)[0].real
         for j in range(R):
             upd(j, a[:, :, j] * f)
+    elif typ == OP_HPHASE:
+        # marker of a straight-line H phase: its sub-ops follow as ordinary ops
+        # (the kernel folds the trailing scale into the last one: same values)
+        assert b1 >= 1 and creg == 0
     else:
         raise AssertionError(f"unknown op {typ}")
 
