@@ -158,8 +158,12 @@ __device__ __forceinline__ double warp_sum(double x) {
 // at the rounding level of theta) is left alone: their mutual directions carry
 // no information and rotating them again and again only delays convergence of
 // a rank-deficient theta.  A negligible column is still rotated against every
-// significant one, so it ends up orthogonal to the significant subspace (it
-// may be kept when the threshold keeps everything).
+// significant one, so it ends up orthogonal to the significant subspace.  When
+// the threshold keeps such a column (a threshold at or below the rounding
+// level), the split writes it as zeros: its vector is not orthogonal to the
+// other negligible ones, and dividing by its sigma would put O(1) entries
+// into the left tensor for a contribution of order eps |theta|.  The bond
+// dimension is the reference's either way.
 __device__ __forceinline__ bool jacobi_rotation(double al, double be, double gr, double gi, double tol,
                                                 double neg, double& c, double& s, double& ex, double& ey) {
   const double g2 = gr * gr + gi * gi;
@@ -371,7 +375,7 @@ __global__ void __launch_bounds__(1024) k_mps_2q(MpsView v, uint32_t first, uint
     const uint32_t j = perm[k];
     const double sj = sig[j];
     double2 val = zero;
-    if (sj > 0.0) {
+    if (sj > 0.0 && sj * sj > neg) {  // a kept column at the rounding level of theta is left zero
       if (!tr) {
         const double2 g = G[(uint64_t)j * rows + row];
         val = make_double2(g.x / sj, g.y / sj);
@@ -397,7 +401,7 @@ __global__ void __launch_bounds__(1024) k_mps_2q(MpsView v, uint32_t first, uint
     const uint32_t j = perm[k];
     const double sj = sig[j];
     double2 val = zero;
-    if (sj > 0.0) {
+    if (sj > 0.0 && sj * sj > neg) {  // a kept column at the rounding level of theta is left zero
       if (tr) {
         const double2 g = G[(uint64_t)j * rows + col];
         val = make_double2(scale * g.x, -scale * g.y);
@@ -607,7 +611,7 @@ __global__ void __launch_bounds__(kWarpsPer2q * 32) k_mps_2q_warp(MpsView v, uin
     const uint32_t j = perm[k];
     const double sj = sig[j];
     double2 val = zero;
-    if (sj > 0.0) {
+    if (sj > 0.0 && sj * sj > neg) {  // a kept column at the rounding level of theta is left zero
       if (!tr) {
         const double2 g = G[j * ld + row];
         val = make_double2(g.x / sj, g.y / sj);
@@ -632,7 +636,7 @@ __global__ void __launch_bounds__(kWarpsPer2q * 32) k_mps_2q_warp(MpsView v, uin
     const uint32_t j = perm[k];
     const double sj = sig[j];
     double2 val = zero;
-    if (sj > 0.0) {
+    if (sj > 0.0 && sj * sj > neg) {  // a kept column at the rounding level of theta is left zero
       if (tr) {
         const double2 g = G[j * ld + col];
         val = make_double2(scale * g.x, -scale * g.y);
@@ -910,6 +914,7 @@ struct dq_mps_s {
   double2* scratch = nullptr;
   int* flags = nullptr;
   unsigned long long* svd_calls = nullptr;
+  bool broken = false;       // a failed reserve lost the state: every later call fails
   bool smem = true;
   uint64_t scratch_elems = 0;
   size_t work_bytes = 0;
@@ -1247,6 +1252,7 @@ int run_batch(dq_mps_s* h, const std::vector<MpsOp>& ops, const dq_cond* conds, 
 
 int check_mps(dq_mps_t h) {
   if (!h || !h->stream) return fail(DQ_ERR_INVALID_ARG, "null or destroyed MPS handle");
+  if (h->broken) return fail(DQ_ERR_INVALID_ARG, "MPS handle lost its state in a failed reserve");
   return DQ_OK;
 }
 
@@ -1444,18 +1450,36 @@ int dq_mps_reserve(dq_mps_t h, uint32_t capacity) {
   std::vector<uint32_t> key(8);
   DQ_CUDA_TRY(cudaMemcpyAsync(key.data(), h->key, sizeof(uint32_t) * 8, cudaMemcpyDeviceToHost, h->stream));
   DQ_CUDA_TRY(cudaStreamSynchronize(h->stream));
-  DQ_TRY(alloc_buffers(h, 1, capacity, h->ncb));
-  std::vector<double2> wide((size_t)n * 2 * capacity * capacity, make_double2(0.0, 0.0));
+  const uint32_t ncb = h->ncb;
+  uint32_t cap = capacity;
+  int rc = alloc_buffers(h, 1, capacity, ncb);
+  if (rc != DQ_OK) {
+    // The wider buffers could not be had (alloc_buffers freed the old ones
+    // first): put the state back at its old capacity from the host copy, so
+    // the handle stays usable and the caller sees the allocation error.
+    const std::string why = dq_last_error();
+    if (alloc_buffers(h, 1, old, ncb) != DQ_OK) {
+      free_buffers(h);
+      h->broken = true;
+      return fail(rc, why + " (the MPS state could not be restored: the handle is unusable)");
+    }
+    cap = old;
+  }
+  std::vector<double2> wide((size_t)n * 2 * cap * cap, make_double2(0.0, 0.0));
   for (uint32_t k = 0; k < n; ++k)
     for (uint32_t row = 0; row < 2 * old; ++row)
       for (uint32_t r = 0; r < old; ++r)
-        wide[(size_t)k * 2 * capacity * capacity + (size_t)row * capacity + r] =
+        wide[(size_t)k * 2 * cap * cap + (size_t)row * cap + r] =
             host[(size_t)k * 2 * old * old + (size_t)row * old + r];
   DQ_CUDA_TRY(cudaMemcpyAsync(h->t, wide.data(), sizeof(double2) * wide.size(), cudaMemcpyHostToDevice, h->stream));
   DQ_CUDA_TRY(cudaMemcpyAsync(h->dims, dims.data(), sizeof(uint32_t) * (n + 1), cudaMemcpyHostToDevice, h->stream));
   DQ_CUDA_TRY(cudaMemcpyAsync(h->ctr, ctr.data(), sizeof(unsigned long long), cudaMemcpyHostToDevice, h->stream));
   DQ_CUDA_TRY(cudaMemcpyAsync(h->key, key.data(), sizeof(uint32_t) * 8, cudaMemcpyHostToDevice, h->stream));
   DQ_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  if (rc != DQ_OK) {
+    const std::string why = dq_last_error();
+    return fail(rc, why + " (the MPS state is kept at bond capacity " + std::to_string(old) + ")");
+  }
   return DQ_OK;
 }
 

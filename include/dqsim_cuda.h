@@ -465,11 +465,17 @@ DQ_API int dq_mps_run(dq_mps_t h, const dq_inst* prog, uint64_t ninst, const dq_
                       uint64_t nconds, uint64_t seed, int32_t* cbits, uint64_t ncbits,
                       dq_mps_stats* stats);
 /* Mps::apply_2q (:115-135) on the current state: u = 4x4 row-major complex
- * (interleaved re/im, 32 doubles), a = most significant qubit of the row. */
+ * (interleaved re/im, 32 doubles), a = most significant qubit of the row.
+ * A step that needs a wider bond capacity widens the handle (dq_mps_reserve)
+ * and redoes the step; if that allocation fails the call returns DQ_ERR_OOM
+ * with the swap-chain steps done so far applied and the handle still usable. */
 DQ_API int dq_mps_apply_2q(dq_mps_t h, uint32_t a, uint32_t b, const double* u);
 /* Widen the bond capacity of a single-state handle, keeping its state, bond
  * dimensions and RNG position (its classical bits are not kept: a later
- * dq_mps_run starts them afresh). */
+ * dq_mps_run starts them afresh).  If the wider buffers cannot be allocated
+ * the state is put back at the old capacity and the allocation error is
+ * returned; only if that also fails is the handle left unusable (every later
+ * call on it fails; destroy it). */
 DQ_API int dq_mps_reserve(dq_mps_t h, uint32_t capacity);
 DQ_API int dq_mps_bond_dims(dq_mps_t h, uint32_t* dims);   /* n + 1 entries */
 DQ_API int dq_mps_to_state(dq_mps_t h, dq_state_t out);

@@ -421,3 +421,26 @@ def test_apply_2q_widens_a_live_handle():
     assert h.bond_dims() == ref.bond_dims()
     assert np.max(np.abs(h.to_state().download() - ref.to_statevector())) < 1e-12
     h.release()
+
+
+@pytest.mark.parametrize("thr", [0.0, -1.0])
+def test_rank_deficient_thetas_at_rounding_threshold_match_exact_state(thr):
+    # A GHZ chain makes every theta rank 2 and the swap chains of long-range gates
+    # move product-like bonds: their other singular values sit at the rounding level,
+    # and a threshold of 0 (or below) keeps them.  Such kept columns are written as
+    # zeros by the split, so later steps see no O(1) non-isometric entries: the
+    # state after further entangling gates still equals the exact statevector.
+    n = 8
+    rng = np.random.default_rng(11)
+    insts = [g("h", 0)] + [g("cx", q, q + 1) for q in range(n - 1)]
+    insts += [g("swap", 0, 5), g("swap", 7, 2), g("cx", 1, 6), g("cz", 6, 0)]
+    insts += [random_gate(rng, n, "u3") for _ in range(n)]
+    insts += [g("rzz", 3, 4, 0.3), g("cx", 0, 7), g("swap", 2, 6)]
+    insts += [random_gate(rng, n, "ry") for _ in range(n)]
+    c = JsonCircuit(n, insts)
+    prog = prog_of(c)
+    exact = _oracle.run(prog, SEED)[0]
+    sv, _, dims, _ = device_run(c, SEED, thr=thr)
+    assert np.max(np.abs(sv - exact)) < 1e-12
+    assert abs(np.vdot(sv, sv).real - 1.0) < 1e-12
+    assert max(dims) <= 16
