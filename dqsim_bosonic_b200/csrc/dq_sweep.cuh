@@ -496,26 +496,28 @@ __device__ __forceinline__ void sweep_tiles(double2* __restrict__ state, const u
       base = advance(base);
       continue;
     }
-    // per-tile phase factors: few slots with many entries take a warp
-    // each (lane products, then a butterfly over the lanes); otherwise one
-    // thread per slot
-    if (nslots <= 4 * NW) {
-      for (uint32_t s = warp; s < nslots; s += NW) {
-        const uint32_t c = SL[s].count, st = SL[s].start;
+    // per-tile phase factors: up to 16 slots per warp take an 8-lane group
+    // each (lane products over every 8th entry, then a three-round butterfly
+    // over the group); more slots take one thread each
+    if (nslots <= 16 * NW) {
+      const uint32_t gl = lane & 7u, grp = lane >> 3;
+      for (uint32_t s0 = warp * 4u; s0 < nslots; s0 += NW * 4u) {
+        const uint32_t s = s0 + grp;
         double2 w = make_double2(1.0, 0.0);
-        for (uint32_t e = lane; e < c; e += 32) {
-          const SwSlotEnt& E = SE[st + e];
-          if ((base & E.mask) == E.mask) w = cmul_f(w, E.w);
-        }
-        if (c > 1) {
-#pragma unroll
-          for (int o = 16; o > 0; o >>= 1) {
-            const double2 q = make_double2(__shfl_xor_sync(0xffffffffu, w.x, o),
-                                           __shfl_xor_sync(0xffffffffu, w.y, o));
-            w = cmul_f(w, q);
+        if (s < nslots) {
+          const uint32_t c = SL[s].count, st = SL[s].start;
+          for (uint32_t e = gl; e < c; e += 8u) {
+            const SwSlotEnt& E = SE[st + e];
+            if ((base & E.mask) == E.mask) w = cmul_f(w, E.w);
           }
         }
-        if (lane == 0) slots[s] = cmul_f(SL[s].w0, w);
+#pragma unroll
+        for (int o = 4; o > 0; o >>= 1) {
+          const double2 q = make_double2(__shfl_xor_sync(0xffffffffu, w.x, o),
+                                         __shfl_xor_sync(0xffffffffu, w.y, o));
+          w = cmul_f(w, q);
+        }
+        if (gl == 0 && s < nslots) slots[s] = cmul_f(SL[s].w0, w);
       }
     } else {
       for (uint32_t s = tid; s < nslots; s += kSwThreads) {
