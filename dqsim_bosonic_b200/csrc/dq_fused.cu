@@ -43,8 +43,10 @@ namespace {
 // loads.  S = 2: the next tile's load is in flight while the current one is
 // computed.  The sweep program is staged in shared memory once per launch
 // (read from global memory per op instead, QFT30 ran 38% slower).
-template <int TB, int RB, int S, int RUNB>
-__global__ void __launch_bounds__(1 << TB, (S == 1 && TB == 7 ? 3 : (TB + RB <= 11 ? 2 : 1)))
+// HONLY (every phase an H phase): built without the generic op interpreter,
+// in few enough registers for four CTAs per SM.
+template <int TB, int RB, int S, int RUNB, bool HONLY = false>
+__global__ void __launch_bounds__(1 << TB, (S == 1 && TB == 7 ? (HONLY ? 4 : 3) : (TB + RB <= 11 ? 2 : 1)))
     k_sweep(double2* __restrict__ state, const uint8_t* __restrict__ gprog, uint32_t prog_bytes,
             uint32_t ntiles, long long synth) {
   constexpr int T = 1 << (TB + RB);
@@ -55,7 +57,7 @@ __global__ void __launch_bounds__(1 << TB, (S == 1 && TB == 7 ? 3 : (TB + RB <= 
   for (uint32_t i = threadIdx.x * 16u; i < prog_bytes; i += (1u << TB) * 16u)
     *reinterpret_cast<uint4*>(sprog + i) = __ldg(reinterpret_cast<const uint4*>(gprog + i));
   __syncthreads();
-  sweep_tiles<TB, RB, S, RUNB>(state, sprog, ntiles, synth, bufs, slots, blockIdx.x, gridDim.x);
+  sweep_tiles<TB, RB, S, RUNB, HONLY>(state, sprog, ntiles, synth, bufs, slots, blockIdx.x, gridDim.x);
 }
 
 // Sweep k of many states in one launch: job j's tiles are split into chunks
@@ -826,6 +828,12 @@ int encode_sweep(const PSweep& sw_in, const std::vector<PGate>& G, uint32_t TBn,
   }
   h.nphase = (uint32_t)P.size();
   h.nslots = (uint32_t)SL.size();
+  {
+    bool honly = !P.empty();
+    for (const SwPhase& sp : P)
+      if (sp.op_begin >= sp.op_end || O[sp.op_begin].type != OP_HPHASE) honly = false;
+    h.flags = honly ? SWF_HONLY : 0u;
+  }
   h.tile_xload = tile_xload;
   for (uint32_t k = 0; k < m; ++k) h.local_pos[k] = sw.local[k];
   const size_t hoff = blob.put(&h, 1);
@@ -987,7 +995,7 @@ bool convert_inst(const dq_inst& in, const uint32_t* perm, std::vector<PGate>& o
   }
 }
 
-template <int TB, int RB, int S, int RUNB>
+template <int TB, int RB, int S, int RUNB, bool HONLY = false>
 int launch_sweep_r(double2* amp, uint32_t n, const uint8_t* dblob, uint32_t prog_bytes,
                    cudaStream_t st, long long synth) {
   constexpr int M = TB + RB;
@@ -1005,7 +1013,7 @@ int launch_sweep_r(double2* amp, uint32_t n, const uint8_t* dblob, uint32_t prog
   {
     std::lock_guard<std::mutex> lk(mu);
     if (!attr_done[dev & 63]) {
-      DQ_CUDA_TRY(cudaFuncSetAttribute(k_sweep<TB, RB, S, RUNB>,
+      DQ_CUDA_TRY(cudaFuncSetAttribute(k_sweep<TB, RB, S, RUNB, HONLY>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_max));
       attr_done[dev & 63] = true;
     }
@@ -1014,7 +1022,7 @@ int launch_sweep_r(double2* amp, uint32_t n, const uint8_t* dblob, uint32_t prog
     int& r = per_sm[dev & 63][bucket];
     if (r == 0) {
       int b = 1;
-      DQ_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_sweep<TB, RB, S, RUNB>,
+      DQ_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_sweep<TB, RB, S, RUNB, HONLY>,
                                                                 1 << TB, smem_b));
       r = b < 1 ? 1 : b;
     }
@@ -1024,14 +1032,15 @@ int launch_sweep_r(double2* amp, uint32_t n, const uint8_t* dblob, uint32_t prog
   DQ_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
   const uint64_t tiles = 1ULL << (n - M);
   const unsigned grid = (unsigned)std::min<uint64_t>(tiles, (uint64_t)sms * resident);
-  k_sweep<TB, RB, S, RUNB><<<grid, 1 << TB, smem, st>>>(amp, dblob, prog_bytes, (uint32_t)tiles, synth);
+  k_sweep<TB, RB, S, RUNB, HONLY><<<grid, 1 << TB, smem, st>>>(amp, dblob, prog_bytes, (uint32_t)tiles,
+                                                               synth);
   DQ_CUDA_TRY(cudaGetLastError());
   return DQ_OK;
 }
 
 template <int TB, int RB>
 int launch_sweep_rb(double2* amp, uint32_t n, const uint8_t* dblob, uint32_t prog_bytes,
-                    cudaStream_t st, long long synth, uint32_t run_bits) {
+                    cudaStream_t st, long long synth, uint32_t run_bits, uint32_t flags) {
   // default: single-buffered tiles, three 128-thread CTAs per SM (measured
   // faster than two double-buffered CTAs: the extra warps hide more of the
   // per-op latency than the prefetch saves); DQSIM_SWEEP_STAGES=2 selects
@@ -1040,27 +1049,32 @@ int launch_sweep_rb(double2* amp, uint32_t n, const uint8_t* dblob, uint32_t pro
     const char* e = getenv("DQSIM_SWEEP_STAGES");
     return e ? atoi(e) : 1;
   }();
-  if (TB == 7 && stages != 2)
+  if (TB == 7 && stages != 2) {
+    if (RB == 4 && (flags & SWF_HONLY))
+      return run_bits == 3 ? launch_sweep_r<7, 4, 1, 3, true>(amp, n, dblob, prog_bytes, st, synth)
+                           : launch_sweep_r<7, 4, 1, 5, true>(amp, n, dblob, prog_bytes, st, synth);
     return run_bits == 3 ? launch_sweep_r<7, RB, 1, 3>(amp, n, dblob, prog_bytes, st, synth)
                          : launch_sweep_r<7, RB, 1, 5>(amp, n, dblob, prog_bytes, st, synth);
+  }
   return run_bits == 3 ? launch_sweep_r<TB, RB, 2, 3>(amp, n, dblob, prog_bytes, st, synth)
                        : launch_sweep_r<TB, RB, 2, 5>(amp, n, dblob, prog_bytes, st, synth);
 }
 
 int launch_sweep(double2* amp, uint32_t n, uint32_t TB, uint32_t RB, const uint8_t* dblob,
-                 uint32_t prog_bytes, cudaStream_t st, long long synth, uint32_t run_bits) {
+                 uint32_t prog_bytes, cudaStream_t st, long long synth, uint32_t run_bits,
+                 uint32_t flags) {
   if (TB == 8) {
     switch (RB) {
-      case 2: return launch_sweep_rb<8, 2>(amp, n, dblob, prog_bytes, st, synth, run_bits);
-      case 3: return launch_sweep_rb<8, 3>(amp, n, dblob, prog_bytes, st, synth, run_bits);
-      case 4: return launch_sweep_rb<8, 4>(amp, n, dblob, prog_bytes, st, synth, run_bits);
+      case 2: return launch_sweep_rb<8, 2>(amp, n, dblob, prog_bytes, st, synth, run_bits, flags);
+      case 3: return launch_sweep_rb<8, 3>(amp, n, dblob, prog_bytes, st, synth, run_bits, flags);
+      case 4: return launch_sweep_rb<8, 4>(amp, n, dblob, prog_bytes, st, synth, run_bits, flags);
       default: break;
     }
   } else if (TB == 7) {
     switch (RB) {
-      case 2: return launch_sweep_rb<7, 2>(amp, n, dblob, prog_bytes, st, synth, run_bits);
-      case 3: return launch_sweep_rb<7, 3>(amp, n, dblob, prog_bytes, st, synth, run_bits);
-      case 4: return launch_sweep_rb<7, 4>(amp, n, dblob, prog_bytes, st, synth, run_bits);
+      case 2: return launch_sweep_rb<7, 2>(amp, n, dblob, prog_bytes, st, synth, run_bits, flags);
+      case 3: return launch_sweep_rb<7, 3>(amp, n, dblob, prog_bytes, st, synth, run_bits, flags);
+      case 4: return launch_sweep_rb<7, 4>(amp, n, dblob, prog_bytes, st, synth, run_bits, flags);
       default: break;
     }
   }
@@ -1268,7 +1282,7 @@ int fused_run_segment(double2* amp, uint32_t n, std::vector<PGate>& G, Planner& 
     // a pending basis state is consumed by the first sweep (it writes every amplitude)
     const long long synth = (lazy_basis && *lazy_basis >= 0) ? (long long)*lazy_basis : -1;
     DQ_TRY(launch_sweep(amp, n, pl.TB, pl.RB, fw.d_blob + offs[i], hh->prog_bytes, st, synth,
-                        hh->run_bits));
+                        hh->run_bits, hh->flags));
     if (lazy_basis) *lazy_basis = -1;
     if (timing) {
       cudaEventRecord(e1, st);

@@ -66,8 +66,12 @@ struct SwHeader {
   // 2^(m - run_bits) entries each, stored after the header:
   uint32_t off_runoff;         // u64 physical offset of run r (local bits run_bits..m-1 = r)
   uint32_t off_runswz;         // u32 swizzled shared-memory index of run r's first element
-  uint32_t pad0, pad1;
+  uint32_t flags;              // SWF_* (host side: kernel choice)
+  uint32_t pad1;
 };
+// every phase of the sweep is an H phase (OP_HPHASE): the launch may use the
+// kernel built with the H-phase path only
+constexpr uint32_t SWF_HONLY = 1u;
 struct SwPhase {
   uint32_t lanesw[32];         // swizzled local index of the lane bits (thread bits 0..4)
   uint32_t warpsw[8];          // swizzled local index of the warp bits (thread bits 5..7)
@@ -406,8 +410,10 @@ __device__ __forceinline__ void exec_op(const uint4 o0, const uint4 o1, double2 
 // `slots` (shared memory).  Every thread of the CTA calls it; no copy is in
 // flight on return.  S tile buffers form a cp.async pipeline with S - 1
 // tiles prefetched while the current one is computed.
-// RUNB: the program's run_bits (5 or 3), fixed at compile time.
-template <int TB, int RB, int S, int RUNB>
+// RUNB: the program's run_bits (5 or 3), fixed at compile time.  HONLY: the
+// program's phases are all H phases (SWF_HONLY), so the generic op
+// interpreter is left out of the build.
+template <int TB, int RB, int S, int RUNB, bool HONLY = false>
 __device__ __forceinline__ void sweep_tiles(double2* __restrict__ state, const uint8_t* prog,
                                             uint32_t ntiles, long long synth, double2* bufs,
                                             double2* slots, uint32_t first_tile, uint32_t tile_step) {
@@ -556,7 +562,9 @@ __device__ __forceinline__ void sweep_tiles(double2* __restrict__ state, const u
         c0 = OP4[2 * ob];
         c1 = OP4[2 * ob + 1];
       }
-      if (ob < oe && (c0.x & 0xffu) == OP_HPHASE) {
+      if constexpr (HONLY) {
+        h_phase<RB>(c0, OP4 + 2 * ob + 2, a, DATA, slots, tid);
+      } else if (ob < oe && (c0.x & 0xffu) == OP_HPHASE) {
         h_phase<RB>(c0, OP4 + 2 * ob + 2, a, DATA, slots, tid);
       } else {
         for (uint32_t o = ob; o < oe; ++o) {
