@@ -559,6 +559,52 @@ __device__ __forceinline__ void phase_one(double2 (&a)[8], double2 (&b)[8], cons
   }
 }
 
+// One op of a straight-line phase on register bit PB: its gradient term from
+// the amplitudes before it, then V on psi and lambda.
+template <int VK, int PB>
+__device__ __forceinline__ double fast_op(double2 (&a)[8], double2 (&b)[8], const PSub& P) {
+  const double acc = grad_terms<PB>(a, b, P.d[0], P.tm[0]);
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const int i = pair_lo<PB>(k), j = i | (1 << PB);
+    apply2<VK>(P.v, a[i], a[j]);
+    apply2<VK>(P.v, b[i], b[j]);
+  }
+  return acc;
+}
+
+// A register phase of two or three ops on distinct phase bits PB0 < PB1 (<
+// PB2), each with one derivative and the same V shape VK (the encoder sorts
+// such ops by target: ops on distinct qubits commute), as straight-line code;
+// the ops' warp reductions run after all of them, side by side.
+template <int VK, int PB0, int PB1, int PB2>
+__device__ __forceinline__ void phase_fast(double2 (&a)[8], double2 (&b)[8], const PSub* ps,
+                                           double* accw, int lane, int w) {
+  double g0 = fast_op<VK, PB0>(a, b, ps[0]);
+  double g1 = fast_op<VK, PB1>(a, b, ps[1]);
+  double g2 = 0.0;
+  if constexpr (PB2 >= 0) g2 = fast_op<VK, PB2>(a, b, ps[2]);
+  g0 = warp_sum_d(g0);
+  g1 = warp_sum_d(g1);
+  if constexpr (PB2 >= 0) g2 = warp_sum_d(g2);
+  if (lane == 0) {
+    accw[ps[0].slot * kAWarps + w] += g0;
+    accw[ps[1].slot * kAWarps + w] += g1;
+    if constexpr (PB2 >= 0) accw[ps[2].slot * kAWarps + w] += g2;
+  }
+}
+
+template <int VK>
+__device__ __forceinline__ void phase_fast_bits(uint32_t form, double2 (&a)[8], double2 (&b)[8],
+                                                const PSub* ps, double* accw, int lane, int w) {
+  switch (form) {
+    case 0: phase_fast<VK, 0, 1, 2>(a, b, ps, accw, lane, w); break;
+    case 1: phase_fast<VK, 0, 1, -1>(a, b, ps, accw, lane, w); break;
+    case 2: phase_fast<VK, 0, 2, -1>(a, b, ps, accw, lane, w); break;
+    default: phase_fast<VK, 1, 2, -1>(a, b, ps, accw, lane, w); break;
+  }
+}
+
 // The op data of one register phase: threads < cnt fill ps[0 .. cnt).
 __device__ __forceinline__ void stage_phase(const AOp& hdr, const AOp* sub, const double2* pool,
                                             PSub* ps) {
@@ -623,8 +669,16 @@ __device__ __noinline__ void op_phase(double2* sp, double2* sl, const AOp& hdr, 
       a[i] = valid ? sp[off(i)] : make_double2(0.0, 0.0);
       b[i] = valid ? sl[off(i)] : make_double2(0.0, 0.0);
     }
+    // straight-line form (header pad[0] = 1 + VK * 4 + bit form)
+    const uint32_t fast = hdr.pad[0];
+    if (fast) {
+      const uint32_t vk = (fast - 1u) >> 2, form = (fast - 1u) & 3u;
+      if (vk == 1) phase_fast_bits<1>(form, a, b, ps, accw, lane, w);
+      else if (vk == 2) phase_fast_bits<2>(form, a, b, ps, accw, lane, w);
+      else phase_fast_bits<0>(form, a, b, ps, accw, lane, w);
+    }
 #pragma unroll 1
-    for (uint32_t u = 0; u < cnt; ++u) {
+    for (uint32_t u = 0; u < (fast ? 0u : cnt); ++u) {
       const PSub& P = ps[u];
       double acc[4] = {0.0, 0.0, 0.0, 0.0};
       switch (P.pb * 3 + P.vk) {
@@ -1142,8 +1196,42 @@ int encode_asweep(const ASweepPlan& sp, uint32_t n, ASweepHdr& hdr, std::vector<
       h.lt = (uint8_t)bits[0];
       h.lt2 = (uint8_t)bits[1];
       h.dq[0] = (uint8_t)bits[2];
+      std::vector<AOp> run(ops.begin() + (ptrdiff_t)i, ops.begin() + (ptrdiff_t)j);
+      // Straight-line form: two or three ops on distinct qubits, one derivative
+      // each, one V shape.  Such ops commute, so they are sorted by target bit
+      // and the kernel runs them with compile-time register bits.
+      {
+        auto vk_of = [&](const AOp& q) -> int {
+          const double2* mt = pool.data() + q.mat;
+          const bool real = mt[0].y == 0.0 && mt[1].y == 0.0 && mt[2].y == 0.0 && mt[3].y == 0.0;
+          const bool rxl = mt[0].y == 0.0 && mt[3].y == 0.0 && mt[1].x == 0.0 && mt[2].x == 0.0;
+          return real ? 1 : (rxl ? 2 : 0);
+        };
+        bool fast = (run.size() == 2 || run.size() == 3) && nones == run.size();
+        uint32_t distinct = 0;
+        for (size_t a = 0; a < run.size(); ++a) {
+          bool dup = false;
+          for (size_t b2 = 0; b2 < a; ++b2) dup = dup || run[b2].lt == run[a].lt;
+          if (!dup) ++distinct;
+          fast = fast && run[a].np == 1 && vk_of(run[a]) == vk_of(run[0]);
+        }
+        fast = fast && distinct == run.size();
+        if (fast) {
+          std::sort(run.begin(), run.end(), [](const AOp& x, const AOp& y) { return x.lt < y.lt; });
+          uint32_t pb[3] = {0, 0, 0};
+          for (size_t a = 0; a < run.size(); ++a)
+            for (uint32_t b2 = 0; b2 < 3; ++b2)
+              if (bits[b2] == run[a].lt) pb[a] = b2;
+          int form = -1;
+          if (run.size() == 3) form = 0;
+          else if (pb[0] == 0 && pb[1] == 1) form = 1;
+          else if (pb[0] == 0 && pb[1] == 2) form = 2;
+          else if (pb[0] == 1 && pb[1] == 2) form = 3;
+          if (form >= 0) h.pad[0] = (uint8_t)(1 + vk_of(run[0]) * 4 + form);
+        }
+      }
       phased.push_back(h);
-      for (size_t k = i; k < j; ++k) phased.push_back(ops[k]);
+      for (const AOp& q : run) phased.push_back(q);
       i = j;
     }
     ops.swap(phased);
