@@ -566,12 +566,10 @@ int dq_adjoint(dq_state_t h, const dq_inst* prog, uint64_t ninst, const int32_t*
     if (ev[i]) cudaEventRecord(ev[i], h->stream);
   };
 
-  // forward pass
-  mark(0);
-  DQ_TRY(dq_run(h, prog, ninst, nullptr, 0, 0, nullptr, 0, &o, nullptr));
-  DQ_TRY(canonicalize(h));
-  mark(1);
-
+  // The observable's terms, lambda and the gradient slots are set up before
+  // the forward pass (the term upload waits for the stream, an allocation
+  // may block the host), so forward pass, lambda = H psi and backward pass
+  // run back to back on the stream.
   DeviceTerms t;
   DQ_TRY(upload_terms(terms, nterms, h->n, h->stream, &t));
   void* lam_v = nullptr;
@@ -582,6 +580,12 @@ int dq_adjoint(dq_state_t h, const dq_inst* prog, uint64_t ninst, const int32_t*
     cudaError_t e = cudaMallocAsync((void**)&slots, sizeof(double) * (nslots + 1), h->stream);
     if (e != cudaSuccess) rc = fail(DQ_ERR_OOM, std::string("cudaMallocAsync: ") + cudaGetErrorString(e));
   }
+
+  // forward pass
+  mark(0);
+  if (rc == DQ_OK) rc = dq_run(h, prog, ninst, nullptr, 0, 0, nullptr, 0, &o, nullptr);
+  if (rc == DQ_OK) rc = canonicalize(h);
+  mark(1);
   if (rc == DQ_OK) rc = launch_pauli(h, lam, t, slots + nslots);
   mark(2);
 
