@@ -130,6 +130,29 @@ def ragged_batch(count: int = 1024, seed: int = 99, n_lo: int = 10, n_hi: int = 
             for k, (n, d) in enumerate(zip(ns, ds))]
 
 
+def hadamard_diagonal_circuit(n, layers, seed):
+    """Layers of Hadamards on random qubit subsets with random diagonal gates in between:
+    register phases made only of Hadamards, whose pending phases pair them with qubits
+    above and below them, local or not (the straight-line H phases of the sweep kernel)."""
+    rng = np.random.default_rng(seed)
+    insts = []
+    diag2 = ["cp", "crz", "cu1", "rzz", "cz"]
+    diag1 = ["p", "rz", "t", "s", "sdg", "z"]
+    for _ in range(layers):
+        for q in rng.permutation(n)[: int(rng.integers(1, n + 1))]:
+            insts.append(g("h", int(q)))
+        for _ in range(int(rng.integers(1, 2 * n))):
+            if rng.random() < 0.6:
+                a, b = (int(v) for v in rng.permutation(n)[:2])
+                k = diag2[rng.integers(len(diag2))]
+                insts.append(g(k, a, b) if k == "cz" else g(k, a, b, float(rng.uniform(-3, 3))))
+            else:
+                q = int(rng.integers(n))
+                k = diag1[rng.integers(len(diag1))]
+                insts.append(g(k, q, float(rng.uniform(-3, 3))) if k in ("p", "rz") else g(k, q))
+    return JsonCircuit(n, insts)
+
+
 def qft_with_x(n: int = 30, seed: int = 1234) -> JsonCircuit:
     """x on a seeded random subset (p = 0.5), then the textbook QFT with swaps."""
     rng = np.random.default_rng(seed)

@@ -363,3 +363,27 @@ def test_diagonal_gates_with_two_trainable_angles(gpu):
     assert np.max(np.abs(g1 - g2)) < 1e-11
     ps = orc.param_shift(c, theta, H.array())
     assert np.max(np.abs(g1 - ps)) < TOL_SHIFT
+
+
+@pytest.mark.parametrize("n,seed", [(11, 1), (13, 2), (17, 3)])
+def test_straight_line_phases_match_per_gate(gpu, n, seed):
+    # layers of ry and rx on every qubit in a random order, separated by rzz rings: the
+    # backward sweeps' register phases of two or three commuting one-parameter ops (real
+    # and rx-shaped matrices, every two-op placement of the phase bits), which the fused
+    # backward sorts by target and runs as straight-line code
+    rng = np.random.default_rng(seed)
+    c = ParamCircuit(n)
+    k = 0
+    for layer in range(4):
+        for q in rng.permutation(n):
+            (c.rx if layer % 2 else c.ry)(int(q), Param(k))
+            k += 1
+        for q in range(n):
+            c.add("rzz", [q, (q + 1) % n], [Param(k)])
+            k += 1
+    theta = rng.uniform(-np.pi, np.pi, size=k)
+    H = random_observable(n, 10, seed=seed + 20)
+    e1, g1 = adjoint_gradient(c, theta, H, exec="fused")
+    e2, g2 = adjoint_gradient(c, theta, H, exec="per_gate")
+    assert abs(e1 - e2) < 1e-12
+    assert np.max(np.abs(g1 - g2)) < 1e-11, np.max(np.abs(g1 - g2))

@@ -12,8 +12,8 @@ import numpy as np
 import pytest
 
 import _oracle
-from _circuits import (JsonCircuit, brickwork_u3_cx, cond, g, gate, hea_ansatz, qft_with_x,
-                       random_circuit, trajectory_circuit)
+from _circuits import (JsonCircuit, brickwork_u3_cx, cond, g, gate, hadamard_diagonal_circuit,
+                       hea_ansatz, qft_with_x, random_circuit, trajectory_circuit)
 from dqsim_bosonic_b200 import StatevectorSimulator
 from dqsim_bosonic_b200 import _native as nat
 from dqsim_bosonic_b200.circuit import decode_circuit_json, encode
@@ -205,4 +205,15 @@ def test_distributed_variant_fused(gpu):
     prog = prog_of(c)
     want, _, _, _ = _oracle.run(prog, 0)
     st, _, _ = fused_run(prog)
+    assert np.max(np.abs(st.download() - want)) < ATOL
+
+
+@pytest.mark.parametrize("n,layers,seed", [(12, 12, 1), (15, 10, 2), (18, 8, 3), (21, 6, 4)])
+def test_hadamard_phases_with_diagonals(gpu, n, layers, seed):
+    prog = prog_of(hadamard_diagonal_circuit(n, layers, seed))
+    init = random_state(n, seed)
+    want, _, rc, _ = _oracle.run(prog, 0, init)
+    assert rc == 0
+    st, _, prof = fused_run(prog, 0, init)
+    assert prof.sweeps >= 1
     assert np.max(np.abs(st.download() - want)) < ATOL

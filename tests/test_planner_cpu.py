@@ -9,7 +9,8 @@ import numpy as np
 import pytest
 
 import _oracle
-from _circuits import JsonCircuit, brickwork_u3_cx, g, gate, hea_ansatz, qft_with_x, random_circuit
+from _circuits import (JsonCircuit, brickwork_u3_cx, g, gate, hadamard_diagonal_circuit, hea_ansatz,
+                       qft_with_x, random_circuit)
 from _sweep_emu import canonical, emulate
 from dqsim_bosonic_b200 import _native as nat
 from dqsim_bosonic_b200.circuit import decode_circuit_json, encode
@@ -110,3 +111,52 @@ def test_leading_x_gates_fold_into_the_load():
     insts += [g("cx", 0, 5), g("x", 5), g("x", 0), g("cp", 3, 7, 0.7), g("x", 7)]
     check(JsonCircuit(12, insts), seed=4)
     check(JsonCircuit(12, insts[::-1]), seed=5)
+
+
+def _plan_ops(prog):
+    """(sweep header flags, [(type, b0, b1, flags) per op]) of every planned sweep."""
+    import struct
+
+    from _sweep_emu import plan
+
+    blobs, _, _, _ = plan(prog)
+    out = []
+    for b in blobs:
+        off_op = struct.unpack_from("<I", b, 68)[0]
+        hflags = struct.unpack_from("<I", b, 104)[0]
+        nph = struct.unpack_from("<I", b, 8)[0]
+        off_phase = struct.unpack_from("<I", b, 64)[0]
+        ops = []
+        for p in range(nph):
+            ob, oe = struct.unpack_from("<2I", b, off_phase + p * 192 + 176)
+            for o in range(ob, oe):
+                w0, w1 = struct.unpack_from("<2I", b, off_op + 32 * o)
+                ops.append((w0 & 0xFF, (w0 >> 8) & 0xFF, (w0 >> 16) & 0xFF, (w1 >> 8) & 0xFF))
+        out.append((hflags, ops))
+    return out
+
+
+def test_hadamard_phases_are_marked(engine_lib):
+    # QFT: every phase of every sweep is an H phase (the H-only kernel build); the cp
+    # phases of a target whose partners on register bits are all below it get FL_LOWF
+    # tables (2^b products), the others (lower qubits on higher register bits) full ones
+    sweeps = _plan_ops(prog_of(qft_with_x(14, 3)))
+    assert all(fl & 1 for fl, _ in sweeps)
+    subs = [op for _, ops in sweeps for op in ops if op[0] == 7 and op[3] & 6 == 6]
+    assert any(op[3] & 8 for op in subs) and any(not op[3] & 8 for op in subs)
+    # an H phase's ops sit on register bits 0..K-1 in order right after the marker
+    for _, ops in sweeps:
+        for i, op in enumerate(ops):
+            if op[0] == 9:
+                k = op[2]
+                assert [o[1] for o in ops[i + 1:i + 1 + k]] == list(range(k))
+    # pending phases on higher qubits: H phases whose flush tables need every register bit
+    sweeps = _plan_ops(prog_of(hadamard_diagonal_circuit(15, 10, 2)))
+    subs = [op for _, ops in sweeps for op in ops if op[0] == 7 and op[3] & 6 == 6]
+    assert any(op[3] & 8 == 0 for op in subs)
+    assert any(op[0] == 9 for _, ops in sweeps for op in ops)
+
+
+@pytest.mark.parametrize("n,layers,seed", [(12, 12, 1), (14, 10, 2)])
+def test_hadamard_diagonal_circuits_planned(engine_lib, n, layers, seed):
+    check(hadamard_diagonal_circuit(n, layers, seed), seed)
