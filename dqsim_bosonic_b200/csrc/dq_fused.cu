@@ -43,10 +43,12 @@ namespace {
 // loads.  S = 2: the next tile's load is in flight while the current one is
 // computed.  The sweep program is staged in shared memory once per launch
 // (read from global memory per op instead, QFT30 ran 38% slower).
-// HONLY (every phase an H phase): built without the generic op interpreter,
+// FORM_H (every phase an H phase) and FORM_U (plain one-qubit ops only): built
+// without the generic op interpreter (FORM_U: with its one-qubit part only),
 // in few enough registers for four CTAs per SM.
-template <int TB, int RB, int S, int RUNB, bool HONLY = false>
-__global__ void __launch_bounds__(1 << TB, (S == 1 && TB == 7 ? (HONLY ? 4 : 3) : (TB + RB <= 11 ? 2 : 1)))
+template <int TB, int RB, int S, int RUNB, int FORM = FORM_ALL>
+__global__ void __launch_bounds__(1 << TB, (S == 1 && TB == 7 ? (FORM != FORM_ALL ? 4 : 3)
+                                                              : (TB + RB <= 11 ? 2 : 1)))
     k_sweep(double2* __restrict__ state, const uint8_t* __restrict__ gprog, uint32_t prog_bytes,
             uint32_t ntiles, long long synth) {
   constexpr int T = 1 << (TB + RB);
@@ -57,7 +59,7 @@ __global__ void __launch_bounds__(1 << TB, (S == 1 && TB == 7 ? (HONLY ? 4 : 3) 
   for (uint32_t i = threadIdx.x * 16u; i < prog_bytes; i += (1u << TB) * 16u)
     *reinterpret_cast<uint4*>(sprog + i) = __ldg(reinterpret_cast<const uint4*>(gprog + i));
   __syncthreads();
-  sweep_tiles<TB, RB, S, RUNB, HONLY>(state, sprog, ntiles, synth, bufs, slots, blockIdx.x, gridDim.x);
+  sweep_tiles<TB, RB, S, RUNB, FORM>(state, sprog, ntiles, synth, bufs, slots, blockIdx.x, gridDim.x);
 }
 
 // Sweep k of many states in one launch: job j's tiles are split into chunks
@@ -833,6 +835,10 @@ int encode_sweep(const PSweep& sw_in, const std::vector<PGate>& G, uint32_t TBn,
     for (const SwPhase& sp : P)
       if (sp.op_begin >= sp.op_end || O[sp.op_begin].type != OP_HPHASE) honly = false;
     h.flags = honly ? SWF_HONLY : 0u;
+    bool uonly = !P.empty() && !honly;
+    for (const EncOp& e : O)
+      if (!(e.type == OP_U1 || e.type == OP_U1R || e.type == OP_U1X) || (e.flags & FL_PRE)) uonly = false;
+    if (uonly) h.flags |= SWF_UONLY;
   }
   h.tile_xload = tile_xload;
   for (uint32_t k = 0; k < m; ++k) h.local_pos[k] = sw.local[k];
@@ -995,7 +1001,7 @@ bool convert_inst(const dq_inst& in, const uint32_t* perm, std::vector<PGate>& o
   }
 }
 
-template <int TB, int RB, int S, int RUNB, bool HONLY = false>
+template <int TB, int RB, int S, int RUNB, int FORM = FORM_ALL>
 int launch_sweep_r(double2* amp, uint32_t n, const uint8_t* dblob, uint32_t prog_bytes,
                    cudaStream_t st, long long synth) {
   constexpr int M = TB + RB;
@@ -1013,7 +1019,7 @@ int launch_sweep_r(double2* amp, uint32_t n, const uint8_t* dblob, uint32_t prog
   {
     std::lock_guard<std::mutex> lk(mu);
     if (!attr_done[dev & 63]) {
-      DQ_CUDA_TRY(cudaFuncSetAttribute(k_sweep<TB, RB, S, RUNB, HONLY>,
+      DQ_CUDA_TRY(cudaFuncSetAttribute(k_sweep<TB, RB, S, RUNB, FORM>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_max));
       attr_done[dev & 63] = true;
     }
@@ -1022,7 +1028,7 @@ int launch_sweep_r(double2* amp, uint32_t n, const uint8_t* dblob, uint32_t prog
     int& r = per_sm[dev & 63][bucket];
     if (r == 0) {
       int b = 1;
-      DQ_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_sweep<TB, RB, S, RUNB, HONLY>,
+      DQ_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_sweep<TB, RB, S, RUNB, FORM>,
                                                                 1 << TB, smem_b));
       r = b < 1 ? 1 : b;
     }
@@ -1032,7 +1038,7 @@ int launch_sweep_r(double2* amp, uint32_t n, const uint8_t* dblob, uint32_t prog
   DQ_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
   const uint64_t tiles = 1ULL << (n - M);
   const unsigned grid = (unsigned)std::min<uint64_t>(tiles, (uint64_t)sms * resident);
-  k_sweep<TB, RB, S, RUNB, HONLY><<<grid, 1 << TB, smem, st>>>(amp, dblob, prog_bytes, (uint32_t)tiles,
+  k_sweep<TB, RB, S, RUNB, FORM><<<grid, 1 << TB, smem, st>>>(amp, dblob, prog_bytes, (uint32_t)tiles,
                                                                synth);
   DQ_CUDA_TRY(cudaGetLastError());
   return DQ_OK;
@@ -1051,8 +1057,11 @@ int launch_sweep_rb(double2* amp, uint32_t n, const uint8_t* dblob, uint32_t pro
   }();
   if (TB == 7 && stages != 2) {
     if (RB == 4 && (flags & SWF_HONLY))
-      return run_bits == 3 ? launch_sweep_r<7, 4, 1, 3, true>(amp, n, dblob, prog_bytes, st, synth)
-                           : launch_sweep_r<7, 4, 1, 5, true>(amp, n, dblob, prog_bytes, st, synth);
+      return run_bits == 3 ? launch_sweep_r<7, 4, 1, 3, FORM_H>(amp, n, dblob, prog_bytes, st, synth)
+                           : launch_sweep_r<7, 4, 1, 5, FORM_H>(amp, n, dblob, prog_bytes, st, synth);
+    if (RB == 4 && (flags & SWF_UONLY))
+      return run_bits == 3 ? launch_sweep_r<7, 4, 1, 3, FORM_U>(amp, n, dblob, prog_bytes, st, synth)
+                           : launch_sweep_r<7, 4, 1, 5, FORM_U>(amp, n, dblob, prog_bytes, st, synth);
     return run_bits == 3 ? launch_sweep_r<7, RB, 1, 3>(amp, n, dblob, prog_bytes, st, synth)
                          : launch_sweep_r<7, RB, 1, 5>(amp, n, dblob, prog_bytes, st, synth);
   }

@@ -72,6 +72,13 @@ struct SwHeader {
 // every phase of the sweep is an H phase (OP_HPHASE): the launch may use the
 // kernel built with the H-phase path only
 constexpr uint32_t SWF_HONLY = 1u;
+// every op of the sweep is a one-qubit op without a flush (OP_U1, OP_U1R,
+// OP_U1X; controls allowed): the launch may use the kernel built with that
+// part of the interpreter only
+constexpr uint32_t SWF_UONLY = 2u;
+// Builds of the tile loop: the whole op interpreter, H phases only, plain
+// one-qubit ops only.
+enum : int { FORM_ALL = 0, FORM_H = 1, FORM_U = 2 };
 struct SwPhase {
   uint32_t lanesw[32];         // swizzled local index of the lane bits (thread bits 0..4)
   uint32_t warpsw[8];          // swizzled local index of the warp bits (thread bits 5..7)
@@ -340,6 +347,29 @@ __device__ __forceinline__ void h_phase(const uint4 hdr, const uint4* __restrict
   }
 }
 
+// The interpreter for SWF_UONLY programs: one-qubit ops (general, real, X)
+// with register, thread or non-local controls and no flush.
+template <int RB>
+__device__ __forceinline__ void exec_u(const uint4 o0, const uint4 o1, double2 (&a)[1 << RB],
+                                       const double2* __restrict__ DATA, uint32_t tid,
+                                       uint64_t base) {
+  const uint32_t type = o0.x & 0xffu, b0 = (o0.x >> 8) & 0xffu;
+  const uint32_t creg = o0.x >> 24, ctl = o0.y & 0xffu;
+  const uint64_t cnl = ((uint64_t)o1.y << 32) | o1.x;
+  if ((base & cnl) != cnl) return;
+  if ((tid & ctl) != ctl) return;
+  const double2* D = DATA + o0.z;
+  const double2 W = make_double2(1.0, 0.0);
+  const double2* F = nullptr;
+  if (type == OP_U1) {
+    DQ_SW_U1(0, 0)
+  } else if (type == OP_U1R) {
+    DQ_SW_U1(1, 0)
+  } else {
+    DQ_SW_U1(3, 0)
+  }
+}
+
 template <int RB>
 __device__ __forceinline__ void exec_op(const uint4 o0, const uint4 o1, double2 (&a)[1 << RB],
                                         const double2* __restrict__ DATA,
@@ -412,8 +442,10 @@ __device__ __forceinline__ void exec_op(const uint4 o0, const uint4 o1, double2 
 // tiles prefetched while the current one is computed.
 // RUNB: the program's run_bits (5 or 3), fixed at compile time.  HONLY: the
 // program's phases are all H phases (SWF_HONLY), so the generic op
-// interpreter is left out of the build.
-template <int TB, int RB, int S, int RUNB, bool HONLY = false>
+// interpreter is left out of the build.  FORM: FORM_H for SWF_HONLY programs
+// (no op interpreter), FORM_U for SWF_UONLY programs (the one-qubit part of
+// it), FORM_ALL otherwise.
+template <int TB, int RB, int S, int RUNB, int FORM = FORM_ALL>
 __device__ __forceinline__ void sweep_tiles(double2* __restrict__ state, const uint8_t* prog,
                                             uint32_t ntiles, long long synth, double2* bufs,
                                             double2* slots, uint32_t first_tile, uint32_t tile_step) {
@@ -562,8 +594,19 @@ __device__ __forceinline__ void sweep_tiles(double2* __restrict__ state, const u
         c0 = OP4[2 * ob];
         c1 = OP4[2 * ob + 1];
       }
-      if constexpr (HONLY) {
+      if constexpr (FORM == FORM_H) {
         h_phase<RB>(c0, OP4 + 2 * ob + 2, a, DATA, slots, tid);
+      } else if constexpr (FORM == FORM_U) {
+        for (uint32_t o = ob; o < oe; ++o) {
+          uint4 n0 = c0, n1 = c1;
+          if (o + 1 < oe) {
+            n0 = OP4[2 * o + 2];
+            n1 = OP4[2 * o + 3];
+          }
+          exec_u<RB>(c0, c1, a, DATA, tid, base);
+          c0 = n0;
+          c1 = n1;
+        }
       } else if (ob < oe && (c0.x & 0xffu) == OP_HPHASE) {
         h_phase<RB>(c0, OP4 + 2 * ob + 2, a, DATA, slots, tid);
       } else {
