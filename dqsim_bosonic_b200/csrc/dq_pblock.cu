@@ -29,6 +29,13 @@ namespace {
 
 constexpr uint32_t kMergeMaxBytes = (kMaxQubits + 7) / 8;  // index bytes of a merged state
 
+// Merged element i = a[la(i)] * b[lb(i)], the gather offsets la / lb the OR of
+// one table entry per index byte.  A warp writes runs of 256 consecutive
+// elements (one value of the high index bytes, looked up once per run); each
+// lane keeps the low-byte entries of its 8 elements of a run (lane + 32 k) in
+// registers for the whole launch, so a run costs it 8 independent gathers,
+// products and stores.  States of fewer than 256 amplitudes take one thread
+// per element.
 __global__ void __launch_bounds__(256) k_block_merge(double2* __restrict__ out, uint64_t len,
                                                      const double2* __restrict__ a,
                                                      const double2* __restrict__ b,
@@ -37,15 +44,36 @@ __global__ void __launch_bounds__(256) k_block_merge(double2* __restrict__ out, 
   __shared__ ulonglong2 tab[kMergeMaxBytes][256];
   for (uint32_t t = threadIdx.x; t < nbytes * 256u; t += blockDim.x) tab[t >> 8][t & 255u] = gtab[t];
   __syncthreads();
-  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < len; i += stride) {
+  if (len < 256) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < len;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+      const ulonglong2 e = tab[0][i];
+      out[i] = cmul_x(a[e.x], b[e.y]);
+    }
+    return;
+  }
+  const uint32_t lane = threadIdx.x & 31u;
+  ulonglong2 lo[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) lo[k] = tab[0][lane + 32u * k];
+  const uint64_t nruns = len >> 8;
+  const uint64_t wstride = (uint64_t)gridDim.x * (blockDim.x >> 5);
+  for (uint64_t r = (uint64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); r < nruns; r += wstride) {
     uint64_t la = 0, lb = 0;
-    for (uint32_t c = 0; c < nbytes; ++c) {
-      const ulonglong2 e = tab[c][(i >> (8u * c)) & 255u];
+    for (uint32_t c = 1; c < nbytes; ++c) {
+      const ulonglong2 e = tab[c][(r >> (8u * (c - 1u))) & 255u];
       la |= e.x;
       lb |= e.y;
     }
-    out[i] = cmul_x(a[la], b[lb]);
+    double2* o = out + (r << 8) + lane;
+    double2 x[8], y[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      x[k] = a[la | lo[k].x];
+      y[k] = b[lb | lo[k].y];
+    }
+#pragma unroll
+    for (int k = 0; k < 8; ++k) o[32 * k] = cmul_x(x[k], y[k]);
   }
 }
 
@@ -134,7 +162,13 @@ int dq_block_merge(dq_state_t a, const uint32_t* a_qubits, uint32_t na, dq_state
     // persistent CTAs: every CTA stages the gather tables once (up to 20 KB)
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, out->device);
-    const unsigned grid = std::min<unsigned>(grid_for(out->len, 256, out->device), (unsigned)sms * 8u);
+    // persistent CTAs (as many as are resident), one warp per run of 256
+    // elements at most
+    int per_sm = 1;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_block_merge, 256, 0);
+    const uint64_t runs = out->len >> 8;
+    const unsigned grid = std::min<unsigned>((unsigned)std::max<uint64_t>(1, (runs + 7) / 8),
+                                             (unsigned)sms * (unsigned)std::max(per_sm, 1));
     k_block_merge<<<grid, 256, 0, out->stream>>>(out->amp, out->len, a->amp, b->amp, d_tab, nbytes);
     e = cudaGetLastError();
   }
