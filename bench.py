@@ -358,6 +358,10 @@ def profile_case(spec: str) -> None:
             tm = {}
             adjoint_gradient(c, theta, H, device=0, timing=tm)
         print(f"adjoint n={n} " + " ".join(f"{k}={v}" for k, v in tm.items()))
+    elif kind == "merge":
+        n = int(rest[0])
+        r = pblock_merge_section(0, n)
+        print(f"merge n={n} ms={r['ms']:.4f} frac={r['roofline']['frac']:.4f}")
     else:
         raise SystemExit(f"unknown profile case {spec!r}")
 
@@ -382,8 +386,10 @@ def main():
     ap.add_argument("--profile-case", default=None,
                     help="run one small case of one kernel for a profiler and exit: "
                          "ragged:<n>:<items> (run_batch over the first <items> items of <n> "
-                         "qubits of the 1024-circuit ragged set, twice) or adjoint:<n> "
-                         "(two adjoint gradients of the 16-layer ansatz on <n> qubits)")
+                         "qubits of the 1024-circuit ragged set, twice), adjoint:<n> "
+                         "(two adjoint gradients of the 16-layer ansatz on <n> qubits) or "
+                         "merge:<n> (the merge section's 3 warm-up and 5 timed block merges "
+                         "into an <n>-qubit block)")
     args = ap.parse_args()
     if args.profile_case:
         profile_case(args.profile_case)
