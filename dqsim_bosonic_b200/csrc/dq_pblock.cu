@@ -17,6 +17,8 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <string.h>
+
 #include <string>
 #include <vector>
 
@@ -153,27 +155,33 @@ int dq_block_merge(dq_state_t a, const uint32_t* a_qubits, uint32_t na, dq_state
   }
   out->lazy_basis = -1;
   reset_perm(out);
-  ulonglong2* d_tab = nullptr;
-  DQ_CUDA_TRY(cudaMallocAsync((void**)&d_tab, sizeof(ulonglong2) * tab.size(), out->stream));
+  // the tables go through the merged state's query buffers (pinned host and
+  // device, kept by the handle): the call allocates nothing once they exist
+  const size_t tab_bytes = sizeof(ulonglong2) * tab.size();
+  DQ_TRY(ensure_query_buffers(out, tab_bytes, tab_bytes));
+  memcpy(out->q_host, tab.data(), tab_bytes);
+  ulonglong2* d_tab = reinterpret_cast<ulonglong2*>(out->q_dev);
   int rc = DQ_OK;
-  cudaError_t e = cudaMemcpyAsync(d_tab, tab.data(), sizeof(ulonglong2) * tab.size(),
-                                  cudaMemcpyHostToDevice, out->stream);
+  cudaError_t e = cudaMemcpyAsync(d_tab, out->q_host, tab_bytes, cudaMemcpyHostToDevice, out->stream);
   if (e == cudaSuccess) {
-    // persistent CTAs: every CTA stages the gather tables once (up to 20 KB)
-    int sms = 148;
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, out->device);
     // persistent CTAs (as many as are resident), one warp per run of 256
     // elements at most
-    int per_sm = 1;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_block_merge, 256, 0);
+    static int per_sm[64];
+    int& r = per_sm[out->device & 63];
+    if (r == 0) {
+      int v = 1;
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, k_block_merge, 256, 0);
+      r = v < 1 ? 1 : v;
+    }
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, out->device);
     const uint64_t runs = out->len >> 8;
     const unsigned grid = std::min<unsigned>((unsigned)std::max<uint64_t>(1, (runs + 7) / 8),
-                                             (unsigned)sms * (unsigned)std::max(per_sm, 1));
+                                             (unsigned)sms * (unsigned)r);
     k_block_merge<<<grid, 256, 0, out->stream>>>(out->amp, out->len, a->amp, b->amp, d_tab, nbytes);
     e = cudaGetLastError();
   }
   if (e != cudaSuccess) rc = fail(DQ_ERR_CUDA, std::string("block merge: ") + cudaGetErrorString(e));
-  cudaFreeAsync(d_tab, out->stream);
   const int rs = sync_stream(out);
   return rc != DQ_OK ? rc : rs;
 }
