@@ -422,8 +422,8 @@ int upload_terms(const dq_pauli_term* terms, uint64_t nterms, uint32_t n, cudaSt
   }
   if (g.empty()) g.push_back(PauliGroup{0, 0, 0});
   out->ngroups = (uint32_t)g.size();
-  DQ_CUDA_TRY(cudaMallocAsync((void**)&out->groups, sizeof(PauliGroup) * g.size(), st));
-  DQ_CUDA_TRY(cudaMallocAsync((void**)&out->terms, sizeof(PauliTerm) * tv.size(), st));
+  DQ_CUDA_TRY(pool_malloc_async((void**)&out->groups, sizeof(PauliGroup) * g.size(), st));
+  DQ_CUDA_TRY(pool_malloc_async((void**)&out->terms, sizeof(PauliTerm) * tv.size(), st));
   DQ_CUDA_TRY(cudaMemcpyAsync(out->groups, g.data(), sizeof(PauliGroup) * g.size(),
                               cudaMemcpyHostToDevice, st));
   DQ_CUDA_TRY(cudaMemcpyAsync(out->terms, tv.data(), sizeof(PauliTerm) * tv.size(),
@@ -577,7 +577,7 @@ int dq_adjoint(dq_state_t h, const dq_inst* prog, uint64_t ninst, const int32_t*
   double2* lam = (double2*)lam_v;
   double* slots = nullptr;
   if (rc == DQ_OK) {
-    cudaError_t e = cudaMallocAsync((void**)&slots, sizeof(double) * (nslots + 1), h->stream);
+    cudaError_t e = pool_malloc_async((void**)&slots, sizeof(double) * (nslots + 1), h->stream);
     if (e != cudaSuccess) rc = fail(DQ_ERR_OOM, std::string("cudaMallocAsync: ") + cudaGetErrorString(e));
   }
 

@@ -42,6 +42,7 @@
 #include "dq_common.cuh"
 #include "dq_engine.cuh"
 #include "dq_gates.hpp"
+#include "dq_handle.cuh"
 
 namespace dq {
 namespace {
@@ -1420,11 +1421,11 @@ int adjoint_backward_fused(double2* psi, double2* lam, uint32_t n, const dq_inst
                 std::string(what) + ": " + cudaGetErrorString(e));
     }
   };
-  cu(cudaMallocAsync((void**)&d_hdr, sizeof(ASweepHdr) * hdrs.size(), st), "cudaMallocAsync(hdr)");
-  cu(cudaMallocAsync((void**)&d_ops, sizeof(AOp) * ops.size(), st), "cudaMallocAsync(ops)");
-  cu(cudaMallocAsync((void**)&d_pool, sizeof(double2) * pool.size(), st), "cudaMallocAsync(pool)");
-  cu(cudaMallocAsync((void**)&d_map, sizeof(uint32_t) * slot_map.size(), st), "cudaMallocAsync(map)");
-  cu(cudaMallocAsync((void**)&d_part, sizeof(double) * max_partial, st), "cudaMallocAsync(partials)");
+  cu(pool_malloc_async((void**)&d_hdr, sizeof(ASweepHdr) * hdrs.size(), st), "cudaMallocAsync(hdr)");
+  cu(pool_malloc_async((void**)&d_ops, sizeof(AOp) * ops.size(), st), "cudaMallocAsync(ops)");
+  cu(pool_malloc_async((void**)&d_pool, sizeof(double2) * pool.size(), st), "cudaMallocAsync(pool)");
+  cu(pool_malloc_async((void**)&d_map, sizeof(uint32_t) * slot_map.size(), st), "cudaMallocAsync(map)");
+  cu(pool_malloc_async((void**)&d_part, sizeof(double) * max_partial, st), "cudaMallocAsync(partials)");
   if (rc == DQ_OK) {
     cu(cudaMemcpyAsync(d_hdr, hdrs.data(), sizeof(ASweepHdr) * hdrs.size(), cudaMemcpyHostToDevice, st), "copy");
     cu(cudaMemcpyAsync(d_ops, ops.data(), sizeof(AOp) * ops.size(), cudaMemcpyHostToDevice, st), "copy");
@@ -1590,12 +1591,26 @@ int adjoint_backward_batch(double2* const* psi, double2* const* lam, const std::
                 std::string(what) + ": " + cudaGetErrorString(e));
     }
   };
-  cu(cudaMalloc((void**)&d_hdr, sizeof(ASweepHdr) * hdrs.size()), "cudaMalloc(hdr)");
-  cu(cudaMalloc((void**)&d_ops, sizeof(AOp) * ops.size()), "cudaMalloc(ops)");
-  cu(cudaMalloc((void**)&d_pool, sizeof(double2) * pool.size()), "cudaMalloc(pool)");
-  cu(cudaMalloc((void**)&d_map, sizeof(uint32_t) * map.size()), "cudaMalloc(map)");
-  cu(cudaMalloc((void**)&d_part, sizeof(double) * part_per_job * max_jobs), "cudaMalloc(partials)");
-  cu(cudaMalloc((void**)&d_jobs, sizeof(AJob) * std::max<size_t>(jobs.size(), 1)), "cudaMalloc(jobs)");
+  // the device arrays come from the engine's size-keyed buffer cache: an
+  // optimiser loop repeats their sizes, so its steps pay no cudaMalloc/cudaFree
+  std::vector<std::pair<void*, size_t>> owned;
+  auto take = [&](void** p, size_t bytes) {
+    if (rc != DQ_OK) return;
+    bytes = std::max<size_t>(bytes, 16);
+    const int r = cache_alloc(device, bytes, p);
+    if (r != DQ_OK) {
+      rc = r;
+      *p = nullptr;
+      return;
+    }
+    owned.push_back({*p, bytes});
+  };
+  take((void**)&d_hdr, sizeof(ASweepHdr) * hdrs.size());
+  take((void**)&d_ops, sizeof(AOp) * ops.size());
+  take((void**)&d_pool, sizeof(double2) * pool.size());
+  take((void**)&d_map, sizeof(uint32_t) * map.size());
+  take((void**)&d_part, sizeof(double) * part_per_job * max_jobs);
+  take((void**)&d_jobs, sizeof(AJob) * std::max<size_t>(jobs.size(), 1));
   if (rc == DQ_OK) {
     for (size_t k = 0; k < kmax; ++k)
       for (size_t i = job0[k]; i < job0[k + 1]; ++i) {
@@ -1638,12 +1653,7 @@ int adjoint_backward_batch(double2* const* psi, double2* const* lam, const std::
     }
   }
   cudaStreamSynchronize(st);
-  if (d_hdr) cudaFree(d_hdr);
-  if (d_ops) cudaFree(d_ops);
-  if (d_pool) cudaFree(d_pool);
-  if (d_map) cudaFree(d_map);
-  if (d_part) cudaFree(d_part);
-  if (d_jobs) cudaFree(d_jobs);
+  for (auto& o : owned) cache_free(device, o.second, o.first);
   return rc;
 }
 

@@ -32,6 +32,39 @@ static thread_local std::string g_err;
 void set_error(const std::string& msg) { g_err = msg; }
 void clear_error() { g_err.clear(); }
 
+// ---- stream-ordered scratch ----------------------------------------------------
+// Small per-call device buffers (observable terms, sweep programs of the
+// adjoint pass, reduction workspaces) come from one memory pool per device
+// that keeps up to 256 MiB when idle: the default pool returns its memory at
+// every synchronisation, so the next call would map it again.
+cudaError_t pool_malloc_async(void** p, size_t bytes, cudaStream_t st) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  static std::mutex mu;
+  static cudaMemPool_t pools[64];
+  cudaMemPool_t pool = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    if (!pools[dev & 63]) {
+      cudaMemPoolProps props{};
+      props.allocType = cudaMemAllocationTypePinned;
+      props.location.type = cudaMemLocationTypeDevice;
+      props.location.id = dev;
+      e = cudaMemPoolCreate(&pools[dev & 63], &props);
+      if (e != cudaSuccess) {
+        pools[dev & 63] = nullptr;
+        return e;
+      }
+      uint64_t keep = 256ull << 20;
+      e = cudaMemPoolSetAttribute(pools[dev & 63], cudaMemPoolAttrReleaseThreshold, &keep);
+      if (e != cudaSuccess) return e;
+    }
+    pool = pools[dev & 63];
+  }
+  return cudaMallocFromPoolAsync(p, bytes, pool, st);
+}
+
 // ---- HBM buffer cache ---------------------------------------------------------
 // State vectors are large (16 GiB at 30 qubits); a destroyed state's buffer is
 // kept for the next state of the same size on the same device.
@@ -983,7 +1016,7 @@ int dq_inner(dq_state_t h, const double* other, uint64_t len, double* re, double
   DeviceGuard g(h->device);
   DQ_TRY(canonicalize(h));
   double2* d = nullptr;
-  DQ_CUDA_TRY(cudaMallocAsync((void**)&d, h->bytes, h->stream));
+  DQ_CUDA_TRY(pool_malloc_async((void**)&d, h->bytes, h->stream));
   int rc = DQ_OK;
   cudaError_t e = cudaMemcpyAsync(d, other, h->bytes, cudaMemcpyHostToDevice, h->stream);
   if (e != cudaSuccess) rc = fail(DQ_ERR_CUDA, cudaGetErrorString(e));

@@ -81,6 +81,11 @@ __host__ __device__ __forceinline__ uint64_t insert_zero(uint64_t k, uint32_t p)
   return ((k >> p) << (p + 1)) | (k & ((1ULL << p) - 1ULL));
 }
 
+// Stream-ordered allocation from the engine's per-device memory pool on the
+// current device (free with cudaFreeAsync); the pool keeps freed memory for
+// the next call instead of returning it at every synchronisation.
+cudaError_t pool_malloc_async(void** p, size_t bytes, cudaStream_t st);
+
 // Grid sizing: blocks for `work` items, capped at a multiple of the SM count.
 unsigned grid_for(uint64_t work, unsigned threads, int device);
 

@@ -644,7 +644,7 @@ int launch_marginal(const double2* s, uint32_t n, const uint32_t* qubits, uint32
   double* tmp = nullptr;  // allocated here only when the caller gave no workspace
   double* work = d_work;
   if (m.work && !work) {
-    DQ_CUDA_TRY(cudaMallocAsync((void**)&tmp, sizeof(double) * m.work, st));
+    DQ_CUDA_TRY(pool_malloc_async((void**)&tmp, sizeof(double) * m.work, st));
     work = tmp;
   }
   if (m.kind == 0) {
@@ -671,7 +671,7 @@ int launch_cdf(double* d, uint64_t len, double* d_work, cudaStream_t st, int dev
   double* tmp = nullptr;  // allocated here only when the caller gave no workspace
   double* sums = d_work;
   if (!sums) {
-    DQ_CUDA_TRY(cudaMallocAsync((void**)&tmp, sizeof(double) * nb, st));
+    DQ_CUDA_TRY(pool_malloc_async((void**)&tmp, sizeof(double) * nb, st));
     sums = tmp;
   }
   k_scan_sums<<<(unsigned)nb, kScanThreads, 0, st>>>(d, len, sums);

@@ -915,6 +915,7 @@ struct dq_mps_s {
   int* flags = nullptr;
   unsigned long long* svd_calls = nullptr;
   bool broken = false;       // a failed reserve lost the state: every later call fails
+  size_t buf_bytes[8] = {};  // sizes of t, dims, key, ctr, cbits, flags, svd_calls, scratch
   bool smem = true;
   uint64_t scratch_elems = 0;
   size_t work_bytes = 0;
@@ -933,16 +934,37 @@ uint32_t bond_bound(uint32_t n, uint32_t max_bond) {
   return (uint32_t)r;
 }
 
+// The batch buffers come from the engine's size-keyed device buffer cache:
+// repeated shot runs and simulations of one shape pay no cudaMalloc / cudaFree
+// (a shot run creates and destroys its handle every call).
+void** mps_buf(dq_mps_s* h, int i) {
+  void** p[8] = {(void**)&h->t, (void**)&h->dims, (void**)&h->key, (void**)&h->ctr,
+                 (void**)&h->cbits, (void**)&h->flags, (void**)&h->svd_calls, (void**)&h->scratch};
+  return p[i];
+}
+
+int mps_take(dq_mps_s* h, int i, size_t bytes) {
+  bytes = std::max<size_t>(bytes, 16);
+  void** p = mps_buf(h, i);
+  const int rc = cache_alloc(h->device, bytes, p);
+  if (rc != DQ_OK) {
+    *p = nullptr;
+    return rc;
+  }
+  h->buf_bytes[i] = bytes;
+  return DQ_OK;
+}
+
 void free_buffers(dq_mps_s* h) {
-  cudaFree(h->t);
-  cudaFree(h->dims);
-  cudaFree(h->key);
-  cudaFree(h->ctr);
-  cudaFree(h->cbits);
+  // a cached buffer may be handed out at once: nothing may still use it
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  for (int i = 0; i < 8; ++i) {
+    void** p = mps_buf(h, i);
+    if (*p) cache_free(h->device, h->buf_bytes[i], *p);
+    *p = nullptr;
+    h->buf_bytes[i] = 0;
+  }
   cudaFree(h->conds);
-  cudaFree(h->scratch);
-  cudaFree(h->flags);
-  cudaFree(h->svd_calls);
   cudaFree(h->ops);
   h->ops = nullptr;
   h->ops_cap = 0;
@@ -975,14 +997,14 @@ int alloc_buffers(dq_mps_s* h, uint32_t batch, uint32_t cap, uint32_t ncb) {
   h->smem = work_bytes <= kMaxSmem;
   h->work_bytes = work_bytes;
   h->scratch_elems = theta_elems(cap) + (h->smem ? 0 : svd_work_elems(cap));
-  DQ_CUDA_TRY(cudaMalloc((void**)&h->t, sizeof(double2) * site * h->n * batch));
-  DQ_CUDA_TRY(cudaMalloc((void**)&h->dims, sizeof(uint32_t) * (h->n + 1) * batch));
-  DQ_CUDA_TRY(cudaMalloc((void**)&h->key, sizeof(uint32_t) * 8 * batch));
-  DQ_CUDA_TRY(cudaMalloc((void**)&h->ctr, sizeof(unsigned long long) * batch));
-  DQ_CUDA_TRY(cudaMalloc((void**)&h->cbits, sizeof(int32_t) * h->ncb * batch));
-  DQ_CUDA_TRY(cudaMalloc((void**)&h->flags, sizeof(int) * 4));
-  DQ_CUDA_TRY(cudaMalloc((void**)&h->svd_calls, sizeof(unsigned long long)));
-  DQ_CUDA_TRY(cudaMalloc((void**)&h->scratch, sizeof(double2) * h->scratch_elems * h->slots * batch));
+  DQ_TRY(mps_take(h, 0, sizeof(double2) * site * h->n * batch));
+  DQ_TRY(mps_take(h, 1, sizeof(uint32_t) * (h->n + 1) * batch));
+  DQ_TRY(mps_take(h, 2, sizeof(uint32_t) * 8 * batch));
+  DQ_TRY(mps_take(h, 3, sizeof(unsigned long long) * batch));
+  DQ_TRY(mps_take(h, 4, sizeof(int32_t) * h->ncb * batch));
+  DQ_TRY(mps_take(h, 5, sizeof(int) * 4));
+  DQ_TRY(mps_take(h, 6, sizeof(unsigned long long)));
+  DQ_TRY(mps_take(h, 7, sizeof(double2) * h->scratch_elems * h->slots * batch));
   if (cap <= kWarpCap)
     DQ_CUDA_TRY(cudaFuncSetAttribute(k_mps_measure_warp, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)(kRepsPer2q * warp_measure_bytes(cap))));
@@ -1509,9 +1531,9 @@ int dq_mps_to_state(dq_mps_t h, dq_state_t out) {
   // W_k lives in `out` when n - 1 - k is even, else in tmp (both 2^n amplitudes)
   double2* tmp = nullptr;
   const size_t bytes = sizeof(double2) * (size_t)out->len;
-  if (h->n > 1) DQ_CUDA_TRY(cudaMallocAsync((void**)&tmp, bytes, h->stream));
+  if (h->n > 1) DQ_CUDA_TRY(pool_malloc_async((void**)&tmp, bytes, h->stream));
   double2* one = nullptr;
-  DQ_CUDA_TRY(cudaMallocAsync((void**)&one, sizeof(double2), h->stream));
+  DQ_CUDA_TRY(pool_malloc_async((void**)&one, sizeof(double2), h->stream));
   const double2 o = make_double2(1.0, 0.0);
   cudaError_t e = cudaMemcpyAsync(one, &o, sizeof(o), cudaMemcpyHostToDevice, h->stream);
   const double2* w = one;
