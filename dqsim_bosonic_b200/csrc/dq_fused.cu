@@ -749,14 +749,18 @@ int encode_sweep(const PSweep& sw_in, const std::vector<PGate>& G, uint32_t TBn,
           sc = true;
           continue;
         }
-        ok = x.type == OP_U1H && x.creg == 0 && x.ctl_thr == 0 && x.cnl == 0 && x.b0 == (uint32_t)k;
+        ok = (x.type == OP_U1H || x.type == OP_U1R) && x.creg == 0 && x.ctl_thr == 0 && x.cnl == 0 &&
+             x.b0 == (uint32_t)k;
         ++k;
       }
+      // the deferred scale folds into the last op, which must then be a Hadamard
+      if (sc && k >= 1 && O[ob + k - 1].type != OP_U1H) ok = false;
       if (ok && k >= 1 && k <= RB) {
         for (size_t i = ob; i < ob + k; ++i) {
           EncOp& x = O[i];
           if (!(x.flags & FL_PRE) || !(x.flags & FL_REG)) continue;
           // register-partner table entries equal to the entry of their low bits
+          // (after the op's 4 matrix entries and, with FL_THR, its 40 thread factors)
           const size_t f0 = x.data + 4 + ((x.flags & FL_THR) ? 40 : 0);
           const uint32_t lowmask = (1u << x.b0) - 1u;
           bool low = true;
@@ -831,11 +835,18 @@ int encode_sweep(const PSweep& sw_in, const std::vector<PGate>& G, uint32_t TBn,
   h.nphase = (uint32_t)P.size();
   h.nslots = (uint32_t)SL.size();
   {
-    bool honly = !P.empty();
+    // every phase a straight-line phase: Hadamard-pattern sub-ops only, or
+    // real 2x2 sub-ops only, select a restricted build
+    bool marked = !P.empty(), had = false, real = false;
     for (const SwPhase& sp : P)
-      if (sp.op_begin >= sp.op_end || O[sp.op_begin].type != OP_HPHASE) honly = false;
-    h.flags = honly ? SWF_HONLY : 0u;
-    bool uonly = !P.empty() && !honly;
+      if (sp.op_begin >= sp.op_end || O[sp.op_begin].type != OP_HPHASE) marked = false;
+    for (const EncOp& e : O) {
+      had = had || e.type == OP_U1H;
+      real = real || e.type == OP_U1R;
+    }
+    const bool honly = marked && !real;
+    h.flags = honly ? SWF_HONLY : (marked && !had ? SWF_RONLY : 0u);
+    bool uonly = !P.empty() && !marked;
     for (const EncOp& e : O)
       if (!(e.type == OP_U1 || e.type == OP_U1R || e.type == OP_U1X) || (e.flags & FL_PRE)) uonly = false;
     if (uonly) h.flags |= SWF_UONLY;
@@ -1059,6 +1070,9 @@ int launch_sweep_rb(double2* amp, uint32_t n, const uint8_t* dblob, uint32_t pro
     if (RB == 4 && (flags & SWF_HONLY))
       return run_bits == 3 ? launch_sweep_r<7, 4, 1, 3, FORM_H>(amp, n, dblob, prog_bytes, st, synth)
                            : launch_sweep_r<7, 4, 1, 5, FORM_H>(amp, n, dblob, prog_bytes, st, synth);
+    if (RB == 4 && (flags & SWF_RONLY))
+      return run_bits == 3 ? launch_sweep_r<7, 4, 1, 3, FORM_R>(amp, n, dblob, prog_bytes, st, synth)
+                           : launch_sweep_r<7, 4, 1, 5, FORM_R>(amp, n, dblob, prog_bytes, st, synth);
     if (RB == 4 && (flags & SWF_UONLY))
       return run_bits == 3 ? launch_sweep_r<7, 4, 1, 3, FORM_U>(amp, n, dblob, prog_bytes, st, synth)
                            : launch_sweep_r<7, 4, 1, 5, FORM_U>(amp, n, dblob, prog_bytes, st, synth);

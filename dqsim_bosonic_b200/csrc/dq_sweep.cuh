@@ -76,9 +76,13 @@ constexpr uint32_t SWF_HONLY = 1u;
 // OP_U1X; controls allowed): the launch may use the kernel built with that
 // part of the interpreter only
 constexpr uint32_t SWF_UONLY = 2u;
-// Builds of the tile loop: the whole op interpreter, H phases only, plain
-// one-qubit ops only.
-enum : int { FORM_ALL = 0, FORM_H = 1, FORM_U = 2 };
+// every phase of the sweep is a straight-line phase (OP_HPHASE) of real 2x2
+// sub-ops only: the launch may use the build with that path only
+constexpr uint32_t SWF_RONLY = 4u;
+// Builds of the tile loop: the whole op interpreter, Hadamard-pattern
+// straight-line phases only, plain one-qubit ops only, real-2x2 straight-line
+// phases only.
+enum : int { FORM_ALL = 0, FORM_H = 1, FORM_U = 2, FORM_R = 3 };
 struct SwPhase {
   uint32_t lanesw[32];         // swizzled local index of the lane bits (thread bits 0..4)
   uint32_t warpsw[8];          // swizzled local index of the warp bits (thread bits 5..7)
@@ -115,9 +119,10 @@ constexpr uint32_t FL_PRE = 4u;   // 1q op: flush its target first (data = 4 mat
 // register bits below its target (entries 0 .. 2^b0 - 1 hold every value)
 constexpr uint32_t FL_LOWF = 8u;
 // OP_HPHASE marks a phase whose ops are K = b1 uncontrolled Hadamard-pattern
-// ops (OP_U1H) on register bits 0, 1, ..., K-1 in that order, optionally
-// followed by the deferred OP_SCALE (flags bit 0 set, data = the scale): the
-// kernel runs them as straight-line code instead of interpreting them.
+// or real 2x2 ops (OP_U1H, OP_U1R) on register bits 0, 1, ..., K-1 in that
+// order, optionally followed by the deferred OP_SCALE when the last op is a
+// Hadamard (flags bit 0 set, data = the scale): the kernel runs them as
+// straight-line code instead of interpreting them.
 constexpr uint32_t HPH_SCALE = 1u;
 
 // ---- device helpers -------------------------------------------------------------------
@@ -260,12 +265,18 @@ __device__ __forceinline__ void u2_dispatch(double2 (&a)[1 << RB], uint32_t b0, 
 // once per distinct F entry: 2^B of them when LOWF), then the butterfly
 // (x + y', x - y').  SC: the phase's deferred scale s folds into this op as
 // (s x + y', s x - y') with s already in W (PRE 0: y' = s y).
-template <int RB, int B, int PRE, bool LOWF, bool SC>
+template <int RB, int B, int PRE, bool LOWF, bool SC, bool REAL = false>
 __device__ __forceinline__ void hph_op(double2 (&a)[1 << RB], double2 W, const double2* __restrict__ F,
-                                       double s) {
-  constexpr int NF = (PRE == 2) ? (LOWF ? (1 << B) : (1 << (RB - 1))) : 1;
+                                       double s, const double2* __restrict__ U = nullptr) {
+  double u00 = 0.0, u01 = 0.0, u10 = 0.0, u11 = 0.0;
+  if constexpr (REAL) {
+    u00 = U[0].x; u01 = U[1].x; u10 = U[2].x; u11 = U[3].x;
+  }
+  // real ops form each pair's W * F on the spot (fewer live registers next to
+  // their matrix)
+  constexpr int NF = (PRE == 2 && !REAL) ? (LOWF ? (1 << B) : (1 << (RB - 1))) : 1;
   double2 WF[NF];
-  if (PRE == 2) {
+  if (PRE == 2 && !REAL) {
 #pragma unroll
     for (int i = 0; i < NF; ++i) WF[i] = cmul_f(W, F[i]);
   }
@@ -277,13 +288,17 @@ __device__ __forceinline__ void hph_op(double2 (&a)[1 << RB], double2 W, const d
     double2 y = a[k];
     if (PRE == 2) {
       const int idx = LOWF ? (k & ((1 << B) - 1)) : (((k >> (B + 1)) << B) | (k & ((1 << B) - 1)));
-      y = cmul_f(y, WF[idx]);
+      if constexpr (REAL) y = cmul_f(y, cmul_f(W, F[idx]));
+      else y = cmul_f(y, WF[idx]);
     } else if (PRE == 1) {
       y = cmul_f(y, W);
     } else if (SC) {
       y = make_double2(y.x * s, y.y * s);
     }
-    if (SC) {
+    if constexpr (REAL) {  // real 2x2 (same arithmetic as u1_op's KIND 1)
+      a[j] = make_double2(fma(u00, x.x, u01 * y.x), fma(u00, x.y, u01 * y.y));
+      a[k] = make_double2(fma(u10, x.x, u11 * y.x), fma(u10, x.y, u11 * y.y));
+    } else if (SC) {
       a[j] = make_double2(fma(x.x, s, y.x), fma(x.y, s, y.y));
       a[k] = make_double2(fma(x.x, s, -y.x), fma(x.y, s, -y.y));
     } else {
@@ -293,17 +308,22 @@ __device__ __forceinline__ void hph_op(double2 (&a)[1 << RB], double2 W, const d
   }
 }
 
-template <int RB, int B, bool SC>
+template <int RB, int B, bool SC, bool REAL = false>
 __device__ __forceinline__ void hph_flags(double2 (&a)[1 << RB], uint32_t fl, double2 W,
-                                          const double2* __restrict__ F, double s) {
-  if (!(fl & FL_PRE)) hph_op<RB, B, 0, false, SC>(a, W, F, s);
-  else if (!(fl & FL_REG)) hph_op<RB, B, 1, false, SC>(a, W, F, s);
-  else if (fl & FL_LOWF) hph_op<RB, B, 2, true, SC>(a, W, F, s);
-  else hph_op<RB, B, 2, false, SC>(a, W, F, s);
+                                          const double2* __restrict__ F, double s,
+                                          const double2* __restrict__ U = nullptr) {
+  if (!(fl & FL_PRE)) hph_op<RB, B, 0, false, SC, REAL>(a, W, F, s, U);
+  else if (!(fl & FL_REG)) hph_op<RB, B, 1, false, SC, REAL>(a, W, F, s, U);
+  else if (fl & FL_LOWF) hph_op<RB, B, 2, true, SC, REAL>(a, W, F, s, U);
+  else hph_op<RB, B, 2, false, SC, REAL>(a, W, F, s, U);
 }
 
-// sub-op I of K (register bit I), then the rest
-template <int RB, int K, int I>
+// Sub-op kinds a build of the straight-line phases handles.
+enum : int { HPK_H = 1, HPK_R = 2, HPK_ANY = 3 };
+
+// sub-op I of K (register bit I), then the rest.  KINDS: HPK_H (Hadamard-
+// pattern sub-ops only), HPK_R (real 2x2 only) or HPK_ANY.
+template <int RB, int K, int I, int KINDS>
 __device__ __forceinline__ void hph_run(double2 (&a)[1 << RB], const uint4* __restrict__ SUB,
                                         const double2* __restrict__ DATA,
                                         const double2* __restrict__ slots, uint32_t tid, double s,
@@ -320,18 +340,24 @@ __device__ __forceinline__ void hph_run(double2 (&a)[1 << RB], const uint4* __re
         T += 40;
       }
     }
-    if (I == K - 1 && sc) {
-      W = make_double2(W.x * s, W.y * s);
-      hph_flags<RB, I, true>(a, fl, W, T, s);
+    if constexpr (KINDS == HPK_R) {
+      hph_flags<RB, I, false, true>(a, fl, W, T, s, DATA + o0.z);
     } else {
-      hph_flags<RB, I, false>(a, fl, W, T, s);
+      if (KINDS == HPK_ANY && (o0.x & 0xffu) == OP_U1R) {  // the phase's scale belongs to its H ops
+        if constexpr (KINDS == HPK_ANY) hph_flags<RB, I, false, true>(a, fl, W, T, s, DATA + o0.z);
+      } else if (I == K - 1 && sc) {
+        W = make_double2(W.x * s, W.y * s);
+        hph_flags<RB, I, true>(a, fl, W, T, s);
+      } else {
+        hph_flags<RB, I, false>(a, fl, W, T, s);
+      }
     }
-    hph_run<RB, K, I + 1>(a, SUB, DATA, slots, tid, s, sc);
+    hph_run<RB, K, I + 1, KINDS>(a, SUB, DATA, slots, tid, s, sc);
   }
 }
 
 // An OP_HPHASE marker (hdr) and its sub-ops at SUB (two uint4 per op).
-template <int RB>
+template <int RB, int KINDS = HPK_ANY>
 __device__ __forceinline__ void h_phase(const uint4 hdr, const uint4* __restrict__ SUB,
                                         double2 (&a)[1 << RB], const double2* __restrict__ DATA,
                                         const double2* __restrict__ slots, uint32_t tid) {
@@ -339,10 +365,10 @@ __device__ __forceinline__ void h_phase(const uint4 hdr, const uint4* __restrict
   const bool sc = ((hdr.y >> 8) & HPH_SCALE) != 0u;
   const double s = sc ? DATA[hdr.z].x : 1.0;
   switch (K) {
-    case 1: hph_run<RB, 1, 0>(a, SUB, DATA, slots, tid, s, sc); break;
-    case 2: if constexpr (RB >= 2) hph_run<RB, 2, 0>(a, SUB, DATA, slots, tid, s, sc); break;
-    case 3: if constexpr (RB >= 3) hph_run<RB, 3, 0>(a, SUB, DATA, slots, tid, s, sc); break;
-    case 4: if constexpr (RB >= 4) hph_run<RB, 4, 0>(a, SUB, DATA, slots, tid, s, sc); break;
+    case 1: hph_run<RB, 1, 0, KINDS>(a, SUB, DATA, slots, tid, s, sc); break;
+    case 2: if constexpr (RB >= 2) hph_run<RB, 2, 0, KINDS>(a, SUB, DATA, slots, tid, s, sc); break;
+    case 3: if constexpr (RB >= 3) hph_run<RB, 3, 0, KINDS>(a, SUB, DATA, slots, tid, s, sc); break;
+    case 4: if constexpr (RB >= 4) hph_run<RB, 4, 0, KINDS>(a, SUB, DATA, slots, tid, s, sc); break;
     default: break;
   }
 }
@@ -595,7 +621,9 @@ __device__ __forceinline__ void sweep_tiles(double2* __restrict__ state, const u
         c1 = OP4[2 * ob + 1];
       }
       if constexpr (FORM == FORM_H) {
-        h_phase<RB>(c0, OP4 + 2 * ob + 2, a, DATA, slots, tid);
+        h_phase<RB, HPK_H>(c0, OP4 + 2 * ob + 2, a, DATA, slots, tid);
+      } else if constexpr (FORM == FORM_R) {
+        h_phase<RB, HPK_R>(c0, OP4 + 2 * ob + 2, a, DATA, slots, tid);
       } else if constexpr (FORM == FORM_U) {
         for (uint32_t o = ob; o < oe; ++o) {
           uint4 n0 = c0, n1 = c1;
