@@ -859,23 +859,24 @@ int dq_adjoint_batch(int device, uint32_t n, const dq_inst* prog, uint64_t ninst
     const uint64_t g1 = std::min(nsets, g0 + G), ng = g1 - g0;
     ++acc.groups;
     // forward: sweep k of every set of the group in one launch per run width
-    struct Range { size_t begin, end; uint32_t run_bits, max_bytes; };
+    struct Range { size_t begin, end; uint32_t run_bits, max_bytes, flags; };
     std::vector<SweepJob> jobs;
     std::vector<Range> ranges;
     for (size_t k = 0; k < kf; ++k)
       for (uint32_t rbits : {5u, 3u}) {
         const size_t b0 = jobs.size();
-        uint32_t mb = 0;
+        uint32_t mb = 0, fl = ~0u;
         for (uint64_t s = g0; s < g1; ++s) {
           if (k >= plans[s].foffs.size()) continue;
           const uint8_t* hp = plans[s].fblob.data() + plans[s].foffs[k];
           if (sweep_run_bits(hp) != rbits) continue;
           const uint32_t pb = sweep_prog_bytes(hp);
           mb = std::max(mb, pb);
+          fl &= sweep_flags(hp);
           jobs.push_back(SweepJob{psi + (s - g0) * len, fblob + fbase[s] + plans[s].foffs[k],
                                   k == 0 ? (long long)plans[s].synth : -1LL, pb, 0});
         }
-        if (jobs.size() > b0) ranges.push_back(Range{b0, jobs.size(), rbits, mb});
+        if (jobs.size() > b0) ranges.push_back(Range{b0, jobs.size(), rbits, mb, fl});
       }
     if (!jobs.empty())
       cu(cudaMemcpyAsync(d_jobs, jobs.data(), sizeof(SweepJob) * jobs.size(), cudaMemcpyHostToDevice, st),
@@ -884,7 +885,7 @@ int dq_adjoint_batch(int device, uint32_t n, const dq_inst* prog, uint64_t ninst
     for (const Range& r : ranges) {
       if (rc != DQ_OK) break;
       rc = launch_sweep_multi(d_jobs + r.begin, (uint32_t)(r.end - r.begin), n, rb, r.run_bits,
-                              r.max_bytes, st);
+                              r.max_bytes, st, r.flags);
       ++acc.launches;
     }
     for (uint64_t s = g0; s < g1 && rc == DQ_OK; ++s) {

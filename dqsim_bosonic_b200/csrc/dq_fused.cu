@@ -66,8 +66,8 @@ __global__ void __launch_bounds__(1 << TB, (S == 1 && TB == 7 ? (FORM != FORM_AL
 // of chunk_tiles consecutive tiles and the CTAs take (job, chunk) work items
 // in order; a CTA stages a job's program in shared memory when it moves to
 // that job (a few KB per chunk of 2 MB of tiles).
-template <int TB, int RB, int RUNB>
-__global__ void __launch_bounds__(1 << TB, TB == 7 ? 3 : 2)
+template <int TB, int RB, int RUNB, int FORM = FORM_ALL>
+__global__ void __launch_bounds__(1 << TB, TB == 7 ? (FORM != FORM_ALL ? 4 : 3) : 2)
     k_sweep_multi(const SweepJob* __restrict__ jobs, uint32_t njobs, uint32_t nchunks,
                   uint32_t chunk_tiles, uint32_t ntiles) {
   constexpr int T = 1 << (TB + RB);
@@ -89,7 +89,7 @@ __global__ void __launch_bounds__(1 << TB, TB == 7 ? 3 : 2)
     const uint32_t c = (uint32_t)(w % nchunks);
     const uint32_t t0 = c * chunk_tiles;
     const uint32_t t1 = min(t0 + chunk_tiles, ntiles);
-    sweep_tiles<TB, RB, 1, RUNB>(J.state, sprog, t1, J.synth, bufs, slots, t0, 1);
+    sweep_tiles<TB, RB, 1, RUNB, FORM>(J.state, sprog, t1, J.synth, bufs, slots, t0, 1);
     __syncthreads();
   }
 }
@@ -1104,28 +1104,37 @@ int launch_sweep(double2* amp, uint32_t n, uint32_t TB, uint32_t RB, const uint8
   return fail(DQ_ERR_INTERNAL, "unsupported sweep geometry");
 }
 
-template <int TB, int RB, int RUNB>
+template <int TB, int RB, int RUNB, int FORM = FORM_ALL>
 int launch_sweep_multi_t(const SweepJob* d_jobs, uint32_t njobs, uint32_t n, uint32_t max_bytes,
                          cudaStream_t st) {
   constexpr int M = TB + RB;
   const size_t smem_max = sizeof(double2) * ((1u << M) + kMaxSlots) + max_prog(M);
   const size_t smem = sizeof(double2) * ((1u << M) + kMaxSlots) + max_bytes;
+  // resident CTAs per SM for this launch's shared memory, cached per 4 KB of
+  // program size (programs are mostly far below the maximum)
   static std::mutex mu;
-  static int per_sm[64];
+  static bool attr_done[64];
+  static int per_sm[64][17];
   int dev = 0;
   DQ_CUDA_TRY(cudaGetDevice(&dev));
   int resident;
   {
     std::lock_guard<std::mutex> lk(mu);
-    if (per_sm[dev & 63] == 0) {
-      DQ_CUDA_TRY(cudaFuncSetAttribute(k_sweep_multi<TB, RB, RUNB>,
+    if (!attr_done[dev & 63]) {
+      DQ_CUDA_TRY(cudaFuncSetAttribute(k_sweep_multi<TB, RB, RUNB, FORM>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_max));
-      int b = 1;
-      DQ_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_sweep_multi<TB, RB, RUNB>,
-                                                                1 << TB, smem_max));
-      per_sm[dev & 63] = b < 1 ? 1 : b;
+      attr_done[dev & 63] = true;
     }
-    resident = per_sm[dev & 63];
+    const uint32_t bucket = std::min<uint32_t>(16, (max_bytes + 4095) / 4096);
+    const size_t smem_b = std::min(smem_max, smem - max_bytes + 4096 * (size_t)bucket);
+    int& r = per_sm[dev & 63][bucket];
+    if (r == 0) {
+      int b = 1;
+      DQ_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_sweep_multi<TB, RB, RUNB, FORM>,
+                                                                1 << TB, smem_b));
+      r = b < 1 ? 1 : b;
+    }
+    resident = r;
   }
   int sms = 148;
   DQ_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
@@ -1134,7 +1143,7 @@ int launch_sweep_multi_t(const SweepJob* d_jobs, uint32_t njobs, uint32_t n, uin
   const uint32_t nchunks = (ntiles + chunk - 1) / chunk;
   const uint64_t work = (uint64_t)njobs * nchunks;
   const unsigned grid = (unsigned)std::min<uint64_t>(work, (uint64_t)sms * resident);
-  k_sweep_multi<TB, RB, RUNB><<<grid, 1 << TB, smem, st>>>(d_jobs, njobs, nchunks, chunk, ntiles);
+  k_sweep_multi<TB, RB, RUNB, FORM><<<grid, 1 << TB, smem, st>>>(d_jobs, njobs, nchunks, chunk, ntiles);
   DQ_CUDA_TRY(cudaGetLastError());
   return DQ_OK;
 }
@@ -1510,8 +1519,12 @@ uint32_t sweep_prog_bytes(const uint8_t* prog) {
   return reinterpret_cast<const SwHeader*>(prog)->prog_bytes;
 }
 
+uint32_t sweep_flags(const uint8_t* prog) {
+  return reinterpret_cast<const SwHeader*>(prog)->flags;
+}
+
 int launch_sweep_multi(const SweepJob* d_jobs, uint32_t njobs, uint32_t n, uint32_t rb,
-                       uint32_t run_bits, uint32_t max_bytes, cudaStream_t st) {
+                       uint32_t run_bits, uint32_t max_bytes, cudaStream_t st, uint32_t flags) {
   if (!njobs) return DQ_OK;
   if (n < 7 + rb) return fail(DQ_ERR_INVALID_ARG, "state smaller than a tile");
   if (max_bytes > (uint32_t)max_prog(7 + (int)rb)) return fail(DQ_ERR_INTERNAL, "sweep program too large");
@@ -1521,8 +1534,19 @@ int launch_sweep_multi(const SweepJob* d_jobs, uint32_t njobs, uint32_t n, uint3
                       : launch_sweep_multi_t<7, 2, 5>(d_jobs, njobs, n, max_bytes, st);
     case 3: return r3 ? launch_sweep_multi_t<7, 3, 3>(d_jobs, njobs, n, max_bytes, st)
                       : launch_sweep_multi_t<7, 3, 5>(d_jobs, njobs, n, max_bytes, st);
-    case 4: return r3 ? launch_sweep_multi_t<7, 4, 3>(d_jobs, njobs, n, max_bytes, st)
-                      : launch_sweep_multi_t<7, 4, 5>(d_jobs, njobs, n, max_bytes, st);
+    case 4:
+      // every job's program allows a restricted build (the flags of all of them ANDed)
+      if (flags & SWF_HONLY)
+        return r3 ? launch_sweep_multi_t<7, 4, 3, FORM_H>(d_jobs, njobs, n, max_bytes, st)
+                  : launch_sweep_multi_t<7, 4, 5, FORM_H>(d_jobs, njobs, n, max_bytes, st);
+      if (flags & SWF_RONLY)
+        return r3 ? launch_sweep_multi_t<7, 4, 3, FORM_R>(d_jobs, njobs, n, max_bytes, st)
+                  : launch_sweep_multi_t<7, 4, 5, FORM_R>(d_jobs, njobs, n, max_bytes, st);
+      if (flags & SWF_UONLY)
+        return r3 ? launch_sweep_multi_t<7, 4, 3, FORM_U>(d_jobs, njobs, n, max_bytes, st)
+                  : launch_sweep_multi_t<7, 4, 5, FORM_U>(d_jobs, njobs, n, max_bytes, st);
+      return r3 ? launch_sweep_multi_t<7, 4, 3>(d_jobs, njobs, n, max_bytes, st)
+                : launch_sweep_multi_t<7, 4, 5>(d_jobs, njobs, n, max_bytes, st);
     default: return fail(DQ_ERR_INTERNAL, "unsupported multi-sweep geometry");
   }
 }

@@ -89,12 +89,16 @@ struct SweepJob {
 
 // Runs one sweep of each of njobs states (all of n qubits, programs planned
 // with 7 thread bits, register width rb and the same run width run_bits, none
-// longer than max_bytes) in ONE launch; d_jobs is device memory.
+// longer than max_bytes) in ONE launch; d_jobs is device memory.  flags: the
+// AND of the programs' header flags (sweep_flags), which selects a restricted
+// kernel build when every program allows it.
 int launch_sweep_multi(const SweepJob* d_jobs, uint32_t njobs, uint32_t n, uint32_t rb,
-                       uint32_t run_bits, uint32_t max_bytes, cudaStream_t st);
+                       uint32_t run_bits, uint32_t max_bytes, cudaStream_t st, uint32_t flags);
 
 // The run width (5 or 3) and the size of an encoded sweep program in host memory.
 uint32_t sweep_run_bits(const uint8_t* prog);
 uint32_t sweep_prog_bytes(const uint8_t* prog);
+// The kernel-choice flags of an encoded sweep program in host memory.
+uint32_t sweep_flags(const uint8_t* prog);
 
 }  // namespace dq
