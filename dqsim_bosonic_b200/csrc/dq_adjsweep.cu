@@ -71,7 +71,8 @@ struct AOp {
   uint8_t ndq;       // A_DIAG: 1 or 2 qubits (dq[0] = MSB of the diagonal index)
   uint8_t cnt;       // A_DRUN / A_PHASE: number of ops that follow it
   uint8_t pad[2];
-  uint32_t lctrl;    // A_ONE: local control mask (tile offset bits); A_DIAG: run record (pool offset)
+  uint32_t lctrl;    // A_ONE: local control mask (tile offset bits); A_DIAG: run record (pool offset);
+                     // A_DRUN: how many of its ops touch a local qubit (those come first)
   uint32_t slot;     // first sweep-local gradient slot
   uint32_t mat;      // offset of the op's matrices in the pool (double2 units)
 };
@@ -345,12 +346,25 @@ __device__ __forceinline__ void gadd(double& g0, double& g1, double& g2, uint32_
 __device__ __noinline__ void op_drun(double2* sp, double2* sl, const AOp& hdr, const AOp* sub,
                                      const double2* pool, uint32_t m, uint64_t base, double* accw,
                                      DRec* ds) {
-  const uint32_t cnt = hdr.cnt;
+  const uint32_t cnt = hdr.cnt, nloc = hdr.lctrl;  // ops [nloc, cnt) touch non-local qubits only
+  __shared__ double s_tconst;
   for (uint32_t j = threadIdx.x; j < cnt; j += kAThreads) drec_stage(ds[j], sub[j], pool, base);
   __syncthreads();
   const uint32_t L = 1u << m;
   const uint32_t tid = threadIdx.x;
   const int lane = tid & 31, w = tid >> 5;
+  // the tile-constant phase of the ops on non-local qubits: one warp, lanes
+  // over the ops, a fixed-order butterfly (read after the barrier below)
+  if (w == 0) {
+    double t = 0.0;
+    for (uint32_t u = nloc + (uint32_t)lane; u < cnt; u += 32) {
+      const DRec& D = ds[u];
+      t += D.al + (D.p0 ? D.be : 0.0) + (D.p1 ? D.ga : 0.0) + ((D.p0 && D.p1) ? D.de : 0.0);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+    if (lane == 0) s_tconst = t;
+  }
   if (hdr.np) {
     double2 z[8];
 #pragma unroll
@@ -434,10 +448,11 @@ __device__ __noinline__ void op_drun(double2* sp, double2* sl, const AOp& hdr, c
       if (slot != 0xffffffffu) accw[slot * kAWarps + w] += contrib;
     }
   }
-  // the run's phase polynomial for this thread's eight elements
+  // the run's phase polynomial for this thread's eight elements (the ops on a
+  // local qubit; the others' constant comes from warp 0)
   double T = 0.0, G0 = 0.0, G1 = 0.0, G2 = 0.0, H01 = 0.0, H02 = 0.0, H12 = 0.0;
 #pragma unroll 2
-  for (uint32_t u = 0; u < cnt; ++u) {
+  for (uint32_t u = 0; u < nloc; ++u) {
     const DRec& D = ds[u];
     const bool r0 = D.k0 == 2, r1 = D.k1 == 2;
     const bool c0 = D.k0 == 1 ? ((tid >> D.p0) & 1u) != 0 : D.p0 != 0;
@@ -457,6 +472,8 @@ __device__ __noinline__ void op_drun(double2* sp, double2* sl, const AOp& hdr, c
       gadd(H01, H02, H12, D.p0 + D.p1 - 1u, D.de);
     }
   }
+  __syncthreads();
+  T += s_tconst;
 #pragma unroll
   for (int i = 0; i < 8; ++i) {
     const uint32_t o = tid + (uint32_t)i * kAThreads;
@@ -1256,6 +1273,18 @@ int encode_asweep(const ASweepPlan& sp, uint32_t n, ASweepHdr& hdr, std::vector<
       h.type = A_DRUN;
       h.cnt = (uint8_t)(j - i);
       for (size_t k = i; k < j; ++k) h.np = (uint8_t)(h.np | (ops[k].np ? 1 : 0));
+      // ops on a local qubit first, ops on non-local qubits only (a constant
+      // phase over a tile) last; diagonal ops commute.  lctrl = how many
+      // touch a local qubit.
+      auto local = [](const AOp& o) {
+        bool l = false;
+        for (uint32_t a = 0; a < o.ndq; ++a) l = l || (o.dq[a] & 0x80u) != 0;
+        return l;
+      };
+      std::stable_partition(ops.begin() + (ptrdiff_t)i, ops.begin() + (ptrdiff_t)j, local);
+      uint32_t nloc = 0;
+      for (size_t k = i; k < j; ++k) nloc += local(ops[k]) ? 1u : 0u;
+      h.lctrl = nloc;
       grouped.push_back(h);
     }
     for (size_t k = i; k < j; ++k) grouped.push_back(ops[k]);
