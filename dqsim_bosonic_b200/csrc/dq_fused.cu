@@ -542,10 +542,14 @@ int encode_sweep(const PSweep& sw_in, const std::vector<PGate>& G, uint32_t TBn,
   };
 
   uint32_t carry_xload = 0;
+  std::vector<uint32_t> last_tb, last_regs;  // thread / register bits of the last phase
   for (const PhaseTmp& ph : phases) {
     SwPhase sp{};
+    // spare register slots take the highest unused local bits, so that the
+    // lowest ones (qubits 0..2) stay thread bits: lanes 0..2 then cover
+    // 128-byte runs, which the last phase's direct writes need
     std::vector<uint32_t> regs = ph.regs;
-    for (uint32_t b = 0; b < m && regs.size() < RB; ++b)
+    for (uint32_t b = m; b-- > 0 && regs.size() < RB;)
       if (std::find(regs.begin(), regs.end(), b) == regs.end()) regs.push_back(b);
     std::vector<uint32_t> tb;
     for (uint32_t b = 0; b < m; ++b)
@@ -786,6 +790,8 @@ int encode_sweep(const PSweep& sw_in, const std::vector<PGate>& G, uint32_t TBn,
       carry_xload = sp.xload;
       continue;
     }
+    last_tb = tb;
+    last_regs = regs;
     P.push_back(sp);
   }
   if (SL.size() > (size_t)kMaxSlots) return fail(DQ_ERR_INTERNAL, "too many per-tile slots");
@@ -861,9 +867,25 @@ int encode_sweep(const PSweep& sw_in, const std::vector<PGate>& G, uint32_t TBn,
   const size_t dd = D.empty() ? blob.align16() : blob.put(D.data(), D.size());
   const size_t ro = blob.put(runoff.data(), runoff.size());
   const size_t rs = blob.put(runswz.data(), runswz.size());
+  // The last phase writes straight to the state when its lanes 0..2 are local
+  // bits 0..2 (qubits 0..2): every 8-lane group then writes one 128-byte run.
+  size_t go = 0;
+  if (!P.empty() && last_tb.size() >= 3 && last_tb[0] == 0 && last_tb[1] == 1 && last_tb[2] == 2 &&
+      sw.local[0] == 0 && sw.local[1] == 1 && sw.local[2] == 2) {
+    SwGStore g{};
+    for (uint32_t ln = 0; ln < 32; ++ln)
+      for (int i = 0; i < 5; ++i)
+        if ((ln >> i) & 1u) g.glane[ln] |= 1ULL << sw.local[last_tb[i]];
+    for (uint32_t wp = 0; wp < 8; ++wp)
+      for (int i = 0; i + 5 < kSwTB; ++i)
+        if ((wp >> i) & 1u) g.gwarp[wp] |= 1ULL << sw.local[last_tb[5 + i]];
+    for (uint32_t b = 0; b < RB && b < 4; ++b) g.gV[b] = 1ULL << sw.local[last_regs[b]];
+    go = blob.put(&g, 1);
+  }
   SwHeader* hp = reinterpret_cast<SwHeader*>(blob.buf.data() + hoff);
   hp->off_runoff = (uint32_t)(ro - hoff);
   hp->off_runswz = (uint32_t)(rs - hoff);
+  hp->off_gstore = go ? (uint32_t)(go - hoff) : 0u;
   hp->off_phase = (uint32_t)(po - hoff);
   hp->off_op = (uint32_t)(oo - hoff);
   hp->off_slot = (uint32_t)(so - hoff);

@@ -67,7 +67,16 @@ struct SwHeader {
   uint32_t off_runoff;         // u64 physical offset of run r (local bits run_bits..m-1 = r)
   uint32_t off_runswz;         // u32 swizzled shared-memory index of run r's first element
   uint32_t flags;              // SWF_* (host side: kernel choice)
-  uint32_t pad1;
+  uint32_t off_gstore;         // SwGStore of the last phase (0: none)
+};
+// Global offsets for the last phase to write its amplitudes straight to the
+// state (present when the phase's lanes 0..2 are local bits 0..2, i.e. each
+// 8-lane group writes one 128-byte run): element j of thread (lane, warp) is
+// at tile base + glane[lane] + gwarp[warp] + sum of gV[b] over the bits b of j.
+struct SwGStore {
+  uint64_t glane[32];
+  uint64_t gwarp[8];
+  uint64_t gV[4];
 };
 // every phase of the sweep is an H phase (OP_HPHASE): the launch may use the
 // kernel built with the H-phase path only
@@ -105,7 +114,8 @@ struct SwSlotEnt {
   uint64_t mask, pad;
   double2 w;
 };
-static_assert(sizeof(SwHeader) % 16 == 0 && sizeof(SwPhase) % 16 == 0, "layout");
+static_assert(sizeof(SwHeader) % 16 == 0 && sizeof(SwPhase) % 16 == 0 && sizeof(SwGStore) % 16 == 0,
+              "layout");
 static_assert(sizeof(SwOp) % 16 == 0 && sizeof(SwSlot) % 16 == 0 && sizeof(SwSlotEnt) % 16 == 0,
               "layout");
 
@@ -492,6 +502,8 @@ __device__ __forceinline__ void sweep_tiles(double2* __restrict__ state, const u
   const uint64_t* RUNOFF = reinterpret_cast<const uint64_t*>(prog + H->off_runoff);
   const uint32_t* RUNSWZ = reinterpret_cast<const uint32_t*>(prog + H->off_runswz);
   const uint32_t nph = H->nphase, nslots = H->nslots;
+  const SwGStore* GS =
+      (H->off_gstore && nph) ? reinterpret_cast<const SwGStore*>(prog + H->off_gstore) : nullptr;
   // element e = 32 c + lane of a tile (c: the warp's chunk) lies in run
   // e >> run_bits at offset e & (2^run_bits - 1)
   constexpr uint32_t run_bits = RUNB, cshift = 5u - RUNB;
@@ -649,6 +661,21 @@ __device__ __forceinline__ void sweep_tiles(double2* __restrict__ state, const u
           c1 = n1;
         }
       }
+      if (GS && p + 1 == nph) {
+        // the last phase writes its amplitudes straight to the state; the
+        // barrier that ends the tile orders these reads of cur before the
+        // next tile's load into it
+        const uint64_t gt = base + GS->glane[lane] + GS->gwarp[warp];
+#pragma unroll
+        for (int j = 0; j < R; ++j) {
+          uint64_t g = gt;
+#pragma unroll
+          for (int b = 0; b < RB; ++b)
+            if ((j >> b) & 1) g += GS->gV[b];
+          state[g] = a[j];
+        }
+        continue;
+      }
       const uint32_t pt2 = opaque(pt);
 #pragma unroll
       for (int b = 0; b < RB; ++b) V[b] = opaque(V[b]);
@@ -663,10 +690,12 @@ __device__ __forceinline__ void sweep_tiles(double2* __restrict__ state, const u
       __syncthreads();
     }
 
+    if (!GS) {
 #pragma unroll
-    for (int i = 0; i < NI; ++i) {
-      const uint32_t r = ((warp + (uint32_t)i * NW) << cshift) + lane_run;
-      state[base + RUNOFF[r] + lane_off] = cur[RUNSWZ[r] ^ swl];
+      for (int i = 0; i < NI; ++i) {
+        const uint32_t r = ((warp + (uint32_t)i * NW) << cshift) + lane_run;
+        state[base + RUNOFF[r] + lane_off] = cur[RUNSWZ[r] ^ swl];
+      }
     }
     base = advance(base);
     __syncthreads();

@@ -102,6 +102,8 @@ def run_sweep(state: np.ndarray, n: int, blob: bytes) -> None:
             w = np.where(hit, w * we, w)
         slots[:, s] = w
     tid = np.arange(THREADS)
+    off_gstore = struct.unpack_from("<I", blob, 108)[0] if nphase else 0
+    direct = None  # the last phase's straight-to-state writes: (global offsets, values)
     for p in range(nphase):
         po = off_phase + 192 * p
         lanesw = np.array(struct.unpack_from("<32I", blob, po), dtype=np.int64)
@@ -114,7 +116,26 @@ def run_sweep(state: np.ndarray, n: int, blob: bytes) -> None:
         a = smem[:, X ^ xload]            # X gates folded into the load address   # tiles x threads x R
         for o in range(ob, oe):
             _exec(blob, off_op + 32 * o, off_data, a, slots, base, tid, rb)
+        if off_gstore and p + 1 == nphase:
+            # like the kernel: element j of thread (lane, warp) goes to tile base +
+            # glane[lane] + gwarp[warp] + the gV of j's bits
+            glane = np.array(struct.unpack_from("<32Q", blob, off_gstore), dtype=np.uint64)
+            gwarp = np.array(struct.unpack_from("<8Q", blob, off_gstore + 256), dtype=np.uint64)
+            gV = struct.unpack_from("<4Q", blob, off_gstore + 320)[:rb]
+            gthr = glane[tid & 31] + gwarp[tid >> 5]                               # threads
+            goff = np.array([gthr + np.uint64(sum(v for b, v in enumerate(gV) if (j >> b) & 1))
+                             for j in range(R)], dtype=np.uint64).T               # threads x R
+            # the writes cover each tile element exactly once, at its own address
+            assert sorted(goff.reshape(-1).tolist()) == sorted(
+                (runoff[:, None] + lane[None, :]).reshape(-1).tolist())
+            direct = (base[:, None, None] + goff[None, :, :], a)
+            continue
         smem[:, X] = a
+    if direct is not None:
+        g, a = direct
+        assert int(g.max()) < len(state)
+        state[g.reshape(-1).astype(np.int64)] = a.reshape(-1)
+        return
     state[gidx.reshape(ntiles, -1).astype(np.int64)] = smem[:, sidx.reshape(-1)]
 
 
