@@ -10,7 +10,7 @@ import pytest
 
 import _oracle
 from _circuits import (JsonCircuit, brickwork_u3_cx, g, gate, hadamard_diagonal_circuit, hea_ansatz,
-                       qft_with_x, random_circuit)
+                       hea_param_circuit, qft_with_x, random_circuit)
 from _sweep_emu import canonical, emulate
 from dqsim_bosonic_b200 import _native as nat
 from dqsim_bosonic_b200.circuit import decode_circuit_json, encode
@@ -160,3 +160,34 @@ def test_hadamard_phases_are_marked(engine_lib):
 @pytest.mark.parametrize("n,layers,seed", [(12, 12, 1), (14, 10, 2)])
 def test_hadamard_diagonal_circuits_planned(engine_lib, n, layers, seed):
     check(hadamard_diagonal_circuit(n, layers, seed), seed)
+
+
+def test_sweep_builds_chosen_per_workload(engine_lib):
+    # header flags pick the kernel build: QFT sweeps are all Hadamard straight-line
+    # phases (SWF_HONLY = 1), u3 + cx brickwork sweeps plain one-qubit ops (SWF_UONLY = 2),
+    # the HEA forward pass real-2x2 straight-line phases (SWF_RONLY = 4) except its last
+    # sweep, which also carries the final phase flushes
+    import struct
+
+    from _sweep_emu import plan
+
+    def flags(prog):
+        blobs, _, _, _ = plan(prog)
+        return [struct.unpack_from("<I", b, 104)[0] for b in blobs], \
+               [struct.unpack_from("<I", b, 108)[0] for b in blobs]
+
+    f, g = flags(prog_of(qft_with_x(20, 3)))
+    assert f and all(x == 1 for x in f)
+    assert any(g)  # some sweeps' last phase writes straight to the state
+    f, g = flags(prog_of(brickwork_u3_cx(20, 6, 1)))
+    assert f and all(x == 2 for x in f) and any(g)
+    c, theta, _ = hea_param_circuit(16, 4, seed=1)
+
+    class P:
+        pass
+
+    p = P()
+    p.insts = c.bind(np.asarray(theta))
+    p.num_qubits, p.ninst = 16, len(p.insts)
+    f, _ = flags(p)
+    assert f[:-1] and all(x == 4 for x in f[:-1])
